@@ -1,0 +1,139 @@
+/*
+ * pvfmm.h -- C interface of the B200 particle-FMM library (libpvfmm_b200.so).
+ *
+ * The particle entry points keep the names, argument meaning and layouts of
+ * the reference C interface (dmalhotra/pvfmm include/pvfmm.h:238-303), so a
+ * caller of the reference links against this library unchanged:
+ *
+ *   positions  AoS [x1 y1 z1 x2 y2 z2 ...]
+ *   densities  [q1 ... qn] (k0 values per point: 1 for Laplace, 3 for Stokes)
+ *   outputs    n_trg x k1 values, overwritten (not accumulated)
+ *
+ * Free space only: box_size <= 0 maps the points into the unit box with the
+ * reference's bounding-box rule and rescales densities and outputs by the
+ * kernel's scale exponents (src/pvfmm-wrapper.cpp:458-541, 800-808).
+ * box_size > 0 (periodic) is rejected with an error.
+ *
+ * Errors: the reference signatures return void.  On failure an evaluation
+ * fills trg_val with NaN and records a message for PVFMMGetLastError().
+ *
+ * Threading: one CUDA stream per context; contexts are independent; calls on
+ * one context must not overlap.
+ */
+#ifndef PVFMM_B200_PVFMM_H_
+#define PVFMM_B200_PVFMM_H_
+
+#include "pvfmm_mpi_stub.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Kernel functions; values 0-5 as in the reference (include/pvfmm.h:21-28).
+ * Implemented: LaplacePotential, LaplaceGradient, StokesVelocity, and the
+ * extension LaplacePotGrad (potential and -grad in one pass, 4 outputs).
+ * The other reference values are rejected with an error. */
+enum PVFMMKernel {
+  PVFMMLaplacePotential    = 0,
+  PVFMMLaplaceGradient     = 1,
+  PVFMMStokesPressure      = 2,
+  PVFMMStokesVelocity      = 3,
+  PVFMMStokesVelocityGrad  = 4,
+  PVFMMBiotSavartPotential = 5,
+  PVFMMLaplacePotGrad      = 6   /* extension: no reference counterpart */
+};
+
+/* ---------------------------------------------------------------------------
+ * Reference entry points (include/pvfmm.h:254-301 of the reference).
+ * ------------------------------------------------------------------------- */
+
+/* Replaces PVFMMCreateContextD/F (reference include/pvfmm.h:254-255,
+ * src/pvfmm-wrapper.cpp:385-443): builds the translation operators (FP64 on
+ * the host) for kernel `kernel`, multipole order `m` (even, 2..16) and at most
+ * `n` points per leaf.  `comm` must be a single-rank communicator.  The D
+ * context evaluates in FP64 ("plain" form); the F context evaluates in the
+ * mixed form (FP32 near field, FFT and translations; FP64 pseudo-inverses). */
+void* PVFMMCreateContextD(double box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm);
+void* PVFMMCreateContextF(float box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm);
+
+/* Replaces PVFMMCreateContextDWorld/FWorld (reference include/pvfmm.h:256-257). */
+void* PVFMMCreateContextDWorld(double box_size, int n, int m, enum PVFMMKernel kernel);
+void* PVFMMCreateContextFWorld(float box_size, int n, int m, enum PVFMMKernel kernel);
+
+/* Replaces PVFMMEvalD/F (reference include/pvfmm.h:290-291,
+ * src/pvfmm-wrapper.cpp:445-811).  Host pointers.  setup=1 rebuilds the tree
+ * for new positions; setup=0 reuses it (same positions, new densities).
+ * dl_den must be NULL (double-layer sources are not implemented). */
+void PVFMMEvalD(const double* src_pos, const double* sl_den, const double* dl_den, long n_src,
+                const double* trg_pos, double* trg_val, long n_trg, const void* ctx, int setup);
+void PVFMMEvalF(const float* src_pos, const float* sl_den, const float* dl_den, long n_src,
+                const float* trg_pos, float* trg_val, long n_trg, const void* ctx, int setup);
+
+/* Replaces PVFMMDestroyContextD/F (reference include/pvfmm.h:299-300):
+ * releases the context and sets *ctx to NULL. */
+void PVFMMDestroyContextD(void** ctx);
+void PVFMMDestroyContextF(void** ctx);
+
+/* ---------------------------------------------------------------------------
+ * Extensions (no counterpart in the reference).
+ * ------------------------------------------------------------------------- */
+
+enum PVFMMPrecision {
+  PVFMMPrecisionPlain = 0,   /* FP64 everywhere */
+  PVFMMPrecisionMixed = 1    /* FP32 P2P (rsqrt + Newton, compensated sums),
+                                FP32 FFT/Hadamard, FP32-accumulated translations,
+                                FP64 pseudo-inverse precompute */
+};
+
+/* Context on double-precision inputs with an explicit precision form, so the
+ * plain and the mixed form can run on the same FP64 inputs. */
+void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision);
+
+/* Evaluation on device pointers (CUDA global memory), on `stream`
+ * (a cudaStream_t, or NULL for the context's own stream).  Returns 0 on
+ * success, nonzero on error (message in PVFMMGetLastError()). */
+int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_den, long n_src,
+                     const double* trg_pos, double* trg_val, long n_trg, int setup, void* stream);
+int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den, long n_src,
+                     const float* trg_pos, float* trg_val, long n_trg, int setup, void* stream);
+
+/* Adjoint (transposed) evaluation on the tree of the last setup=1 call:
+ * src_val[j] = sum_i K(x_i - y_j)^T trg_den[i], i.e. the FMM with densities at
+ * the targets evaluated at the sources.  Needs a symmetric kernel matrix
+ * (LaplacePotential, StokesVelocity).  Device pointers. */
+int PVFMMEvalAdjointDeviceD(const void* ctx, const double* trg_den, double* src_val, void* stream);
+int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_val, void* stream);
+
+/* Last error message of the calling thread ("" if none). */
+const char* PVFMMGetLastError(void);
+
+/* Device time in milliseconds of the stages of the last evaluation on ctx, in
+ * the order of the reference profile tags: 0 setup (tree + lists),
+ * 1 S2U, 2 U2U, 3 V-list FFT, 4 V-list Hadamard, 5 V-list IFFT, 6 X-list,
+ * 7 D2D, 8 D2T+W+U (fused near field), 9 total.  Returns the number written. */
+int PVFMMGetStageTimes(const void* ctx, double* ms, int n);
+
+/* Tree and evaluation introspection for parity tests.  `what`:
+ *   0: number of nodes            1: tree depth
+ *   2: node Morton coordinates (x, y, z, depth) as 4 x int64 per node
+ *   3: node flags (is_leaf) as int64     4: src ranges (lo, hi) x int64
+ *   5: trg ranges (lo, hi) x int64        6: parent index x int64
+ *   7: upward equivalent densities (n_nodes x ns*k0, double)
+ *   8: downward check potentials   (n_nodes x ns*k1, double)
+ *   9: source permutation (sorted -> input index) x int64
+ *  10: target permutation x int64
+ * Copies at most `n` elements into out and returns the element count needed. */
+long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
+
+/* Host precompute of one operator (FP64 row-major), for tests.  `which`:
+ * 0 UC2UE0, 1 UC2UE1, 2 DC2DE0, 3 DC2DE1, 4 U2U (8 stacked, child-major rows),
+ * 5 D2D (8 stacked, child-major columns), 6 unit surface (ns x 3),
+ * 7 V-list Hadamard operators (complex, [f][offset 26][j1 8][j2 8][k0][k1]).
+ * Returns the element count needed (copies at most n). */
+long PVFMMPrecompOperator(enum PVFMMKernel kernel, int m, int precision, int which, double* out, long n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PVFMM_B200_PVFMM_H_ */

@@ -1,0 +1,421 @@
+// C interface of libpvfmm_b200 (declared in include/pvfmm.h).
+//
+// Mirrors the particle half of the reference C interface
+// (src/pvfmm-wrapper.cpp:367-928): a context owns the operators, the device
+// buffers and the tree of the last setup; PVFMMEval* copies host arrays to
+// the device, runs the GPU pipeline and copies the values back.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../../include/pvfmm.h"
+#include "fmm_context.cuh"
+
+using namespace pvfmm_b200;
+
+namespace {
+
+constexpr unsigned int kMagic = 0x50564642u;  // "PVFB"
+
+struct Handle {
+  unsigned int magic = kMagic;
+  Context ctx;
+};
+
+Handle* as_handle(const void* p) {
+  Handle* h = (Handle*)p;
+  if (!h || h->magic != kMagic) throw std::runtime_error("invalid PVFMM context pointer");
+  return h;
+}
+
+void destroy_context(Context& c) {
+  cudaSetDevice(c.device);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  DevBuf* bufs[] = {&c.dops.uc2ue0, &c.dops.uc2ue1, &c.dops.dc2de0, &c.dops.dc2de1, &c.dops.u2u, &c.dops.d2d,
+                    &c.dops.vop, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den, &c.pot, &c.ue, &c.dc,
+                    &c.uc_c, &c.tmp_c, &c.de_c, &c.spec_in, &c.spec_out, &c.scratch, &c.scratch2, &c.io_src,
+                    &c.io_trg, &c.io_den, &c.io_val, &c.stat};
+  for (DevBuf* b : bufs) b->release();
+  for (auto& b : c.t) b.release();
+  for (auto& b : c.lvlR) b.release();
+  for (auto& b : c.lvlS) b.release();
+  DevTree& T = c.tree;
+  DevBuf* tb[] = {&T.key, &T.leaf, &T.parent, &T.child0, &T.src_lo, &T.src_hi, &T.trg_lo, &T.trg_hi, &T.colleague,
+                  &T.int_idx, &T.src_perm, &T.trg_perm, &T.src_key, &T.trg_key, &T.src_leaf, &T.trg_leaf, &T.sx,
+                  &T.sy, &T.sz, &T.tx, &T.ty, &T.tz, &T.sleaf, &T.tleaf, &T.vsrc, &T.vtrg, &T.node2vsrc, &T.vtab,
+                  &T.xtrg, &T.x_off, &T.x_list, &T.p_off, &T.p_list, &T.w_off, &T.w_list};
+  for (DevBuf* b : tb) b->release();
+  if (c.events_ready)
+    for (auto& e : c.ev) cudaEventDestroy(e);
+  if (c.cublas) cublasDestroy(c.cublas);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  if (c.pinned) cudaFreeHost(c.pinned);
+}
+
+void* create_context(double box_size, int n, int m, int kernel, int precision, bool float_api) {
+  try {
+    if (box_size > 0) throw std::runtime_error("periodic boundary conditions (box_size > 0) are not supported");
+    if (n < 1) throw std::runtime_error("max points per leaf must be positive");
+    KernelInfo ki;
+    if (!kernel_info(kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value " + std::to_string(kernel));
+    if (precision != 0 && precision != 1) throw std::runtime_error("unknown precision form");
+    std::unique_ptr<Handle> h(new Handle);
+    Context& c = h->ctx;
+    c.kernel = kernel;
+    c.ki = ki;
+    c.m = m;
+    c.ns = 6 * (m - 1) * (m - 1) + 2;
+    c.max_pts = n;
+    c.precision = precision;
+    c.float_api = float_api;
+    build_operators(kernel, m, precision == 1, c.hops);
+    PVFMM_CUDA_CHECK(cudaGetDevice(&c.device));
+    PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    if (cublasCreate(&c.cublas) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasCreate failed");
+    cublasSetMathMode(c.cublas, CUBLAS_PEDANTIC_MATH);
+    for (auto& e : c.ev) PVFMM_CUDA_CHECK(cudaEventCreate(&e));
+    c.events_ready = true;
+    upload_operators(c);
+    set_last_error("");
+    return h.release();
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return nullptr;
+  }
+}
+
+template <class T>
+int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const T* trg, T* val, long n_trg, int setup,
+                void* stream) {
+  try {
+    Handle* h = as_handle(ctx_);
+    Context& c = h->ctx;
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    const bool is_f = std::is_same<T, float>::value;
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user && user != c.stream) {
+      // order the context stream after the caller's stream
+      PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], user));
+      PVFMM_CUDA_CHECK(cudaStreamWaitEvent(c.stream, c.ev[11], 0));
+    }
+    if (n_trg <= 0) return 0;
+    if (n_src <= 0) {
+      PVFMM_CUDA_CHECK(cudaMemsetAsync(val, 0, (size_t)n_trg * c.ki.k1 * sizeof(T), c.stream));
+      PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+      return 0;
+    }
+    const bool alias = (src == trg) && (n_src == n_trg);
+    if (setup || !c.tree.valid) {
+      PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
+      build_tree(c, src, n_src, trg, n_trg, is_f, den != nullptr, alias);
+    } else if (c.tree.n_src != n_src || c.tree.n_trg != n_trg) {
+      throw std::runtime_error("setup=0 requires the point counts of the last setup");
+    } else {
+      PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
+    }
+    evaluate(c, den, is_f, val, is_f);
+    if (user && user != c.stream) {
+      PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[10], c.stream));
+      PVFMM_CUDA_CHECK(cudaStreamWaitEvent(user, c.ev[10], 0));
+    } else {
+      PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    }
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
+
+template <class T>
+void eval_host(const T* src_pos, const T* sl_den, const T* dl_den, long n_src, const T* trg_pos, T* trg_val, long n_trg,
+               const void* ctx_, int setup) {
+  int k1 = 1;
+  try {
+    Handle* h = as_handle(ctx_);
+    Context& c = h->ctx;
+    k1 = c.ki.k1;
+    if (dl_den) throw std::runtime_error("double-layer densities (dl_den) are not supported");
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    if (n_trg <= 0) return;
+    const bool alias = (src_pos == trg_pos) && (n_src == n_trg);
+    T* d_src = c.io_src.as<T>(std::max(n_src, 1L) * 3);
+    T* d_den = sl_den ? c.io_den.as<T>(std::max(n_src, 1L) * c.ki.k0) : nullptr;
+    T* d_trg = alias ? d_src : c.io_trg.as<T>(n_trg * 3);
+    T* d_val = c.io_val.as<T>(n_trg * c.ki.k1);
+    if (n_src > 0) {
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_src, src_pos, n_src * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+      if (sl_den)
+        PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    }
+    if (!alias) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_trg, trg_pos, n_trg * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    if (eval_device<T>(ctx_, d_src, d_den, n_src, d_trg, d_val, n_trg, setup, nullptr) != 0)
+      throw std::runtime_error(get_last_error());
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_trg * c.ki.k1 * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    set_last_error("");
+  } catch (const std::exception& e) {
+    const std::string msg = e.what();
+    if (trg_val)
+      for (long i = 0; i < n_trg * (long)k1; ++i) trg_val[i] = std::numeric_limits<T>::quiet_NaN();
+    set_last_error(msg);
+  }
+}
+
+void destroy(void** ctx) {
+  if (!ctx || !ctx[0]) return;
+  try {
+    Handle* h = as_handle(ctx[0]);
+    destroy_context(h->ctx);
+    h->magic = 0;
+    delete h;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+  }
+  ctx[0] = nullptr;
+}
+
+template <class T>
+long copy_dev(const DevBuf& b, long count, void* out, long n, cudaStream_t s) {
+  if (out && n > 0 && count > 0) {
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(out, b.ptr, std::min(count, n) * sizeof(T), cudaMemcpyDeviceToHost, s));
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+  return count;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* PVFMMCreateContextD(double box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm) {
+  (void)comm;
+  return create_context(box_size, n, m, (int)kernel, PVFMMPrecisionPlain, false);
+}
+void* PVFMMCreateContextF(float box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm) {
+  (void)comm;
+  return create_context(box_size, n, m, (int)kernel, PVFMMPrecisionMixed, true);
+}
+void* PVFMMCreateContextDWorld(double box_size, int n, int m, enum PVFMMKernel kernel) {
+  return create_context(box_size, n, m, (int)kernel, PVFMMPrecisionPlain, false);
+}
+void* PVFMMCreateContextFWorld(float box_size, int n, int m, enum PVFMMKernel kernel) {
+  return create_context(box_size, n, m, (int)kernel, PVFMMPrecisionMixed, true);
+}
+void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision) {
+  return create_context(box_size, n, m, (int)kernel, precision, false);
+}
+
+void PVFMMEvalD(const double* src_pos, const double* sl_den, const double* dl_den, long n_src, const double* trg_pos,
+                double* trg_val, long n_trg, const void* ctx, int setup) {
+  eval_host<double>(src_pos, sl_den, dl_den, n_src, trg_pos, trg_val, n_trg, ctx, setup);
+}
+void PVFMMEvalF(const float* src_pos, const float* sl_den, const float* dl_den, long n_src, const float* trg_pos,
+                float* trg_val, long n_trg, const void* ctx, int setup) {
+  eval_host<float>(src_pos, sl_den, dl_den, n_src, trg_pos, trg_val, n_trg, ctx, setup);
+}
+
+int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_den, long n_src, const double* trg_pos,
+                     double* trg_val, long n_trg, int setup, void* stream) {
+  return eval_device<double>(ctx, src_pos, sl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+}
+int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den, long n_src, const float* trg_pos,
+                     float* trg_val, long n_trg, int setup, void* stream) {
+  return eval_device<float>(ctx, src_pos, sl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+}
+
+int PVFMMEvalAdjointDeviceD(const void* ctx, const double* trg_den, double* src_val, void* stream) {
+  try {
+    Handle* h = as_handle(ctx);
+    Context& c = h->ctx;
+    if (!c.tree.valid) throw std::runtime_error("adjoint evaluation needs a prior setup=1 evaluation");
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    (void)stream;
+    evaluate_adjoint(c, trg_den, false, src_val, false);
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
+int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_val, void* stream) {
+  try {
+    Handle* h = as_handle(ctx);
+    Context& c = h->ctx;
+    if (!c.tree.valid) throw std::runtime_error("adjoint evaluation needs a prior setup=1 evaluation");
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    (void)stream;
+    evaluate_adjoint(c, trg_den, true, src_val, true);
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
+
+void PVFMMDestroyContextD(void** ctx) { destroy(ctx); }
+void PVFMMDestroyContextF(void** ctx) { destroy(ctx); }
+
+const char* PVFMMGetLastError(void) { return get_last_error(); }
+
+int PVFMMGetStageTimes(const void* ctx, double* ms, int n) {
+  try {
+    Handle* h = as_handle(ctx);
+    Context& c = h->ctx;
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    float t[10] = {0};
+    auto el = [&](int a, int b) {
+      float x = 0;
+      if (cudaEventElapsedTime(&x, c.ev[a], c.ev[b]) != cudaSuccess) x = 0;
+      return x;
+    };
+    t[0] = el(11, 0);
+    t[1] = el(1, 2);
+    t[2] = el(2, 3);
+    t[3] = el(3, 4);
+    t[4] = el(4, 5);
+    t[5] = el(5, 6);
+    t[6] = el(6, 7);
+    t[7] = el(7, 8);
+    t[8] = el(8, 9);
+    t[9] = el(11, 10);
+    const int k = std::min(n, 10);
+    for (int i = 0; i < k; ++i) ms[i] = t[i];
+    return k;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 0;
+  }
+}
+
+long PVFMMGetTreeData(const void* ctx, int what, void* out, long n) {
+  try {
+    Handle* h = as_handle(ctx);
+    Context& c = h->ctx;
+    DevTree& T = c.tree;
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    if (!T.valid) throw std::runtime_error("no tree: call an evaluation with setup=1 first");
+    const long N = T.n_nodes;
+    const int dim = c.ns * c.ki.ke;
+    auto s = c.stream;
+    switch (what) {
+      case 0:
+        if (out && n > 0) *(long long*)out = N;
+        return 1;
+      case 1:
+        if (out && n > 0) *(long long*)out = T.depth;
+        return 1;
+      case 2: {
+        std::vector<MKey> k(N);
+        PVFMM_CUDA_CHECK(cudaMemcpy(k.data(), T.key.ptr, N * sizeof(MKey), cudaMemcpyDeviceToHost));
+        if (out)
+          for (long i = 0; i < N && 4 * i + 3 < n; ++i) {
+            unsigned int X, Y, Z, d;
+            decode_key(k[i], X, Y, Z, d);
+            long long* o = (long long*)out + 4 * i;
+            o[0] = X;
+            o[1] = Y;
+            o[2] = Z;
+            o[3] = d;
+          }
+        return 4 * N;
+      }
+      case 3: {
+        std::vector<unsigned char> l(N);
+        PVFMM_CUDA_CHECK(cudaMemcpy(l.data(), T.leaf.ptr, N, cudaMemcpyDeviceToHost));
+        if (out)
+          for (long i = 0; i < N && i < n; ++i) ((long long*)out)[i] = l[i];
+        return N;
+      }
+      case 4:
+      case 5: {
+        std::vector<int> lo(N), hi(N);
+        PVFMM_CUDA_CHECK(cudaMemcpy(lo.data(), (what == 4 ? T.src_lo : T.trg_lo).ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(hi.data(), (what == 4 ? T.src_hi : T.trg_hi).ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        if (out)
+          for (long i = 0; i < N && 2 * i + 1 < n; ++i) {
+            ((long long*)out)[2 * i] = lo[i];
+            ((long long*)out)[2 * i + 1] = hi[i];
+          }
+        return 2 * N;
+      }
+      case 6: {
+        std::vector<int> p(N);
+        PVFMM_CUDA_CHECK(cudaMemcpy(p.data(), T.parent.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        if (out)
+          for (long i = 0; i < N && i < n; ++i) ((long long*)out)[i] = p[i];
+        return N;
+      }
+      case 7:
+      case 8: {
+        const long cnt = N * dim;
+        if (!out) return cnt;
+        const DevBuf& b = what == 7 ? c.ue : c.dc;
+        const long k = std::min(cnt, n);
+        if (c.precision == 0) {
+          PVFMM_CUDA_CHECK(cudaMemcpy(out, b.ptr, k * sizeof(double), cudaMemcpyDeviceToHost));
+        } else {
+          std::vector<float> f(k);
+          PVFMM_CUDA_CHECK(cudaMemcpy(f.data(), b.ptr, k * sizeof(float), cudaMemcpyDeviceToHost));
+          for (long i = 0; i < k; ++i) ((double*)out)[i] = f[i];
+        }
+        return cnt;
+      }
+      case 9:
+      case 10: {
+        const long cnt = what == 9 ? T.n_src : T.n_trg;
+        std::vector<int> p(cnt);
+        PVFMM_CUDA_CHECK(cudaMemcpy(p.data(), (what == 9 ? T.src_perm : T.trg_perm).ptr, cnt * sizeof(int), cudaMemcpyDeviceToHost));
+        if (out)
+          for (long i = 0; i < cnt && i < n; ++i) ((long long*)out)[i] = p[i];
+        return cnt;
+      }
+      default:
+        throw std::runtime_error("unknown tree data selector");
+    }
+    (void)s;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return -1;
+  }
+}
+
+long PVFMMPrecompOperator(enum PVFMMKernel kernel, int m, int precision, int which, double* out, long n) {
+  static std::mutex mu;
+  static HostOperators ops;
+  std::lock_guard<std::mutex> lock(mu);
+  try {
+    if (ops.kernel != (int)kernel || ops.m != m || ops.mixed != (precision == 1))
+      build_operators((int)kernel, m, precision == 1, ops);
+    const std::vector<double>* v = nullptr;
+    switch (which) {
+      case 0: v = &ops.uc2ue0; break;
+      case 1: v = &ops.uc2ue1; break;
+      case 2: v = &ops.dc2de0; break;
+      case 3: v = &ops.dc2de1; break;
+      case 4: v = &ops.u2u; break;
+      case 5: v = &ops.d2d; break;
+      case 6: v = &ops.usurf; break;
+      case 7: v = &ops.vop; break;
+      default: throw std::runtime_error("unknown operator selector");
+    }
+    if (out && n > 0) std::memcpy(out, v->data(), sizeof(double) * std::min<long>(n, (long)v->size()));
+    return (long)v->size();
+  } catch (const std::exception& e) {
+    ops.kernel = -1;
+    set_last_error(e.what());
+    return -1;
+  }
+}
+
+}  // extern "C"

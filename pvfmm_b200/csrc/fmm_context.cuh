@@ -1,0 +1,99 @@
+// Per-context state of libpvfmm_b200: operators on the device, the octree of
+// the last setup, interaction lists and evaluation buffers.
+#pragma once
+
+#include <cublas_v2.h>
+
+#include <array>
+#include <vector>
+
+#include "fmm_device.cuh"
+#include "fmm_host.hpp"
+
+namespace pvfmm_b200 {
+
+// Octree of the last setup=1 call, all on the device except the level table.
+// Nodes are stored level by level; each level is in Morton order and the 8
+// children of an internal node are consecutive in the next level.
+struct DevTree {
+  long n_nodes = 0;
+  int depth = 0;                      // deepest level
+  std::vector<long> level_off;        // level d occupies [level_off[d], level_off[d+1])
+  std::vector<long> n_internal;       // internal nodes per level
+  DevBuf key;                         // MKey per node
+  DevBuf leaf;                        // uint8 per node
+  DevBuf parent, child0;              // int per node (-1 if none)
+  DevBuf src_lo, src_hi, trg_lo, trg_hi;   // int per node: ranges into the sorted points
+  DevBuf colleague;                   // int[27] per node
+  DevBuf int_idx;                     // internal node ids, level by level (offsets int_off)
+  std::vector<long> int_off;
+  // point data (sorted)
+  long n_src = 0, n_trg = 0;
+  bool src_counted = true;            // false when sl_den == NULL
+  DevBuf src_perm, trg_perm;          // int: sorted index -> input index
+  DevBuf src_key, trg_key;            // MKey (sorted)
+  DevBuf src_leaf, trg_leaf;          // int: leaf node id of each sorted point
+  DevBuf sx, sy, sz, tx, ty, tz;      // Real coordinates relative to the point's leaf centre
+  // compact node lists
+  long n_sleaf = 0, n_tleaf = 0, n_vsrc = 0, n_vtrg = 0, n_xtrg = 0;
+  DevBuf sleaf, tleaf;                // leaves with sources / targets
+  DevBuf vsrc, vtrg;                  // non-leaf nodes: spectra sources / targets
+  DevBuf node2vsrc;                   // int per node (-1)
+  DevBuf vtab;                        // int[26] per vtrg: vsrc index per colleague offset (-1)
+  DevBuf xtrg;                        // target nodes with X-list entries
+  DevBuf x_off, x_list;               // CSR over xtrg
+  DevBuf p_off, p_list;               // CSR over tleaf: P2P source leaves
+  DevBuf w_off, w_list;               // CSR over tleaf: W source nodes
+  long n_p2p = 0, n_x = 0, n_w = 0;   // list sizes
+  double scale_x = 1, shift_x[3] = {0, 0, 0};
+  bool valid = false;
+};
+
+// Device copies of the operators in the working precision.
+struct DevOps {
+  DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
+  DevBuf usurf;     // ns x 3 (Real)
+  DevBuf fft_map, ifft_map;
+};
+
+struct Context {
+  int kernel = 0;
+  KernelInfo ki{};
+  int m = 0, ns = 0, max_pts = 0;
+  int precision = 0;      // 0 plain FP64, 1 mixed FP32
+  bool float_api = false; // created by the F entry points
+  HostOperators hops;
+  DevOps dops;
+  DevTree tree;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  int device = 0;
+  // evaluation buffers
+  DevBuf den;             // sorted densities (Real, n_src x k0)
+  DevBuf pot;             // sorted target values (Real, n_trg x k1)
+  DevBuf ue, dc;          // per node (Real)
+  DevBuf uc_c, tmp_c, de_c;  // compact GEMM buffers
+  DevBuf spec_in, spec_out;  // V-list spectra
+  DevBuf scratch;         // sort / scan temporaries
+  DevBuf scratch2;
+  DevBuf io_src, io_trg, io_den, io_val;  // staging for host-pointer calls
+  DevBuf stat;            // small status / reduction buffer
+  DevBuf t[24];           // temporaries of the tree build, reused across calls
+  std::vector<DevBuf> lvlR, lvlS;  // per-level internal-node keys (refined / balanced)
+  std::vector<float> stage_ms;
+  std::array<cudaEvent_t, 12> ev{};
+  bool events_ready = false;
+  // pinned host staging
+  void* pinned = nullptr;
+  size_t pinned_cap = 0;
+};
+
+// tree.cu
+void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
+                bool src_counted, bool trg_alias);
+// eval.cu
+void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
+void evaluate_adjoint(Context& ctx, const void* trg_den, bool in_float, void* src_out, bool out_float);
+void upload_operators(Context& ctx);
+
+}  // namespace pvfmm_b200

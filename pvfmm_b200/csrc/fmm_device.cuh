@@ -1,0 +1,231 @@
+// Device-side building blocks of libpvfmm_b200: Morton keys, kernel
+// functions, error handling and the per-context device buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace pvfmm_b200 {
+
+#define PVFMM_CUDA_CHECK(expr)                                                                  \
+  do {                                                                                          \
+    cudaError_t err__ = (expr);                                                                 \
+    if (err__ != cudaSuccess)                                                                   \
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(err__) + " at " \
+                               + __FILE__ + ":" + std::to_string(__LINE__));                    \
+  } while (0)
+
+constexpr int kMaxDepth = 30;          // PVFMM_MAX_DEPTH (include/pvfmm_common.hpp:29)
+constexpr double kRad0 = 1.05;         // PVFMM_RAD0
+constexpr double kRad1 = 2.95;         // PVFMM_RAD1
+constexpr uint32_t kTwo30 = 1u << 30;
+
+// ---------------------------------------------------------------------------
+// Morton keys.  The order of (hi, lo) equals MortonId::operator<
+// (reference include/mortonid.txx:107-118): the most significant differing
+// coordinate bit decides, z before y before x at equal bits; equal
+// coordinates order by depth.  hi holds coordinate bits 29..9 interleaved
+// (63 bits), lo holds bits 8..0 interleaved (27 bits) << 5 | depth.
+// ---------------------------------------------------------------------------
+struct MKey {
+  unsigned long long hi;
+  unsigned int lo;
+  unsigned int pad;
+};
+
+__host__ __device__ inline bool key_less(const MKey& a, const MKey& b) {
+  return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo);
+}
+__host__ __device__ inline bool key_eq(const MKey& a, const MKey& b) { return a.hi == b.hi && a.lo == b.lo; }
+
+__host__ __device__ inline unsigned long long spread3(unsigned int v) {  // 21 bits -> every 3rd bit
+  unsigned long long x = v & 0x1fffffu;
+  x = (x | (x << 32)) & 0x1f00000000ffffULL;
+  x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
+  x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+  x = (x | (x << 2)) & 0x1249249249249249ULL;
+  return x;
+}
+__host__ __device__ inline unsigned int compact3(unsigned long long x) {
+  x &= 0x1249249249249249ULL;
+  x = (x | (x >> 2)) & 0x10c30c30c30c30c3ULL;
+  x = (x | (x >> 4)) & 0x100f00f00f00f00fULL;
+  x = (x | (x >> 8)) & 0x1f0000ff0000ffULL;
+  x = (x | (x >> 16)) & 0x1f00000000ffffULL;
+  x = (x | (x >> 32)) & 0x1fffffULL;
+  return (unsigned int)x;
+}
+
+__host__ __device__ inline MKey make_key(unsigned int X, unsigned int Y, unsigned int Z, unsigned int depth) {
+  MKey k;
+  k.hi = spread3(X >> 9) | (spread3(Y >> 9) << 1) | (spread3(Z >> 9) << 2);
+  const unsigned long long l = spread3(X & 511u) | (spread3(Y & 511u) << 1) | (spread3(Z & 511u) << 2);
+  k.lo = (unsigned int)((l << 5) | depth);
+  k.pad = 0;
+  return k;
+}
+
+__host__ __device__ inline void decode_key(const MKey& k, unsigned int& X, unsigned int& Y, unsigned int& Z,
+                                           unsigned int& depth) {
+  const unsigned long long l = k.lo >> 5;
+  X = (compact3(k.hi) << 9) | compact3(l);
+  Y = (compact3(k.hi >> 1) << 9) | compact3(l >> 1);
+  Z = (compact3(k.hi >> 2) << 9) | compact3(l >> 2);
+  depth = k.lo & 31u;
+}
+
+// Key larger than every point in node (X,Y,Z,d) and smaller than every key
+// after the node's subtree.
+__host__ __device__ inline MKey node_end_key(unsigned int X, unsigned int Y, unsigned int Z, unsigned int d) {
+  const unsigned int w = kTwo30 >> d;
+  return make_key(X + w - 1, Y + w - 1, Z + w - 1, 31);
+}
+
+// First index i in sorted [0,n) with !(a[i] < k).
+__device__ inline long lower_bound_key(const MKey* a, long n, const MKey& k) {
+  long lo = 0, hi = n;
+  while (lo < hi) {
+    const long mid = (lo + hi) >> 1;
+    if (key_less(a[mid], k)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Reciprocal square root.  FP64: FP32 hardware estimate refined by two
+// Newton-Raphson steps y <- y (3/2 - r2 y^2 / 2) in FP64 (full double accuracy
+// is reached after two steps from a 2^-22 estimate); tiny r2 outside the FP32
+// range take the FP64 library rsqrt.  FP32: hardware estimate + one Newton
+// step.  r2 == 0 gives 0 (the kernels' mask, kernel.txx:1283).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rsqrt_nr(double r2) {
+  if (r2 < 1e-30) return r2 > 0 ? rsqrt(r2) : 0.0;
+  double y = (double)rsqrtf((float)r2);
+  const double h = 0.5 * r2;
+  y = y * (1.5 - h * y * y);
+  y = y * (1.5 - h * y * y);
+  return y;
+}
+__device__ __forceinline__ float rsqrt_nr(float r2) {
+  if (!(r2 > 0.f)) return 0.f;
+  float y = rsqrtf(r2);
+  y = y * (1.5f - 0.5f * r2 * y * y);
+  return y;
+}
+
+// Accumulator: plain sum in FP64; Kahan-compensated sum in FP32.
+template <class Real>
+struct Acc {
+  Real s;
+  __device__ __forceinline__ void init() { s = 0; }
+  __device__ __forceinline__ void add(Real v) { s += v; }
+  __device__ __forceinline__ Real get() const { return s; }
+};
+template <>
+struct Acc<float> {
+  float s, c;
+  __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
+  __device__ __forceinline__ void add(float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ float get() const { return s; }
+};
+
+// ---------------------------------------------------------------------------
+// Kernel functions (reference include/kernel.txx:1276-1364), unscaled: the
+// 1/(4 pi) or 1/(8 pi) factor is applied once to the summed result, as
+// GenericKernel::Eval does after each source block (kernel.txx:1243-1246).
+// KS: number of source components, KT: number of target components.
+// ---------------------------------------------------------------------------
+enum KerType { kKerLaplace = 0, kKerLaplaceGrad = 1, kKerStokes = 2, kKerLaplacePG = 3 };
+
+template <int KT>
+struct KerTraits;
+
+template <int Ker>
+struct KerDims;
+template <>
+struct KerDims<kKerLaplace> { static constexpr int KS = 1, KT = 1; };
+template <>
+struct KerDims<kKerLaplaceGrad> { static constexpr int KS = 1, KT = 3; };
+template <>
+struct KerDims<kKerStokes> { static constexpr int KS = 3, KT = 3; };
+template <>
+struct KerDims<kKerLaplacePG> { static constexpr int KS = 1, KT = 4; };
+
+// Adds K(r) f to u (r = target - source).
+template <int Ker, class Real>
+__device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* f, Acc<Real>* u) {
+  const Real r2 = rx * rx + ry * ry + rz * rz;
+  const Real rinv = rsqrt_nr(r2);
+  if constexpr (Ker == kKerLaplace) {
+    u[0].add(rinv * f[0]);
+  } else if constexpr (Ker == kKerLaplaceGrad) {
+    const Real fr3 = rinv * rinv * rinv * f[0];
+    u[0].add(rx * fr3);
+    u[1].add(ry * fr3);
+    u[2].add(rz * fr3);
+  } else if constexpr (Ker == kKerLaplacePG) {
+    const Real fr = rinv * f[0];
+    const Real fr3 = rinv * rinv * fr;
+    u[0].add(fr);
+    u[1].add(rx * fr3);
+    u[2].add(ry * fr3);
+    u[3].add(rz * fr3);
+  } else {  // Stokes velocity
+    const Real rinv2 = rinv * rinv;
+    const Real ip = (f[0] * rx + f[1] * ry + f[2] * rz) * rinv2;
+    u[0].add(rinv * (f[0] + rx * ip));
+    u[1].add(rinv * (f[1] + ry * ip));
+    u[2].add(rinv * (f[2] + rz * ip));
+  }
+}
+
+__host__ __device__ constexpr double ker_scale(int ker) {
+  return ker == kKerStokes ? 1.0 / (8 * 3.14159265358979323846) : 1.0 / (4 * 3.14159265358979323846);
+}
+
+// ---------------------------------------------------------------------------
+// Reusable device buffer: grows, never shrinks, freed with the context.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  void* ensure(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (bytes > cap) {
+      if (ptr) PVFMM_CUDA_CHECK(cudaFree(ptr));
+      ptr = nullptr;
+      cap = 0;
+      PVFMM_CUDA_CHECK(cudaMalloc(&ptr, bytes));
+      cap = bytes;
+    }
+    return ptr;
+  }
+  template <class T>
+  T* as(size_t n) {
+    return static_cast<T*>(ensure(n * sizeof(T)));
+  }
+  template <class T>
+  T* get() const {
+    return static_cast<T*>(ptr);
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+inline unsigned int ceil_div(long a, long b) { return (unsigned int)((a + b - 1) / b); }
+
+}  // namespace pvfmm_b200

@@ -1,0 +1,68 @@
+// Host-side declarations shared by the precompute, the tree/evaluation driver
+// and the C interface of libpvfmm_b200.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace pvfmm_b200 {
+
+// Kernel ids follow the PVFMMKernel enum (reference include/pvfmm.h:21-28),
+// plus 6 = Laplace potential+gradient.
+enum KernelId { kLaplacePot = 0, kLaplaceGrad = 1, kStokesVel = 3, kLaplacePotGrad = 6 };
+
+// Expansion kernels (the k_s2m/k_m2m/k_m2l/k_l2l sub-kernels of
+// include/kernel.txx:1333-1344, 1475-1479).
+enum ExpKernel { kExpLaplace = 0, kExpStokes = 1 };
+
+struct KernelInfo {
+  int id;
+  const char* name;        // reference ker_name (kernel.txx:1334, 1341, 1476)
+  int k0, k1;              // source / target dims of the s2t kernel
+  int exp_kernel;          // ExpKernel of the expansions
+  int ke;                  // dims of the expansion kernel (ke x ke)
+  double src_scal[3];      // scale exponents of the s2t kernel (kernel.txx:64-196)
+  double trg_scal[4];
+  int flops;               // per-pair flop count convention (kernel.txx:1277,1317,1352)
+};
+
+bool kernel_info(int id, KernelInfo* out);
+
+// Level-0 operators of one kernel and multipole order.  All FP64, row-major,
+// row-vector convention (out_row = in_row * M), as in fmm_pts.txx:453-764.
+struct HostOperators {
+  int kernel = -1, m = 0, ns = 0, ke = 1, n1 = 0, n3 = 0, n3h = 0;
+  bool mixed = false;
+  std::vector<double> usurf;            // ns x 3 unit cube-surface points u in [-1,1]^3
+  std::vector<double> uc2ue0, uc2ue1;   // (ns*ke) x (ns*ke): check -> equivalent factors
+  std::vector<double> dc2de0, dc2de1;
+  std::vector<double> u2u;              // (8*ns*ke) x (ns*ke), row block c = child octant c
+  std::vector<double> d2d;              // (ns*ke) x (8*ns*ke), column block c = child octant c
+  std::vector<double> vop;              // complex (re,im): [n3h][26][8][8][ke][ke]
+  std::vector<int> fft_map, ifft_map;   // ns grid indices (x + n1*y + n1*n1*z)
+};
+
+// Builds the operators.  `mixed` selects the pseudo-inverse cutoff of the
+// mixed form: singular values below 4*eps32*max are dropped (the cutoff the
+// reference's float build uses), otherwise 4*eps64*max (fmm_pts.txx:496-504).
+void build_operators(int kernel, int m, bool mixed, HostOperators& ops);
+
+// One-sided Jacobi SVD of a rows x cols row-major matrix (rows >= cols):
+// A = U diag(S) V^T with U rows x cols (column j scaled to unit length, or
+// zero when S_j == 0), V cols x cols.  Public for the CPU tests.
+void jacobi_svd(int rows, int cols, const double* A, std::vector<double>& U, std::vector<double>& S,
+                std::vector<double>& V);
+
+// FP64 kernel matrix, BuildMatrix layout (kernel.txx:1059-1135):
+// M[i*k0+j][t*k1+k] = K_jk(trg_t - src_i), r == 0 gives 0.
+void exp_kernel_matrix(int exp_kernel, const double* src, int n_src, const double* trg, int n_trg,
+                       double* M);
+
+// Unit surface of PVFMM's surface() (fmm_pts.txx:54-97) as u in [-1,1]^3.
+std::vector<double> unit_surface(int m);
+
+void set_last_error(const std::string& msg);
+const char* get_last_error();
+
+}  // namespace pvfmm_b200

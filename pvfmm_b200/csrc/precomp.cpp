@@ -1,0 +1,363 @@
+// Host FP64 precompute of the translation operators.
+//
+// Follows FMM_Pts::Precomp (reference include/fmm_pts.txx:453-764):
+//   UC2UE0/1, DC2DE0/1  pseudo-inverse factors of the equivalent->check kernel
+//                       matrices, by SVD with the 4*eps*max(S) cutoff (:478-581)
+//   U2U, D2D            child<->parent translations (:582-643), one per octant
+//   V / V1              kernel on the (2m)^3 convolution grid, r2c DFT, and the
+//                       8x8 child blocks per parent offset divided by n3 (:671-764)
+// Scale invariance (all expansion kernels here are homogeneous of degree -1
+// with uniform exponents src=0, trg=1) makes the level-0 operators valid on
+// every level; the level factors are applied at evaluation time.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <stdexcept>
+
+#include "fmm_host.hpp"
+
+namespace pvfmm_b200 {
+
+namespace {
+constexpr double kRad0 = 1.05;  // PVFMM_RAD0 (include/pvfmm_common.hpp:33)
+constexpr double kRad1 = 2.95;  // PVFMM_RAD1 (include/pvfmm_common.hpp:34)
+constexpr double kPi = 3.14159265358979323846;
+
+thread_local std::string g_last_error;
+
+// Row-major dense product C = A(r x k) * B(k x c).
+std::vector<double> matmul(const std::vector<double>& A, const std::vector<double>& B, int r, int k, int c) {
+  std::vector<double> C((size_t)r * c, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < r; ++i) {
+    double* ci = &C[(size_t)i * c];
+    for (int l = 0; l < k; ++l) {
+      const double a = A[(size_t)i * k + l];
+      if (a == 0.0) continue;
+      const double* bl = &B[(size_t)l * c];
+      for (int j = 0; j < c; ++j) ci[j] += a * bl[j];
+    }
+  }
+  return C;
+}
+
+// Points center + half*rad*u for the unit surface u.
+std::vector<double> place_surface(const std::vector<double>& u, const double* center, double half, double rad) {
+  std::vector<double> p(u.size());
+  for (size_t i = 0; i < u.size() / 3; ++i)
+    for (int d = 0; d < 3; ++d) p[i * 3 + d] = center[d] + half * rad * u[i * 3 + d];
+  return p;
+}
+
+// Pseudo-inverse factors (fmm_pts.txx:478-537): for M (rows x cols) = U S V^T,
+// C2E0 = V S^+ (cols x cols), C2E1 = U^T (cols x rows).
+void pinv_factors(const std::vector<double>& M, int rows, int cols, double eps, std::vector<double>& c2e0,
+                  std::vector<double>& c2e1) {
+  std::vector<double> U, S, V;
+  jacobi_svd(rows, cols, M.data(), U, S, V);
+  double smax = 0;
+  for (double s : S) smax = std::max(smax, std::fabs(s));
+  const double cut = eps * smax * 4;
+  c2e0.assign((size_t)cols * cols, 0.0);
+  for (int r = 0; r < cols; ++r)
+    for (int j = 0; j < cols; ++j) c2e0[(size_t)r * cols + j] = (S[j] > cut) ? V[(size_t)r * cols + j] / S[j] : 0.0;
+  c2e1.assign((size_t)cols * rows, 0.0);
+  for (int j = 0; j < cols; ++j)
+    for (int r = 0; r < rows; ++r) c2e1[(size_t)j * rows + r] = U[(size_t)r * cols + j];
+}
+
+// 1D complex DFT of length n along a strided line, sign -1 (forward).
+void dft_line(std::complex<double>* x, int n, int stride, const std::vector<std::complex<double>>& w,
+              std::vector<std::complex<double>>& tmp) {
+  for (int k = 0; k < n; ++k) {
+    std::complex<double> s = 0;
+    for (int j = 0; j < n; ++j) s += x[(size_t)j * stride] * w[(size_t)(k * j) % n];
+    tmp[k] = s;
+  }
+  for (int k = 0; k < n; ++k) x[(size_t)k * stride] = tmp[k];
+}
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* get_last_error() { return g_last_error.c_str(); }
+
+bool kernel_info(int id, KernelInfo* out) {
+  KernelInfo k{};
+  switch (id) {
+    case kLaplacePot:
+      k = {id, "laplace", 1, 1, kExpLaplace, 1, {0, 0, 0}, {1, 0, 0, 0}, 9};
+      break;
+    case kLaplaceGrad:
+      k = {id, "laplace_grad", 1, 3, kExpLaplace, 1, {0, 0, 0}, {2, 2, 2, 0}, 16};
+      break;
+    case kStokesVel:
+      k = {id, "stokes_vel", 3, 3, kExpStokes, 3, {0, 0, 0}, {1, 1, 1, 0}, 29};
+      break;
+    case kLaplacePotGrad:
+      k = {id, "laplace_potgrad", 1, 4, kExpLaplace, 1, {0, 0, 0}, {1, 2, 2, 2}, 18};
+      break;
+    default:
+      return false;
+  }
+  if (out) *out = k;
+  return true;
+}
+
+std::vector<double> unit_surface(int p) {
+  // Same point order as surface() (fmm_pts.txx:54-97), unscaled.
+  const int n = 6 * (p - 1) * (p - 1) + 2;
+  std::vector<double> c((size_t)n * 3);
+  c[0] = c[1] = c[2] = -1.0;
+  int cnt = 1;
+  for (int i = 0; i < p - 1; ++i)
+    for (int j = 0; j < p - 1; ++j, ++cnt) {
+      c[cnt * 3 + 0] = -1;
+      c[cnt * 3 + 1] = (2.0 * (i + 1) - p + 1) / (p - 1);
+      c[cnt * 3 + 2] = (2.0 * j - p + 1) / (p - 1);
+    }
+  for (int i = 0; i < p - 1; ++i)
+    for (int j = 0; j < p - 1; ++j, ++cnt) {
+      c[cnt * 3 + 0] = (2.0 * i - p + 1) / (p - 1);
+      c[cnt * 3 + 1] = -1;
+      c[cnt * 3 + 2] = (2.0 * (j + 1) - p + 1) / (p - 1);
+    }
+  for (int i = 0; i < p - 1; ++i)
+    for (int j = 0; j < p - 1; ++j, ++cnt) {
+      c[cnt * 3 + 0] = (2.0 * (i + 1) - p + 1) / (p - 1);
+      c[cnt * 3 + 1] = (2.0 * j - p + 1) / (p - 1);
+      c[cnt * 3 + 2] = -1;
+    }
+  for (int i = 0; i < (n / 2) * 3; ++i) c[(size_t)cnt * 3 + i] = -c[i];
+  return c;
+}
+
+void exp_kernel_matrix(int exp_kernel, const double* src, int n_src, const double* trg, int n_trg, double* M) {
+  if (exp_kernel == kExpLaplace) {
+    const double s = 1.0 / (4 * kPi);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_src; ++i)
+      for (int t = 0; t < n_trg; ++t) {
+        const double dx = trg[t * 3] - src[i * 3], dy = trg[t * 3 + 1] - src[i * 3 + 1],
+                     dz = trg[t * 3 + 2] - src[i * 3 + 2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        M[(size_t)i * n_trg + t] = r2 > 0 ? s / std::sqrt(r2) : 0.0;
+      }
+  } else {
+    const double s = 1.0 / (8 * kPi);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_src; ++i)
+      for (int t = 0; t < n_trg; ++t) {
+        const double r[3] = {trg[t * 3] - src[i * 3], trg[t * 3 + 1] - src[i * 3 + 1], trg[t * 3 + 2] - src[i * 3 + 2]};
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const double rinv = r2 > 0 ? 1.0 / std::sqrt(r2) : 0.0;
+        const double rinv3 = rinv * rinv * rinv;
+        for (int j = 0; j < 3; ++j)
+          for (int k = 0; k < 3; ++k)
+            M[((size_t)i * 3 + j) * n_trg * 3 + (size_t)t * 3 + k] =
+                s * ((j == k ? rinv : 0.0) + r[j] * r[k] * rinv3);
+      }
+  }
+}
+
+void jacobi_svd(int rows, int cols, const double* A, std::vector<double>& U, std::vector<double>& S,
+                std::vector<double>& V) {
+  if (rows < cols) throw std::runtime_error("jacobi_svd: rows < cols");
+  const int n = cols;
+  const int np = n + (n & 1);  // padded to even for the round-robin pairing
+  // Column-major working copies: W[j] = column j of A*V, Vc[j] = column j of V.
+  std::vector<double> W((size_t)np * rows, 0.0), Vc((size_t)np * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < rows; ++i) W[(size_t)j * rows + i] = A[(size_t)i * cols + j];
+    Vc[(size_t)j * n + j] = 1.0;
+  }
+  std::vector<int> order(np);
+  for (int i = 0; i < np; ++i) order[i] = i;
+  const double tol = 1e-15;
+  for (int sweep = 0; sweep < 80; ++sweep) {
+    long rotations = 0;
+    for (int round = 0; round < np - 1; ++round) {
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : rotations)
+      for (int k = 0; k < np / 2; ++k) {
+        int p = order[k], q = order[np - 1 - k];
+        if (p >= n || q >= n) continue;
+        if (p > q) std::swap(p, q);
+        double* wp = &W[(size_t)p * rows];
+        double* wq = &W[(size_t)q * rows];
+        double a = 0, b = 0, g = 0;
+        for (int i = 0; i < rows; ++i) {
+          a += wp[i] * wp[i];
+          b += wq[i] * wq[i];
+          g += wp[i] * wq[i];
+        }
+        if (a == 0 || b == 0 || std::fabs(g) <= tol * std::sqrt(a * b)) continue;
+        const double zeta = (b - a) / (2 * g);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+        const double c = 1 / std::sqrt(1 + t * t), s = c * t;
+        for (int i = 0; i < rows; ++i) {
+          const double x = wp[i], y = wq[i];
+          wp[i] = c * x - s * y;
+          wq[i] = s * x + c * y;
+        }
+        double* vp = &Vc[(size_t)p * n];
+        double* vq = &Vc[(size_t)q * n];
+        for (int i = 0; i < n; ++i) {
+          const double x = vp[i], y = vq[i];
+          vp[i] = c * x - s * y;
+          vq[i] = s * x + c * y;
+        }
+        ++rotations;
+      }
+      // rotate all but the first entry
+      const int last = order[np - 1];
+      for (int i = np - 1; i > 1; --i) order[i] = order[i - 1];
+      order[1] = last;
+    }
+    if (rotations == 0) break;
+  }
+  S.assign(n, 0.0);
+  U.assign((size_t)rows * n, 0.0);
+  V.assign((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double nrm = 0;
+    for (int i = 0; i < rows; ++i) nrm += W[(size_t)j * rows + i] * W[(size_t)j * rows + i];
+    nrm = std::sqrt(nrm);
+    S[j] = nrm;
+    for (int i = 0; i < rows; ++i) U[(size_t)i * n + j] = nrm > 0 ? W[(size_t)j * rows + i] / nrm : 0.0;
+    for (int i = 0; i < n; ++i) V[(size_t)i * n + j] = Vc[(size_t)j * n + i];
+  }
+}
+
+void build_operators(int kernel, int m, bool mixed, HostOperators& ops) {
+  KernelInfo ki;
+  if (!kernel_info(kernel, &ki)) throw std::runtime_error("unsupported kernel");
+  if (m < 2 || m > 16 || (m & 1)) throw std::runtime_error("multipole order must be even and in [2,16]");
+  const int ke = ki.ke;
+  const int ns = 6 * (m - 1) * (m - 1) + 2;
+  const int dim = ns * ke;
+  ops.kernel = kernel;
+  ops.m = m;
+  ops.ns = ns;
+  ops.ke = ke;
+  ops.mixed = mixed;
+  ops.n1 = 2 * m;
+  ops.n3 = ops.n1 * ops.n1 * ops.n1;
+  ops.n3h = ops.n1 * ops.n1 * (ops.n1 / 2 + 1);
+  ops.usurf = unit_surface(m);
+  const double eps = mixed ? std::ldexp(1.0, -23) : std::ldexp(1.0, -52);
+  const double zero[3] = {0, 0, 0};
+
+  // UC2UE0/1: upward equivalent (RAD0) -> upward check (RAD1), level 0 (:478-537)
+  {
+    auto ue = place_surface(ops.usurf, zero, 0.5, kRad0);
+    auto uc = place_surface(ops.usurf, zero, 0.5, kRad1);
+    std::vector<double> M((size_t)dim * dim);
+    exp_kernel_matrix(ki.exp_kernel, ue.data(), ns, uc.data(), ns, M.data());
+    pinv_factors(M, dim, dim, eps, ops.uc2ue0, ops.uc2ue1);
+  }
+  // DC2DE0/1: downward equivalent (RAD1) -> downward check (RAD0) (:538-581)
+  {
+    auto de = place_surface(ops.usurf, zero, 0.5, kRad1);
+    auto dc = place_surface(ops.usurf, zero, 0.5, kRad0);
+    std::vector<double> M((size_t)dim * dim);
+    exp_kernel_matrix(ki.exp_kernel, de.data(), ns, dc.data(), ns, M.data());
+    pinv_factors(M, dim, dim, eps, ops.dc2de0, ops.dc2de1);
+  }
+  // U2U (:582-606): (M_ce2c * UC2UE0) * UC2UE1, child c of a level-0 parent.
+  ops.u2u.assign((size_t)8 * dim * dim, 0.0);
+  ops.d2d.assign((size_t)dim * 8 * dim, 0.0);
+  for (int c = 0; c < 8; ++c) {
+    const double cc[3] = {((c & 1) ? 0.25 : -0.25), ((c & 2) ? 0.25 : -0.25), ((c & 4) ? 0.25 : -0.25)};
+    {
+      auto ce = place_surface(ops.usurf, cc, 0.25, kRad0);
+      auto pc = place_surface(ops.usurf, zero, 0.5, kRad1);
+      std::vector<double> M((size_t)dim * dim);
+      exp_kernel_matrix(ki.exp_kernel, ce.data(), ns, pc.data(), ns, M.data());
+      auto T = matmul(matmul(M, ops.uc2ue0, dim, dim, dim), ops.uc2ue1, dim, dim, dim);
+      std::memcpy(&ops.u2u[(size_t)c * dim * dim], T.data(), sizeof(double) * dim * dim);
+    }
+    // D2D (:607-643): DC2DE0 * (DC2DE1 * M_pe2c), parent level 0 -> child c.
+    {
+      auto pe = place_surface(ops.usurf, zero, 0.5, kRad1);
+      auto cc2 = place_surface(ops.usurf, cc, 0.25, kRad0);
+      std::vector<double> M((size_t)dim * dim);
+      exp_kernel_matrix(ki.exp_kernel, pe.data(), ns, cc2.data(), ns, M.data());
+      auto T = matmul(ops.dc2de0, matmul(ops.dc2de1, M, dim, dim, dim), dim, dim, dim);
+      for (int r = 0; r < dim; ++r)
+        std::memcpy(&ops.d2d[(size_t)r * 8 * dim + (size_t)c * dim], &T[(size_t)r * dim], sizeof(double) * dim);
+    }
+  }
+  // FFT maps (:2703-2712, :2790-2797): lattice index s = (u+1)(m-1)/2.
+  ops.fft_map.resize(ns);
+  ops.ifft_map.resize(ns);
+  const int n1 = ops.n1;
+  for (int i = 0; i < ns; ++i) {
+    int s[3];
+    for (int d = 0; d < 3; ++d) s[d] = (int)std::lround((ops.usurf[i * 3 + d] + 1.0) * (m - 1) * 0.5);
+    ops.fft_map[i] = (m - 1 - s[0]) + (m - 1 - s[1]) * n1 + (m - 1 - s[2]) * n1 * n1;
+    ops.ifft_map[i] = (2 * m - 1 - s[0]) + (2 * m - 1 - s[1]) * n1 + (2 * m - 1 - s[2]) * n1 * n1;
+  }
+  // V operators (:671-718): for source-minus-target child offset rel (child
+  // units, box 1), kernel from the conv grid (i-m)*RAD0/(m-1)+rel to the
+  // origin, then a 3D r2c DFT with x the halved axis.
+  const int n3 = ops.n3, nh = n1 / 2 + 1, n3h = ops.n3h, kk = ke * ke;
+  std::vector<std::complex<double>> w(n1);
+  for (int j = 0; j < n1; ++j) w[j] = std::polar(1.0, -2 * kPi * j / n1);
+  std::vector<std::vector<std::complex<double>>> vhat(343);  // index (i+3)+7(j+3)+49(k+3)
+#pragma omp parallel for schedule(dynamic)
+  for (int idx = 0; idx < 343; ++idx) {
+    const int ri = idx % 7 - 3, rj = (idx / 7) % 7 - 3, rk = idx / 49 - 3;
+    if (std::max(std::abs(ri), std::max(std::abs(rj), std::abs(rk))) <= 1) continue;
+    std::vector<double> grid((size_t)n3 * 3);
+    for (int k = 0; k < n1; ++k)
+      for (int j = 0; j < n1; ++j)
+        for (int i = 0; i < n1; ++i) {
+          const size_t g = (size_t)i + (size_t)n1 * j + (size_t)n1 * n1 * k;
+          grid[g * 3 + 0] = (i - m) * kRad0 / (m - 1) + ri;
+          grid[g * 3 + 1] = (j - m) * kRad0 / (m - 1) + rj;
+          grid[g * 3 + 2] = (k - m) * kRad0 / (m - 1) + rk;
+        }
+    std::vector<double> P((size_t)n3 * kk);
+    exp_kernel_matrix(ki.exp_kernel, grid.data(), n3, zero, 1, P.data());  // P[g*ke+i][k]
+    std::vector<std::complex<double>> out((size_t)n3h * kk);
+    std::vector<std::complex<double>> cube((size_t)n3), tmp(n1);
+    for (int comp = 0; comp < kk; ++comp) {
+      for (int g = 0; g < n3; ++g) cube[g] = P[(size_t)g * kk + comp];
+      for (int k = 0; k < n1; ++k)
+        for (int j = 0; j < n1; ++j) dft_line(&cube[(size_t)n1 * j + (size_t)n1 * n1 * k], n1, 1, w, tmp);
+      for (int k = 0; k < n1; ++k)
+        for (int i = 0; i < nh; ++i) dft_line(&cube[(size_t)i + (size_t)n1 * n1 * k], n1, n1, w, tmp);
+      for (int j = 0; j < n1; ++j)
+        for (int i = 0; i < nh; ++i) dft_line(&cube[(size_t)i + (size_t)n1 * j], n1, n1 * n1, w, tmp);
+      for (int k = 0; k < n1; ++k)
+        for (int j = 0; j < n1; ++j)
+          for (int i = 0; i < nh; ++i)
+            out[(((size_t)k * n1 + j) * nh + i) * kk + comp] = cube[(size_t)i + (size_t)n1 * j + (size_t)n1 * n1 * k];
+    }
+    vhat[idx] = std::move(out);
+  }
+  // Hadamard operators (V1, :719-764): parent offset o (colleague index ci,
+  // ci != 13), target child j1, source child j2: rel = 2*po - bits(j1) + bits(j2);
+  // adjacent children give zero blocks.  Divided by n3 (inverse DFT scale).
+  ops.vop.assign((size_t)n3h * 26 * 64 * kk * 2, 0.0);
+  for (int ci = 0, o = 0; ci < 27; ++ci) {
+    if (ci == 13) continue;
+    const int po[3] = {ci % 3 - 1, (ci / 3) % 3 - 1, ci / 9 - 1};
+    for (int j1 = 0; j1 < 8; ++j1)
+      for (int j2 = 0; j2 < 8; ++j2) {
+        int rel[3];
+        for (int d = 0; d < 3; ++d) rel[d] = 2 * po[d] - ((j1 >> d) & 1) + ((j2 >> d) & 1);
+        if (std::max(std::abs(rel[0]), std::max(std::abs(rel[1]), std::abs(rel[2]))) <= 1) continue;
+        const auto& vh = vhat[(rel[0] + 3) + 7 * (rel[1] + 3) + 49 * (rel[2] + 3)];
+        for (int f = 0; f < n3h; ++f)
+          for (int c = 0; c < kk; ++c) {
+            const size_t dst = ((((size_t)f * 26 + o) * 64 + j1 * 8 + j2) * kk + c) * 2;
+            ops.vop[dst + 0] = vh[(size_t)f * kk + c].real() / n3;
+            ops.vop[dst + 1] = vh[(size_t)f * kk + c].imag() / n3;
+          }
+      }
+    ++o;
+  }
+}
+
+}  // namespace pvfmm_b200

@@ -1,0 +1,835 @@
+// GPU octree construction for the particle FMM.
+//
+// Reproduces, on the device, the tree PVFMM builds on one rank:
+//   * bounding-box map into [0,1)^3        src/pvfmm-wrapper.cpp:458-590
+//   * Morton ids + stable sort              include/mortonid.txx:25-53,107-118,
+//                                           include/parUtils.txx:527 (ties keep input order)
+//   * refinement: a leaf splits while depth < MAX_DEPTH-1 and either the
+//     context's seed grid (pvfmm-wrapper.cpp:416-432) or src+trg counts exceed
+//     max_pts                               include/fmm_node.txx:63-98, mpi_tree.txx:403-492
+//   * 2:1 balance as the closure of the internal-node set under
+//     X -> parent(NbrList(X))              include/mpi_tree.txx:745-943
+//   * colleagues                            include/mpi_tree.txx:1136-1256
+//   * U/V/W/X lists with the Nsrf rule      include/interac_list.txx:98-279,
+//                                           include/fmm_pts.txx:4629, 4929, 5295, 5325
+// Each level is a Morton-sorted array; children of an internal node are the
+// 8 consecutive nodes of the next level.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "fmm_context.cuh"
+
+namespace pvfmm_b200 {
+namespace {
+
+constexpr int kThreads = 256;
+
+// ------------------------------------------------------------------ bbox
+template <class T>
+__global__ void bbox_partial(const T* __restrict__ pos, long n, double* __restrict__ part) {
+  __shared__ double smin[3][kThreads], smax[3][kThreads];
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      const double v = (double)pos[i * 3 + d];
+      mn[d] = fmin(mn[d], v);
+      mx[d] = fmax(mx[d], v);
+    }
+  for (int d = 0; d < 3; ++d) {
+    smin[d][threadIdx.x] = mn[d];
+    smax[d][threadIdx.x] = mx[d];
+  }
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int d = 0; d < 3; ++d) {
+        smin[d][threadIdx.x] = fmin(smin[d][threadIdx.x], smin[d][threadIdx.x + s]);
+        smax[d][threadIdx.x] = fmax(smax[d][threadIdx.x], smax[d][threadIdx.x + s]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      part[blockIdx.x * 6 + d] = smin[d][0];
+      part[blockIdx.x * 6 + 3 + d] = smax[d][0];
+    }
+}
+
+__global__ void bbox_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double r[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  for (int b = 0; b < nb; ++b)
+    for (int d = 0; d < 3; ++d) {
+      r[d] = fmin(r[d], part[b * 6 + d]);
+      r[3 + d] = fmax(r[3 + d], part[b * 6 + 3 + d]);
+    }
+  for (int d = 0; d < 6; ++d) out[d] = r[d];
+}
+
+// ------------------------------------------------------------------ keys
+// c = pos*scale + shift in the input precision, without fused multiply-add
+// (pvfmm-wrapper.cpp:582-586), wrapped into [0,1); Morton coordinate
+// floor(c*2^30) (mortonid.txx:39-53).
+template <class T>
+__device__ __forceinline__ T map_coord(T x, T s, T sh);
+template <>
+__device__ __forceinline__ double map_coord<double>(double x, double s, double sh) {
+  double c = __dadd_rn(__dmul_rn(x, s), sh);
+  while (c < 0.0) c = __dadd_rn(c, 1.0);
+  while (c >= 1.0) c = __dadd_rn(c, -1.0);
+  return c;
+}
+template <>
+__device__ __forceinline__ float map_coord<float>(float x, float s, float sh) {
+  float c = __fadd_rn(__fmul_rn(x, s), sh);
+  while (c < 0.f) c = __fadd_rn(c, 1.f);
+  while (c >= 1.f) c = __fadd_rn(c, -1.f);
+  return c;
+}
+
+template <class T>
+__global__ void map_and_key(const T* __restrict__ pos, long n, T scale, T sh0, T sh1, T sh2,
+                            double* __restrict__ mapped, unsigned long long* __restrict__ hi,
+                            unsigned int* __restrict__ lo, int* __restrict__ idx) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T sh[3] = {sh0, sh1, sh2};
+  unsigned int q[3];
+  for (int d = 0; d < 3; ++d) {
+    const T c = map_coord<T>(pos[i * 3 + d], scale, sh[d]);
+    mapped[i * 3 + d] = (double)c;
+    q[d] = (unsigned int)floor((double)c * (double)kTwo30);
+  }
+  const MKey k = make_key(q[0], q[1], q[2], kMaxDepth);
+  hi[i] = k.hi;
+  lo[i] = k.lo;
+  idx[i] = (int)i;
+}
+
+__global__ void gather_u64(const unsigned long long* __restrict__ in, const int* __restrict__ perm, long n,
+                           unsigned long long* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[perm[i]];
+}
+
+__global__ void assemble_keys(const unsigned long long* __restrict__ hi, const unsigned int* __restrict__ lo_unsorted,
+                              const int* __restrict__ perm, long n, MKey* __restrict__ keys) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  MKey k;
+  k.hi = hi[i];
+  k.lo = lo_unsorted[perm[i]];
+  k.pad = 0;
+  keys[i] = k;
+}
+
+// ------------------------------------------------------------------ refine
+__global__ void refine_level(const MKey* __restrict__ cur, long n_cur, int d, const MKey* __restrict__ sk, long n_s,
+                             const MKey* __restrict__ tk, long n_t, const MKey* __restrict__ gk, long n_g, long max_pts,
+                             int max_depth, int* __restrict__ split) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_cur) return;
+  unsigned int X, Y, Z, dd;
+  decode_key(cur[i], X, Y, Z, dd);
+  int s = 0;
+  if (d < max_depth - 1) {
+    const MKey b = cur[i], e = node_end_key(X, Y, Z, d);
+    const long g = lower_bound_key(gk, n_g, e) - lower_bound_key(gk, n_g, b);
+    long c = 0;
+    if (sk) c += lower_bound_key(sk, n_s, e) - lower_bound_key(sk, n_s, b);
+    c += lower_bound_key(tk, n_t, e) - lower_bound_key(tk, n_t, b);
+    s = (g > max_pts || c > max_pts) ? 1 : 0;
+  }
+  split[i] = s;
+}
+
+__global__ void make_children(const MKey* __restrict__ cur, const int* __restrict__ flag, const int* __restrict__ offs,
+                              long n_cur, int d, MKey* __restrict__ next, MKey* __restrict__ internal_out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_cur || !flag[i]) return;
+  const long k = offs[i];
+  if (internal_out) internal_out[k] = cur[i];
+  if (next) {
+    unsigned int X, Y, Z, dd;
+    decode_key(cur[i], X, Y, Z, dd);
+    const unsigned int w = kTwo30 >> (d + 1);
+    for (int c = 0; c < 8; ++c)
+      next[k * 8 + c] = make_key(X + ((c & 1) ? w : 0), Y + ((c & 2) ? w : 0), Z + ((c & 4) ? w : 0), d + 1);
+  }
+}
+
+// ------------------------------------------------------------------ balance
+// For internal node X at level d: parents (level d-1) of its 3^3 neighbours
+// clipped to the unit box; per axis these are parent(x) and the parent on the
+// side of x within its parent.  Invalid candidates get the sentinel key.
+__global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, MKey* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned int q[3], dd;
+  decode_key(S[i], q[0], q[1], q[2], dd);
+  const unsigned int w = kTwo30 >> d;
+  const unsigned int pmask = ~((kTwo30 >> (d - 1)) - 1u);
+  long cand[3][2];
+  for (int a = 0; a < 3; ++a) {
+    const long p0 = (long)(q[a] & pmask);
+    cand[a][0] = p0;
+    if (q[a] & w) cand[a][1] = (q[a] + (long)w < (long)kTwo30) ? p0 + 2L * w : -1;
+    else cand[a][1] = ((long)q[a] - (long)w >= 0) ? p0 - 2L * w : -1;
+  }
+  for (int c = 0; c < 8; ++c) {
+    const long x = cand[0][c & 1], y = cand[1][(c >> 1) & 1], z = cand[2][(c >> 2) & 1];
+    out[i * 8 + c] = (x < 0 || y < 0 || z < 0) ? MKey{~0ULL, ~0u, 0}
+                                               : make_key((unsigned int)x, (unsigned int)y, (unsigned int)z, d - 1);
+  }
+}
+
+__global__ void split_keys(const MKey* __restrict__ k, long n, unsigned long long* __restrict__ hi,
+                           unsigned int* __restrict__ lo, int* __restrict__ idx) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  hi[i] = k[i].hi;
+  lo[i] = k[i].lo;
+  idx[i] = (int)i;
+}
+
+__global__ void unique_flags(const unsigned long long* __restrict__ hi, const unsigned int* __restrict__ lo, long n,
+                             int* __restrict__ flag) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool sentinel = hi[i] == ~0ULL && lo[i] == ~0u;
+  const bool first = i == 0 || hi[i] != hi[i - 1] || lo[i] != lo[i - 1];
+  flag[i] = (first && !sentinel) ? 1 : 0;
+}
+
+__global__ void compact_keys(const unsigned long long* __restrict__ hi, const unsigned int* __restrict__ lo,
+                             const int* __restrict__ flag, const int* __restrict__ offs, long n, MKey* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n || !flag[i]) return;
+  MKey k;
+  k.hi = hi[i];
+  k.lo = lo[i];
+  k.pad = 0;
+  out[offs[i]] = k;
+}
+
+// ------------------------------------------------------------------ final tree
+__global__ void children_of(const MKey* __restrict__ S, long n, int d, MKey* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned int X, Y, Z, dd;
+  decode_key(S[i], X, Y, Z, dd);
+  const unsigned int w = kTwo30 >> (d + 1);
+  for (int c = 0; c < 8; ++c)
+    out[i * 8 + c] = make_key(X + ((c & 1) ? w : 0), Y + ((c & 2) ? w : 0), Z + ((c & 4) ? w : 0), d + 1);
+}
+
+__global__ void member_flags(const MKey* __restrict__ keys, long n, const MKey* __restrict__ S, long nS,
+                             int* __restrict__ internal) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int f = 0;
+  if (nS > 0) {
+    const long p = lower_bound_key(S, nS, keys[i]);
+    f = (p < nS && key_eq(S[p], keys[i])) ? 1 : 0;
+  }
+  internal[i] = f;
+}
+
+__global__ void level_links(const int* __restrict__ internal, const int* __restrict__ offs, long n, long base,
+                            long next_base, long int_base, unsigned char* __restrict__ leaf, int* __restrict__ child0,
+                            int* __restrict__ parent, int* __restrict__ int_idx) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long g = base + i;
+  if (internal[i]) {
+    const long k = offs[i];
+    leaf[g] = 0;
+    child0[g] = (int)(next_base + 8 * k);
+    int_idx[int_base + k] = (int)g;
+    for (int c = 0; c < 8; ++c) parent[next_base + 8 * k + c] = (int)g;
+  } else {
+    leaf[g] = 1;
+    child0[g] = -1;
+  }
+}
+
+__global__ void node_ranges(const MKey* __restrict__ keys, long n, const MKey* __restrict__ sk, long n_s,
+                            const MKey* __restrict__ tk, long n_t, int* __restrict__ slo, int* __restrict__ shi,
+                            int* __restrict__ tlo, int* __restrict__ thi) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned int X, Y, Z, d;
+  decode_key(keys[i], X, Y, Z, d);
+  const MKey e = node_end_key(X, Y, Z, d);
+  if (sk) {
+    slo[i] = (int)lower_bound_key(sk, n_s, keys[i]);
+    shi[i] = (int)lower_bound_key(sk, n_s, e);
+  } else {
+    slo[i] = shi[i] = 0;
+  }
+  tlo[i] = (int)lower_bound_key(tk, n_t, keys[i]);
+  thi[i] = (int)lower_bound_key(tk, n_t, e);
+}
+
+// Colleague index ((z+1)*3+(y+1))*3+(x+1) (mpi_tree.txx:1143-1145).
+__global__ void colleagues_kernel(const MKey* __restrict__ keys, long base, long n_level, int* __restrict__ coll) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_level) return;
+  unsigned int X, Y, Z, d;
+  decode_key(keys[base + i], X, Y, Z, d);
+  const long w = (long)(kTwo30 >> d);
+  for (int ci = 0; ci < 27; ++ci) {
+    const long x = X + (ci % 3 - 1) * w, y = Y + ((ci / 3) % 3 - 1) * w, z = Z + (ci / 9 - 1) * w;
+    int r = -1;
+    if (x >= 0 && y >= 0 && z >= 0 && x < kTwo30 && y < kTwo30 && z < kTwo30) {
+      const MKey k = make_key((unsigned int)x, (unsigned int)y, (unsigned int)z, d);
+      const long p = lower_bound_key(keys + base, n_level, k);
+      if (p < n_level && key_eq(keys[base + p], k)) r = (int)(base + p);
+    }
+    coll[(base + i) * 27 + ci] = r;
+  }
+}
+
+// Point -> leaf map and coordinates relative to the leaf centre.
+template <class Real>
+__global__ void localize(const int* __restrict__ leaves, long n_leaves, const MKey* __restrict__ keys,
+                         const int* __restrict__ lo, const int* __restrict__ hi, const double* __restrict__ coord,
+                         Real* __restrict__ x, Real* __restrict__ y, Real* __restrict__ z, int* __restrict__ pt_leaf) {
+  const long li = blockIdx.x;
+  if (li >= n_leaves) return;
+  const int node = leaves[li];
+  unsigned int X, Y, Z, d;
+  decode_key(keys[node], X, Y, Z, d);
+  const double h = 1.0 / (double)(1u << d);
+  const double c[3] = {X * (1.0 / kTwo30) + 0.5 * h, Y * (1.0 / kTwo30) + 0.5 * h, Z * (1.0 / kTwo30) + 0.5 * h};
+  for (int p = lo[node] + threadIdx.x; p < hi[node]; p += blockDim.x) {
+    x[p] = (Real)(coord[p * 3 + 0] - c[0]);
+    y[p] = (Real)(coord[p * 3 + 1] - c[1]);
+    z[p] = (Real)(coord[p * 3 + 2] - c[2]);
+    pt_leaf[p] = node;
+  }
+}
+
+__global__ void gather_coords(const double* __restrict__ in, const int* __restrict__ perm, long n,
+                              double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long p = perm[i];
+  out[i * 3 + 0] = in[p * 3 + 0];
+  out[i * 3 + 1] = in[p * 3 + 1];
+  out[i * 3 + 2] = in[p * 3 + 2];
+}
+
+// ------------------------------------------------------------------ lists
+// One pass per target node (n_trg > 0); `mode` 0 counts, 1 fills.
+// Relative coordinates follow InteracList::BuildList (interac_list.txx:98-279).
+__global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf, const int* __restrict__ parent,
+                            const int* __restrict__ child0, const int* __restrict__ coll, const int* __restrict__ slo,
+                            const int* __restrict__ shi, const int* __restrict__ tlo, const int* __restrict__ thi,
+                            long nsrf, int mode, int* __restrict__ p_cnt, int* __restrict__ x_cnt, int* __restrict__ w_cnt,
+                            int* __restrict__ v_cnt, const int* __restrict__ p_off, const int* __restrict__ x_off,
+                            const int* __restrict__ w_off, int* __restrict__ p_list, int* __restrict__ x_list,
+                            int* __restrict__ w_list) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n_nodes) return;
+  const int nt = thi[t] - tlo[t];
+  int np = 0, nx = 0, nw = 0, nv = 0;
+  if (nt > 0) {
+    const bool tleaf = leaf[t];
+    int* pl = mode ? p_list + p_off[t] : nullptr;
+    int* xl = mode ? x_list + x_off[t] : nullptr;
+    int* wl = mode ? w_list + w_off[t] : nullptr;
+#define ADD(list, cnt, v) \
+  do {                    \
+    if (mode) list[cnt] = (v); \
+    ++cnt;                \
+  } while (0)
+    if (tleaf) {
+      for (int ci = 0; ci < 27; ++ci) {
+        const int c = coll[t * 27 + ci];
+        if (c < 0) continue;
+        if (leaf[c]) {
+          if (shi[c] > slo[c]) ADD(pl, np, c);  // U1
+        } else {
+          for (int j = 0; j < 8; ++j) {
+            const int ch = child0[c] + j;
+            const int rx = (ci % 3) * 4 - 4 + ((j & 1) ? 2 : 0) - 1;
+            const int ry = ((ci / 3) % 3) * 4 - 4 + ((j & 2) ? 2 : 0) - 1;
+            const int rz = (ci / 9) * 4 - 4 + ((j & 4) ? 2 : 0) - 1;
+            const int ns_ch = shi[ch] - slo[ch];
+            if (ns_ch <= 0) continue;
+            if (max(abs(rx), max(abs(ry), abs(rz))) <= 3) {
+              ADD(pl, np, ch);  // U2
+            } else if (leaf[ch] && ns_ch <= nsrf) {
+              ADD(pl, np, ch);  // W handled as P2P (fmm_pts.txx:5325)
+            } else {
+              ADD(wl, nw, ch);  // W (fmm_pts.txx:4929)
+            }
+          }
+        }
+      }
+    }
+    const int p = parent[t];
+    if (p >= 0) {
+      int p2n = 0;
+      {
+        const int c0 = child0[p];
+        p2n = (int)(t - c0);
+      }
+      for (int ci = 0; ci < 27; ++ci) {
+        const int c = coll[(long)p * 27 + ci];
+        if (c < 0 || !leaf[c]) continue;
+        if (shi[c] <= slo[c]) continue;
+        const int rx = (ci % 3) * 4 - 4 - ((p2n & 1) ? 2 : 0) + 1;
+        const int ry = ((ci / 3) % 3) * 4 - 4 - ((p2n & 2) ? 2 : 0) + 1;
+        const int rz = (ci / 9) * 4 - 4 - ((p2n & 4) ? 2 : 0) + 1;
+        if (max(abs(rx), max(abs(ry), abs(rz))) <= 3) {
+          if (tleaf) ADD(pl, np, c);  // U0
+        } else if (tleaf && nt <= nsrf) {
+          ADD(pl, np, c);  // X handled as P2P (fmm_pts.txx:5295)
+        } else {
+          ADD(xl, nx, c);  // X (fmm_pts.txx:4629)
+        }
+      }
+    }
+    if (!tleaf) {
+      for (int ci = 0; ci < 27; ++ci) {
+        if (ci == 13) continue;
+        const int c = coll[t * 27 + ci];
+        if (c >= 0 && !leaf[c] && shi[c] > slo[c]) ++nv;
+      }
+    }
+#undef ADD
+  }
+  if (!mode) {
+    p_cnt[t] = np;
+    x_cnt[t] = nx;
+    w_cnt[t] = nw;
+    v_cnt[t] = nv;
+  }
+}
+
+__global__ void fill_vtab(const int* __restrict__ vtrg, long n_vtrg, const int* __restrict__ coll,
+                          const int* __restrict__ node2vsrc, int* __restrict__ vtab) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_vtrg) return;
+  const long t = vtrg[i];
+  for (int ci = 0, o = 0; ci < 27; ++ci) {
+    if (ci == 13) continue;
+    const int c = coll[t * 27 + ci];
+    vtab[i * 26 + o] = (c >= 0) ? node2vsrc[c] : -1;
+    ++o;
+  }
+}
+
+template <class Pred>
+__global__ void flag_nodes(long n, Pred pred, int* __restrict__ flag) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = pred(i) ? 1 : 0;
+}
+
+__global__ void compact_index(const int* __restrict__ flag, const int* __restrict__ offs, long n, int* __restrict__ out,
+                              int* __restrict__ map) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flag[i]) out[offs[i]] = (int)i;
+  if (map) map[i] = flag[i] ? offs[i] : -1;
+}
+
+__global__ void gather_u32(const unsigned int* __restrict__ in, const int* __restrict__ perm, long n,
+                           unsigned int* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[perm[i]];
+}
+
+__global__ void iota_kernel(int* __restrict__ a, long n) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = (int)i;
+}
+
+// Exclusive prefix sum of n ints; returns the total (synchronous read).
+long exclusive_scan(Context& ctx, const int* in, int* out, long n) {
+  if (n <= 0) return 0;
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx.stream);
+  void* tmp = ctx.scratch2.ensure(bytes);
+  cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx.stream);
+  int h[2];
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(&h[0], out + n - 1, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(&h[1], in + n - 1, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+  return (long)h[0] + h[1];
+}
+
+// Stable sort of 96-bit keys (hi, lo): by lo, then stably by hi.  On return
+// perm[i] is the input position of the i-th smallest key and hs/ls hold the
+// sorted halves.  Uses temporaries t[base..base+2].
+void sort_hilo(Context& ctx, long n, const unsigned long long* hi, const unsigned int* lo, unsigned long long* hs,
+               unsigned int* ls, int* perm, int base) {
+  auto& s = ctx.stream;
+  int* idx = ctx.t[base].as<int>(n);
+  int* p1 = ctx.t[base + 1].as<int>(n);
+  unsigned long long* hg = ctx.t[base + 2].as<unsigned long long>(n);
+  iota_kernel<<<ceil_div(n, kThreads), kThreads, 0, s>>>(idx, n);
+  size_t b1 = 0, b2 = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b1, lo, ls, idx, p1, (int)n, 0, 32, s);
+  cub::DeviceRadixSort::SortPairs(nullptr, b2, hg, hs, p1, perm, (int)n, 0, 64, s);
+  void* tmp = ctx.scratch.ensure(std::max(b1, b2));
+  cub::DeviceRadixSort::SortPairs(tmp, b1, lo, ls, idx, p1, (int)n, 0, 32, s);
+  gather_u64<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hi, p1, n, hg);
+  cub::DeviceRadixSort::SortPairs(tmp, b2, hg, hs, p1, perm, (int)n, 0, 64, s);
+  gather_u32<<<ceil_div(n, kThreads), kThreads, 0, s>>>(lo, perm, n, ls);
+}
+
+// Sorts node keys and removes duplicates and sentinels; returns the count.
+long sort_unique(Context& ctx, const MKey* in, long n, DevBuf& out) {
+  auto& s = ctx.stream;
+  if (n == 0) return 0;
+  unsigned long long* h = ctx.t[10].as<unsigned long long>(n);
+  unsigned int* l = ctx.t[11].as<unsigned int>(n);
+  int* ix = ctx.t[12].as<int>(n);
+  split_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(in, n, h, l, ix);
+  unsigned long long* hs = ctx.t[13].as<unsigned long long>(n);
+  unsigned int* ls = ctx.t[14].as<unsigned int>(n);
+  int* perm = ctx.t[15].as<int>(n);
+  sort_hilo(ctx, n, h, l, hs, ls, perm, 16);
+  int* fl = ctx.t[19].as<int>(n);
+  int* of = ctx.t[20].as<int>(n);
+  unique_flags<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, ls, n, fl);
+  const long cnt = exclusive_scan(ctx, fl, of, n);
+  MKey* o = out.as<MKey>(std::max(cnt, 1L));
+  compact_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, ls, fl, of, n, o);
+  return cnt;
+}
+
+// Sorts mapped points: perm (sorted -> input), sorted keys, sorted coords.
+void sort_point_set(Context& ctx, long n, const unsigned long long* hi, const unsigned int* lo, const double* mapped,
+                    DevBuf& perm_out, DevBuf& keys_out, DevBuf& coord_out) {
+  auto& s = ctx.stream;
+  unsigned long long* hs = ctx.t[5].as<unsigned long long>(n);
+  unsigned int* ls = ctx.t[6].as<unsigned int>(n);
+  int* perm = perm_out.as<int>(n);
+  sort_hilo(ctx, n, hi, lo, hs, ls, perm, 16);
+  MKey* keys = keys_out.as<MKey>(n);
+  assemble_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, lo, perm, n, keys);
+  double* c = coord_out.as<double>(n * 3);
+  gather_coords<<<ceil_div(n, kThreads), kThreads, 0, s>>>(mapped, perm, n, c);
+}
+
+// Reference bounding-box rule (pvfmm-wrapper.cpp:469-520) in precision Real.
+template <class Real>
+void bbox_scale_shift(const double* bs, const double* bt, double& scale_out, double* shift_out) {
+  const Real eps = std::numeric_limits<Real>::epsilon() * (Real)64;
+  auto one = [&](const double* b, Real& sc, Real* sh) {
+    const double* mn = b;
+    const double* mx = b + 3;
+    sc = (Real)1 / (Real)(mx[0] - mn[0] + 2 * (double)eps);
+    for (int k = 0; k < 3; ++k) sc = std::min(sc, (Real)(1.0 / (mx[k] - mn[k] + 2 * (double)eps)));
+    if (sc * (Real)0 != (Real)0) sc = (Real)1;
+    for (int k = 0; k < 3; ++k) sh[k] = (Real)(-mn[k]) * sc + eps;
+  };
+  Real s0, x0[3], s1, x1[3];
+  one(bs, s0, x0);
+  one(bt, s1, x1);
+  Real c0[3], c1[3];
+  for (int k = 0; k < 3; ++k) {
+    c0[k] = (Real)(0.5 - (double)x0[k]) / s0;
+    c1[k] = (Real)(0.5 - (double)x1[k]) / s1;
+  }
+  Real sc = 0;
+  for (int k = 0; k < 3; ++k) sc = std::max(sc, (Real)std::fabs(c0[k] - c1[k]));
+  sc = (Real)1 / (sc + (Real)1 / s0 + (Real)1 / s1);
+  scale_out = (double)sc;
+  for (int k = 0; k < 3; ++k) shift_out[k] = (double)((Real)0.5 - (c0[k] + c1[k]) * sc / (Real)2);
+}
+
+template <class T>
+void point_bbox(Context& ctx, const T* pos, long n, double* host6) {
+  const int nb = (int)std::min<long>(1024, std::max<long>(1, ceil_div(n, kThreads)));
+  double* part = ctx.t[0].as<double>((size_t)nb * 6 + 6);
+  bbox_partial<T><<<nb, kThreads, 0, ctx.stream>>>(pos, n, part);
+  bbox_final<<<1, 32, 0, ctx.stream>>>(part, nb, part + (size_t)nb * 6);
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(host6, part + (size_t)nb * 6, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+}
+
+template <class T>
+void map_points(Context& ctx, const T* pos, long n, double scale, const double* shift, DevBuf& mapped,
+                DevBuf& hi, DevBuf& lo) {
+  double* mp = mapped.as<double>(n * 3);
+  unsigned long long* h = hi.as<unsigned long long>(n);
+  unsigned int* l = lo.as<unsigned int>(n);
+  int* idx = ctx.t[4].as<int>(n);
+  map_and_key<T><<<ceil_div(n, kThreads), kThreads, 0, ctx.stream>>>(pos, n, (T)scale, (T)shift[0], (T)shift[1],
+                                                                      (T)shift[2], mp, h, l, idx);
+}
+
+}  // namespace
+
+// Seed grid of the context's initial tree (pvfmm-wrapper.cpp:416-432), as
+// sorted Morton keys, in the precision of the context.
+static std::vector<MKey> seed_grid_keys(int max_pts, bool real_float) {
+  std::vector<MKey> keys;
+  long NN;
+  if (real_float) NN = (long)std::ceil(std::pow((float)max_pts, 1.0 / 3.0));
+  else NN = (long)std::ceil(std::pow((double)max_pts, 1.0 / 3.0));
+  keys.reserve(NN * NN * NN);
+  for (long i = 0; i < NN * NN * NN; ++i) {
+    unsigned int q[3];
+    const long comp[3] = {i % NN, (i / NN) % NN, (i / (NN * NN)) % NN};
+    for (int d = 0; d < 3; ++d) {
+      if (real_float) {
+        const float c = (float)((float)comp[d] + 0.5f) / (float)NN;
+        q[d] = (unsigned int)std::floor((double)c * (double)kTwo30);
+      } else {
+        const double c = ((double)comp[d] + 0.5) / (double)NN;
+        q[d] = (unsigned int)std::floor(c * (double)kTwo30);
+      }
+    }
+    keys.push_back(make_key(q[0], q[1], q[2], kMaxDepth));
+  }
+  std::sort(keys.begin(), keys.end(), [](const MKey& a, const MKey& b) { return key_less(a, b); });
+  return keys;
+}
+
+void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
+                bool src_counted, bool trg_alias) {
+  if (n_src < 1 || n_trg < 1) throw std::runtime_error("build_tree needs at least one source and one target");
+  DevTree& T = ctx.tree;
+  auto& s = ctx.stream;
+  T.valid = false;
+  T.n_src = n_src;
+  T.n_trg = n_trg;
+  T.src_counted = src_counted && n_src > 0;
+  // 1. bounding box and map
+  double bs[6], bt[6];
+  if (pos_float) {
+    point_bbox<float>(ctx, (const float*)src_pos, n_src, bs);
+    if (trg_alias) std::copy(bs, bs + 6, bt);
+    else point_bbox<float>(ctx, (const float*)trg_pos, n_trg, bt);
+    bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
+  } else {
+    point_bbox<double>(ctx, (const double*)src_pos, n_src, bs);
+    if (trg_alias) std::copy(bs, bs + 6, bt);
+    else point_bbox<double>(ctx, (const double*)trg_pos, n_trg, bt);
+    bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
+  }
+  DevBuf& src_mapped = ctx.t[1];
+  DevBuf& trg_mapped = ctx.t[2];
+  DevBuf& hi = ctx.t[7];
+  DevBuf& lo = ctx.t[8];
+  DevBuf& coords_s = ctx.t[21];
+  DevBuf& coords_t = ctx.t[22];
+  // 2. sources
+  if (pos_float) map_points<float>(ctx, (const float*)src_pos, n_src, T.scale_x, T.shift_x, src_mapped, hi, lo);
+  else map_points<double>(ctx, (const double*)src_pos, n_src, T.scale_x, T.shift_x, src_mapped, hi, lo);
+  sort_point_set(ctx, n_src, hi.get<unsigned long long>(), lo.get<unsigned int>(), src_mapped.get<double>(),
+                 T.src_perm, T.src_key, coords_s);
+  // 3. targets
+  if (trg_alias) {
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(T.trg_perm.as<int>(n_src), T.src_perm.get<int>(), n_src * sizeof(int),
+                                     cudaMemcpyDeviceToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(T.trg_key.as<MKey>(n_src), T.src_key.get<MKey>(), n_src * sizeof(MKey),
+                                     cudaMemcpyDeviceToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(coords_t.as<double>(n_src * 3), coords_s.get<double>(), n_src * 3 * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, s));
+  } else {
+    if (pos_float) map_points<float>(ctx, (const float*)trg_pos, n_trg, T.scale_x, T.shift_x, trg_mapped, hi, lo);
+    else map_points<double>(ctx, (const double*)trg_pos, n_trg, T.scale_x, T.shift_x, trg_mapped, hi, lo);
+    sort_point_set(ctx, n_trg, hi.get<unsigned long long>(), lo.get<unsigned int>(), trg_mapped.get<double>(),
+                   T.trg_perm, T.trg_key, coords_t);
+  }
+  // 4. seed grid
+  const std::vector<MKey> gk = seed_grid_keys(ctx.max_pts, pos_float);
+  MKey* d_gk = ctx.t[9].as<MKey>(gk.size());
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_gk, gk.data(), gk.size() * sizeof(MKey), cudaMemcpyHostToDevice, s));
+  const MKey* sk = T.src_counted ? T.src_key.get<MKey>() : nullptr;
+  const MKey* tk = T.trg_key.get<MKey>();
+  // 5. refinement, level by level
+  std::vector<long> nR;
+  {
+    DevBuf cur_b, next_b;
+    MKey root = make_key(0, 0, 0, 0);
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(cur_b.as<MKey>(1), &root, sizeof(MKey), cudaMemcpyHostToDevice, s));
+    long n_cur = 1;
+    int d = 0;
+    while (n_cur > 0) {
+      int* split = ctx.t[3].as<int>(n_cur);
+      int* offs = ctx.t[23].as<int>(n_cur);
+      refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), n_cur, d, sk, T.n_src, tk,
+                                                                   T.n_trg, d_gk, (long)gk.size(), ctx.max_pts,
+                                                                   kMaxDepth, split);
+      const long n_split = exclusive_scan(ctx, split, offs, n_cur);
+      if (n_split == 0) break;
+      if ((long)ctx.lvlR.size() <= d) ctx.lvlR.resize(d + 1);
+      MKey* R = ctx.lvlR[d].as<MKey>(n_split);
+      MKey* next = next_b.as<MKey>(n_split * 8);
+      make_children<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), split, offs, n_cur, d, next, R);
+      nR.push_back(n_split);
+      std::swap(cur_b, next_b);
+      n_cur = n_split * 8;
+      ++d;
+    }
+    cur_b.release();
+    next_b.release();
+  }
+  const int dint = (int)nR.size() - 1;  // deepest level with internal nodes (-1: root is a leaf)
+  // 6. 2:1 balance closure
+  std::vector<long> nS(std::max(dint + 1, 0), 0);
+  if ((long)ctx.lvlS.size() < dint + 1) ctx.lvlS.resize(dint + 1);
+  if (dint >= 0) {
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(ctx.lvlS[dint].as<MKey>(nR[dint]), ctx.lvlR[dint].get<MKey>(),
+                                     nR[dint] * sizeof(MKey), cudaMemcpyDeviceToDevice, s));
+    nS[dint] = nR[dint];
+    for (int d = dint; d >= 1; --d) {
+      const long nc = nR[d - 1] + 8 * nS[d];
+      MKey* cand = ctx.t[9].as<MKey>(nc);
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(cand, ctx.lvlR[d - 1].get<MKey>(), nR[d - 1] * sizeof(MKey),
+                                       cudaMemcpyDeviceToDevice, s));
+      nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d, cand + nR[d - 1]);
+      nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1]);
+    }
+  }
+  // 7. final node arrays
+  const int D = dint + 1;  // deepest level
+  T.depth = D;
+  T.level_off.assign(D + 2, 0);
+  T.n_internal.assign(D + 1, 0);
+  T.level_off[0] = 0;
+  T.level_off[1] = 1;
+  for (int d = 1; d <= D; ++d) T.level_off[d + 1] = T.level_off[d] + 8 * nS[d - 1];
+  const long N = T.level_off[D + 1];
+  T.n_nodes = N;
+  MKey* keys = T.key.as<MKey>(N);
+  unsigned char* leaf = T.leaf.as<unsigned char>(N);
+  int* parent = T.parent.as<int>(N);
+  int* child0 = T.child0.as<int>(N);
+  long n_int_total = 0;
+  for (int d = 0; d < D; ++d) n_int_total += nS[d];
+  int* int_idx = T.int_idx.as<int>(std::max(n_int_total, 1L));
+  T.int_off.assign(D + 1, 0);
+  {
+    MKey root = make_key(0, 0, 0, 0);
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(keys, &root, sizeof(MKey), cudaMemcpyHostToDevice, s));
+    const int minus1 = -1;
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(parent, &minus1, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  long int_base = 0;
+  for (int d = 0; d <= D; ++d) {
+    const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
+    if (d > 0) children_of<<<ceil_div(nS[d - 1], kThreads), kThreads, 0, s>>>(ctx.lvlS[d - 1].get<MKey>(), nS[d - 1],
+                                                                              d - 1, keys + base);
+    int* internal = ctx.t[3].as<int>(nl);
+    int* offs = ctx.t[23].as<int>(nl);
+    const long nSd = d < D ? nS[d] : 0;
+    member_flags<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys + base, nl, d < D ? ctx.lvlS[d].get<MKey>() : nullptr,
+                                                             nSd, internal);
+    const long nint = exclusive_scan(ctx, internal, offs, nl);
+    if (nint != nSd) throw std::runtime_error("octree build: balanced internal set is not closed");
+    T.n_internal[d] = nint;
+    T.int_off[d] = int_base;
+    level_links<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(internal, offs, nl, base, T.level_off[d + 1], int_base,
+                                                            leaf, child0, parent, int_idx);
+    int_base += nint;
+  }
+  // 8. point ranges and colleagues
+  int* slo = T.src_lo.as<int>(N);
+  int* shi = T.src_hi.as<int>(N);
+  int* tlo = T.trg_lo.as<int>(N);
+  int* thi = T.trg_hi.as<int>(N);
+  node_ranges<<<ceil_div(N, kThreads), kThreads, 0, s>>>(keys, N, sk, T.n_src, tk, T.n_trg, slo, shi, tlo, thi);
+  int* coll = T.colleague.as<int>(N * 27);
+  for (int d = 0; d <= D; ++d) {
+    const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
+    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys, base, nl, coll);
+  }
+  // 9. compact node lists
+  {
+    int* flag = ctx.t[3].as<int>(N);
+    int* offs = ctx.t[23].as<int>(N);
+    auto compact = [&](auto pred, DevBuf& out, int* map) -> long {
+      flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, pred, flag);
+      const long c = exclusive_scan(ctx, flag, offs, N);
+      int* o = out.as<int>(std::max(c, 1L));
+      compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, o, map);
+      return c;
+    };
+    T.n_sleaf = compact([=] __device__(long i) { return leaf[i] && shi[i] > slo[i]; }, T.sleaf, nullptr);
+    T.n_tleaf = compact([=] __device__(long i) { return leaf[i] && thi[i] > tlo[i]; }, T.tleaf, nullptr);
+    int* n2v = T.node2vsrc.as<int>(N);
+    T.n_vsrc = compact([=] __device__(long i) { return !leaf[i] && shi[i] > slo[i]; }, T.vsrc, n2v);
+    // lists: count
+    int* pc = ctx.t[4].as<int>(N);
+    int* xc = ctx.t[5].as<int>(N);
+    int* wc = ctx.t[6].as<int>(N);
+    int* vc = ctx.t[0].as<int>(N);
+    const long nsrf = ctx.ns;
+    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 0, pc, xc,
+                                                 wc, vc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    int* po = T.p_off.as<int>(N + 1);
+    int* xo = T.x_off.as<int>(N + 1);
+    int* wo = T.w_off.as<int>(N + 1);
+    T.n_p2p = exclusive_scan(ctx, pc, po, N);
+    T.n_x = exclusive_scan(ctx, xc, xo, N);
+    T.n_w = exclusive_scan(ctx, wc, wo, N);
+    {
+      const int tot[3] = {(int)T.n_p2p, (int)T.n_x, (int)T.n_w};
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(po + N, &tot[0], sizeof(int), cudaMemcpyHostToDevice, s));
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(xo + N, &tot[1], sizeof(int), cudaMemcpyHostToDevice, s));
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(wo + N, &tot[2], sizeof(int), cudaMemcpyHostToDevice, s));
+      PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+    }
+    int* pl = T.p_list.as<int>(std::max(T.n_p2p, 1L));
+    int* xl = T.x_list.as<int>(std::max(T.n_x, 1L));
+    int* wl = T.w_list.as<int>(std::max(T.n_w, 1L));
+    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 1, nullptr,
+                                                 nullptr, nullptr, nullptr, po, xo, wo, pl, xl, wl);
+    T.n_xtrg = compact([=] __device__(long i) { return xc[i] > 0; }, T.xtrg, nullptr);
+    T.n_vtrg = compact([=] __device__(long i) { return vc[i] > 0; }, T.vtrg, nullptr);
+    int* vt = T.vtab.as<int>(std::max(T.n_vtrg, 1L) * 26);
+    if (T.n_vtrg > 0)
+      fill_vtab<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), T.n_vtrg, coll, n2v, vt);
+  }
+  // 10. point -> leaf and local coordinates
+  {
+    const long n_leaves_all = N - n_int_total;
+    int* flag = ctx.t[3].as<int>(N);
+    int* offs = ctx.t[23].as<int>(N);
+    flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, [=] __device__(long i) { return leaf[i] != 0; }, flag);
+    const long nl = exclusive_scan(ctx, flag, offs, N);
+    if (nl != n_leaves_all) throw std::runtime_error("octree build: leaf count mismatch");
+    int* leaves = ctx.t[0].as<int>(std::max(nl, 1L));
+    compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, leaves, nullptr);
+    const bool f32 = ctx.precision == 1;
+    const size_t rs = f32 ? sizeof(float) : sizeof(double);
+    void* sx = T.sx.ensure(std::max(T.n_src, 1L) * rs);
+    void* sy = T.sy.ensure(std::max(T.n_src, 1L) * rs);
+    void* sz = T.sz.ensure(std::max(T.n_src, 1L) * rs);
+    void* tx = T.tx.ensure(std::max(T.n_trg, 1L) * rs);
+    void* ty = T.ty.ensure(std::max(T.n_trg, 1L) * rs);
+    void* tz = T.tz.ensure(std::max(T.n_trg, 1L) * rs);
+    int* sl = T.src_leaf.as<int>(std::max(T.n_src, 1L));
+    int* tl = T.trg_leaf.as<int>(std::max(T.n_trg, 1L));
+    if (nl > 0) {
+      if (f32) {
+        // source coordinates are localized even when sl_den is NULL (unused then)
+        localize<float><<<nl, 128, 0, s>>>(leaves, nl, keys, slo, shi, coords_s.get<double>(), (float*)sx, (float*)sy,
+                                           (float*)sz, sl);
+        localize<float><<<nl, 128, 0, s>>>(leaves, nl, keys, tlo, thi, coords_t.get<double>(), (float*)tx, (float*)ty,
+                                           (float*)tz, tl);
+      } else {
+        localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, slo, shi, coords_s.get<double>(), (double*)sx,
+                                            (double*)sy, (double*)sz, sl);
+        localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, tlo, thi, coords_t.get<double>(), (double*)tx,
+                                            (double*)ty, (double*)tz, tl);
+      }
+    }
+  }
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+  PVFMM_CUDA_CHECK(cudaGetLastError());
+  T.valid = true;
+}
+
+}  // namespace pvfmm_b200
