@@ -113,6 +113,10 @@ const char* PVFMMGetLastError(void);
  * 7 D2D, 8 D2T+W+U (fused near field), 9 total.  Returns the number written. */
 int PVFMMGetStageTimes(const void* ctx, double* ms, int n);
 
+/* Number of this library's own CUDA kernels launched on ctx since its
+ * creation (library calls such as cuBLAS GEMMs and CUB sorts not counted). */
+long PVFMMGetLaunchCount(const void* ctx);
+
 /* Tree and evaluation introspection for parity tests.  `what`:
  *   0: number of nodes            1: tree depth
  *   2: node Morton coordinates (x, y, z, depth) as 4 x int64 per node
@@ -122,6 +126,9 @@ int PVFMMGetStageTimes(const void* ctx, double* ms, int n);
  *   8: downward check potentials   (n_nodes x ns*k1, double)
  *   9: source permutation (sorted -> input index) x int64
  *  10: target permutation x int64
+ *  11: 18 doubles of tree/list statistics: n_nodes, depth, n_sleaf, n_tleaf,
+ *      n_vsrc, n_vtrg, n_xtrg, list entries (p2p, x, w), pair counts (p2p,
+ *      x, w, d2t, s2u), n_leaves, n_src, n_trg
  * Copies at most `n` elements into out and returns the element count needed. */
 long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
 

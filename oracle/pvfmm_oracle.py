@@ -176,6 +176,19 @@ def key_int(X: int, Y: int, Z: int, depth: int) -> int:
     return (int(hi[0]) << 32) | int(lo[0])
 
 
+def nbr_list(X: int, Y: int, Z: int, depth: int) -> list:
+    """MortonId::NbrList at the node's own depth, non-periodic
+    (src/mortonid.cpp:15-55): the 3^3 same-depth cells around (X,Y,Z) that lie
+    in the unit box, in the order x fastest, then y, then z."""
+    w = TWO30 >> depth
+    out = []
+    for i in range(27):
+        x, y, z = X + (i % 3 - 1) * w, Y + ((i // 3) % 3 - 1) * w, Z + (i // 9 - 1) * w
+        if 0 <= x < TWO30 and 0 <= y < TWO30 and 0 <= z < TWO30:
+            out.append((x, y, z, depth))
+    return out
+
+
 def node_end_key(X: int, Y: int, Z: int, depth: int) -> int:
     """A key larger than every point key inside node (X,Y,Z,depth) and smaller
     than every key after the node's subtree in Morton order."""
@@ -340,23 +353,11 @@ class Tree:
         S = {d: set(v) for d, v in internal.items()}
         dmax = max(S)
         for l in range(dmax, 0, -1):
-            w = TWO30 >> l
             pmask = ~((TWO30 >> (l - 1)) - 1)
             tgt = S.setdefault(l - 1, set())
             for (X, Y, Z) in S.get(l, ()):
-                for dz in (-1, 0, 1):
-                    z = Z + dz * w
-                    if z < 0 or z >= TWO30:
-                        continue
-                    for dy in (-1, 0, 1):
-                        y = Y + dy * w
-                        if y < 0 or y >= TWO30:
-                            continue
-                        for dx in (-1, 0, 1):
-                            x = X + dx * w
-                            if x < 0 or x >= TWO30:
-                                continue
-                            tgt.add((x & pmask, y & pmask, z & pmask))
+                for (x, y, z, _) in nbr_list(X, Y, Z, l):
+                    tgt.add((x & pmask, y & pmask, z & pmask))
         return S
 
     def _build_nodes(self):
@@ -608,6 +609,52 @@ class Operators:
         self.ifft_map = np.array([(int(m * 2 - 0.5 - s[i, 0]), int(m * 2 - 0.5 - s[i, 1]), int(m * 2 - 0.5 - s[i, 2]))
                                   for i in range(self.ns)])
 
+    @classmethod
+    def from_arrays(cls, kernel: Kernel, m: int, arrays: dict) -> "Operators":
+        """Operators given as arrays in the layout of the CUDA library's
+        precompute (``PVFMMPrecompOperator``): uc2ue0/1, dc2de0/1 (dim x dim),
+        u2u (8*dim x dim, child-major rows), d2d (dim x 8*dim, child-major
+        columns) and vop (complex [f][26][8][8][ke][ke], divided by n3).  Lets
+        the oracle run on exactly the operators the GPU runs on."""
+        self = cls.__new__(cls)
+        self.kernel, self.m = kernel, m
+        self.ns = 6 * (m - 1) ** 2 + 2
+        ke = kernel.exp.k0
+        dim = self.ns * ke
+        self.uc2ue0 = arrays["uc2ue0"].reshape(dim, dim)
+        self.uc2ue1 = arrays["uc2ue1"].reshape(dim, dim)
+        self.dc2de0 = arrays["dc2de0"].reshape(dim, dim)
+        self.dc2de1 = arrays["dc2de1"].reshape(dim, dim)
+        self.u2u = list(arrays["u2u"].reshape(8, dim, dim))
+        d2d = arrays["d2d"].reshape(dim, 8, dim)
+        self.d2d = [np.ascontiguousarray(d2d[:, c, :]) for c in range(8)]
+        n1 = 2 * m
+        self.n1 = n1
+        n3 = n1 ** 3
+        vop = arrays["vop"].reshape(-1, 2)
+        vop = (vop[:, 0] + 1j * vop[:, 1]).reshape(n1, n1, n1 // 2 + 1, 26, 8, 8, ke, ke)
+        self.vhat = {}
+        for ci in range(27):
+            if ci == 13:
+                continue
+            o = ci if ci < 13 else ci - 1
+            po = np.array([ci % 3 - 1, (ci // 3) % 3 - 1, ci // 9 - 1])
+            for j1 in range(8):
+                b1 = np.array([j1 & 1, (j1 >> 1) & 1, (j1 >> 2) & 1])
+                for j2 in range(8):
+                    b2 = np.array([j2 & 1, (j2 >> 1) & 1, (j2 >> 2) & 1])
+                    rel = tuple(int(v) for v in (2 * po - b1 + b2))
+                    if max(abs(r) for r in rel) <= 1 or rel in self.vhat:
+                        continue
+                    self.vhat[rel] = vop[:, :, :, o, j1, j2] * n3
+        z = np.zeros(3)
+        s = surface(m, z, m - 1, 0)
+        self.fft_map = np.array([(int(m - 1 - s[i, 0] + 0.5), int(m - 1 - s[i, 1] + 0.5), int(m - 1 - s[i, 2] + 0.5))
+                                 for i in range(self.ns)])
+        self.ifft_map = np.array([(int(m * 2 - 0.5 - s[i, 0]), int(m * 2 - 0.5 - s[i, 1]), int(m * 2 - 0.5 - s[i, 2]))
+                                  for i in range(self.ns)])
+        return self
+
     def _v_operator(self, rel):
         m, n1, ke = self.m, self.n1, self.kernel.exp
         a = RAD0
@@ -668,13 +715,24 @@ class FMM:
         dc = np.zeros((nn, ns * k1e))
         out = np.zeros((len(self.trg), K.k1))
 
+        # All kernel evaluations use coordinates relative to the corner of the
+        # node being evaluated, as the reference does through coord_shift and
+        # surfaces built at c = 0 (fmm_pts.txx:2489-2496, 4645-4650, 4947-4952,
+        # 5262-5340); corner differences are exact dyadic numbers.
+        def rel(n, T):
+            return np.array([n.X - T.X, n.Y - T.Y, n.Z - T.Z], dtype=np.float64) / TWO30
+
+        def pts_rel(arr, lo, hi, T):
+            return arr[lo:hi] - self._corner(T)
+
         # --- S2U (fmm_pts.txx:2275-2637 + EvalListPts 4390-4426) ---------
         # The two pseudo-inverse factors are applied one after the other, as
         # the reference does: multiplying them out first loses the accuracy.
+        z3 = np.zeros(3)
         for i, n in enumerate(N):
             if n.leaf and n.n_src > 0:
-                c = self._corner(n)
-                chk = ke.eval(self.src[n.src[0]:n.src[1]], den[n.src[0]:n.src[1]], u_check_surf(m, c, n.depth))
+                chk = ke.eval(pts_rel(self.src, n.src[0], n.src[1], n), den[n.src[0]:n.src[1]],
+                              u_check_surf(m, z3, n.depth))
                 ue[i] = ((chk.reshape(-1) * 2.0 ** (-e_exp * n.depth)) @ ops.uc2ue0) @ ops.uc2ue1
         # --- U2U bottom-up (fmm_pts.txx:2602-2630, EvalList) ------------
         for d in range(tree.depth - 1, -1, -1):
@@ -690,24 +748,25 @@ class FMM:
         # --- X-list (fmm_pts.txx:4444-4736) ------------------------------
         for t, srcs in xl.items():
             T = N[t]
-            pts = d_check_surf(m, self._corner(T), T.depth)
+            pts = d_check_surf(m, z3, T.depth)
             for s in srcs:
                 S = N[s]
-                dc[t] += ke.eval(self.src[S.src[0]:S.src[1]], den[S.src[0]:S.src[1]], pts).reshape(-1)
+                dc[t] += ke.eval(pts_rel(self.src, S.src[0], S.src[1], T), den[S.src[0]:S.src[1]], pts).reshape(-1)
         # --- W-list (fmm_pts.txx:4746-5022) ------------------------------
         for t, srcs in wl.items():
             T = N[t]
-            tp = self.trg[T.trg[0]:T.trg[1]]
+            tp = pts_rel(self.trg, T.trg[0], T.trg[1], T)
             for s in srcs:
                 S = N[s]
-                out[T.trg[0]:T.trg[1]] += kt.eval(u_equiv_surf(m, self._corner(S), S.depth), ue[s], tp)
+                out[T.trg[0]:T.trg[1]] += kt.eval(u_equiv_surf(m, rel(S, T), S.depth), ue[s], tp)
         # --- U-list (fmm_pts.txx:5032-5418) ------------------------------
         for t, srcs in p2p.items():
             T = N[t]
             if not srcs:
                 continue
             idx = np.concatenate([np.arange(N[s].src[0], N[s].src[1]) for s in srcs])
-            out[T.trg[0]:T.trg[1]] += kt.eval(self.src[idx], den[idx], self.trg[T.trg[0]:T.trg[1]])
+            out[T.trg[0]:T.trg[1]] += kt.eval(self.src[idx] - self._corner(T), den[idx],
+                                              pts_rel(self.trg, T.trg[0], T.trg[1], T))
         # --- V-list via FFT (fmm_pts.txx:3597-3759, 2689-2858) ----------
         self._vlist(ue, dc, v1)
         # --- D2D top-down (fmm_pts.txx:3762-3790) ------------------------
@@ -722,8 +781,8 @@ class FMM:
         for i, n in enumerate(N):
             if n.leaf and n.n_trg > 0:
                 de = ((dc[i] * 2.0 ** (-e_exp * n.depth)) @ ops.dc2de0) @ ops.dc2de1
-                out[n.trg[0]:n.trg[1]] += kt.eval(d_equiv_surf(m, self._corner(n), n.depth), de,
-                                                  self.trg[n.trg[0]:n.trg[1]])
+                out[n.trg[0]:n.trg[1]] += kt.eval(d_equiv_surf(m, z3, n.depth), de,
+                                                  pts_rel(self.trg, n.trg[0], n.trg[1], n))
         self.ue, self.dc = ue, dc
         return out
 

@@ -81,6 +81,7 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMDestroyContextF": (None, [ctypes.POINTER(vp)]),
         "PVFMMGetLastError": (ctypes.c_char_p, []),
         "PVFMMGetStageTimes": (ci, [vp, vp, ci]),
+        "PVFMMGetLaunchCount": (cl, [vp]),
         "PVFMMGetTreeData": (cl, [vp, ci, vp, cl]),
         "PVFMMPrecompOperator": (cl, [ci, ci, ci, ci, vp, cl]),
     }
@@ -220,11 +221,22 @@ class FMMParticleContext:
         names = ["setup", "S2U", "U2U", "V-FFT", "V-Hadamard", "V-IFFT", "X-List", "D2D", "D2T+W+U", "total"]
         return dict(zip(names, buf.tolist()))
 
+    STAT_NAMES = ["n_nodes", "depth", "n_sleaf", "n_tleaf", "n_vsrc", "n_vtrg", "n_xtrg", "p2p_entries",
+                  "x_entries", "w_entries", "p2p_pairs", "x_pairs", "w_pairs", "d2t_pairs", "s2u_pairs",
+                  "n_leaves", "n_src", "n_trg"]
+
+    def tree_stats(self) -> dict:
+        """Sizes of the tree and lists of the last setup (for roofline bookkeeping)."""
+        return dict(zip(self.STAT_NAMES, self.tree_data(11).tolist()))
+
+    def launch_count(self) -> int:
+        return int(self._lib.PVFMMGetLaunchCount(self._ptr))
+
     def tree_data(self, what: int) -> np.ndarray:
         n = self._lib.PVFMMGetTreeData(self._ptr, what, None, 0)
         if n < 0:
             raise RuntimeError(last_error())
-        dt = np.float64 if what in (7, 8) else np.int64
+        dt = np.float64 if what in (7, 8, 11) else np.int64
         out = np.empty(n, dtype=dt)
         self._lib.PVFMMGetTreeData(self._ptr, what, _ptr(out), n)
         return out

@@ -73,7 +73,9 @@ void* create_context(double box_size, int n, int m, int kernel, int precision, b
     c.max_pts = n;
     c.precision = precision;
     c.float_api = float_api;
-    build_operators(kernel, m, precision == 1, c.hops);
+    // Both forms use the FP64-cutoff operators: the mixed form keeps the
+    // check->equivalent chain in FP64 (see eval.cu).
+    build_operators(kernel, m, false, c.hops);
     PVFMM_CUDA_CHECK(cudaGetDevice(&c.device));
     PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     if (cublasCreate(&c.cublas) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasCreate failed");
@@ -266,6 +268,15 @@ void PVFMMDestroyContextF(void** ctx) { destroy(ctx); }
 
 const char* PVFMMGetLastError(void) { return get_last_error(); }
 
+long PVFMMGetLaunchCount(const void* ctx) {
+  try {
+    return as_handle(ctx)->ctx.n_launch;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return -1;
+  }
+}
+
 int PVFMMGetStageTimes(const void* ctx, double* ms, int n) {
   try {
     Handle* h = as_handle(ctx);
@@ -379,6 +390,40 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n) {
         if (out)
           for (long i = 0; i < cnt && i < n; ++i) ((long long*)out)[i] = p[i];
         return cnt;
+      }
+      case 11: {
+        // [n_nodes, depth, n_sleaf, n_tleaf, n_vsrc, n_vtrg, n_xtrg, p2p list entries, x entries,
+        //  w entries, p2p pairs, x pairs (sources x check points), w pairs (surface x targets),
+        //  d2t pairs, s2u pairs, n_leaves, n_src, n_trg]
+        std::vector<int> slo(N), shi(N), tlo(N), thi(N), po(N + 1), xo(N + 1), wo(N + 1);
+        std::vector<unsigned char> lf(N);
+        PVFMM_CUDA_CHECK(cudaMemcpy(slo.data(), T.src_lo.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(shi.data(), T.src_hi.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(tlo.data(), T.trg_lo.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(thi.data(), T.trg_hi.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(po.data(), T.p_off.ptr, (N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(xo.data(), T.x_off.ptr, (N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(wo.data(), T.w_off.ptr, (N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        PVFMM_CUDA_CHECK(cudaMemcpy(lf.data(), T.leaf.ptr, N, cudaMemcpyDeviceToHost));
+        std::vector<int> pl(std::max(T.n_p2p, 1L)), xl(std::max(T.n_x, 1L));
+        if (T.n_p2p) PVFMM_CUDA_CHECK(cudaMemcpy(pl.data(), T.p_list.ptr, T.n_p2p * sizeof(int), cudaMemcpyDeviceToHost));
+        if (T.n_x) PVFMM_CUDA_CHECK(cudaMemcpy(xl.data(), T.x_list.ptr, T.n_x * sizeof(int), cudaMemcpyDeviceToHost));
+        double p2p = 0, xp = 0, wp = 0, d2t = 0, s2u = 0, nleaf = 0;
+        for (long t = 0; t < N; ++t) {
+          const double nt = thi[t] - tlo[t];
+          nleaf += lf[t];
+          for (int q = po[t]; q < po[t + 1]; ++q) p2p += nt * (shi[pl[q]] - slo[pl[q]]);
+          for (int q = xo[t]; q < xo[t + 1]; ++q) xp += (double)c.ns * (shi[xl[q]] - slo[xl[q]]);
+          wp += nt * (double)c.ns * (wo[t + 1] - wo[t]);
+          if (lf[t] && nt > 0) d2t += nt * c.ns;
+          if (lf[t]) s2u += (double)c.ns * (shi[t] - slo[t]);
+        }
+        const double v[18] = {(double)N, (double)T.depth, (double)T.n_sleaf, (double)T.n_tleaf, (double)T.n_vsrc,
+                              (double)T.n_vtrg, (double)T.n_xtrg, (double)T.n_p2p, (double)T.n_x, (double)T.n_w,
+                              p2p, xp, wp, d2t, s2u, nleaf, (double)T.n_src, (double)T.n_trg};
+        if (out)
+          for (long i = 0; i < 18 && i < n; ++i) ((double*)out)[i] = v[i];
+        return 18;
       }
       default:
         throw std::runtime_error("unknown tree data selector");

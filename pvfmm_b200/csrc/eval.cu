@@ -1,26 +1,39 @@
 // FMM evaluation on the device (FMM_Tree::RunFMM, reference
-// include/fmm_tree.txx:237-738, FMM_Pts eval halves in include/fmm_pts.txx).
+// include/fmm_tree.txx:237-738, evaluation halves of include/fmm_pts.txx).
 //
-// Data layout in HBM (Real = double for the plain form, float for the mixed form):
-//   points     sorted by Morton key, SoA coordinates relative to the centre of
-//              the point's leaf, densities [n_src][k0], values [n_trg][k1]
-//   UE, DC     per node, [n_nodes][ns*ke]: upward equivalent densities and
-//              downward check potentials (the reference's upward_equiv and
-//              dnward_equiv, fmm_pts.txx:1306-1480)
-//   spectra    per V-list parent, [parent][freq][child*ke+comp] complex
+// Data layout in HBM:
+//   points     sorted by Morton key; FP64 SoA coordinates relative to the
+//              centre of the point's leaf; FP64 densities [n_src][k0]
+//   UE, DC     FP64 per node, [n_nodes][ns*ke]: upward equivalent densities
+//              and downward check potentials (the reference's upward_equiv
+//              and dnward_equiv, fmm_pts.txx:1306-1480)
+//   spectra    per V-list parent, [parent][freq][child*ke+comp] complex, in
+//              the working precision Real
+// Precision forms:
+//   plain  Real = double everywhere.
+//   mixed  Real = float for the two dominant stages, the V-list (DFTs and
+//          Hadamard products) and the near field (U list P2P, W list, D2T
+//          target evaluation); FP32 tile sums are promoted to FP64 per
+//          tile.  The check->equivalent chain (S2U and X check potentials,
+//          the pseudo-inverse GEMMs, U2U, D2D) stays FP64: the SVD
+//          pseudo-inverse amplifies check-potential errors by up to 1/(4 eps
+//          max S), so FP32 check potentials would need the FP32 cutoff,
+//          which alone costs ~8e-7 relative error at m=8.
 // Stages:
-//   S2U   surface evaluation to the upward check surface + 2 GEMMs (pinv factors)
-//   U2U   one GEMM per level over the contiguous child blocks
+//   S2U   check-surface evaluation + 2 GEMMs (pinv factors, fmm_pts.txx:4390-4426)
+//   U2U   one GEMM per level over the contiguous child blocks (fmm_pts.txx:2017-2271)
 //   V     pruned DFT of the 8 children, Hadamard with the 26 parent offsets,
-//         pruned inverse DFT onto the children's check surfaces
-//   X     surface evaluation to the downward check surface
-//   D2D   one GEMM per level into the contiguous child blocks
-//   D2T   2 GEMMs (pinv factors), then together with W and U one fused
-//         near-field kernel per target leaf.
+//         pruned inverse DFT onto the children's check surfaces (fmm_pts.txx:2689-3759)
+//   X     check-surface evaluation (fmm_pts.txx:4444-4736)
+//   D2D   one GEMM per level into the contiguous child blocks (fmm_pts.txx:3762-3790)
+//   D2T   2 GEMMs (pinv factors), then with W and U one fused near-field
+//         kernel per target leaf (fmm_pts.txx:4246-4426, 4746-5022, 5032-5418).
 #include <cublas_v2.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 
 #include "fmm_context.cuh"
 
@@ -46,85 +59,192 @@ __device__ __forceinline__ void node_geom(const MKey& k, double& cx, double& cy,
 }
 
 // ---------------------------------------------------------------------------
-// Source tiles in shared memory.
+// Source tiles in shared memory and the per-thread evaluation loop.
 // ---------------------------------------------------------------------------
 template <class Real, int KS>
 struct Tile {
   Real x[kNT], y[kNT], z[kNT], f[KS][kNT];
+  // FP32 tiles carry the rounding remainder of each coordinate, so that the
+  // difference target - source is as accurate as FP32 rounding of the
+  // difference itself (close pairs dominate the gradient kernels).
+  Real xl[sizeof(Real) == 4 ? kNT : 1], yl[sizeof(Real) == 4 ? kNT : 1], zl[sizeof(Real) == 4 ? kNT : 1];
 };
 
-template <class Real, int Ker>
-__device__ __forceinline__ void accumulate_tile(const Tile<Real, KerDims<Ker>::KS>& tl, int n, Real px, Real py,
-                                                Real pz, Acc<Real>* acc) {
-  constexpr int KS = KerDims<Ker>::KS;
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    Real f[KS];
-#pragma unroll
-    for (int i = 0; i < KS; ++i) f[i] = tl.f[i][j];
-    ker_eval<Ker, Real>(px - tl.x[j], py - tl.y[j], pz - tl.z[j], f, acc);
+// Target coordinate as (hi, lo) in Real.
+template <class Real>
+struct Pt {
+  Real x, y, z, xl, yl, zl;
+};
+template <class Real>
+__device__ __forceinline__ Pt<Real> make_pt(double x, double y, double z) {
+  Pt<Real> p;
+  p.x = (Real)x;
+  p.y = (Real)y;
+  p.z = (Real)z;
+  p.xl = (Real)(x - (double)p.x);
+  p.yl = (Real)(y - (double)p.y);
+  p.zl = (Real)(z - (double)p.z);
+  return p;
+}
+
+template <class Real, int KS>
+__device__ __forceinline__ void tile_store(Tile<Real, KS>& tl, int i, double x, double y, double z) {
+  tl.x[i] = (Real)x;
+  tl.y[i] = (Real)y;
+  tl.z[i] = (Real)z;
+  if constexpr (sizeof(Real) == 4) {
+    tl.xl[i] = (Real)(x - (double)tl.x[i]);
+    tl.yl[i] = (Real)(y - (double)tl.y[i]);
+    tl.zl[i] = (Real)(z - (double)tl.z[i]);
   }
 }
 
-// Sources on a cube surface: centre offset (ox,oy,oz), points off + hr*u_k.
+template <class Real, int KS>
+__device__ __forceinline__ void tile_diff(const Tile<Real, KS>& tl, int j, const Pt<Real>& p, Real& rx, Real& ry,
+                                          Real& rz) {
+  if constexpr (sizeof(Real) == 4) {
+    rx = (p.x - tl.x[j]) + (p.xl - tl.xl[j]);
+    ry = (p.y - tl.y[j]) + (p.yl - tl.yl[j]);
+    rz = (p.z - tl.z[j]) + (p.zl - tl.zl[j]);
+  } else {
+    rx = p.x - tl.x[j];
+    ry = p.y - tl.y[j];
+    rz = p.z - tl.z[j];
+  }
+}
+
+// Sums sources j = j0, j0+js, ... < n of the tile into acc (FP64).  Two
+// independent partial sums in Real give ILP; the tile sum is promoted to
+// FP64, so FP32 rounding never accumulates over more than one tile.
 template <class Real, int Ker>
-__device__ void surface_sources(Tile<Real, KerDims<Ker>::KS>& tl, const Real* __restrict__ usurf, int ns, Real ox,
-                                Real oy, Real oz, Real hr, const Real* __restrict__ dens, bool active, Real px, Real py,
-                                Real pz, Acc<Real>* acc) {
+__device__ __forceinline__ void tile_sum(const Tile<Real, KerDims<Ker>::KS>& tl, int n, int j0, int js,
+                                         const Pt<Real>& p, double* acc) {
+  constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
+  Real u0[KT], u1[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) u0[k] = u1[k] = 0;
+  int j = j0;
+  for (; j + js < n; j += 2 * js) {
+    Real f0[KS], f1[KS];
+#pragma unroll
+    for (int i = 0; i < KS; ++i) {
+      f0[i] = tl.f[i][j];
+      f1[i] = tl.f[i][j + js];
+    }
+    Real rx, ry, rz;
+    tile_diff(tl, j, p, rx, ry, rz);
+    ker_eval<Ker, Real>(rx, ry, rz, f0, u0);
+    tile_diff(tl, j + js, p, rx, ry, rz);
+    ker_eval<Ker, Real>(rx, ry, rz, f1, u1);
+  }
+  if (j < n) {
+    Real f0[KS];
+#pragma unroll
+    for (int i = 0; i < KS; ++i) f0[i] = tl.f[i][j];
+    Real rx, ry, rz;
+    tile_diff(tl, j, p, rx, ry, rz);
+    ker_eval<Ker, Real>(rx, ry, rz, f0, u0);
+  }
+#pragma unroll
+  for (int k = 0; k < KT; ++k) acc[k] += (double)u0[k] + (double)u1[k];
+}
+
+// Work split of a block over a chunk of nc targets: thread t evaluates target
+// t % nc against the sources j == t / nc (mod G) of every tile.
+struct Split {
+  int nc, G, ti, g;
+  bool active;
+  __device__ explicit Split(int n_targets) {
+    nc = max(1, min(kNT, n_targets));
+    G = min(8, kNT / nc);
+    ti = threadIdx.x % nc;
+    g = threadIdx.x / nc;
+    active = g < G && ti < n_targets;
+  }
+};
+
+// Sources on a cube surface: points off + hr*u_k, FP64 densities.
+template <class Real, int Ker>
+__device__ void surface_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __restrict__ usurf, int ns, double ox,
+                                double oy, double oz, double hr, const double* __restrict__ dens, const Split& sp,
+                                const Pt<Real>& p, double* acc) {
   constexpr int KS = KerDims<Ker>::KS;
   for (int k0 = 0; k0 < ns; k0 += kNT) {
     const int n = min(kNT, ns - k0);
     __syncthreads();
     if (threadIdx.x < n) {
       const int k = k0 + threadIdx.x;
-      tl.x[threadIdx.x] = ox + hr * usurf[k * 3 + 0];
-      tl.y[threadIdx.x] = oy + hr * usurf[k * 3 + 1];
-      tl.z[threadIdx.x] = oz + hr * usurf[k * 3 + 2];
+      tile_store(tl, threadIdx.x, ox + hr * usurf[k * 3 + 0], oy + hr * usurf[k * 3 + 1], oz + hr * usurf[k * 3 + 2]);
 #pragma unroll
-      for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = dens[k * KS + i];
+      for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = (Real)dens[k * KS + i];
     }
     __syncthreads();
-    if (active) accumulate_tile<Real, Ker>(tl, n, px, py, pz, acc);
+    if (sp.active) tile_sum<Real, Ker>(tl, n, sp.g, sp.G, p, acc);
   }
 }
 
 // Sources = sorted points [lo,hi) of a leaf whose centre is at offset (ox,oy,oz).
 template <class Real, int Ker>
-__device__ void point_sources(Tile<Real, KerDims<Ker>::KS>& tl, const Real* __restrict__ sx, const Real* __restrict__ sy,
-                              const Real* __restrict__ sz, const Real* __restrict__ den, int lo, int hi, Real ox, Real oy,
-                              Real oz, bool active, Real px, Real py, Real pz, Acc<Real>* acc) {
+__device__ void point_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __restrict__ sx,
+                              const double* __restrict__ sy, const double* __restrict__ sz,
+                              const double* __restrict__ den, int lo, int hi, double ox, double oy, double oz,
+                              const Split& sp, const Pt<Real>& pt, double* acc) {
   constexpr int KS = KerDims<Ker>::KS;
   for (int p0 = lo; p0 < hi; p0 += kNT) {
     const int n = min(kNT, hi - p0);
     __syncthreads();
     if (threadIdx.x < n) {
       const int p = p0 + threadIdx.x;
-      tl.x[threadIdx.x] = sx[p] + ox;
-      tl.y[threadIdx.x] = sy[p] + oy;
-      tl.z[threadIdx.x] = sz[p] + oz;
+      tile_store(tl, threadIdx.x, sx[p] + ox, sy[p] + oy, sz[p] + oz);
 #pragma unroll
-      for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = den[(long)p * KS + i];
+      for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = (Real)den[(long)p * KS + i];
     }
     __syncthreads();
-    if (active) accumulate_tile<Real, Ker>(tl, n, px, py, pz, acc);
+    if (sp.active) tile_sum<Real, Ker>(tl, n, sp.g, sp.G, pt, acc);
+  }
+}
+
+// Adds the G partial sums of each target (deterministic order) and stores.
+template <int KT>
+__device__ void reduce_store(double (*red)[KT], const Split& sp, const double* acc, double scale, double* out,
+                             bool accumulate) {
+  __syncthreads();
+  if (sp.active)
+#pragma unroll
+    for (int k = 0; k < KT; ++k) red[threadIdx.x][k] = acc[k];
+  __syncthreads();
+  if (sp.active && sp.g == 0) {
+    double s[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) s[k] = red[sp.ti][k];
+    for (int g = 1; g < sp.G; ++g)
+#pragma unroll
+      for (int k = 0; k < KT; ++k) s[k] += red[g * sp.nc + sp.ti][k];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+      if (accumulate) out[sp.ti * KT + k] += s[k] * scale;
+      else out[sp.ti * KT + k] = s[k] * scale;
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Near field of one target leaf: D2T (own downward equivalent surface), W
-// (upward equivalent surfaces) and U (points), fused (fmm_pts.txx:4246-4426,
-// 4746-5022, 5032-5418).  One block per target leaf.
+// (upward equivalent surfaces) and U (points), fused.  One block per leaf.
 // ---------------------------------------------------------------------------
 template <class Real, int Ker>
 __global__ void __launch_bounds__(kNT) near_field_kernel(
     const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo, const int* __restrict__ thi,
     const int* __restrict__ slo, const int* __restrict__ shi, const int* __restrict__ p_off, const int* __restrict__ p_list,
-    const int* __restrict__ w_off, const int* __restrict__ w_list, const Real* __restrict__ tx, const Real* __restrict__ ty,
-    const Real* __restrict__ tz, const Real* __restrict__ sx, const Real* __restrict__ sy, const Real* __restrict__ sz,
-    const Real* __restrict__ den, const Real* __restrict__ ue, const Real* __restrict__ de, const Real* __restrict__ usurf,
-    int ns, Real scale, Real* __restrict__ pot) {
+    const int* __restrict__ w_off, const int* __restrict__ w_list, const double* __restrict__ tx,
+    const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ sx,
+    const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ den,
+    const double* __restrict__ ue, const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
+    double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   __shared__ Tile<Real, KS> tl;
+  __shared__ Tile<double, KS> tl64;
+  __shared__ double red[kNT][KT];
   const int b = blockIdx.x;
   const int T = tleaf[b];
   double cx, cy, cz, half;
@@ -133,334 +253,412 @@ __global__ void __launch_bounds__(kNT) near_field_kernel(
   const int t0 = tlo[T], nt = thi[T] - t0;
   const int dim = ns * KS;
   for (int c0 = 0; c0 < nt; c0 += kNT) {
-    const int t = c0 + threadIdx.x;
-    const bool active = t < nt;
-    Real px = 0, py = 0, pz = 0;
-    if (active) {
-      px = tx[t0 + t];
-      py = ty[t0 + t];
-      pz = tz[t0 + t];
+    const Split sp(nt - c0);
+    const int t = t0 + c0 + sp.ti;
+    double qx = 0, qy = 0, qz = 0;
+    if (sp.active) {
+      qx = tx[t];
+      qy = ty[t];
+      qz = tz[t];
     }
-    Acc<Real> acc[KT];
+    const Pt<Real> pt = make_pt<Real>(qx, qy, qz);
+    const Pt<double> pt64 = make_pt<double>(qx, qy, qz);
+    double acc[KT];
 #pragma unroll
-    for (int k = 0; k < KT; ++k) acc[k].init();
-    // D2T: downward equivalent surface of T (radius RAD1)
-    if (de) surface_sources<Real, Ker>(tl, usurf, ns, 0, 0, 0, (Real)(half * kRad1), de + (long)b * dim, active, px, py, pz, acc);
-    // W: upward equivalent surfaces (radius RAD0) of the W-list nodes
+    for (int k = 0; k < KT; ++k) acc[k] = 0;
+    // D2T in FP64 in both forms: the downward equivalent densities come from
+    // the FP64-cutoff pseudo-inverse, whose large cancelling components only
+    // FP64 sums resolve.
+    if (de) surface_sources<double, Ker>(tl64, usurf, ns, 0, 0, 0, half * kRad1, de + (long)b * dim, sp, pt64, acc);
     for (int w = w_off[T]; w < w_off[T + 1]; ++w) {
       const int S = w_list[w];
       double sxc, syc, szc, sh;
       int dS;
       node_geom(keys[S], sxc, syc, szc, sh, dS);
-      surface_sources<Real, Ker>(tl, usurf, ns, (Real)(sxc - cx), (Real)(syc - cy), (Real)(szc - cz), (Real)(sh * kRad0),
-                                 ue + (long)S * dim, active, px, py, pz, acc);
+      surface_sources<Real, Ker>(tl, usurf, ns, sxc - cx, syc - cy, szc - cz, sh * kRad0, ue + (long)S * dim, sp, pt,
+                                 acc);
     }
-    // U: point-to-point from the P2P list
     for (int q = p_off[T]; q < p_off[T + 1]; ++q) {
       const int S = p_list[q];
       double sxc, syc, szc, sh;
       int dS;
       node_geom(keys[S], sxc, syc, szc, sh, dS);
-      point_sources<Real, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], (Real)(sxc - cx), (Real)(syc - cy), (Real)(szc - cz),
-                               active, px, py, pz, acc);
+      point_sources<Real, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], sxc - cx, syc - cy, szc - cz, sp, pt, acc);
     }
-    if (active)
-#pragma unroll
-      for (int k = 0; k < KT; ++k) pot[(long)(t0 + t) * KT + k] = acc[k].get() * scale;
+    reduce_store<KT>(red, sp, acc, scale, pot + (long)(t0 + c0) * KT, false);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Sources -> check surface of a node.  mode 0 (S2U, fmm_pts.txx:2275-2637):
-// node = sleaf[b], sources = its own points, output row b of `out` scaled by
-// scale*2^-depth (the level factor of the check->equivalent operator).
-// mode 1 (X, fmm_pts.txx:4444-4736): node = xtrg[b], sources = the X list,
-// added to DC[node].
+// Sources -> check surface of a node, FP64.  mode 0 (S2U, fmm_pts.txx:
+// 2275-2637): node = sleaf[b], sources = its own points, output row b of
+// `out` scaled by scale*2^-depth (level factor of the check->equivalent
+// operator).  mode 1 (X, fmm_pts.txx:4444-4736): node = xtrg[b], sources =
+// the X list, added to DC[node].
 // ---------------------------------------------------------------------------
-template <class Real, int Ker>
+template <int Ker>
 __global__ void __launch_bounds__(kNT) surface_check_kernel(
     int mode, const int* __restrict__ nodes, const MKey* __restrict__ keys, const int* __restrict__ slo,
-    const int* __restrict__ shi, const int* __restrict__ x_off, const int* __restrict__ x_list, const Real* __restrict__ sx,
-    const Real* __restrict__ sy, const Real* __restrict__ sz, const Real* __restrict__ den, const Real* __restrict__ usurf,
-    int ns, Real rad, Real scale, Real* __restrict__ out) {
-  constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
-  __shared__ Tile<Real, KS> tl;
+    const int* __restrict__ shi, const int* __restrict__ x_off, const int* __restrict__ x_list,
+    const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz,
+    const double* __restrict__ den, const double* __restrict__ usurf, int ns, double rad, double scale,
+    double* __restrict__ out) {
+  constexpr int KT = KerDims<Ker>::KT;
+  __shared__ Tile<double, KerDims<Ker>::KS> tl;
+  __shared__ double red[kNT][KT];
   const int b = blockIdx.x;
   const int T = nodes[b];
   double cx, cy, cz, half;
   int dT;
   node_geom(keys[T], cx, cy, cz, half, dT);
-  const Real hr = (Real)(half * rad);
+  const double hr = half * rad;
   const int dim = ns * KT;
-  Real* o = mode == 0 ? out + (long)b * dim : out + (long)T * dim;
-  const Real oscale = mode == 0 ? (Real)((double)scale * ldexp(1.0, -dT)) : scale;
+  double* o = mode == 0 ? out + (long)b * dim : out + (long)T * dim;
+  const double oscale = mode == 0 ? scale * ldexp(1.0, -dT) : scale;
   for (int c0 = 0; c0 < ns; c0 += kNT) {
-    const int k = c0 + threadIdx.x;
-    const bool active = k < ns;
-    Real px = 0, py = 0, pz = 0;
-    if (active) {
+    const Split sp(ns - c0);
+    const int k = c0 + sp.ti;
+    double px = 0, py = 0, pz = 0;
+    if (sp.active) {
       px = hr * usurf[k * 3 + 0];
       py = hr * usurf[k * 3 + 1];
       pz = hr * usurf[k * 3 + 2];
     }
-    Acc<Real> acc[KT];
+    const Pt<double> pt = make_pt<double>(px, py, pz);
+    double acc[KT];
 #pragma unroll
-    for (int c = 0; c < KT; ++c) acc[c].init();
+    for (int c = 0; c < KT; ++c) acc[c] = 0;
     if (mode == 0) {
-      point_sources<Real, Ker>(tl, sx, sy, sz, den, slo[T], shi[T], 0, 0, 0, active, px, py, pz, acc);
+      point_sources<double, Ker>(tl, sx, sy, sz, den, slo[T], shi[T], 0, 0, 0, sp, pt, acc);
     } else {
       for (int q = x_off[T]; q < x_off[T + 1]; ++q) {
         const int S = x_list[q];
         double sxc, syc, szc, sh;
         int dS;
         node_geom(keys[S], sxc, syc, szc, sh, dS);
-        point_sources<Real, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], (Real)(sxc - cx), (Real)(syc - cy),
-                                 (Real)(szc - cz), active, px, py, pz, acc);
+        point_sources<double, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], sxc - cx, syc - cy, szc - cz, sp, pt, acc);
       }
     }
-    if (active) {
-      if (mode == 0) {
-#pragma unroll
-        for (int c = 0; c < KT; ++c) o[k * KT + c] = acc[c].get() * oscale;
-      } else {
-#pragma unroll
-        for (int c = 0; c < KT; ++c) o[k * KT + c] += acc[c].get() * oscale;
-      }
-    }
+    reduce_store<KT>(red, sp, acc, oscale, o + c0 * KT, mode == 1);
   }
 }
 
 // ---------------------------------------------------------------------------
 // V-list: pruned separable DFTs over the (2m)^3 grid (FFT_UpEquiv /
 // FFT_Check2Equiv, fmm_pts.txx:2689-2858) and the Hadamard products
-// (VListHadamard, fmm_pts.txx:3249-3344).  Only the m^3 corner that holds
-// the upward equivalent surface is transformed forward, and only the m^3
-// corner that holds the check surface is produced by the inverse.
+// (VListHadamard, fmm_pts.txx:3249-3344).  Only the m^3 corner holding the
+// upward equivalent surface enters the forward transform and only the m^3
+// corner holding the check surface is produced by the inverse.  The grid
+// size is a compile-time constant.  A block handles G grids (child x
+// component) of one parent.
 // ---------------------------------------------------------------------------
-struct FftDims {
-  int m, n1, nh, n3h, ns, ke, G;
+template <class Real, int M>
+struct FftSizes {
+  static constexpr int N1 = 2 * M, NH = M + 1, M3 = M * M * M, N3H = N1 * N1 * NH;
+  static constexpr size_t up_grid_bytes = sizeof(Real) * (M3 + 2 * (M * M * NH + M * N1 * NH));
+  static constexpr size_t dn_grid_bytes = sizeof(Real) * (2 * N3H + 2 * (M * N1 * NH + M * M * NH) + M3);
+  static constexpr size_t tw_bytes = sizeof(Real) * 2 * N1;
 };
 
-template <class Real>
-__global__ void fft_up_kernel(FftDims fd, const int* __restrict__ vsrc, const int* __restrict__ child0,
-                              const Real* __restrict__ ue, const int* __restrict__ fft_map, Cplx<Real>* __restrict__ spec) {
-  extern __shared__ unsigned char smem_raw[];
-  Real* sm = reinterpret_cast<Real*>(smem_raw);
-  const int m = fd.m, n1 = fd.n1, nh = fd.nh, ns = fd.ns, ke = fd.ke, G = fd.G;
-  const int m3 = m * m * m;
+template <class Real, int M>
+__global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
+                                                     const int* __restrict__ child0, const double* __restrict__ ue,
+                                                     const int* __restrict__ fft_map, int ns,
+                                                     Cplx<Real>* __restrict__ spec) {
+  using F = FftSizes<Real, M>;
+  constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* twr = reinterpret_cast<Real*>(smem_raw);
+  Real* twi = twr + N1;
+  Real* g = twi + N1;                                          // G * M3
+  Cplx<Real>* a1 = reinterpret_cast<Cplx<Real>*>(g + G * M3);  // G * M*M*NH
+  Cplx<Real>* a2 = a1 + G * M * M * NH;                        // G * M*N1*NH
+  const int q = blockIdx.x / ngroups;
+  const int gb = (blockIdx.x % ngroups) * G;
   const int ngrid = 8 * ke;
-  Real* twr = sm;
-  Real* twi = twr + n1;
-  Real* g = twi + n1;                          // G * m3
-  Cplx<Real>* a1 = reinterpret_cast<Cplx<Real>*>(g + G * m3);  // G * m*m*nh
-  Cplx<Real>* a2 = a1 + G * m * m * nh;        // G * m*n1*nh
-  const int q = blockIdx.x;
+  const int gn = min(G, ngrid - gb);
   const int P = vsrc[q];
   const int c0 = child0[P];
   const int dim = ns * ke;
-  for (int j = threadIdx.x; j < n1; j += blockDim.x) {
+  for (int j = threadIdx.x; j < N1; j += blockDim.x) {
     double s, c;
-    sincospi(-2.0 * j / n1, &s, &c);
+    sincospi(-2.0 * j / N1, &s, &c);
     twr[j] = (Real)c;
     twi[j] = (Real)s;
   }
-  Cplx<Real>* out = spec + (long)q * fd.n3h * ngrid;
-  for (int gb = 0; gb < ngrid; gb += G) {
-    const int gn = min(G, ngrid - gb);
-    __syncthreads();
-    for (int i = threadIdx.x; i < gn * m3; i += blockDim.x) g[i] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < gn * ns; i += blockDim.x) {
-      const int gi = i / ns, k = i % ns;
-      const int gg = gb + gi, c = gg / ke, comp = gg % ke;
-      const int idx = fft_map[k];  // x + n1*y + n1*n1*z, all < m
-      const int x = idx % n1, y = (idx / n1) % n1, z = idx / (n1 * n1);
-      g[gi * m3 + x + m * (y + m * z)] = ue[(long)(c0 + c) * dim + k * ke + comp];
+  for (int i = threadIdx.x; i < gn * M3; i += blockDim.x) g[i] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * ns; i += blockDim.x) {
+    const int gi = i / ns, k = i % ns;
+    const int gg = gb + gi, c = gg / ke, comp = gg % ke;
+    const int idx = fft_map[k];  // x + N1*y + N1*N1*z, all < M
+    const int x = idx % N1, y = (idx / N1) % N1, z = idx / (N1 * N1);
+    g[gi * M3 + x + M * (y + M * z)] = (Real)ue[(long)(c0 + c) * dim + k * ke + comp];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * M * M * NH; i += blockDim.x) {  // x -> kx (real input)
+    const int kx = i % NH, yz = i / NH;
+    const Real* row = g + (yz / (M * M)) * M3 + M * (yz % (M * M));
+    Real re = 0, im = 0;
+#pragma unroll
+    for (int x = 0; x < M; ++x) {
+      const int w = (kx * x) % N1;
+      re += row[x] * twr[w];
+      im += row[x] * twi[w];
     }
-    __syncthreads();
-    // x -> kx (real input)
-    for (int i = threadIdx.x; i < gn * m * m * nh; i += blockDim.x) {
-      const int kx = i % nh, y = (i / nh) % m, z = (i / (nh * m)) % m, gi = i / (nh * m * m);
-      const Real* row = g + gi * m3 + m * (y + m * z);
-      Real re = 0, im = 0;
-      for (int x = 0; x < m; ++x) {
-        const int w = (kx * x) % n1;
-        re += row[x] * twr[w];
-        im += row[x] * twi[w];
-      }
-      a1[i] = {re, im};
+    a1[i] = {re, im};
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * M * N1 * NH; i += blockDim.x) {  // y -> ky
+    const int kx = i % NH, ky = (i / NH) % N1, zg = i / (NH * N1);  // zg = gi*M + z
+    const Cplx<Real>* col = a1 + (zg * M) * NH + kx;
+    Real re = 0, im = 0;
+#pragma unroll
+    for (int y = 0; y < M; ++y) {
+      const int w = (ky * y) % N1;
+      const Cplx<Real> v = col[y * NH];
+      re += v.re * twr[w] - v.im * twi[w];
+      im += v.re * twi[w] + v.im * twr[w];
     }
-    __syncthreads();
-    // y -> ky
-    for (int i = threadIdx.x; i < gn * m * n1 * nh; i += blockDim.x) {
-      const int kx = i % nh, ky = (i / nh) % n1, z = (i / (nh * n1)) % m, gi = i / (nh * n1 * m);
-      const Cplx<Real>* col = a1 + ((gi * m + z) * m) * nh + kx;
-      Real re = 0, im = 0;
-      for (int y = 0; y < m; ++y) {
-        const int w = (ky * y) % n1;
-        const Cplx<Real> v = col[y * nh];
-        re += v.re * twr[w] - v.im * twi[w];
-        im += v.re * twi[w] + v.im * twr[w];
-      }
-      a2[i] = {re, im};
+    a2[i] = {re, im};
+  }
+  __syncthreads();
+  Cplx<Real>* out = spec + (long)q * N3H * ngrid;
+  for (int i = threadIdx.x; i < gn * N3H; i += blockDim.x) {  // z -> kz, stored spec[q][f][grid]
+    const int gi = i % gn, f = i / gn;
+    const int kx = f % NH, ky = (f / NH) % N1, kz = f / (NH * N1);
+    const Cplx<Real>* col = a2 + ((gi * M) * N1 + ky) * NH + kx;
+    Real re = 0, im = 0;
+#pragma unroll
+    for (int z = 0; z < M; ++z) {
+      const int w = (kz * z) % N1;
+      const Cplx<Real> v = col[z * N1 * NH];
+      re += v.re * twr[w] - v.im * twi[w];
+      im += v.re * twi[w] + v.im * twr[w];
     }
-    __syncthreads();
-    // z -> kz, written as spec[q][f][grid]
-    for (int i = threadIdx.x; i < gn * fd.n3h; i += blockDim.x) {
-      const int gi = i % gn, f = i / gn;
-      const int kx = f % nh, ky = (f / nh) % n1, kz = f / (nh * n1);
-      const Cplx<Real>* col = a2 + ((gi * m) * n1 + ky) * nh + kx;
-      Real re = 0, im = 0;
-      for (int z = 0; z < m; ++z) {
-        const int w = (kz * z) % n1;
-        const Cplx<Real> v = col[z * n1 * nh];
-        re += v.re * twr[w] - v.im * twi[w];
-        im += v.re * twi[w] + v.im * twr[w];
-      }
-      out[(long)f * ngrid + gb + gi] = {re, im};
-    }
+    out[(long)f * ngrid + gb + gi] = {re, im};
   }
 }
 
-// One thread per (target parent, frequency); the 26 parent offsets are walked
-// in the same order by every thread, so the operator loads are uniform.
-template <class Real, int KE>
+template <class Real, int M>
+__global__ void __launch_bounds__(256) ifft_dn_kernel(int ke, int G, int ngroups, const int* __restrict__ vtrg,
+                                                      const int* __restrict__ child0, const MKey* __restrict__ keys,
+                                                      const Cplx<Real>* __restrict__ spec,
+                                                      const int* __restrict__ ifft_map, int ns,
+                                                      double* __restrict__ dc) {
+  using F = FftSizes<Real, M>;
+  constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* twr = reinterpret_cast<Real*>(smem_raw);
+  Real* twi = twr + N1;
+  Cplx<Real>* S = reinterpret_cast<Cplx<Real>*>(twi + N1);  // G * N3H
+  Cplx<Real>* b1 = S + G * N3H;                             // G * M*N1*NH
+  Cplx<Real>* b2 = b1 + G * M * N1 * NH;                    // G * M*M*NH
+  Real* o = reinterpret_cast<Real*>(b2 + G * M * M * NH);   // G * M3
+  const int vt = blockIdx.x / ngroups;
+  const int gb = (blockIdx.x % ngroups) * G;
+  const int ngrid = 8 * ke;
+  const int gn = min(G, ngrid - gb);
+  const int P = vtrg[vt];
+  const int c0 = child0[P];
+  unsigned int X, Y, Z, dP;
+  decode_key(keys[P], X, Y, Z, dP);
+  const double lscale = ldexp(1.0, (int)dP + 1);  // 2^(trg_scal * level of the children)
+  const int dim = ns * ke;
+  for (int j = threadIdx.x; j < N1; j += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * j / N1, &s, &c);  // inverse twiddles
+    twr[j] = (Real)c;
+    twi[j] = (Real)s;
+  }
+  const Cplx<Real>* in = spec + (long)vt * N3H * ngrid;
+  for (int i = threadIdx.x; i < gn * N3H; i += blockDim.x) {
+    const int gi = i % gn, f = i / gn;
+    S[gi * N3H + f] = in[(long)f * ngrid + gb + gi];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * M * N1 * NH; i += blockDim.x) {  // kz -> z in [M, 2M)
+    const int kx = i % NH, ky = (i / NH) % N1, zp = (i / (NH * N1)) % M, gi = i / (NH * N1 * M);
+    const int z = M + zp;
+    const Cplx<Real>* col = S + gi * N3H + ky * NH + kx;
+    Real re = 0, im = 0;
+#pragma unroll
+    for (int kz = 0; kz < N1; ++kz) {
+      const int w = (kz * z) % N1;
+      const Cplx<Real> v = col[kz * N1 * NH];
+      re += v.re * twr[w] - v.im * twi[w];
+      im += v.re * twi[w] + v.im * twr[w];
+    }
+    b1[i] = {re, im};
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * M * M * NH; i += blockDim.x) {  // ky -> y in [M, 2M)
+    const int kx = i % NH, yp = (i / NH) % M, zg = i / (NH * M);  // zg = gi*M + zp
+    const int y = M + yp;
+    const Cplx<Real>* col = b1 + (zg * N1) * NH + kx;
+    Real re = 0, im = 0;
+#pragma unroll
+    for (int ky = 0; ky < N1; ++ky) {
+      const int w = (ky * y) % N1;
+      const Cplx<Real> v = col[ky * NH];
+      re += v.re * twr[w] - v.im * twi[w];
+      im += v.re * twi[w] + v.im * twr[w];
+    }
+    b2[i] = {re, im};
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * M3; i += blockDim.x) {  // kx -> x in [M, 2M), c2r
+    const int xp = i % M, zy = i / M;  // zy = (gi*M + zp)*M + yp
+    const int x = M + xp;
+    const Cplx<Real>* row = b2 + zy * NH;
+    Real acc = 0;
+#pragma unroll
+    for (int kx = 0; kx < NH; ++kx) {
+      const int w = (kx * x) % N1;
+      const Cplx<Real> v = row[kx];
+      const Real t = v.re * twr[w] - v.im * twi[w];
+      acc += (kx == 0 || 2 * kx == N1) ? t : (Real)2 * t;
+    }
+    o[i] = acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < gn * ns; i += blockDim.x) {
+    const int gi = i / ns, k = i % ns;
+    const int gg = gb + gi, c = gg / ke, comp = gg % ke;
+    const int idx = ifft_map[k];
+    const int x = idx % N1 - M, y = (idx / N1) % N1 - M, z = idx / (N1 * N1) - M;
+    dc[(long)(c0 + c) * dim + k * ke + comp] += (double)o[gi * M3 + x + M * (y + M * z)] * lscale;
+  }
+}
+
+// 16-byte asynchronous global->shared copy; src_bytes = 0 zero-fills.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Hadamard products (VListHadamard, fmm_pts.txx:3249-3344), organised as a
+// register-tiled SIMT product per frequency f:
+//   OUT[P][j1] += sum_{offset o, source child j2} M[f][o][j1][j2] * IN[Q_o(P)][f][j2].
+// A block owns 128*PB target parents at one frequency; a thread owns PB of
+// them and all their 8 x ke outputs.  The offset blocks of frequency f sit in
+// shared memory (chunks of OC offsets), read by every thread at the same
+// address (broadcast).  The neighbour spectra of offset o+1 are copied
+// asynchronously into a second shared buffer while offset o is computed;
+// a thread only reads the rows it copied itself, so waiting on its own copy
+// group is enough.  Missing neighbours are zero-filled and skipped.
+template <class Real, int KE, int PB, int OC>
 __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, const int* __restrict__ vtab,
                                                        const Cplx<Real>* __restrict__ spec_in,
                                                        const Cplx<Real>* __restrict__ vop,
                                                        Cplx<Real>* __restrict__ spec_out) {
   constexpr int NG = 8 * KE;
-  const long vt = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  constexpr int BLK = 64 * KE * KE;                              // complex entries per offset
+  constexpr int ROW = NG * sizeof(Cplx<Real>) / 16;              // 16-byte chunks per spectrum row
+  constexpr int STRIDE = NG + 16 / (int)sizeof(Cplx<Real>) * 1;  // padded row (complex), breaks bank aliasing
+  constexpr int NT = 128;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cplx<Real>* Ms = reinterpret_cast<Cplx<Real>*>(smem_raw);      // OC * BLK
+  Cplx<Real>* xb = Ms + OC * BLK;                                // 2 * NT*PB * STRIDE
   const int f = blockIdx.y;
-  if (vt >= n_vtrg) return;
-  Real ar[NG], ai[NG];
+  const long base = (long)blockIdx.x * NT * PB + threadIdx.x;
+  Real ar[PB][NG], ai[PB][NG];
 #pragma unroll
-  for (int j = 0; j < NG; ++j) ar[j] = ai[j] = 0;
-  for (int o = 0; o < 26; ++o) {
-    const int q = vtab[vt * 26 + o];
-    if (q < 0) continue;
-    const Cplx<Real>* in = spec_in + ((long)q * n3h + f) * NG;
-    const Cplx<Real>* M = vop + ((long)f * 26 + o) * 64 * KE * KE;
+  for (int k = 0; k < PB; ++k)
 #pragma unroll
-    for (int j2 = 0; j2 < 8; ++j2) {
-      Cplx<Real> x[KE];
+    for (int j = 0; j < NG; ++j) ar[k][j] = ai[k][j] = 0;
+  auto issue = [&](int o, int buf, int* q) {
 #pragma unroll
-      for (int i = 0; i < KE; ++i) x[i] = in[j2 * KE + i];
+    for (int k = 0; k < PB; ++k) {
+      const long p = base + (long)k * NT;
+      q[k] = (o < 26 && p < n_vtrg) ? __ldg(vtab + (long)o * n_vtrg + p) : -1;
+      const Cplx<Real>* src = spec_in + ((long)(q[k] < 0 ? 0 : q[k]) * n3h + f) * NG;
+      Cplx<Real>* dst = xb + ((long)buf * NT * PB + threadIdx.x + k * NT) * STRIDE;
 #pragma unroll
-      for (int j1 = 0; j1 < 8; ++j1)
+      for (int c = 0; c < ROW; ++c)
+        cp_async16(reinterpret_cast<unsigned char*>(dst) + 16 * c, reinterpret_cast<const unsigned char*>(src) + 16 * c,
+                   q[k] >= 0 ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+  int qc[PB], qn[PB];
+  issue(0, 0, qc);
+  for (int oc = 0; oc < 26; oc += OC) {
+    const int no = min(OC, 26 - oc);
+    __syncthreads();
+    const Cplx<Real>* src = vop + ((long)f * 26 + oc) * BLK;
+    for (int i = threadIdx.x; i < no * BLK; i += NT) Ms[i] = src[i];
+    __syncthreads();
+    for (int oo = 0; oo < no; ++oo) {
+      const int o = oc + oo;
+      issue(o + 1, (o + 1) & 1, qn);   // empty group past the last offset
+      cp_async_wait<1>();              // this thread's rows of offset o have landed
+      const Cplx<Real>* Mo = Ms + oo * BLK;
 #pragma unroll
-        for (int i = 0; i < KE; ++i)
+      for (int k = 0; k < PB; ++k) {
+        if (qc[k] < 0) continue;
+        const Cplx<Real>* xr = xb + ((long)(o & 1) * NT * PB + threadIdx.x + k * NT) * STRIDE;
 #pragma unroll
-          for (int k = 0; k < KE; ++k) {
-            const Cplx<Real> a = M[((j1 * 8 + j2) * KE + i) * KE + k];
-            ar[j1 * KE + k] += a.re * x[i].re - a.im * x[i].im;
-            ai[j1 * KE + k] += a.re * x[i].im + a.im * x[i].re;
-          }
+        for (int j2 = 0; j2 < 8; ++j2) {
+          Cplx<Real> x[KE];
+#pragma unroll
+          for (int i = 0; i < KE; ++i) x[i] = xr[j2 * KE + i];
+#pragma unroll
+          for (int j1 = 0; j1 < 8; ++j1)
+#pragma unroll
+            for (int i = 0; i < KE; ++i)
+#pragma unroll
+              for (int c = 0; c < KE; ++c) {
+                const Cplx<Real> a = Mo[((j1 * 8 + j2) * KE + i) * KE + c];
+                ar[k][j1 * KE + c] += a.re * x[i].re - a.im * x[i].im;
+                ai[k][j1 * KE + c] += a.re * x[i].im + a.im * x[i].re;
+              }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < PB; ++k) qc[k] = qn[k];
     }
   }
-  Cplx<Real>* out = spec_out + ((long)vt * n3h + f) * NG;
+  cp_async_wait<0>();
 #pragma unroll
-  for (int j = 0; j < NG; ++j) out[j] = {ar[j], ai[j]};
+  for (int k = 0; k < PB; ++k) {
+    const long p = base + (long)k * NT;
+    if (p >= n_vtrg) continue;
+    Cplx<Real>* out = spec_out + (p * n3h + f) * NG;
+#pragma unroll
+    for (int j = 0; j < NG; ++j) out[j] = {ar[k][j], ai[k][j]};
+  }
 }
 
-template <class Real>
-__global__ void ifft_dn_kernel(FftDims fd, const int* __restrict__ vtrg, const int* __restrict__ child0,
-                               const MKey* __restrict__ keys, const Cplx<Real>* __restrict__ spec,
-                               const int* __restrict__ ifft_map, Real* __restrict__ dc) {
-  extern __shared__ unsigned char smem_raw[];
-  Real* sm = reinterpret_cast<Real*>(smem_raw);
-  const int m = fd.m, n1 = fd.n1, nh = fd.nh, ns = fd.ns, ke = fd.ke, G = fd.G, n3h = fd.n3h;
-  const int m3 = m * m * m;
-  const int ngrid = 8 * ke;
-  Real* twr = sm;
-  Real* twi = twr + n1;
-  Cplx<Real>* S = reinterpret_cast<Cplx<Real>*>(twi + n1);  // G * n3h
-  Cplx<Real>* b1 = S + G * n3h;                             // G * m*n1*nh
-  Cplx<Real>* b2 = b1 + G * m * n1 * nh;                    // G * m*m*nh
-  Real* o = reinterpret_cast<Real*>(b2 + G * m * m * nh);   // G * m3
-  const int vt = blockIdx.x;
-  const int P = vtrg[vt];
-  const int c0 = child0[P];
-  unsigned int X, Y, Z, dP;
-  decode_key(keys[P], X, Y, Z, dP);
-  const Real lscale = (Real)ldexp(1.0, (int)dP + 1);  // trg_scal * level of the children
-  const int dim = ns * ke;
-  for (int j = threadIdx.x; j < n1; j += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * j / n1, &s, &c);  // inverse twiddles
-    twr[j] = (Real)c;
-    twi[j] = (Real)s;
-  }
-  const Cplx<Real>* in = spec + (long)vt * n3h * ngrid;
-  for (int gb = 0; gb < ngrid; gb += G) {
-    const int gn = min(G, ngrid - gb);
-    __syncthreads();
-    for (int i = threadIdx.x; i < gn * n3h; i += blockDim.x) {
-      const int gi = i % gn, f = i / gn;
-      S[gi * n3h + f] = in[(long)f * ngrid + gb + gi];
-    }
-    __syncthreads();
-    // kz -> z in [m, 2m)
-    for (int i = threadIdx.x; i < gn * m * n1 * nh; i += blockDim.x) {
-      const int kx = i % nh, ky = (i / nh) % n1, zp = (i / (nh * n1)) % m, gi = i / (nh * n1 * m);
-      const int z = m + zp;
-      const Cplx<Real>* col = S + gi * n3h + ky * nh + kx;
-      Real re = 0, im = 0;
-      for (int kz = 0; kz < n1; ++kz) {
-        const int w = (kz * z) % n1;
-        const Cplx<Real> v = col[kz * n1 * nh];
-        re += v.re * twr[w] - v.im * twi[w];
-        im += v.re * twi[w] + v.im * twr[w];
-      }
-      b1[i] = {re, im};
-    }
-    __syncthreads();
-    // ky -> y in [m, 2m)
-    for (int i = threadIdx.x; i < gn * m * m * nh; i += blockDim.x) {
-      const int kx = i % nh, yp = (i / nh) % m, zp = (i / (nh * m)) % m, gi = i / (nh * m * m);
-      const int y = m + yp;
-      const Cplx<Real>* col = b1 + ((gi * m + zp) * n1) * nh + kx;
-      Real re = 0, im = 0;
-      for (int ky = 0; ky < n1; ++ky) {
-        const int w = (ky * y) % n1;
-        const Cplx<Real> v = col[ky * nh];
-        re += v.re * twr[w] - v.im * twi[w];
-        im += v.re * twi[w] + v.im * twr[w];
-      }
-      b2[i] = {re, im};
-    }
-    __syncthreads();
-    // kx -> x in [m, 2m), real output (Hermitian weights, c2r)
-    for (int i = threadIdx.x; i < gn * m3; i += blockDim.x) {
-      const int xp = i % m, yp = (i / m) % m, zp = (i / (m * m)) % m, gi = i / m3;
-      const int x = m + xp;
-      const Cplx<Real>* row = b2 + ((gi * m + zp) * m + yp) * nh;
-      Real acc = 0;
-      for (int kx = 0; kx < nh; ++kx) {
-        const int w = (kx * x) % n1;
-        const Cplx<Real> v = row[kx];
-        const Real t = v.re * twr[w] - v.im * twi[w];
-        acc += (kx == 0 || 2 * kx == n1) ? t : (Real)2 * t;
-      }
-      o[i] = acc;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < gn * ns; i += blockDim.x) {
-      const int gi = i / ns, k = i % ns;
-      const int gg = gb + gi, c = gg / ke, comp = gg % ke;
-      const int idx = ifft_map[k];
-      const int x = idx % n1 - m, y = (idx / n1) % n1 - m, z = idx / (n1 * n1) - m;
-      dc[(long)(c0 + c) * dim + k * ke + comp] += o[gi * m3 + x + m * (y + m * z)] * lscale;
-    }
-  }
+template <class Real, int KE, int PB, int OC>
+size_t hadamard_smem() {
+  constexpr int NG = 8 * KE;
+  constexpr int STRIDE = NG + 16 / (int)sizeof(Cplx<Real>);
+  return sizeof(Cplx<Real>) * ((size_t)OC * 64 * KE * KE + 2 * 128 * PB * STRIDE);
+}
+
+template <class Real, int KE, int PB, int OC>
+void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout) {
+  DevTree& T = ctx.tree;
+  const size_t sm = hadamard_smem<Real, KE, PB, OC>();
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_kernel<Real, KE, PB, OC>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(ceil_div(T.n_vtrg, 128 * PB), n3h);
+  ++ctx.n_launch;
+  hadamard_kernel<Real, KE, PB, OC><<<grid, 128, sm, ctx.stream>>>(n3h, T.n_vtrg, T.vtab.get<int>(), sin_,
+                                                                   ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------
-template <class Real>
-__global__ void scatter_rows(const Real* __restrict__ src, const int* __restrict__ rows, long n, int dim,
-                             Real* __restrict__ dst) {
+__global__ void scatter_rows(const double* __restrict__ src, const int* __restrict__ rows, long n, int dim,
+                             double* __restrict__ dst) {
   const long i = blockIdx.x;
   if (i >= n) return;
   const long r = rows[i];
@@ -468,29 +666,27 @@ __global__ void scatter_rows(const Real* __restrict__ src, const int* __restrict
 }
 
 // dst[i] = src[rows[i]] * 2^(-depth(rows[i])) if scale_level else src[rows[i]].
-template <class Real>
-__global__ void gather_rows(const Real* __restrict__ src, const int* __restrict__ rows, long n, int dim,
-                            const MKey* __restrict__ keys, int scale_level, Real* __restrict__ dst) {
+__global__ void gather_rows(const double* __restrict__ src, const int* __restrict__ rows, long n, int dim,
+                            const MKey* __restrict__ keys, int scale_level, double* __restrict__ dst) {
   const long i = blockIdx.x;
   if (i >= n) return;
   const long r = rows[i];
-  Real s = 1;
-  if (scale_level) s = (Real)ldexp(1.0, -(int)(keys[r].lo & 31u));
+  const double s = scale_level ? ldexp(1.0, -(int)(keys[r].lo & 31u)) : 1.0;
   for (int j = threadIdx.x; j < dim; j += blockDim.x) dst[i * dim + j] = src[r * dim + j] * s;
 }
 
-template <class Tin, class Real>
-__global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict__ perm, long n, int k0,
-                               double s0, double s1, double s2, Real* __restrict__ out) {
+template <class Tin>
+__global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict__ perm, long n, int k0, double s0,
+                               double s1, double s2, double* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const long p = perm[i];
   const double sc[3] = {s0, s1, s2};
-  for (int j = 0; j < k0; ++j) out[i * k0 + j] = (Real)((Tin)in[p * k0 + j] * (Tin)sc[j]);
+  for (int j = 0; j < k0; ++j) out[i * k0 + j] = (double)((Tin)in[p * k0 + j] * (Tin)sc[j]);
 }
 
-template <class Real, class Tout>
-__global__ void unsort_values(const Real* __restrict__ pot, const int* __restrict__ perm, long n, int k1, double s0,
+template <class Tout>
+__global__ void unsort_values(const double* __restrict__ pot, const int* __restrict__ perm, long n, int k1, double s0,
                               double s1, double s2, double s3, Tout* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -499,27 +695,13 @@ __global__ void unsort_values(const Real* __restrict__ pot, const int* __restric
   for (int k = 0; k < k1; ++k) out[p * k1 + k] = (Tout)((Tout)pot[i * k1 + k] * (Tout)sc[k]);
 }
 
-template <class Real>
-struct Blas;
-template <>
-struct Blas<double> {
-  static void gemm(cublasHandle_t h, int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
-                   int ldc, double beta) {
-    const double one = 1.0;
-    // Row-major C(MxN) = A(MxK) B(KxN)  <=>  column-major C^T = B^T A^T.
-    if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, M, K, &one, B, ldb, A, lda, &beta, C, ldc) != CUBLAS_STATUS_SUCCESS)
-      throw std::runtime_error("cublasDgemm failed");
-  }
-};
-template <>
-struct Blas<float> {
-  static void gemm(cublasHandle_t h, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
-                   int ldc, float beta) {
-    const float one = 1.0f;
-    if (cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, M, K, &one, B, ldb, A, lda, &beta, C, ldc) != CUBLAS_STATUS_SUCCESS)
-      throw std::runtime_error("cublasSgemm failed");
-  }
-};
+void dgemm(cublasHandle_t h, int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C, int ldc,
+           double beta) {
+  const double one = 1.0;
+  // Row-major C(MxN) = A(MxK) B(KxN)  <=>  column-major C^T = B^T A^T.
+  if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, M, K, &one, B, ldb, A, lda, &beta, C, ldc) != CUBLAS_STATUS_SUCCESS)
+    throw std::runtime_error("cublasDgemm failed");
+}
 
 template <class Real>
 void upload_vec(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
@@ -529,10 +711,64 @@ void upload_vec(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
-int fft_batch(size_t per_grid_bytes, size_t fixed_bytes, int ngrid) {
-  const size_t budget = 200 * 1024;
-  int G = (int)((budget - fixed_bytes) / per_grid_bytes);
-  return std::max(1, std::min(G, ngrid));
+// Largest divisor G of ngrid with fixed + G*per_grid <= budget (at least 1).
+int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
+  int best = 1;
+  for (int G = 1; G <= ngrid; ++G)
+    if (ngrid % G == 0 && fixed + G * per_grid <= budget) best = G;
+  return best;
+}
+
+template <class Real, int M>
+void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int ke,
+                 const std::function<void(int)>& ev) {
+  DevTree& T = ctx.tree;
+  auto s = ctx.stream;
+  using F = FftSizes<Real, M>;
+  const int ngrid = 8 * ke;
+  const int Gu = grids_per_block(F::up_grid_bytes, F::tw_bytes, ngrid, 64 * 1024);
+  const size_t sm_up = F::tw_bytes + Gu * F::up_grid_bytes;
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(fft_up_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_up));
+  ++ctx.n_launch;
+  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid / Gu), 256, sm_up, s>>>(ke, Gu, ngrid / Gu, T.vsrc.get<int>(),
+                                                                     T.child0.get<int>(), ue,
+                                                                     ctx.dops.fft_map.get<int>(), ctx.ns, sin_);
+  ev(4);
+  const int n3h = F::N3H;
+  if (ke == 1) {
+    if constexpr (sizeof(Real) == 8) launch_hadamard<Real, 1, 2, 26>(ctx, n3h, sin_, sout);
+    else launch_hadamard<Real, 1, 4, 26>(ctx, n3h, sin_, sout);
+  } else {
+    launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout);
+  }
+  ev(5);
+  const int Gd = grids_per_block(F::dn_grid_bytes, F::tw_bytes, ngrid, 80 * 1024);
+  const size_t sm_dn = F::tw_bytes + Gd * F::dn_grid_bytes;
+  PVFMM_CUDA_CHECK(
+      cudaFuncSetAttribute(ifft_dn_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
+  ++ctx.n_launch;
+  ifft_dn_kernel<Real, M><<<T.n_vtrg * (ngrid / Gd), 256, sm_dn, s>>>(ke, Gd, ngrid / Gd, T.vtrg.get<int>(),
+                                                                      T.child0.get<int>(), T.key.get<MKey>(), sout,
+                                                                      ctx.dops.ifft_map.get<int>(), ctx.ns, dc);
+}
+
+template <class Real>
+void vlist(Context& ctx, const double* ue, double* dc, int ke, const std::function<void(int)>& ev) {
+  DevTree& T = ctx.tree;
+  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * 8 * ke);
+  Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)T.n_vtrg * n3h * 8 * ke);
+  switch (m) {
+    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    default: throw std::runtime_error("unsupported multipole order");
+  }
 }
 
 template <class Real, int KerS2T, int KerExp>
@@ -543,47 +779,50 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   const int k0 = ctx.ki.k0, k1 = ctx.ki.k1;
   const long N = T.n_nodes;
   const MKey* keys = T.key.get<MKey>();
-  auto ev = [&](int i) {
+  const std::function<void(int)> ev = [&](int i) {
     if (ctx.events_ready) PVFMM_CUDA_CHECK(cudaEventRecord(ctx.ev[i], s));
   };
   ev(0);
   // densities (sorted, scaled by scale_x^src_scal: pvfmm-wrapper.cpp:522-541, 591-595)
-  Real* den = ctx.den.as<Real>(std::max(T.n_src, 1L) * k0);
+  double* den = ctx.den.as<double>(std::max(T.n_src, 1L) * k0);
   double ss[3], ts[4];
   for (int j = 0; j < 3; ++j) ss[j] = den_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.src_scal[j])
                                                 : std::pow(T.scale_x, ctx.ki.src_scal[j]);
   for (int j = 0; j < 4; ++j) ts[j] = out_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.trg_scal[j])
                                                 : std::pow(T.scale_x, ctx.ki.trg_scal[j]);
   if (T.src_counted) {
+    ++ctx.n_launch;
     if (den_float)
-      sort_densities<float, Real><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const float*)den_in, T.src_perm.get<int>(),
-                                                                          T.n_src, k0, ss[0], ss[1], ss[2], den);
+      sort_densities<float><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const float*)den_in, T.src_perm.get<int>(), T.n_src,
+                                                                   k0, ss[0], ss[1], ss[2], den);
     else
-      sort_densities<double, Real><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const double*)den_in, T.src_perm.get<int>(),
-                                                                           T.n_src, k0, ss[0], ss[1], ss[2], den);
+      sort_densities<double><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const double*)den_in, T.src_perm.get<int>(),
+                                                                    T.n_src, k0, ss[0], ss[1], ss[2], den);
   }
-  Real* ue = ctx.ue.as<Real>((size_t)N * dim);
-  Real* dc = ctx.dc.as<Real>((size_t)N * dim);
-  PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * dim * sizeof(Real), s));
-  PVFMM_CUDA_CHECK(cudaMemsetAsync(dc, 0, (size_t)N * dim * sizeof(Real), s));
-  const Real* usurf = ctx.dops.usurf.get<Real>();
-  const Real* sx = T.sx.get<Real>();
-  const Real* sy = T.sy.get<Real>();
-  const Real* sz = T.sz.get<Real>();
+  double* ue = ctx.ue.as<double>((size_t)N * dim);
+  double* dc = ctx.dc.as<double>((size_t)N * dim);
+  PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * dim * sizeof(double), s));
+  PVFMM_CUDA_CHECK(cudaMemsetAsync(dc, 0, (size_t)N * dim * sizeof(double), s));
+  const double* usurf = ctx.dops.usurf.get<double>();
+  const double* sx = T.sx.get<double>();
+  const double* sy = T.sy.get<double>();
+  const double* sz = T.sz.get<double>();
   const int* slo = T.src_lo.get<int>();
   const int* shi = T.src_hi.get<int>();
   if (cublasSetStream(ctx.cublas, s) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasSetStream failed");
-  const Real kscale_exp = (Real)ker_scale(KerExp);
+  const double kscale_exp = ker_scale(KerExp);
   ev(1);
   // ---- S2U
   if (T.src_counted && T.n_sleaf > 0) {
-    Real* uc = ctx.uc_c.as<Real>((size_t)T.n_sleaf * dim);
-    Real* t1 = ctx.tmp_c.as<Real>((size_t)T.n_sleaf * dim);
-    surface_check_kernel<Real, KerExp><<<T.n_sleaf, kNT, 0, s>>>(0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr,
-                                                                  sx, sy, sz, den, usurf, ns, (Real)kRad1, kscale_exp, uc);
-    Blas<Real>::gemm(ctx.cublas, (int)T.n_sleaf, dim, dim, uc, dim, ctx.dops.uc2ue0.get<Real>(), dim, t1, dim, 0);
-    Blas<Real>::gemm(ctx.cublas, (int)T.n_sleaf, dim, dim, t1, dim, ctx.dops.uc2ue1.get<Real>(), dim, uc, dim, 0);
-    scatter_rows<Real><<<T.n_sleaf, 128, 0, s>>>(uc, T.sleaf.get<int>(), T.n_sleaf, dim, ue);
+    double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dim);
+    double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * dim);
+    ++ctx.n_launch;
+    surface_check_kernel<KerExp><<<T.n_sleaf, kNT, 0, s>>>(0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx,
+                                                            sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
+    dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, uc, dim, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, 0);
+    dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, t1, dim, ctx.dops.uc2ue1.get<double>(), dim, uc, dim, 0);
+    ++ctx.n_launch;
+    scatter_rows<<<T.n_sleaf, 128, 0, s>>>(uc, T.sleaf.get<int>(), T.n_sleaf, dim, ue);
   }
   ev(2);
   // ---- U2U, bottom-up
@@ -591,87 +830,66 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     for (int d = T.depth - 1; d >= 0; --d) {
       const long ni = T.n_internal[d];
       if (ni == 0) continue;
-      Real* c = ctx.tmp_c.as<Real>((size_t)ni * dim);
-      Blas<Real>::gemm(ctx.cublas, (int)ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim,
-                       ctx.dops.u2u.get<Real>(), dim, c, dim, 0);
-      scatter_rows<Real><<<ni, 128, 0, s>>>(c, T.int_idx.get<int>() + T.int_off[d], ni, dim, ue);
+      double* c = ctx.tmp_c.as<double>((size_t)ni * dim);
+      dgemm(ctx.cublas, (int)ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim,
+            ctx.dops.u2u.get<double>(), dim, c, dim, 0);
+      ++ctx.n_launch;
+      scatter_rows<<<ni, 128, 0, s>>>(c, T.int_idx.get<int>() + T.int_off[d], ni, dim, ue);
     }
   }
   ev(3);
   // ---- V-list
-  const int m = ctx.m, n1 = 2 * m, nh = m + 1, n3h = n1 * n1 * nh;
-  const int ngrid = 8 * ke;
-  const bool vlist = T.src_counted && T.n_vtrg > 0 && T.n_vsrc > 0;
-  if (vlist) {
-    Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * ngrid);
-    Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)T.n_vtrg * n3h * ngrid);
-    FftDims fd{m, n1, nh, n3h, ns, ke, 1};
-    const size_t per_up = sizeof(Real) * (m * m * m + 2 * m * m * nh + 2 * m * n1 * nh);
-    fd.G = fft_batch(per_up, sizeof(Real) * 2 * n1, ngrid);
-    const size_t sm_up = sizeof(Real) * 2 * n1 + per_up * fd.G;
-    PVFMM_CUDA_CHECK(cudaFuncSetAttribute(fft_up_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_up));
-    fft_up_kernel<Real><<<T.n_vsrc, 256, sm_up, s>>>(fd, T.vsrc.get<int>(), T.child0.get<int>(), ue,
-                                                     ctx.dops.fft_map.get<int>(), sin_);
-    ev(4);
-    dim3 grid(ceil_div(T.n_vtrg, 128), n3h);
-    hadamard_kernel<Real, (KerExp == kKerStokes ? 3 : 1)><<<grid, 128, 0, s>>>(
-        n3h, T.n_vtrg, T.vtab.get<int>(), sin_, ctx.dops.vop.get<Cplx<Real>>(), sout);
-    ev(5);
-    FftDims fi = fd;
-    const size_t per_dn = sizeof(Real) * (2 * n3h + 2 * m * n1 * nh + 2 * m * m * nh + m * m * m);
-    fi.G = fft_batch(per_dn, sizeof(Real) * 2 * n1, ngrid);
-    const size_t sm_dn = sizeof(Real) * 2 * n1 + per_dn * fi.G;
-    PVFMM_CUDA_CHECK(cudaFuncSetAttribute(ifft_dn_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
-    ifft_dn_kernel<Real><<<T.n_vtrg, 256, sm_dn, s>>>(fi, T.vtrg.get<int>(), T.child0.get<int>(), keys, sout,
-                                                      ctx.dops.ifft_map.get<int>(), dc);
+  if (T.src_counted && T.n_vtrg > 0 && T.n_vsrc > 0) {
+    vlist<Real>(ctx, ue, dc, ke, ev);
   } else {
     ev(4);
     ev(5);
   }
   ev(6);
   // ---- X-list
-  if (T.src_counted && T.n_xtrg > 0)
-    surface_check_kernel<Real, KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
-                                                                 T.x_list.get<int>(), sx, sy, sz, den, usurf, ns,
-                                                                 (Real)kRad0, kscale_exp, dc);
+  if (T.src_counted && T.n_xtrg > 0) {
+    ++ctx.n_launch;
+    surface_check_kernel<KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
+                                                           T.x_list.get<int>(), sx, sy, sz, den, usurf, ns, kRad0,
+                                                           kscale_exp, dc);
+  }
   ev(7);
   // ---- D2D, top-down
   for (int d = 0; d < T.depth; ++d) {
     const long ni = T.n_internal[d];
     if (ni == 0) continue;
-    Real* g = ctx.tmp_c.as<Real>((size_t)ni * dim);
-    gather_rows<Real><<<ni, 128, 0, s>>>(dc, T.int_idx.get<int>() + T.int_off[d], ni, dim, keys, 0, g);
-    Blas<Real>::gemm(ctx.cublas, (int)ni, 8 * dim, dim, g, dim, ctx.dops.d2d.get<Real>(), 8 * dim,
-                     dc + (size_t)T.level_off[d + 1] * dim, 8 * dim, 1);
+    double* g = ctx.tmp_c.as<double>((size_t)ni * dim);
+    ++ctx.n_launch;
+    gather_rows<<<ni, 128, 0, s>>>(dc, T.int_idx.get<int>() + T.int_off[d], ni, dim, keys, 0, g);
+    dgemm(ctx.cublas, (int)ni, 8 * dim, dim, g, dim, ctx.dops.d2d.get<double>(), 8 * dim,
+          dc + (size_t)T.level_off[d + 1] * dim, 8 * dim, 1);
   }
   ev(8);
-  // ---- D2T equivalent densities
-  Real* de = nullptr;
+  // ---- D2T equivalent densities, then the fused near field
+  double* pot = ctx.pot.as<double>(std::max(T.n_trg, 1L) * k1);
   if (T.n_tleaf > 0) {
-    Real* g = ctx.tmp_c.as<Real>((size_t)T.n_tleaf * dim);
-    de = ctx.de_c.as<Real>((size_t)T.n_tleaf * dim);
-    Real* t1 = ctx.uc_c.as<Real>((size_t)T.n_tleaf * dim);
-    gather_rows<Real><<<T.n_tleaf, 128, 0, s>>>(dc, T.tleaf.get<int>(), T.n_tleaf, dim, keys, 1, g);
-    Blas<Real>::gemm(ctx.cublas, (int)T.n_tleaf, dim, dim, g, dim, ctx.dops.dc2de0.get<Real>(), dim, t1, dim, 0);
-    Blas<Real>::gemm(ctx.cublas, (int)T.n_tleaf, dim, dim, t1, dim, ctx.dops.dc2de1.get<Real>(), dim, de, dim, 0);
-    // ---- fused near field: D2T + W + U
-    Real* pot = ctx.pot.as<Real>(std::max(T.n_trg, 1L) * k1);
+    double* g = ctx.tmp_c.as<double>((size_t)T.n_tleaf * dim);
+    double* de = ctx.de_c.as<double>((size_t)T.n_tleaf * dim);
+    double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * dim);
+    ++ctx.n_launch;
+    gather_rows<<<T.n_tleaf, 128, 0, s>>>(dc, T.tleaf.get<int>(), T.n_tleaf, dim, keys, 1, g);
+    dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, g, dim, ctx.dops.dc2de0.get<double>(), dim, t1, dim, 0);
+    dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, t1, dim, ctx.dops.dc2de1.get<double>(), dim, de, dim, 0);
+    ++ctx.n_launch;
     near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNT, 0, s>>>(
         T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
-        T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<Real>(), T.ty.get<Real>(),
-        T.tz.get<Real>(), sx, sy, sz, den, ue, T.src_counted ? de : nullptr, usurf, ns, (Real)ker_scale(KerS2T), pot);
+        T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
+        T.tz.get<double>(), sx, sy, sz, den, ue, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T), pot);
   }
   ev(9);
   // ---- output in input order, scaled by scale_x^trg_scal
-  {
-    const Real* pot = ctx.pot.get<Real>();
-    if (out_float)
-      unsort_values<Real, float><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts[0],
-                                                                         ts[1], ts[2], ts[3], (float*)out);
-    else
-      unsort_values<Real, double><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1,
-                                                                          ts[0], ts[1], ts[2], ts[3], (double*)out);
-  }
+  ++ctx.n_launch;
+  if (out_float)
+    unsort_values<float><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts[0], ts[1],
+                                                                ts[2], ts[3], (float*)out);
+  else
+    unsort_values<double><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts[0], ts[1],
+                                                                 ts[2], ts[3], (double*)out);
   ev(10);
   PVFMM_CUDA_CHECK(cudaGetLastError());
 }
@@ -681,25 +899,15 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
 void upload_operators(Context& ctx) {
   const HostOperators& h = ctx.hops;
   auto s = ctx.stream;
-  if (ctx.precision == 0) {
-    upload_vec<double>(ctx.dops.uc2ue0, h.uc2ue0, s);
-    upload_vec<double>(ctx.dops.uc2ue1, h.uc2ue1, s);
-    upload_vec<double>(ctx.dops.dc2de0, h.dc2de0, s);
-    upload_vec<double>(ctx.dops.dc2de1, h.dc2de1, s);
-    upload_vec<double>(ctx.dops.u2u, h.u2u, s);
-    upload_vec<double>(ctx.dops.d2d, h.d2d, s);
-    upload_vec<double>(ctx.dops.vop, h.vop, s);
-    upload_vec<double>(ctx.dops.usurf, h.usurf, s);
-  } else {
-    upload_vec<float>(ctx.dops.uc2ue0, h.uc2ue0, s);
-    upload_vec<float>(ctx.dops.uc2ue1, h.uc2ue1, s);
-    upload_vec<float>(ctx.dops.dc2de0, h.dc2de0, s);
-    upload_vec<float>(ctx.dops.dc2de1, h.dc2de1, s);
-    upload_vec<float>(ctx.dops.u2u, h.u2u, s);
-    upload_vec<float>(ctx.dops.d2d, h.d2d, s);
-    upload_vec<float>(ctx.dops.vop, h.vop, s);
-    upload_vec<float>(ctx.dops.usurf, h.usurf, s);
-  }
+  upload_vec<double>(ctx.dops.uc2ue0, h.uc2ue0, s);
+  upload_vec<double>(ctx.dops.uc2ue1, h.uc2ue1, s);
+  upload_vec<double>(ctx.dops.dc2de0, h.dc2de0, s);
+  upload_vec<double>(ctx.dops.dc2de1, h.dc2de1, s);
+  upload_vec<double>(ctx.dops.u2u, h.u2u, s);
+  upload_vec<double>(ctx.dops.d2d, h.d2d, s);
+  upload_vec<double>(ctx.dops.usurf, h.usurf, s);
+  if (ctx.precision == 0) upload_vec<double>(ctx.dops.vop, h.vop, s);
+  else upload_vec<float>(ctx.dops.vop, h.vop, s);
   int* fm = ctx.dops.fft_map.as<int>(h.fft_map.size());
   int* im = ctx.dops.ifft_map.as<int>(h.ifft_map.size());
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(fm, h.fft_map.data(), h.fft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -731,11 +939,13 @@ void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool 
   }
 }
 
-}  // namespace pvfmm_b200
-
-namespace pvfmm_b200 {
 void evaluate_adjoint(Context& ctx, const void* trg_den, bool in_float, void* src_out, bool out_float) {
-  (void)ctx; (void)trg_den; (void)in_float; (void)src_out; (void)out_float;
+  (void)ctx;
+  (void)trg_den;
+  (void)in_float;
+  (void)src_out;
+  (void)out_float;
   throw std::runtime_error("adjoint evaluation is not available in this build");
 }
+
 }  // namespace pvfmm_b200

@@ -80,6 +80,7 @@ struct Context {
   DevBuf stat;            // small status / reduction buffer
   DevBuf t[24];           // temporaries of the tree build, reused across calls
   std::vector<DevBuf> lvlR, lvlS;  // per-level internal-node keys (refined / balanced)
+  long n_launch = 0;      // own kernels launched since context creation
   std::vector<float> stage_ms;
   std::array<cudaEvent_t, 12> ev{};
   bool events_ready = false;

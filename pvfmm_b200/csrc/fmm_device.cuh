@@ -98,11 +98,11 @@ __device__ inline long lower_bound_key(const MKey* a, long n, const MKey& k) {
 }
 
 // ---------------------------------------------------------------------------
-// Reciprocal square root.  FP64: FP32 hardware estimate refined by two
-// Newton-Raphson steps y <- y (3/2 - r2 y^2 / 2) in FP64 (full double accuracy
-// is reached after two steps from a 2^-22 estimate); tiny r2 outside the FP32
-// range take the FP64 library rsqrt.  FP32: hardware estimate + one Newton
-// step.  r2 == 0 gives 0 (the kernels' mask, kernel.txx:1283).
+// Reciprocal square root with the kernels' r == 0 mask (kernel.txx:1283).
+// FP64: FP32 hardware estimate refined by two Newton-Raphson steps
+// y <- y (3/2 - r2 y^2 / 2) in FP64 (from a 2^-22 estimate two steps reach
+// full double accuracy); r2 below the FP32 normal range takes the FP64
+// library rsqrt.  FP32: hardware estimate + one Newton step.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double rsqrt_nr(double r2) {
   if (r2 < 1e-30) return r2 > 0 ? rsqrt(r2) : 0.0;
@@ -113,32 +113,10 @@ __device__ __forceinline__ double rsqrt_nr(double r2) {
   return y;
 }
 __device__ __forceinline__ float rsqrt_nr(float r2) {
-  if (!(r2 > 0.f)) return 0.f;
-  float y = rsqrtf(r2);
-  y = y * (1.5f - 0.5f * r2 * y * y);
-  return y;
+  const float y0 = rsqrtf(r2);
+  const float y = y0 * (1.5f - 0.5f * r2 * y0 * y0);
+  return r2 > 0.f ? y : 0.f;
 }
-
-// Accumulator: plain sum in FP64; Kahan-compensated sum in FP32.
-template <class Real>
-struct Acc {
-  Real s;
-  __device__ __forceinline__ void init() { s = 0; }
-  __device__ __forceinline__ void add(Real v) { s += v; }
-  __device__ __forceinline__ Real get() const { return s; }
-};
-template <>
-struct Acc<float> {
-  float s, c;
-  __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
-  __device__ __forceinline__ void add(float v) {
-    const float y = v - c;
-    const float t = s + y;
-    c = (t - s) - y;
-    s = t;
-  }
-  __device__ __forceinline__ float get() const { return s; }
-};
 
 // ---------------------------------------------------------------------------
 // Kernel functions (reference include/kernel.txx:1276-1364), unscaled: the
@@ -147,9 +125,6 @@ struct Acc<float> {
 // KS: number of source components, KT: number of target components.
 // ---------------------------------------------------------------------------
 enum KerType { kKerLaplace = 0, kKerLaplaceGrad = 1, kKerStokes = 2, kKerLaplacePG = 3 };
-
-template <int KT>
-struct KerTraits;
 
 template <int Ker>
 struct KerDims;
@@ -164,29 +139,29 @@ struct KerDims<kKerLaplacePG> { static constexpr int KS = 1, KT = 4; };
 
 // Adds K(r) f to u (r = target - source).
 template <int Ker, class Real>
-__device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* f, Acc<Real>* u) {
+__device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* f, Real* u) {
   const Real r2 = rx * rx + ry * ry + rz * rz;
   const Real rinv = rsqrt_nr(r2);
   if constexpr (Ker == kKerLaplace) {
-    u[0].add(rinv * f[0]);
+    u[0] += rinv * f[0];
   } else if constexpr (Ker == kKerLaplaceGrad) {
     const Real fr3 = rinv * rinv * rinv * f[0];
-    u[0].add(rx * fr3);
-    u[1].add(ry * fr3);
-    u[2].add(rz * fr3);
+    u[0] += rx * fr3;
+    u[1] += ry * fr3;
+    u[2] += rz * fr3;
   } else if constexpr (Ker == kKerLaplacePG) {
     const Real fr = rinv * f[0];
     const Real fr3 = rinv * rinv * fr;
-    u[0].add(fr);
-    u[1].add(rx * fr3);
-    u[2].add(ry * fr3);
-    u[3].add(rz * fr3);
+    u[0] += fr;
+    u[1] += rx * fr3;
+    u[2] += ry * fr3;
+    u[3] += rz * fr3;
   } else {  // Stokes velocity
     const Real rinv2 = rinv * rinv;
     const Real ip = (f[0] * rx + f[1] * ry + f[2] * rz) * rinv2;
-    u[0].add(rinv * (f[0] + rx * ip));
-    u[1].add(rinv * (f[1] + ry * ip));
-    u[2].add(rinv * (f[2] + rz * ip));
+    u[0] += rinv * (f[0] + rx * ip);
+    u[1] += rinv * (f[1] + ry * ip);
+    u[2] += rinv * (f[2] + rz * ip);
   }
 }
 

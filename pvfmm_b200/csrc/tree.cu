@@ -58,14 +58,31 @@ __global__ void bbox_partial(const T* __restrict__ pos, long n, double* __restri
 }
 
 __global__ void bbox_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
-  if (threadIdx.x != 0) return;
-  double r[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
-  for (int b = 0; b < nb; ++b)
+  __shared__ double smin[3][kThreads], smax[3][kThreads];
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
     for (int d = 0; d < 3; ++d) {
-      r[d] = fmin(r[d], part[b * 6 + d]);
-      r[3 + d] = fmax(r[3 + d], part[b * 6 + 3 + d]);
+      mn[d] = fmin(mn[d], part[b * 6 + d]);
+      mx[d] = fmax(mx[d], part[b * 6 + 3 + d]);
     }
-  for (int d = 0; d < 6; ++d) out[d] = r[d];
+  for (int d = 0; d < 3; ++d) {
+    smin[d][threadIdx.x] = mn[d];
+    smax[d][threadIdx.x] = mx[d];
+  }
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int d = 0; d < 3; ++d) {
+        smin[d][threadIdx.x] = fmin(smin[d][threadIdx.x], smin[d][threadIdx.x + st]);
+        smax[d][threadIdx.x] = fmax(smax[d][threadIdx.x], smax[d][threadIdx.x + st]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      out[d] = smin[d][0];
+      out[3 + d] = smax[d][0];
+    }
 }
 
 // ------------------------------------------------------------------ keys
@@ -419,7 +436,7 @@ __global__ void fill_vtab(const int* __restrict__ vtrg, long n_vtrg, const int* 
   for (int ci = 0, o = 0; ci < 27; ++ci) {
     if (ci == 13) continue;
     const int c = coll[t * 27 + ci];
-    vtab[i * 26 + o] = (c >= 0) ? node2vsrc[c] : -1;
+    vtab[(long)o * n_vtrg + i] = (c >= 0) ? node2vsrc[c] : -1;  // offset-major: coalesced per offset
     ++o;
   }
 }
@@ -472,14 +489,17 @@ void sort_hilo(Context& ctx, long n, const unsigned long long* hi, const unsigne
   int* idx = ctx.t[base].as<int>(n);
   int* p1 = ctx.t[base + 1].as<int>(n);
   unsigned long long* hg = ctx.t[base + 2].as<unsigned long long>(n);
+  ++ctx.n_launch;
   iota_kernel<<<ceil_div(n, kThreads), kThreads, 0, s>>>(idx, n);
   size_t b1 = 0, b2 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, lo, ls, idx, p1, (int)n, 0, 32, s);
   cub::DeviceRadixSort::SortPairs(nullptr, b2, hg, hs, p1, perm, (int)n, 0, 64, s);
   void* tmp = ctx.scratch.ensure(std::max(b1, b2));
   cub::DeviceRadixSort::SortPairs(tmp, b1, lo, ls, idx, p1, (int)n, 0, 32, s);
+  ++ctx.n_launch;
   gather_u64<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hi, p1, n, hg);
   cub::DeviceRadixSort::SortPairs(tmp, b2, hg, hs, p1, perm, (int)n, 0, 64, s);
+  ++ctx.n_launch;
   gather_u32<<<ceil_div(n, kThreads), kThreads, 0, s>>>(lo, perm, n, ls);
 }
 
@@ -490,6 +510,7 @@ long sort_unique(Context& ctx, const MKey* in, long n, DevBuf& out) {
   unsigned long long* h = ctx.t[10].as<unsigned long long>(n);
   unsigned int* l = ctx.t[11].as<unsigned int>(n);
   int* ix = ctx.t[12].as<int>(n);
+  ++ctx.n_launch;
   split_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(in, n, h, l, ix);
   unsigned long long* hs = ctx.t[13].as<unsigned long long>(n);
   unsigned int* ls = ctx.t[14].as<unsigned int>(n);
@@ -497,9 +518,11 @@ long sort_unique(Context& ctx, const MKey* in, long n, DevBuf& out) {
   sort_hilo(ctx, n, h, l, hs, ls, perm, 16);
   int* fl = ctx.t[19].as<int>(n);
   int* of = ctx.t[20].as<int>(n);
+  ++ctx.n_launch;
   unique_flags<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, ls, n, fl);
   const long cnt = exclusive_scan(ctx, fl, of, n);
   MKey* o = out.as<MKey>(std::max(cnt, 1L));
+  ++ctx.n_launch;
   compact_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, ls, fl, of, n, o);
   return cnt;
 }
@@ -513,8 +536,10 @@ void sort_point_set(Context& ctx, long n, const unsigned long long* hi, const un
   int* perm = perm_out.as<int>(n);
   sort_hilo(ctx, n, hi, lo, hs, ls, perm, 16);
   MKey* keys = keys_out.as<MKey>(n);
+  ++ctx.n_launch;
   assemble_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, lo, perm, n, keys);
   double* c = coord_out.as<double>(n * 3);
+  ++ctx.n_launch;
   gather_coords<<<ceil_div(n, kThreads), kThreads, 0, s>>>(mapped, perm, n, c);
 }
 
@@ -549,8 +574,10 @@ template <class T>
 void point_bbox(Context& ctx, const T* pos, long n, double* host6) {
   const int nb = (int)std::min<long>(1024, std::max<long>(1, ceil_div(n, kThreads)));
   double* part = ctx.t[0].as<double>((size_t)nb * 6 + 6);
+  ++ctx.n_launch;
   bbox_partial<T><<<nb, kThreads, 0, ctx.stream>>>(pos, n, part);
-  bbox_final<<<1, 32, 0, ctx.stream>>>(part, nb, part + (size_t)nb * 6);
+  ++ctx.n_launch;
+  bbox_final<<<1, kThreads, 0, ctx.stream>>>(part, nb, part + (size_t)nb * 6);
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(host6, part + (size_t)nb * 6, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
 }
@@ -562,6 +589,7 @@ void map_points(Context& ctx, const T* pos, long n, double scale, const double* 
   unsigned long long* h = hi.as<unsigned long long>(n);
   unsigned int* l = lo.as<unsigned int>(n);
   int* idx = ctx.t[4].as<int>(n);
+  ++ctx.n_launch;
   map_and_key<T><<<ceil_div(n, kThreads), kThreads, 0, ctx.stream>>>(pos, n, (T)scale, (T)shift[0], (T)shift[1],
                                                                       (T)shift[2], mp, h, l, idx);
 }
@@ -658,6 +686,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     while (n_cur > 0) {
       int* split = ctx.t[3].as<int>(n_cur);
       int* offs = ctx.t[23].as<int>(n_cur);
+      ++ctx.n_launch;
       refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), n_cur, d, sk, T.n_src, tk,
                                                                    T.n_trg, d_gk, (long)gk.size(), ctx.max_pts,
                                                                    kMaxDepth, split);
@@ -666,6 +695,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       if ((long)ctx.lvlR.size() <= d) ctx.lvlR.resize(d + 1);
       MKey* R = ctx.lvlR[d].as<MKey>(n_split);
       MKey* next = next_b.as<MKey>(n_split * 8);
+      ++ctx.n_launch;
       make_children<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), split, offs, n_cur, d, next, R);
       nR.push_back(n_split);
       std::swap(cur_b, next_b);
@@ -688,6 +718,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       MKey* cand = ctx.t[9].as<MKey>(nc);
       PVFMM_CUDA_CHECK(cudaMemcpyAsync(cand, ctx.lvlR[d - 1].get<MKey>(), nR[d - 1] * sizeof(MKey),
                                        cudaMemcpyDeviceToDevice, s));
+      ++ctx.n_launch;
       nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d, cand + nR[d - 1]);
       nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1]);
     }
@@ -719,17 +750,20 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   long int_base = 0;
   for (int d = 0; d <= D; ++d) {
     const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
+    if (d > 0) ++ctx.n_launch;
     if (d > 0) children_of<<<ceil_div(nS[d - 1], kThreads), kThreads, 0, s>>>(ctx.lvlS[d - 1].get<MKey>(), nS[d - 1],
                                                                               d - 1, keys + base);
     int* internal = ctx.t[3].as<int>(nl);
     int* offs = ctx.t[23].as<int>(nl);
     const long nSd = d < D ? nS[d] : 0;
+    ++ctx.n_launch;
     member_flags<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys + base, nl, d < D ? ctx.lvlS[d].get<MKey>() : nullptr,
                                                              nSd, internal);
     const long nint = exclusive_scan(ctx, internal, offs, nl);
     if (nint != nSd) throw std::runtime_error("octree build: balanced internal set is not closed");
     T.n_internal[d] = nint;
     T.int_off[d] = int_base;
+    ++ctx.n_launch;
     level_links<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(internal, offs, nl, base, T.level_off[d + 1], int_base,
                                                             leaf, child0, parent, int_idx);
     int_base += nint;
@@ -739,10 +773,12 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   int* shi = T.src_hi.as<int>(N);
   int* tlo = T.trg_lo.as<int>(N);
   int* thi = T.trg_hi.as<int>(N);
+  ++ctx.n_launch;
   node_ranges<<<ceil_div(N, kThreads), kThreads, 0, s>>>(keys, N, sk, T.n_src, tk, T.n_trg, slo, shi, tlo, thi);
   int* coll = T.colleague.as<int>(N * 27);
   for (int d = 0; d <= D; ++d) {
     const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
+    ++ctx.n_launch;
     colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys, base, nl, coll);
   }
   // 9. compact node lists
@@ -750,9 +786,11 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* flag = ctx.t[3].as<int>(N);
     int* offs = ctx.t[23].as<int>(N);
     auto compact = [&](auto pred, DevBuf& out, int* map) -> long {
+      ++ctx.n_launch;
       flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, pred, flag);
       const long c = exclusive_scan(ctx, flag, offs, N);
       int* o = out.as<int>(std::max(c, 1L));
+      ++ctx.n_launch;
       compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, o, map);
       return c;
     };
@@ -766,6 +804,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* wc = ctx.t[6].as<int>(N);
     int* vc = ctx.t[0].as<int>(N);
     const long nsrf = ctx.ns;
+    ++ctx.n_launch;
     build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 0, pc, xc,
                                                  wc, vc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     int* po = T.p_off.as<int>(N + 1);
@@ -784,47 +823,43 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* pl = T.p_list.as<int>(std::max(T.n_p2p, 1L));
     int* xl = T.x_list.as<int>(std::max(T.n_x, 1L));
     int* wl = T.w_list.as<int>(std::max(T.n_w, 1L));
+    ++ctx.n_launch;
     build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 1, nullptr,
                                                  nullptr, nullptr, nullptr, po, xo, wo, pl, xl, wl);
     T.n_xtrg = compact([=] __device__(long i) { return xc[i] > 0; }, T.xtrg, nullptr);
     T.n_vtrg = compact([=] __device__(long i) { return vc[i] > 0; }, T.vtrg, nullptr);
     int* vt = T.vtab.as<int>(std::max(T.n_vtrg, 1L) * 26);
-    if (T.n_vtrg > 0)
+    if (T.n_vtrg > 0) {
+      ++ctx.n_launch;
       fill_vtab<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), T.n_vtrg, coll, n2v, vt);
+    }
   }
   // 10. point -> leaf and local coordinates
   {
     const long n_leaves_all = N - n_int_total;
     int* flag = ctx.t[3].as<int>(N);
     int* offs = ctx.t[23].as<int>(N);
+    ++ctx.n_launch;
     flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, [=] __device__(long i) { return leaf[i] != 0; }, flag);
     const long nl = exclusive_scan(ctx, flag, offs, N);
     if (nl != n_leaves_all) throw std::runtime_error("octree build: leaf count mismatch");
     int* leaves = ctx.t[0].as<int>(std::max(nl, 1L));
+    ++ctx.n_launch;
     compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, leaves, nullptr);
-    const bool f32 = ctx.precision == 1;
-    const size_t rs = f32 ? sizeof(float) : sizeof(double);
-    void* sx = T.sx.ensure(std::max(T.n_src, 1L) * rs);
-    void* sy = T.sy.ensure(std::max(T.n_src, 1L) * rs);
-    void* sz = T.sz.ensure(std::max(T.n_src, 1L) * rs);
-    void* tx = T.tx.ensure(std::max(T.n_trg, 1L) * rs);
-    void* ty = T.ty.ensure(std::max(T.n_trg, 1L) * rs);
-    void* tz = T.tz.ensure(std::max(T.n_trg, 1L) * rs);
+    double* sx = T.sx.as<double>(std::max(T.n_src, 1L));
+    double* sy = T.sy.as<double>(std::max(T.n_src, 1L));
+    double* sz = T.sz.as<double>(std::max(T.n_src, 1L));
+    double* tx = T.tx.as<double>(std::max(T.n_trg, 1L));
+    double* ty = T.ty.as<double>(std::max(T.n_trg, 1L));
+    double* tz = T.tz.as<double>(std::max(T.n_trg, 1L));
     int* sl = T.src_leaf.as<int>(std::max(T.n_src, 1L));
     int* tl = T.trg_leaf.as<int>(std::max(T.n_trg, 1L));
     if (nl > 0) {
-      if (f32) {
-        // source coordinates are localized even when sl_den is NULL (unused then)
-        localize<float><<<nl, 128, 0, s>>>(leaves, nl, keys, slo, shi, coords_s.get<double>(), (float*)sx, (float*)sy,
-                                           (float*)sz, sl);
-        localize<float><<<nl, 128, 0, s>>>(leaves, nl, keys, tlo, thi, coords_t.get<double>(), (float*)tx, (float*)ty,
-                                           (float*)tz, tl);
-      } else {
-        localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, slo, shi, coords_s.get<double>(), (double*)sx,
-                                            (double*)sy, (double*)sz, sl);
-        localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, tlo, thi, coords_t.get<double>(), (double*)tx,
-                                            (double*)ty, (double*)tz, tl);
-      }
+      // source coordinates are localized even when sl_den is NULL (unused then)
+      ++ctx.n_launch;
+      localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, slo, shi, coords_s.get<double>(), sx, sy, sz, sl);
+      ++ctx.n_launch;
+      localize<double><<<nl, 128, 0, s>>>(leaves, nl, keys, tlo, thi, coords_t.get<double>(), tx, ty, tz, tl);
     }
   }
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
