@@ -104,6 +104,15 @@ int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den,
 int PVFMMEvalAdjointDeviceD(const void* ctx, const double* trg_den, double* src_val, void* stream);
 int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_val, void* stream);
 
+/* Replaces Kernel<T>::ker_poten (reference include/kernel.hpp:40-41,
+ * include/kernel.txx:1137-1265): FP64 direct evaluation on the device of the
+ * kernel function, trg_val[t*k1+k] += sum_s K_k(trg_t - src_s) den_s, r == 0
+ * excluded, for every source.  Device pointers, on `stream` (NULL: legacy
+ * default stream).  Uses stream-ordered scratch of n_chunks*n_trg*k1 doubles.
+ * Returns 0 on success. */
+int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
+                           const double* trg_pos, double* trg_val, long n_trg, void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* PVFMMGetLastError(void);
 

@@ -84,6 +84,7 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMGetLaunchCount": (cl, [vp]),
         "PVFMMGetTreeData": (cl, [vp, ci, vp, cl]),
         "PVFMMPrecompOperator": (cl, [ci, ci, ci, ci, vp, cl]),
+        "PVFMMKernelEvalDeviceD": (ci, [ci, vp, vp, cl, vp, vp, cl, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -111,6 +112,18 @@ def precomp_operator(kernel: FMMKernel, m: int, precision: int, which: int) -> n
     out = np.empty(n, dtype=np.float64)
     lib.PVFMMPrecompOperator(int(kernel.value), m, precision, which, _ptr(out), n)
     return out
+
+
+def kernel_eval_device(kernel: FMMKernel, src_ptr: int, den_ptr: int, n_src: int, trg_ptr: int, out_ptr: int,
+                       n_trg: int, stream: int = 0) -> None:
+    """Direct FP64 kernel sum on device pointers, accumulated into out
+    (the GPU form of Kernel<T>::ker_poten)."""
+    lib = load_library()
+    rc = lib.PVFMMKernelEvalDeviceD(int(kernel.value), ctypes.c_void_p(src_ptr), ctypes.c_void_p(den_ptr), n_src,
+                                    ctypes.c_void_p(trg_ptr), ctypes.c_void_p(out_ptr), n_trg,
+                                    ctypes.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise RuntimeError(f"PVFMMKernelEvalDeviceD failed: {last_error()}")
 
 
 OPERATOR_NAMES = ["uc2ue0", "uc2ue1", "dc2de0", "dc2de1", "u2u", "d2d", "usurf", "vop"]

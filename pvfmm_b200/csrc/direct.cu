@@ -1,0 +1,163 @@
+// Direct kernel evaluation on the device: the GPU counterpart of the
+// reference's Kernel<T>::ker_poten (include/kernel.hpp:40-41,
+// GenericKernel::Eval in include/kernel.txx:1137-1265): k_out += sum over
+// all sources of K(trg - src) den, r == 0 excluded.
+//
+// Work split: targets in tiles of 128 (one thread each), sources in S chunks,
+// one block per (target tile, source chunk).  Each block writes FP64 partial
+// sums to scratch[chunk][target][k]; a second kernel adds the S partials of
+// every target in chunk order (deterministic) into k_out.  S is chosen so
+// that there are about four blocks per SM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/pvfmm.h"
+#include "fmm_device.cuh"
+#include "fmm_host.hpp"
+
+namespace pvfmm_b200 {
+namespace {
+
+constexpr int kDT = 128;
+
+template <int Ker>
+__global__ void __launch_bounds__(kDT) direct_partial_kernel(const double* __restrict__ src,
+                                                             const double* __restrict__ den, long n_src,
+                                                             const double* __restrict__ trg, long n_trg, int n_chunks,
+                                                             double* __restrict__ partial) {
+  constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
+  __shared__ double sx[kDT], sy[kDT], sz[kDT], sf[KS][kDT];
+  const long t = (long)blockIdx.x * kDT + threadIdx.x;
+  const int chunk = blockIdx.y;
+  const long per = (n_src + n_chunks - 1) / n_chunks;
+  const long lo = chunk * per, hi = min(n_src, lo + per);
+  double px = 0, py = 0, pz = 0;
+  if (t < n_trg) {
+    px = trg[t * 3 + 0];
+    py = trg[t * 3 + 1];
+    pz = trg[t * 3 + 2];
+  }
+  double u[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) u[k] = 0;
+  for (long s0 = lo; s0 < hi; s0 += kDT) {
+    const int n = (int)min((long)kDT, hi - s0);
+    __syncthreads();
+    if (threadIdx.x < n) {
+      const long s = s0 + threadIdx.x;
+      sx[threadIdx.x] = src[s * 3 + 0];
+      sy[threadIdx.x] = src[s * 3 + 1];
+      sz[threadIdx.x] = src[s * 3 + 2];
+#pragma unroll
+      for (int i = 0; i < KS; ++i) sf[i][threadIdx.x] = den[s * KS + i];
+    }
+    __syncthreads();
+    if (t < n_trg)
+      for (int j = 0; j < n; ++j) {
+        double f[KS];
+#pragma unroll
+        for (int i = 0; i < KS; ++i) f[i] = sf[i][j];
+        ker_eval<Ker, double>(px - sx[j], py - sy[j], pz - sz[j], f, u);
+      }
+  }
+  if (t < n_trg)
+#pragma unroll
+    for (int k = 0; k < KT; ++k) partial[((long)chunk * n_trg + t) * KT + k] = u[k];
+}
+
+template <int KT>
+__global__ void direct_reduce_kernel(const double* __restrict__ partial, long n_trg, int n_chunks, double scale,
+                                     double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_trg * KT) return;
+  double s = 0;
+  for (int c = 0; c < n_chunks; ++c) s += partial[(long)c * n_trg * KT + i];
+  out[i] += s * scale;
+}
+
+int ker_type(int kernel) {
+  switch (kernel) {
+    case kLaplacePot: return kKerLaplace;
+    case kLaplaceGrad: return kKerLaplaceGrad;
+    case kStokesVel: return kKerStokes;
+    case kLaplacePotGrad: return kKerLaplacePG;
+    default: throw std::runtime_error("unsupported PVFMMKernel value " + std::to_string(kernel));
+  }
+}
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return n;
+}
+
+// Number of source chunks: about 4 blocks per SM, at most one chunk per 512
+// sources, at most `cap` partial rows.
+int choose_chunks(long n_src, long n_trg, long cap_chunks) {
+  const long tiles = (n_trg + kDT - 1) / kDT;
+  long S = std::max(1L, (4L * sm_count() + tiles - 1) / tiles);
+  S = std::min(S, std::max(1L, n_src / 512));
+  S = std::min(S, cap_chunks);
+  return (int)std::max(1L, S);
+}
+
+}  // namespace
+
+// Launches the two kernels with `partial` holding n_chunks * n_trg * KT doubles.
+void direct_eval(int kernel, const double* src, const double* den, long n_src, const double* trg, double* out, long n_trg,
+                 int n_chunks, double* partial, cudaStream_t s) {
+  const int kt = ker_type(kernel);
+  dim3 grid((unsigned)((n_trg + kDT - 1) / kDT), (unsigned)n_chunks);
+  const long nout = n_trg * (kernel == kLaplacePot ? 1 : kernel == kLaplacePotGrad ? 4 : 3);
+  const unsigned rb = (unsigned)((nout + 255) / 256);
+  switch (kt) {
+    case kKerLaplace:
+      direct_partial_kernel<kKerLaplace><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
+      direct_reduce_kernel<1><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplace), out);
+      break;
+    case kKerLaplaceGrad:
+      direct_partial_kernel<kKerLaplaceGrad><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
+      direct_reduce_kernel<3><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplaceGrad), out);
+      break;
+    case kKerStokes:
+      direct_partial_kernel<kKerStokes><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
+      direct_reduce_kernel<3><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerStokes), out);
+      break;
+    default:
+      direct_partial_kernel<kKerLaplacePG><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
+      direct_reduce_kernel<4><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplacePG), out);
+      break;
+  }
+  PVFMM_CUDA_CHECK(cudaGetLastError());
+}
+
+int direct_chunks(long n_src, long n_trg, long cap_chunks) { return choose_chunks(n_src, n_trg, cap_chunks); }
+
+}  // namespace pvfmm_b200
+
+using namespace pvfmm_b200;
+
+extern "C" int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
+                                      const double* trg_pos, double* trg_val, long n_trg, void* stream) {
+  try {
+    KernelInfo ki;
+    if (!kernel_info((int)kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value");
+    if (n_trg <= 0 || n_src <= 0) return 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int S = choose_chunks(n_src, n_trg, 1L << 20);
+    double* partial = nullptr;
+    PVFMM_CUDA_CHECK(cudaMallocAsync((void**)&partial, (size_t)S * n_trg * ki.k1 * sizeof(double), s));
+    direct_eval((int)kernel, src_pos, den, n_src, trg_pos, trg_val, n_trg, S, partial, s);
+    PVFMM_CUDA_CHECK(cudaFreeAsync(partial, s));
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}

@@ -257,3 +257,21 @@ def test_large_mixed_accuracy(big):
     idx = np.random.default_rng(33).choice(len(x), 500, replace=False)
     ref = _direct_sample(x, q1, idx, torch)
     assert O.rel_l2(a[idx], ref) < 1e-5
+
+
+@pytest.mark.parametrize("kid", [0, 1, 3, 6])
+def test_kernel_eval_device_matches_direct_sum(kid):
+    """PVFMMKernelEvalDeviceD (Kernel<T>::ker_poten on the GPU) accumulates the
+    FP64 direct sum into its output."""
+    torch = pytest.importorskip("torch")
+    K = O.KERNELS[kid]
+    rng = np.random.default_rng(40 + kid)
+    src = rng.random((3000, 3))
+    trg = np.concatenate([rng.random((700, 3)), src[:50]])      # includes r == 0 pairs
+    den = rng.uniform(-1, 1, (3000, K.k0))
+    ref = O.direct_sum(kid, src, den, trg)
+    ds, dd, dt = (torch.as_tensor(a, device="cuda") for a in (src, den, trg))
+    out = torch.full((len(trg), K.k1), 0.5, device="cuda", dtype=torch.float64)
+    P.kernel_eval_device(P.FMMKernel(kid), ds.data_ptr(), dd.data_ptr(), 3000, dt.data_ptr(), out.data_ptr(), len(trg))
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(out.cpu().numpy() - 0.5, ref, rtol=1e-11, atol=1e-11 * np.abs(ref).max())
