@@ -113,6 +113,18 @@ int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_va
 int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
                            const double* trg_pos, double* trg_val, long n_trg, void* stream);
 
+/* Allocation-free form of PVFMMKernelEvalDeviceD, for callers that cannot
+ * allocate device memory at the call (a host framework that owns the device
+ * memory pool, or a loop that must not pay for an allocation).  No
+ * counterpart in the reference.  The partial sums use a fixed 8 MiB array in
+ * the library's device image instead of allocated scratch, so
+ * n_trg * k1 <= 1048576 (larger requests return an error).  The first call on
+ * a device looks up the array's address; make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race, and the
+ * caller must serialise them.  Returns 0 on success. */
+int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
+                                  const double* trg_pos, double* trg_val, long n_trg, void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* PVFMMGetLastError(void);
 

@@ -161,3 +161,69 @@ extern "C" int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src
     return 1;
   }
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the direct evaluation.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// direct sum: code that runs inside a host framework which owns the whole
+// device memory pool (a cudaMalloc there would go around its allocator or
+// fail once the pool has reserved the memory), and latency-critical loops
+// that must not pay for an allocation, which can synchronize the device.
+// For them the partial sums live in a fixed array in this library's device
+// image: 1 Mi doubles (8 MiB), held by every GPU that loads the library until
+// the process exits.
+//
+// The array's host-side name is only a stand-in for the symbol, not a device
+// address, so the first call on each device looks up the real address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.  Every call shares the array and
+// leaves its partial sums in it; nothing in it needs to start at zero, because
+// each call writes every entry it later reads.  Calls whose work overlaps on
+// the GPU (concurrent streams, or other host threads) race on the array and
+// must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr long kNoAllocScratchDoubles = 1L << 20;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[128] = {nullptr};
+
+double* noalloc_scratch_address() {
+  int dev = 0;
+  PVFMM_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw std::runtime_error("device index out of range for the fixed scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess)
+      throw std::runtime_error(std::string("cudaGetSymbolAddress of the fixed scratch failed: ") + cudaGetErrorString(err));
+    g_noalloc_addr[dev] = (double*)p;
+  }
+  return g_noalloc_addr[dev];
+}
+}  // namespace
+
+extern "C" int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const double* src_pos, const double* den,
+                                             long n_src, const double* trg_pos, double* trg_val, long n_trg,
+                                             void* stream) {
+  try {
+    KernelInfo ki;
+    if (!kernel_info((int)kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value");
+    if (n_trg <= 0 || n_src <= 0) return 0;
+    const long rows = n_trg * ki.k1;
+    if (rows > kNoAllocScratchDoubles)
+      throw std::runtime_error("n_trg * k1 = " + std::to_string(rows) + " exceeds the fixed scratch of " +
+                               std::to_string(kNoAllocScratchDoubles) +
+                               " doubles of the allocation-free entry point; split the targets");
+    double* scratch = noalloc_scratch_address();
+    const int S = choose_chunks(n_src, n_trg, kNoAllocScratchDoubles / rows);
+    direct_eval((int)kernel, src_pos, den, n_src, trg_pos, trg_val, n_trg, S, scratch, (cudaStream_t)stream);
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
