@@ -97,12 +97,21 @@ int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_de
 int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den, long n_src,
                      const float* trg_pos, float* trg_val, long n_trg, int setup, void* stream);
 
-/* Adjoint (transposed) evaluation on the tree of the last setup=1 call:
- * src_val[j] = sum_i K(x_i - y_j)^T trg_den[i], i.e. the FMM with densities at
- * the targets evaluated at the sources.  Needs a symmetric kernel matrix
- * (LaplacePotential, StokesVelocity).  Device pointers. */
-int PVFMMEvalAdjointDeviceD(const void* ctx, const double* trg_den, double* src_val, void* stream);
-int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_val, void* stream);
+/* Evaluation with the roles of sources and targets exchanged (for adjoints and
+ * gradients; no counterpart in the reference):
+ *   src_val[j*k1+k] = sum_i K_k(src_j - trg_i) trg_den[i*k0 ...],
+ * i.e. densities at the targets, values at the sources, with ctx's kernel.
+ * For LaplacePotential (a symmetric kernel) this is the transpose of the
+ * forward map; with LaplacePotGrad the last three values are the -gradient
+ * that position derivatives need.  When src_pos == trg_pos (same array and
+ * count) ctx's own tree is used, and setup=0 reuses the tree of the last
+ * forward evaluation; otherwise a companion context with the same kernel,
+ * order, leaf size and precision holds the exchanged tree (setup=0 reuses
+ * it).  Device pointers, ordered after `stream`.  Returns 0 on success. */
+int PVFMMEvalAdjointDeviceD(const void* ctx, const double* src_pos, long n_src, const double* trg_pos,
+                            const double* trg_den, long n_trg, double* src_val, int setup, void* stream);
+int PVFMMEvalAdjointDeviceF(const void* ctx, const float* src_pos, long n_src, const float* trg_pos,
+                            const float* trg_den, long n_trg, float* src_val, int setup, void* stream);
 
 /* Replaces Kernel<T>::ker_poten (reference include/kernel.hpp:40-41,
  * include/kernel.txx:1137-1265): FP64 direct evaluation on the device of the
@@ -112,6 +121,13 @@ int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_va
  * Returns 0 on success. */
 int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
                            const double* trg_pos, double* trg_val, long n_trg, void* stream);
+
+/* Host-pointer form of PVFMMKernelEvalDeviceD with the calling convention of
+ * Kernel<T>::ker_poten (reference include/kernel.hpp:40-41): copies the
+ * arrays to the current device, evaluates there and adds the result into
+ * trg_val.  Returns 0 on success. */
+int PVFMMKernelEvalD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
+                     const double* trg_pos, double* trg_val, long n_trg);
 
 /* Allocation-free form of PVFMMKernelEvalDeviceD, for callers that cannot
  * allocate device memory at the call (a host framework that owns the device
@@ -124,6 +140,14 @@ int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src_pos, const
  * caller must serialise them.  Returns 0 on success. */
 int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
                                   const double* trg_pos, double* trg_val, long n_trg, void* stream);
+
+/* Unit-box mode (on != 0), the tree rule of the reference C++ interface
+ * (include/pvfmm.txx:216-244, PtFMM_CreateTree): coordinates are used as given
+ * and must lie in [0,1)^3 (no bounding-box rescale), and the tree's point set
+ * is the targets instead of the seed grid of PVFMMCreateContext
+ * (src/pvfmm-wrapper.cpp:416-432).  The next evaluation rebuilds the tree.
+ * Returns 0 on success. */
+int PVFMMSetUnitBox(void* ctx, int on);
 
 /* Last error message of the calling thread ("" if none). */
 const char* PVFMMGetLastError(void);

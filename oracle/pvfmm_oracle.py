@@ -683,11 +683,18 @@ class FMM:
         self.ns = self.ops.ns
 
     # ------------------------------------------------------------------
-    def setup(self, src_c: np.ndarray, trg_c: np.ndarray, real=np.float64, src_counted=True):
-        """Tree for unit-box coordinates (pvfmm-wrapper.cpp:543-775)."""
+    def setup(self, src_c: np.ndarray, trg_c: np.ndarray, real=np.float64, src_counted=True,
+              pt_coord="seed"):
+        """Tree for unit-box coordinates (pvfmm-wrapper.cpp:543-775).  The
+        tree's point set is the context's seed grid (pt_coord="seed",
+        pvfmm-wrapper.cpp:416-432) or the targets (pt_coord="trg", the C++
+        interface, pvfmm.txx:238)."""
         self.src_perm, src_keys = sorted_keys(src_c)
         self.trg_perm, trg_keys = sorted_keys(trg_c)
-        _, grid_keys = sorted_keys(seed_grid_coords(self.max_pts, real))
+        if pt_coord == "seed":
+            _, grid_keys = sorted_keys(seed_grid_coords(self.max_pts, real))
+        else:
+            grid_keys = trg_keys
         self.tree = Tree(src_keys, trg_keys, grid_keys, self.max_pts, src_counted=src_counted)
         self.src = np.asarray(src_c, dtype=np.float64)[self.src_perm]
         self.trg = np.asarray(trg_c, dtype=np.float64)[self.trg_perm]
@@ -852,6 +859,25 @@ def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, o
     out = out * trg_scal[None, :]
     if return_fmm:
         return out, fmm
+    return out
+
+
+def ptfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None):
+    """C++ interface: PtFMM_CreateTree + SetupFMM + PtFMM_Evaluate
+    (pvfmm.txx:216-328).  Coordinates in [0,1)^3 are used as given (no
+    bounding-box map, so no kernel-exponent scaling) and the tree's point set
+    is the targets."""
+    K = KERNELS[kernel_id]
+    src_c = np.asarray(src_pos, dtype=np.float64).reshape(-1, 3)
+    trg_c = np.asarray(trg_pos, dtype=np.float64).reshape(-1, 3)
+    if src_c.min() < 0 or trg_c.min() < 0 or src_c.max() >= 1 or trg_c.max() >= 1:
+        raise ValueError("coordinates must lie in [0,1)^3")
+    sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
+    fmm = FMM(kernel_id, m, max_pts, ops)
+    fmm.setup(src_c, trg_c, pt_coord="trg")
+    out_sorted = fmm.evaluate(sl_den[fmm.src_perm])
+    out = np.empty_like(out_sorted)
+    out[fmm.trg_perm] = out_sorted
     return out
 
 

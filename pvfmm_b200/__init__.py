@@ -75,8 +75,11 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMEvalF": (None, [vp, vp, vp, cl, vp, vp, cl, vp, ci]),
         "PVFMMEvalDeviceD": (ci, [vp, vp, vp, cl, vp, vp, cl, ci, vp]),
         "PVFMMEvalDeviceF": (ci, [vp, vp, vp, cl, vp, vp, cl, ci, vp]),
-        "PVFMMEvalAdjointDeviceD": (ci, [vp, vp, vp, vp]),
-        "PVFMMEvalAdjointDeviceF": (ci, [vp, vp, vp, vp]),
+        "PVFMMEvalAdjointDeviceD": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
+        "PVFMMEvalAdjointDeviceF": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
+        "PVFMMSetUnitBox": (ci, [vp, ci]),
+        "PVFMMKernelEvalD": (ci, [ci, vp, vp, cl, vp, vp, cl]),
+        "PVFMMKernelEvalDeviceNoAllocD": (ci, [ci, vp, vp, cl, vp, vp, cl, vp]),
         "PVFMMDestroyContextD": (None, [ctypes.POINTER(vp)]),
         "PVFMMDestroyContextF": (None, [ctypes.POINTER(vp)]),
         "PVFMMGetLastError": (ctypes.c_char_p, []),
@@ -124,6 +127,27 @@ def kernel_eval_device(kernel: FMMKernel, src_ptr: int, den_ptr: int, n_src: int
                                     ctypes.c_void_p(stream) if stream else None)
     if rc != 0:
         raise RuntimeError(f"PVFMMKernelEvalDeviceD failed: {last_error()}")
+
+
+def kernel_eval(kernel: FMMKernel, src_pos: np.ndarray, den: np.ndarray, trg_pos: np.ndarray,
+                out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Direct FP64 kernel sum on host arrays (PVFMMKernelEvalD), accumulated
+    into ``out`` (zeros when not given); evaluated on the current GPU."""
+    k0, k1 = KERNEL_DIMS[kernel]
+    src = np.ascontiguousarray(src_pos, dtype=np.float64).reshape(-1)
+    trg = np.ascontiguousarray(trg_pos, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(den, dtype=np.float64).reshape(-1)
+    n_src, n_trg = src.size // 3, trg.size // 3
+    if q.size != n_src * k0:
+        raise ValueError("density length does not match the source count")
+    if out is None:
+        out = np.zeros(n_trg * k1)
+    elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != n_trg * k1:
+        raise ValueError("out must be a C-contiguous float64 array of n_trg*k1 values")
+    rc = load_library().PVFMMKernelEvalD(int(kernel.value), _ptr(src), _ptr(q), n_src, _ptr(trg), _ptr(out), n_trg)
+    if rc != 0:
+        raise RuntimeError(f"PVFMMKernelEvalD failed: {last_error()}")
+    return out
 
 
 OPERATOR_NAMES = ["uc2ue0", "uc2ue1", "dc2de0", "dc2de1", "u2u", "d2d", "usurf", "vop"]
@@ -221,12 +245,22 @@ class FMMParticleContext:
         if rc != 0:
             raise RuntimeError(f"PVFMMEvalDevice failed: {last_error()}")
 
-    def evaluate_adjoint_device(self, trg_den_ptr: int, src_out_ptr: int, stream: int = 0) -> None:
+    def evaluate_adjoint_device(self, src_ptr: int, n_src: int, trg_ptr: int, trg_den_ptr: int, n_trg: int,
+                                out_ptr: int, setup: bool = True, stream: int = 0) -> None:
+        """PVFMMEvalAdjointDevice*: densities at the targets, values at the
+        sources (same kernel).  With src_ptr == trg_ptr the forward tree is
+        reused when setup is False."""
         f = self._lib.PVFMMEvalAdjointDeviceD if self.dtype == np.float64 else self._lib.PVFMMEvalAdjointDeviceF
-        rc = f(self._ptr, ctypes.c_void_p(trg_den_ptr), ctypes.c_void_p(src_out_ptr),
-               ctypes.c_void_p(stream) if stream else None)
+        rc = f(self._ptr, ctypes.c_void_p(src_ptr), n_src, ctypes.c_void_p(trg_ptr), ctypes.c_void_p(trg_den_ptr),
+               n_trg, ctypes.c_void_p(out_ptr), int(setup), ctypes.c_void_p(stream) if stream else None)
         if rc != 0:
             raise RuntimeError(f"PVFMMEvalAdjointDevice failed: {last_error()}")
+
+    def set_unit_box(self, on: bool = True) -> None:
+        """Tree rule of the reference C++ interface: coordinates used as given
+        in [0,1)^3, tree points = targets (PVFMMSetUnitBox)."""
+        if self._lib.PVFMMSetUnitBox(self._ptr, int(on)) != 0:
+            raise RuntimeError(last_error())
 
     def stage_times(self) -> dict:
         buf = np.zeros(10)

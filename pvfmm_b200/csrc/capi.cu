@@ -25,6 +25,7 @@ constexpr unsigned int kMagic = 0x50564642u;  // "PVFB"
 struct Handle {
   unsigned int magic = kMagic;
   Context ctx;
+  void* adjoint = nullptr;  // companion context with sources and targets exchanged
 };
 
 Handle* as_handle(const void* p) {
@@ -174,6 +175,7 @@ void destroy(void** ctx) {
   if (!ctx || !ctx[0]) return;
   try {
     Handle* h = as_handle(ctx[0]);
+    if (h->adjoint) destroy(&h->adjoint);
     destroy_context(h->ctx);
     h->magic = 0;
     delete h;
@@ -181,6 +183,31 @@ void destroy(void** ctx) {
     set_last_error(e.what());
   }
   ctx[0] = nullptr;
+}
+
+// src_val = the context's kernel with sources and targets exchanged:
+// src_val[j*k1+k] = sum_i K_k(src_j - trg_i) trg_den_i.  When the two point
+// sets are the same array the context's own tree serves (setup=0 reuses the
+// tree of the forward evaluation); otherwise a companion context with the same
+// kernel, order, leaf size, precision and tree rule holds the exchanged tree.
+template <class T>
+int eval_adjoint(const void* ctx, const T* src, long n_src, const T* trg, const T* trg_den, long n_trg, T* src_val,
+                 int setup, void* stream) {
+  try {
+    Handle* h = as_handle(ctx);
+    Context& c = h->ctx;
+    if (src == trg && n_src == n_trg) return eval_device<T>(ctx, trg, trg_den, n_trg, src, src_val, n_src, setup, stream);
+    if (!h->adjoint) {
+      h->adjoint = create_context(-1.0, c.max_pts, c.m, c.kernel, c.precision, c.float_api);
+      if (!h->adjoint) throw std::runtime_error(std::string("companion context: ") + get_last_error());
+      as_handle(h->adjoint)->ctx.unit_box = c.unit_box;
+      setup = 1;
+    }
+    return eval_device<T>(h->adjoint, trg, trg_den, n_trg, src, src_val, n_src, setup, stream);
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
 }
 
 template <class T>
@@ -232,30 +259,21 @@ int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den,
   return eval_device<float>(ctx, src_pos, sl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
 }
 
-int PVFMMEvalAdjointDeviceD(const void* ctx, const double* trg_den, double* src_val, void* stream) {
-  try {
-    Handle* h = as_handle(ctx);
-    Context& c = h->ctx;
-    if (!c.tree.valid) throw std::runtime_error("adjoint evaluation needs a prior setup=1 evaluation");
-    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
-    (void)stream;
-    evaluate_adjoint(c, trg_den, false, src_val, false);
-    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
-    return 0;
-  } catch (const std::exception& e) {
-    set_last_error(e.what());
-    return 1;
-  }
+int PVFMMEvalAdjointDeviceD(const void* ctx, const double* src_pos, long n_src, const double* trg_pos,
+                            const double* trg_den, long n_trg, double* src_val, int setup, void* stream) {
+  return eval_adjoint<double>(ctx, src_pos, n_src, trg_pos, trg_den, n_trg, src_val, setup, stream);
 }
-int PVFMMEvalAdjointDeviceF(const void* ctx, const float* trg_den, float* src_val, void* stream) {
+int PVFMMEvalAdjointDeviceF(const void* ctx, const float* src_pos, long n_src, const float* trg_pos,
+                            const float* trg_den, long n_trg, float* src_val, int setup, void* stream) {
+  return eval_adjoint<float>(ctx, src_pos, n_src, trg_pos, trg_den, n_trg, src_val, setup, stream);
+}
+
+int PVFMMSetUnitBox(void* ctx, int on) {
   try {
     Handle* h = as_handle(ctx);
-    Context& c = h->ctx;
-    if (!c.tree.valid) throw std::runtime_error("adjoint evaluation needs a prior setup=1 evaluation");
-    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
-    (void)stream;
-    evaluate_adjoint(c, trg_den, true, src_val, true);
-    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    h->ctx.unit_box = on != 0;
+    h->ctx.tree.valid = false;
+    set_last_error("");
     return 0;
   } catch (const std::exception& e) {
     set_last_error(e.what());

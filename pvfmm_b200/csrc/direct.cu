@@ -162,6 +162,49 @@ extern "C" int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src
   }
 }
 
+// Host-pointer form (the calling convention of Kernel<T>::ker_poten): copies
+// the arrays to the current device, runs the same two kernels on a private
+// stream and copies the accumulated values back.
+extern "C" int PVFMMKernelEvalD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,
+                                const double* trg_pos, double* trg_val, long n_trg) {
+  cudaStream_t s = nullptr;
+  double* buf = nullptr;
+  try {
+    KernelInfo ki;
+    if (!kernel_info((int)kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value");
+    if (n_trg <= 0 || n_src <= 0) {
+      set_last_error("");
+      return 0;
+    }
+    PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const int S = choose_chunks(n_src, n_trg, 1L << 20);
+    const size_t n_s3 = (size_t)n_src * 3, n_sd = (size_t)n_src * ki.k0, n_t3 = (size_t)n_trg * 3,
+                 n_tv = (size_t)n_trg * ki.k1, n_p = (size_t)S * n_trg * ki.k1;
+    PVFMM_CUDA_CHECK(cudaMallocAsync((void**)&buf, (n_s3 + n_sd + n_t3 + n_tv + n_p) * sizeof(double), s));
+    double *d_src = buf, *d_den = d_src + n_s3, *d_trg = d_den + n_sd, *d_val = d_trg + n_t3, *d_part = d_val + n_tv;
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_src, src_pos, n_s3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, den, n_sd * sizeof(double), cudaMemcpyHostToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_trg, trg_pos, n_t3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_val, trg_val, n_tv * sizeof(double), cudaMemcpyHostToDevice, s));
+    direct_eval((int)kernel, d_src, d_den, n_src, d_trg, d_val, n_trg, S, d_part, s);
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_tv * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PVFMM_CUDA_CHECK(cudaFreeAsync(buf, s));
+    buf = nullptr;
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+    PVFMM_CUDA_CHECK(cudaStreamDestroy(s));
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    if (s) {
+      if (buf) cudaFreeAsync(buf, s);
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+    set_last_error(e.what());
+    return 1;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free variant of the direct evaluation.
 //

@@ -939,13 +939,4 @@ void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool 
   }
 }
 
-void evaluate_adjoint(Context& ctx, const void* trg_den, bool in_float, void* src_out, bool out_float) {
-  (void)ctx;
-  (void)trg_den;
-  (void)in_float;
-  (void)src_out;
-  (void)out_float;
-  throw std::runtime_error("adjoint evaluation is not available in this build");
-}
-
 }  // namespace pvfmm_b200

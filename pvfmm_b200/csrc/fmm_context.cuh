@@ -62,6 +62,7 @@ struct Context {
   int m = 0, ns = 0, max_pts = 0;
   int precision = 0;      // 0 plain FP64, 1 mixed FP32
   bool float_api = false; // created by the F entry points
+  bool unit_box = false;  // coordinates used as given in [0,1)^3, tree points = targets
   HostOperators hops;
   DevOps dops;
   DevTree tree;
@@ -94,7 +95,6 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
                 bool src_counted, bool trg_alias);
 // eval.cu
 void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
-void evaluate_adjoint(Context& ctx, const void* trg_den, bool in_float, void* src_out, bool out_float);
 void upload_operators(Context& ctx);
 
 }  // namespace pvfmm_b200

@@ -637,12 +637,22 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     point_bbox<float>(ctx, (const float*)src_pos, n_src, bs);
     if (trg_alias) std::copy(bs, bs + 6, bt);
     else point_bbox<float>(ctx, (const float*)trg_pos, n_trg, bt);
-    bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
+    if (!ctx.unit_box) bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
   } else {
     point_bbox<double>(ctx, (const double*)src_pos, n_src, bs);
     if (trg_alias) std::copy(bs, bs + 6, bt);
     else point_bbox<double>(ctx, (const double*)trg_pos, n_trg, bt);
-    bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
+    if (!ctx.unit_box) bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
+  }
+  if (ctx.unit_box) {
+    // C++ interface (include/pvfmm.txx:216-244): coordinates are used as
+    // given, so they must lie in the unit cube.
+    for (const double* b : {bs, bt})
+      for (int k = 0; k < 3; ++k)
+        if (!(b[k] >= 0.0) || !(b[3 + k] < 1.0))
+          throw std::runtime_error("coordinates must lie in [0,1)^3 for a unit-box tree");
+    T.scale_x = 1.0;
+    T.shift_x[0] = T.shift_x[1] = T.shift_x[2] = 0.0;
   }
   DevBuf& src_mapped = ctx.t[1];
   DevBuf& trg_mapped = ctx.t[2];
@@ -669,12 +679,20 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     sort_point_set(ctx, n_trg, hi.get<unsigned long long>(), lo.get<unsigned int>(), trg_mapped.get<double>(),
                    T.trg_perm, T.trg_key, coords_t);
   }
-  // 4. seed grid
-  const std::vector<MKey> gk = seed_grid_keys(ctx.max_pts, pos_float);
-  MKey* d_gk = ctx.t[9].as<MKey>(gk.size());
-  PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_gk, gk.data(), gk.size() * sizeof(MKey), cudaMemcpyHostToDevice, s));
+  // 4. the tree's point set: the seed grid of the C interface, or the
+  //    targets for a unit-box tree (pt_coord = trg_coord, pvfmm.txx:238)
   const MKey* sk = T.src_counted ? T.src_key.get<MKey>() : nullptr;
   const MKey* tk = T.trg_key.get<MKey>();
+  std::vector<MKey> gk;
+  const MKey* d_gk = tk;
+  long n_gk = n_trg;
+  if (!ctx.unit_box) {
+    gk = seed_grid_keys(ctx.max_pts, pos_float);
+    MKey* g = ctx.t[9].as<MKey>(gk.size());
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(g, gk.data(), gk.size() * sizeof(MKey), cudaMemcpyHostToDevice, s));
+    d_gk = g;
+    n_gk = (long)gk.size();
+  }
   // 5. refinement, level by level
   std::vector<long> nR;
   {
@@ -688,7 +706,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       int* offs = ctx.t[23].as<int>(n_cur);
       ++ctx.n_launch;
       refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), n_cur, d, sk, T.n_src, tk,
-                                                                   T.n_trg, d_gk, (long)gk.size(), ctx.max_pts,
+                                                                   T.n_trg, d_gk, n_gk, ctx.max_pts,
                                                                    kMaxDepth, split);
       const long n_split = exclusive_scan(ctx, split, offs, n_cur);
       if (n_split == 0) break;
