@@ -89,8 +89,10 @@ enum PVFMMPrecision {
  * plain and the mixed form can run on the same FP64 inputs. */
 void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision);
 
-/* Evaluation on device pointers (CUDA global memory), on `stream`
- * (a cudaStream_t, or NULL for the context's own stream).  Returns 0 on
+/* Evaluation on device pointers (CUDA global memory).  The work is ordered
+ * after the work already queued on `stream` (a cudaStream_t) and `stream`
+ * waits for its completion; with NULL it is ordered after the legacy default
+ * stream and the call returns when the values are written.  Returns 0 on
  * success, nonzero on error (message in PVFMMGetLastError()). */
 int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_den, long n_src,
                      const double* trg_pos, double* trg_val, long n_trg, int setup, void* stream);

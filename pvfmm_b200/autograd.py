@@ -21,16 +21,21 @@ and targets are the same tensor that evaluation reuses the forward pass's
 octree; otherwise a companion context builds the exchanged tree.  Gradients
 with respect to the same tensor passed as sources and targets add up.
 
-All tensors live on one CUDA device; the computation runs in the dtype of the
-LaplaceFMM object (float32: mixed form; float64: plain FP64 unless the mixed
-form is requested).  Double backward is not supported.
+All tensors live on one CUDA device.  Coordinates always enter the library
+as FP64 (a float32 tensor is widened on the device), so the bounding-box map
+adds no FP32 rounding to the point positions: with FP32 coordinates mapped in
+FP32, as the reference's float interface does, close pairs lose ~1e-4 of the
+gradient's accuracy.  The arithmetic form is `precision`: "mixed" (FP32 near
+field and V-list, FP64 check->equivalent chain) or "plain" (FP64 throughout);
+outputs and gradients come back in the inputs' dtypes.  Double backward is not
+supported.
 """
 from typing import Optional
 
 import numpy as np
 import torch
 
-from . import PRECISION_PLAIN, FMMKernel, FMMParticleContext
+from . import PRECISION_MIXED, PRECISION_PLAIN, FMMKernel, FMMParticleContext
 
 
 class LaplaceFMM:
@@ -40,17 +45,13 @@ class LaplaceFMM:
     both roles); ``fmm(src, den, trg)`` at separate targets.
     """
 
-    def __init__(self, max_points: int = 256, multipole_order: int = 8, dtype: torch.dtype = torch.float32,
-                 precision: Optional[int] = None, unit_box: bool = False):
-        if dtype not in (torch.float32, torch.float64):
-            raise ValueError("dtype must be torch.float32 or torch.float64")
-        np_dtype = np.float32 if dtype == torch.float32 else np.float64
-        if dtype == torch.float64 and precision is None:
-            precision = PRECISION_PLAIN
-        self.dtype = dtype
-        self.ctx = FMMParticleContext(-1.0, max_points, multipole_order, FMMKernel.LaplacePotGrad,
-                                      dtype=np_dtype, precision=precision)
-        self.precision = self.ctx.precision
+    def __init__(self, max_points: int = 256, multipole_order: int = 8, precision: str = "mixed",
+                 unit_box: bool = False):
+        if precision not in ("mixed", "plain"):
+            raise ValueError('precision must be "mixed" or "plain"')
+        self.precision = precision
+        self.ctx = FMMParticleContext(-1.0, max_points, multipole_order, FMMKernel.LaplacePotGrad, dtype=np.float64,
+                                      precision=PRECISION_MIXED if precision == "mixed" else PRECISION_PLAIN)
         if unit_box:
             self.ctx.set_unit_box(True)
         self.generation = 0   # trees built so far; backward reuses the tree only if unchanged
@@ -83,7 +84,7 @@ class _LaplaceFMMFunction(torch.autograd.Function):
             raise ValueError("den must have one value per source")
         alias = trg is src or (trg.data_ptr() == src.data_ptr() and trg.shape == src.shape
                                and trg.stride() == src.stride() and trg.dtype == src.dtype)
-        dt = fmm.dtype
+        dt = torch.float64
         s = src.detach().to(dt).contiguous()
         q = den.detach().to(dt).contiguous()
         t = s if alias else trg.detach().to(dt).contiguous()
@@ -106,10 +107,10 @@ class _LaplaceFMMFunction(torch.autograd.Function):
         s, q, t, out = ctx.saved_tensors
         fmm = ctx.fmm
         need_src, need_den, need_trg = ctx.needs_input_grad[1], ctx.needs_input_grad[2], ctx.needs_input_grad[3]
-        g = grad_phi.detach().to(fmm.dtype).contiguous()
+        g = grad_phi.detach().to(torch.float64).contiguous()
         g_src = g_den = g_trg = None
         if need_src or need_den:
-            adj = torch.empty(s.shape[0], 4, dtype=fmm.dtype, device=s.device)
+            adj = torch.empty(s.shape[0], 4, dtype=torch.float64, device=s.device)
             reuse = ctx.alias and fmm.generation == ctx.gen
             stream = torch.cuda.current_stream(s.device).cuda_stream
             with torch.cuda.device(s.device):

@@ -100,8 +100,9 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
     Context& c = h->ctx;
     PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
     const bool is_f = std::is_same<T, float>::value;
-    cudaStream_t user = (cudaStream_t)stream;
-    if (user && user != c.stream) {
+    // NULL: the legacy default stream (the call then returns on completion)
+    cudaStream_t user = stream ? (cudaStream_t)stream : cudaStreamLegacy;
+    if (user != c.stream) {
       // order the context stream after the caller's stream
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], user));
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(c.stream, c.ev[11], 0));
@@ -122,7 +123,7 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
     }
     evaluate(c, den, is_f, val, is_f);
-    if (user && user != c.stream) {
+    if (stream && user != c.stream) {
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[10], c.stream));
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(user, c.ev[10], 0));
     } else {
@@ -158,7 +159,7 @@ void eval_host(const T* src_pos, const T* sl_den, const T* dl_den, long n_src, c
         PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
     }
     if (!alias) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_trg, trg_pos, n_trg * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
-    if (eval_device<T>(ctx_, d_src, d_den, n_src, d_trg, d_val, n_trg, setup, nullptr) != 0)
+    if (eval_device<T>(ctx_, d_src, d_den, n_src, d_trg, d_val, n_trg, setup, c.stream) != 0)
       throw std::runtime_error(get_last_error());
     PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_trg * c.ki.k1 * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
     PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));

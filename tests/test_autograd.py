@@ -3,7 +3,7 @@
 Workload: N = 1,000,000 points uniform in [0,1)^3 (seed 31), densities
 q ~ U[-1,1] (seed 32), weights w ~ U[0,1] (seed 33), loss L = sum_i w_i phi_i^2
 with phi the Laplace single-layer potential of the points at themselves,
-m = 8, 256 points per leaf, FP32 inputs (mixed form).
+m = 8, 256 points per leaf, FP32 tensors, mixed form.
 
 * Against an FP64 direct-sum gradient on a 20,000-point subset (seed 35):
   dL/dq and dL/dx, rel-L2 <= 1e-5.
@@ -66,7 +66,7 @@ def test_gradients_match_direct_sum_on_subset():
     xs = torch.tensor(x[idx], dtype=torch.float32, device=dev).requires_grad_(True)
     qs = torch.tensor(q[idx], dtype=torch.float32, device=dev).requires_grad_(True)
     ws = torch.tensor(w[idx], dtype=torch.float64, device=dev)
-    fmm = PA.LaplaceFMM(256, 8, torch.float32)
+    fmm = PA.LaplaceFMM(256, 8, "mixed")
     phi = fmm(xs, qs)
     L = (ws * phi.double() ** 2).sum()
     L.backward()
@@ -90,7 +90,7 @@ def test_gradients_plain_fp64_separate_targets():
     x = torch.tensor(rng.random((5000, 3)), device=dev).requires_grad_(True)
     q = torch.tensor(rng.uniform(-1, 1, 6000), device=dev).requires_grad_(True)
     w = torch.tensor(rng.uniform(0, 1, 5000), device=dev)
-    fmm = PA.LaplaceFMM(64, 8, torch.float64)
+    fmm = PA.LaplaceFMM(64, 8, "plain")
     phi = fmm(y, q, x)
     (w * phi ** 2).sum().backward()
     Y, X, Q = y.detach(), x.detach(), q.detach()
@@ -119,7 +119,7 @@ def test_gradients_match_finite_differences_full_size():
     x32 = torch.tensor(x, dtype=torch.float32, device=dev).requires_grad_(True)
     q32 = torch.tensor(q, dtype=torch.float32, device=dev).requires_grad_(True)
     wt = torch.tensor(w, dtype=torch.float64, device=dev)
-    fmm = PA.LaplaceFMM(256, 8, torch.float32)
+    fmm = PA.LaplaceFMM(256, 8, "mixed")
     (wt * fmm(x32, q32).double() ** 2).sum().backward()
     gq = q32.grad.double().cpu().numpy()
     gx = x32.grad.double().cpu().numpy()
@@ -178,12 +178,12 @@ def test_gradients_match_finite_differences_full_size():
     assert rel_x < 1e-5, rel_x
 
 
-def test_double_tensor_inputs_on_float_object_keep_input_dtype():
+def test_outputs_keep_the_input_dtype():
     dev = torch.device("cuda:0")
     rng = np.random.default_rng(2)
     x = torch.tensor(rng.random((3000, 3)), device=dev).requires_grad_(True)
     q = torch.tensor(rng.uniform(-1, 1, 3000), device=dev).requires_grad_(True)
-    fmm = PA.LaplaceFMM(128, 6, torch.float32)
+    fmm = PA.LaplaceFMM(128, 6, "mixed")
     phi = fmm(x, q)
     assert phi.dtype == torch.float64
     phi.sum().backward()

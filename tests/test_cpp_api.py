@@ -87,7 +87,7 @@ def test_cpp_interface_matches_oracle(tmp_path, kid, m, mp, ns, nt, real, tol):
     assert O.rel_l2(val1, ref1) < tol
     assert O.rel_l2(val2, ref2) < tol
     # the FMM itself is accurate (guards against a wrong tree rule on both sides)
-    assert O.rel_l2(ref1, O.direct_sum(kid, src, den, trg)) < 1e-3
+    assert O.rel_l2(ref1, O.direct_sum(kid, src, den, trg)) < (5e-3 if m == 4 else 1e-4)
     # ker_poten accumulated twice; BuildMatrix layout
     ds, dt = min(ns, 200), min(nt, 64)
     direct = K.s2t.eval(src[:ds], den.reshape(-1, K.k0)[:ds].reshape(-1), trg[:dt])
