@@ -163,26 +163,6 @@ struct Split {
   }
 };
 
-// Sources on a cube surface: points off + hr*u_k, FP64 densities.
-template <class Real, int Ker>
-__device__ void surface_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __restrict__ usurf, int ns, double ox,
-                                double oy, double oz, double hr, const double* __restrict__ dens, const Split& sp,
-                                const Pt<Real>& p, double* acc) {
-  constexpr int KS = KerDims<Ker>::KS;
-  for (int k0 = 0; k0 < ns; k0 += kNT) {
-    const int n = min(kNT, ns - k0);
-    __syncthreads();
-    if (threadIdx.x < n) {
-      const int k = k0 + threadIdx.x;
-      tile_store(tl, threadIdx.x, ox + hr * usurf[k * 3 + 0], oy + hr * usurf[k * 3 + 1], oz + hr * usurf[k * 3 + 2]);
-#pragma unroll
-      for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = (Real)dens[k * KS + i];
-    }
-    __syncthreads();
-    if (sp.active) tile_sum<Real, Ker>(tl, n, sp.g, sp.G, p, acc);
-  }
-}
-
 // Sources = sorted points [lo,hi) of a leaf whose centre is at offset (ox,oy,oz).
 template <class Real, int Ker>
 __device__ void point_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __restrict__ sx,
@@ -230,10 +210,127 @@ __device__ void reduce_store(double (*red)[KT], const Split& sp, const double* a
 
 // ---------------------------------------------------------------------------
 // Near field of one target leaf: D2T (own downward equivalent surface), W
-// (upward equivalent surfaces) and U (points), fused.  One block per leaf.
+// (upward equivalent surfaces of the W list) and U (points of the P2P list),
+// fused.  One block per target leaf.
+//
+// The sources of all list entries are packed back to back into tiles of
+// kTile records in shared memory (leaves hold a few dozen points, so one tile
+// spans many entries), double-buffered so that one barrier per tile suffices.
+// A record is one source point relative to the target leaf's centre plus its
+// KS densities, stored as 16-byte chunks, chunk-major.  FP32 records also
+// carry each coordinate's rounding remainder (hi + lo), so target - source
+// keeps FP32 relative accuracy for close pairs.  Every thread evaluates two
+// targets per loaded record; when a leaf has fewer than 2*kNF targets the
+// source records are split among G groups of threads and the G partial sums
+// are added in a fixed order.
 // ---------------------------------------------------------------------------
+constexpr int kNF = 128;        // threads per near-field block
+#ifndef PVFMM_NEAR_MIN_BLOCKS_F32
+#define PVFMM_NEAR_MIN_BLOCKS_F32 5  // resident blocks per SM the register budget is sized for
+#endif
+#ifndef PVFMM_NEAR_MIN_BLOCKS_F64
+#define PVFMM_NEAR_MIN_BLOCKS_F64 5
+#endif
+constexpr int kTile = 2 * kNF;  // source records per tile
+
+template <class Real>
+struct Vec16 {
+  using type = double2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+
+template <class Real, int KS>
+struct Rec {
+  static constexpr bool kLo = sizeof(Real) == 4;
+  static constexpr int NV = (kLo ? 6 : 3) + KS;
+  static constexpr int PER = 16 / (int)sizeof(Real);
+  static constexpr int NC = (NV + PER - 1) / PER;
+  static constexpr int NVP = NC * PER;
+  // value slots: x y z f0 | xl yl zl f1 f2 (FP32);  x y z f0 f1 f2 (FP64)
+  __host__ __device__ static constexpr int F(int i) { return kLo ? (i == 0 ? 3 : 6 + i) : 3 + i; }
+};
+
+template <class Real, int KS>
+__device__ __forceinline__ void rec_store(typename Vec16<Real>::type* tile, int j, double x, double y, double z,
+                                          const Real* f) {
+  using R = Rec<Real, KS>;
+  Real v[R::NVP];
+#pragma unroll
+  for (int i = 0; i < R::NVP; ++i) v[i] = 0;
+  v[0] = (Real)x;
+  v[1] = (Real)y;
+  v[2] = (Real)z;
+  if constexpr (R::kLo) {
+    v[4] = (Real)(x - (double)v[0]);
+    v[5] = (Real)(y - (double)v[1]);
+    v[6] = (Real)(z - (double)v[2]);
+  }
+#pragma unroll
+  for (int i = 0; i < KS; ++i) v[R::F(i)] = f[i];
+#pragma unroll
+  for (int c = 0; c < R::NC; ++c) {
+    typename Vec16<Real>::type w;
+    memcpy(&w, &v[c * R::PER], 16);
+    tile[c * kTile + j] = w;
+  }
+}
+
+// Adds the records j = j0, j0+js, ... < n to two targets (FP64 accumulators;
+// FP32 sums never run over more than one tile).
+template <class Real, int Ker, bool Surface1 = false>
+__device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile, int n, int j0, int js,
+                                         const Pt<Real>& pa, const Pt<Real>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
+  constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
+  using R = Rec<Real, KS>;
+  Real ua[KT], ub[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) ua[k] = ub[k] = 0;
+#pragma unroll 2
+  for (int j = j0; j < n; j += js) {
+    Real v[R::NVP];
+#pragma unroll
+    for (int c = 0; c < R::NC; ++c) {
+      const typename Vec16<Real>::type w = tile[c * kTile + j];
+      memcpy(&v[c * R::PER], &w, 16);
+    }
+    Real f[KS];
+#pragma unroll
+    for (int i = 0; i < KS; ++i) f[i] = v[R::F(i)];
+    Real rx, ry, rz;
+    if constexpr (R::kLo) {
+      rx = (pa.x - v[0]) + (pa.xl - v[4]);
+      ry = (pa.y - v[1]) + (pa.yl - v[5]);
+      rz = (pa.z - v[2]) + (pa.zl - v[6]);
+    } else {
+      rx = pa.x - v[0];
+      ry = pa.y - v[1];
+      rz = pa.z - v[2];
+    }
+    ker_eval<Ker, Real, Surface1>(rx, ry, rz, f, ua);
+    if constexpr (R::kLo) {
+      rx = (pb.x - v[0]) + (pb.xl - v[4]);
+      ry = (pb.y - v[1]) + (pb.yl - v[5]);
+      rz = (pb.z - v[2]) + (pb.zl - v[6]);
+    } else {
+      rx = pb.x - v[0];
+      ry = pb.y - v[1];
+      rz = pb.z - v[2];
+    }
+    ker_eval<Ker, Real, Surface1>(rx, ry, rz, f, ub);
+  }
+#pragma unroll
+  for (int k = 0; k < KT; ++k) {
+    acc[0][k] += (double)ua[k];
+    acc[1][k] += (double)ub[k];
+  }
+}
+
 template <class Real, int Ker>
-__global__ void __launch_bounds__(kNT) near_field_kernel(
+__global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS_F32 : PVFMM_NEAR_MIN_BLOCKS_F64)
+    near_field_kernel(
     const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo, const int* __restrict__ thi,
     const int* __restrict__ slo, const int* __restrict__ shi, const int* __restrict__ p_off, const int* __restrict__ p_list,
     const int* __restrict__ w_off, const int* __restrict__ w_list, const double* __restrict__ tx,
@@ -242,9 +339,11 @@ __global__ void __launch_bounds__(kNT) near_field_kernel(
     const double* __restrict__ ue, const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
     double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
-  __shared__ Tile<Real, KS> tl;
-  __shared__ Tile<double, KS> tl64;
-  __shared__ double red[kNT][KT];
+  constexpr bool kF32 = sizeof(Real) == 4;
+  using V = typename Vec16<Real>::type;
+  __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
+  __shared__ double2 tile64[kF32 ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
+  __shared__ double red[kNF][2][KT];
   const int b = blockIdx.x;
   const int T = tleaf[b];
   double cx, cy, cz, half;
@@ -252,40 +351,125 @@ __global__ void __launch_bounds__(kNT) near_field_kernel(
   node_geom(keys[T], cx, cy, cz, half, dT);
   const int t0 = tlo[T], nt = thi[T] - t0;
   const int dim = ns * KS;
-  for (int c0 = 0; c0 < nt; c0 += kNT) {
-    const Split sp(nt - c0);
-    const int t = t0 + c0 + sp.ti;
-    double qx = 0, qy = 0, qz = 0;
-    if (sp.active) {
-      qx = tx[t];
-      qy = ty[t];
-      qz = tz[t];
-    }
-    const Pt<Real> pt = make_pt<Real>(qx, qy, qz);
-    const Pt<double> pt64 = make_pt<double>(qx, qy, qz);
-    double acc[KT];
+  int buf = 0;
+  for (int c0 = 0; c0 < nt; c0 += 2 * kNF) {
+    const int m = min(2 * kNF, nt - c0);
+    const int nc = (m + 1) >> 1;
+    const int G = min(8, kNF / nc);
+    const int ti = threadIdx.x % nc, g = threadIdx.x / nc;
+    const bool active = g < G;
+    const bool vb = ti + nc < m;
+    const int ta = t0 + c0 + ti, tb = vb ? ta + nc : ta;
+    const Pt<Real> pa = make_pt<Real>(tx[ta], ty[ta], tz[ta]);
+    const Pt<Real> pb = make_pt<Real>(tx[tb], ty[tb], tz[tb]);
+    double acc[2][KT];
 #pragma unroll
-    for (int k = 0; k < KT; ++k) acc[k] = 0;
-    // D2T in FP64 in both forms: the downward equivalent densities come from
-    // the FP64-cutoff pseudo-inverse, whose large cancelling components only
-    // FP64 sums resolve.
-    if (de) surface_sources<double, Ker>(tl64, usurf, ns, 0, 0, 0, half * kRad1, de + (long)b * dim, sp, pt64, acc);
+    for (int k = 0; k < KT; ++k) acc[0][k] = acc[1][k] = 0;
+    __syncthreads();  // the previous chunk is done with the tiles and with red
+    int fill = 0;
+    auto flush = [&]() {
+      __syncthreads();  // records of tiles[buf] visible; tiles[buf^1] no longer read
+      if (active) rec_sum2<Real, Ker>(tiles[buf], fill, g, G, pa, pb, acc);
+      buf ^= 1;
+      fill = 0;
+    };
+    // sources on a cube surface: off + hr * u_k, FP64 densities `dens`
+    auto add_surface = [&](double ox, double oy, double oz, double hr, const double* __restrict__ dens) {
+      for (int done = 0; done < ns;) {
+        const int take = min(ns - done, kTile - fill);
+        for (int i = threadIdx.x; i < take; i += kNF) {
+          const int k = done + i;
+          Real f[KS];
+#pragma unroll
+          for (int c = 0; c < KS; ++c) f[c] = (Real)dens[k * KS + c];
+          rec_store<Real, KS>(tiles[buf], fill + i, ox + hr * usurf[k * 3 + 0], oy + hr * usurf[k * 3 + 1],
+                              oz + hr * usurf[k * 3 + 2], f);
+        }
+        fill += take;
+        done += take;
+        if (fill == kTile) flush();
+      }
+    };
+    // sorted points [lo, hi) of a leaf whose centre is at offset (ox, oy, oz)
+    auto add_points = [&](int lo, int hi, double ox, double oy, double oz) {
+      for (int p0 = lo; p0 < hi;) {
+        const int take = min(hi - p0, kTile - fill);
+        for (int i = threadIdx.x; i < take; i += kNF) {
+          const int p = p0 + i;
+          Real f[KS];
+#pragma unroll
+          for (int c = 0; c < KS; ++c) f[c] = (Real)den[(long)p * KS + c];
+          rec_store<Real, KS>(tiles[buf], fill + i, sx[p] + ox, sy[p] + oy, sz[p] + oz, f);
+        }
+        fill += take;
+        p0 += take;
+        if (fill == kTile) flush();
+      }
+    };
+    // D2T: the downward equivalent densities come from the FP64-cutoff
+    // pseudo-inverse, whose large cancelling components only FP64 sums
+    // resolve, so the mixed form evaluates them from FP64 records.
+    if (de) {
+      const double hr = half * kRad1;
+      const double* dens = de + (long)b * dim;
+      if constexpr (kF32) {
+        const Pt<double> pa64 = make_pt<double>(tx[ta], ty[ta], tz[ta]);
+        const Pt<double> pb64 = make_pt<double>(tx[tb], ty[tb], tz[tb]);
+        for (int k0 = 0; k0 < ns; k0 += kTile) {
+          const int n = min(kTile, ns - k0);
+          for (int i = threadIdx.x; i < n; i += kNF) {
+            const int k = k0 + i;
+            double f[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) f[c] = dens[k * KS + c];
+            rec_store<double, KS>(tile64, i, hr * usurf[k * 3 + 0], hr * usurf[k * 3 + 1], hr * usurf[k * 3 + 2], f);
+          }
+          __syncthreads();
+          if (active) rec_sum2<double, Ker, true>(tile64, n, g, G, pa64, pb64, acc);
+          __syncthreads();
+        }
+      } else {
+        add_surface(0, 0, 0, hr, dens);
+      }
+    }
     for (int w = w_off[T]; w < w_off[T + 1]; ++w) {
       const int S = w_list[w];
       double sxc, syc, szc, sh;
       int dS;
       node_geom(keys[S], sxc, syc, szc, sh, dS);
-      surface_sources<Real, Ker>(tl, usurf, ns, sxc - cx, syc - cy, szc - cz, sh * kRad0, ue + (long)S * dim, sp, pt,
-                                 acc);
+      add_surface(sxc - cx, syc - cy, szc - cz, sh * kRad0, ue + (long)S * dim);
     }
     for (int q = p_off[T]; q < p_off[T + 1]; ++q) {
       const int S = p_list[q];
       double sxc, syc, szc, sh;
       int dS;
       node_geom(keys[S], sxc, syc, szc, sh, dS);
-      point_sources<Real, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], sxc - cx, syc - cy, szc - cz, sp, pt, acc);
+      add_points(slo[S], shi[S], sxc - cx, syc - cy, szc - cz);
     }
-    reduce_store<KT>(red, sp, acc, scale, pot + (long)(t0 + c0) * KT, false);
+    if (fill > 0) flush();
+    // fixed-order sum of the G partial sums of each target
+    if (active)
+#pragma unroll
+      for (int k = 0; k < KT; ++k) {
+        red[threadIdx.x][0][k] = acc[0][k];
+        red[threadIdx.x][1][k] = acc[1][k];
+      }
+    __syncthreads();
+    if (active && g == 0) {
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        if (t == 1 && !vb) break;
+        double sum[KT];
+#pragma unroll
+        for (int k = 0; k < KT; ++k) sum[k] = red[ti][t][k];
+        for (int gg = 1; gg < G; ++gg)
+#pragma unroll
+          for (int k = 0; k < KT; ++k) sum[k] += red[gg * nc + ti][t][k];
+        const long o = (long)(t0 + c0 + ti + (t ? nc : 0)) * KT;
+#pragma unroll
+        for (int k = 0; k < KT; ++k) pot[o + k] = sum[k] * scale;
+      }
+    }
   }
 }
 
@@ -876,7 +1060,7 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, g, dim, ctx.dops.dc2de0.get<double>(), dim, t1, dim, 0);
     dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, t1, dim, ctx.dops.dc2de1.get<double>(), dim, de, dim, 0);
     ++ctx.n_launch;
-    near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNT, 0, s>>>(
+    near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNF, 0, s>>>(
         T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
         T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
         T.tz.get<double>(), sx, sy, sz, den, ue, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T), pot);

@@ -112,10 +112,24 @@ __device__ __forceinline__ double rsqrt_nr(double r2) {
   y = y * (1.5 - h * y * y);
   return y;
 }
+// FP32: one hardware reciprocal square root (rsqrt.approx.ftz, relative
+// error about 2^-22) refined by one Newton-Raphson step for f(y) = 1/y^2 - x,
+// y <- y (3 - x y^2) / 2; 0 for r2 == 0 (and for r2 below the FP32 normal
+// range, which flushes to zero).
 __device__ __forceinline__ float rsqrt_nr(float r2) {
-  const float y0 = rsqrtf(r2);
+  float y0;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(r2));
   const float y = y0 * (1.5f - 0.5f * r2 * y0 * y0);
   return r2 > 0.f ? y : 0.f;
+}
+// FP64 with one Newton step from the FP32 seed (relative error ~1e-13), for
+// r2 in the FP32 normal range; used where the pair distance is bounded away
+// from zero (equivalent-surface sources).
+__device__ __forceinline__ double rsqrt_nr1(double r2) {
+  float y0;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"((float)r2));
+  const double y = (double)y0;
+  return y * (1.5 - 0.5 * r2 * y * y);
 }
 
 // ---------------------------------------------------------------------------
@@ -138,10 +152,14 @@ template <>
 struct KerDims<kKerLaplacePG> { static constexpr int KS = 1, KT = 4; };
 
 // Adds K(r) f to u (r = target - source).
-template <int Ker, class Real>
+// Surface1 = true: the source is an equivalent-surface point at a distance
+// bounded away from zero, and FP64 needs only one Newton step.
+template <int Ker, class Real, bool Surface1 = false>
 __device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* f, Real* u) {
   const Real r2 = rx * rx + ry * ry + rz * rz;
-  const Real rinv = rsqrt_nr(r2);
+  Real rinv;
+  if constexpr (Surface1 && sizeof(Real) == 8) rinv = rsqrt_nr1(r2);
+  else rinv = rsqrt_nr(r2);
   if constexpr (Ker == kKerLaplace) {
     u[0] += rinv * f[0];
   } else if constexpr (Ker == kKerLaplaceGrad) {

@@ -696,32 +696,32 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   // 5. refinement, level by level
   std::vector<long> nR;
   {
-    DevBuf cur_b, next_b;
+    // two persistent level buffers (no allocation in steady state)
+    DevBuf* cur_b = &ctx.t[16];
+    DevBuf* next_b = &ctx.t[17];
     MKey root = make_key(0, 0, 0, 0);
-    PVFMM_CUDA_CHECK(cudaMemcpyAsync(cur_b.as<MKey>(1), &root, sizeof(MKey), cudaMemcpyHostToDevice, s));
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(cur_b->as<MKey>(1), &root, sizeof(MKey), cudaMemcpyHostToDevice, s));
     long n_cur = 1;
     int d = 0;
     while (n_cur > 0) {
       int* split = ctx.t[3].as<int>(n_cur);
       int* offs = ctx.t[23].as<int>(n_cur);
       ++ctx.n_launch;
-      refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), n_cur, d, sk, T.n_src, tk,
+      refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b->get<MKey>(), n_cur, d, sk, T.n_src, tk,
                                                                    T.n_trg, d_gk, n_gk, ctx.max_pts,
                                                                    kMaxDepth, split);
       const long n_split = exclusive_scan(ctx, split, offs, n_cur);
       if (n_split == 0) break;
       if ((long)ctx.lvlR.size() <= d) ctx.lvlR.resize(d + 1);
       MKey* R = ctx.lvlR[d].as<MKey>(n_split);
-      MKey* next = next_b.as<MKey>(n_split * 8);
+      MKey* next = next_b->as<MKey>(n_split * 8);
       ++ctx.n_launch;
-      make_children<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b.get<MKey>(), split, offs, n_cur, d, next, R);
+      make_children<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b->get<MKey>(), split, offs, n_cur, d, next, R);
       nR.push_back(n_split);
       std::swap(cur_b, next_b);
       n_cur = n_split * 8;
       ++d;
     }
-    cur_b.release();
-    next_b.release();
   }
   const int dint = (int)nR.size() - 1;  // deepest level with internal nodes (-1: root is a leaf)
   // 6. 2:1 balance closure
