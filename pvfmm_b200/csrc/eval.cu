@@ -819,6 +819,138 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, con
   }
 }
 
+// Hadamard products for scalar expansions (ke = 1), register form.  Same
+// product as hadamard_kernel,
+//   OUT[P][j1] += sum_{offset o, source child j2} M[f][o][j1][j2] * IN[Q_o(P)][f][j2],
+// but each thread gathers the neighbour spectrum rows of its PB target
+// parents straight from global memory (L2) into registers, one offset ahead
+// of the one it multiplies, so shared memory holds only the 26 operator
+// blocks of the block's frequency (read as 16-byte broadcasts).  Offsets that
+// none of the thread's parents has are skipped.
+template <class Real, int PB>
+__global__ void __launch_bounds__(128) hadamard_rd_kernel(int n3h, long n_vtrg, const int* __restrict__ vtab,
+                                                          const Cplx<Real>* __restrict__ spec_in,
+                                                          const Cplx<Real>* __restrict__ vop,
+                                                          Cplx<Real>* __restrict__ spec_out) {
+  constexpr int NT = 128;
+  constexpr int BLK = 64;                                       // 8 x 8 complex per offset
+  using V = typename Vec16<Real>::type;                         // 16 bytes
+  constexpr int CPV = 16 / (int)sizeof(Cplx<Real>);             // complex values per vector (2 or 1)
+  constexpr int NV = 8 / CPV;                                   // vectors per spectrum row
+  __shared__ V Ms[26 * BLK / CPV];
+  const int f = blockIdx.y;
+  const long pbase = (long)blockIdx.x * NT * PB + threadIdx.x;
+  {
+    const V* src = reinterpret_cast<const V*>(vop + (long)f * 26 * BLK);
+    for (int i = threadIdx.x; i < 26 * BLK / CPV; i += NT) Ms[i] = __ldg(src + i);
+  }
+  long prow[PB];
+  bool pin[PB];
+#pragma unroll
+  for (int k = 0; k < PB; ++k) {
+    prow[k] = pbase + (long)k * NT;
+    pin[k] = prow[k] < n_vtrg;
+  }
+  Real ar[PB][8], ai[PB][8];
+#pragma unroll
+  for (int k = 0; k < PB; ++k)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ar[k][j] = ai[k][j] = 0;
+  V xc[PB][NV], xn[PB][NV];
+  unsigned mc = 0, mn = 0;  // bit k: parent k has offset o
+  auto load = [&](int o, V (&x)[PB][NV], unsigned& mask) {
+    mask = 0;
+#pragma unroll
+    for (int k = 0; k < PB; ++k) {
+      const int q = pin[k] ? __ldg(vtab + (long)o * n_vtrg + prow[k]) : -1;
+      if (q >= 0) {
+        mask |= 1u << k;
+        const V* r = reinterpret_cast<const V*>(spec_in + ((long)q * n3h + f) * 8);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) x[k][v] = __ldg(r + v);
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) memset(&x[k][v], 0, 16);
+      }
+    }
+  };
+  load(0, xc, mc);
+  __syncthreads();
+#pragma unroll 1
+  for (int o = 0; o < 26; ++o) {
+    if (o + 1 < 26) load(o + 1, xn, mn);
+    if (mc) {
+      const V* Mo = Ms + o * (BLK / CPV);
+#pragma unroll
+      for (int jv = 0; jv < NV; ++jv) {  // source children j2 = jv*CPV .. jv*CPV+CPV-1
+        Real xr[PB][CPV], xi[PB][CPV];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+          Real t[2 * CPV];
+          memcpy(t, &xc[k][jv], 16);
+#pragma unroll
+          for (int c = 0; c < CPV; ++c) {
+            xr[k][c] = t[2 * c];
+            xi[k][c] = t[2 * c + 1];
+          }
+        }
+#pragma unroll
+        for (int j1 = 0; j1 < 8; ++j1) {
+          Real m[2 * CPV];
+          const V mv = Mo[(j1 * 8) / CPV + jv];
+          memcpy(m, &mv, 16);
+#pragma unroll
+          for (int c = 0; c < CPV; ++c)
+#pragma unroll
+            for (int k = 0; k < PB; ++k) {
+              ar[k][j1] += m[2 * c] * xr[k][c] - m[2 * c + 1] * xi[k][c];
+              ai[k][j1] += m[2 * c] * xi[k][c] + m[2 * c + 1] * xr[k][c];
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PB; ++k)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) xc[k][v] = xn[k][v];
+    mc = mn;
+  }
+#pragma unroll
+  for (int k = 0; k < PB; ++k) {
+    if (!pin[k]) continue;
+    V* out = reinterpret_cast<V*>(spec_out + (prow[k] * n3h + f) * 8);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      Real t[2 * CPV];
+#pragma unroll
+      for (int c = 0; c < CPV; ++c) {
+        t[2 * c] = ar[k][v * CPV + c];
+        t[2 * c + 1] = ai[k][v * CPV + c];
+      }
+      V w;
+      memcpy(&w, t, 16);
+      out[v] = w;
+    }
+  }
+}
+
+template <class Real, int PB>
+void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout) {
+  DevTree& T = ctx.tree;
+  dim3 grid(ceil_div(T.n_vtrg, 128 * PB), n3h);
+  ++ctx.n_launch;
+  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, T.n_vtrg, T.vtab.get<int>(), sin_,
+                                                             ctx.dops.vop.get<Cplx<Real>>(), sout);
+}
+
+// Target parents per thread (register tile) of the scalar-kernel Hadamard.
+#ifndef PVFMM_HAD_PB_F32
+#define PVFMM_HAD_PB_F32 2
+#endif
+#ifndef PVFMM_HAD_PB_F64
+#define PVFMM_HAD_PB_F64 1
+#endif
+
 template <class Real, int KE, int PB, int OC>
 size_t hadamard_smem() {
   constexpr int NG = 8 * KE;
@@ -920,8 +1052,8 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
   ev(4);
   const int n3h = F::N3H;
   if (ke == 1) {
-    if constexpr (sizeof(Real) == 8) launch_hadamard<Real, 1, 2, 26>(ctx, n3h, sin_, sout);
-    else launch_hadamard<Real, 1, 4, 26>(ctx, n3h, sin_, sout);
+    if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout);
+    else launch_hadamard_rd<Real, PVFMM_HAD_PB_F32>(ctx, n3h, sin_, sout);
   } else {
     launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout);
   }
