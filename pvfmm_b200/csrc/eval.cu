@@ -116,7 +116,7 @@ __device__ __forceinline__ void tile_diff(const Tile<Real, KS>& tl, int j, const
 // Sums sources j = j0, j0+js, ... < n of the tile into acc (FP64).  Two
 // independent partial sums in Real give ILP; the tile sum is promoted to
 // FP64, so FP32 rounding never accumulates over more than one tile.
-template <class Real, int Ker>
+template <class Real, int Ker, bool Surface1 = false>
 __device__ __forceinline__ void tile_sum(const Tile<Real, KerDims<Ker>::KS>& tl, int n, int j0, int js,
                                          const Pt<Real>& p, double* acc) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
@@ -133,9 +133,9 @@ __device__ __forceinline__ void tile_sum(const Tile<Real, KerDims<Ker>::KS>& tl,
     }
     Real rx, ry, rz;
     tile_diff(tl, j, p, rx, ry, rz);
-    ker_eval<Ker, Real>(rx, ry, rz, f0, u0);
+    ker_eval<Ker, Real, Surface1>(rx, ry, rz, f0, u0);
     tile_diff(tl, j + js, p, rx, ry, rz);
-    ker_eval<Ker, Real>(rx, ry, rz, f1, u1);
+    ker_eval<Ker, Real, Surface1>(rx, ry, rz, f1, u1);
   }
   if (j < n) {
     Real f0[KS];
@@ -143,7 +143,7 @@ __device__ __forceinline__ void tile_sum(const Tile<Real, KerDims<Ker>::KS>& tl,
     for (int i = 0; i < KS; ++i) f0[i] = tl.f[i][j];
     Real rx, ry, rz;
     tile_diff(tl, j, p, rx, ry, rz);
-    ker_eval<Ker, Real>(rx, ry, rz, f0, u0);
+    ker_eval<Ker, Real, Surface1>(rx, ry, rz, f0, u0);
   }
 #pragma unroll
   for (int k = 0; k < KT; ++k) acc[k] += (double)u0[k] + (double)u1[k];
@@ -164,7 +164,7 @@ struct Split {
 };
 
 // Sources = sorted points [lo,hi) of a leaf whose centre is at offset (ox,oy,oz).
-template <class Real, int Ker>
+template <class Real, int Ker, bool Surface1 = false>
 __device__ void point_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __restrict__ sx,
                               const double* __restrict__ sy, const double* __restrict__ sz,
                               const double* __restrict__ den, int lo, int hi, double ox, double oy, double oz,
@@ -180,7 +180,7 @@ __device__ void point_sources(Tile<Real, KerDims<Ker>::KS>& tl, const double* __
       for (int i = 0; i < KS; ++i) tl.f[i][threadIdx.x] = (Real)den[(long)p * KS + i];
     }
     __syncthreads();
-    if (sp.active) tile_sum<Real, Ker>(tl, n, sp.g, sp.G, pt, acc);
+    if (sp.active) tile_sum<Real, Ker, Surface1>(tl, n, sp.g, sp.G, pt, acc);
   }
 }
 
@@ -328,22 +328,36 @@ __device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile,
   }
 }
 
+// One list entry of a target leaf as a segment of the packed source stream:
+// the points of a leaf (kind 0, `node` = first point), the upward equivalent
+// surface of a node (kind 1, `node` = node index) or the leaf's own downward
+// equivalent surface (kind 2, `node` = row of the D2T densities).  The offset
+// between node centres is a small multiple of a power of two, exact in FP32.
+struct NearSeg {
+  float ox, oy, oz;
+  int node;
+  int kind_depth;  // kind | depth << 4
+};
+constexpr int kSegCap = 128;  // list entries per batch
+
 template <class Real, int Ker>
 __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS_F32 : PVFMM_NEAR_MIN_BLOCKS_F64)
-    near_field_kernel(
-    const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo, const int* __restrict__ thi,
-    const int* __restrict__ slo, const int* __restrict__ shi, const int* __restrict__ p_off, const int* __restrict__ p_list,
-    const int* __restrict__ w_off, const int* __restrict__ w_list, const double* __restrict__ tx,
-    const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ sx,
-    const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ den,
-    const double* __restrict__ ue, const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
-    double* __restrict__ pot) {
+    near_field_kernel(const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo,
+                      const int* __restrict__ thi, const int* __restrict__ slo, const int* __restrict__ shi,
+                      const int* __restrict__ p_off, const int* __restrict__ p_list, const int* __restrict__ w_off,
+                      const int* __restrict__ w_list, const double* __restrict__ tx, const double* __restrict__ ty,
+                      const double* __restrict__ tz, const double* __restrict__ sx, const double* __restrict__ sy,
+                      const double* __restrict__ sz, const double* __restrict__ den, const double* __restrict__ ue,
+                      const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
+                      double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   constexpr bool kF32 = sizeof(Real) == 4;
   using V = typename Vec16<Real>::type;
   __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
   __shared__ double2 tile64[kF32 ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
   __shared__ double red[kNF][2][KT];
+  __shared__ NearSeg seg[kSegCap];
+  __shared__ int start[kSegCap + 1];
   const int b = blockIdx.x;
   const int T = tleaf[b];
   double cx, cy, cz, half;
@@ -351,6 +365,10 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
   node_geom(keys[T], cx, cy, cz, half, dT);
   const int t0 = tlo[T], nt = thi[T] - t0;
   const int dim = ns * KS;
+  const int wb = w_off[T], nW = w_off[T + 1] - wb;
+  const int pbeg = p_off[T], nP = p_off[T + 1] - pbeg;
+  const int nD = (de && !kF32) ? 1 : 0;  // plain form: D2T is a segment of the stream
+  const int n_ent = nD + nW + nP;
   int buf = 0;
   for (int c0 = 0; c0 < nt; c0 += 2 * kNF) {
     const int m = min(2 * kNF, nt - c0);
@@ -365,58 +383,18 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
     double acc[2][KT];
 #pragma unroll
     for (int k = 0; k < KT; ++k) acc[0][k] = acc[1][k] = 0;
-    __syncthreads();  // the previous chunk is done with the tiles and with red
-    int fill = 0;
-    auto flush = [&]() {
-      __syncthreads();  // records of tiles[buf] visible; tiles[buf^1] no longer read
-      if (active) rec_sum2<Real, Ker>(tiles[buf], fill, g, G, pa, pb, acc);
-      buf ^= 1;
-      fill = 0;
-    };
-    // sources on a cube surface: off + hr * u_k, FP64 densities `dens`
-    auto add_surface = [&](double ox, double oy, double oz, double hr, const double* __restrict__ dens) {
-      for (int done = 0; done < ns;) {
-        const int take = min(ns - done, kTile - fill);
-        for (int i = threadIdx.x; i < take; i += kNF) {
-          const int k = done + i;
-          Real f[KS];
-#pragma unroll
-          for (int c = 0; c < KS; ++c) f[c] = (Real)dens[k * KS + c];
-          rec_store<Real, KS>(tiles[buf], fill + i, ox + hr * usurf[k * 3 + 0], oy + hr * usurf[k * 3 + 1],
-                              oz + hr * usurf[k * 3 + 2], f);
-        }
-        fill += take;
-        done += take;
-        if (fill == kTile) flush();
-      }
-    };
-    // sorted points [lo, hi) of a leaf whose centre is at offset (ox, oy, oz)
-    auto add_points = [&](int lo, int hi, double ox, double oy, double oz) {
-      for (int p0 = lo; p0 < hi;) {
-        const int take = min(hi - p0, kTile - fill);
-        for (int i = threadIdx.x; i < take; i += kNF) {
-          const int p = p0 + i;
-          Real f[KS];
-#pragma unroll
-          for (int c = 0; c < KS; ++c) f[c] = (Real)den[(long)p * KS + c];
-          rec_store<Real, KS>(tiles[buf], fill + i, sx[p] + ox, sy[p] + oy, sz[p] + oz, f);
-        }
-        fill += take;
-        p0 += take;
-        if (fill == kTile) flush();
-      }
-    };
-    // D2T: the downward equivalent densities come from the FP64-cutoff
-    // pseudo-inverse, whose large cancelling components only FP64 sums
-    // resolve, so the mixed form evaluates them from FP64 records.
-    if (de) {
-      const double hr = half * kRad1;
-      const double* dens = de + (long)b * dim;
-      if constexpr (kF32) {
+    // D2T of the mixed form: the downward equivalent densities come from the
+    // FP64-cutoff pseudo-inverse, whose large cancelling components only FP64
+    // sums resolve, so they are evaluated from FP64 records.
+    if constexpr (kF32) {
+      if (de) {
+        const double hr = half * kRad1;
+        const double* dens = de + (long)b * dim;
         const Pt<double> pa64 = make_pt<double>(tx[ta], ty[ta], tz[ta]);
         const Pt<double> pb64 = make_pt<double>(tx[tb], ty[tb], tz[tb]);
         for (int k0 = 0; k0 < ns; k0 += kTile) {
           const int n = min(kTile, ns - k0);
+          __syncthreads();
           for (int i = threadIdx.x; i < n; i += kNF) {
             const int k = k0 + i;
             double f[KS];
@@ -426,27 +404,122 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
           }
           __syncthreads();
           if (active) rec_sum2<double, Ker, true>(tile64, n, g, G, pa64, pb64, acc);
-          __syncthreads();
         }
-      } else {
-        add_surface(0, 0, 0, hr, dens);
       }
     }
-    for (int w = w_off[T]; w < w_off[T + 1]; ++w) {
-      const int S = w_list[w];
-      double sxc, syc, szc, sh;
-      int dS;
-      node_geom(keys[S], sxc, syc, szc, sh, dS);
-      add_surface(sxc - cx, syc - cy, szc - cz, sh * kRad0, ue + (long)S * dim);
+    for (int e0 = 0; e0 < n_ent; e0 += kSegCap) {
+      const int ne = min(kSegCap, n_ent - e0);
+      __syncthreads();  // the previous batch (or chunk) is done with seg, start and the tiles
+      for (int i = threadIdx.x; i < ne; i += kNF) {
+        const int e = e0 + i;
+        NearSeg sg;
+        int cnt;
+        if (e < nD) {
+          sg = {0.f, 0.f, 0.f, b, 2 | (dT << 4)};
+          cnt = ns;
+        } else {
+          const bool is_w = e < nD + nW;
+          const int S = is_w ? w_list[wb + e - nD] : p_list[pbeg + e - nD - nW];
+          double sxc, syc, szc, sh;
+          int dS;
+          node_geom(keys[S], sxc, syc, szc, sh, dS);
+          sg.ox = (float)(sxc - cx);
+          sg.oy = (float)(syc - cy);
+          sg.oz = (float)(szc - cz);
+          if (is_w) {
+            sg.node = S;
+            sg.kind_depth = 1 | (dS << 4);
+            cnt = ns;
+          } else {
+            sg.node = slo[S];
+            sg.kind_depth = 0;
+            cnt = shi[S] - slo[S];
+          }
+        }
+        seg[i] = sg;
+        start[i] = cnt;
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {  // exclusive scan of the counts (4 entries per lane)
+        const int lane = threadIdx.x;
+        int v[4], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int idx = lane * 4 + q;
+          v[q] = idx < ne ? start[idx] : 0;
+          sum += v[q];
+        }
+        int inc = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, inc, d);
+          if (lane >= d) inc += y;
+        }
+        int ex = inc - sum;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int idx = lane * 4 + q;
+          if (idx < ne) start[idx] = ex;
+          ex += v[q];
+        }
+        if (lane == 31) start[ne] = inc;
+      }
+      __syncthreads();
+      const int total = start[ne];
+      const int ntile = (total + kTile - 1) / kTile;
+      // records j = threadIdx.x + u * kNF of a tile, fetched one tile ahead
+      double rx_[2], ry_[2], rz_[2], rf_[2][KS];
+      auto fetch = [&](int t) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = t * kTile + threadIdx.x + u * kNF;
+          if (r >= total) continue;
+          int lo = 0, hi = ne;  // largest s with start[s] <= r
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (start[mid] <= r) lo = mid;
+            else hi = mid;
+          }
+          const NearSeg sg = seg[lo];
+          const int i = r - start[lo];
+          const int kind = sg.kind_depth & 15;
+          if (kind == 0) {
+            const int p = sg.node + i;
+            rx_[u] = sx[p] + (double)sg.ox;
+            ry_[u] = sy[p] + (double)sg.oy;
+            rz_[u] = sz[p] + (double)sg.oz;
+#pragma unroll
+            for (int c = 0; c < KS; ++c) rf_[u][c] = den[(long)p * KS + c];
+          } else {
+            const double hr = ldexp(kind == 1 ? kRad0 : kRad1, -((sg.kind_depth >> 4) + 1));
+            const double* dens = (kind == 1 ? ue : de) + (long)sg.node * dim;
+            rx_[u] = (double)sg.ox + hr * usurf[i * 3 + 0];
+            ry_[u] = (double)sg.oy + hr * usurf[i * 3 + 1];
+            rz_[u] = (double)sg.oz + hr * usurf[i * 3 + 2];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) rf_[u][c] = dens[i * KS + c];
+          }
+        }
+      };
+      if (ntile > 0) fetch(0);
+      for (int t = 0; t < ntile; ++t) {
+        const int n = min(kTile, total - t * kTile);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int j = threadIdx.x + u * kNF;
+          if (j < n) {
+            Real f[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) f[c] = (Real)rf_[u][c];
+            rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
+          }
+        }
+        if (t + 1 < ntile) fetch(t + 1);
+        __syncthreads();  // tiles[buf] complete; tiles[buf^1] no longer read (its readers passed this barrier)
+        if (active) rec_sum2<Real, Ker>(tiles[buf], n, g, G, pa, pb, acc);
+        buf ^= 1;
+      }
     }
-    for (int q = p_off[T]; q < p_off[T + 1]; ++q) {
-      const int S = p_list[q];
-      double sxc, syc, szc, sh;
-      int dS;
-      node_geom(keys[S], sxc, syc, szc, sh, dS);
-      add_points(slo[S], shi[S], sxc - cx, syc - cy, szc - cz);
-    }
-    if (fill > 0) flush();
     // fixed-order sum of the G partial sums of each target
     if (active)
 #pragma unroll
@@ -480,7 +553,9 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
 // operator).  mode 1 (X, fmm_pts.txx:4444-4736): node = xtrg[b], sources =
 // the X list, added to DC[node].
 // ---------------------------------------------------------------------------
-template <int Ker>
+// Surface1 (mode 0 only): the check surface lies at least 1.2 half-widths
+// from every point of the leaf, so FP64 needs one Newton step (mixed form).
+template <int Ker, bool Surface1 = false>
 __global__ void __launch_bounds__(kNT) surface_check_kernel(
     int mode, const int* __restrict__ nodes, const MKey* __restrict__ keys, const int* __restrict__ slo,
     const int* __restrict__ shi, const int* __restrict__ x_off, const int* __restrict__ x_list,
@@ -513,7 +588,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
 #pragma unroll
     for (int c = 0; c < KT; ++c) acc[c] = 0;
     if (mode == 0) {
-      point_sources<double, Ker>(tl, sx, sy, sz, den, slo[T], shi[T], 0, 0, 0, sp, pt, acc);
+      point_sources<double, Ker, Surface1>(tl, sx, sy, sz, den, slo[T], shi[T], 0, 0, 0, sp, pt, acc);
     } else {
       for (int q = x_off[T]; q < x_off[T + 1]; ++q) {
         const int S = x_list[q];
@@ -544,10 +619,14 @@ struct FftSizes {
   static constexpr size_t tw_bytes = sizeof(Real) * 2 * N1;
 };
 
+// Output layout: ke == 1 writes the spectra piece-major, spec[f][piece][q],
+// a piece being the 16 bytes of children (2v, 2v+1) (FP32) or child v (FP64),
+// so that the Hadamard's gathers over Morton-adjacent parents coalesce;
+// ke > 1 writes spec[q][f][child*ke+comp].
 template <class Real, int M>
 __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
                                                      const int* __restrict__ child0, const double* __restrict__ ue,
-                                                     const int* __restrict__ fft_map, int ns,
+                                                     const int* __restrict__ fft_map, int ns, long n_q,
                                                      Cplx<Real>* __restrict__ spec) {
   using F = FftSizes<Real, M>;
   constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
@@ -620,7 +699,13 @@ __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups,
       re += v.re * twr[w] - v.im * twi[w];
       im += v.re * twi[w] + v.im * twr[w];
     }
-    out[(long)f * ngrid + gb + gi] = {re, im};
+    if (ke == 1) {
+      constexpr int CPV = 16 / (int)sizeof(Cplx<Real>);
+      const int child = gb + gi;
+      spec[(((long)f * (8 / CPV) + child / CPV) * n_q + q) * CPV + child % CPV] = {re, im};
+    } else {
+      out[(long)f * ngrid + gb + gi] = {re, im};
+    }
   }
 }
 
@@ -822,13 +907,15 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, con
 // Hadamard products for scalar expansions (ke = 1), register form.  Same
 // product as hadamard_kernel,
 //   OUT[P][j1] += sum_{offset o, source child j2} M[f][o][j1][j2] * IN[Q_o(P)][f][j2],
-// but each thread gathers the neighbour spectrum rows of its PB target
-// parents straight from global memory (L2) into registers, one offset ahead
-// of the one it multiplies, so shared memory holds only the 26 operator
-// blocks of the block's frequency (read as 16-byte broadcasts).  Offsets that
-// none of the thread's parents has are skipped.
+// but each thread gathers the neighbour spectra of its PB target parents
+// straight from global memory (L2) into registers, one offset ahead of the one
+// it multiplies, so shared memory holds only the 26 operator blocks of the
+// block's frequency (read as 16-byte broadcasts).  The input spectra are
+// piece-major (IN[f][piece][Q]): the neighbours Q_o(P) of the Morton-ordered
+// parents of a warp are mostly adjacent, so each 16-byte gather of a warp
+// coalesces.  Offsets that none of the thread's parents has are skipped.
 template <class Real, int PB>
-__global__ void __launch_bounds__(128) hadamard_rd_kernel(int n3h, long n_vtrg, const int* __restrict__ vtab,
+__global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtrg, long n_vsrc, const int* __restrict__ vtab,
                                                           const Cplx<Real>* __restrict__ spec_in,
                                                           const Cplx<Real>* __restrict__ vop,
                                                           Cplx<Real>* __restrict__ spec_out) {
@@ -865,55 +952,56 @@ __global__ void __launch_bounds__(128) hadamard_rd_kernel(int n3h, long n_vtrg, 
       const int q = pin[k] ? __ldg(vtab + (long)o * n_vtrg + prow[k]) : -1;
       if (q >= 0) {
         mask |= 1u << k;
-        const V* r = reinterpret_cast<const V*>(spec_in + ((long)q * n3h + f) * 8);
+        const V* r = reinterpret_cast<const V*>(spec_in) + (long)f * NV * n_vsrc + q;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) x[k][v] = __ldg(r + v);
+        for (int v = 0; v < NV; ++v) x[k][v] = __ldg(r + (long)v * n_vsrc);
       } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v) memset(&x[k][v], 0, 16);
       }
     }
   };
+  auto compute = [&](int o, const V (&x)[PB][NV], unsigned mask) {
+    if (!mask) return;
+    const V* Mo = Ms + o * (BLK / CPV);
+#pragma unroll
+    for (int jv = 0; jv < NV; ++jv) {  // source children j2 = jv*CPV .. jv*CPV+CPV-1
+      Real xr[PB][CPV], xi[PB][CPV];
+#pragma unroll
+      for (int k = 0; k < PB; ++k) {
+        Real t[2 * CPV];
+        memcpy(t, &x[k][jv], 16);
+#pragma unroll
+        for (int c = 0; c < CPV; ++c) {
+          xr[k][c] = t[2 * c];
+          xi[k][c] = t[2 * c + 1];
+        }
+      }
+#pragma unroll
+      for (int j1 = 0; j1 < 8; ++j1) {
+        Real m[2 * CPV];
+        const V mv = Mo[(j1 * 8) / CPV + jv];
+        memcpy(m, &mv, 16);
+#pragma unroll
+        for (int c = 0; c < CPV; ++c)
+#pragma unroll
+          for (int k = 0; k < PB; ++k) {
+            ar[k][j1] += m[2 * c] * xr[k][c] - m[2 * c + 1] * xi[k][c];
+            ai[k][j1] += m[2 * c] * xi[k][c] + m[2 * c + 1] * xr[k][c];
+          }
+      }
+    }
+  };
+  // two register sets in turn: the gathers of offset o+1 are in flight while
+  // offset o is multiplied (26 offsets, an even count)
   load(0, xc, mc);
   __syncthreads();
 #pragma unroll 1
-  for (int o = 0; o < 26; ++o) {
-    if (o + 1 < 26) load(o + 1, xn, mn);
-    if (mc) {
-      const V* Mo = Ms + o * (BLK / CPV);
-#pragma unroll
-      for (int jv = 0; jv < NV; ++jv) {  // source children j2 = jv*CPV .. jv*CPV+CPV-1
-        Real xr[PB][CPV], xi[PB][CPV];
-#pragma unroll
-        for (int k = 0; k < PB; ++k) {
-          Real t[2 * CPV];
-          memcpy(t, &xc[k][jv], 16);
-#pragma unroll
-          for (int c = 0; c < CPV; ++c) {
-            xr[k][c] = t[2 * c];
-            xi[k][c] = t[2 * c + 1];
-          }
-        }
-#pragma unroll
-        for (int j1 = 0; j1 < 8; ++j1) {
-          Real m[2 * CPV];
-          const V mv = Mo[(j1 * 8) / CPV + jv];
-          memcpy(m, &mv, 16);
-#pragma unroll
-          for (int c = 0; c < CPV; ++c)
-#pragma unroll
-            for (int k = 0; k < PB; ++k) {
-              ar[k][j1] += m[2 * c] * xr[k][c] - m[2 * c + 1] * xi[k][c];
-              ai[k][j1] += m[2 * c] * xi[k][c] + m[2 * c + 1] * xr[k][c];
-            }
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < PB; ++k)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) xc[k][v] = xn[k][v];
-    mc = mn;
+  for (int o = 0; o < 26; o += 2) {
+    load(o + 1, xn, mn);
+    compute(o, xc, mc);
+    if (o + 2 < 26) load(o + 2, xc, mc);
+    compute(o + 1, xn, mn);
   }
 #pragma unroll
   for (int k = 0; k < PB; ++k) {
@@ -939,7 +1027,7 @@ void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real
   DevTree& T = ctx.tree;
   dim3 grid(ceil_div(T.n_vtrg, 128 * PB), n3h);
   ++ctx.n_launch;
-  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, T.n_vtrg, T.vtab.get<int>(), sin_,
+  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, T.n_vtrg, T.n_vsrc, T.vtab.get<int>(), sin_,
                                                              ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
@@ -1048,7 +1136,8 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
   ++ctx.n_launch;
   fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid / Gu), 256, sm_up, s>>>(ke, Gu, ngrid / Gu, T.vsrc.get<int>(),
                                                                      T.child0.get<int>(), ue,
-                                                                     ctx.dops.fft_map.get<int>(), ctx.ns, sin_);
+                                                                     ctx.dops.fft_map.get<int>(), ctx.ns, T.n_vsrc,
+                                                                     sin_);
   ev(4);
   const int n3h = F::N3H;
   if (ke == 1) {
@@ -1133,8 +1222,8 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dim);
     double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * dim);
     ++ctx.n_launch;
-    surface_check_kernel<KerExp><<<T.n_sleaf, kNT, 0, s>>>(0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx,
-                                                            sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
+    surface_check_kernel<KerExp, sizeof(Real) == 4><<<T.n_sleaf, kNT, 0, s>>>(
+        0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
     dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, uc, dim, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, 0);
     dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, t1, dim, ctx.dops.uc2ue1.get<double>(), dim, uc, dim, 0);
     ++ctx.n_launch;
