@@ -194,6 +194,66 @@ def cpu_baseline(args):
                       f"one thread, setup=1, {dt:.1f} s"}
 
 
+# Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# two dominant kernels, measured by ncu at 1,000,000 points of the same
+# distribution (profiles/hadamard_rd_mixed_1M.md, profiles/near_field_mixed_1M.md)
+# and scaled here by the units a launch processes (traffic grows in proportion).
+TRAFFIC_1M = {
+    "hadamard": {"bytes": 735288320 + 663280640, "units": 4768 + 4767},   # units: n_vsrc + n_vtrg
+    "near_field": {"bytes": 150417920 + 23502592, "units": 1000000},      # units: n_trg
+}
+
+
+def roofline(B, peaks):
+    """Roofline objects of the V-list Hadamard and the fused near field.
+
+    Both kernels are bound by the SIMT FP32 (mixed) / FP64 (plain) pipe, not
+    by HBM or the tensor cores; the HBM view (algorithmic bytes / kernel time
+    against the measured copy bandwidth) is the reported `achieved`/`peak`,
+    and `compute` gives the FLOP view against the nominal SIMT peak
+    (148 SMs x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock).
+    Algorithmic units:
+      Hadamard: bytes = (n_vsrc + n_vtrg) * n3h * 8 children * 2 * rb (input
+        spectra read once, output spectra written once) + 26 * n3h * 64 * 2 * rb
+        (operators read once); flops = 512 * n3h * v_pairs (8x8 complex
+        matrix-vector product per (target parent, offset, frequency)).
+      near field: bytes = n_src * 32 + n_trg * 56 (sorted points and densities
+        read once, 4 outputs written) + n_tleaf * ns * 8 (D2T densities);
+        flops = 18 per pair (pot+grad) over p2p + w + d2t pairs.
+    """
+    st = B["stats"]
+    rb = B["real_bytes"]
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    smax = (B["clocks"] or {}).get("sm_max_mhz") or 1965.0
+    lanes = 128 if rb == 4 else 64
+    simt_peak = 148 * lanes * 2 * smax * 1e6 / 1e12
+    n3h = (2 * M_ORDER) ** 2 * (M_ORDER + 1)
+    ns = 6 * (M_ORDER - 1) ** 2 + 2
+    out = {}
+    had_ms = B["stages_ms"]["V-Hadamard"]
+    had_bytes = (st["n_vsrc"] + st["n_vtrg"]) * n3h * 8 * 2 * rb + 26 * n3h * 64 * 2 * rb
+    had_flops = 512.0 * n3h * st["v_pairs"]
+    near_ms = B["stages_ms"]["near-field kernel"]
+    near_bytes = st["n_src"] * 32 + st["n_trg"] * 56 + st["n_tleaf"] * ns * 8
+    near_flops = 18.0 * (st["p2p_pairs"] + st["w_pairs"] + st["d2t_pairs"])
+    for name, ms, byts, flops, tkey, units in (
+            ("hadamard_rd_kernel (V-list M2L)", had_ms, had_bytes, had_flops, "hadamard", st["n_vsrc"] + st["n_vtrg"]),
+            ("near_field_kernel (U-list P2P + W + D2T)", near_ms, near_bytes, near_flops, "near_field", st["n_trg"])):
+        ach = byts / (ms / 1000) / 1e9 if ms > 0 else 0.0
+        tr = TRAFFIC_1M[tkey]
+        traffic = tr["bytes"] * units / tr["units"] if tr["bytes"] else None
+        tflops = flops / (ms / 1000) / 1e12 if ms > 0 else 0.0
+        out[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic_bytes": byts, "kernel_ms": ms,
+                     "compute": {"pipe": "fp32 simt" if rb == 4 else "fp64 simt", "achieved_tflops": tflops,
+                                 "nominal_peak_tflops": simt_peak, "frac": tflops / simt_peak,
+                                 "flops": flops}}
+    ranked = sorted(out.values(), key=lambda r: -r["kernel_ms"])
+    return ranked[0], ranked[1]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -299,23 +359,13 @@ def main():
     ok = [f for f in forms if forms[f]["rel_l2"] <= TOL]
     best = max(ok, key=lambda f: forms[f]["targets_per_s"]) if ok else "plain"
     B = forms[best]
-    # roofline of the dominant kernel: the V-list Hadamard (HBM-bound per
-    # launch: input spectra read once, output spectra written once, the 26
-    # offset operators streamed once).
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             peaks = json.load(fh)
     except OSError:
         pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    st = B["stats"]
-    rb = B["real_bytes"]
-    n3h = (2 * M_ORDER) ** 2 * (M_ORDER + 1)
-    had_bytes = (st["n_vsrc"] + st["n_vtrg"]) * n3h * 8 * 2 * rb + 26 * n3h * 64 * 2 * rb
-    had_ms = B["stages_ms"]["V-Hadamard"]
-    achieved = had_bytes / (had_ms / 1000) / 1e9 if had_ms > 0 else 0.0
+    roof = roofline(B, peaks)
     line = {
         "metric": METRIC,
         "value": B["targets_per_s"],
@@ -334,16 +384,15 @@ def main():
                    "l2": "no flush: per-step working set (128 MB inputs + tree + GB-size spectra) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
         "form": best,
-        "forms": {f: {k: v for k, v in d.items() if k not in ("stats",)} for f, d in forms.items()},
+        "forms": forms,
         "mixed_over_plain": (forms["mixed"]["targets_per_s"] / forms["plain"]["targets_per_s"]
                              if "mixed" in forms and "plain" in forms else None),
         "e2e": {"value": B["e2e_targets_per_s"], "unit": "targets/s",
                 "h2d_bytes_per_step": N * 3 * 8 + N * 8, "d2h_bytes_per_step": N * 4 * 8},
         "gpu_launches": B["gpu_launches"],
         "clocks": B["clocks"],
-        "roofline": {"kernel": "hadamard_kernel (V-list M2L)", "bound": "hbm", "achieved": achieved,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_src,
-                     "traffic": None, "algorithmic_bytes": had_bytes, "kernel_ms": had_ms},
+        "roofline": roof[0],
+        "roofline_next": roof[1],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)

@@ -157,7 +157,9 @@ const char* PVFMMGetLastError(void);
 /* Device time in milliseconds of the stages of the last evaluation on ctx, in
  * the order of the reference profile tags: 0 setup (tree + lists),
  * 1 S2U, 2 U2U, 3 V-list FFT, 4 V-list Hadamard, 5 V-list IFFT, 6 X-list,
- * 7 D2D, 8 D2T+W+U (fused near field), 9 total.  Returns the number written. */
+ * 7 D2D, 8 D2T+W+U (D2T pseudo-inverse GEMMs and the fused near field),
+ * 9 total, 10 the near-field kernel alone, 11 the D2T GEMMs alone.  Returns
+ * the number written. */
 int PVFMMGetStageTimes(const void* ctx, double* ms, int n);
 
 /* Number of this library's own CUDA kernels launched on ctx since its
@@ -173,9 +175,10 @@ long PVFMMGetLaunchCount(const void* ctx);
  *   8: downward check potentials   (n_nodes x ns*k1, double)
  *   9: source permutation (sorted -> input index) x int64
  *  10: target permutation x int64
- *  11: 18 doubles of tree/list statistics: n_nodes, depth, n_sleaf, n_tleaf,
+ *  11: 19 doubles of tree/list statistics: n_nodes, depth, n_sleaf, n_tleaf,
  *      n_vsrc, n_vtrg, n_xtrg, list entries (p2p, x, w), pair counts (p2p,
- *      x, w, d2t, s2u), n_leaves, n_src, n_trg
+ *      x, w, d2t, s2u), n_leaves, n_src, n_trg, V-list (target parent,
+ *      offset) pairs
  * Copies at most `n` elements into out and returns the element count needed. */
 long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
 

@@ -263,14 +263,15 @@ class FMMParticleContext:
             raise RuntimeError(last_error())
 
     def stage_times(self) -> dict:
-        buf = np.zeros(10)
-        self._lib.PVFMMGetStageTimes(self._ptr, _ptr(buf), 10)
-        names = ["setup", "S2U", "U2U", "V-FFT", "V-Hadamard", "V-IFFT", "X-List", "D2D", "D2T+W+U", "total"]
+        buf = np.zeros(12)
+        self._lib.PVFMMGetStageTimes(self._ptr, _ptr(buf), 12)
+        names = ["setup", "S2U", "U2U", "V-FFT", "V-Hadamard", "V-IFFT", "X-List", "D2D", "D2T+W+U", "total",
+                 "near-field kernel", "D2T GEMMs"]
         return dict(zip(names, buf.tolist()))
 
     STAT_NAMES = ["n_nodes", "depth", "n_sleaf", "n_tleaf", "n_vsrc", "n_vtrg", "n_xtrg", "p2p_entries",
                   "x_entries", "w_entries", "p2p_pairs", "x_pairs", "w_pairs", "d2t_pairs", "s2u_pairs",
-                  "n_leaves", "n_src", "n_trg"]
+                  "n_leaves", "n_src", "n_trg", "v_pairs"]
 
     def tree_stats(self) -> dict:
         """Sizes of the tree and lists of the last setup (for roofline bookkeeping)."""

@@ -302,7 +302,7 @@ int PVFMMGetStageTimes(const void* ctx, double* ms, int n) {
     Context& c = h->ctx;
     PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
     PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
-    float t[10] = {0};
+    float t[12] = {0};
     auto el = [&](int a, int b) {
       float x = 0;
       if (cudaEventElapsedTime(&x, c.ev[a], c.ev[b]) != cudaSuccess) x = 0;
@@ -318,7 +318,9 @@ int PVFMMGetStageTimes(const void* ctx, double* ms, int n) {
     t[7] = el(7, 8);
     t[8] = el(8, 9);
     t[9] = el(11, 10);
-    const int k = std::min(n, 10);
+    t[10] = el(12, 9);
+    t[11] = el(8, 12);
+    const int k = std::min(n, 12);
     for (int i = 0; i < k; ++i) ms[i] = t[i];
     return k;
   } catch (const std::exception& e) {
@@ -413,7 +415,7 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n) {
       case 11: {
         // [n_nodes, depth, n_sleaf, n_tleaf, n_vsrc, n_vtrg, n_xtrg, p2p list entries, x entries,
         //  w entries, p2p pairs, x pairs (sources x check points), w pairs (surface x targets),
-        //  d2t pairs, s2u pairs, n_leaves, n_src, n_trg]
+        //  d2t pairs, s2u pairs, n_leaves, n_src, n_trg, V-list parent pairs]
         std::vector<int> slo(N), shi(N), tlo(N), thi(N), po(N + 1), xo(N + 1), wo(N + 1);
         std::vector<unsigned char> lf(N);
         PVFMM_CUDA_CHECK(cudaMemcpy(slo.data(), T.src_lo.ptr, N * sizeof(int), cudaMemcpyDeviceToHost));
@@ -437,12 +439,19 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n) {
           if (lf[t] && nt > 0) d2t += nt * c.ns;
           if (lf[t]) s2u += (double)c.ns * (shi[t] - slo[t]);
         }
-        const double v[18] = {(double)N, (double)T.depth, (double)T.n_sleaf, (double)T.n_tleaf, (double)T.n_vsrc,
+        // V-list (target parent, offset) pairs with a source parent
+        double vpairs = 0;
+        if (T.n_vtrg > 0) {
+          std::vector<int> vt((size_t)T.n_vtrg * 26);
+          PVFMM_CUDA_CHECK(cudaMemcpy(vt.data(), T.vtab.ptr, vt.size() * sizeof(int), cudaMemcpyDeviceToHost));
+          for (int q : vt) vpairs += q >= 0;
+        }
+        const double v[19] = {(double)N, (double)T.depth, (double)T.n_sleaf, (double)T.n_tleaf, (double)T.n_vsrc,
                               (double)T.n_vtrg, (double)T.n_xtrg, (double)T.n_p2p, (double)T.n_x, (double)T.n_w,
-                              p2p, xp, wp, d2t, s2u, nleaf, (double)T.n_src, (double)T.n_trg};
+                              p2p, xp, wp, d2t, s2u, nleaf, (double)T.n_src, (double)T.n_trg, vpairs};
         if (out)
-          for (long i = 0; i < 18 && i < n; ++i) ((double*)out)[i] = v[i];
-        return 18;
+          for (long i = 0; i < 19 && i < n; ++i) ((double*)out)[i] = v[i];
+        return 19;
       }
       default:
         throw std::runtime_error("unknown tree data selector");

@@ -1280,11 +1280,14 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     gather_rows<<<T.n_tleaf, 128, 0, s>>>(dc, T.tleaf.get<int>(), T.n_tleaf, dim, keys, 1, g);
     dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, g, dim, ctx.dops.dc2de0.get<double>(), dim, t1, dim, 0);
     dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, t1, dim, ctx.dops.dc2de1.get<double>(), dim, de, dim, 0);
+    ev(12);
     ++ctx.n_launch;
     near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNF, 0, s>>>(
         T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
         T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
         T.tz.get<double>(), sx, sy, sz, den, ue, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T), pot);
+  } else {
+    ev(12);
   }
   ev(9);
   // ---- output in input order, scaled by scale_x^trg_scal

@@ -83,7 +83,7 @@ struct Context {
   std::vector<DevBuf> lvlR, lvlS;  // per-level internal-node keys (refined / balanced)
   long n_launch = 0;      // own kernels launched since context creation
   std::vector<float> stage_ms;
-  std::array<cudaEvent_t, 12> ev{};
+  std::array<cudaEvent_t, 13> ev{};
   bool events_ready = false;
   // pinned host staging
   void* pinned = nullptr;
