@@ -619,10 +619,11 @@ struct FftSizes {
   static constexpr size_t tw_bytes = sizeof(Real) * 2 * N1;
 };
 
-// Output layout: ke == 1 writes the spectra piece-major, spec[f][piece][q],
-// a piece being the 16 bytes of children (2v, 2v+1) (FP32) or child v (FP64),
-// so that the Hadamard's gathers over Morton-adjacent parents coalesce;
-// ke > 1 writes spec[q][f][child*ke+comp].
+// Output layout: FP64 with ke == 1 writes the spectra piece-major,
+// spec[f][child][q] (16 bytes per child), so that the scalar Hadamard's
+// gathers over Morton-adjacent parents coalesce; otherwise rows
+// spec[q][f][child*ke+comp] (the tensor-core Hadamard reads a 64-byte FP32
+// row with four lanes).
 template <class Real, int M>
 __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
                                                      const int* __restrict__ child0, const double* __restrict__ ue,
@@ -699,10 +700,8 @@ __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups,
       re += v.re * twr[w] - v.im * twi[w];
       im += v.re * twi[w] + v.im * twr[w];
     }
-    if (ke == 1) {
-      constexpr int CPV = 16 / (int)sizeof(Cplx<Real>);
-      const int child = gb + gi;
-      spec[(((long)f * (8 / CPV) + child / CPV) * n_q + q) * CPV + child % CPV] = {re, im};
+    if (sizeof(Real) == 8 && ke == 1) {
+      spec[((long)f * 8 + gb + gi) * n_q + q] = {re, im};
     } else {
       out[(long)f * ngrid + gb + gi] = {re, im};
     }
@@ -1022,6 +1021,158 @@ __global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtr
   }
 }
 
+// ---------------------------------------------------------------------------
+// Hadamard products of the mixed form (ke = 1) on the tensor cores:
+// mma.sync m16n8k8 TF32 with FP32 accumulation, each product split into
+// three (a_hi b_hi + a_hi b_lo + a_lo b_hi, hi = the TF32 head of an FP32
+// value, lo = the exact FP32 remainder), which carries the products to within
+// ~2^-20 of FP32 (an emulation of the whole FMM with this split changes the
+// result by ~1e-8 relative).
+//
+// Per frequency f the product is a real GEMM over parent rows:
+//   OUT[P][(j1, re|im)] += sum_o sum_(j2, re|im) IN[Q_o(P)][(j2, re|im)] * B_o[(j2, re|im)][(j1, re|im)]
+// with B_o the real form of the complex 8x8 block M[f][o].  A warp owns MT
+// tiles of 16 target parents.  The A fragments come straight from the input
+// spectrum rows in L2: lane (g, t) loads the 16-byte piece t (children 2t and
+// 2t+1, re and im) of rows g and g+8 (four lanes read one 64-byte row), which
+// is exactly its fragment once the K order is chosen as k-step s, column
+// c -> float 4t + 2s (+1 for c = t + 4).  The B fragments of every (f, o, lane) are precomputed on the
+// host in that order, hi and lo, and staged per block in shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// hi = the value with its low 13 mantissa bits cleared (a TF32 number);
+// lo = x - hi, exact in FP32.
+__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
+  const unsigned h = __float_as_uint(x) & 0xffffe000u;
+  hi = h;
+  lo = __float_as_uint(x - __uint_as_float(h));
+}
+
+constexpr int kTcWarps = 8;  // warps per block of the tensor-core Hadamard
+#ifndef PVFMM_TC_MIN_BLOCKS
+#define PVFMM_TC_MIN_BLOCKS 2
+#endif
+
+template <int MT>
+__global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_tc_kernel(int n3h, long n_vtrg, long n_vsrc,
+                                                                       const int* __restrict__ vtab,
+                                                                       const float4* __restrict__ spec_in,
+                                                                       const float4* __restrict__ bfrag,
+                                                                       float2* __restrict__ spec_out) {
+  extern __shared__ float4 Bs[];  // [26 offsets][32 lanes][2]: (b0, b1) of the 4 (s, nt) blocks
+  constexpr int NP = kTcWarps * 16 * MT;  // target parents of the block
+  int* qs = reinterpret_cast<int*>(Bs + 26 * 32 * 2);  // [26][NP] source parent of each (offset, parent)
+  const int f = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long pb = (long)blockIdx.x * NP;
+  {
+    const float4* src = bfrag + (long)f * 26 * 32 * 2;
+    for (int i = threadIdx.x; i < 26 * 32 * 2; i += 32 * kTcWarps) Bs[i] = __ldg(src + i);
+    for (int i = threadIdx.x; i < 26 * NP; i += 32 * kTcWarps) {
+      const int o = i / NP;
+      const long p = pb + i % NP;
+      qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * n_vtrg + p) : -1;
+    }
+  }
+  __syncthreads();
+  const int w0 = warp * 16 * MT;  // first parent of the warp within the block
+  const long p0 = pb + w0;
+  const float4* in_f = spec_in + (long)f * 4 + t;  // row q: in_f[q * n3h * 4]
+  float acc[MT][2][4];
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.f;
+  float4 xa[MT][2], xb[MT][2], xc[MT][2];
+  auto load = [&](int o, float4 (&x)[MT][2]) {
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = qs[o * NP + w0 + mt * 16 + g + 8 * h];
+        x[mt][h] = q >= 0 ? __ldg(in_f + (long)q * n3h * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+  };
+  auto compute = [&](int o, const float4 (&x)[MT][2]) {
+    const float4* bl = Bs + (o * 32 + lane) * 2;
+    const float4 bv0 = bl[0], bv1 = bl[1];
+    const float bval[8] = {bv0.x, bv0.y, bv0.z, bv0.w, bv1.x, bv1.y, bv1.z, bv1.w};
+    unsigned bh[8], blo[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tf32_split(bval[i], bh[i], blo[i]);
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      unsigned ah[2][4], al[2][4];
+      tf32_split(x[mt][0].x, ah[0][0], al[0][0]);
+      tf32_split(x[mt][1].x, ah[0][1], al[0][1]);
+      tf32_split(x[mt][0].y, ah[0][2], al[0][2]);
+      tf32_split(x[mt][1].y, ah[0][3], al[0][3]);
+      tf32_split(x[mt][0].z, ah[1][0], al[1][0]);
+      tf32_split(x[mt][1].z, ah[1][1], al[1][1]);
+      tf32_split(x[mt][0].w, ah[1][2], al[1][2]);
+      tf32_split(x[mt][1].w, ah[1][3], al[1][3]);
+#pragma unroll
+      for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          const int bi = (s * 2 + nt) * 2;
+          const unsigned bh0 = bh[bi], bh1 = bh[bi + 1];
+          const unsigned bl0 = blo[bi], bl1 = blo[bi + 1];
+          mma_tf32_16x8x8(acc[mt][nt], al[s], bh0, bh1);
+          mma_tf32_16x8x8(acc[mt][nt], ah[s], bl0, bl1);
+          mma_tf32_16x8x8(acc[mt][nt], ah[s], bh0, bh1);
+        }
+    }
+  };
+  // three register sets in turn: the gathers of the next two offsets are in
+  // flight while one offset is multiplied
+  load(0, xa);
+  load(1, xb);
+#pragma unroll 1
+  for (int o = 0; o < 26; o += 3) {
+    if (o + 2 < 26) load(o + 2, xc);
+    compute(o, xa);
+    if (o + 3 < 26) load(o + 3, xa);
+    if (o + 1 < 26) compute(o + 1, xb);
+    if (o + 4 < 26) load(o + 4, xb);
+    if (o + 2 < 26) compute(o + 2, xc);
+  }
+  // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); column
+  // n = nt*8 + 2t (+1) is child j1 = 4nt + t, re (im).
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long p = p0 + mt * 16 + g + 8 * h;
+      if (p >= n_vtrg) continue;
+      float2* out = spec_out + (p * n3h + f) * 8;
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) out[4 * nt + t] = make_float2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+    }
+}
+
+void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout) {
+  DevTree& T = ctx.tree;
+  constexpr int MT = 2;
+  const size_t sm = (size_t)26 * 32 * 2 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(ceil_div(T.n_vtrg, 16 * MT * kTcWarps), n3h);
+  ++ctx.n_launch;
+  hadamard_tc_kernel<MT><<<grid, 32 * kTcWarps, sm, ctx.stream>>>(
+      n3h, T.n_vtrg, T.n_vsrc, T.vtab.get<int>(), reinterpret_cast<const float4*>(sin_),
+      ctx.dops.vop_frag.get<float4>(), reinterpret_cast<float2*>(sout));
+}
+
 template <class Real, int PB>
 void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout) {
   DevTree& T = ctx.tree;
@@ -1031,10 +1182,7 @@ void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real
                                                              ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
-// Target parents per thread (register tile) of the scalar-kernel Hadamard.
-#ifndef PVFMM_HAD_PB_F32
-#define PVFMM_HAD_PB_F32 2
-#endif
+// Target parents per thread (register tile) of the FP64 scalar Hadamard.
 #ifndef PVFMM_HAD_PB_F64
 #define PVFMM_HAD_PB_F64 1
 #endif
@@ -1142,7 +1290,7 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
   const int n3h = F::N3H;
   if (ke == 1) {
     if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout);
-    else launch_hadamard_rd<Real, PVFMM_HAD_PB_F32>(ctx, n3h, sin_, sout);
+    else launch_hadamard_tc(ctx, n3h, sin_, sout);
   } else {
     launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout);
   }
@@ -1304,6 +1452,39 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
 
 }  // namespace
 
+// B fragments of hadamard_tc_kernel: for frequency f, offset o, lane (g, t)
+// and block (k-step s, n-tile nt): b0 = B[(j2, re)][(j1, pout)],
+// b1 = B[(j2, im)][(j1, pout)] with j2 = 2t + s, j1 = 4 nt + g/2,
+// pout = g % 2, where the real form of the complex block M = M[f][o][j1][j2]
+// is B[(j2,re)][(j1,re)] = Re M, B[(j2,im)][(j1,re)] = -Im M,
+// B[(j2,re)][(j1,im)] = Im M, B[(j2,im)][(j1,im)] = Re M.  Each value is
+// stored in FP32 as (b0, b1) for the blocks (s, nt) = (0,0), (0,1), (1,0),
+// (1,1); the kernel splits them into TF32 head and remainder.
+static void upload_vop_fragments(Context& ctx) {
+  const HostOperators& h = ctx.hops;
+  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  std::vector<float> fr((size_t)n3h * 26 * 32 * 8);
+  for (int f = 0; f < n3h; ++f)
+    for (int o = 0; o < 26; ++o)
+      for (int lane = 0; lane < 32; ++lane) {
+        const int g = lane >> 2, t = lane & 3;
+        for (int s = 0; s < 2; ++s)
+          for (int nt = 0; nt < 2; ++nt) {
+            const int j2 = 2 * t + s, j1 = 4 * nt + (g >> 1), pout = g & 1;
+            const size_t src = ((((size_t)f * 26 + o) * 8 + j1) * 8 + j2) * 2;
+            const float mr = (float)h.vop[src], mi = (float)h.vop[src + 1];
+            const float b0 = pout == 0 ? mr : mi;   // from (j2, re)
+            const float b1 = pout == 0 ? -mi : mr;  // from (j2, im)
+            float* d = &fr[((((size_t)f * 26 + o) * 32 + lane) * 4 + s * 2 + nt) * 2];
+            d[0] = b0;
+            d[1] = b1;
+          }
+      }
+  float* dev = ctx.dops.vop_frag.as<float>(fr.size());
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(dev, fr.data(), fr.size() * sizeof(float), cudaMemcpyHostToDevice, ctx.stream));
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+}
+
 void upload_operators(Context& ctx) {
   const HostOperators& h = ctx.hops;
   auto s = ctx.stream;
@@ -1316,6 +1497,7 @@ void upload_operators(Context& ctx) {
   upload_vec<double>(ctx.dops.usurf, h.usurf, s);
   if (ctx.precision == 0) upload_vec<double>(ctx.dops.vop, h.vop, s);
   else upload_vec<float>(ctx.dops.vop, h.vop, s);
+  if (ctx.precision == 1 && ctx.ki.ke == 1) upload_vop_fragments(ctx);
   int* fm = ctx.dops.fft_map.as<int>(h.fft_map.size());
   int* im = ctx.dops.ifft_map.as<int>(h.ifft_map.size());
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(fm, h.fft_map.data(), h.fft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));

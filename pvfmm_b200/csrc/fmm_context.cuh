@@ -52,6 +52,7 @@ struct DevTree {
 // Device copies of the operators in the working precision.
 struct DevOps {
   DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
+  DevBuf vop_frag;  // mixed form, ke = 1: Hadamard operators as TF32 hi/lo MMA fragments
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
 };
