@@ -231,7 +231,11 @@ constexpr int kNF = 128;        // threads per near-field block
 #ifndef PVFMM_NEAR_MIN_BLOCKS_F64
 #define PVFMM_NEAR_MIN_BLOCKS_F64 5
 #endif
-constexpr int kTile = 2 * kNF;  // source records per tile
+#ifndef PVFMM_NEAR_TILE_MULT
+#define PVFMM_NEAR_TILE_MULT 2
+#endif
+constexpr int kTile = PVFMM_NEAR_TILE_MULT * kNF;  // source records per tile
+constexpr int kRPT = kTile / kNF;                   // records each thread fetches per tile
 
 template <class Real>
 struct Vec16 {
@@ -468,10 +472,10 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
       const int total = start[ne];
       const int ntile = (total + kTile - 1) / kTile;
       // records j = threadIdx.x + u * kNF of a tile, fetched one tile ahead
-      double rx_[2], ry_[2], rz_[2], rf_[2][KS];
+      double rx_[kRPT], ry_[kRPT], rz_[kRPT], rf_[kRPT][KS];
       auto fetch = [&](int t) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kRPT; ++u) {
           const int r = t * kTile + threadIdx.x + u * kNF;
           if (r >= total) continue;
           int lo = 0, hi = ne;  // largest s with start[s] <= r
@@ -505,7 +509,7 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
       for (int t = 0; t < ntile; ++t) {
         const int n = min(kTile, total - t * kTile);
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kRPT; ++u) {
           const int j = threadIdx.x + u * kNF;
           if (j < n) {
             Real f[KS];

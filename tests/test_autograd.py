@@ -8,10 +8,12 @@ m = 8, 256 points per leaf, FP32 tensors, mixed form.
 * Against an FP64 direct-sum gradient on a 20,000-point subset (seed 35):
   dL/dq and dL/dx, rel-L2 <= 1e-5.
 * Against central finite differences of FP64 FMM evaluations at full size on
-  20 coordinates chosen with seed 34 (10 densities, 10 position components),
-  h = 1e-4: densities by one central difference (L is quadratic in q, so it
-  is exact up to rounding), positions by Richardson extrapolation of the
-  central differences at h and h/2 (truncation O(h^4)).  The FP64 evaluations
+  20 coordinates chosen with seed 34 (10 densities, 10 position components):
+  densities by one central difference with h = 1e-4 (L is quadratic in q, so
+  it is exact up to rounding), positions by Richardson extrapolation of the
+  central differences at h = 1e-5 and h/2 (truncation O(h^4 / r^4) for a
+  neighbour at distance r: at h = 1e-4 a neighbour 1e-3 away would already
+  leave ~1e-4).  The FP64 evaluations
   use a unit-box tree (coordinates as given), and a position coordinate whose
   perturbation changes the octree is replaced by the next candidate, so every
   difference is taken on one fixed octree.  Differences of L are summed as
@@ -150,14 +152,15 @@ def test_gradients_match_finite_differences_full_size():
         fd_q.append(np.sum(w * (pp - pm) * (pp + pm)) / (2 * h))
         ag_q.append(gq[j])
     fd_x, ag_x = [], []
+    hx = 1e-5
     for j, k in zip(rng.choice(n, 40, replace=False), rng.integers(0, 3, 40)):
         if len(fd_x) == 10:
             break
-        if not (h < X[j, k] < 1 - h):
+        if not (hx < X[j, k] < 1 - hx):
             continue
         d = []
         same_tree = True
-        for step in (h, h / 2):
+        for step in (hx, hx / 2):
             xp, xm = X.copy(), X.copy()
             xp[j, k] += step
             xm[j, k] -= step
@@ -174,8 +177,9 @@ def test_gradients_match_finite_differences_full_size():
     assert len(fd_x) == 10
     rel_q = np.linalg.norm(np.array(ag_q) - fd_q) / np.linalg.norm(fd_q)
     rel_x = np.linalg.norm(np.array(ag_x) - fd_x) / np.linalg.norm(fd_x)
+    per_x = np.abs(np.array(ag_x) - fd_x) / np.abs(fd_x)
     assert rel_q < 1e-5, rel_q
-    assert rel_x < 1e-5, rel_x
+    assert rel_x < 1e-5, (rel_x, per_x)
 
 
 def test_outputs_keep_the_input_dtype():
