@@ -618,29 +618,39 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
 template <class Real, int M>
 struct FftSizes {
   static constexpr int N1 = 2 * M, NH = M + 1, M3 = M * M * M, N3H = N1 * N1 * NH;
-  static constexpr size_t up_grid_bytes = sizeof(Real) * (M3 + 2 * (M * M * NH + M * N1 * NH));
-  static constexpr size_t dn_grid_bytes = sizeof(Real) * (2 * N3H + 2 * (M * N1 * NH + M * M * NH) + M3);
+  // forward: grid g [M3] real, a1 [M*M][NH] complex, a2 [M][N1][NH] complex
+  // (+4 complex of padding per grid, so that the z-lines of 4 neighbouring
+  // grids fall into different banks)
+  static constexpr int A2S = M * N1 * NH + 4;
+  static constexpr size_t up_grid_bytes = sizeof(Real) * (M3 + 2 * (M * M * NH + A2S));
+  // inverse: b1 [M][N1][NH] (+4 padding), b2 [M][M][NH] complex, o [M3] real
+  static constexpr int B1S = M * N1 * NH + 4;
+  static constexpr size_t dn_grid_bytes = sizeof(Real) * (2 * (B1S + M * M * NH) + M3);
   static constexpr size_t tw_bytes = sizeof(Real) * 2 * N1;
+  static constexpr int threads(int G) { return ((8 * NH * G + 31) / 32) * 32; }  // one thread per line of the widest stage
 };
 
+// Each stage of the separable DFTs: one thread per input line; it loads the
+// line into registers once and writes every output along that axis
+// (twiddle index (k * x) mod N1 known at compile time, read as a broadcast).
 // Output layout: FP64 with ke == 1 writes the spectra piece-major,
 // spec[f][child][q] (16 bytes per child), so that the scalar Hadamard's
 // gathers over Morton-adjacent parents coalesce; otherwise rows
 // spec[q][f][child*ke+comp] (the tensor-core Hadamard reads a 64-byte FP32
 // row with four lanes).
 template <class Real, int M>
-__global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
-                                                     const int* __restrict__ child0, const double* __restrict__ ue,
-                                                     const int* __restrict__ fft_map, int ns, long n_q,
-                                                     Cplx<Real>* __restrict__ spec) {
+__global__ void __launch_bounds__(288) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
+                                                      const int* __restrict__ child0, const double* __restrict__ ue,
+                                                      const int* __restrict__ fft_map, int ns, long n_q,
+                                                      Cplx<Real>* __restrict__ spec) {
   using F = FftSizes<Real, M>;
-  constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
+  constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H, A2S = F::A2S;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* twr = reinterpret_cast<Real*>(smem_raw);
   Real* twi = twr + N1;
   Real* g = twi + N1;                                          // G * M3
   Cplx<Real>* a1 = reinterpret_cast<Cplx<Real>*>(g + G * M3);  // G * M*M*NH
-  Cplx<Real>* a2 = a1 + G * M * M * NH;                        // G * M*N1*NH
+  Cplx<Real>* a2 = a1 + G * M * M * NH;                        // G * A2S
   const int q = blockIdx.x / ngroups;
   const int gb = (blockIdx.x % ngroups) * G;
   const int ngrid = 8 * ke;
@@ -649,10 +659,10 @@ __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups,
   const int c0 = child0[P];
   const int dim = ns * ke;
   for (int j = threadIdx.x; j < N1; j += blockDim.x) {
-    double s, c;
-    sincospi(-2.0 * j / N1, &s, &c);
-    twr[j] = (Real)c;
-    twi[j] = (Real)s;
+    double sn, cs;
+    sincospi(-2.0 * j / N1, &sn, &cs);
+    twr[j] = (Real)cs;
+    twi[j] = (Real)sn;
   }
   for (int i = threadIdx.x; i < gn * M3; i += blockDim.x) g[i] = 0;
   __syncthreads();
@@ -664,69 +674,86 @@ __global__ void __launch_bounds__(256) fft_up_kernel(int ke, int G, int ngroups,
     g[gi * M3 + x + M * (y + M * z)] = (Real)ue[(long)(c0 + c) * dim + k * ke + comp];
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < gn * M * M * NH; i += blockDim.x) {  // x -> kx (real input)
-    const int kx = i % NH, yz = i / NH;
-    const Real* row = g + (yz / (M * M)) * M3 + M * (yz % (M * M));
-    Real re = 0, im = 0;
+  // x -> kx (real input): line = (gi, z, y)
+  for (int r = threadIdx.x; r < gn * M * M; r += blockDim.x) {
+    const Real* row = g + r * M;
+    Real v[M];
 #pragma unroll
-    for (int x = 0; x < M; ++x) {
-      const int w = (kx * x) % N1;
-      re += row[x] * twr[w];
-      im += row[x] * twi[w];
+    for (int x = 0; x < M; ++x) v[x] = row[x];
+#pragma unroll
+    for (int kx = 0; kx < NH; ++kx) {
+      Real re = 0, im = 0;
+#pragma unroll
+      for (int x = 0; x < M; ++x) {
+        const int w = (kx * x) % N1;
+        re += v[x] * twr[w];
+        im += v[x] * twi[w];
+      }
+      a1[r * NH + kx] = {re, im};
     }
-    a1[i] = {re, im};
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < gn * M * N1 * NH; i += blockDim.x) {  // y -> ky
-    const int kx = i % NH, ky = (i / NH) % N1, zg = i / (NH * N1);  // zg = gi*M + z
+  // y -> ky: line = (gi, z, kx), kx fastest
+  for (int i = threadIdx.x; i < gn * M * NH; i += blockDim.x) {
+    const int kx = i % NH, zg = i / NH;  // zg = gi*M + z
+    const int gi = zg / M, z = zg % M;
     const Cplx<Real>* col = a1 + (zg * M) * NH + kx;
-    Real re = 0, im = 0;
+    Cplx<Real> v[M];
 #pragma unroll
-    for (int y = 0; y < M; ++y) {
-      const int w = (ky * y) % N1;
-      const Cplx<Real> v = col[y * NH];
-      re += v.re * twr[w] - v.im * twi[w];
-      im += v.re * twi[w] + v.im * twr[w];
+    for (int y = 0; y < M; ++y) v[y] = col[y * NH];
+    Cplx<Real>* dst = a2 + gi * A2S + (z * N1) * NH + kx;
+#pragma unroll
+    for (int ky = 0; ky < N1; ++ky) {
+      Real re = 0, im = 0;
+#pragma unroll
+      for (int y = 0; y < M; ++y) {
+        const int w = (ky * y) % N1;
+        re += v[y].re * twr[w] - v[y].im * twi[w];
+        im += v[y].re * twi[w] + v[y].im * twr[w];
+      }
+      dst[ky * NH] = {re, im};
     }
-    a2[i] = {re, im};
   }
   __syncthreads();
+  // z -> kz: line = (gi, ky, kx), gi fastest; spectrum index f = kx + NH*(ky + N1*kz)
   Cplx<Real>* out = spec + (long)q * N3H * ngrid;
-  for (int i = threadIdx.x; i < gn * N3H; i += blockDim.x) {  // z -> kz, stored spec[q][f][grid]
-    const int gi = i % gn, f = i / gn;
-    const int kx = f % NH, ky = (f / NH) % N1, kz = f / (NH * N1);
-    const Cplx<Real>* col = a2 + ((gi * M) * N1 + ky) * NH + kx;
-    Real re = 0, im = 0;
+  for (int i = threadIdx.x; i < gn * N1 * NH; i += blockDim.x) {
+    const int gi = i % gn, l = i / gn;  // l = ky*NH + kx
+    const Cplx<Real>* col = a2 + gi * A2S + l;
+    Cplx<Real> v[M];
 #pragma unroll
-    for (int z = 0; z < M; ++z) {
-      const int w = (kz * z) % N1;
-      const Cplx<Real> v = col[z * N1 * NH];
-      re += v.re * twr[w] - v.im * twi[w];
-      im += v.re * twi[w] + v.im * twr[w];
-    }
-    if (sizeof(Real) == 8 && ke == 1) {
-      spec[((long)f * 8 + gb + gi) * n_q + q] = {re, im};
-    } else {
-      out[(long)f * ngrid + gb + gi] = {re, im};
+    for (int z = 0; z < M; ++z) v[z] = col[z * N1 * NH];
+#pragma unroll
+    for (int kz = 0; kz < N1; ++kz) {
+      Real re = 0, im = 0;
+#pragma unroll
+      for (int z = 0; z < M; ++z) {
+        const int w = (kz * z) % N1;
+        re += v[z].re * twr[w] - v[z].im * twi[w];
+        im += v[z].re * twi[w] + v[z].im * twr[w];
+      }
+      const int f = l + N1 * NH * kz;
+      if (sizeof(Real) == 8 && ke == 1) spec[((long)f * 8 + gb + gi) * n_q + q] = {re, im};
+      else out[(long)f * ngrid + gb + gi] = {re, im};
     }
   }
 }
 
 template <class Real, int M>
-__global__ void __launch_bounds__(256) ifft_dn_kernel(int ke, int G, int ngroups, const int* __restrict__ vtrg,
-                                                      const int* __restrict__ child0, const MKey* __restrict__ keys,
-                                                      const Cplx<Real>* __restrict__ spec,
-                                                      const int* __restrict__ ifft_map, int ns,
-                                                      double* __restrict__ dc) {
+__global__ void __launch_bounds__(288) ifft_dn_kernel(int ke, int G, int ngroups, const int* __restrict__ vtrg,
+                                                       const int* __restrict__ child0, const MKey* __restrict__ keys,
+                                                       const Cplx<Real>* __restrict__ spec,
+                                                       const int* __restrict__ ifft_map, int ns,
+                                                       double* __restrict__ dc) {
   using F = FftSizes<Real, M>;
   constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* twr = reinterpret_cast<Real*>(smem_raw);
   Real* twi = twr + N1;
-  Cplx<Real>* S = reinterpret_cast<Cplx<Real>*>(twi + N1);  // G * N3H
-  Cplx<Real>* b1 = S + G * N3H;                             // G * M*N1*NH
-  Cplx<Real>* b2 = b1 + G * M * N1 * NH;                    // G * M*M*NH
-  Real* o = reinterpret_cast<Real*>(b2 + G * M * M * NH);   // G * M3
+  constexpr int B1S = F::B1S;
+  Cplx<Real>* b1 = reinterpret_cast<Cplx<Real>*>(twi + N1);  // G * B1S
+  Cplx<Real>* b2 = b1 + G * B1S;                             // G * M*M*NH
+  Real* o = reinterpret_cast<Real*>(b2 + G * M * M * NH);    // G * M3
   const int vt = blockIdx.x / ngroups;
   const int gb = (blockIdx.x % ngroups) * G;
   const int ngrid = 8 * ke;
@@ -738,60 +765,71 @@ __global__ void __launch_bounds__(256) ifft_dn_kernel(int ke, int G, int ngroups
   const double lscale = ldexp(1.0, (int)dP + 1);  // 2^(trg_scal * level of the children)
   const int dim = ns * ke;
   for (int j = threadIdx.x; j < N1; j += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * j / N1, &s, &c);  // inverse twiddles
-    twr[j] = (Real)c;
-    twi[j] = (Real)s;
-  }
-  const Cplx<Real>* in = spec + (long)vt * N3H * ngrid;
-  for (int i = threadIdx.x; i < gn * N3H; i += blockDim.x) {
-    const int gi = i % gn, f = i / gn;
-    S[gi * N3H + f] = in[(long)f * ngrid + gb + gi];
+    double sn, cs;
+    sincospi(2.0 * j / N1, &sn, &cs);  // inverse twiddles
+    twr[j] = (Real)cs;
+    twi[j] = (Real)sn;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < gn * M * N1 * NH; i += blockDim.x) {  // kz -> z in [M, 2M)
-    const int kx = i % NH, ky = (i / NH) % N1, zp = (i / (NH * N1)) % M, gi = i / (NH * N1 * M);
-    const int z = M + zp;
-    const Cplx<Real>* col = S + gi * N3H + ky * NH + kx;
-    Real re = 0, im = 0;
+  const Cplx<Real>* in = spec + (long)vt * N3H * ngrid + gb;
+  // kz -> z in [M, 2M): line = (gi, ky, kx) read straight from the spectrum
+  // row of the parent (gi fastest: neighbouring threads read neighbouring
+  // children of one frequency)
+  for (int i = threadIdx.x; i < gn * N1 * NH; i += blockDim.x) {
+    const int gi = i % gn, l = i / gn;  // l = ky*NH + kx
+    Cplx<Real> v[N1];
 #pragma unroll
-    for (int kz = 0; kz < N1; ++kz) {
-      const int w = (kz * z) % N1;
-      const Cplx<Real> v = col[kz * N1 * NH];
-      re += v.re * twr[w] - v.im * twi[w];
-      im += v.re * twi[w] + v.im * twr[w];
+    for (int kz = 0; kz < N1; ++kz) v[kz] = in[(long)(l + N1 * NH * kz) * ngrid + gi];
+#pragma unroll
+    for (int zp = 0; zp < M; ++zp) {
+      Real re = 0, im = 0;
+#pragma unroll
+      for (int kz = 0; kz < N1; ++kz) {
+        const int w = (kz * (M + zp)) % N1;
+        re += v[kz].re * twr[w] - v[kz].im * twi[w];
+        im += v[kz].re * twi[w] + v[kz].im * twr[w];
+      }
+      b1[gi * B1S + zp * N1 * NH + l] = {re, im};
     }
-    b1[i] = {re, im};
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < gn * M * M * NH; i += blockDim.x) {  // ky -> y in [M, 2M)
-    const int kx = i % NH, yp = (i / NH) % M, zg = i / (NH * M);  // zg = gi*M + zp
-    const int y = M + yp;
-    const Cplx<Real>* col = b1 + (zg * N1) * NH + kx;
-    Real re = 0, im = 0;
+  // ky -> y in [M, 2M): line = (gi, zp, kx), kx fastest
+  for (int i = threadIdx.x; i < gn * M * NH; i += blockDim.x) {
+    const int kx = i % NH, zg = i / NH;  // zg = gi*M + zp
+    const Cplx<Real>* col = b1 + (zg / M) * B1S + ((zg % M) * N1) * NH + kx;
+    Cplx<Real> v[N1];
 #pragma unroll
-    for (int ky = 0; ky < N1; ++ky) {
-      const int w = (ky * y) % N1;
-      const Cplx<Real> v = col[ky * NH];
-      re += v.re * twr[w] - v.im * twi[w];
-      im += v.re * twi[w] + v.im * twr[w];
+    for (int ky = 0; ky < N1; ++ky) v[ky] = col[ky * NH];
+#pragma unroll
+    for (int yp = 0; yp < M; ++yp) {
+      Real re = 0, im = 0;
+#pragma unroll
+      for (int ky = 0; ky < N1; ++ky) {
+        const int w = (ky * (M + yp)) % N1;
+        re += v[ky].re * twr[w] - v[ky].im * twi[w];
+        im += v[ky].re * twi[w] + v[ky].im * twr[w];
+      }
+      b2[(zg * M + yp) * NH + kx] = {re, im};
     }
-    b2[i] = {re, im};
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < gn * M3; i += blockDim.x) {  // kx -> x in [M, 2M), c2r
-    const int xp = i % M, zy = i / M;  // zy = (gi*M + zp)*M + yp
-    const int x = M + xp;
-    const Cplx<Real>* row = b2 + zy * NH;
-    Real acc = 0;
+  // kx -> x in [M, 2M), c2r: line = (gi, zp, yp)
+  for (int r = threadIdx.x; r < gn * M * M; r += blockDim.x) {
+    const Cplx<Real>* row = b2 + r * NH;
+    Cplx<Real> v[NH];
 #pragma unroll
-    for (int kx = 0; kx < NH; ++kx) {
-      const int w = (kx * x) % N1;
-      const Cplx<Real> v = row[kx];
-      const Real t = v.re * twr[w] - v.im * twi[w];
-      acc += (kx == 0 || 2 * kx == N1) ? t : (Real)2 * t;
+    for (int kx = 0; kx < NH; ++kx) v[kx] = row[kx];
+#pragma unroll
+    for (int xp = 0; xp < M; ++xp) {
+      Real acc = 0;
+#pragma unroll
+      for (int kx = 0; kx < NH; ++kx) {
+        const int w = (kx * (M + xp)) % N1;
+        const Real t = v[kx].re * twr[w] - v[kx].im * twi[w];
+        acc += (kx == 0 || 2 * kx == N1) ? t : (Real)2 * t;
+      }
+      o[r * M + xp] = acc;
     }
-    o[i] = acc;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < gn * ns; i += blockDim.x) {
@@ -1267,11 +1305,13 @@ void upload_vec(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
-// Largest divisor G of ngrid with fixed + G*per_grid <= budget (at least 1).
+// Largest divisor G of ngrid with fixed + G*per_grid <= budget and at most
+// 288 threads (the DFT kernels' launch bound) for threads(G) (at least 1).
+template <class F>
 int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
   int best = 1;
   for (int G = 1; G <= ngrid; ++G)
-    if (ngrid % G == 0 && fixed + G * per_grid <= budget) best = G;
+    if (ngrid % G == 0 && fixed + G * per_grid <= budget && F::threads(G) <= 288) best = G;
   return best;
 }
 
@@ -1282,11 +1322,11 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
   auto s = ctx.stream;
   using F = FftSizes<Real, M>;
   const int ngrid = 8 * ke;
-  const int Gu = grids_per_block(F::up_grid_bytes, F::tw_bytes, ngrid, 64 * 1024);
+  const int Gu = grids_per_block<F>(F::up_grid_bytes, F::tw_bytes, ngrid, 64 * 1024);
   const size_t sm_up = F::tw_bytes + Gu * F::up_grid_bytes;
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(fft_up_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_up));
   ++ctx.n_launch;
-  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid / Gu), 256, sm_up, s>>>(ke, Gu, ngrid / Gu, T.vsrc.get<int>(),
+  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid / Gu), F::threads(Gu), sm_up, s>>>(ke, Gu, ngrid / Gu, T.vsrc.get<int>(),
                                                                      T.child0.get<int>(), ue,
                                                                      ctx.dops.fft_map.get<int>(), ctx.ns, T.n_vsrc,
                                                                      sin_);
@@ -1299,12 +1339,12 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
     launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout);
   }
   ev(5);
-  const int Gd = grids_per_block(F::dn_grid_bytes, F::tw_bytes, ngrid, 80 * 1024);
+  const int Gd = grids_per_block<F>(F::dn_grid_bytes, F::tw_bytes, ngrid, 80 * 1024);
   const size_t sm_dn = F::tw_bytes + Gd * F::dn_grid_bytes;
   PVFMM_CUDA_CHECK(
       cudaFuncSetAttribute(ifft_dn_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
   ++ctx.n_launch;
-  ifft_dn_kernel<Real, M><<<T.n_vtrg * (ngrid / Gd), 256, sm_dn, s>>>(ke, Gd, ngrid / Gd, T.vtrg.get<int>(),
+  ifft_dn_kernel<Real, M><<<T.n_vtrg * (ngrid / Gd), F::threads(Gd), sm_dn, s>>>(ke, Gd, ngrid / Gd, T.vtrg.get<int>(),
                                                                       T.child0.get<int>(), T.key.get<MKey>(), sout,
                                                                       ctx.dops.ifft_map.get<int>(), ctx.ns, dc);
 }
