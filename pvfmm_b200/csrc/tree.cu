@@ -291,21 +291,34 @@ __global__ void node_ranges(const MKey* __restrict__ keys, long n, const MKey* _
 }
 
 // Colleague index ((z+1)*3+(y+1))*3+(x+1) (mpi_tree.txx:1143-1145).
-__global__ void colleagues_kernel(const MKey* __restrict__ keys, long base, long n_level, int* __restrict__ coll) {
+// Colleagues (the 27 same-level cells around a node, itself included; slot
+// ci = (dx+1) + 3(dy+1) + 9(dz+1)), from the parent's colleagues: the cell at
+// offset d from octant c of parent P is octant (c + d) mod 2 of P's colleague
+// at offset floor((c + d) / 2), which exists at this level iff that colleague
+// is internal (every internal node has all 8 children in the level arrays).
+// Same result as searching the level's sorted keys (interac_list.txx:98-130).
+__global__ void colleagues_kernel(long base, long n_level, const int* __restrict__ parent,
+                                  const int* __restrict__ child0, int* __restrict__ coll) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n_level) return;
-  unsigned int X, Y, Z, d;
-  decode_key(keys[base + i], X, Y, Z, d);
-  const long w = (long)(kTwo30 >> d);
+  const long v = base + i;
+  if (v == 0) {
+    for (int ci = 0; ci < 27; ++ci) coll[ci] = ci == 13 ? 0 : -1;
+    return;
+  }
+  const int P = parent[v];
+  const int oc = (int)(v - child0[P]);
+  const int ox = oc & 1, oy = (oc >> 1) & 1, oz = (oc >> 2) & 1;
   for (int ci = 0; ci < 27; ++ci) {
-    const long x = X + (ci % 3 - 1) * w, y = Y + ((ci / 3) % 3 - 1) * w, z = Z + (ci / 9 - 1) * w;
+    const int cx = ox + ci % 3 - 1, cy = oy + (ci / 3) % 3 - 1, cz = oz + ci / 9 - 1;  // in [-1, 2]
+    const int pci = ((cx >> 1) + 1) + 3 * ((cy >> 1) + 1) + 9 * ((cz >> 1) + 1);
+    const int pc = coll[(long)P * 27 + pci];
     int r = -1;
-    if (x >= 0 && y >= 0 && z >= 0 && x < kTwo30 && y < kTwo30 && z < kTwo30) {
-      const MKey k = make_key((unsigned int)x, (unsigned int)y, (unsigned int)z, d);
-      const long p = lower_bound_key(keys + base, n_level, k);
-      if (p < n_level && key_eq(keys[base + p], k)) r = (int)(base + p);
+    if (pc >= 0) {
+      const int c0 = child0[pc];
+      if (c0 >= 0) r = c0 + ((cx & 1) | ((cy & 1) << 1) | ((cz & 1) << 2));
     }
-    coll[(base + i) * 27 + ci] = r;
+    coll[v * 27 + ci] = r;
   }
 }
 
@@ -503,10 +516,56 @@ void sort_hilo(Context& ctx, long n, const unsigned long long* hi, const unsigne
   gather_u32<<<ceil_div(n, kThreads), kThreads, 0, s>>>(lo, perm, n, ls);
 }
 
-// Sorts node keys and removes duplicates and sentinels; returns the count.
-long sort_unique(Context& ctx, const MKey* in, long n, DevBuf& out) {
+__global__ void unique_flags_hi(const unsigned long long* __restrict__ hi, long n, int* __restrict__ flag) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flag[i] = (hi[i] != ~0ULL && (i == 0 || hi[i] != hi[i - 1])) ? 1 : 0;
+}
+
+__global__ void compact_keys_hi(const unsigned long long* __restrict__ hi, const int* __restrict__ flag,
+                                const int* __restrict__ offs, long n, unsigned int lo, MKey* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n || !flag[i]) return;
+  MKey k;
+  k.hi = hi[i];
+  k.lo = lo;
+  k.pad = 0;
+  out[offs[i]] = k;
+}
+
+__global__ void key_hi(const MKey* __restrict__ k, long n, unsigned long long* __restrict__ hi) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) hi[i] = k[i].hi;
+}
+
+// Sorts node keys of one depth and removes duplicates and sentinels; returns
+// the count.  A node of depth L <= 21 has zero coordinate bits below 30 - L,
+// so its key is hi (top 3L bits of the 63-bit interleave) with lo = L: one
+// keys-only radix sort over those bits (and bit 63, which only the sentinels
+// set) orders them.  Deeper levels use the full 96-bit sort.
+long sort_unique(Context& ctx, const MKey* in, long n, DevBuf& out, int depth) {
   auto& s = ctx.stream;
   if (n == 0) return 0;
+  if (depth <= 21) {
+    unsigned long long* h = ctx.t[10].as<unsigned long long>(n);
+    unsigned long long* hs = ctx.t[13].as<unsigned long long>(n);
+    ++ctx.n_launch;
+    key_hi<<<ceil_div(n, kThreads), kThreads, 0, s>>>(in, n, h);
+    const int begin_bit = 3 * (21 - depth);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, h, hs, (int)n, begin_bit, 64, s);
+    void* tmp = ctx.scratch.ensure(bytes);
+    cub::DeviceRadixSort::SortKeys(tmp, bytes, h, hs, (int)n, begin_bit, 64, s);
+    int* fl = ctx.t[19].as<int>(n);
+    int* of = ctx.t[20].as<int>(n);
+    ++ctx.n_launch;
+    unique_flags_hi<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, n, fl);
+    const long cnt = exclusive_scan(ctx, fl, of, n);
+    MKey* o = out.as<MKey>(std::max(cnt, 1L));
+    ++ctx.n_launch;
+    compact_keys_hi<<<ceil_div(n, kThreads), kThreads, 0, s>>>(hs, fl, of, n, (unsigned int)depth, o);
+    return cnt;
+  }
   unsigned long long* h = ctx.t[10].as<unsigned long long>(n);
   unsigned int* l = ctx.t[11].as<unsigned int>(n);
   int* ix = ctx.t[12].as<int>(n);
@@ -738,7 +797,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
                                        cudaMemcpyDeviceToDevice, s));
       ++ctx.n_launch;
       nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d, cand + nR[d - 1]);
-      nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1]);
+      nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1], d - 1);
     }
   }
   // 7. final node arrays
@@ -797,7 +856,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   for (int d = 0; d <= D; ++d) {
     const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
     ++ctx.n_launch;
-    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys, base, nl, coll);
+    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0, coll);
   }
   // 9. compact node lists
   {
