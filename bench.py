@@ -6,10 +6,13 @@ full FMM -- of the Laplace potential+gradient kernel on N = 4,000,000 points
 drawn from a mixture of 8 isotropic Gaussians (sigma 0.02, centres uniform in
 [0.1,0.9]^3, clipped to [0,1]^3), sources = targets, densities uniform
 [-1,1], multipole order 8, at most 256 points per leaf.  Both forms run:
-plain FP64 and mixed (FP32 near field / FFT / translations, FP64 pinv).
-Each form's error is the relative L2 error of all 4 outputs against an FP64
-direct sum over all sources on 2,000 sampled targets; ``value`` is the
-targets/s of the fastest form that meets rel-L2 <= 1e-6.
+plain FP64 and mixed (FP32 near field and V-list DFTs, split-TF32 tensor-core
+V-list products, FP64 check->equivalent chain).  Each form's error is the
+relative L2 error of all 4 outputs against an FP64 direct sum over all
+sources on 2,000 sampled targets; ``value`` is the targets/s of the fastest
+form that meets rel-L2 <= 1e-6.  `--workload` selects the other benchmark
+configurations (100k uniform Laplace m=6, 2M Stokes m=10, 30M ellipsoid
+surface m=8); the default is the one above.
 
 Data are synthetic (seeded numpy; no dataset is named by the reference).
 `value` is measured with inputs resident in HBM through the device entry
@@ -41,12 +44,50 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "targets/s Laplace FMM at rel-L2 ≤1e-6 vs FP64 direct: mixed vs plain, 1 B200"
-N_DEFAULT = 4_000_000
-M_ORDER = 8
-MAX_PTS = 256
-N_CHECK = 2000
-KERNEL_ID = 6          # Laplace potential + gradient (4 outputs)
 TOL = 1e-6
+
+# Workloads (the default is the headline one; the others are the remaining
+# benchmark configurations, run with --workload NAME).
+WORKLOADS = {
+    "gaussian4m": dict(kernel=6, m=8, max_pts=256, n=4_000_000, gen="gauss", check_seed=14, n_check=2000,
+                       desc="laplace pot+grad FMM (setup=1 per step), {n} gaussian-mixture points "
+                            "(8 centres, sigma 0.02), m=8, 256/leaf"),
+    "uniform100k": dict(kernel=0, m=6, max_pts=300, n=100_000, gen="uniform", seeds=(1, 2), check_seed=3,
+                        n_check=1000, desc="laplace potential FMM (setup=1 per step), {n} uniform points, m=6, 300/leaf"),
+    "stokes2m": dict(kernel=3, m=10, max_pts=300, n=2_000_000, gen="stokes", seeds=(21, 22), check_seed=23,
+                     n_check=1000, desc="stokes velocity FMM (setup=1 per step), {n} uniform points, N(0,1) forces, "
+                                        "m=10, 300/leaf"),
+    "ellipsoid30m": dict(kernel=0, m=8, max_pts=128, n=30_000_000, gen="ellipsoid", seeds=(41, 42), check_seed=44,
+                         n_check=1000, desc="laplace potential FMM (setup=1 per step), {n} points uniform by area on "
+                                            "the (0.45, 0.3, 0.15) ellipsoid, m=8, 128/leaf"),
+}
+W = WORKLOADS["gaussian4m"]
+KDIM = {0: (1, 1), 3: (3, 3), 6: (1, 4)}          # kernel id -> (k0, k1)
+PAIR_FLOPS = {0: 9, 3: 29, 6: 18}                 # flops per pair (kernel.txx:1277,1317,1352; pot+grad 18)
+
+
+def make_points(w, n):
+    """Seeded synthetic inputs of a workload: positions (n,3), densities (n,k0)."""
+    if w["gen"] == "gauss":
+        return gaussian_mixture(n)
+    s0, s1 = w["seeds"]
+    if w["gen"] == "uniform":
+        return np.random.default_rng(s0).random((n, 3)), np.random.default_rng(s1).uniform(-1, 1, n)
+    if w["gen"] == "stokes":
+        return np.random.default_rng(s0).random((n, 3)), np.random.default_rng(s1).standard_normal((n, 3))
+    if w["gen"] == "ellipsoid":
+        rng = np.random.default_rng(s0)
+        a = np.array([0.45, 0.3, 0.15])
+        out, have = [], 0
+        while have < n:
+            m = int((n - have) * 2.2) + 1000
+            u = rng.standard_normal((m, 3))
+            u /= np.linalg.norm(u, axis=1, keepdims=True)
+            acc = rng.random(m) < np.linalg.norm(u / a, axis=1) * a.min()
+            out.append(0.5 + u[acc] * a)
+            have += int(acc.sum())
+        return np.concatenate(out)[:n], np.random.default_rng(s1).uniform(-1, 1, n)
+    raise ValueError(w["gen"])
 
 
 def gaussian_mixture(n, seed_c=11, seed_p=12, seed_q=13):
@@ -59,21 +100,29 @@ def gaussian_mixture(n, seed_c=11, seed_p=12, seed_q=13):
     return np.ascontiguousarray(x), q
 
 
-def direct_potgrad_gpu(torch, x, q, idx):
-    """FP64 direct sum of [phi, r/r^3 q] / 4 pi at targets x[idx] (GPU, torch)."""
+def direct_gpu(torch, kid, x, q, idx):
+    """FP64 direct sum at targets x[idx] over all points (GPU, torch), r == 0
+    excluded: Laplace potential (0), Stokes velocity (3) or Laplace potential
+    and r q / r^3 (6), with the kernels' 1/(4 pi) or 1/(8 pi)."""
     X = torch.as_tensor(x, device="cuda", dtype=torch.float64)
-    Q = torch.as_tensor(q, device="cuda", dtype=torch.float64)
+    Q = torch.as_tensor(q, device="cuda", dtype=torch.float64).reshape(X.shape[0], -1)
     T = X[torch.as_tensor(idx, device="cuda")]
-    out = torch.zeros((len(idx), 4), device="cuda", dtype=torch.float64)
+    out = torch.zeros((len(idx), KDIM[kid][1]), device="cuda", dtype=torch.float64)
     chunk = 1 << 14
     for a in range(0, X.shape[0], chunk):
         d = T[:, None, :] - X[None, a:a + chunk, :]
         r2 = (d * d).sum(-1)
         rinv = torch.where(r2 > 0, r2.clamp_min(1e-300).rsqrt(), torch.zeros_like(r2))
-        qr = rinv * Q[None, a:a + chunk]
-        out[:, 0] += qr.sum(1)
-        out[:, 1:] += (d * (qr * rinv * rinv)[:, :, None]).sum(1)
-    return (out / (4 * math.pi)).cpu().numpy()
+        qa = Q[a:a + chunk]
+        if kid == 3:
+            ip = torch.einsum("tsk,sk->ts", d, qa) * rinv * rinv
+            out += torch.einsum("ts,sk->tk", rinv, qa) + torch.einsum("ts,tsk->tk", rinv * ip, d)
+        else:
+            qr = rinv * qa[None, :, 0]
+            out[:, 0] += qr.sum(1)
+            if kid == 6:
+                out[:, 1:] += (d * (qr * rinv * rinv)[:, :, None]).sum(1)
+    return (out / (8 * math.pi if kid == 3 else 4 * math.pi)).cpu().numpy()
 
 
 class ClockSampler:
@@ -144,16 +193,16 @@ def run_reference(args, world, rank):
         threadpool_limits = None
     from oracle import pvfmm_oracle as O
     n_sample = args.ref_sample
-    x, q = gaussian_mixture(args.n)
+    x, q = make_points(W, args.n)
     sel = np.random.default_rng(15).choice(args.n, n_sample, replace=False)
     xs, qs = x[sel], q[sel]
     cores = os.cpu_count() or 1
-    ops = O.Operators(O.KERNELS[KERNEL_ID], M_ORDER)     # context creation, not timed
+    ops = O.Operators(O.KERNELS[W["kernel"]], W["m"])     # context creation, not timed
     times = []
     ctxm = threadpool_limits(limits=cores) if threadpool_limits else None
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        O.pvfmm_eval(KERNEL_ID, M_ORDER, MAX_PTS, xs, qs, xs, ops=ops)
+        O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], xs, qs, xs, ops=ops)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             times.append(dt)
@@ -161,13 +210,12 @@ def run_reference(args, world, rank):
         ctxm.unregister() if hasattr(ctxm, "unregister") else None
     ms = 1000 * float(np.mean(times))
     value = n_sample / (ms / 1000)
-    sample = (f"{n_sample} points subsampled (seed 15) from the {args.n}-point Gaussian mixture, "
-              f"Laplace pot+grad, m={M_ORDER}, {MAX_PTS}/leaf, FP64, numpy oracle, setup=1 per step")
+    sample = (f"{n_sample} points subsampled (seed 15) from the workload's {args.n} points "
+              f"({args.workload}), FP64 numpy oracle, setup=1 per step")
     line = {"metric": METRIC, "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"laplace pot+grad FMM, {args.n} gaussian-mixture points, m={M_ORDER}, "
-                                   f"{MAX_PTS}/leaf (bounded CPU sample: {n_sample} points)"},
+            "config": {"workload": W["desc"].format(n=args.n) + f" (bounded CPU sample: {n_sample} points)"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -182,15 +230,15 @@ def cpu_baseline(args):
         lim = threadpool_limits(limits=1)
     except ImportError:  # pragma: no cover
         lim = None
-    x, q = gaussian_mixture(args.n)
+    x, q = make_points(W, args.n)
     sel = np.random.default_rng(15).choice(args.n, args.ref_sample, replace=False)
-    ops = O.Operators(O.KERNELS[KERNEL_ID], M_ORDER)
+    ops = O.Operators(O.KERNELS[W["kernel"]], W["m"])
     t0 = time.perf_counter()
-    O.pvfmm_eval(KERNEL_ID, M_ORDER, MAX_PTS, x[sel], q[sel], x[sel], ops=ops)
+    O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], x[sel], q[sel], x[sel], ops=ops)
     dt = time.perf_counter() - t0
     del lim
     return {"value": args.ref_sample / dt, "unit": "targets/s", "cores": 1, "kind": "port",
-            "sample": f"{args.ref_sample} points subsampled (seed 15) from the same mixture, FP64 numpy oracle, "
+            "sample": f"{args.ref_sample} points subsampled (seed 15) from the same workload, FP64 numpy oracle, "
                       f"one thread, setup=1, {dt:.1f} s"}
 
 
@@ -228,15 +276,18 @@ def roofline(B, peaks):
     smax = (B["clocks"] or {}).get("sm_max_mhz") or 1965.0
     lanes = 128 if rb == 4 else 64
     simt_peak = 148 * lanes * 2 * smax * 1e6 / 1e12
-    n3h = (2 * M_ORDER) ** 2 * (M_ORDER + 1)
-    ns = 6 * (M_ORDER - 1) ** 2 + 2
+    m, kid = W["m"], W["kernel"]
+    ke = 3 if kid == 3 else 1
+    k0, k1 = KDIM[kid]
+    n3h = (2 * m) ** 2 * (m + 1)
+    ns = 6 * (m - 1) ** 2 + 2
     out = {}
     had_ms = B["stages_ms"]["V-Hadamard"]
-    had_bytes = (st["n_vsrc"] + st["n_vtrg"]) * n3h * 8 * 2 * rb + 26 * n3h * 64 * 2 * rb
-    had_flops = 512.0 * n3h * st["v_pairs"]
+    had_bytes = (st["n_vsrc"] + st["n_vtrg"]) * n3h * 8 * ke * 2 * rb + 26 * n3h * 64 * ke * ke * 2 * rb
+    had_flops = 512.0 * ke * ke * n3h * st["v_pairs"]
     near_ms = B["stages_ms"]["near-field kernel"]
-    near_bytes = st["n_src"] * 32 + st["n_trg"] * 56 + st["n_tleaf"] * ns * 8
-    near_flops = 18.0 * (st["p2p_pairs"] + st["w_pairs"] + st["d2t_pairs"])
+    near_bytes = st["n_src"] * (24 + 8 * k0) + st["n_trg"] * (24 + 8 * k1) + st["n_tleaf"] * ns * ke * 8
+    near_flops = float(PAIR_FLOPS[kid]) * (st["p2p_pairs"] + st["w_pairs"] + st["d2t_pairs"])
     for name, ms, byts, flops, tkey, units in (
             ("hadamard_rd_kernel (V-list M2L)", had_ms, had_bytes, had_flops, "hadamard", st["n_vsrc"] + st["n_vtrg"]),
             ("near_field_kernel (U-list P2P + W + D2T)", near_ms, near_bytes, near_flops, "near_field", st["n_trg"])):
@@ -260,11 +311,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--workload", default="gaussian4m", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=None, help="point count (default: the workload's)")
     ap.add_argument("--ref-sample", type=int, default=12000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain,mixed")
     args = ap.parse_args()
+    global W
+    W = WORKLOADS[args.workload]
+    if args.n is None:
+        args.n = W["n"]
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -290,17 +346,20 @@ def main():
         return float(t.item())
 
     N = args.n
-    x, q = gaussian_mixture(N)
-    idx = np.random.default_rng(14).choice(N, N_CHECK, replace=False)
-    ref = direct_potgrad_gpu(torch, x, q, idx)
+    kid = W["kernel"]
+    k0, k1 = KDIM[kid]
+    x, q = make_points(W, N)
+    q = np.ascontiguousarray(q.reshape(-1))
+    idx = np.random.default_rng(W["check_seed"]).choice(N, W["n_check"], replace=False)
+    ref = direct_gpu(torch, kid, x, q, idx)
     d_x = torch.as_tensor(x, device="cuda")
     d_q = torch.as_tensor(q, device="cuda")
-    d_out = torch.empty((N, 4), device="cuda", dtype=torch.float64)
+    d_out = torch.empty((N, k1), device="cuda", dtype=torch.float64)
     stream = torch.cuda.current_stream()
     forms = {}
     for form in args.forms.split(","):
         prec = P.PRECISION_PLAIN if form == "plain" else P.PRECISION_MIXED
-        ctx = P.FMMParticleContext(-1, MAX_PTS, M_ORDER, P.FMMKernel.LaplacePotGrad, precision=prec)
+        ctx = P.FMMParticleContext(-1, W["max_pts"], W["m"], P.FMMKernel(kid), precision=prec)
 
         def step():
             ctx.evaluate_device(d_x.data_ptr(), d_q.data_ptr(), N, d_x.data_ptr(), d_out.data_ptr(), N, True,
@@ -311,7 +370,7 @@ def main():
         torch.cuda.synchronize()
         out = d_out.cpu().numpy()[idx]
         err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
-        err_comp = [float(np.linalg.norm(out[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])) for k in range(4)]
+        err_comp = [float(np.linalg.norm(out[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])) for k in range(k1)]
         stats = ctx.tree_stats()
         l0 = ctx.launch_count()
         clocks = ClockSampler(local)
@@ -336,7 +395,7 @@ def main():
         lib = P.load_library()
         h_x = torch.from_numpy(x.reshape(-1)).pin_memory()
         h_q = torch.from_numpy(q).pin_memory()
-        h_out = torch.empty(N * 4, dtype=torch.float64).pin_memory()
+        h_out = torch.empty(N * k1, dtype=torch.float64).pin_memory()
         f = lib.PVFMMEvalD
         for _ in range(2):
             f(ctypes.c_void_p(h_x.data_ptr()), ctypes.c_void_p(h_q.data_ptr()), None, N, ctypes.c_void_p(h_x.data_ptr()),
@@ -379,8 +438,7 @@ def main():
         "vs_baseline": None,
         "dtype": "f64" if best == "plain" else "f32",
         "data": "synthetic",
-        "config": {"workload": f"laplace pot+grad FMM (setup=1 per step), {N} gaussian-mixture points "
-                               f"(8 centres, sigma 0.02), m={M_ORDER}, {MAX_PTS}/leaf, form={best}",
+        "config": {"workload": W["desc"].format(n=N) + f", form={best}",
                    "l2": "no flush: per-step working set (128 MB inputs + tree + GB-size spectra) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
         "form": best,
@@ -388,7 +446,7 @@ def main():
         "mixed_over_plain": (forms["mixed"]["targets_per_s"] / forms["plain"]["targets_per_s"]
                              if "mixed" in forms and "plain" in forms else None),
         "e2e": {"value": B["e2e_targets_per_s"], "unit": "targets/s",
-                "h2d_bytes_per_step": N * 3 * 8 + N * 8, "d2h_bytes_per_step": N * 4 * 8},
+                "h2d_bytes_per_step": N * 3 * 8 + N * k0 * 8, "d2h_bytes_per_step": N * k1 * 8},
         "gpu_launches": B["gpu_launches"],
         "clocks": B["clocks"],
         "roofline": roof[0],

@@ -38,7 +38,7 @@ void destroy_context(Context& c) {
   cudaSetDevice(c.device);
   if (c.stream) cudaStreamSynchronize(c.stream);
   DevBuf* bufs[] = {&c.dops.uc2ue0, &c.dops.uc2ue1, &c.dops.dc2de0, &c.dops.dc2de1, &c.dops.u2u, &c.dops.d2d,
-                    &c.dops.vop, &c.dops.vop_frag, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den, &c.pot, &c.ue, &c.dc,
+                    &c.dops.vop, &c.dops.vop_frag, &c.dops.ue_proj, &c.ue_c, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den, &c.pot, &c.ue, &c.dc,
                     &c.uc_c, &c.tmp_c, &c.de_c, &c.spec_in, &c.spec_out, &c.scratch, &c.scratch2, &c.io_src,
                     &c.io_trg, &c.io_den, &c.io_val, &c.stat};
   for (DevBuf* b : bufs) b->release();
@@ -76,7 +76,13 @@ void* create_context(double box_size, int n, int m, int kernel, int precision, b
     c.float_api = float_api;
     // Both forms use the FP64-cutoff operators: the mixed form keeps the
     // check->equivalent chain in FP64 (see eval.cu).
-    build_operators(kernel, m, false, c.hops);
+    // Mixed form of the Stokes kernel: FP32 cutoff in the downward
+    // check -> equivalent factors.  The downward pseudo-inverse amplifies the
+    // FP32 rounding of the V-list output for targets outside the downward
+    // check surface (leaf corners); with the FP64 cutoff the 2M-point m=10
+    // Stokes error was 2.8e-5, with the FP32 cutoff 3.7e-7.  The Laplace
+    // kernels keep the FP64 cutoff (the FP32 one raised their error).
+    build_operators(kernel, m, false, c.hops, precision == 1 && ki.ke == 3);
     PVFMM_CUDA_CHECK(cudaGetDevice(&c.device));
     PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     if (cublasCreate(&c.cublas) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasCreate failed");

@@ -53,6 +53,7 @@ struct DevTree {
 struct DevOps {
   DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
   DevBuf vop_frag;  // mixed form, ke = 1: Hadamard operators as TF32 hi/lo MMA fragments
+  DevBuf ue_proj;   // mixed form: projector applied to the upward equivalent densities
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
 };
@@ -72,6 +73,7 @@ struct Context {
   int device = 0;
   // evaluation buffers
   DevBuf den;             // sorted densities (Real, n_src x k0)
+  DevBuf ue_c;            // mixed form: projected upward equivalent densities
   DevBuf pot;             // sorted target values (Real, n_trg x k1)
   DevBuf ue, dc;          // per node (Real)
   DevBuf uc_c, tmp_c, de_c;  // compact GEMM buffers

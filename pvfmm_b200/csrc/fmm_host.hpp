@@ -36,6 +36,11 @@ struct HostOperators {
   bool mixed = false;
   std::vector<double> usurf;            // ns x 3 unit cube-surface points u in [-1,1]^3
   std::vector<double> uc2ue0, uc2ue1;   // (ns*ke) x (ns*ke): check -> equivalent factors
+  // (ns*ke) x (ns*ke): orthogonal projector onto the upward equivalent
+  // directions whose singular value (equivalent -> check) is above the FP32
+  // cutoff 4*eps32*max; the mixed form applies it to the upward equivalent
+  // densities before its FP32 stages
+  std::vector<double> ue_proj;
   std::vector<double> dc2de0, dc2de1;
   std::vector<double> u2u;              // (8*ns*ke) x (ns*ke), row block c = child octant c
   std::vector<double> d2d;              // (ns*ke) x (8*ns*ke), column block c = child octant c
@@ -46,7 +51,9 @@ struct HostOperators {
 // Builds the operators.  `mixed` selects the pseudo-inverse cutoff of the
 // mixed form: singular values below 4*eps32*max are dropped (the cutoff the
 // reference's float build uses), otherwise 4*eps64*max (fmm_pts.txx:496-504).
-void build_operators(int kernel, int m, bool mixed, HostOperators& ops);
+// down_eps32: FP32 cutoff for the downward check -> equivalent factors only
+// (and so for D2D), the mixed form's downward chain.
+void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool down_eps32 = false);
 
 // One-sided Jacobi SVD of a rows x cols row-major matrix (rows >= cols):
 // A = U diag(S) V^T with U rows x cols (column j scaled to unit length, or

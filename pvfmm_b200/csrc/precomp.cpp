@@ -228,7 +228,7 @@ void jacobi_svd(int rows, int cols, const double* A, std::vector<double>& U, std
   }
 }
 
-void build_operators(int kernel, int m, bool mixed, HostOperators& ops) {
+void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool down_eps32) {
   KernelInfo ki;
   if (!kernel_info(kernel, &ki)) throw std::runtime_error("unsupported kernel");
   if (m < 2 || m > 16 || (m & 1)) throw std::runtime_error("multipole order must be even and in [2,16]");
@@ -254,6 +254,24 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops) {
     std::vector<double> M((size_t)dim * dim);
     exp_kernel_matrix(ki.exp_kernel, ue.data(), ns, uc.data(), ns, M.data());
     pinv_factors(M, dim, dim, eps, ops.uc2ue0, ops.uc2ue1);
+    // ue = (uc V S+) U^T lies in the span of U's columns; its components
+    // along singular values below 4*eps32*max are amplified FP64 rounding
+    // of the check potentials, cancelling in exact arithmetic but not in
+    // FP32.  P = U_k U_k^T over the columns above that cutoff.
+    std::vector<double> U, S, V;
+    jacobi_svd(dim, dim, M.data(), U, S, V);
+    double smax = 0;
+    for (double v : S) smax = std::max(smax, std::fabs(v));
+    const double cut32 = 4.0 * std::ldexp(1.0, -23) * smax;
+    ops.ue_proj.assign((size_t)dim * dim, 0.0);
+    for (int j = 0; j < dim; ++j) {
+      if (!(S[j] > cut32)) continue;
+      for (int a = 0; a < dim; ++a) {
+        const double ua = U[(size_t)a * dim + j];
+        double* row = &ops.ue_proj[(size_t)a * dim];
+        for (int b = 0; b < dim; ++b) row[b] += ua * U[(size_t)b * dim + j];
+      }
+    }
   }
   // DC2DE0/1: downward equivalent (RAD1) -> downward check (RAD0) (:538-581)
   {
@@ -261,7 +279,7 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops) {
     auto dc = place_surface(ops.usurf, zero, 0.5, kRad0);
     std::vector<double> M((size_t)dim * dim);
     exp_kernel_matrix(ki.exp_kernel, de.data(), ns, dc.data(), ns, M.data());
-    pinv_factors(M, dim, dim, eps, ops.dc2de0, ops.dc2de1);
+    pinv_factors(M, dim, dim, down_eps32 ? std::ldexp(1.0, -23) : eps, ops.dc2de0, ops.dc2de1);
   }
   // U2U (:582-606): (M_ce2c * UC2UE0) * UC2UE1, child c of a level-0 parent.
   ops.u2u.assign((size_t)8 * dim * dim, 0.0);

@@ -103,15 +103,24 @@ def test_plain_matches_oracle(name, kid, m, n, mp, dist, sep):
     assert ctx.launch_count() > 0
 
 
-@pytest.mark.parametrize("kid,m", [(0, 6), (3, 6), (6, 8)])
+@pytest.mark.parametrize("kid,m", [(0, 6), (3, 6), (3, 8), (6, 8)])
 def test_mixed_matches_oracle(kid, m):
+    """Laplace kernels: the mixed form matches the oracle (FP64-cutoff
+    operators) to MIXED_TOL.  Stokes: the mixed form uses the FP32 cutoff in
+    the downward pseudo-inverse and projects the upward equivalent densities,
+    so it is a different approximation; it must be as accurate as the plain
+    FMM against the direct sum."""
     K = O.KERNELS[kid]
     src = points("unif", 3000, 4)
     den = np.random.default_rng(5).uniform(-1, 1, (3000, K.k0))
     out, ctx = gpu_eval(kid, m, 50, src, den, src, prec=P.PRECISION_MIXED)
     ref, fmm = O.pvfmm_eval(kid, m, 50, src, den, src, ops=oracle_ops(kid, m), return_fmm=True)
     tree_matches(ctx, fmm)
-    assert O.rel_l2(out, ref) < MIXED_TOL
+    if kid == 3:
+        direct = O.direct_sum(kid, src, den, src)
+        assert O.rel_l2(out, direct) < 1.5 * O.rel_l2(ref, direct) + 1e-6
+    else:
+        assert O.rel_l2(out, ref) < MIXED_TOL
 
 
 def test_float_api_matches_oracle():
