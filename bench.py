@@ -352,71 +352,85 @@ def main():
     q = np.ascontiguousarray(q.reshape(-1))
     idx = np.random.default_rng(W["check_seed"]).choice(N, W["n_check"], replace=False)
     ref = direct_gpu(torch, kid, x, q, idx)
+    torch.cuda.empty_cache()  # the direct sum's temporaries go back to the device
     d_x = torch.as_tensor(x, device="cuda")
     d_q = torch.as_tensor(q, device="cuda")
     d_out = torch.empty((N, k1), device="cuda", dtype=torch.float64)
     stream = torch.cuda.current_stream()
-    forms = {}
-    for form in args.forms.split(","):
+
+    def run_form(form):
         prec = P.PRECISION_PLAIN if form == "plain" else P.PRECISION_MIXED
         ctx = P.FMMParticleContext(-1, W["max_pts"], W["m"], P.FMMKernel(kid), precision=prec)
+        try:
+            def step():
+                ctx.evaluate_device(d_x.data_ptr(), d_q.data_ptr(), N, d_x.data_ptr(), d_out.data_ptr(), N, True,
+                                    stream.cuda_stream)
 
-        def step():
-            ctx.evaluate_device(d_x.data_ptr(), d_q.data_ptr(), N, d_x.data_ptr(), d_out.data_ptr(), N, True,
-                                stream.cuda_stream)
+            for _ in range(args.warmup):
+                step()
+            torch.cuda.synchronize()
+            out = d_out.cpu().numpy()[idx]
+            err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
+            err_comp = [float(np.linalg.norm(out[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])) for k in range(k1)]
+            stats = ctx.tree_stats()
+            l0 = ctx.launch_count()
+            clocks = ClockSampler(local)
+            barrier()
+            torch.cuda.synchronize()
+            clocks.start()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            stage_sum = None
+            for _ in range(args.steps):
+                step()
+                st = ctx.stage_times()
+                stage_sum = st if stage_sum is None else {k: stage_sum[k] + st[k] for k in st}
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            cl = clocks.stop()
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            launches = (ctx.launch_count() - l0) / args.steps
+            stage = {k: v / args.steps for k, v in stage_sum.items()}
+            # e2e: public C ABI on pinned host buffers, copies inside the timed region
+            lib = P.load_library()
+            h_x = torch.from_numpy(x.reshape(-1)).pin_memory()
+            h_q = torch.from_numpy(q).pin_memory()
+            h_out = torch.empty(N * k1, dtype=torch.float64).pin_memory()
+            f = lib.PVFMMEvalD
+            for _ in range(2):
+                f(ctypes.c_void_p(h_x.data_ptr()), ctypes.c_void_p(h_q.data_ptr()), None, N, ctypes.c_void_p(h_x.data_ptr()),
+                  ctypes.c_void_p(h_out.data_ptr()), N, ctypes.c_void_p(ctx._ptr), 1)
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                f(ctypes.c_void_p(h_x.data_ptr()), ctypes.c_void_p(h_q.data_ptr()), None, N, ctypes.c_void_p(h_x.data_ptr()),
+                  ctypes.c_void_p(h_out.data_ptr()), N, ctypes.c_void_p(ctx._ptr), 1)
+            e2e_ms = max_over_ranks(1000 * (time.perf_counter() - t0) / args.steps)
+            if P.last_error():
+                raise RuntimeError(P.last_error())
+            res = {"ms_per_step": ms, "targets_per_s": world * N / (ms / 1000), "rel_l2": err,
+                   "rel_l2_components": err_comp, "stages_ms": stage, "stats": stats, "gpu_launches": launches,
+                   "clocks": cl, "e2e_ms": e2e_ms, "e2e_targets_per_s": world * N / (e2e_ms / 1000),
+                   "real_bytes": 8 if form == "plain" else 4}
+            return res
+        finally:
+            ctx.close()
 
-        for _ in range(args.warmup):
-            step()
-        torch.cuda.synchronize()
-        out = d_out.cpu().numpy()[idx]
-        err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
-        err_comp = [float(np.linalg.norm(out[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])) for k in range(k1)]
-        stats = ctx.tree_stats()
-        l0 = ctx.launch_count()
-        clocks = ClockSampler(local)
-        barrier()
-        torch.cuda.synchronize()
-        clocks.start()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        stage_sum = None
-        for _ in range(args.steps):
-            step()
-            st = ctx.stage_times()
-            stage_sum = st if stage_sum is None else {k: stage_sum[k] + st[k] for k in st}
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        cl = clocks.stop()
-        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-        launches = (ctx.launch_count() - l0) / args.steps
-        stage = {k: v / args.steps for k, v in stage_sum.items()}
-        # e2e: public C ABI on pinned host buffers, copies inside the timed region
-        lib = P.load_library()
-        h_x = torch.from_numpy(x.reshape(-1)).pin_memory()
-        h_q = torch.from_numpy(q).pin_memory()
-        h_out = torch.empty(N * k1, dtype=torch.float64).pin_memory()
-        f = lib.PVFMMEvalD
-        for _ in range(2):
-            f(ctypes.c_void_p(h_x.data_ptr()), ctypes.c_void_p(h_q.data_ptr()), None, N, ctypes.c_void_p(h_x.data_ptr()),
-              ctypes.c_void_p(h_out.data_ptr()), N, ctypes.c_void_p(ctx._ptr), 1)
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            f(ctypes.c_void_p(h_x.data_ptr()), ctypes.c_void_p(h_q.data_ptr()), None, N, ctypes.c_void_p(h_x.data_ptr()),
-              ctypes.c_void_p(h_out.data_ptr()), N, ctypes.c_void_p(ctx._ptr), 1)
-        e2e_ms = max_over_ranks(1000 * (time.perf_counter() - t0) / args.steps)
-        if P.last_error():
-            raise RuntimeError(P.last_error())
-        forms[form] = {"ms_per_step": ms, "targets_per_s": world * N / (ms / 1000), "rel_l2": err,
-                       "rel_l2_components": err_comp, "stages_ms": stage, "stats": stats, "gpu_launches": launches,
-                       "clocks": cl, "e2e_ms": e2e_ms, "e2e_targets_per_s": world * N / (e2e_ms / 1000),
-                       "real_bytes": 8 if form == "plain" else 4}
-        ctx.close()
+    forms = {}
+    for form in args.forms.split(","):
+        try:
+            forms[form] = run_form(form)
+        except RuntimeError as e:  # e.g. a workload too large for one GPU in this form
+            forms[form] = {"error": str(e)}
+    forms_ok = {f: d for f, d in forms.items() if "error" not in d}
+    if not forms_ok:
+        raise RuntimeError(f"no form completed: {forms}")
 
-    ok = [f for f in forms if forms[f]["rel_l2"] <= TOL]
-    best = max(ok, key=lambda f: forms[f]["targets_per_s"]) if ok else "plain"
+
+    ok = [f for f in forms_ok if forms_ok[f]["rel_l2"] <= TOL]
+    best = max(ok, key=lambda f: forms_ok[f]["targets_per_s"]) if ok else next(iter(forms_ok))
     B = forms[best]
     peaks = {}
     try:
@@ -443,8 +457,8 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "form": best,
         "forms": forms,
-        "mixed_over_plain": (forms["mixed"]["targets_per_s"] / forms["plain"]["targets_per_s"]
-                             if "mixed" in forms and "plain" in forms else None),
+        "mixed_over_plain": (forms_ok["mixed"]["targets_per_s"] / forms_ok["plain"]["targets_per_s"]
+                             if "mixed" in forms_ok and "plain" in forms_ok else None),
         "e2e": {"value": B["e2e_targets_per_s"], "unit": "targets/s",
                 "h2d_bytes_per_step": N * 3 * 8 + N * k0 * 8, "d2h_bytes_per_step": N * k1 * 8},
         "gpu_launches": B["gpu_launches"],

@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 
@@ -868,7 +869,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // a thread only reads the rows it copied itself, so waiting on its own copy
 // group is enough.  Missing neighbours are zero-filled and skipped.
 template <class Real, int KE, int PB, int OC>
-__global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, const int* __restrict__ vtab,
+__global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, long vt_stride, const int* __restrict__ vtab,
                                                        const Cplx<Real>* __restrict__ spec_in,
                                                        const Cplx<Real>* __restrict__ vop,
                                                        Cplx<Real>* __restrict__ spec_out) {
@@ -891,7 +892,7 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, con
 #pragma unroll
     for (int k = 0; k < PB; ++k) {
       const long p = base + (long)k * NT;
-      q[k] = (o < 26 && p < n_vtrg) ? __ldg(vtab + (long)o * n_vtrg + p) : -1;
+      q[k] = (o < 26 && p < n_vtrg) ? __ldg(vtab + (long)o * vt_stride + p) : -1;
       const Cplx<Real>* src = spec_in + ((long)(q[k] < 0 ? 0 : q[k]) * n3h + f) * NG;
       Cplx<Real>* dst = xb + ((long)buf * NT * PB + threadIdx.x + k * NT) * STRIDE;
 #pragma unroll
@@ -961,7 +962,8 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, con
 // parents of a warp are mostly adjacent, so each 16-byte gather of a warp
 // coalesces.  Offsets that none of the thread's parents has are skipped.
 template <class Real, int PB>
-__global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtrg, long n_vsrc, const int* __restrict__ vtab,
+__global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc,
+                                                             const int* __restrict__ vtab,
                                                           const Cplx<Real>* __restrict__ spec_in,
                                                           const Cplx<Real>* __restrict__ vop,
                                                           Cplx<Real>* __restrict__ spec_out) {
@@ -995,7 +997,7 @@ __global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtr
     mask = 0;
 #pragma unroll
     for (int k = 0; k < PB; ++k) {
-      const int q = pin[k] ? __ldg(vtab + (long)o * n_vtrg + prow[k]) : -1;
+      const int q = pin[k] ? __ldg(vtab + (long)o * vt_stride + prow[k]) : -1;
       if (q >= 0) {
         mask |= 1u << k;
         const V* r = reinterpret_cast<const V*>(spec_in) + (long)f * NV * n_vsrc + q;
@@ -1071,10 +1073,10 @@ __global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtr
 // ---------------------------------------------------------------------------
 // Hadamard products of the mixed form (ke = 1) on the tensor cores:
 // mma.sync m16n8k8 TF32 with FP32 accumulation, each product split into
-// three (a_hi b_hi + a_hi b_lo + a_lo b_hi, hi = the TF32 head of an FP32
-// value, lo = the exact FP32 remainder), which carries the products to within
-// ~2^-20 of FP32 (an emulation of the whole FMM with this split changes the
-// result by ~1e-8 relative).
+// three (a_hi b_hi + a_hi b_lo + a_lo b_hi, hi = the value rounded to TF32,
+// lo = the remainder rounded to TF32), which carries the products to ~2^-22
+// relative (an emulation of the whole FMM with this split changes the result
+// by ~1e-8 relative).
 //
 // Per frequency f the product is a real GEMM over parent rows:
 //   OUT[P][(j1, re|im)] += sum_o sum_(j2, re|im) IN[Q_o(P)][(j2, re|im)] * B_o[(j2, re|im)][(j1, re|im)]
@@ -1094,12 +1096,17 @@ __device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const unsigned (&
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// hi = the value with its low 13 mantissa bits cleared (a TF32 number);
-// lo = x - hi, exact in FP32.
+// hi = x rounded to TF32 (cvt.rna), lo = (x - hi) rounded to TF32: hi + lo
+// carries x to ~2^-23 relative.  (Passing unrounded FP32 values leaves the
+// conversion to the MMA's truncation, up to 2^-20 relative per product,
+// which showed as ~1e-6 in the FMM result.)
 __device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
-  const unsigned h = __float_as_uint(x) & 0xffffe000u;
+  unsigned h, l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  const float r = x - __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
   hi = h;
-  lo = __float_as_uint(x - __uint_as_float(h));
+  lo = l;
 }
 
 constexpr int kTcWarps = 8;  // warps per block of the tensor-core Hadamard
@@ -1108,7 +1115,7 @@ constexpr int kTcWarps = 8;  // warps per block of the tensor-core Hadamard
 #endif
 
 template <int MT>
-__global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_tc_kernel(int n3h, long n_vtrg, long n_vsrc,
+__global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_tc_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc,
                                                                        const int* __restrict__ vtab,
                                                                        const float4* __restrict__ spec_in,
                                                                        const float4* __restrict__ bfrag,
@@ -1126,7 +1133,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
     for (int i = threadIdx.x; i < 26 * NP; i += 32 * kTcWarps) {
       const int o = i / NP;
       const long p = pb + i % NP;
-      qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * n_vtrg + p) : -1;
+      qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
     }
   }
   __syncthreads();
@@ -1208,24 +1215,25 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
     }
 }
 
-void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout) {
+// Target parents [p0, p0 + np) of the V-list; sout holds their rows.
+void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout, long p0, long np) {
   DevTree& T = ctx.tree;
   constexpr int MT = 2;
   const size_t sm = (size_t)26 * 32 * 2 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dim3 grid(ceil_div(T.n_vtrg, 16 * MT * kTcWarps), n3h);
+  dim3 grid(ceil_div(np, 16 * MT * kTcWarps), n3h);
   ++ctx.n_launch;
   hadamard_tc_kernel<MT><<<grid, 32 * kTcWarps, sm, ctx.stream>>>(
-      n3h, T.n_vtrg, T.n_vsrc, T.vtab.get<int>(), reinterpret_cast<const float4*>(sin_),
+      n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0, reinterpret_cast<const float4*>(sin_),
       ctx.dops.vop_frag.get<float4>(), reinterpret_cast<float2*>(sout));
 }
 
 template <class Real, int PB>
-void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout) {
+void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0, long np) {
   DevTree& T = ctx.tree;
-  dim3 grid(ceil_div(T.n_vtrg, 128 * PB), n3h);
+  dim3 grid(ceil_div(np, 128 * PB), n3h);
   ++ctx.n_launch;
-  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, T.n_vtrg, T.n_vsrc, T.vtab.get<int>(), sin_,
+  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0, sin_,
                                                              ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
@@ -1242,14 +1250,14 @@ size_t hadamard_smem() {
 }
 
 template <class Real, int KE, int PB, int OC>
-void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout) {
+void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0, long np) {
   DevTree& T = ctx.tree;
   const size_t sm = hadamard_smem<Real, KE, PB, OC>();
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_kernel<Real, KE, PB, OC>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dim3 grid(ceil_div(T.n_vtrg, 128 * PB), n3h);
+  dim3 grid(ceil_div(np, 128 * PB), n3h);
   ++ctx.n_launch;
-  hadamard_kernel<Real, KE, PB, OC><<<grid, 128, sm, ctx.stream>>>(n3h, T.n_vtrg, T.vtab.get<int>(), sin_,
+  hadamard_kernel<Real, KE, PB, OC><<<grid, 128, sm, ctx.stream>>>(n3h, np, T.n_vtrg, T.vtab.get<int>() + p0, sin_,
                                                                    ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
@@ -1320,8 +1328,13 @@ int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
   return best;
 }
 
+// V-list: forward DFTs of every source parent, then the Hadamard products
+// and inverse DFTs of the target parents in chunks of `chunk` parents (the
+// output spectra of one chunk at a time; one chunk when device memory
+// allows).  With several chunks, stage 4 ends after the first chunk's
+// products and stage 5 covers the rest.
 template <class Real, int M>
-void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int ke,
+void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int ke, long chunk,
                  const std::function<void(int)>& ev) {
   DevTree& T = ctx.tree;
   auto s = ctx.stream;
@@ -1337,21 +1350,24 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
                                                                      sin_);
   ev(4);
   const int n3h = F::N3H;
-  if (ke == 1) {
-    if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout);
-    else launch_hadamard_tc(ctx, n3h, sin_, sout);
-  } else {
-    launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout);
-  }
-  ev(5);
   const int Gd = grids_per_block<F>(F::dn_grid_bytes, F::tw_bytes, ngrid, 80 * 1024);
   const size_t sm_dn = F::tw_bytes + Gd * F::dn_grid_bytes;
   PVFMM_CUDA_CHECK(
       cudaFuncSetAttribute(ifft_dn_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
-  ++ctx.n_launch;
-  ifft_dn_kernel<Real, M><<<T.n_vtrg * (ngrid / Gd), F::threads(Gd), sm_dn, s>>>(ke, Gd, ngrid / Gd, T.vtrg.get<int>(),
-                                                                      T.child0.get<int>(), T.key.get<MKey>(), sout,
-                                                                      ctx.dops.ifft_map.get<int>(), ctx.ns, dc);
+  for (long p0 = 0; p0 < T.n_vtrg; p0 += chunk) {
+    const long np = std::min(chunk, T.n_vtrg - p0);
+    if (ke == 1) {
+      if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout, p0, np);
+      else launch_hadamard_tc(ctx, n3h, sin_, sout, p0, np);
+    } else {
+      launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout, p0, np);
+    }
+    if (p0 == 0) ev(5);
+    ++ctx.n_launch;
+    ifft_dn_kernel<Real, M><<<np * (ngrid / Gd), F::threads(Gd), sm_dn, s>>>(
+        ke, Gd, ngrid / Gd, T.vtrg.get<int>() + p0, T.child0.get<int>(), T.key.get<MKey>(), sout,
+        ctx.dops.ifft_map.get<int>(), ctx.ns, dc);
+  }
 }
 
 template <class Real>
@@ -1359,16 +1375,30 @@ void vlist(Context& ctx, const double* ue, double* dc, int ke, const std::functi
   DevTree& T = ctx.tree;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);
   Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * 8 * ke);
-  Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)T.n_vtrg * n3h * 8 * ke);
+  // output spectra: all target parents at once when they fit in 90% of the
+  // free device memory (counting this buffer's current allocation), else
+  // chunks of that size
+  const size_t row = (size_t)n3h * 8 * ke * sizeof(Cplx<Real>);
+  size_t free_b = 0, total_b = 0;
+  PVFMM_CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+  const double avail = 0.9 * (double)(free_b + ctx.spec_out.cap);
+  long chunk = T.n_vtrg;
+  if ((double)T.n_vtrg * row > avail) chunk = std::max(256L, (long)(avail / row));
+  // PVFMM_B200_VLIST_CHUNK caps the chunk (to exercise the chunked path)
+  if (const char* e = std::getenv("PVFMM_B200_VLIST_CHUNK")) {
+    const long c = std::atol(e);
+    if (c > 0) chunk = std::min(chunk, c);
+  }
+  Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * ke);
   switch (m) {
-    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, ke, ev); break;
-    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, ke, ev); break;
+    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
     default: throw std::runtime_error("unsupported multipole order");
   }
 }
@@ -1518,7 +1548,7 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
 // is B[(j2,re)][(j1,re)] = Re M, B[(j2,im)][(j1,re)] = -Im M,
 // B[(j2,re)][(j1,im)] = Im M, B[(j2,im)][(j1,im)] = Re M.  Each value is
 // stored in FP32 as (b0, b1) for the blocks (s, nt) = (0,0), (0,1), (1,0),
-// (1,1); the kernel splits them into TF32 head and remainder.
+// (1,1); the kernel splits them into rounded TF32 head and remainder.
 static void upload_vop_fragments(Context& ctx) {
   const HostOperators& h = ctx.hops;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);

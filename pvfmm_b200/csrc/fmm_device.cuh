@@ -202,7 +202,15 @@ struct DevBuf {
       if (ptr) PVFMM_CUDA_CHECK(cudaFree(ptr));
       ptr = nullptr;
       cap = 0;
-      PVFMM_CUDA_CHECK(cudaMalloc(&ptr, bytes));
+      const cudaError_t e = cudaMalloc(&ptr, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        throw std::runtime_error("device allocation of " + std::to_string(bytes >> 20) + " MiB failed (" +
+                                 cudaGetErrorString(e) + "; " + std::to_string(fr >> 20) + " MiB free of " +
+                                 std::to_string(tot >> 20) + ")");
+      }
       cap = bytes;
     }
     return ptr;

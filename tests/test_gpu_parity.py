@@ -284,3 +284,19 @@ def test_kernel_eval_device_matches_direct_sum(kid):
     P.kernel_eval_device(P.FMMKernel(kid), ds.data_ptr(), dd.data_ptr(), 3000, dt.data_ptr(), out.data_ptr(), len(trg))
     torch.cuda.synchronize()
     np.testing.assert_allclose(out.cpu().numpy() - 0.5, ref, rtol=1e-11, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("prec", [P.PRECISION_PLAIN, P.PRECISION_MIXED])
+def test_vlist_chunks_give_identical_results(monkeypatch, prec):
+    """The V-list runs its target parents in chunks when the output spectra
+    do not fit in device memory; every parent's products are independent of
+    the chunking, so the results are bit-identical."""
+    src = points("gauss", 20000, 31)
+    den = np.random.default_rng(32).uniform(-1, 1, 20000)
+    whole, ctx = gpu_eval(6, 6, 40, src, den, src, prec=prec)
+    ctx.close()
+    monkeypatch.setenv("PVFMM_B200_VLIST_CHUNK", "100")
+    chunked, ctx = gpu_eval(6, 6, 40, src, den, src, prec=prec)
+    assert ctx.tree_stats()["n_vtrg"] > 300
+    ctx.close()
+    assert np.array_equal(whole, chunked)
