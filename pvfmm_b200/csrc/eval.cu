@@ -1120,16 +1120,16 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
                                                                        const float4* __restrict__ spec_in,
                                                                        const float4* __restrict__ bfrag,
                                                                        float2* __restrict__ spec_out) {
-  extern __shared__ float4 Bs[];  // [26 offsets][32 lanes][2]: (b0, b1) of the 4 (s, nt) blocks
+  extern __shared__ float4 Bs[];  // [26 offsets][4 blocks (s, nt)][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
   constexpr int NP = kTcWarps * 16 * MT;  // target parents of the block
-  int* qs = reinterpret_cast<int*>(Bs + 26 * 32 * 2);  // [26][NP] source parent of each (offset, parent)
+  int* qs = reinterpret_cast<int*>(Bs + 26 * 4 * 32);  // [26][NP] source parent of each (offset, parent)
   const int f = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const long pb = (long)blockIdx.x * NP;
   {
-    const float4* src = bfrag + (long)f * 26 * 32 * 2;
-    for (int i = threadIdx.x; i < 26 * 32 * 2; i += 32 * kTcWarps) Bs[i] = __ldg(src + i);
+    const float4* src = bfrag + (long)f * 26 * 4 * 32;
+    for (int i = threadIdx.x; i < 26 * 4 * 32; i += 32 * kTcWarps) Bs[i] = __ldg(src + i);
     for (int i = threadIdx.x; i < 26 * NP; i += 32 * kTcWarps) {
       const int o = i / NP;
       const long p = pb + i % NP;
@@ -1158,12 +1158,9 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
       }
   };
   auto compute = [&](int o, const float4 (&x)[MT][2]) {
-    const float4* bl = Bs + (o * 32 + lane) * 2;
-    const float4 bv0 = bl[0], bv1 = bl[1];
-    const float bval[8] = {bv0.x, bv0.y, bv0.z, bv0.w, bv1.x, bv1.y, bv1.z, bv1.w};
-    unsigned bh[8], blo[8];
+    float4 bq[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) tf32_split(bval[i], bh[i], blo[i]);
+    for (int i = 0; i < 4; ++i) bq[i] = Bs[(o * 4 + i) * 32 + lane];  // consecutive lanes: conflict-free
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt) {
       unsigned ah[2][4], al[2][4];
@@ -1179,9 +1176,9 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
       for (int s = 0; s < 2; ++s)
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
-          const int bi = (s * 2 + nt) * 2;
-          const unsigned bh0 = bh[bi], bh1 = bh[bi + 1];
-          const unsigned bl0 = blo[bi], bl1 = blo[bi + 1];
+          const float4 b = bq[s * 2 + nt];
+          const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
+          const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
           mma_tf32_16x8x8(acc[mt][nt], al[s], bh0, bh1);
           mma_tf32_16x8x8(acc[mt][nt], ah[s], bl0, bl1);
           mma_tf32_16x8x8(acc[mt][nt], ah[s], bh0, bh1);
@@ -1219,7 +1216,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout, long p0, long np) {
   DevTree& T = ctx.tree;
   constexpr int MT = 2;
-  const size_t sm = (size_t)26 * 32 * 2 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
+  const size_t sm = (size_t)26 * 4 * 32 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(ceil_div(np, 16 * MT * kTcWarps), n3h);
   ++ctx.n_launch;
@@ -1379,11 +1376,13 @@ void vlist(Context& ctx, const double* ue, double* dc, int ke, const std::functi
   // free device memory (counting this buffer's current allocation), else
   // chunks of that size
   const size_t row = (size_t)n3h * 8 * ke * sizeof(Cplx<Real>);
-  size_t free_b = 0, total_b = 0;
-  PVFMM_CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
-  const double avail = 0.9 * (double)(free_b + ctx.spec_out.cap);
   long chunk = T.n_vtrg;
-  if ((double)T.n_vtrg * row > avail) chunk = std::max(256L, (long)(avail / row));
+  if ((size_t)T.n_vtrg * row > ctx.spec_out.cap) {  // query the device only when the buffer must grow
+    size_t free_b = 0, total_b = 0;
+    PVFMM_CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    const double avail = 0.9 * (double)(free_b + ctx.spec_out.cap);
+    if ((double)T.n_vtrg * row > avail) chunk = std::max(256L, (long)(avail / row));
+  }
   // PVFMM_B200_VLIST_CHUNK caps the chunk (to exercise the chunked path)
   if (const char* e = std::getenv("PVFMM_B200_VLIST_CHUNK")) {
     const long c = std::atol(e);
@@ -1547,12 +1546,27 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
 // pout = g % 2, where the real form of the complex block M = M[f][o][j1][j2]
 // is B[(j2,re)][(j1,re)] = Re M, B[(j2,im)][(j1,re)] = -Im M,
 // B[(j2,re)][(j1,im)] = Im M, B[(j2,im)][(j1,im)] = Re M.  Each value is
-// stored in FP32 as (b0, b1) for the blocks (s, nt) = (0,0), (0,1), (1,0),
-// (1,1); the kernel splits them into rounded TF32 head and remainder.
+// stored as [f][o][block (s, nt)][lane] float4 = (b0 hi, b1 hi, b0 lo, b1 lo),
+// hi = the value rounded to TF32, lo = the remainder rounded to TF32 (round
+// half away from zero, as cvt.rna), so that a warp's loads of one block are
+// consecutive.
+static float tf32_rna(float x) {
+  unsigned u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
 static void upload_vop_fragments(Context& ctx) {
   const HostOperators& h = ctx.hops;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);
-  std::vector<float> fr((size_t)n3h * 26 * 32 * 8);
+  std::vector<float> fr((size_t)n3h * 26 * 4 * 32 * 4);
+  auto split = [](float x, float& hi, float& lo) {
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - hi);
+  };
   for (int f = 0; f < n3h; ++f)
     for (int o = 0; o < 26; ++o)
       for (int lane = 0; lane < 32; ++lane) {
@@ -1564,9 +1578,9 @@ static void upload_vop_fragments(Context& ctx) {
             const float mr = (float)h.vop[src], mi = (float)h.vop[src + 1];
             const float b0 = pout == 0 ? mr : mi;   // from (j2, re)
             const float b1 = pout == 0 ? -mi : mr;  // from (j2, im)
-            float* d = &fr[((((size_t)f * 26 + o) * 32 + lane) * 4 + s * 2 + nt) * 2];
-            d[0] = b0;
-            d[1] = b1;
+            float* d = &fr[((((size_t)f * 26 + o) * 4 + s * 2 + nt) * 32 + lane) * 4];
+            split(b0, d[0], d[2]);
+            split(b1, d[1], d[3]);
           }
       }
   float* dev = ctx.dops.vop_frag.as<float>(fr.size());
