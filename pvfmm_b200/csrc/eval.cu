@@ -1172,6 +1172,15 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
       tf32_split(x[mt][1].z, ah[1][1], al[1][1]);
       tf32_split(x[mt][0].w, ah[1][2], al[1][2]);
       tf32_split(x[mt][1].w, ah[1][3], al[1][3]);
+      // this offset's products accumulate in a fresh fragment and join the
+      // running sum with rounded FP32 adds: the tensor cores' own FP32
+      // accumulation is not round-to-nearest and, carried over all 26
+      // offsets, left a bias of ~2e-6 in the far-field potential
+      float d[2][4];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d[nt][i] = 0.f;
 #pragma unroll
       for (int s = 0; s < 2; ++s)
 #pragma unroll
@@ -1179,10 +1188,14 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
           const float4 b = bq[s * 2 + nt];
           const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
           const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
-          mma_tf32_16x8x8(acc[mt][nt], al[s], bh0, bh1);
-          mma_tf32_16x8x8(acc[mt][nt], ah[s], bl0, bl1);
-          mma_tf32_16x8x8(acc[mt][nt], ah[s], bh0, bh1);
+          mma_tf32_16x8x8(d[nt], al[s], bh0, bh1);
+          mma_tf32_16x8x8(d[nt], ah[s], bl0, bl1);
+          mma_tf32_16x8x8(d[nt], ah[s], bh0, bh1);
         }
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[mt][nt][i] += d[nt][i];
     }
   };
   // three register sets in turn: the gathers of the next two offsets are in
@@ -1448,7 +1461,12 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dim);
     double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * dim);
     ++ctx.n_launch;
-    surface_check_kernel<KerExp, sizeof(Real) == 4><<<T.n_sleaf, kNT, 0, s>>>(
+    // full FP64 rsqrt here in both forms: the check potentials feed the
+    // FP64-cutoff pseudo-inverse, which amplifies their rounding into
+    // near-null components of the equivalent densities; the mixed form's FP32
+    // V-list does not cancel those (one Newton step here raised the 4M-point
+    // potential error from 3e-7 to 2.5e-6)
+    surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
         0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
     dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, uc, dim, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, 0);
     dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, t1, dim, ctx.dops.uc2ue1.get<double>(), dim, uc, dim, 0);
