@@ -10,7 +10,7 @@ plain FP64 and mixed (FP32 near field and V-list DFTs, split-TF32 tensor-core
 V-list products, FP64 check->equivalent chain).  Each form's error is the
 relative L2 error of all 4 outputs against an FP64 direct sum over all
 sources on 2,000 sampled targets; ``value`` is the targets/s of the fastest
-form that meets rel-L2 <= 1e-6.  `--workload` selects the other benchmark
+form whose combined and per-component rel-L2 are all <= 1e-6.  `--workload` selects the other benchmark
 configurations (100k uniform Laplace m=6, 2M Stokes m=10, 30M ellipsoid
 surface m=8); the default is the one above.
 
@@ -429,7 +429,8 @@ def main():
         raise RuntimeError(f"no form completed: {forms}")
 
 
-    ok = [f for f in forms_ok if forms_ok[f]["rel_l2"] <= TOL]
+    # a form meets the bar when the combined error and every output component do
+    ok = [f for f in forms_ok if max([forms_ok[f]["rel_l2"]] + forms_ok[f]["rel_l2_components"]) <= TOL]
     best = max(ok, key=lambda f: forms_ok[f]["targets_per_s"]) if ok else next(iter(forms_ok))
     B = forms[best]
     peaks = {}
