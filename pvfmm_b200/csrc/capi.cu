@@ -56,6 +56,10 @@ void destroy_context(Context& c) {
   if (c.cublas) cublasDestroy(c.cublas);
   if (c.stream) cudaStreamDestroy(c.stream);
   if (c.pinned) cudaFreeHost(c.pinned);
+  if (c.chk) cudaFreeHost(c.chk);
+  if (c.side) cudaStreamSynchronize(c.side);
+  if (c.den_ev) cudaEventDestroy(c.den_ev);
+  if (c.side) cudaStreamDestroy(c.side);
 }
 
 void* create_context(double box_size, int n, int m, int kernel, int precision, bool float_api) {
@@ -159,12 +163,19 @@ void eval_host(const T* src_pos, const T* sl_den, const T* dl_den, long n_src, c
     T* d_den = sl_den ? c.io_den.as<T>(std::max(n_src, 1L) * c.ki.k0) : nullptr;
     T* d_trg = alias ? d_src : c.io_trg.as<T>(n_trg * 3);
     T* d_val = c.io_val.as<T>(n_trg * c.ki.k1);
-    if (n_src > 0) {
-      PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_src, src_pos, n_src * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
-      if (sl_den)
-        PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
-    }
+    if (n_src > 0) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_src, src_pos, n_src * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
     if (!alias) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_trg, trg_pos, n_trg * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    if (n_src > 0 && sl_den) {
+      // the densities are first read after the tree build: upload them on a
+      // side stream meanwhile (overlaps when sl_den is pinned host memory)
+      if (!c.side) {
+        PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+        PVFMM_CUDA_CHECK(cudaEventCreateWithFlags(&c.den_ev, cudaEventDisableTiming));
+      }
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.side));
+      PVFMM_CUDA_CHECK(cudaEventRecord(c.den_ev, c.side));
+      c.den_pending = true;
+    }
     if (eval_device<T>(ctx_, d_src, d_den, n_src, d_trg, d_val, n_trg, setup, c.stream) != 0)
       throw std::runtime_error(get_last_error());
     PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_trg * c.ki.k1 * sizeof(T), cudaMemcpyDeviceToHost, c.stream));

@@ -1427,6 +1427,10 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     if (ctx.events_ready) PVFMM_CUDA_CHECK(cudaEventRecord(ctx.ev[i], s));
   };
   ev(0);
+  if (ctx.den_pending) {  // densities uploaded on the side stream during the tree build
+    PVFMM_CUDA_CHECK(cudaStreamWaitEvent(s, ctx.den_ev, 0));
+    ctx.den_pending = false;
+  }
   // densities (sorted, scaled by scale_x^src_scal: pvfmm-wrapper.cpp:522-541, 591-595)
   double* den = ctx.den.as<double>(std::max(T.n_src, 1L) * k0);
   double ss[3], ts[4];

@@ -91,6 +91,12 @@ struct Context {
   // pinned host staging
   void* pinned = nullptr;
   size_t pinned_cap = 0;
+  int* chk = nullptr;  // pinned slots for counts read back at the end of a tree build
+  // host-pointer evaluations upload the densities on a side stream while the
+  // tree is built; the evaluation waits for den_ev when den_pending
+  cudaStream_t side = nullptr;
+  cudaEvent_t den_ev = nullptr;
+  bool den_pending = false;
 };
 
 // tree.cu

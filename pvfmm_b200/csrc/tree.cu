@@ -493,6 +493,26 @@ long exclusive_scan(Context& ctx, const int* in, int* out, long n) {
   return (long)h[0] + h[1];
 }
 
+// Exclusive prefix sum of n ints without reading the total back; the total
+// (out[n-1] + in[n-1]) is copied into the pinned slot *slot (valid after the
+// stream's next synchronisation).
+__global__ void scan_total(const int* __restrict__ in, const int* __restrict__ out, long n, int* __restrict__ slot) {
+  *slot = out[n - 1] + in[n - 1];
+}
+
+void exclusive_scan_deferred(Context& ctx, const int* in, int* out, long n, int* slot) {
+  if (n <= 0) {
+    *slot = 0;
+    return;
+  }
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx.stream);
+  void* tmp = ctx.scratch2.ensure(bytes);
+  cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx.stream);
+  ++ctx.n_launch;
+  scan_total<<<1, 1, 0, ctx.stream>>>(in, out, n, slot);
+}
+
 // Stable sort of 96-bit keys (hi, lo): by lo, then stably by hi.  On return
 // perm[i] is the input position of the i-th smallest key and hs/ls hold the
 // sorted halves.  Uses temporaries t[base..base+2].
@@ -684,6 +704,7 @@ static std::vector<MKey> seed_grid_keys(int max_pts, bool real_float) {
 void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
                 bool src_counted, bool trg_alias) {
   if (n_src < 1 || n_trg < 1) throw std::runtime_error("build_tree needs at least one source and one target");
+  if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, 64 * sizeof(int)));
   DevTree& T = ctx.tree;
   auto& s = ctx.stream;
   T.valid = false;
@@ -836,8 +857,10 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     ++ctx.n_launch;
     member_flags<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(keys + base, nl, d < D ? ctx.lvlS[d].get<MKey>() : nullptr,
                                                              nSd, internal);
-    const long nint = exclusive_scan(ctx, internal, offs, nl);
-    if (nint != nSd) throw std::runtime_error("octree build: balanced internal set is not closed");
+    // the count is known (nSd); the scan's total is checked after the build's
+    // final synchronisation instead of waiting for it here
+    exclusive_scan_deferred(ctx, internal, offs, nl, ctx.chk + d);
+    const long nint = nSd;
     T.n_internal[d] = nint;
     T.int_off[d] = int_base;
     ++ctx.n_launch;
@@ -941,6 +964,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   }
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
   PVFMM_CUDA_CHECK(cudaGetLastError());
+  for (int d = 0; d <= D; ++d)
+    if (ctx.chk[d] != (int)T.n_internal[d]) throw std::runtime_error("octree build: balanced internal set is not closed");
   T.valid = true;
 }
 
