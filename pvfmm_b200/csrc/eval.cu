@@ -235,6 +235,10 @@ constexpr int kNF = 128;        // threads per near-field block
 #ifndef PVFMM_NEAR_TILE_MULT
 #define PVFMM_NEAR_TILE_MULT 2
 #endif
+#ifndef PVFMM_NEAR_UNROLL
+#define PVFMM_NEAR_UNROLL 1
+#endif
+constexpr int kNearUnroll = PVFMM_NEAR_UNROLL;      // unroll of the record loop
 constexpr int kTile = PVFMM_NEAR_TILE_MULT * kNF;  // source records per tile
 constexpr int kRPT = kTile / kNF;                   // records each thread fetches per tile
 
@@ -297,7 +301,7 @@ __device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile,
   Real ua[KT], ub[KT];
 #pragma unroll
   for (int k = 0; k < KT; ++k) ua[k] = ub[k] = 0;
-#pragma unroll 2
+#pragma unroll kNearUnroll
   for (int j = jb; j < jend; j += js) {
     Real v[R::NVP];
 #pragma unroll
@@ -1113,116 +1117,126 @@ constexpr int kTcWarps = 8;  // warps per block of the tensor-core Hadamard
 #ifndef PVFMM_TC_MIN_BLOCKS
 #define PVFMM_TC_MIN_BLOCKS 2
 #endif
+#ifndef PVFMM_TC_CHUNKS
+#define PVFMM_TC_CHUNKS 8  // target-parent chunks per block (operator fragments staged once)
+#endif
 
 template <int MT>
 __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_tc_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc,
+                                                                       int chunks,
                                                                        const int* __restrict__ vtab,
                                                                        const float4* __restrict__ spec_in,
                                                                        const float4* __restrict__ bfrag,
                                                                        float2* __restrict__ spec_out) {
   extern __shared__ float4 Bs[];  // [26 offsets][4 blocks (s, nt)][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
-  constexpr int NP = kTcWarps * 16 * MT;  // target parents of the block
+  constexpr int NP = kTcWarps * 16 * MT;  // target parents of a chunk
   int* qs = reinterpret_cast<int*>(Bs + 26 * 4 * 32);  // [26][NP] source parent of each (offset, parent)
   const int f = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  const long pb = (long)blockIdx.x * NP;
   {
     const float4* src = bfrag + (long)f * 26 * 4 * 32;
     for (int i = threadIdx.x; i < 26 * 4 * 32; i += 32 * kTcWarps) Bs[i] = __ldg(src + i);
+  }
+  // the block's operator fragments stay staged over `chunks` chunks of NP
+  // target parents (the condition below is uniform across the block)
+  for (int c = 0; c < chunks; ++c) {
+    const long pb = ((long)blockIdx.x * chunks + c) * NP;
+    if (pb >= n_vtrg) break;
+    if (c > 0) __syncthreads();  // every warp is done with the previous chunk's qs
     for (int i = threadIdx.x; i < 26 * NP; i += 32 * kTcWarps) {
       const int o = i / NP;
       const long p = pb + i % NP;
       qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
     }
-  }
-  __syncthreads();
-  const int w0 = warp * 16 * MT;  // first parent of the warp within the block
-  const long p0 = pb + w0;
-  const float4* in_f = spec_in + (long)f * 4 + t;  // row q: in_f[q * n3h * 4]
-  float acc[MT][2][4];
+    __syncthreads();
+    const int w0 = warp * 16 * MT;  // first parent of the warp within the chunk
+    const long p0 = pb + w0;
+    const float4* in_f = spec_in + (long)f * 4 + t;  // row q: in_f[q * n3h * 4]
+    float acc[MT][2][4];
 #pragma unroll
-  for (int mt = 0; mt < MT; ++mt)
+    for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
+      for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.f;
-  float4 xa[MT][2], xb[MT][2], xc[MT][2];
-  auto load = [&](int o, float4 (&x)[MT][2]) {
+        for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.f;
+    float4 xa[MT][2], xb[MT][2], xc[MT][2];
+    auto load = [&](int o, float4 (&x)[MT][2]) {
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int q = qs[o * NP + w0 + mt * 16 + g + 8 * h];
+          x[mt][h] = q >= 0 ? __ldg(in_f + (long)q * n3h * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    auto compute = [&](int o, const float4 (&x)[MT][2]) {
+      float4 bq[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) bq[i] = Bs[(o * 4 + i) * 32 + lane];  // consecutive lanes: conflict-free
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        unsigned ah[2][4], al[2][4];
+        tf32_split(x[mt][0].x, ah[0][0], al[0][0]);
+        tf32_split(x[mt][1].x, ah[0][1], al[0][1]);
+        tf32_split(x[mt][0].y, ah[0][2], al[0][2]);
+        tf32_split(x[mt][1].y, ah[0][3], al[0][3]);
+        tf32_split(x[mt][0].z, ah[1][0], al[1][0]);
+        tf32_split(x[mt][1].z, ah[1][1], al[1][1]);
+        tf32_split(x[mt][0].w, ah[1][2], al[1][2]);
+        tf32_split(x[mt][1].w, ah[1][3], al[1][3]);
+        // this offset's products accumulate in a fresh fragment and join the
+        // running sum with rounded FP32 adds: the tensor cores' own FP32
+        // accumulation is not round-to-nearest and, carried over all 26
+        // offsets, left a bias of ~2e-6 in the far-field potential
+        float d[2][4];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) d[nt][i] = 0.f;
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt) {
+            const float4 b = bq[s * 2 + nt];
+            const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
+            const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
+            mma_tf32_16x8x8(d[nt], al[s], bh0, bh1);
+            mma_tf32_16x8x8(d[nt], ah[s], bl0, bl1);
+            mma_tf32_16x8x8(d[nt], ah[s], bh0, bh1);
+          }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[mt][nt][i] += d[nt][i];
+      }
+    };
+    // three register sets in turn: the gathers of the next two offsets are in
+    // flight while one offset is multiplied
+    load(0, xa);
+    load(1, xb);
+#pragma unroll 1
+    for (int o = 0; o < 26; o += 3) {
+      if (o + 2 < 26) load(o + 2, xc);
+      compute(o, xa);
+      if (o + 3 < 26) load(o + 3, xa);
+      if (o + 1 < 26) compute(o + 1, xb);
+      if (o + 4 < 26) load(o + 4, xb);
+      if (o + 2 < 26) compute(o + 2, xc);
+    }
+    // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); column
+    // n = nt*8 + 2t (+1) is child j1 = 4nt + t, re (im).
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int q = qs[o * NP + w0 + mt * 16 + g + 8 * h];
-        x[mt][h] = q >= 0 ? __ldg(in_f + (long)q * n3h * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const long p = p0 + mt * 16 + g + 8 * h;
+        if (p >= n_vtrg) continue;
+        float2* out = spec_out + (p * n3h + f) * 8;
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) out[4 * nt + t] = make_float2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
       }
-  };
-  auto compute = [&](int o, const float4 (&x)[MT][2]) {
-    float4 bq[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) bq[i] = Bs[(o * 4 + i) * 32 + lane];  // consecutive lanes: conflict-free
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      unsigned ah[2][4], al[2][4];
-      tf32_split(x[mt][0].x, ah[0][0], al[0][0]);
-      tf32_split(x[mt][1].x, ah[0][1], al[0][1]);
-      tf32_split(x[mt][0].y, ah[0][2], al[0][2]);
-      tf32_split(x[mt][1].y, ah[0][3], al[0][3]);
-      tf32_split(x[mt][0].z, ah[1][0], al[1][0]);
-      tf32_split(x[mt][1].z, ah[1][1], al[1][1]);
-      tf32_split(x[mt][0].w, ah[1][2], al[1][2]);
-      tf32_split(x[mt][1].w, ah[1][3], al[1][3]);
-      // this offset's products accumulate in a fresh fragment and join the
-      // running sum with rounded FP32 adds: the tensor cores' own FP32
-      // accumulation is not round-to-nearest and, carried over all 26
-      // offsets, left a bias of ~2e-6 in the far-field potential
-      float d[2][4];
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) d[nt][i] = 0.f;
-#pragma unroll
-      for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-          const float4 b = bq[s * 2 + nt];
-          const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
-          const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
-          mma_tf32_16x8x8(d[nt], al[s], bh0, bh1);
-          mma_tf32_16x8x8(d[nt], ah[s], bl0, bl1);
-          mma_tf32_16x8x8(d[nt], ah[s], bh0, bh1);
-        }
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) acc[mt][nt][i] += d[nt][i];
-    }
-  };
-  // three register sets in turn: the gathers of the next two offsets are in
-  // flight while one offset is multiplied
-  load(0, xa);
-  load(1, xb);
-#pragma unroll 1
-  for (int o = 0; o < 26; o += 3) {
-    if (o + 2 < 26) load(o + 2, xc);
-    compute(o, xa);
-    if (o + 3 < 26) load(o + 3, xa);
-    if (o + 1 < 26) compute(o + 1, xb);
-    if (o + 4 < 26) load(o + 4, xb);
-    if (o + 2 < 26) compute(o + 2, xc);
   }
-  // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); column
-  // n = nt*8 + 2t (+1) is child j1 = 4nt + t, re (im).
-#pragma unroll
-  for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long p = p0 + mt * 16 + g + 8 * h;
-      if (p >= n_vtrg) continue;
-      float2* out = spec_out + (p * n3h + f) * 8;
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) out[4 * nt + t] = make_float2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
-    }
 }
 
 // Target parents [p0, p0 + np) of the V-list; sout holds their rows.
@@ -1231,10 +1245,11 @@ void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<flo
   constexpr int MT = 2;
   const size_t sm = (size_t)26 * 4 * 32 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dim3 grid(ceil_div(np, 16 * MT * kTcWarps), n3h);
+  const int chunks = PVFMM_TC_CHUNKS;
+  dim3 grid(ceil_div(np, (long)16 * MT * kTcWarps * chunks), n3h);
   ++ctx.n_launch;
   hadamard_tc_kernel<MT><<<grid, 32 * kTcWarps, sm, ctx.stream>>>(
-      n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0, reinterpret_cast<const float4*>(sin_),
+      n3h, np, T.n_vtrg, T.n_vsrc, chunks, T.vtab.get<int>() + p0, reinterpret_cast<const float4*>(sin_),
       ctx.dops.vop_frag.get<float4>(), reinterpret_cast<float2*>(sout));
 }
 
