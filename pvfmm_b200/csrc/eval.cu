@@ -1125,12 +1125,14 @@ template <int MT>
 __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_tc_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc,
                                                                        int chunks,
                                                                        const int* __restrict__ vtab,
+                                                                       const unsigned* __restrict__ vmask,
                                                                        const float4* __restrict__ spec_in,
                                                                        const float4* __restrict__ bfrag,
                                                                        float2* __restrict__ spec_out) {
   extern __shared__ float4 Bs[];  // [26 offsets][4 blocks (s, nt)][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
   constexpr int NP = kTcWarps * 16 * MT;  // target parents of a chunk
   int* qs = reinterpret_cast<int*>(Bs + 26 * 4 * 32);  // [26][NP] source parent of each (offset, parent)
+  unsigned* ms = reinterpret_cast<unsigned*>(qs + 26 * NP);  // [NP] occupied-offset pattern of each parent
   const int f = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -1149,6 +1151,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
       const long p = pb + i % NP;
       qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
     }
+    for (int i = threadIdx.x; i < NP; i += 32 * kTcWarps) ms[i] = pb + i < n_vtrg ? __ldg(vmask + pb + i) : 0u;
     __syncthreads();
     const int w0 = warp * 16 * MT;  // first parent of the warp within the chunk
     const long p0 = pb + w0;
@@ -1161,6 +1164,12 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 #pragma unroll
         for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.f;
     float4 xa[MT][2], xb[MT][2], xc[MT][2];
+    // offsets without a source parent for any of the warp's parents are
+    // neither loaded nor multiplied (their products are zero); the targets
+    // are ordered by occupied-offset pattern, so such offsets are common
+    unsigned live = 0;
+    for (int k = lane; k < 16 * MT; k += 32) live |= ms[w0 + k];
+    live = __reduce_or_sync(0xffffffffu, live);
     auto load = [&](int o, float4 (&x)[MT][2]) {
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt)
@@ -1211,18 +1220,42 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
           for (int i = 0; i < 4; ++i) acc[mt][nt][i] += d[nt][i];
       }
     };
-    // three register sets in turn: the gathers of the next two offsets are in
-    // flight while one offset is multiplied
-    load(0, xa);
-    load(1, xb);
+    // The warp's occupied offsets in increasing order, one set bit at a
+    // time; three register sets in turn: the gathers of the next two offsets
+    // are in flight while one offset is multiplied.
+    unsigned rem = live;
+    const int nlive = __popc(live);
+    auto take = [&]() {
+      const int o = __ffs(rem) - 1;
+      rem &= rem - 1;
+      return o;
+    };
+    int oa = 0, ob = 0, oc = 0;
+    if (nlive > 0) {
+      oa = take();
+      load(oa, xa);
+    }
+    if (nlive > 1) {
+      ob = take();
+      load(ob, xb);
+    }
 #pragma unroll 1
-    for (int o = 0; o < 26; o += 3) {
-      if (o + 2 < 26) load(o + 2, xc);
-      compute(o, xa);
-      if (o + 3 < 26) load(o + 3, xa);
-      if (o + 1 < 26) compute(o + 1, xb);
-      if (o + 4 < 26) load(o + 4, xb);
-      if (o + 2 < 26) compute(o + 2, xc);
+    for (int i = 0; i < nlive; i += 3) {
+      if (i + 2 < nlive) {
+        oc = take();
+        load(oc, xc);
+      }
+      compute(oa, xa);
+      if (i + 3 < nlive) {
+        oa = take();
+        load(oa, xa);
+      }
+      if (i + 1 < nlive) compute(ob, xb);
+      if (i + 4 < nlive) {
+        ob = take();
+        load(ob, xb);
+      }
+      if (i + 2 < nlive) compute(oc, xc);
     }
     // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); column
     // n = nt*8 + 2t (+1) is child j1 = 4nt + t, re (im).
@@ -1243,13 +1276,14 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout, long p0, long np) {
   DevTree& T = ctx.tree;
   constexpr int MT = 2;
-  const size_t sm = (size_t)26 * 4 * 32 * sizeof(float4) + (size_t)26 * kTcWarps * 16 * MT * sizeof(int);
+  const size_t sm = (size_t)26 * 4 * 32 * sizeof(float4) + (size_t)27 * kTcWarps * 16 * MT * sizeof(int);
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int chunks = PVFMM_TC_CHUNKS;
   dim3 grid(ceil_div(np, (long)16 * MT * kTcWarps * chunks), n3h);
   ++ctx.n_launch;
   hadamard_tc_kernel<MT><<<grid, 32 * kTcWarps, sm, ctx.stream>>>(
-      n3h, np, T.n_vtrg, T.n_vsrc, chunks, T.vtab.get<int>() + p0, reinterpret_cast<const float4*>(sin_),
+      n3h, np, T.n_vtrg, T.n_vsrc, chunks, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
+      reinterpret_cast<const float4*>(sin_),
       ctx.dops.vop_frag.get<float4>(), reinterpret_cast<float2*>(sout));
 }
 

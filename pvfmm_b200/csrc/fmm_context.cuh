@@ -40,6 +40,7 @@ struct DevTree {
   DevBuf vsrc, vtrg;                  // non-leaf nodes: spectra sources / targets
   DevBuf node2vsrc;                   // int per node (-1)
   DevBuf vtab;                        // int[26] per vtrg: vsrc index per colleague offset (-1)
+  DevBuf vmask;                       // unsigned per vtrg: bit o set when vtab[o] >= 0 (vtrg sorted by it)
   DevBuf xtrg;                        // target nodes with X-list entries
   DevBuf x_off, x_list;               // CSR over xtrg
   DevBuf p_off, p_list;               // CSR over tleaf: P2P source leaves

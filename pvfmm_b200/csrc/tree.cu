@@ -441,6 +441,33 @@ __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf
   }
 }
 
+// V-list targets are ordered by their pattern of occupied offsets within
+// windows of kVsortWindow consecutive (Morton-ordered) targets: bit o of the
+// pattern is set when the target has a source parent at colleague offset o
+// (the offsets of fill_vtab).  key[i] = window << 26 | pattern.
+#ifndef PVFMM_VSORT_WINDOW
+#define PVFMM_VSORT_WINDOW 2048
+#endif
+constexpr long kVsortWindow = PVFMM_VSORT_WINDOW;
+__global__ void vlist_keys(const int* __restrict__ vtrg, long n_vtrg, const int* __restrict__ coll,
+                           const int* __restrict__ node2vsrc, unsigned long long* __restrict__ key) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n_vtrg) return;
+  const long t = vtrg[i];
+  unsigned m = 0;
+  for (int ci = 0, o = 0; ci < 27; ++ci) {
+    if (ci == 13) continue;
+    const int c = coll[t * 27 + ci];
+    if (c >= 0 && node2vsrc[c] >= 0) m |= 1u << o;
+    ++o;
+  }
+  key[i] = (unsigned long long)(i / kVsortWindow) << 26 | m;
+}
+__global__ void vlist_patterns(const unsigned long long* __restrict__ key, long n, unsigned* __restrict__ mask) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) mask[i] = (unsigned)(key[i] & ((1u << 26) - 1));
+}
+
 __global__ void fill_vtab(const int* __restrict__ vtrg, long n_vtrg, const int* __restrict__ coll,
                           const int* __restrict__ node2vsrc, int* __restrict__ vtab) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -493,14 +520,22 @@ long exclusive_scan(Context& ctx, const int* in, int* out, long n) {
   return (long)h[0] + h[1];
 }
 
+// Pinned count slots of a tree build: [0, kMaxDepth] internal nodes per level,
+// then the compacted list sizes and the leaf count.
+constexpr int kChkLists = 40, kChkLeaves = 48, kChkSlots = 64;
+static_assert(kMaxDepth < kChkLists, "per-level slots overlap the list slots");
+
 // Exclusive prefix sum of n ints without reading the total back; the total
 // (out[n-1] + in[n-1]) is copied into the pinned slot *slot (valid after the
-// stream's next synchronisation).
-__global__ void scan_total(const int* __restrict__ in, const int* __restrict__ out, long n, int* __restrict__ slot) {
-  *slot = out[n - 1] + in[n - 1];
+// stream's next synchronisation) and, with `close`, also stored as out[n].
+__global__ void scan_total(const int* __restrict__ in, int* __restrict__ out, long n, int* __restrict__ slot,
+                           bool close) {
+  const int t = out[n - 1] + in[n - 1];
+  *slot = t;
+  if (close) out[n] = t;
 }
 
-void exclusive_scan_deferred(Context& ctx, const int* in, int* out, long n, int* slot) {
+void exclusive_scan_deferred(Context& ctx, const int* in, int* out, long n, int* slot, bool close = false) {
   if (n <= 0) {
     *slot = 0;
     return;
@@ -510,7 +545,7 @@ void exclusive_scan_deferred(Context& ctx, const int* in, int* out, long n, int*
   void* tmp = ctx.scratch2.ensure(bytes);
   cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx.stream);
   ++ctx.n_launch;
-  scan_total<<<1, 1, 0, ctx.stream>>>(in, out, n, slot);
+  scan_total<<<1, 1, 0, ctx.stream>>>(in, out, n, slot, close);
 }
 
 // Stable sort of 96-bit keys (hi, lo): by lo, then stably by hi.  On return
@@ -704,7 +739,7 @@ static std::vector<MKey> seed_grid_keys(int max_pts, bool real_float) {
 void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
                 bool src_counted, bool trg_alias) {
   if (n_src < 1 || n_trg < 1) throw std::runtime_error("build_tree needs at least one source and one target");
-  if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, 64 * sizeof(int)));
+  if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, kChkSlots * sizeof(int)));
   DevTree& T = ctx.tree;
   auto& s = ctx.stream;
   T.valid = false;
@@ -881,23 +916,24 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     ++ctx.n_launch;
     colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0, coll);
   }
-  // 9. compact node lists
+  // 9. compact node lists.  The compacted lists are sized for all N nodes so
+  //    that the eight counts are read back together at one synchronisation.
   {
     int* flag = ctx.t[3].as<int>(N);
     int* offs = ctx.t[23].as<int>(N);
-    auto compact = [&](auto pred, DevBuf& out, int* map) -> long {
+    int* cnt = ctx.chk + kChkLists;  // sleaf tleaf vsrc p2p x w xtrg vtrg
+    auto compact = [&](auto pred, DevBuf& out, int* map, int* slot) {
       ++ctx.n_launch;
       flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, pred, flag);
-      const long c = exclusive_scan(ctx, flag, offs, N);
-      int* o = out.as<int>(std::max(c, 1L));
+      exclusive_scan_deferred(ctx, flag, offs, N, slot);
+      int* o = out.as<int>(N);
       ++ctx.n_launch;
       compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, o, map);
-      return c;
     };
-    T.n_sleaf = compact([=] __device__(long i) { return leaf[i] && shi[i] > slo[i]; }, T.sleaf, nullptr);
-    T.n_tleaf = compact([=] __device__(long i) { return leaf[i] && thi[i] > tlo[i]; }, T.tleaf, nullptr);
+    compact([=] __device__(long i) { return leaf[i] && shi[i] > slo[i]; }, T.sleaf, nullptr, cnt + 0);
+    compact([=] __device__(long i) { return leaf[i] && thi[i] > tlo[i]; }, T.tleaf, nullptr, cnt + 1);
     int* n2v = T.node2vsrc.as<int>(N);
-    T.n_vsrc = compact([=] __device__(long i) { return !leaf[i] && shi[i] > slo[i]; }, T.vsrc, n2v);
+    compact([=] __device__(long i) { return !leaf[i] && shi[i] > slo[i]; }, T.vsrc, n2v, cnt + 2);
     // lists: count
     int* pc = ctx.t[4].as<int>(N);
     int* xc = ctx.t[5].as<int>(N);
@@ -910,26 +946,50 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* po = T.p_off.as<int>(N + 1);
     int* xo = T.x_off.as<int>(N + 1);
     int* wo = T.w_off.as<int>(N + 1);
-    T.n_p2p = exclusive_scan(ctx, pc, po, N);
-    T.n_x = exclusive_scan(ctx, xc, xo, N);
-    T.n_w = exclusive_scan(ctx, wc, wo, N);
-    {
-      const int tot[3] = {(int)T.n_p2p, (int)T.n_x, (int)T.n_w};
-      PVFMM_CUDA_CHECK(cudaMemcpyAsync(po + N, &tot[0], sizeof(int), cudaMemcpyHostToDevice, s));
-      PVFMM_CUDA_CHECK(cudaMemcpyAsync(xo + N, &tot[1], sizeof(int), cudaMemcpyHostToDevice, s));
-      PVFMM_CUDA_CHECK(cudaMemcpyAsync(wo + N, &tot[2], sizeof(int), cudaMemcpyHostToDevice, s));
-      PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
-    }
+    exclusive_scan_deferred(ctx, pc, po, N, cnt + 3, true);
+    exclusive_scan_deferred(ctx, xc, xo, N, cnt + 4, true);
+    exclusive_scan_deferred(ctx, wc, wo, N, cnt + 5, true);
+    compact([=] __device__(long i) { return xc[i] > 0; }, T.xtrg, nullptr, cnt + 6);
+    compact([=] __device__(long i) { return vc[i] > 0; }, T.vtrg, nullptr, cnt + 7);
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+    T.n_sleaf = cnt[0];
+    T.n_tleaf = cnt[1];
+    T.n_vsrc = cnt[2];
+    T.n_p2p = cnt[3];
+    T.n_x = cnt[4];
+    T.n_w = cnt[5];
+    T.n_xtrg = cnt[6];
+    T.n_vtrg = cnt[7];
     int* pl = T.p_list.as<int>(std::max(T.n_p2p, 1L));
     int* xl = T.x_list.as<int>(std::max(T.n_x, 1L));
     int* wl = T.w_list.as<int>(std::max(T.n_w, 1L));
     ++ctx.n_launch;
     build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 1, nullptr,
                                                  nullptr, nullptr, nullptr, po, xo, wo, pl, xl, wl);
-    T.n_xtrg = compact([=] __device__(long i) { return xc[i] > 0; }, T.xtrg, nullptr);
-    T.n_vtrg = compact([=] __device__(long i) { return vc[i] > 0; }, T.vtrg, nullptr);
     int* vt = T.vtab.as<int>(std::max(T.n_vtrg, 1L) * 26);
+    unsigned* vm = T.vmask.as<unsigned>(std::max(T.n_vtrg, 1L));
     if (T.n_vtrg > 0) {
+      // V-list targets ordered by their pattern of occupied offsets within
+      // windows of Morton order (stable: Morton order within a pattern), so
+      // that the Hadamard kernels can skip the offsets that are empty for all
+      // the parents of a tile while a block's parents stay close in space.
+      // Every target is computed independently: the order changes no value.
+      unsigned long long* key = ctx.t[10].as<unsigned long long>(T.n_vtrg);
+      unsigned long long* keys_sorted = ctx.t[13].as<unsigned long long>(T.n_vtrg);
+      int* vs = ctx.t[11].as<int>(T.n_vtrg);
+      ++ctx.n_launch;
+      vlist_keys<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), T.n_vtrg, coll, n2v, key);
+      int end_bit = 27;
+      while (end_bit < 64 && ((T.n_vtrg - 1) / kVsortWindow) >> (end_bit - 26)) ++end_bit;
+      size_t bytes = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, keys_sorted, T.vtrg.get<int>(), vs, (int)T.n_vtrg, 0,
+                                      end_bit, s);
+      void* tmp = ctx.scratch.ensure(bytes);
+      cub::DeviceRadixSort::SortPairs(tmp, bytes, key, keys_sorted, T.vtrg.get<int>(), vs, (int)T.n_vtrg, 0, end_bit,
+                                      s);
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(T.vtrg.get<int>(), vs, T.n_vtrg * sizeof(int), cudaMemcpyDeviceToDevice, s));
+      ++ctx.n_launch;
+      vlist_patterns<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(keys_sorted, T.n_vtrg, vm);
       ++ctx.n_launch;
       fill_vtab<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), T.n_vtrg, coll, n2v, vt);
     }
@@ -941,8 +1001,9 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* offs = ctx.t[23].as<int>(N);
     ++ctx.n_launch;
     flag_nodes<<<ceil_div(N, kThreads), kThreads, 0, s>>>(N, [=] __device__(long i) { return leaf[i] != 0; }, flag);
-    const long nl = exclusive_scan(ctx, flag, offs, N);
-    if (nl != n_leaves_all) throw std::runtime_error("octree build: leaf count mismatch");
+    // the leaf count is known; the scan's total is checked at the end
+    exclusive_scan_deferred(ctx, flag, offs, N, ctx.chk + kChkLeaves);
+    const long nl = n_leaves_all;
     int* leaves = ctx.t[0].as<int>(std::max(nl, 1L));
     ++ctx.n_launch;
     compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, leaves, nullptr);
@@ -966,6 +1027,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   PVFMM_CUDA_CHECK(cudaGetLastError());
   for (int d = 0; d <= D; ++d)
     if (ctx.chk[d] != (int)T.n_internal[d]) throw std::runtime_error("octree build: balanced internal set is not closed");
+  if (ctx.chk[kChkLeaves] != (int)(N - n_int_total)) throw std::runtime_error("octree build: leaf count mismatch");
   T.valid = true;
 }
 
