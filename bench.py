@@ -139,12 +139,18 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        # the timed region starts once the sampler is producing samples
+        t0 = time.perf_counter()
+        while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.01)
+        self.lines.clear()
 
     def _read(self):
         for line in self.proc.stdout:
@@ -243,13 +249,22 @@ def cpu_baseline(args):
 
 
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# two dominant kernels, measured by ncu at 1,000,000 points of the same
-# distribution (profiles/hadamard_rd_mixed_1M.md, profiles/near_field_mixed_1M.md)
-# and scaled here by the units a launch processes (traffic grows in proportion).
+# two dominant kernels of each form, measured by ncu at 1,000,000 points of the
+# same distribution (profiles/traffic_laplace_potgrad_1M.md) and scaled here by
+# the units a launch processes (traffic grows in proportion).  Units: n_vsrc +
+# n_vtrg for the Hadamard kernels, n_trg for the near field.
 TRAFFIC_1M = {
-    "hadamard": {"bytes": 735288320 + 663280640, "units": 4768 + 4767},   # units: n_vsrc + n_vtrg
-    "near_field": {"bytes": 150417920 + 23502592, "units": 1000000},      # units: n_trg
+    ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
+    ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
+    ("near_field", 4): {"bytes": 149822464 + 20088064, "units": 1000000},        # near_field_kernel<float>
+    ("near_field", 8): {"bytes": 151890688 + 20192256, "units": 1000000},        # near_field_kernel<double>
 }
+TF32_DENSE_NOMINAL_TFLOPS = 1100.0  # B200 dense TF32 tensor throughput (nominal)
+# kernel that computes the V-list Hadamard products: (real bytes, ke) -> name
+HADAMARD_KERNEL = {(4, 1): "hadamard_tc_kernel (V-list M2L, TF32 mma.sync, 3-term split)",
+                   (8, 1): "hadamard_rd_kernel<double> (V-list M2L)",
+                   (4, 3): "hadamard_kernel<float, 3> (V-list M2L)",
+                   (8, 3): "hadamard_kernel<double, 3> (V-list M2L)"}
 
 
 def roofline(B, peaks):
@@ -259,7 +274,9 @@ def roofline(B, peaks):
     by HBM or the tensor cores; the HBM view (algorithmic bytes / kernel time
     against the measured copy bandwidth) is the reported `achieved`/`peak`,
     and `compute` gives the FLOP view against the nominal SIMT peak
-    (148 SMs x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock).
+    (148 SMs x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock), or for the
+    tensor-core Hadamard against the nominal dense TF32 tensor peak (its
+    algorithmic flops; the 3-term split issues three MMAs per product).
     Algorithmic units:
       Hadamard: bytes = (n_vsrc + n_vtrg) * n3h * 8 children * 2 * rb (input
         spectra read once, output spectra written once) + 26 * n3h * 64 * 2 * rb
@@ -288,18 +305,21 @@ def roofline(B, peaks):
     near_ms = B["stages_ms"]["near-field kernel"]
     near_bytes = st["n_src"] * (24 + 8 * k0) + st["n_trg"] * (24 + 8 * k1) + st["n_tleaf"] * ns * ke * 8
     near_flops = float(PAIR_FLOPS[kid]) * (st["p2p_pairs"] + st["w_pairs"] + st["d2t_pairs"])
+    had_name = HADAMARD_KERNEL[(rb, ke)]
     for name, ms, byts, flops, tkey, units in (
-            ("hadamard_rd_kernel (V-list M2L)", had_ms, had_bytes, had_flops, "hadamard", st["n_vsrc"] + st["n_vtrg"]),
+            (had_name, had_ms, had_bytes, had_flops, "hadamard", st["n_vsrc"] + st["n_vtrg"]),
             ("near_field_kernel (U-list P2P + W + D2T)", near_ms, near_bytes, near_flops, "near_field", st["n_trg"])):
         ach = byts / (ms / 1000) / 1e9 if ms > 0 else 0.0
-        tr = TRAFFIC_1M[tkey]
+        tr = TRAFFIC_1M[(tkey, rb)] if kid == 6 else {"bytes": None}
         traffic = tr["bytes"] * units / tr["units"] if tr["bytes"] else None
         tflops = flops / (ms / 1000) / 1e12 if ms > 0 else 0.0
+        peak_tf = TF32_DENSE_NOMINAL_TFLOPS if name.startswith("hadamard_tc") else simt_peak
         out[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes": byts, "kernel_ms": ms,
-                     "compute": {"pipe": "fp32 simt" if rb == 4 else "fp64 simt", "achieved_tflops": tflops,
-                                 "nominal_peak_tflops": simt_peak, "frac": tflops / simt_peak,
+                     "compute": {"pipe": ("tf32 mma.sync x3" if name.startswith("hadamard_tc") else
+                                          "fp32 simt" if rb == 4 else "fp64 simt"), "achieved_tflops": tflops,
+                                 "nominal_peak_tflops": peak_tf, "frac": tflops / peak_tf,
                                  "flops": flops}}
     ranked = sorted(out.values(), key=lambda r: -r["kernel_ms"])
     return ranked[0], ranked[1]
@@ -308,7 +328,7 @@ def roofline(B, peaks):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gaussian4m", choices=sorted(WORKLOADS))
