@@ -10,18 +10,18 @@ plain FP64 and mixed (FP32 near field and V-list DFTs, split-TF32 tensor-core
 V-list products, FP64 check->equivalent chain).  Each form's error is the
 relative L2 error of all 4 outputs against an FP64 direct sum over all
 sources on 2,000 sampled targets; ``value`` is the targets/s of the fastest
-form whose combined and per-component rel-L2 are all <= 1e-6.  `--workload` selects the other benchmark
-configurations (100k uniform Laplace m=6, 2M Stokes m=10, 30M ellipsoid
-surface m=8); the default is the one above.
+form whose combined and per-component rel-L2 are all <= 1e-6.  `--workload`
+selects the other benchmark configurations (100k uniform Laplace m=6, 2M
+Stokes m=10, 30M ellipsoid surface m=8); the default is the one above.
 
 Data are synthetic (seeded numpy; no dataset is named by the reference).
 `value` is measured with inputs resident in HBM through the device entry
 point PVFMMEvalDeviceD; `e2e` through PVFMMEvalD on pinned host buffers
 (host<->device copies inside the timed region).
 
-Multi-GPU: the path does not shard in this build (one rank, no MPI across
-GPUs), so `--gpus N` under torchrun runs N independent replicas (weak
-scaling) and reports the summed throughput over the max-over-ranks time.
+Multi-GPU: the evaluation runs on a single rank (no MPI across GPUs), so
+`--gpus N` under torchrun runs N independent replicas (weak scaling) and
+reports the summed throughput over the max-over-ranks time.
 
 `--impl reference` times the CPU restatement of the reference algorithm
 (oracle/pvfmm_oracle.py) on a bounded sample of the same workload.
@@ -249,10 +249,10 @@ def cpu_baseline(args):
 
 
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# two dominant kernels of each form, measured by ncu at 1,000,000 points of the
-# same distribution (profiles/traffic_laplace_potgrad_1M.md) and scaled here by
-# the units a launch processes (traffic grows in proportion).  Units: n_vsrc +
-# n_vtrg for the Hadamard kernels, n_trg for the near field.
+# two dominant kernels of each form, measured by ncu on one launch at 1,000,000
+# points of the same distribution (m=8, 256/leaf) and scaled here by the units
+# a launch processes (traffic grows in proportion).  Units: n_vsrc + n_vtrg for
+# the Hadamard kernels, n_trg for the near field.
 TRAFFIC_1M = {
     ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
     ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
