@@ -270,9 +270,11 @@ HADAMARD_KERNEL = {(4, 1): "hadamard_tc_kernel (V-list M2L, TF32 mma.sync, 3-ter
 def roofline(B, peaks):
     """Roofline objects of the V-list Hadamard and the fused near field.
 
-    Both kernels are bound by the SIMT FP32 (mixed) / FP64 (plain) pipe, not
-    by HBM or the tensor cores; the HBM view (algorithmic bytes / kernel time
-    against the measured copy bandwidth) is the reported `achieved`/`peak`,
+    Neither kernel is HBM-bound: the near field is bound by the SIMT FP32
+    (mixed) / FP64 (plain) pipes and issue, the mixed form's Hadamard by the
+    tensor pipe and issue, the plain form's by the FP64 pipe.  The HBM view
+    (algorithmic bytes / kernel time against the measured copy bandwidth) is
+    the reported `achieved`/`peak`,
     and `compute` gives the FLOP view against the nominal SIMT peak
     (148 SMs x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock), or for the
     tensor-core Hadamard against the nominal dense TF32 tensor peak (its

@@ -1,0 +1,81 @@
+"""Host-side logic of bench.py, without a GPU: the roofline objects of its
+JSON line (bound, achieved / peak, DRAM traffic scaled from the 1M-point ncu
+capture by the units a launch processes) and the seeded synthetic workloads.
+"""
+import numpy as np
+import pytest
+
+import bench
+
+# tree statistics of the 1,000,000-point Gaussian-mixture workload (m=8,
+# 256/leaf), the size at which the DRAM traffic was captured
+STATS_1M = {"n_vsrc": 4768.0, "n_vtrg": 4767.0, "v_pairs": 86308.0, "n_src": 1e6, "n_trg": 1e6,
+            "n_tleaf": 31479.0, "p2p_pairs": 1832521088.0, "w_pairs": 24364056.0, "d2t_pairs": 296000000.0}
+
+
+def _run(rb, had_ms, near_ms, stats=STATS_1M, peaks=None):
+    B = {"stats": stats, "real_bytes": rb, "clocks": {"sm_max_mhz": 1965.0},
+         "stages_ms": {"V-Hadamard": had_ms, "near-field kernel": near_ms}}
+    return bench.roofline(B, {"hbm_gbs": 6449.1} if peaks is None else peaks)
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+def test_roofline_objects_follow_the_contract(rb):
+    dom, nxt = _run(rb, 3.26, 3.18)
+    assert dom["kernel_ms"] >= nxt["kernel_ms"]
+    for r in (dom, nxt):
+        assert r["bound"] in ("hbm", "tensor")
+        assert r["unit"] == "GB/s" and r["peak"] == 6449.1 and r["peak_source"] == "measured"
+        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+        assert r["achieved"] == pytest.approx(r["algorithmic_bytes"] / (r["kernel_ms"] / 1000) / 1e9)
+        c = r["compute"]
+        assert c["frac"] == pytest.approx(c["achieved_tflops"] / c["nominal_peak_tflops"])
+    names = {dom["kernel"], nxt["kernel"]}
+    assert any(n.startswith("hadamard_tc" if rb == 4 else "hadamard_rd") for n in names)
+
+
+@pytest.mark.parametrize("rb", [4, 8])
+def test_traffic_at_the_capture_size_is_the_capture(rb):
+    dom, nxt = _run(rb, 3.26, 3.18)
+    by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
+    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    assert had["traffic"] == bench.TRAFFIC_1M[("hadamard", rb)]["bytes"]
+    assert by["near_field_kernel"]["traffic"] == bench.TRAFFIC_1M[("near_field", rb)]["bytes"]
+
+
+def test_traffic_scales_with_the_units_of_a_launch():
+    st = dict(STATS_1M, n_vsrc=2 * 4768.0, n_vtrg=2 * 4767.0, n_trg=4e6)
+    dom, nxt = _run(4, 10.0, 12.0, stats=st)
+    by = {r["kernel"].split()[0]: r for r in (dom, nxt)}
+    assert by["hadamard_tc_kernel"]["traffic"] == pytest.approx(2 * bench.TRAFFIC_1M[("hadamard", 4)]["bytes"])
+    assert by["near_field_kernel"]["traffic"] == pytest.approx(4 * bench.TRAFFIC_1M[("near_field", 4)]["bytes"])
+
+
+def test_hadamard_algorithmic_bytes_at_1m():
+    # input spectra read once + output spectra written once + operators once (FP32)
+    dom, nxt = _run(4, 3.26, 3.18)
+    had = dom if dom["kernel"].startswith("hadamard") else nxt
+    assert had["algorithmic_bytes"] == (4768 + 4767) * 2304 * 8 * 2 * 4 + 26 * 2304 * 64 * 2 * 4 == 1436663808
+
+
+def test_fallback_peak_is_labelled():
+    dom, _ = _run(4, 3.26, 3.18, peaks={})
+    assert dom["peak"] == 6650.0 and dom["peak_source"] == "fallback"
+
+
+@pytest.mark.parametrize("name", sorted(bench.WORKLOADS))
+def test_workloads_are_seeded(name):
+    w = bench.WORKLOADS[name]
+    x1, q1 = bench.make_points(w, 2000)
+    x2, q2 = bench.make_points(w, 2000)
+    assert x1.shape == (2000, 3)
+    assert np.array_equal(x1, x2) and np.array_equal(q1, q2)
+    assert x1.min() >= 0.0 and x1.max() <= 1.0
+    k0 = bench.KDIM[w["kernel"]][0]
+    assert q1.reshape(2000, -1).shape[1] == k0
+
+
+def test_ellipsoid_points_lie_on_the_surface():
+    x, _ = bench.make_points(bench.WORKLOADS["ellipsoid30m"], 5000)
+    a = np.array([0.45, 0.3, 0.15])
+    assert np.allclose((((x - 0.5) / a) ** 2).sum(1), 1.0, atol=1e-12)
