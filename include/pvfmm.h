@@ -52,7 +52,7 @@ enum PVFMMKernel {
  * the host) for kernel `kernel`, multipole order `m` (even, 2..16) and at most
  * `n` points per leaf.  `comm` must be a single-rank communicator.  The D
  * context evaluates in FP64 ("plain" form); the F context evaluates in the
- * mixed form (FP32 near field, FFT and translations; FP64 pseudo-inverses). */
+ * mixed form (see PVFMMPrecisionMixed). */
 void* PVFMMCreateContextD(double box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm);
 void* PVFMMCreateContextF(float box_size, int n, int m, enum PVFMMKernel kernel, MPI_Comm comm);
 
@@ -80,9 +80,14 @@ void PVFMMDestroyContextF(void** ctx);
 
 enum PVFMMPrecision {
   PVFMMPrecisionPlain = 0,   /* FP64 everywhere */
-  PVFMMPrecisionMixed = 1    /* FP32 P2P (rsqrt + Newton, compensated sums),
-                                FP32 FFT/Hadamard, FP32-accumulated translations,
-                                FP64 pseudo-inverse precompute */
+  PVFMMPrecisionMixed = 1    /* FP32 near field (U and W lists: rsqrt + one
+                                Newton step, hi+lo coordinates, partial sums
+                                promoted to FP64 every 16 sources), FP32
+                                V-list DFTs, V-list products on the tensor
+                                cores as 3-term split TF32; FP64 for the
+                                check-to-equivalent chain (S2U and X check
+                                potentials, pseudo-inverse GEMMs, U2U, D2D,
+                                D2T evaluation) */
 };
 
 /* Context on double-precision inputs with an explicit precision form, so the
