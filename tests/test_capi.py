@@ -117,8 +117,7 @@ def test_invalid_context_pointer_is_rejected():
     assert "invalid" in P.last_error()
 
 
-@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) == "" or
-                    __import__("torch").cuda.is_available(), reason="checks the no-GPU failure path")
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-GPU failure path")
 def test_no_gpu_means_no_context():
     with pytest.raises(RuntimeError):
         P.FMMParticleContext(-1, 100, 4, P.FMMKernel.LaplacePotential)
