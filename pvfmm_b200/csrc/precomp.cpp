@@ -51,9 +51,11 @@ std::vector<double> place_surface(const std::vector<double>& u, const double* ce
 }
 
 // Pseudo-inverse factors (fmm_pts.txx:478-537): for M (rows x cols) = U S V^T,
-// C2E0 = V S^+ (cols x cols), C2E1 = U^T (cols x rows).
+// C2E0 = V S^+ (cols x cols), C2E1 = U^T (cols x rows).  With U_out / S_out
+// the SVD's U and S are handed back as well.
 void pinv_factors(const std::vector<double>& M, int rows, int cols, double eps, std::vector<double>& c2e0,
-                  std::vector<double>& c2e1) {
+                  std::vector<double>& c2e1, std::vector<double>* U_out = nullptr,
+                  std::vector<double>* S_out = nullptr) {
   std::vector<double> U, S, V;
   jacobi_svd(rows, cols, M.data(), U, S, V);
   double smax = 0;
@@ -65,6 +67,8 @@ void pinv_factors(const std::vector<double>& M, int rows, int cols, double eps, 
   c2e1.assign((size_t)cols * rows, 0.0);
   for (int j = 0; j < cols; ++j)
     for (int r = 0; r < rows; ++r) c2e1[(size_t)j * rows + r] = U[(size_t)r * cols + j];
+  if (U_out) *U_out = std::move(U);
+  if (S_out) *S_out = std::move(S);
 }
 
 // 1D complex DFT of length n along a strided line, sign -1 (forward).
@@ -253,13 +257,13 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
     auto uc = place_surface(ops.usurf, zero, 0.5, kRad1);
     std::vector<double> M((size_t)dim * dim);
     exp_kernel_matrix(ki.exp_kernel, ue.data(), ns, uc.data(), ns, M.data());
-    pinv_factors(M, dim, dim, eps, ops.uc2ue0, ops.uc2ue1);
     // ue = (uc V S+) U^T lies in the span of U's columns; its components
     // along singular values below 4*eps32*max are amplified FP64 rounding
     // of the check potentials, cancelling in exact arithmetic but not in
-    // FP32.  P = U_k U_k^T over the columns above that cutoff.
-    std::vector<double> U, S, V;
-    jacobi_svd(dim, dim, M.data(), U, S, V);
+    // FP32.  P = U_k U_k^T over the columns above that cutoff, from the
+    // same SVD as the factors.
+    std::vector<double> U, S;
+    pinv_factors(M, dim, dim, eps, ops.uc2ue0, ops.uc2ue1, &U, &S);
     double smax = 0;
     for (double v : S) smax = std::max(smax, std::fabs(v));
     const double cut32 = 4.0 * std::ldexp(1.0, -23) * smax;
