@@ -190,8 +190,20 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
 /* Host precompute of one operator (FP64 row-major), for tests.  `which`:
  * 0 UC2UE0, 1 UC2UE1, 2 DC2DE0, 3 DC2DE1, 4 U2U (8 stacked, child-major rows),
  * 5 D2D (8 stacked, child-major columns), 6 unit surface (ns x 3),
- * 7 V-list Hadamard operators (complex, [f][offset 26][j1 8][j2 8][k0][k1]).
- * Returns the element count needed (copies at most n). */
+ * 7 V-list Hadamard operators (complex, [f][offset 26][j1 8][j2 8][k0][k1]),
+ * 8 projector onto the upward equivalent directions above the FP32 cutoff.
+ * Returns the element count needed (copies at most n).
+ *
+ * Operator cache (contexts and this function alike): when the environment
+ * variable PVFMM_DIR names a directory, the pseudo-inverse factors (the SVD
+ * part of the precompute) are read from PVFMM_DIR/Precomp_<kernel name>_m<m>.data
+ * if it exists and written there otherwise, in the layout of the reference's
+ * precompute files (include/precomp_mat.txx:213-345, file name
+ * include/fmm_pts.txx:246-276): entry 0 of matrix types 0-3 (UC2UE0, UC2UE1,
+ * DC2DE0, DC2DE1, FP64 cutoff); other entries are skipped on reading and left
+ * empty on writing.  Operators built from the cache equal the computed ones.
+ * A file that exists but is not a usable cache is an error; a directory that
+ * cannot be written is skipped.  Without PVFMM_DIR no file is touched. */
 long PVFMMPrecompOperator(enum PVFMMKernel kernel, int m, int precision, int which, double* out, long n);
 
 #ifdef __cplusplus

@@ -497,6 +497,7 @@ long PVFMMPrecompOperator(enum PVFMMKernel kernel, int m, int precision, int whi
       case 5: v = &ops.d2d; break;
       case 6: v = &ops.usurf; break;
       case 7: v = &ops.vop; break;
+      case 8: v = &ops.ue_proj; break;
       default: throw std::runtime_error("unknown operator selector");
     }
     if (out && n > 0) std::memcpy(out, v->data(), sizeof(double) * std::min<long>(n, (long)v->size()));

@@ -12,8 +12,14 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <iterator>
 #include <stdexcept>
+#include <string>
+#include <unistd.h>
 
 #include "fmm_host.hpp"
 
@@ -69,6 +75,127 @@ void pinv_factors(const std::vector<double>& M, int rows, int cols, double eps, 
     for (int r = 0; r < rows; ++r) c2e1[(size_t)j * rows + r] = U[(size_t)r * cols + j];
   if (U_out) *U_out = std::move(U);
   if (S_out) *S_out = std::move(S);
+}
+
+// Pseudo-inverse factors with the FP64 cutoff and the singular values they
+// were formed with (S_j = 0 for dropped directions).
+struct PinvFactors {
+  std::vector<double> c2e0, c2e1, S;
+};
+
+// c2e0 with the columns whose singular value is not above 4*eps*max zeroed:
+// the factor pinv_factors forms with cutoff eps (eps >= the FP64 cutoff the
+// columns were kept with), entry for entry.
+std::vector<double> with_cutoff(const PinvFactors& f, int dim, double eps) {
+  double smax = 0;
+  for (double v : f.S) smax = std::max(smax, std::fabs(v));
+  const double cut = eps * smax * 4;
+  std::vector<double> c = f.c2e0;
+  for (int j = 0; j < dim; ++j)
+    if (!(f.S[j] > cut))
+      for (int r = 0; r < dim; ++r) c[(size_t)r * dim + j] = 0.0;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// Operator cache in the reference's precompute-file layout (Save2File and
+// LoadFile, include/precomp_mat.txx:213-345; file name
+// include/fmm_pts.txx:246-276): int sizeof(real) (8), int scale_invar (1),
+// then for each of the 16 matrix types in Mat_Type order
+// (include/precomp_mat.hpp:20-39) an int count n followed by n matrices, each
+// int rows, int cols and rows*cols reals, row-major.  This library writes the
+// pseudo-inverse factors UC2UE0, UC2UE1, DC2DE0, DC2DE1 (FP64 cutoff, the
+// expensive SVD part of the precompute) as entry 0 of types 0-3 and leaves the
+// other types empty, which a reference build fills itself; it reads entry 0
+// of types 0-3 of any file in this layout and skips all other entries.  The
+// cache is used only when the environment variable PVFMM_DIR names its
+// directory (the reference's fallback location); without it no file is read
+// or written.
+// ---------------------------------------------------------------------------
+constexpr int kMatTypes = 16;  // Type_Count
+
+std::string cache_path(const KernelInfo& ki, int m) {
+  const char* dir = std::getenv("PVFMM_DIR");
+  if (!dir || !*dir) return "";
+  return std::string(dir) + "/Precomp_" + ki.name + "_m" + std::to_string(m) + ".data";
+}
+
+// Reads the factors of f[0] (upward) and f[1] (downward); false when the file
+// does not exist, an exception when it exists but is not a usable cache.
+bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) return false;
+  std::vector<char> buf((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  size_t pos = 0;
+  auto bad = [&](const std::string& why) { return std::runtime_error("operator cache " + path + ": " + why); };
+  auto get_int = [&]() {
+    if (pos + sizeof(int) > buf.size()) throw bad("truncated");
+    int v;
+    std::memcpy(&v, buf.data() + pos, sizeof(int));
+    pos += sizeof(int);
+    return v;
+  };
+  if (get_int() != (int)sizeof(double)) throw bad("not an FP64 operator file");
+  if (get_int() != 1) throw bad("operators of a kernel that is not scale-invariant");
+  std::vector<double> mats[4];
+  for (int t = 0; t < kMatTypes; ++t) {
+    const int n = get_int();
+    if (n < 0) throw bad("negative matrix count");
+    for (int j = 0; j < n; ++j) {
+      const int n1 = get_int(), n2 = get_int();
+      if (n1 < 0 || n2 < 0) throw bad("negative matrix size");
+      const size_t bytes = (size_t)n1 * n2 * sizeof(double);
+      if (pos + bytes > buf.size()) throw bad("truncated");
+      if (t < 4 && j == 0) {
+        if (n1 != dim || n2 != dim)
+          throw bad("matrix type " + std::to_string(t) + " is " + std::to_string(n1) + " x " + std::to_string(n2) +
+                    ", expected " + std::to_string(dim) + " x " + std::to_string(dim));
+        mats[t].resize((size_t)dim * dim);
+        std::memcpy(mats[t].data(), buf.data() + pos, bytes);
+      }
+      pos += bytes;
+    }
+  }
+  for (int t = 0; t < 4; ++t)
+    if (mats[t].empty()) throw bad("lacks matrix type " + std::to_string(t));
+  for (int k = 0; k < 2; ++k) {
+    f[k].c2e0 = std::move(mats[2 * k]);
+    f[k].c2e1 = std::move(mats[2 * k + 1]);
+    // C2E0 = V S^+ with orthonormal V: column j has length 1 / S_j (0 when dropped)
+    f[k].S.assign(dim, 0.0);
+    for (int j = 0; j < dim; ++j) {
+      double n2 = 0;
+      for (int r = 0; r < dim; ++r) n2 += f[k].c2e0[(size_t)r * dim + j] * f[k].c2e0[(size_t)r * dim + j];
+      f[k].S[j] = n2 > 0 ? 1.0 / std::sqrt(n2) : 0.0;
+    }
+  }
+  return true;
+}
+
+// Writes the factors (through a temporary file renamed into place, so that a
+// concurrent reader never sees a partial file).  A directory that cannot be
+// written is skipped silently, as the reference does.
+void save_factors(const std::string& path, int dim, const PinvFactors (&f)[2]) {
+  const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+  FILE* fp = std::fopen(tmp.c_str(), "wb");
+  if (!fp) return;
+  bool ok = true;
+  auto put_int = [&](int v) { ok = ok && std::fwrite(&v, sizeof(int), 1, fp) == 1; };
+  put_int((int)sizeof(double));
+  put_int(1);
+  for (int t = 0; t < kMatTypes; ++t) {
+    if (t >= 4) {
+      put_int(0);
+      continue;
+    }
+    const std::vector<double>& M = (t & 1) ? f[t / 2].c2e1 : f[t / 2].c2e0;
+    put_int(1);
+    put_int(dim);
+    put_int(dim);
+    ok = ok && std::fwrite(M.data(), sizeof(double), M.size(), fp) == M.size();
+  }
+  ok = (std::fclose(fp) == 0) && ok;
+  if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
 }
 
 // 1D complex DFT of length n along a strided line, sign -1 (forward).
@@ -251,39 +378,45 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
   const double eps = mixed ? std::ldexp(1.0, -23) : std::ldexp(1.0, -52);
   const double zero[3] = {0, 0, 0};
 
-  // UC2UE0/1: upward equivalent (RAD0) -> upward check (RAD1), level 0 (:478-537)
+  // Pseudo-inverse factors with the FP64 cutoff, from the operator cache or
+  // from the SVDs: f[0] UC2UE0/1, upward equivalent (RAD0) -> upward check
+  // (RAD1), level 0 (:478-537); f[1] DC2DE0/1, downward equivalent (RAD1) ->
+  // downward check (RAD0) (:538-581).  A larger cutoff drops further columns.
+  const double eps64 = std::ldexp(1.0, -52), eps32 = std::ldexp(1.0, -23);
+  PinvFactors f[2];
+  const std::string cache = cache_path(ki, m);
+  if (cache.empty() || !load_factors(cache, dim, f)) {
+    for (int k = 0; k < 2; ++k) {
+      auto eq = place_surface(ops.usurf, zero, 0.5, k == 0 ? kRad0 : kRad1);
+      auto ck = place_surface(ops.usurf, zero, 0.5, k == 0 ? kRad1 : kRad0);
+      std::vector<double> M((size_t)dim * dim);
+      exp_kernel_matrix(ki.exp_kernel, eq.data(), ns, ck.data(), ns, M.data());
+      pinv_factors(M, dim, dim, eps64, f[k].c2e0, f[k].c2e1, nullptr, &f[k].S);
+    }
+    if (!cache.empty()) save_factors(cache, dim, f);
+  }
+  ops.uc2ue0 = with_cutoff(f[0], dim, eps);
+  ops.uc2ue1 = f[0].c2e1;
+  ops.dc2de0 = with_cutoff(f[1], dim, down_eps32 ? eps32 : eps);
+  ops.dc2de1 = f[1].c2e1;
+  // ue = (uc V S+) U^T lies in the span of U's columns (U^T = UC2UE1); its
+  // components along singular values below 4*eps32*max are amplified FP64
+  // rounding of the check potentials, cancelling in exact arithmetic but not
+  // in FP32.  P = U_k U_k^T over the columns above that cutoff.
   {
-    auto ue = place_surface(ops.usurf, zero, 0.5, kRad0);
-    auto uc = place_surface(ops.usurf, zero, 0.5, kRad1);
-    std::vector<double> M((size_t)dim * dim);
-    exp_kernel_matrix(ki.exp_kernel, ue.data(), ns, uc.data(), ns, M.data());
-    // ue = (uc V S+) U^T lies in the span of U's columns; its components
-    // along singular values below 4*eps32*max are amplified FP64 rounding
-    // of the check potentials, cancelling in exact arithmetic but not in
-    // FP32.  P = U_k U_k^T over the columns above that cutoff, from the
-    // same SVD as the factors.
-    std::vector<double> U, S;
-    pinv_factors(M, dim, dim, eps, ops.uc2ue0, ops.uc2ue1, &U, &S);
+    const std::vector<double>& Ut = f[0].c2e1;  // Ut[j][a] = U[a][j]
     double smax = 0;
-    for (double v : S) smax = std::max(smax, std::fabs(v));
-    const double cut32 = 4.0 * std::ldexp(1.0, -23) * smax;
+    for (double v : f[0].S) smax = std::max(smax, std::fabs(v));
+    const double cut32 = 4.0 * eps32 * smax;
     ops.ue_proj.assign((size_t)dim * dim, 0.0);
     for (int j = 0; j < dim; ++j) {
-      if (!(S[j] > cut32)) continue;
+      if (!(f[0].S[j] > cut32)) continue;
       for (int a = 0; a < dim; ++a) {
-        const double ua = U[(size_t)a * dim + j];
+        const double ua = Ut[(size_t)j * dim + a];
         double* row = &ops.ue_proj[(size_t)a * dim];
-        for (int b = 0; b < dim; ++b) row[b] += ua * U[(size_t)b * dim + j];
+        for (int b = 0; b < dim; ++b) row[b] += ua * Ut[(size_t)j * dim + b];
       }
     }
-  }
-  // DC2DE0/1: downward equivalent (RAD1) -> downward check (RAD0) (:538-581)
-  {
-    auto de = place_surface(ops.usurf, zero, 0.5, kRad1);
-    auto dc = place_surface(ops.usurf, zero, 0.5, kRad0);
-    std::vector<double> M((size_t)dim * dim);
-    exp_kernel_matrix(ki.exp_kernel, de.data(), ns, dc.data(), ns, M.data());
-    pinv_factors(M, dim, dim, down_eps32 ? std::ldexp(1.0, -23) : eps, ops.dc2de0, ops.dc2de1);
   }
   // U2U (:582-606): (M_ce2c * UC2UE0) * UC2UE1, child c of a level-0 parent.
   ops.u2u.assign((size_t)8 * dim * dim, 0.0);
