@@ -32,17 +32,25 @@ constexpr double kPi = 3.14159265358979323846;
 
 thread_local std::string g_last_error;
 
-// Row-major dense product C = A(r x k) * B(k x c).
+// Row-major dense product C = A(r x k) * B(k x c).  Blocks of 8 rows x 256
+// columns share each row segment of B from cache; every C[i][j] is still the
+// sum over l in increasing order.
 std::vector<double> matmul(const std::vector<double>& A, const std::vector<double>& B, int r, int k, int c) {
+  constexpr int kRows = 8, kCols = 256;
   std::vector<double> C((size_t)r * c, 0.0);
+  const int nrb = (r + kRows - 1) / kRows, ncb = (c + kCols - 1) / kCols;
 #pragma omp parallel for schedule(static)
-  for (int i = 0; i < r; ++i) {
-    double* ci = &C[(size_t)i * c];
+  for (int blk = 0; blk < nrb * ncb; ++blk) {
+    const int i0 = (blk / ncb) * kRows, i1 = std::min(r, i0 + kRows);
+    const int j0 = (blk % ncb) * kCols, j1 = std::min(c, j0 + kCols);
     for (int l = 0; l < k; ++l) {
-      const double a = A[(size_t)i * k + l];
-      if (a == 0.0) continue;
       const double* bl = &B[(size_t)l * c];
-      for (int j = 0; j < c; ++j) ci[j] += a * bl[j];
+      for (int i = i0; i < i1; ++i) {
+        const double a = A[(size_t)i * k + l];
+        if (a == 0.0) continue;
+        double* ci = &C[(size_t)i * c];
+        for (int j = j0; j < j1; ++j) ci[j] += a * bl[j];
+      }
     }
   }
   return C;
