@@ -23,6 +23,8 @@
 #ifndef PVFMM_B200_PVFMM_H_
 #define PVFMM_B200_PVFMM_H_
 
+#include <stdint.h>
+
 #include "pvfmm_mpi_stub.h"
 
 #ifdef __cplusplus
@@ -73,6 +75,20 @@ void PVFMMEvalF(const float* src_pos, const float* sl_den, const float* dl_den, 
  * releases the context and sets *ctx to NULL. */
 void PVFMMDestroyContextD(void** ctx);
 void PVFMMDestroyContextF(void** ctx);
+
+/* Replace the Fortran bindings pvfmmcreatecontextd_/f_, pvfmmevald_/f_ and
+ * pvfmmdestroycontextd_/f_ (reference src/pvfmm-wrapper.cpp:831-875): the same
+ * functions with every argument passed by reference, 32-bit integers for the
+ * leaf size, order, kernel and setup flag, 64-bit point counts, and the
+ * communicator as a Fortran handle, which must denote a single rank. */
+void pvfmmcreatecontextd_(void** ctx, double* box_size, int32_t* n, int32_t* m, int32_t* kernel, int32_t* fcomm);
+void pvfmmcreatecontextf_(void** ctx, float* box_size, int32_t* n, int32_t* m, int32_t* kernel, int32_t* fcomm);
+void pvfmmevald_(const double* src_pos, const double* sl_den, int64_t* n_src, const double* trg_pos, double* trg_val,
+                 int64_t* n_trg, void** ctx, int32_t* setup);
+void pvfmmevalf_(const float* src_pos, const float* sl_den, int64_t* n_src, const float* trg_pos, float* trg_val,
+                 int64_t* n_trg, void** ctx, int32_t* setup);
+void pvfmmdestroycontextd_(void** ctx);
+void pvfmmdestroycontextf_(void** ctx);
 
 /* ---------------------------------------------------------------------------
  * Extensions (no counterpart in the reference).

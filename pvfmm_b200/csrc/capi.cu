@@ -302,6 +302,27 @@ int PVFMMSetUnitBox(void* ctx, int on) {
 void PVFMMDestroyContextD(void** ctx) { destroy(ctx); }
 void PVFMMDestroyContextF(void** ctx) { destroy(ctx); }
 
+// Fortran bindings (reference src/pvfmm-wrapper.cpp:831-875): every argument
+// by reference, the communicator as a Fortran handle (single rank here).
+void pvfmmcreatecontextd_(void** ctx, double* box_size, int32_t* n, int32_t* m, int32_t* kernel, int32_t* fcomm) {
+  (void)fcomm;
+  *ctx = PVFMMCreateContextD(*box_size, *n, *m, (enum PVFMMKernel) * kernel, MPI_COMM_WORLD);
+}
+void pvfmmcreatecontextf_(void** ctx, float* box_size, int32_t* n, int32_t* m, int32_t* kernel, int32_t* fcomm) {
+  (void)fcomm;
+  *ctx = PVFMMCreateContextF(*box_size, *n, *m, (enum PVFMMKernel) * kernel, MPI_COMM_WORLD);
+}
+void pvfmmevald_(const double* src_pos, const double* sl_den, int64_t* n_src, const double* trg_pos, double* trg_val,
+                 int64_t* n_trg, void** ctx, int32_t* setup) {
+  PVFMMEvalD(src_pos, sl_den, nullptr, (long)*n_src, trg_pos, trg_val, (long)*n_trg, *ctx, *setup);
+}
+void pvfmmevalf_(const float* src_pos, const float* sl_den, int64_t* n_src, const float* trg_pos, float* trg_val,
+                 int64_t* n_trg, void** ctx, int32_t* setup) {
+  PVFMMEvalF(src_pos, sl_den, nullptr, (long)*n_src, trg_pos, trg_val, (long)*n_trg, *ctx, *setup);
+}
+void pvfmmdestroycontextd_(void** ctx) { PVFMMDestroyContextD(ctx); }
+void pvfmmdestroycontextf_(void** ctx) { PVFMMDestroyContextF(ctx); }
+
 const char* PVFMMGetLastError(void) { return get_last_error(); }
 
 long PVFMMGetLaunchCount(const void* ctx) {

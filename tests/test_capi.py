@@ -21,7 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared_functions():
     src = open(os.path.join(ROOT, "include", "pvfmm.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(PVFMM\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(PVFMM\w+|pvfmm\w+_)\s*\(", src)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 def test_python_binding_covers_header():
     lib = P.load_library()
     for n in _declared_functions():
-        assert getattr(lib, n).restype is not None or n.startswith(("PVFMMEval", "PVFMMDestroy")) \
+        assert getattr(lib, n).restype is not None or n.startswith(("PVFMMEval", "PVFMMDestroy", "pvfmm")) \
             or n in ("PVFMMEvalD", "PVFMMEvalF")
 
 
@@ -121,3 +121,32 @@ def test_invalid_context_pointer_is_rejected():
 def test_no_gpu_means_no_context():
     with pytest.raises(RuntimeError):
         P.FMMParticleContext(-1, 100, 4, P.FMMKernel.LaplacePotential)
+
+
+def test_fortran_bindings_pass_every_argument_by_reference():
+    """The Fortran entry points (reference src/pvfmm-wrapper.cpp:831-875),
+    called as a Fortran program calls them: every argument by reference.
+    Without a GPU the context cannot be created: the handle comes back NULL
+    with the message set, and an evaluation on it fills the output with NaN."""
+    if __import__("torch").cuda.is_available():
+        pytest.skip("checks the no-GPU failure path")
+    lib = ctypes.CDLL(str(P.LIB_PATH))
+    c_i32, c_i64 = ctypes.c_int32, ctypes.c_int64
+    ctx = ctypes.c_void_p(1)
+    lib.pvfmmcreatecontextd_(ctypes.byref(ctx), ctypes.byref(ctypes.c_double(-1.0)), ctypes.byref(c_i32(100)),
+                             ctypes.byref(c_i32(6)), ctypes.byref(c_i32(0)), ctypes.byref(c_i32(0)))
+    assert ctx.value is None and P.last_error()
+    x = np.random.default_rng(0).random(3 * 10)
+    q = np.ones(10)
+    out = np.zeros(10)
+    lib.pvfmmevald_(x.ctypes.data_as(ctypes.c_void_p), q.ctypes.data_as(ctypes.c_void_p), ctypes.byref(c_i64(10)),
+                    x.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(c_i64(10)),
+                    ctypes.byref(ctx), ctypes.byref(c_i32(1)))
+    assert np.isnan(out).all()
+    lib.pvfmmdestroycontextd_(ctypes.byref(ctx))
+    assert ctx.value is None
+    ctxf = ctypes.c_void_p(1)
+    lib.pvfmmcreatecontextf_(ctypes.byref(ctxf), ctypes.byref(ctypes.c_float(-1.0)), ctypes.byref(c_i32(100)),
+                             ctypes.byref(c_i32(6)), ctypes.byref(c_i32(0)), ctypes.byref(c_i32(0)))
+    assert ctxf.value is None
+    lib.pvfmmdestroycontextf_(ctypes.byref(ctxf))
