@@ -152,8 +152,9 @@ bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
     for (int j = 0; j < n; ++j) {
       const int n1 = get_int(), n2 = get_int();
       if (n1 < 0 || n2 < 0) throw bad("negative matrix size");
+      const size_t left = (buf.size() - pos) / sizeof(double);
+      if (n1 > 0 && (size_t)n2 > left / (size_t)n1) throw bad("truncated");
       const size_t bytes = (size_t)n1 * n2 * sizeof(double);
-      if (pos + bytes > buf.size()) throw bad("truncated");
       if (t < 4 && j == 0) {
         if (n1 != dim || n2 != dim)
           throw bad("matrix type " + std::to_string(t) + " is " + std::to_string(n1) + " x " + std::to_string(n2) +

@@ -129,6 +129,10 @@ def test_unusable_files_are_errors(cache_dir):
     (cache_dir / "Precomp_laplace_m8.data").write_bytes(np.array([4, 1], np.int32).tobytes())
     with pytest.raises(RuntimeError, match="not an FP64"):
         _all(K.LaplacePotential, 8, 0)
+    # a declared size whose byte count overflows 64 bits
+    (cache_dir / "Precomp_laplace_m10.data").write_bytes(np.array([8, 1, 1, 2**31 - 1, 2**31 - 1], np.int32).tobytes())
+    with pytest.raises(RuntimeError, match="truncated"):
+        _all(K.LaplacePotential, 10, 0)
 
 
 def test_unwritable_directory_is_skipped(monkeypatch, tmp_path):
