@@ -189,6 +189,32 @@ def dist_setup():
     return world, rank, local
 
 
+def rank_tools(world, device):
+    """barrier() and max_over_ranks(v) of the replica group (no-ops for one
+    rank); the process group is initialised by the caller."""
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
+def job_throughput(world, n, ms):
+    """Whole-job targets/s: every replica evaluates n targets; ms is the
+    step time (max over ranks)."""
+    return world * n / (ms / 1000)
+
+
 def run_reference(args, world, rank):
     """CPU restatement of the reference FMM (oracle) on a bounded sample."""
     if rank != 0:
@@ -356,16 +382,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_tools(world, "cuda")
 
     N = args.n
     kid = W["kernel"]
@@ -432,9 +449,9 @@ def main():
             e2e_ms = max_over_ranks(1000 * (time.perf_counter() - t0) / args.steps)
             if P.last_error():
                 raise RuntimeError(P.last_error())
-            res = {"ms_per_step": ms, "targets_per_s": world * N / (ms / 1000), "rel_l2": err,
+            res = {"ms_per_step": ms, "targets_per_s": job_throughput(world, N, ms), "rel_l2": err,
                    "rel_l2_components": err_comp, "stages_ms": stage, "stats": stats, "gpu_launches": launches,
-                   "clocks": cl, "e2e_ms": e2e_ms, "e2e_targets_per_s": world * N / (e2e_ms / 1000),
+                   "clocks": cl, "e2e_ms": e2e_ms, "e2e_targets_per_s": job_throughput(world, N, e2e_ms),
                    "real_bytes": 8 if form == "plain" else 4}
             return res
         finally:
