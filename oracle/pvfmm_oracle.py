@@ -42,15 +42,18 @@ MAX_DEPTH = 30          # PVFMM_MAX_DEPTH, include/pvfmm_common.hpp:29
 RAD0 = 1.05             # PVFMM_RAD0, include/pvfmm_common.hpp:33
 RAD1 = 2.95             # PVFMM_RAD1, include/pvfmm_common.hpp:34
 TWO30 = 1 << MAX_DEPTH
-# Scale exponents of the expansion kernels (laplace / stokes_vel):
-# K(x/2) = 2^(src+trg) K(x) (include/kernel.txx:64-196).
+# Scale exponents of the expansion kernels: K(x/2) = 2^(src+trg) K(x)
+# (include/kernel.txx:64-196).  Every kernel here is homogeneous, so the
+# reference's solve gives src = 0 and trg = the kernel's degree (KernelFn.deg).
 EXP_SRC_SCAL = 0.0
-EXP_TRG_SCAL = 1.0
 
 # PVFMMKernel enum, include/pvfmm.h:21-28 (+ extension value 6 for pot+grad)
 LAPLACE_POTENTIAL = 0
 LAPLACE_GRADIENT = 1
+STOKES_PRESSURE = 2
 STOKES_VELOCITY = 3
+STOKES_VELOCITY_GRAD = 4
+BIOT_SAVART_POTENTIAL = 5
 LAPLACE_POTGRAD = 6
 
 
@@ -59,11 +62,13 @@ LAPLACE_POTGRAD = 6
 # ----------------------------------------------------------------------------
 @dataclass(frozen=True)
 class KernelFn:
-    """One kernel function: k0 source dims -> k1 target dims."""
+    """One kernel function: k0 source dims -> k1 target dims, homogeneous of
+    degree ``deg``: K(x/2) = 2^deg K(x)."""
     name: str
     k0: int
     k1: int
     flops: int
+    deg: float = 1.0
 
     def matrix(self, src: np.ndarray, trg: np.ndarray) -> np.ndarray:
         """BuildMatrix layout (include/kernel.txx:1059-1135):
@@ -92,6 +97,31 @@ class KernelFn:
                 for k in range(3):
                     K[:, j, :, k] = rinv * ((1.0 if j == k else 0.0) + r[:, :, j] * r[:, :, k] * rinv2)
             K /= 8 * math.pi
+        elif self.name == "stokes_press":        # kernel.txx:1366-1378: (r . f) / r^3 / (4 pi)
+            K = (r * (rinv ** 3 / (4 * math.pi))[:, :, None]).transpose(0, 2, 1)[:, :, :, None]   # (ns,3,nt,1)
+        elif self.name == "stokes_grad":         # kernel.txx:1404-1432
+            # u[3a+b] = (r_b f_a - f_b r_a + (r.f)(delta_ab - 3 r_a r_b / r^2)) / r^3 / (8 pi)
+            rinv2, rinv3 = rinv * rinv, rinv ** 3
+            K = np.zeros((ns, 3, nt, 9))
+            for j in range(3):
+                for a in range(3):
+                    for b in range(3):
+                        v = r[:, :, j] * ((1.0 if a == b else 0.0) - 3 * r[:, :, a] * r[:, :, b] * rinv2)
+                        if j == a:
+                            v = v + r[:, :, b]
+                        if j == b:
+                            v = v - r[:, :, a]
+                        K[:, j, :, 3 * a + b] = v * rinv3
+            K /= 8 * math.pi
+        elif self.name == "biot_savart":         # kernel.txx:1492-1505: (f x r) / r^3 / (4 pi)
+            rinv3 = rinv ** 3 / (4 * math.pi)
+            K = np.zeros((ns, 3, nt, 3))
+            for j in range(3):
+                for k in range(3):
+                    for l in range(3):
+                        eps = (j - k) * (k - l) * (l - j) / 2          # Levi-Civita symbol e_jlk
+                        if eps:
+                            K[:, j, :, k] += -eps * r[:, :, l] * rinv3
         else:
             raise ValueError(self.name)
         return K.reshape(ns * self.k0, nt * self.k1)
@@ -110,6 +140,9 @@ LAPLACE = KernelFn("laplace", 1, 1, 9)
 LAPLACE_GRAD = KernelFn("laplace_grad", 1, 3, 16)
 LAPLACE_PG = KernelFn("laplace_potgrad", 1, 4, 18)
 STOKES = KernelFn("stokes_vel", 3, 3, 29)
+STOKES_PRESS = KernelFn("stokes_press", 3, 1, 16, deg=2.0)
+STOKES_GRAD = KernelFn("stokes_grad", 3, 9, 94, deg=2.0)
+BIOT_SAVART = KernelFn("biot_savart", 3, 3, 24, deg=2.0)
 
 
 @dataclass(frozen=True)
@@ -137,6 +170,12 @@ KERNELS = {
     STOKES_VELOCITY: Kernel("stokes_vel", 3, 3, STOKES, STOKES, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0)),
     # extension: potential + gradient in one pass (expansions use the potential)
     LAPLACE_POTGRAD: Kernel("laplace_potgrad", 1, 4, LAPLACE_PG, LAPLACE, (0.0,), (1.0, 2.0, 2.0, 2.0)),
+    # StokesKernel<T>::pressure() / vel_grad(), BiotSavartKernel<T>::potential()
+    # (include/kernel.txx:1480-1491, 1508-1511): no separate expansion kernels,
+    # so the kernel itself is expanded (kernel.txx:894-901)
+    STOKES_PRESSURE: Kernel("stokes_press", 3, 1, STOKES_PRESS, STOKES_PRESS, (0.0,) * 3, (2.0,)),
+    STOKES_VELOCITY_GRAD: Kernel("stokes_grad", 3, 9, STOKES_GRAD, STOKES_GRAD, (0.0,) * 3, (2.0,) * 9),
+    BIOT_SAVART_POTENTIAL: Kernel("biot_savart", 3, 3, BIOT_SAVART, BIOT_SAVART, (0.0,) * 3, (2.0,) * 3),
 }
 
 
@@ -557,7 +596,7 @@ def d_equiv_surf(m, c, depth):
 def pinv_factors(M: np.ndarray):
     """C2E0 = V^T S^+ and C2E1 = U^T with the cutoff S > 4 eps max(S)
     (fmm_pts.txx:478-537).  check_row @ C2E0 @ C2E1 = equiv_row."""
-    U, s, Vh = np.linalg.svd(M)
+    U, s, Vh = np.linalg.svd(M, full_matrices=M.shape[0] == M.shape[1])  # thin SVD when not square
     eps = np.finfo(np.float64).eps
     cut = eps * s.max() * 4
     sinv = np.where(s > cut, 1.0 / np.where(s > cut, s, 1.0), 0.0)
@@ -712,10 +751,10 @@ class FMM:
         tree = self.tree
         N = tree.nodes
         k0, k1e = ke.k0, ke.k1
-        # Expansion kernels in scope (laplace, stokes_vel) have src_scal = 0 and
-        # trg_scal = 1 on every component, so a check->equivalent operator at
-        # level l is 2^(-l) times the level-0 one (fmm_pts.txx:2447-2465).
-        e_exp = EXP_TRG_SCAL - EXP_SRC_SCAL
+        # Expansion kernels have src_scal = 0 and trg_scal = deg on every
+        # component, so a check->equivalent operator at level l is 2^(-deg l)
+        # times the level-0 one (fmm_pts.txx:2447-2465).
+        e_exp = ke.deg - EXP_SRC_SCAL
         den = np.asarray(den_sorted, dtype=np.float64).reshape(-1, K.k0)
         nn = len(N)
         ue = np.zeros((nn, ns * k0))
@@ -833,7 +872,7 @@ class FMM:
             lvl = P.depth + 1
             for c in range(8):
                 vals = res[c][:, im[:, 2], im[:, 1], im[:, 0]].T          # (ns, k1)
-                dc[P.child0 + c] += vals.reshape(-1) * 2.0 ** (EXP_TRG_SCAL * lvl)
+                dc[P.child0 + c] += vals.reshape(-1) * 2.0 ** (ke.deg * lvl)
 
 
 # ----------------------------------------------------------------------------
