@@ -203,7 +203,12 @@ long PVFMMGetLaunchCount(const void* ctx);
  * Copies at most `n` elements into out and returns the element count needed. */
 long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
 
-/* Host precompute of one operator (FP64 row-major), for tests.  `which`:
+/* Host precompute of one operator (FP64 row-major), for tests; every
+ * PVFMMKernel value, including Stokes pressure, Stokes velocity gradient and
+ * Biot-Savart, whose evaluation is not implemented (their expansions use the
+ * kernel itself, so with kin source and kout target dims the check ->
+ * equivalent factors are (ns*kout) x r and r x (ns*kin), r = ns*min(kin, kout)).
+ * `which`:
  * 0 UC2UE0, 1 UC2UE1, 2 DC2DE0, 3 DC2DE1, 4 U2U (8 stacked, child-major rows),
  * 5 D2D (8 stacked, child-major columns), 6 unit surface (ns x 3),
  * 7 V-list Hadamard operators (complex, [f][offset 26][j1 8][j2 8][k0][k1]),

@@ -651,27 +651,30 @@ class Operators:
     @classmethod
     def from_arrays(cls, kernel: Kernel, m: int, arrays: dict) -> "Operators":
         """Operators given as arrays in the layout of the CUDA library's
-        precompute (``PVFMMPrecompOperator``): uc2ue0/1, dc2de0/1 (dim x dim),
-        u2u (8*dim x dim, child-major rows), d2d (dim x 8*dim, child-major
-        columns) and vop (complex [f][26][8][8][ke][ke], divided by n3).  Lets
-        the oracle run on exactly the operators the GPU runs on."""
+        precompute (``PVFMMPrecompOperator``), with din = ns*kin equivalent and
+        dout = ns*kout check values and r = min(din, dout): uc2ue0/dc2de0
+        (dout x r), uc2ue1/dc2de1 (r x din), u2u (8*din x din, child-major
+        rows), d2d (dout x 8*dout, child-major columns) and vop (complex
+        [f][26][8][8][kin][kout], divided by n3).  Lets the oracle run on
+        exactly the operators the library builds."""
         self = cls.__new__(cls)
         self.kernel, self.m = kernel, m
         self.ns = 6 * (m - 1) ** 2 + 2
-        ke = kernel.exp.k0
-        dim = self.ns * ke
-        self.uc2ue0 = arrays["uc2ue0"].reshape(dim, dim)
-        self.uc2ue1 = arrays["uc2ue1"].reshape(dim, dim)
-        self.dc2de0 = arrays["dc2de0"].reshape(dim, dim)
-        self.dc2de1 = arrays["dc2de1"].reshape(dim, dim)
-        self.u2u = list(arrays["u2u"].reshape(8, dim, dim))
-        d2d = arrays["d2d"].reshape(dim, 8, dim)
+        kin, kout = kernel.exp.k0, kernel.exp.k1
+        din, dout = self.ns * kin, self.ns * kout
+        r = min(din, dout)
+        self.uc2ue0 = arrays["uc2ue0"].reshape(dout, r)
+        self.uc2ue1 = arrays["uc2ue1"].reshape(r, din)
+        self.dc2de0 = arrays["dc2de0"].reshape(dout, r)
+        self.dc2de1 = arrays["dc2de1"].reshape(r, din)
+        self.u2u = list(arrays["u2u"].reshape(8, din, din))
+        d2d = arrays["d2d"].reshape(dout, 8, dout)
         self.d2d = [np.ascontiguousarray(d2d[:, c, :]) for c in range(8)]
         n1 = 2 * m
         self.n1 = n1
         n3 = n1 ** 3
         vop = arrays["vop"].reshape(-1, 2)
-        vop = (vop[:, 0] + 1j * vop[:, 1]).reshape(n1, n1, n1 // 2 + 1, 26, 8, 8, ke, ke)
+        vop = (vop[:, 0] + 1j * vop[:, 1]).reshape(n1, n1, n1 // 2 + 1, 26, 8, 8, kin, kout)
         self.vhat = {}
         for ci in range(27):
             if ci == 13:

@@ -10,11 +10,25 @@ namespace pvfmm_b200 {
 
 // Kernel ids follow the PVFMMKernel enum (reference include/pvfmm.h:21-28),
 // plus 6 = Laplace potential+gradient.
-enum KernelId { kLaplacePot = 0, kLaplaceGrad = 1, kStokesVel = 3, kLaplacePotGrad = 6 };
+enum KernelId {
+  kLaplacePot = 0,
+  kLaplaceGrad = 1,
+  kStokesPress = 2,
+  kStokesVel = 3,
+  kStokesVelGrad = 4,
+  kBiotSavart = 5,
+  kLaplacePotGrad = 6
+};
 
 // Expansion kernels (the k_s2m/k_m2m/k_m2l/k_l2l sub-kernels of
 // include/kernel.txx:1333-1344, 1475-1479).
-enum ExpKernel { kExpLaplace = 0, kExpStokes = 1 };
+// Stokes pressure, Stokes velocity gradient and Biot-Savart have no separate
+// expansion kernels and expand themselves (kernel.txx:894-901, 1480-1511).
+enum ExpKernel { kExpLaplace = 0, kExpStokes = 1, kExpStokesPress = 2, kExpStokesGrad = 3, kExpBiotSavart = 4 };
+
+// Source and target dims of an expansion kernel (equivalent densities carry
+// kin components, check potentials kout).
+void exp_kernel_dims(int exp_kernel, int* kin, int* kout);
 
 struct KernelInfo {
   int id;
@@ -27,24 +41,34 @@ struct KernelInfo {
   int flops;               // per-pair flop count convention (kernel.txx:1277,1317,1352)
 };
 
+// Kernels the CUDA evaluation implements.
 bool kernel_info(int id, KernelInfo* out);
+// kernel_info plus the kernels whose operators the host precompute builds
+// but whose evaluation the CUDA path does not implement yet (Stokes pressure,
+// Stokes velocity gradient, Biot-Savart; their scale exponents are not set).
+bool kernel_info_host(int id, KernelInfo* out);
 
 // Level-0 operators of one kernel and multipole order.  All FP64, row-major,
 // row-vector convention (out_row = in_row * M), as in fmm_pts.txx:453-764.
 struct HostOperators {
   int kernel = -1, m = 0, ns = 0, ke = 1, n1 = 0, n3 = 0, n3h = 0;
+  // expansion dims: equivalent densities ns*kin, check potentials ns*kout
+  // (kin = kout = ke for the kernels the CUDA path evaluates)
+  int kin = 1, kout = 1;
   bool mixed = false;
   std::vector<double> usurf;            // ns x 3 unit cube-surface points u in [-1,1]^3
-  std::vector<double> uc2ue0, uc2ue1;   // (ns*ke) x (ns*ke): check -> equivalent factors
-  // (ns*ke) x (ns*ke): orthogonal projector onto the upward equivalent
+  // check -> equivalent factors, r = min(ns*kin, ns*kout):
+  // C2E0 (ns*kout) x r, C2E1 r x (ns*kin)
+  std::vector<double> uc2ue0, uc2ue1;
+  // (ns*kin) x (ns*kin): orthogonal projector onto the upward equivalent
   // directions whose singular value (equivalent -> check) is above the FP32
   // cutoff 4*eps32*max; the mixed form applies it to the upward equivalent
   // densities before its FP32 stages
   std::vector<double> ue_proj;
   std::vector<double> dc2de0, dc2de1;
-  std::vector<double> u2u;              // (8*ns*ke) x (ns*ke), row block c = child octant c
-  std::vector<double> d2d;              // (ns*ke) x (8*ns*ke), column block c = child octant c
-  std::vector<double> vop;              // complex (re,im): [n3h][26][8][8][ke][ke]
+  std::vector<double> u2u;              // (8*ns*kin) x (ns*kin), row block c = child octant c
+  std::vector<double> d2d;              // (ns*kout) x (8*ns*kout), column block c = child octant c
+  std::vector<double> vop;              // complex (re,im): [n3h][26][8][8][kin][kout]
   std::vector<int> fft_map, ifft_map;   // ns grid indices (x + n1*y + n1*n1*z)
 };
 

@@ -64,23 +64,33 @@ std::vector<double> place_surface(const std::vector<double>& u, const double* ce
   return p;
 }
 
-// Pseudo-inverse factors (fmm_pts.txx:478-537): for M (rows x cols) = U S V^T,
-// C2E0 = V S^+ (cols x cols), C2E1 = U^T (cols x rows).  With U_out / S_out
-// the SVD's U and S are handed back as well.
+// Pseudo-inverse factors (fmm_pts.txx:478-537): for M (rows x cols) = U S V^T
+// with r = min(rows, cols) singular values, C2E0 = V S^+ (cols x r) and
+// C2E1 = U^T (r x rows).  With U_out / S_out the SVD's U (rows x r) and S are
+// handed back as well.  A matrix with fewer rows than columns is decomposed
+// through its transpose.
 void pinv_factors(const std::vector<double>& M, int rows, int cols, double eps, std::vector<double>& c2e0,
                   std::vector<double>& c2e1, std::vector<double>* U_out = nullptr,
                   std::vector<double>* S_out = nullptr) {
   std::vector<double> U, S, V;
-  jacobi_svd(rows, cols, M.data(), U, S, V);
+  if (rows >= cols) {
+    jacobi_svd(rows, cols, M.data(), U, S, V);  // U rows x cols, V cols x cols
+  } else {
+    std::vector<double> Mt((size_t)cols * rows);
+    for (int i = 0; i < rows; ++i)
+      for (int j = 0; j < cols; ++j) Mt[(size_t)j * rows + i] = M[(size_t)i * cols + j];
+    jacobi_svd(cols, rows, Mt.data(), V, S, U);  // M^T = V S U^T: V cols x rows, U rows x rows
+  }
+  const int r = std::min(rows, cols);
   double smax = 0;
   for (double s : S) smax = std::max(smax, std::fabs(s));
   const double cut = eps * smax * 4;
-  c2e0.assign((size_t)cols * cols, 0.0);
-  for (int r = 0; r < cols; ++r)
-    for (int j = 0; j < cols; ++j) c2e0[(size_t)r * cols + j] = (S[j] > cut) ? V[(size_t)r * cols + j] / S[j] : 0.0;
-  c2e1.assign((size_t)cols * rows, 0.0);
-  for (int j = 0; j < cols; ++j)
-    for (int r = 0; r < rows; ++r) c2e1[(size_t)j * rows + r] = U[(size_t)r * cols + j];
+  c2e0.assign((size_t)cols * r, 0.0);
+  for (int i = 0; i < cols; ++i)
+    for (int j = 0; j < r; ++j) c2e0[(size_t)i * r + j] = (S[j] > cut) ? V[(size_t)i * r + j] / S[j] : 0.0;
+  c2e1.assign((size_t)r * rows, 0.0);
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < rows; ++i) c2e1[(size_t)j * rows + i] = U[(size_t)i * r + j];
   if (U_out) *U_out = std::move(U);
   if (S_out) *S_out = std::move(S);
 }
@@ -91,17 +101,17 @@ struct PinvFactors {
   std::vector<double> c2e0, c2e1, S;
 };
 
-// c2e0 with the columns whose singular value is not above 4*eps*max zeroed:
-// the factor pinv_factors forms with cutoff eps (eps >= the FP64 cutoff the
-// columns were kept with), entry for entry.
-std::vector<double> with_cutoff(const PinvFactors& f, int dim, double eps) {
+// c2e0 (n x r) with the columns whose singular value is not above
+// 4*eps*max zeroed: the factor pinv_factors forms with cutoff eps (eps >= the
+// FP64 cutoff the columns were kept with), entry for entry.
+std::vector<double> with_cutoff(const PinvFactors& f, int n, int r, double eps) {
   double smax = 0;
   for (double v : f.S) smax = std::max(smax, std::fabs(v));
   const double cut = eps * smax * 4;
   std::vector<double> c = f.c2e0;
-  for (int j = 0; j < dim; ++j)
+  for (int j = 0; j < r; ++j)
     if (!(f.S[j] > cut))
-      for (int r = 0; r < dim; ++r) c[(size_t)r * dim + j] = 0.0;
+      for (int i = 0; i < n; ++i) c[(size_t)i * r + j] = 0.0;
   return c;
 }
 
@@ -130,7 +140,8 @@ std::string cache_path(const KernelInfo& ki, int m) {
 
 // Reads the factors of f[0] (upward) and f[1] (downward); false when the file
 // does not exist, an exception when it exists but is not a usable cache.
-bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
+bool load_factors(const std::string& path, int din, int dout, PinvFactors (&f)[2]) {
+  const int r = std::min(din, dout);
   std::ifstream in(path, std::ios::binary);
   if (!in) return false;
   std::vector<char> buf((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
@@ -156,10 +167,12 @@ bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
       if (n1 > 0 && (size_t)n2 > left / (size_t)n1) throw bad("truncated");
       const size_t bytes = (size_t)n1 * n2 * sizeof(double);
       if (t < 4 && j == 0) {
-        if (n1 != dim || n2 != dim)
+        // C2E0 (types 0, 2): (ns*kout) x r; C2E1 (types 1, 3): r x (ns*kin)
+        const int e1 = (t & 1) ? r : dout, e2 = (t & 1) ? din : r;
+        if (n1 != e1 || n2 != e2)
           throw bad("matrix type " + std::to_string(t) + " is " + std::to_string(n1) + " x " + std::to_string(n2) +
-                    ", expected " + std::to_string(dim) + " x " + std::to_string(dim));
-        mats[t].resize((size_t)dim * dim);
+                    ", expected " + std::to_string(e1) + " x " + std::to_string(e2));
+        mats[t].resize((size_t)n1 * n2);
         std::memcpy(mats[t].data(), buf.data() + pos, bytes);
       }
       pos += bytes;
@@ -171,10 +184,10 @@ bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
     f[k].c2e0 = std::move(mats[2 * k]);
     f[k].c2e1 = std::move(mats[2 * k + 1]);
     // C2E0 = V S^+ with orthonormal V: column j has length 1 / S_j (0 when dropped)
-    f[k].S.assign(dim, 0.0);
-    for (int j = 0; j < dim; ++j) {
+    f[k].S.assign(r, 0.0);
+    for (int j = 0; j < r; ++j) {
       double n2 = 0;
-      for (int r = 0; r < dim; ++r) n2 += f[k].c2e0[(size_t)r * dim + j] * f[k].c2e0[(size_t)r * dim + j];
+      for (int i = 0; i < dout; ++i) n2 += f[k].c2e0[(size_t)i * r + j] * f[k].c2e0[(size_t)i * r + j];
       f[k].S[j] = n2 > 0 ? 1.0 / std::sqrt(n2) : 0.0;
     }
   }
@@ -184,7 +197,8 @@ bool load_factors(const std::string& path, int dim, PinvFactors (&f)[2]) {
 // Writes the factors (through a temporary file renamed into place, so that a
 // concurrent reader never sees a partial file).  A directory that cannot be
 // written is skipped silently, as the reference does.
-void save_factors(const std::string& path, int dim, const PinvFactors (&f)[2]) {
+void save_factors(const std::string& path, int din, int dout, const PinvFactors (&f)[2]) {
+  const int r = std::min(din, dout);
   const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
   FILE* fp = std::fopen(tmp.c_str(), "wb");
   if (!fp) return;
@@ -199,8 +213,8 @@ void save_factors(const std::string& path, int dim, const PinvFactors (&f)[2]) {
     }
     const std::vector<double>& M = (t & 1) ? f[t / 2].c2e1 : f[t / 2].c2e0;
     put_int(1);
-    put_int(dim);
-    put_int(dim);
+    put_int((t & 1) ? r : dout);
+    put_int((t & 1) ? din : r);
     ok = ok && std::fwrite(M.data(), sizeof(double), M.size(), fp) == M.size();
   }
   ok = (std::fclose(fp) == 0) && ok;
@@ -244,6 +258,35 @@ bool kernel_info(int id, KernelInfo* out) {
   return true;
 }
 
+bool kernel_info_host(int id, KernelInfo* out) {
+  if (kernel_info(id, out)) return true;
+  KernelInfo k{};
+  switch (id) {
+    case kStokesPress:  // StokesKernel<T>::pressure(), kernel.txx:1480-1483
+      k = {id, "stokes_press", 3, 1, kExpStokesPress, 3, {0, 0, 0}, {0, 0, 0, 0}, 16};
+      break;
+    case kStokesVelGrad:  // StokesKernel<T>::vel_grad(), kernel.txx:1488-1491
+      k = {id, "stokes_grad", 3, 9, kExpStokesGrad, 3, {0, 0, 0}, {0, 0, 0, 0}, 94};
+      break;
+    case kBiotSavart:  // BiotSavartKernel<T>::potential(), kernel.txx:1508-1511
+      k = {id, "biot_savart", 3, 3, kExpBiotSavart, 3, {0, 0, 0}, {0, 0, 0, 0}, 24};
+      break;
+    default:
+      return false;
+  }
+  *out = k;
+  return true;
+}
+
+void exp_kernel_dims(int exp_kernel, int* kin, int* kout) {
+  switch (exp_kernel) {
+    case kExpLaplace: *kin = 1; *kout = 1; break;
+    case kExpStokesPress: *kin = 3; *kout = 1; break;
+    case kExpStokesGrad: *kin = 3; *kout = 9; break;
+    default: *kin = 3; *kout = 3; break;  // Stokes velocity, Biot-Savart
+  }
+}
+
 std::vector<double> unit_surface(int p) {
   // Same point order as surface() (fmm_pts.txx:54-97), unscaled.
   const int n = 6 * (p - 1) * (p - 1) + 2;
@@ -283,7 +326,7 @@ void exp_kernel_matrix(int exp_kernel, const double* src, int n_src, const doubl
         const double r2 = dx * dx + dy * dy + dz * dz;
         M[(size_t)i * n_trg + t] = r2 > 0 ? s / std::sqrt(r2) : 0.0;
       }
-  } else {
+  } else if (exp_kernel == kExpStokes) {
     const double s = 1.0 / (8 * kPi);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n_src; ++i)
@@ -296,6 +339,39 @@ void exp_kernel_matrix(int exp_kernel, const double* src, int n_src, const doubl
           for (int k = 0; k < 3; ++k)
             M[((size_t)i * 3 + j) * n_trg * 3 + (size_t)t * 3 + k] =
                 s * ((j == k ? rinv : 0.0) + r[j] * r[k] * rinv3);
+      }
+  } else {
+    // Stokes pressure (kernel.txx:1366-1378), Stokes velocity gradient
+    // (:1404-1432) and Biot-Savart (:1492-1505), source component j
+    int kin, kout;
+    exp_kernel_dims(exp_kernel, &kin, &kout);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_src; ++i)
+      for (int t = 0; t < n_trg; ++t) {
+        const double r[3] = {trg[t * 3] - src[i * 3], trg[t * 3 + 1] - src[i * 3 + 1], trg[t * 3 + 2] - src[i * 3 + 2]};
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const double rinv = r2 > 0 ? 1.0 / std::sqrt(r2) : 0.0;
+        const double rinv2 = rinv * rinv, rinv3 = rinv2 * rinv;
+        for (int j = 0; j < 3; ++j) {
+          double* row = &M[((size_t)i * kin + j) * n_trg * kout + (size_t)t * kout];
+          if (exp_kernel == kExpStokesPress) {
+            row[0] = r[j] * rinv3 / (4 * kPi);  // (r . f) / r^3
+          } else if (exp_kernel == kExpStokesGrad) {
+            // u[3a+b] = (r_b f_a - f_b r_a + (r . f)(delta_ab - 3 r_a r_b / r^2)) / r^3
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                double v = r[j] * ((a == b ? 1.0 : 0.0) - 3 * r[a] * r[b] * rinv2);
+                if (j == a) v += r[b];
+                if (j == b) v -= r[a];
+                row[3 * a + b] = v * rinv3 / (8 * kPi);
+              }
+          } else {  // (f x r) / r^3: u_k = e_kjl f_j r_l
+            const int k1 = (j + 1) % 3, k2 = (j + 2) % 3;
+            row[j] = 0.0;
+            row[k2] = r[k1] * rinv3 / (4 * kPi);   // e_{k2 j k1} = +1
+            row[k1] = -r[k2] * rinv3 / (4 * kPi);  // e_{k1 j k2} = -1
+          }
+        }
       }
   }
 }
@@ -370,15 +446,21 @@ void jacobi_svd(int rows, int cols, const double* A, std::vector<double>& U, std
 
 void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool down_eps32) {
   KernelInfo ki;
-  if (!kernel_info(kernel, &ki)) throw std::runtime_error("unsupported kernel");
+  if (!kernel_info_host(kernel, &ki)) throw std::runtime_error("unsupported kernel");
   if (m < 2 || m > 16 || (m & 1)) throw std::runtime_error("multipole order must be even and in [2,16]");
   const int ke = ki.ke;
+  int kin, kout;
+  exp_kernel_dims(ki.exp_kernel, &kin, &kout);
   const int ns = 6 * (m - 1) * (m - 1) + 2;
-  const int dim = ns * ke;
+  // equivalent densities din = ns*kin, check potentials dout = ns*kout, r
+  // singular values per check -> equivalent factor
+  const int din = ns * kin, dout = ns * kout, rk = std::min(din, dout);
   ops.kernel = kernel;
   ops.m = m;
   ops.ns = ns;
   ops.ke = ke;
+  ops.kin = kin;
+  ops.kout = kout;
   ops.mixed = mixed;
   ops.n1 = 2 * m;
   ops.n3 = ops.n1 * ops.n1 * ops.n1;
@@ -394,61 +476,61 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
   const double eps64 = std::ldexp(1.0, -52), eps32 = std::ldexp(1.0, -23);
   PinvFactors f[2];
   const std::string cache = cache_path(ki, m);
-  if (cache.empty() || !load_factors(cache, dim, f)) {
+  if (cache.empty() || !load_factors(cache, din, dout, f)) {
     for (int k = 0; k < 2; ++k) {
       auto eq = place_surface(ops.usurf, zero, 0.5, k == 0 ? kRad0 : kRad1);
       auto ck = place_surface(ops.usurf, zero, 0.5, k == 0 ? kRad1 : kRad0);
-      std::vector<double> M((size_t)dim * dim);
+      std::vector<double> M((size_t)din * dout);
       exp_kernel_matrix(ki.exp_kernel, eq.data(), ns, ck.data(), ns, M.data());
-      pinv_factors(M, dim, dim, eps64, f[k].c2e0, f[k].c2e1, nullptr, &f[k].S);
+      pinv_factors(M, din, dout, eps64, f[k].c2e0, f[k].c2e1, nullptr, &f[k].S);
     }
-    if (!cache.empty()) save_factors(cache, dim, f);
+    if (!cache.empty()) save_factors(cache, din, dout, f);
   }
-  ops.uc2ue0 = with_cutoff(f[0], dim, eps);
+  ops.uc2ue0 = with_cutoff(f[0], dout, rk, eps);
   ops.uc2ue1 = f[0].c2e1;
-  ops.dc2de0 = with_cutoff(f[1], dim, down_eps32 ? eps32 : eps);
+  ops.dc2de0 = with_cutoff(f[1], dout, rk, down_eps32 ? eps32 : eps);
   ops.dc2de1 = f[1].c2e1;
   // ue = (uc V S+) U^T lies in the span of U's columns (U^T = UC2UE1); its
   // components along singular values below 4*eps32*max are amplified FP64
   // rounding of the check potentials, cancelling in exact arithmetic but not
   // in FP32.  P = U_k U_k^T over the columns above that cutoff.
   {
-    const std::vector<double>& Ut = f[0].c2e1;  // Ut[j][a] = U[a][j]
+    const std::vector<double>& Ut = f[0].c2e1;  // Ut[j][a] = U[a][j], r x din
     double smax = 0;
     for (double v : f[0].S) smax = std::max(smax, std::fabs(v));
     const double cut32 = 4.0 * eps32 * smax;
-    ops.ue_proj.assign((size_t)dim * dim, 0.0);
-    for (int j = 0; j < dim; ++j) {
+    ops.ue_proj.assign((size_t)din * din, 0.0);
+    for (int j = 0; j < rk; ++j) {
       if (!(f[0].S[j] > cut32)) continue;
-      for (int a = 0; a < dim; ++a) {
-        const double ua = Ut[(size_t)j * dim + a];
-        double* row = &ops.ue_proj[(size_t)a * dim];
-        for (int b = 0; b < dim; ++b) row[b] += ua * Ut[(size_t)j * dim + b];
+      for (int a = 0; a < din; ++a) {
+        const double ua = Ut[(size_t)j * din + a];
+        double* row = &ops.ue_proj[(size_t)a * din];
+        for (int b = 0; b < din; ++b) row[b] += ua * Ut[(size_t)j * din + b];
       }
     }
   }
   // U2U (:582-606): (M_ce2c * UC2UE0) * UC2UE1, child c of a level-0 parent.
-  ops.u2u.assign((size_t)8 * dim * dim, 0.0);
-  ops.d2d.assign((size_t)dim * 8 * dim, 0.0);
+  ops.u2u.assign((size_t)8 * din * din, 0.0);
+  ops.d2d.assign((size_t)dout * 8 * dout, 0.0);
   for (int c = 0; c < 8; ++c) {
     const double cc[3] = {((c & 1) ? 0.25 : -0.25), ((c & 2) ? 0.25 : -0.25), ((c & 4) ? 0.25 : -0.25)};
     {
       auto ce = place_surface(ops.usurf, cc, 0.25, kRad0);
       auto pc = place_surface(ops.usurf, zero, 0.5, kRad1);
-      std::vector<double> M((size_t)dim * dim);
+      std::vector<double> M((size_t)din * dout);
       exp_kernel_matrix(ki.exp_kernel, ce.data(), ns, pc.data(), ns, M.data());
-      auto T = matmul(matmul(M, ops.uc2ue0, dim, dim, dim), ops.uc2ue1, dim, dim, dim);
-      std::memcpy(&ops.u2u[(size_t)c * dim * dim], T.data(), sizeof(double) * dim * dim);
+      auto T = matmul(matmul(M, ops.uc2ue0, din, dout, rk), ops.uc2ue1, din, rk, din);
+      std::memcpy(&ops.u2u[(size_t)c * din * din], T.data(), sizeof(double) * din * din);
     }
     // D2D (:607-643): DC2DE0 * (DC2DE1 * M_pe2c), parent level 0 -> child c.
     {
       auto pe = place_surface(ops.usurf, zero, 0.5, kRad1);
       auto cc2 = place_surface(ops.usurf, cc, 0.25, kRad0);
-      std::vector<double> M((size_t)dim * dim);
+      std::vector<double> M((size_t)din * dout);
       exp_kernel_matrix(ki.exp_kernel, pe.data(), ns, cc2.data(), ns, M.data());
-      auto T = matmul(ops.dc2de0, matmul(ops.dc2de1, M, dim, dim, dim), dim, dim, dim);
-      for (int r = 0; r < dim; ++r)
-        std::memcpy(&ops.d2d[(size_t)r * 8 * dim + (size_t)c * dim], &T[(size_t)r * dim], sizeof(double) * dim);
+      auto T = matmul(ops.dc2de0, matmul(ops.dc2de1, M, rk, din, dout), dout, rk, dout);
+      for (int r = 0; r < dout; ++r)
+        std::memcpy(&ops.d2d[(size_t)r * 8 * dout + (size_t)c * dout], &T[(size_t)r * dout], sizeof(double) * dout);
     }
   }
   // FFT maps (:2703-2712, :2790-2797): lattice index s = (u+1)(m-1)/2.
@@ -464,7 +546,7 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
   // V operators (:671-718): for source-minus-target child offset rel (child
   // units, box 1), kernel from the conv grid (i-m)*RAD0/(m-1)+rel to the
   // origin, then a 3D r2c DFT with x the halved axis.
-  const int n3 = ops.n3, nh = n1 / 2 + 1, n3h = ops.n3h, kk = ke * ke;
+  const int n3 = ops.n3, nh = n1 / 2 + 1, n3h = ops.n3h, kk = kin * kout;
   std::vector<std::complex<double>> w(n1);
   for (int j = 0; j < n1; ++j) w[j] = std::polar(1.0, -2 * kPi * j / n1);
   std::vector<std::vector<std::complex<double>>> vhat(343);  // index (i+3)+7(j+3)+49(k+3)
@@ -482,7 +564,7 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
           grid[g * 3 + 2] = (k - m) * kRad0 / (m - 1) + rk;
         }
     std::vector<double> P((size_t)n3 * kk);
-    exp_kernel_matrix(ki.exp_kernel, grid.data(), n3, zero, 1, P.data());  // P[g*ke+i][k]
+    exp_kernel_matrix(ki.exp_kernel, grid.data(), n3, zero, 1, P.data());  // P[g*kin+i][k]
     std::vector<std::complex<double>> out((size_t)n3h * kk);
     std::vector<std::complex<double>> cube((size_t)n3), tmp(n1);
     for (int comp = 0; comp < kk; ++comp) {

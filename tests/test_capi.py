@@ -57,6 +57,26 @@ def test_library_operators_reproduce_oracle_fmm(kid, m):
     assert abs(O.rel_l2(a, ref) - err) < 1e-2 * err
 
 
+@pytest.mark.parametrize("kid", [2, 4, 5])
+def test_self_expanded_kernel_operators_reproduce_oracle_fmm(kid):
+    """Stokes pressure (3->1), Stokes velocity gradient (3->9) and Biot-Savart
+    (3->3) expand themselves, with rectangular check->equivalent factors: the
+    library's host precompute drives the oracle FMM to the same result as the
+    oracle's own operators.  The CUDA evaluation does not take these kernels
+    yet: creating a context for one is an error."""
+    K = O.KERNELS[kid]
+    ops_lib = O.Operators.from_arrays(K, 4, P.precomp_operators(P.FMMKernel(kid), 4))
+    rng = np.random.default_rng(50 + kid)
+    x = rng.random((1200, 3))
+    f = rng.standard_normal((1200, 3))
+    a = O.pvfmm_eval(kid, 4, 60, x, f, x, ops=ops_lib)
+    b = O.pvfmm_eval(kid, 4, 60, x, f, x)
+    assert O.rel_l2(a, b) < 1e-3 * O.rel_l2(b, O.direct_sum(kid, x, f, x))
+    lib = P.load_library()
+    assert not lib.PVFMMCreateContextExD(-1.0, 100, 4, kid, 0)
+    assert "unsupported" in P.last_error()
+
+
 def test_stokes_operators_reproduce_oracle_fmm():
     K = O.KERNELS[3]
     ops_lib = O.Operators.from_arrays(K, 4, P.precomp_operators(P.FMMKernel.StokesVelocity, 4))

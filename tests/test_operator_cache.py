@@ -61,8 +61,11 @@ def cache_dir(tmp_path, monkeypatch):
     P.precomp_operator(K.LaplacePotential, 2, 0, 0)  # drop the operator set built with the cache
 
 
-@pytest.mark.parametrize("kernel,m,name", [(K.LaplacePotential, 4, "laplace"), (K.StokesVelocity, 4, "stokes_vel")])
-def test_cache_is_written_and_reread_bit_identically(monkeypatch, cache_dir, kernel, m, name):
+@pytest.mark.parametrize("kernel,m,name,kin,kout", [(K.LaplacePotential, 4, "laplace", 1, 1),
+                                                    (K.StokesVelocity, 4, "stokes_vel", 3, 3),
+                                                    (K.StokesPressure, 4, "stokes_press", 3, 1),
+                                                    (K.StokesVelocityGrad, 4, "stokes_grad", 3, 9)])
+def test_cache_is_written_and_reread_bit_identically(monkeypatch, cache_dir, kernel, m, name, kin, kout):
     monkeypatch.delenv("PVFMM_DIR")
     ref = _all(kernel, m, 0)
     monkeypatch.setenv("PVFMM_DIR", str(cache_dir))
@@ -73,11 +76,13 @@ def test_cache_is_written_and_reread_bit_identically(monkeypatch, cache_dir, ker
     for a, b, c in zip(ref, written, reread):
         assert np.array_equal(a, b) and np.array_equal(a, c)
     types = _read_reference_layout(path)
-    dim = int(np.sqrt(ref[0].size))
+    ns = 6 * (m - 1) ** 2 + 2
+    din, dout = ns * kin, ns * kout
+    r = min(din, dout)
     for t in range(4):
         assert len(types[t]) == 1
         n1, n2, data = types[t][0]
-        assert (n1, n2) == (dim, dim) and np.array_equal(data, ref[t])
+        assert (n1, n2) == ((r, din) if t & 1 else (dout, r)) and np.array_equal(data, ref[t])
     assert all(len(types[t]) == 0 for t in range(4, 16))
 
 
