@@ -232,14 +232,23 @@ def run_reference(args, world, rank):
     t_ops = time.perf_counter()
     ops = O.Operators(O.KERNELS[W["kernel"]], W["m"])     # context creation, outside the timed steps
     ops_ms = 1000 * (time.perf_counter() - t_ops)
-    times = []
+    times, stages = [], {}
     ctxm = threadpool_limits(limits=cores) if threadpool_limits else None
+    fmm = None
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], xs, qs, xs, ops=ops)
+        _, fmm = O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], xs, qs, xs, ops=ops, return_fmm=True)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             times.append(dt)
+            for k, v in fmm.stage_ms.items():
+                stages[k] = stages.get(k, 0.0) + v / args.steps
+    # setup=0 (same points, new densities): the last step's tree reused
+    setup0_ms = None
+    if fmm is not None:
+        t0 = time.perf_counter()
+        O.pvfmm_eval_setup0(fmm, qs)
+        setup0_ms = 1000 * (time.perf_counter() - t0)
     if ctxm is not None:
         ctxm.unregister() if hasattr(ctxm, "unregister") else None
     ms = 1000 * float(np.mean(times))
@@ -252,6 +261,9 @@ def run_reference(args, world, rank):
             "config": {"workload": W["desc"].format(n=args.n) + f" (bounded CPU sample: {n_sample} points)"},
             "impl": "reference",
             "context_create_ms": ops_ms,
+            "stages_ms": stages,
+            "setup0_ms": setup0_ms,
+            "setup0_targets_per_s": n_sample / (setup0_ms / 1000) if setup0_ms else None,
             "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import bisect
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -774,6 +775,15 @@ class FMM:
         def pts_rel(arr, lo, hi, T):
             return arr[lo:hi] - self._corner(T)
 
+        # wall time per stage (ms), named as the library's stage times
+        stage = self.stage_ms = {k: 0.0 for k in ("S2U", "U2U", "X-List", "V-List", "D2D", "D2T+W+U")}
+        clock = [time.perf_counter()]
+
+        def tick(name):
+            now = time.perf_counter()
+            stage[name] += 1000 * (now - clock[0])
+            clock[0] = now
+
         # --- S2U (fmm_pts.txx:2275-2637 + EvalListPts 4390-4426) ---------
         # The two pseudo-inverse factors are applied one after the other, as
         # the reference does: multiplying them out first loses the accuracy.
@@ -783,6 +793,7 @@ class FMM:
                 chk = ke.eval(pts_rel(self.src, n.src[0], n.src[1], n), den[n.src[0]:n.src[1]],
                               u_check_surf(m, z3, n.depth))
                 ue[i] = ((chk.reshape(-1) * 2.0 ** (-e_exp * n.depth)) @ ops.uc2ue0) @ ops.uc2ue1
+        tick("S2U")
         # --- U2U bottom-up (fmm_pts.txx:2602-2630, EvalList) ------------
         for d in range(tree.depth - 1, -1, -1):
             for i in range(tree.level_start[d], tree.level_start[d + 1]):
@@ -793,6 +804,7 @@ class FMM:
                 for c in range(8):
                     acc += ue[n.child0 + c] @ ops.u2u[c]
                 ue[i] = acc
+        tick("U2U")
         p2p, xl, wl, v1 = self.lists
         # --- X-list (fmm_pts.txx:4444-4736) ------------------------------
         for t, srcs in xl.items():
@@ -801,6 +813,7 @@ class FMM:
             for s in srcs:
                 S = N[s]
                 dc[t] += ke.eval(pts_rel(self.src, S.src[0], S.src[1], T), den[S.src[0]:S.src[1]], pts).reshape(-1)
+        tick("X-List")
         # --- W-list (fmm_pts.txx:4746-5022) ------------------------------
         for t, srcs in wl.items():
             T = N[t]
@@ -816,8 +829,10 @@ class FMM:
             idx = np.concatenate([np.arange(N[s].src[0], N[s].src[1]) for s in srcs])
             out[T.trg[0]:T.trg[1]] += kt.eval(self.src[idx] - self._corner(T), den[idx],
                                               pts_rel(self.trg, T.trg[0], T.trg[1], T))
+        tick("D2T+W+U")
         # --- V-list via FFT (fmm_pts.txx:3597-3759, 2689-2858) ----------
         self._vlist(ue, dc, v1)
+        tick("V-List")
         # --- D2D top-down (fmm_pts.txx:3762-3790) ------------------------
         for d in range(0, tree.depth):
             for i in range(tree.level_start[d], tree.level_start[d + 1]):
@@ -826,12 +841,14 @@ class FMM:
                     continue
                 for c in range(8):
                     dc[n.child0 + c] += dc[i] @ ops.d2d[c]
+        tick("D2D")
         # --- D2T (fmm_pts.txx:5427-5737) ---------------------------------
         for i, n in enumerate(N):
             if n.leaf and n.n_trg > 0:
                 de = ((dc[i] * 2.0 ** (-e_exp * n.depth)) @ ops.dc2de0) @ ops.dc2de1
                 out[n.trg[0]:n.trg[1]] += kt.eval(d_equiv_surf(m, z3, n.depth), de,
                                                   pts_rel(self.trg, n.trg[0], n.trg[1], n))
+        tick("D2T+W+U")
         self.ue, self.dc = ue, dc
         return out
 
@@ -893,15 +910,31 @@ def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, o
     src_scal = np.array([scale ** e for e in K.src_scal])
     trg_scal = np.array([scale ** e for e in K.trg_scal])
     fmm = FMM(kernel_id, m, max_pts, ops)
+    t0 = time.perf_counter()
     fmm.setup(src_c, trg_c)
+    setup_ms = 1000 * (time.perf_counter() - t0)
     den = (sl_den * src_scal[None, :])[fmm.src_perm]
     out_sorted = fmm.evaluate(den)
+    fmm.stage_ms["setup"] = setup_ms
     out = np.empty_like(out_sorted)
     out[fmm.trg_perm] = out_sorted
     out = out * trg_scal[None, :]
+    fmm.io_scal = (src_scal, trg_scal)
     if return_fmm:
         return out, fmm
     return out
+
+
+def pvfmm_eval_setup0(fmm: "FMM", sl_den) -> np.ndarray:
+    """PVFMMEvalD with setup=0 (src/pvfmm-wrapper.cpp:637-654): the tree of a
+    previous pvfmm_eval(..., return_fmm=True) on the same points, new
+    densities."""
+    src_scal, trg_scal = fmm.io_scal
+    den = (np.asarray(sl_den, dtype=np.float64).reshape(-1, fmm.kernel.k0) * src_scal[None, :])[fmm.src_perm]
+    out_sorted = fmm.evaluate(den)
+    out = np.empty_like(out_sorted)
+    out[fmm.trg_perm] = out_sorted
+    return out * trg_scal[None, :]
 
 
 def ptfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None):

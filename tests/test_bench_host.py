@@ -79,3 +79,28 @@ def test_ellipsoid_points_lie_on_the_surface():
     x, _ = bench.make_points(bench.WORKLOADS["ellipsoid30m"], 5000)
     a = np.array([0.45, 0.3, 0.15])
     assert np.allclose((((x - 0.5) / a) ** 2).sum(1), 1.0, atol=1e-12)
+
+
+def test_reference_arm_line(capsys):
+    """The reference arm's JSON line: the oracle on a bounded sample, with the
+    per-stage split, the setup=0 rate and the operator build time."""
+    import json
+
+    class Args:
+        ref_sample, n, warmup, steps, workload = 1500, 20000, 0, 1, "gaussian4m"
+    bench.run_reference(Args, 1, 0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert set(line["stages_ms"]) == {"setup", "S2U", "U2U", "X-List", "V-List", "D2D", "D2T+W+U"}
+    assert line["setup0_targets_per_s"] > line["value"]     # no tree build
+    assert line["context_create_ms"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_oracle_setup0_equals_a_fresh_evaluation():
+    from oracle import pvfmm_oracle as O
+    rng = np.random.default_rng(1)
+    x = rng.random((1500, 3))
+    q1, q2 = rng.uniform(-1, 1, 1500), rng.uniform(-1, 1, 1500)
+    _, fmm = O.pvfmm_eval(6, 4, 60, x, q1, x, return_fmm=True)
+    assert np.array_equal(O.pvfmm_eval_setup0(fmm, q2), O.pvfmm_eval(6, 4, 60, x, q2, x))
