@@ -8,7 +8,8 @@ mortonid_ref.npz   outputs of the reference's own Morton-id code
 oracle_*.npz       small FMM cases of the oracle (inputs, leaf ids, outputs),
                    regression pins of the oracle itself.
 
-Run:  python tests/golden/make_golden.py
+Run:  python tests/golden/make_golden.py [--force]   (existing oracle_*.npz are
+kept unless --force)
 """
 import ctypes
 import os
@@ -57,13 +58,18 @@ def morton_golden():
                         nbr_of=sub2, nbrs=nb.reshape(len(sub2), 27, 4))
 
 
-def oracle_golden():
+def oracle_golden(force=False):
     cases = {
         "laplace_m4": (0, 4, 40, 1200, False),
         "stokes_m4": (3, 4, 40, 600, False),
         "laplace_potgrad_m6": (6, 6, 50, 1500, True),
+        "stokes_press_m4": (2, 4, 40, 600, False),
+        "stokes_grad_m4": (4, 4, 40, 600, True),
+        "biot_savart_m4": (5, 4, 40, 600, False),
     }
     for name, (kid, m, mp, n, sep) in cases.items():
+        if not force and os.path.exists(os.path.join(HERE, f"oracle_{name}.npz")):
+            continue
         rng = np.random.default_rng(100 + kid + m)
         K = O.KERNELS[kid]
         src = rng.random((n, 3))
@@ -77,5 +83,5 @@ def oracle_golden():
 if __name__ == "__main__":
     if os.path.isdir("/root/reference"):
         morton_golden()
-    oracle_golden()
+    oracle_golden(force="--force" in sys.argv)
     print("golden fixtures written to", HERE)

@@ -192,7 +192,8 @@ def _children(ids):
 
 
 # --- committed golden fixtures of the oracle
-@pytest.mark.parametrize("name", ["laplace_m4", "stokes_m4", "laplace_potgrad_m6"])
+@pytest.mark.parametrize("name", ["laplace_m4", "stokes_m4", "laplace_potgrad_m6", "stokes_press_m4",
+                                  "stokes_grad_m4", "biot_savart_m4"])
 def test_oracle_golden_fixture(name):
     g = np.load(os.path.join(GOLDEN, f"oracle_{name}.npz"))
     out, fmm = O.pvfmm_eval(int(g["kernel"]), int(g["m"]), int(g["max_pts"]), g["src"], g["den"], g["trg"],
