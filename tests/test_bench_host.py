@@ -104,3 +104,51 @@ def test_oracle_setup0_equals_a_fresh_evaluation():
     q1, q2 = rng.uniform(-1, 1, 1500), rng.uniform(-1, 1, 1500)
     _, fmm = O.pvfmm_eval(6, 4, 60, x, q1, x, return_fmm=True)
     assert np.array_equal(O.pvfmm_eval_setup0(fmm, q2), O.pvfmm_eval(6, 4, 60, x, q2, x))
+
+
+def _form(tps, err, comps, rb):
+    return {"ms_per_step": 4e6 / tps * 1000, "targets_per_s": tps, "rel_l2": err, "rel_l2_components": comps,
+            "stages_ms": {"V-Hadamard": 10.0, "near-field kernel": 12.0}, "gpu_launches": 178.0,
+            "clocks": {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 7},
+            "e2e_targets_per_s": 0.9 * tps, "real_bytes": rb,
+            "stats": dict(STATS_1M, n_vsrc=15240.0, n_vtrg=15237.0, n_trg=4e6, n_src=4e6)}
+
+
+class _Args:
+    steps, warmup = 20, 3
+
+
+def test_json_line_follows_the_contract():
+    forms = {"plain": _form(58e6, 2.1e-7, [6e-8, 2.5e-7, 1.8e-7, 2.0e-7], 8),
+             "mixed": _form(109e6, 5.5e-7, [2.3e-7, 6.4e-7, 4.8e-7, 5.6e-7], 4)}
+    line = bench.build_line(_Args, 1, 4_000_000, forms, {"hbm_gbs": 6449.1})
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "clocks", "roofline"):
+        assert key in line, key
+    assert line["form"] == "mixed" and line["value"] == 109e6 and line["dtype"] == "f32"
+    assert line["higher_is_better"] is True and line["scaling"] == "weak" and line["vs_baseline"] is None
+    assert line["mixed_over_plain"] == pytest.approx(109 / 58)
+    # inputs (positions + densities) in, pot+grad values out, FP64 host buffers
+    assert line["e2e"]["h2d_bytes_per_step"] == 4_000_000 * (3 + 1) * 8
+    assert line["e2e"]["d2h_bytes_per_step"] == 4_000_000 * 4 * 8
+    r = line["roofline"]
+    assert set(r) >= {"bound", "achieved", "peak", "unit", "frac", "traffic"} and r["bound"] in ("hbm", "tensor")
+    assert r["peak_source"] == "measured" and r["traffic"] > 0
+
+
+def test_a_form_over_the_bar_in_one_component_is_not_reported():
+    forms = {"plain": _form(58e6, 2.1e-7, [6e-8, 2.5e-7, 1.8e-7, 2.0e-7], 8),
+             "mixed": _form(109e6, 5.5e-7, [2.3e-7, 1.2e-6, 4.8e-7, 5.6e-7], 4)}   # one component > 1e-6
+    line = bench.build_line(_Args, 1, 4_000_000, forms, {})
+    assert line["form"] == "plain" and line["dtype"] == "f64"
+    assert line["roofline"]["peak_source"] == "fallback"
+
+
+def test_a_form_that_failed_is_kept_in_the_line():
+    forms = {"plain": {"error": "device allocation failed"},
+             "mixed": _form(109e6, 5.5e-7, [2.3e-7, 6.4e-7, 4.8e-7, 5.6e-7], 4)}
+    line = bench.build_line(_Args, 2, 4_000_000, forms, {})
+    assert line["form"] == "mixed" and line["forms"]["plain"]["error"]
+    assert line["mixed_over_plain"] is None and line["n_gpus"] == 2
+    with pytest.raises(RuntimeError, match="no form completed"):
+        bench.build_line(_Args, 1, 4_000_000, {"plain": {"error": "x"}}, {})
