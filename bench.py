@@ -379,6 +379,7 @@ def build_line(args, world, N, forms, peaks):
     ok = [f for f in forms_ok if max([forms_ok[f]["rel_l2"]] + forms_ok[f]["rel_l2_components"]) <= TOL]
     best = max(ok, key=lambda f: forms_ok[f]["targets_per_s"]) if ok else next(iter(forms_ok))
     B = forms[best]
+    worst = max([B["rel_l2"]] + B["rel_l2_components"])
     roof = roofline(B, peaks)
     return {
         "metric": METRIC,
@@ -397,6 +398,9 @@ def build_line(args, world, N, forms, peaks):
                    "l2": "no flush: per-step working set (128 MB inputs + tree + GB-size spectra) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
         "form": best,
+        "meets_bar": bool(ok),
+        "rel_l2_worst_component": worst,
+        "rel_l2_bar": TOL,
         "forms": forms,
         "mixed_over_plain": (forms_ok["mixed"]["targets_per_s"] / forms_ok["plain"]["targets_per_s"]
                              if "mixed" in forms_ok and "plain" in forms_ok else None),

@@ -158,7 +158,9 @@ int PVFMMKernelEvalD(enum PVFMMKernel kernel, const double* src_pos, const doubl
  * counterpart in the reference.  The partial sums use a fixed 8 MiB array in
  * the library's device image instead of allocated scratch, so
  * n_trg * k1 <= 1048576 (larger requests return an error).  The first call on
- * a device looks up the array's address; make it before any stream capture.
+ * a device looks up the array's address and keeps it for the life of the
+ * process (it is stale after cudaDeviceReset); make that call before any
+ * stream capture.
  * All calls share the array: calls that overlap on the GPU race, and the
  * caller must serialise them.  Returns 0 on success. */
 int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const double* src_pos, const double* den, long n_src,

@@ -462,6 +462,61 @@ class Tree:
 # ----------------------------------------------------------------------------
 # Interaction lists (interac_list.txx:98-279, fmm_tree.txx:301-352)
 # ----------------------------------------------------------------------------
+def raw_lists(tree: Tree) -> dict:
+    """The reference's interaction lists before any reassignment
+    (InteracList::BuildList, interac_list.txx:98-279), built for every node
+    with targets in its subtree (FMM_Tree::BuildInteracLists,
+    fmm_tree.txx:301-352): ``{list name: {owner node: [member nodes]}}`` with
+    lists U0 (adjacent coarser leaves, leaf owners), U1 (leaf colleagues incl.
+    self, leaf owners), U2 (adjacent children of non-leaf colleagues, leaf
+    owners), W (non-adjacent children of non-leaf colleagues, leaf owners),
+    X (non-adjacent coarser leaves: leaf colleagues of the parent) and V1
+    (non-leaf colleagues except self, non-leaf owners).  Members are kept
+    whether or not they hold sources."""
+    N = tree.nodes
+    out = {k: {} for k in ("U0", "U1", "U2", "W", "X", "V1")}
+    for ti, T in enumerate(N):
+        if T.n_trg == 0:
+            continue
+        L = {k: [] for k in out}
+        if T.leaf:
+            for ci in range(27):
+                c = T.colleagues[ci]
+                if c < 0:
+                    continue
+                if N[c].leaf:
+                    L["U1"].append(c)
+                    continue
+                C = N[c]
+                for j in range(8):
+                    rel = [(ci % 3) * 4 - 4 + (2 if j & 1 else 0) - 1,
+                           ((ci // 3) % 3) * 4 - 4 + (2 if j & 2 else 0) - 1,
+                           (ci // 9) * 4 - 4 + (2 if j & 4 else 0) - 1]
+                    L["U2" if max(abs(r) for r in rel) <= 3 else "W"].append(C.child0 + j)
+        if T.parent >= 0:
+            par, p2n = N[T.parent], T.path
+            for ci in range(27):
+                c = par.colleagues[ci]
+                if c >= 0 and N[c].leaf:
+                    rel = [(ci % 3) * 4 - 4 - (2 if p2n & 1 else 0) + 1,
+                           ((ci // 3) % 3) * 4 - 4 - (2 if p2n & 2 else 0) + 1,
+                           (ci // 9) * 4 - 4 - (2 if p2n & 4 else 0) + 1]
+                    if max(abs(r) for r in rel) <= 3:
+                        if T.leaf:
+                            L["U0"].append(c)
+                    else:
+                        L["X"].append(c)
+        if not T.leaf:
+            for ci in range(27):
+                c = T.colleagues[ci]
+                if ci != 13 and c >= 0 and not N[c].leaf:
+                    L["V1"].append(c)
+        for k, v in L.items():
+            if v:
+                out[k][ti] = v
+    return out
+
+
 def build_lists(tree: Tree, nsrf: int):
     """Per-target-node lists after the Nsrf reassignment:
 
@@ -472,62 +527,26 @@ def build_lists(tree: Tree, nsrf: int):
     ``w[t]``     source nodes (upward equivalent surface) -> targets of leaf t
                  (fmm_pts.txx:4929)
     ``v1[t]``    (source parent, colleague index) pairs for non-leaf t (V1 list)
-    Only nodes with targets get lists; only sources with points are kept.
+    Built from the reference's raw lists (raw_lists); only sources with points
+    are kept.
     """
     N = tree.nodes
+    raw = raw_lists(tree)
     p2p, xl, wl, v1 = {}, {}, {}, {}
     for ti, T in enumerate(N):
         if T.n_trg == 0:
             continue
-        par = N[T.parent] if T.parent >= 0 else None
-        p2n = T.path
-        U, X, W, V = [], [], [], []
-        if T.leaf:
-            # U1: leaf colleagues (incl. self)
-            for ci in range(27):
-                c = T.colleagues[ci]
-                if c >= 0 and N[c].leaf:
-                    U.append(c)
-            for ci in range(27):
-                c = T.colleagues[ci]
-                if c >= 0 and not N[c].leaf:
-                    C = N[c]
-                    for j in range(8):
-                        rel = [(ci % 3) * 4 - 4 + (2 if j & 1 else 0) - 1,
-                               ((ci // 3) % 3) * 4 - 4 + (2 if j & 2 else 0) - 1,
-                               (ci // 9) * 4 - 4 + (2 if j & 4 else 0) - 1]
-                        if max(abs(r) for r in rel) <= 3:
-                            U.append(C.child0 + j)          # U2 (adjacent children)
-                        else:
-                            W.append(C.child0 + j)          # W (non-adjacent children)
-        if par is not None:
-            for ci in range(27):
-                c = par.colleagues[ci]
-                if c >= 0 and N[c].leaf:
-                    rel = [(ci % 3) * 4 - 4 - (2 if p2n & 1 else 0) + 1,
-                           ((ci // 3) % 3) * 4 - 4 - (2 if p2n & 2 else 0) + 1,
-                           (ci // 9) * 4 - 4 - (2 if p2n & 4 else 0) + 1]
-                    if max(abs(r) for r in rel) <= 3:
-                        if T.leaf:
-                            U.append(c)                     # U0 (adjacent coarser leaf)
-                    else:
-                        X.append(c)                         # X (non-adjacent coarser leaf)
-        if not T.leaf:
-            for ci in range(27):
-                c = T.colleagues[ci]
-                if ci != 13 and c >= 0 and not N[c].leaf and N[c].n_src > 0:
-                    V.append((c, ci))
-        # Nsrf reassignment
-        P = [s for s in U if N[s].leaf and N[s].n_src > 0]
+        U = raw["U1"].get(ti, []) + raw["U2"].get(ti, []) + raw["U0"].get(ti, [])
+        P = [s for s in U if N[s].n_src > 0]
         Xk, Wk = [], []
-        for s in X:
+        for s in raw["X"].get(ti, []):
             if N[s].n_src == 0:
                 continue
             if T.leaf and T.n_trg <= nsrf:
                 P.append(s)
             else:
                 Xk.append(s)
-        for s in W:
+        for s in raw["W"].get(ti, []):
             S = N[s]
             if S.n_src == 0:
                 continue
@@ -539,6 +558,7 @@ def build_lists(tree: Tree, nsrf: int):
             p2p[ti] = P
             wl[ti] = Wk
         xl[ti] = Xk
+        V = [(c, T.colleagues.index(c)) for c in raw["V1"].get(ti, []) if N[c].n_src > 0]
         if V:
             v1[ti] = V
     return p2p, xl, wl, v1

@@ -1,0 +1,104 @@
+// Test-infrastructure driver around the reference's own C interface
+// (src/pvfmm-wrapper.cpp, compiled here from the reference's sources over the
+// stand-ins in shim/).  It adds read-only access to the reference's octree
+// and interaction lists after an evaluation, so that the oracle's tree, lists
+// and FMM values can be pinned to the reference's, and a stage-time hook for
+// the CPU baseline.  Nothing of the product library links this.
+#include "pvfmm-wrapper.cpp"
+
+#include <omp.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+
+extern "C" void scipy_openblas_set_num_threads(int);
+
+namespace {
+typedef pvfmm::FMM_Node<pvfmm::MPI_Node<double> > RefNode;
+
+// The reference calls BLAS from inside its OpenMP loops (one GEMM per block
+// per thread), so the BLAS library itself runs single-threaded.
+__attribute__((constructor)) void single_threaded_blas() { scipy_openblas_set_num_threads(1); }
+
+// (X, Y, Z, depth) of a node's Morton id, X in units of 2^-30.
+void node_key(RefNode* n, int64_t* out) {
+  double c[3];
+  n->GetMortonId().GetCoord(c);
+  for (int k = 0; k < 3; ++k) out[k] = (int64_t)(c[k] * (double)(1u << 30) + 0.5);
+  out[3] = n->Depth();
+}
+
+std::vector<RefNode*> nodes_of(const void* ctx_) {
+  PVFMMContext<double>* ctx = (PVFMMContext<double>*)ctx_;
+  std::vector<RefNode*> out;
+  std::vector<RefNode*>& all = ctx->tree->GetNodeList();
+  for (RefNode* n : all)
+    if (!n->IsGhost()) out.push_back(n);
+  return out;
+}
+}  // namespace
+
+extern "C" {
+
+// Nodes of the last tree, one record of 10 int64 per node in the tree's node
+// order: X, Y, Z, depth, leaf, #sources, #targets (points held by the leaf),
+// pt_cnt[0], pt_cnt[1], 0.  Returns the node count; writes at most cap records.
+long ref_tree_nodes(const void* ctx, int64_t* out, long cap) {
+  std::vector<RefNode*> nodes = nodes_of(ctx);
+  for (long i = 0; i < (long)nodes.size() && i < cap; ++i) {
+    RefNode* n = nodes[i];
+    int64_t* r = out + 10 * i;
+    node_key(n, r);
+    r[4] = n->IsLeaf() ? 1 : 0;
+    r[5] = (int64_t)(n->src_coord.Dim() / 3);
+    r[6] = (int64_t)(n->trg_coord.Dim() / 3);
+    r[7] = (int64_t)n->pt_cnt[0];
+    r[8] = (int64_t)n->pt_cnt[1];
+    r[9] = 0;
+  }
+  return (long)nodes.size();
+}
+
+// Interaction-list entries of the last tree, one record of 6 int64 per
+// non-empty slot: owner node index (tree node order), list type (the
+// reference's Mat_Type: U0 8, U1 9, U2 10, W 12, X 13, V1 14), slot, member
+// node index, 0, 0.  Returns the record count; writes at most cap records.
+long ref_tree_lists(const void* ctx, int64_t* out, long cap) {
+  std::vector<RefNode*> nodes = nodes_of(ctx);
+  std::map<RefNode*, long> index;
+  for (long i = 0; i < (long)nodes.size(); ++i) index[nodes[i]] = i;
+  const int types[] = {pvfmm::U0_Type, pvfmm::U1_Type, pvfmm::U2_Type, pvfmm::W_Type, pvfmm::X_Type, pvfmm::V1_Type};
+  long cnt = 0;
+  for (long i = 0; i < (long)nodes.size(); ++i)
+    for (int t : types) {
+      pvfmm::Vector<RefNode*>& L = nodes[i]->interac_list[t];
+      for (size_t s = 0; s < L.Dim(); ++s) {
+        if (!L[s]) continue;
+        auto it = index.find(L[s]);
+        if (cnt < cap) {
+          int64_t* r = out + 6 * cnt;
+          r[0] = i;
+          r[1] = t;
+          r[2] = (int64_t)s;
+          r[3] = it == index.end() ? -1 : it->second;
+          r[4] = r[5] = 0;
+        }
+        ++cnt;
+      }
+    }
+  return cnt;
+}
+
+// Sets the number of OpenMP threads the reference uses (0 leaves the
+// current setting) and returns the count in effect.
+int ref_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+}
+
+// Enables the reference's profiler (pvfmm::Profile, the per-stage tags of
+// fmm_tree.txx / fmm_pts.txx) for the following evaluations.
+void ref_profile_enable(int on) { pvfmm::Profile::Enable(on != 0); }
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+"""ctypes access to the reference PVFMM built from its own sources
+(``oracle/ref_fmm/build.sh`` -> ``oracle/_ref/libpvfmm_ref_<isa>.so``).
+
+Test infrastructure: the golden-fixture generator, the tests that pin the
+oracle and the CPU-baseline arm of bench.py use it.  It calls the reference's
+C interface (``PVFMMCreateContextDWorld`` / ``PVFMMEvalD`` /
+``PVFMMDestroyContextD``, src/pvfmm-wrapper.cpp:877-928) and the driver's
+read-only tree and list dumps (``ref_driver.cpp``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(os.path.dirname(HERE), "_ref")
+
+# reference Mat_Type values of the interaction lists (include/precomp_mat.hpp:21-38)
+U0, U1, U2, W, X, V1 = 8, 9, 10, 12, 13, 14
+
+_lib = None
+
+
+def _isa() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+    except OSError:
+        return "avx2"
+    return "avx512" if " avx512f" in flags and " avx512dq" in flags and " avx512vl" in flags else "avx2"
+
+
+def library_path(isa: str | None = None) -> str:
+    return os.path.join(REF_DIR, f"libpvfmm_ref_{isa or _isa()}.so")
+
+
+def available() -> bool:
+    return os.path.exists(library_path())
+
+
+def load():
+    """Loads the reference library for this host's instruction set.  The
+    reference reads and writes its precompute files in $PVFMM_DIR (or the
+    working directory); a private temporary directory is used when unset."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"reference library not built: {path} (run oracle/ref_fmm/build.sh)")
+    if not os.environ.get("PVFMM_DIR"):
+        os.environ["PVFMM_DIR"] = tempfile.mkdtemp(prefix="pvfmm_ref_precomp_")
+    lib = ctypes.CDLL(path)
+    vp, lg = ctypes.c_void_p, ctypes.c_long
+    lib.PVFMMCreateContextDWorld.restype = vp
+    lib.PVFMMCreateContextDWorld.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.PVFMMEvalD.restype = None
+    lib.PVFMMEvalD.argtypes = [vp, vp, vp, lg, vp, vp, lg, vp, ctypes.c_int]
+    lib.PVFMMDestroyContextD.restype = None
+    lib.PVFMMDestroyContextD.argtypes = [ctypes.POINTER(vp)]
+    lib.ref_tree_nodes.restype = lg
+    lib.ref_tree_nodes.argtypes = [vp, vp, lg]
+    lib.ref_tree_lists.restype = lg
+    lib.ref_tree_lists.argtypes = [vp, vp, lg]
+    lib.ref_set_threads.restype = ctypes.c_int
+    lib.ref_set_threads.argtypes = [ctypes.c_int]
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+# PVFMMKernel ids of the reference (include/pvfmm.h:21-28) -> (k0, k1)
+KDIM = {0: (1, 1), 1: (1, 3), 2: (3, 1), 3: (3, 3), 4: (3, 9), 5: (3, 3)}
+
+
+class RefContext:
+    """A reference PVFMM context: free space (box_size = -1), `max_pts`
+    points per leaf, multipole order m, kernel id of the C interface."""
+
+    def __init__(self, kernel: int, m: int, max_pts: int, threads: int = 0):
+        self.lib = load()
+        if threads:
+            self.lib.ref_set_threads(threads)
+        self.kernel = kernel
+        self.k0, self.k1 = KDIM[kernel]
+        self.ctx = self.lib.PVFMMCreateContextDWorld(-1.0, max_pts, m, kernel)
+        if not self.ctx:
+            raise RuntimeError("reference context creation failed")
+
+    def evaluate(self, src, den, trg, setup=True) -> np.ndarray:
+        src = np.ascontiguousarray(src, dtype=np.float64).reshape(-1)
+        den = np.ascontiguousarray(den, dtype=np.float64).reshape(-1)
+        same = trg is None
+        trg = src if same else np.ascontiguousarray(trg, dtype=np.float64).reshape(-1)
+        n_src, n_trg = len(src) // 3, len(trg) // 3
+        out = np.zeros(n_trg * self.k1)
+        self.lib.PVFMMEvalD(_p(src), _p(den), None, n_src, _p(trg), _p(out), n_trg, ctypes.c_void_p(self.ctx),
+                            1 if setup else 0)
+        return out.reshape(n_trg, self.k1)
+
+    def tree(self):
+        """Nodes of the last tree: int64 array (n, 10) with X, Y, Z (units of
+        2^-30), depth, leaf, #sources and #targets held, pt_cnt[0], pt_cnt[1]."""
+        n = self.lib.ref_tree_nodes(ctypes.c_void_p(self.ctx), None, 0)
+        a = np.zeros((n, 10), dtype=np.int64)
+        self.lib.ref_tree_nodes(ctypes.c_void_p(self.ctx), _p(a), n)
+        return a
+
+    def lists(self):
+        """Interaction-list entries of the last tree: int64 array (n, 6) with
+        owner node index, list type (U0 8, U1 9, U2 10, W 12, X 13, V1 14),
+        slot, member node index."""
+        n = self.lib.ref_tree_lists(ctypes.c_void_p(self.ctx), None, 0)
+        a = np.zeros((n, 6), dtype=np.int64)
+        self.lib.ref_tree_lists(ctypes.c_void_p(self.ctx), _p(a), n)
+        return a
+
+    def close(self):
+        if self.ctx:
+            c = ctypes.c_void_p(self.ctx)
+            self.lib.PVFMMDestroyContextD(ctypes.byref(c))
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0):
+    ctx = RefContext(kernel, m, max_pts, threads)
+    try:
+        out = ctx.evaluate(src, den, trg)
+        return out, ctx.tree(), ctx.lists()
+    finally:
+        ctx.close()

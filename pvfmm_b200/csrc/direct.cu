@@ -147,7 +147,10 @@ extern "C" int PVFMMKernelEvalDeviceD(enum PVFMMKernel kernel, const double* src
   try {
     KernelInfo ki;
     if (!kernel_info((int)kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value");
-    if (n_trg <= 0 || n_src <= 0) return 0;
+    if (n_trg <= 0 || n_src <= 0) {
+      set_last_error("");
+      return 0;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     const int S = choose_chunks(n_src, n_trg, 1L << 20);
     double* partial = nullptr;
@@ -219,8 +222,10 @@ extern "C" int PVFMMKernelEvalD(enum PVFMMKernel kernel, const double* src_pos, 
 //
 // The array's host-side name is only a stand-in for the symbol, not a device
 // address, so the first call on each device looks up the real address with
-// cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture.  Every call shares the array and
+// cudaGetSymbolAddress (with that device current) and caches it for the life
+// of the process; make that first call before any stream capture.  The cached
+// address belongs to the device's primary context: after cudaDeviceReset it is
+// stale, and this entry point must not be called again in that process.  Every call shares the array and
 // leaves its partial sums in it; nothing in it needs to start at zero, because
 // each call writes every entry it later reads.  Calls whose work overlaps on
 // the GPU (concurrent streams, or other host threads) race on the array and
@@ -254,7 +259,10 @@ extern "C" int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const doub
   try {
     KernelInfo ki;
     if (!kernel_info((int)kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value");
-    if (n_trg <= 0 || n_src <= 0) return 0;
+    if (n_trg <= 0 || n_src <= 0) {
+      set_last_error("");
+      return 0;
+    }
     const long rows = n_trg * ki.k1;
     if (rows > kNoAllocScratchDoubles)
       throw std::runtime_error("n_trg * k1 = " + std::to_string(rows) + " exceeds the fixed scratch of " +

@@ -254,13 +254,18 @@ __global__ void member_flags(const MKey* __restrict__ keys, long n, const MKey* 
   internal[i] = f;
 }
 
+// Links of one level.  `cap` is the level's internal-node count known on the
+// host (the size of the next level / 8 and of this level's int_idx segment);
+// the scan's own total is checked against it only after the build's final
+// synchronisation, so a rank k >= cap is skipped here instead of written out
+// of bounds (the host check then reports the mismatch).
 __global__ void level_links(const int* __restrict__ internal, const int* __restrict__ offs, long n, long base,
-                            long next_base, long int_base, unsigned char* __restrict__ leaf, int* __restrict__ child0,
-                            int* __restrict__ parent, int* __restrict__ int_idx) {
+                            long next_base, long int_base, long cap, unsigned char* __restrict__ leaf,
+                            int* __restrict__ child0, int* __restrict__ parent, int* __restrict__ int_idx) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const long g = base + i;
-  if (internal[i]) {
+  if (internal[i] && offs[i] < cap) {
     const long k = offs[i];
     leaf[g] = 0;
     child0[g] = (int)(next_base + 8 * k);
@@ -330,6 +335,7 @@ __global__ void localize(const int* __restrict__ leaves, long n_leaves, const MK
   const long li = blockIdx.x;
   if (li >= n_leaves) return;
   const int node = leaves[li];
+  if (node < 0) return;  // slot left unfilled by a count mismatch (reported by the host)
   unsigned int X, Y, Z, d;
   decode_key(keys[node], X, Y, Z, d);
   const double h = 1.0 / (double)(1u << d);
@@ -487,12 +493,16 @@ __global__ void flag_nodes(long n, Pred pred, int* __restrict__ flag) {
   if (i < n) flag[i] = pred(i) ? 1 : 0;
 }
 
-__global__ void compact_index(const int* __restrict__ flag, const int* __restrict__ offs, long n, int* __restrict__ out,
-                              int* __restrict__ map) {
+// out[offs[i]] = i for flagged i; ranks >= cap (the capacity of out) are
+// skipped, so a count that disagrees with the host's expectation (checked
+// after the build's final synchronisation) never writes out of bounds.
+__global__ void compact_index(const int* __restrict__ flag, const int* __restrict__ offs, long n, long cap,
+                              int* __restrict__ out, int* __restrict__ map) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (flag[i]) out[offs[i]] = (int)i;
-  if (map) map[i] = flag[i] ? offs[i] : -1;
+  const bool f = flag[i] && offs[i] < cap;
+  if (f) out[offs[i]] = (int)i;
+  if (map) map[i] = f ? offs[i] : -1;
 }
 
 __global__ void gather_u32(const unsigned int* __restrict__ in, const int* __restrict__ perm, long n,
@@ -900,7 +910,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     T.int_off[d] = int_base;
     ++ctx.n_launch;
     level_links<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(internal, offs, nl, base, T.level_off[d + 1], int_base,
-                                                            leaf, child0, parent, int_idx);
+                                                            nSd, leaf, child0, parent, int_idx);
     int_base += nint;
   }
   // 8. point ranges and colleagues
@@ -928,7 +938,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       exclusive_scan_deferred(ctx, flag, offs, N, slot);
       int* o = out.as<int>(N);
       ++ctx.n_launch;
-      compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, o, map);
+      compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, N, o, map);
     };
     compact([=] __device__(long i) { return leaf[i] && shi[i] > slo[i]; }, T.sleaf, nullptr, cnt + 0);
     compact([=] __device__(long i) { return leaf[i] && thi[i] > tlo[i]; }, T.tleaf, nullptr, cnt + 1);
@@ -1005,8 +1015,10 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     exclusive_scan_deferred(ctx, flag, offs, N, ctx.chk + kChkLeaves);
     const long nl = n_leaves_all;
     int* leaves = ctx.t[0].as<int>(std::max(nl, 1L));
+    // -1 marks a slot that no leaf filled (a count mismatch, reported below)
+    PVFMM_CUDA_CHECK(cudaMemsetAsync(leaves, 0xff, std::max(nl, 1L) * sizeof(int), s));
     ++ctx.n_launch;
-    compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, leaves, nullptr);
+    compact_index<<<ceil_div(N, kThreads), kThreads, 0, s>>>(flag, offs, N, nl, leaves, nullptr);
     double* sx = T.sx.as<double>(std::max(T.n_src, 1L));
     double* sy = T.sy.as<double>(std::max(T.n_src, 1L));
     double* sz = T.sz.as<double>(std::max(T.n_src, 1L));
@@ -1032,3 +1044,64 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
 }
 
 }  // namespace pvfmm_b200
+
+// Self-check of the bounded writes of the tree build's deferred count check
+// (internal entry point, used by the GPU tests; no counterpart in the
+// reference).  Runs compact_index and level_links with `n` flagged entries
+// against capacities of `cap` < n, in buffers followed by a guard band, and
+// checks that the ranks below cap are written and nothing at or beyond it.
+// Returns 0 when the bounds hold, 1 otherwise (message in PVFMMGetLastError).
+extern "C" int PVFMMB200CheckBoundedWrites(long n, long cap) {
+  using namespace pvfmm_b200;
+  constexpr long kGuard = 64;
+  int* buf = nullptr;
+  unsigned char* lf = nullptr;
+  try {
+    if (n <= 0 || cap < 0 || cap > n || n > (1L << 24)) throw std::runtime_error("bad sizes");
+    // flag[n] = 1, offs[n] = iota, out[cap + guard], child0/parent/int_idx sized for cap internal nodes
+    const long n_out = cap + kGuard, n_par = 8 * cap + kGuard;
+    const long total = 2 * n + n_out + n + n_par + n_out;
+    PVFMM_CUDA_CHECK(cudaMalloc((void**)&buf, total * sizeof(int)));
+    PVFMM_CUDA_CHECK(cudaMalloc((void**)&lf, n));
+    int* flag = buf;
+    int* offs = flag + n;
+    int* out = offs + n;
+    int* child0 = out + n_out;
+    int* parent = child0 + n;
+    int* int_idx = parent + n_par;
+    std::vector<int> h(total, -7);
+    for (long i = 0; i < n; ++i) {
+      h[i] = 1;
+      h[n + i] = (int)i;
+    }
+    PVFMM_CUDA_CHECK(cudaMemcpy(buf, h.data(), total * sizeof(int), cudaMemcpyHostToDevice));
+    compact_index<<<ceil_div(n, kThreads), kThreads>>>(flag, offs, n, cap, out, nullptr);
+    // one level of n nodes at base 0, its children at next_base = n
+    level_links<<<ceil_div(n, kThreads), kThreads>>>(flag, offs, n, 0, 0, 0, cap, lf, child0, parent, int_idx);
+    PVFMM_CUDA_CHECK(cudaGetLastError());
+    PVFMM_CUDA_CHECK(cudaMemcpy(h.data(), buf, total * sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(buf);
+    cudaFree(lf);
+    buf = nullptr;
+    lf = nullptr;
+    const int* ho = h.data() + 2 * n;
+    const int* hp = ho + n_out + n;
+    const int* hi = hp + n_par;
+    for (long k = 0; k < n_out; ++k) {
+      const int want = k < cap ? (int)k : -7;
+      if (ho[k] != want) throw std::runtime_error("compact_index wrote rank " + std::to_string(k) + " wrongly");
+      if (hi[k] != want) throw std::runtime_error("level_links wrote int_idx rank " + std::to_string(k) + " wrongly");
+    }
+    for (long k = 0; k < n_par; ++k) {
+      const int want = k < 8 * cap ? (int)(k / 8) : -7;
+      if (hp[k] != want) throw std::runtime_error("level_links wrote parent slot " + std::to_string(k) + " wrongly");
+    }
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    if (buf) cudaFree(buf);
+    if (lf) cudaFree(lf);
+    set_last_error(e.what());
+    return 1;
+  }
+}

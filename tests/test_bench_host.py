@@ -152,3 +152,14 @@ def test_a_form_that_failed_is_kept_in_the_line():
     assert line["mixed_over_plain"] is None and line["n_gpus"] == 2
     with pytest.raises(RuntimeError, match="no form completed"):
         bench.build_line(_Args, 1, 4_000_000, {"plain": {"error": "x"}}, {})
+
+
+def test_a_line_where_no_form_meets_the_bar_says_so():
+    forms = {"plain": _form(58e6, 2.1e-6, [6e-8, 2.5e-6, 1.8e-7, 2.0e-7], 8),
+             "mixed": _form(109e6, 5.5e-6, [2.3e-7, 6.4e-6, 4.8e-7, 5.6e-7], 4)}
+    line = bench.build_line(_Args, 1, 4_000_000, forms, {})
+    assert line["meets_bar"] is False
+    assert line["rel_l2_worst_component"] == pytest.approx(2.5e-6) and line["rel_l2_bar"] == 1e-6
+    forms["plain"] = _form(58e6, 2.1e-7, [6e-8, 2.5e-7, 1.8e-7, 2.0e-7], 8)
+    line = bench.build_line(_Args, 1, 4_000_000, forms, {})
+    assert line["meets_bar"] is True and line["form"] == "plain"

@@ -20,7 +20,7 @@ from oracle import pvfmm_oracle as O
 pytestmark = pytest.mark.gpu
 
 PLAIN_TOL = 1e-12      # plain FP64 GPU vs oracle (same operators)
-MIXED_TOL = 2e-5       # mixed form vs oracle
+MIXED_TOL = 1e-6       # mixed form vs oracle (the accuracy bar of the mixed form)
 
 
 def points(dist, n, seed):
@@ -324,3 +324,17 @@ def test_vlist_chunks_give_identical_results(monkeypatch, prec):
     assert ctx.tree_stats()["n_vtrg"] > 300
     ctx.close()
     assert np.array_equal(whole, chunked)
+
+
+def test_tree_build_writes_stay_in_bounds_on_a_count_mismatch():
+    """The tree build checks its per-level internal-node and leaf counts only
+    at its final synchronisation; until then the kernels that write by scan
+    rank skip ranks beyond the buffers' capacities.  The library's self-check
+    runs them with more flagged entries than capacity and checks a guard band
+    after each buffer."""
+    lib = P.load_library()
+    f = lib.PVFMMB200CheckBoundedWrites
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_long, ctypes.c_long]
+    for n, cap in [(1000, 600), (4096, 0), (300, 300)]:
+        assert f(n, cap) == 0, P.last_error()
