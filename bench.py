@@ -23,8 +23,10 @@ Multi-GPU: the evaluation runs on a single rank (no MPI across GPUs), so
 `--gpus N` under torchrun runs N independent replicas (weak scaling) and
 reports the summed throughput over the max-over-ranks time.
 
-`--impl reference` times the CPU restatement of the reference algorithm
-(oracle/pvfmm_oracle.py) on a bounded sample of the same workload.
+`--impl reference` times the reference's own CPU FMM (PVFMM's sources built
+over a single-rank MPI and SCTL stand-in, oracle/ref_fmm/build.sh ->
+oracle/_ref) through its C interface on all host threads, on a bounded sample
+of the same workload (`--ref-sample` points, default 500,000).
 """
 from __future__ import annotations
 
@@ -215,78 +217,128 @@ def job_throughput(world, n, ms):
     return world * n / (ms / 1000)
 
 
+# The reference has no pot+grad kernel: it evaluates the workload's kernel
+# as these C-interface kernels in turn, on the same points (one step = all of
+# them).  PVFMMKernel ids: 0 Laplace potential, 1 Laplace gradient, 3 Stokes
+# velocity.
+REFERENCE_KERNELS = {0: (0,), 3: (3,), 6: (0, 1)}
+REF_STAGES = ("InitFMM_Tree", "SetupFMM", "S2U", "U2U", "U-List", "V-List", "W-List", "X-List", "D2D", "D2T")
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_sample(args):
+    """A bounded sample of the workload for the CPU reference: `ref_sample`
+    points drawn (seed 15) from the workload's points, or all of them."""
+    x, q = make_points(W, args.n)
+    n = min(args.ref_sample, args.n)
+    if n < args.n:
+        sel = np.random.default_rng(15).choice(args.n, n, replace=False)
+        x, q = x[sel], q[sel]
+    return np.ascontiguousarray(x), np.ascontiguousarray(q), n
+
+
+def reference_contexts(threads):
+    """The reference's own FMM (built from its sources, oracle/_ref) through
+    its C interface, one context per C-interface kernel of the workload."""
+    from oracle.ref_fmm import refpvfmm as R
+    t0 = time.perf_counter()
+    ctxs = [R.RefContext(k, W["m"], W["max_pts"], threads=threads) for k in REFERENCE_KERNELS[W["kernel"]]]
+    return R, ctxs, 1000 * (time.perf_counter() - t0)
+
+
+def reference_step(ctxs, x, q, setup=True):
+    for c in ctxs:
+        c.evaluate(x, q, None, setup)
+
+
 def run_reference(args, world, rank):
-    """CPU restatement of the reference FMM (oracle) on a bounded sample."""
+    """The reference's own CPU FMM (compiled from its sources, oracle/_ref)
+    through its C interface PVFMMCreateContextDWorld / PVFMMEvalD, all host
+    threads, FP64, on a bounded sample of the workload; rank 0 only."""
     if rank != 0:
         return
-    try:
-        from threadpoolctl import threadpool_limits
-    except ImportError:  # pragma: no cover
-        threadpool_limits = None
-    from oracle import pvfmm_oracle as O
-    n_sample = args.ref_sample
-    x, q = make_points(W, args.n)
-    sel = np.random.default_rng(15).choice(args.n, n_sample, replace=False)
-    xs, qs = x[sel], q[sel]
+    from oracle.ref_fmm import refpvfmm as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/ref_fmm/build.sh "
+                                                              "needs the reference sources)"}), flush=True)
+        return
+    x, q, n = reference_sample(args)
     cores = os.cpu_count() or 1
-    t_ops = time.perf_counter()
-    ops = O.Operators(O.KERNELS[W["kernel"]], W["m"])     # context creation, outside the timed steps
-    ops_ms = 1000 * (time.perf_counter() - t_ops)
-    times, stages = [], {}
-    ctxm = threadpool_limits(limits=cores) if threadpool_limits else None
-    fmm = None
+    R, ctxs, create_ms = reference_contexts(cores)
+    times = []
+    stages = {}
     for it in range(args.warmup + args.steps):
+        prof = it == args.warmup + args.steps - 1
+        if prof:
+            R.profile_enable(True)
         t0 = time.perf_counter()
-        _, fmm = O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], xs, qs, xs, ops=ops, return_fmm=True)
+        reference_step(ctxs, x, q, True)
         dt = time.perf_counter() - t0
+        if prof:
+            R.profile_enable(False)
+            for _, tag, sec in R.profile_report():
+                if tag in REF_STAGES:
+                    stages[tag] = stages.get(tag, 0.0) + 1000 * sec
         if it >= args.warmup:
             times.append(dt)
-            for k, v in fmm.stage_ms.items():
-                stages[k] = stages.get(k, 0.0) + v / args.steps
-    # setup=0 (same points, new densities): the last step's tree reused
-    setup0_ms = None
-    if fmm is not None:
-        t0 = time.perf_counter()
-        O.pvfmm_eval_setup0(fmm, qs)
-        setup0_ms = 1000 * (time.perf_counter() - t0)
-    if ctxm is not None:
-        ctxm.unregister() if hasattr(ctxm, "unregister") else None
+    t0 = time.perf_counter()
+    reference_step(ctxs, x, q, False)          # setup=0: same points, new densities (the tree reused)
+    setup0_ms = 1000 * (time.perf_counter() - t0)
+    for c in ctxs:
+        c.close()
     ms = 1000 * float(np.mean(times))
-    value = n_sample / (ms / 1000)
-    sample = (f"{n_sample} points subsampled (seed 15) from the workload's {args.n} points "
-              f"({args.workload}), FP64 numpy oracle, setup=1 per step")
+    value = n / (ms / 1000)
+    kernels = "+".join({0: "LaplacePotential", 1: "LaplaceGradient", 3: "StokesVelocity"}[k]
+                       for k in REFERENCE_KERNELS[W["kernel"]])
+    sample = (f"{n} of the workload's {args.n} points (seed 15), the reference's PVFMMEvalD ({kernels}), FP64, "
+              f"setup=1 per step, {cores} threads on {cpu_model()}")
     line = {"metric": METRIC, "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": W["desc"].format(n=args.n) + f" (bounded CPU sample: {n_sample} points)"},
+            "config": {"workload": W["desc"].format(n=args.n) + (f" (bounded CPU sample: {n} points)"
+                                                                 if n < args.n else "")},
             "impl": "reference",
-            "context_create_ms": ops_ms,
+            "context_create_ms": create_ms,
             "stages_ms": stages,
+            "stages_note": "reference profiler tags (pvfmm::Profile) of the last step; V-List runs the reference's "
+                           "built-in matrix DFT (FFTW absent)",
             "setup0_ms": setup0_ms,
-            "setup0_targets_per_s": n_sample / (setup0_ms / 1000) if setup0_ms else None,
-            "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port", "sample": sample},
+            "setup0_targets_per_s": n / (setup0_ms / 1000),
+            "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def cpu_baseline(args):
-    """Oracle timed on one host thread on a bounded sample (about 10-30 s)."""
-    from oracle import pvfmm_oracle as O
-    try:
-        from threadpoolctl import threadpool_limits
-        lim = threadpool_limits(limits=1)
-    except ImportError:  # pragma: no cover
-        lim = None
-    x, q = make_points(W, args.n)
-    sel = np.random.default_rng(15).choice(args.n, args.ref_sample, replace=False)
-    ops = O.Operators(O.KERNELS[W["kernel"]], W["m"])
+    """The reference's own CPU FMM on all host threads, one setup=1 step on a
+    bounded sample of the workload (a few seconds to tens of seconds)."""
+    from oracle.ref_fmm import refpvfmm as R
+    if not R.available():
+        return {"value": None, "unit": "targets/s", "cores": 0, "kind": "reference",
+                "sample": "reference library not built"}
+    x, q, n = reference_sample(args)
+    cores = os.cpu_count() or 1
+    R, ctxs, _ = reference_contexts(cores)
+    reference_step(ctxs, x, q, True)             # first evaluation (allocations)
     t0 = time.perf_counter()
-    O.pvfmm_eval(W["kernel"], W["m"], W["max_pts"], x[sel], q[sel], x[sel], ops=ops)
+    reference_step(ctxs, x, q, True)
     dt = time.perf_counter() - t0
-    del lim
-    return {"value": args.ref_sample / dt, "unit": "targets/s", "cores": 1, "kind": "port",
-            "sample": f"{args.ref_sample} points subsampled (seed 15) from the same workload, FP64 numpy oracle, "
-                      f"one thread, setup=1, {dt:.1f} s"}
+    for c in ctxs:
+        c.close()
+    return {"value": n / dt, "unit": "targets/s", "cores": cores, "kind": "reference",
+            "sample": f"{n} of the workload's {args.n} points (seed 15), the reference's PVFMMEvalD, FP64, setup=1, "
+                      f"{cores} threads on {cpu_model()}, {dt:.2f} s"}
 
 
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
@@ -421,7 +473,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gaussian4m", choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=None, help="point count (default: the workload's)")
-    ap.add_argument("--ref-sample", type=int, default=12000)
+    ap.add_argument("--ref-sample", type=int, default=500_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain,mixed")
     args = ap.parse_args()

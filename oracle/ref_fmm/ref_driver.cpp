@@ -11,6 +11,8 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <iostream>
+#include <sstream>
 
 extern "C" void scipy_openblas_set_num_threads(int);
 
@@ -98,7 +100,34 @@ int ref_set_threads(int n) {
 }
 
 // Enables the reference's profiler (pvfmm::Profile, the per-stage tags of
-// fmm_tree.txx / fmm_pts.txx) for the following evaluations.
-void ref_profile_enable(int on) { pvfmm::Profile::Enable(on != 0); }
+// fmm_tree.txx / fmm_pts.txx) for the following evaluations, with a cleared
+// log, or turns it off (keeping the log).
+void ref_profile_enable(int on) {
+  if (on) pvfmm::Profile::reset();
+  pvfmm::Profile::Enable(on != 0);
+}
+
+// The profiler's table (pvfmm::Profile::print: one line per tag, indented by
+// nesting, then t_min t_avg t_max ... in seconds; printing consumes the log).
+// With buf == NULL the table is formed and kept, and its length returned;
+// a following call with a buffer copies the kept table (at most cap - 1
+// bytes, NUL-terminated).
+long ref_profile_report(char* buf, long cap) {
+  static std::string table;
+  if (!buf) {
+    std::stringstream ss;
+    std::streambuf* old = std::cout.rdbuf(ss.rdbuf());
+    pvfmm::Profile::print();
+    std::cout.rdbuf(old);
+    table = ss.str();
+    return (long)table.size();
+  }
+  if (cap > 0) {
+    const long n = std::min<long>(cap - 1, (long)table.size());
+    std::memcpy(buf, table.data(), n);
+    buf[n] = 0;
+  }
+  return (long)table.size();
+}
 
 }  // extern "C"

@@ -67,6 +67,10 @@ def load():
     lib.ref_tree_lists.argtypes = [vp, vp, lg]
     lib.ref_set_threads.restype = ctypes.c_int
     lib.ref_set_threads.argtypes = [ctypes.c_int]
+    lib.ref_profile_enable.restype = None
+    lib.ref_profile_enable.argtypes = [ctypes.c_int]
+    lib.ref_profile_report.restype = lg
+    lib.ref_profile_report.argtypes = [vp, lg]
     _lib = lib
     return lib
 
@@ -132,6 +136,36 @@ class RefContext:
             self.close()
         except Exception:
             pass
+
+
+def profile_enable(on=True):
+    """Turns the reference's profiler (pvfmm::Profile) on (with a cleared
+    log) or off (keeping the log)."""
+    load().ref_profile_enable(1 if on else 0)
+
+
+def profile_report() -> list:
+    """The reference profiler's log since profile_enable: a list of
+    (indent, tag, t_avg seconds) in the profiler's print order
+    (pvfmm::Profile::print, src/profile.cpp:128-230); the tag names are those
+    of fmm_tree.txx / fmm_pts.txx (S2U, U2U, U-List, V-List, D2T, ...)."""
+    lib = load()
+    n = lib.ref_profile_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.ref_profile_report(buf, n + 1)
+    rows = []
+    for line in buf.value.decode(errors="replace").splitlines():
+        toks = line.split()
+        if len(toks) < 13:
+            continue
+        try:
+            nums = [float(v) for v in toks[-12:]]
+        except ValueError:
+            continue
+        name = " ".join(toks[:-12]).replace("|", " ").replace("+-", " ").strip()
+        indent = len(line) - len(line.lstrip(" |+-"))
+        rows.append((indent, name, nums[1]))
+    return rows
 
 
 def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0):

@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--extended-lambda", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-fopenmp,-O3", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
-SOURCES = ["precomp.cpp", "tree.cu", "eval.cu", "capi.cu", "direct.cu"]
+SOURCES = ["precomp.cpp", "tree.cu", "eval.cu", "translate.cu", "capi.cu", "direct.cu"]
 
 
 def _newer(src: Path, obj: Path, deps) -> bool:
@@ -50,7 +50,7 @@ def build(verbose: bool = False, extra_flags=None) -> Path:
         subprocess.run(cmd, check=True)
     if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + \
-              ["-lcublas", "-lgomp", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
+              ["-lgomp", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -53,7 +53,6 @@ void destroy_context(Context& c) {
   for (DevBuf* b : tb) b->release();
   if (c.events_ready)
     for (auto& e : c.ev) cudaEventDestroy(e);
-  if (c.cublas) cublasDestroy(c.cublas);
   if (c.stream) cudaStreamDestroy(c.stream);
   if (c.pinned) cudaFreeHost(c.pinned);
   if (c.chk) cudaFreeHost(c.chk);
@@ -89,8 +88,6 @@ void* create_context(double box_size, int n, int m, int kernel, int precision, b
     build_operators(kernel, m, false, c.hops, precision == 1 && ki.ke == 3);
     PVFMM_CUDA_CHECK(cudaGetDevice(&c.device));
     PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    if (cublasCreate(&c.cublas) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasCreate failed");
-    cublasSetMathMode(c.cublas, CUBLAS_PEDANTIC_MATH);
     for (auto& e : c.ev) PVFMM_CUDA_CHECK(cudaEventCreate(&e));
     c.events_ready = true;
     upload_operators(c);

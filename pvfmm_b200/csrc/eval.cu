@@ -20,16 +20,19 @@
 //          max S), so FP32 check potentials would need the FP32 cutoff,
 //          which alone costs ~8e-7 relative error at m=8.
 // Stages:
-//   S2U   check-surface evaluation + 2 GEMMs (pinv factors, fmm_pts.txx:4390-4426)
-//   U2U   one GEMM per level over the contiguous child blocks (fmm_pts.txx:2017-2271)
+//   S2U   check-surface evaluation + 2 FP64 tensor-core products (pinv
+//         factors, fmm_pts.txx:4390-4426), the second one writing the leaves'
+//         rows of UE (translate.cu)
+//   U2U   one product per level over the contiguous child blocks, written to
+//         the parents' rows (fmm_pts.txx:2017-2271)
 //   V     pruned DFT of the 8 children, Hadamard with the 26 parent offsets,
 //         pruned inverse DFT onto the children's check surfaces (fmm_pts.txx:2689-3759)
 //   X     check-surface evaluation (fmm_pts.txx:4444-4736)
-//   D2D   one GEMM per level into the contiguous child blocks (fmm_pts.txx:3762-3790)
-//   D2T   2 GEMMs (pinv factors), then with W and U one fused near-field
+//   D2D   one product per level from the parents' rows into the contiguous
+//         child blocks (fmm_pts.txx:3762-3790)
+//   D2T   2 products (pinv factors, leaves' rows gathered and scaled by
+//         2^-depth in the first), then with W and U one fused near-field
 //         kernel per target leaf (fmm_pts.txx:4246-4426, 4746-5022, 5032-5418).
-#include <cublas_v2.h>
-
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -1323,24 +1326,6 @@ void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* 
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------
-__global__ void scatter_rows(const double* __restrict__ src, const int* __restrict__ rows, long n, int dim,
-                             double* __restrict__ dst) {
-  const long i = blockIdx.x;
-  if (i >= n) return;
-  const long r = rows[i];
-  for (int j = threadIdx.x; j < dim; j += blockDim.x) dst[r * dim + j] = src[i * dim + j];
-}
-
-// dst[i] = src[rows[i]] * 2^(-depth(rows[i])) if scale_level else src[rows[i]].
-__global__ void gather_rows(const double* __restrict__ src, const int* __restrict__ rows, long n, int dim,
-                            const MKey* __restrict__ keys, int scale_level, double* __restrict__ dst) {
-  const long i = blockIdx.x;
-  if (i >= n) return;
-  const long r = rows[i];
-  const double s = scale_level ? ldexp(1.0, -(int)(keys[r].lo & 31u)) : 1.0;
-  for (int j = threadIdx.x; j < dim; j += blockDim.x) dst[i * dim + j] = src[r * dim + j] * s;
-}
-
 template <class Tin>
 __global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict__ perm, long n, int k0, double s0,
                                double s1, double s2, double* __restrict__ out) {
@@ -1359,14 +1344,6 @@ __global__ void unsort_values(const double* __restrict__ pot, const int* __restr
   const long p = perm[i];
   const double sc[4] = {s0, s1, s2, s3};
   for (int k = 0; k < k1; ++k) out[p * k1 + k] = (Tout)((Tout)pot[i * k1 + k] * (Tout)sc[k]);
-}
-
-void dgemm(cublasHandle_t h, int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C, int ldc,
-           double beta) {
-  const double one = 1.0;
-  // Row-major C(MxN) = A(MxK) B(KxN)  <=>  column-major C^T = B^T A^T.
-  if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, M, K, &one, B, ldb, A, lda, &beta, C, ldc) != CUBLAS_STATUS_SUCCESS)
-    throw std::runtime_error("cublasDgemm failed");
 }
 
 template <class Real>
@@ -1506,7 +1483,6 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   const double* sz = T.sz.get<double>();
   const int* slo = T.src_lo.get<int>();
   const int* shi = T.src_hi.get<int>();
-  if (cublasSetStream(ctx.cublas, s) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasSetStream failed");
   const double kscale_exp = ker_scale(KerExp);
   ev(1);
   // ---- S2U
@@ -1521,10 +1497,12 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     // potential error from 3e-7 to 2.5e-6)
     surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
         0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
-    dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, uc, dim, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, 0);
-    dgemm(ctx.cublas, (int)T.n_sleaf, dim, dim, t1, dim, ctx.dops.uc2ue1.get<double>(), dim, uc, dim, 0);
-    ++ctx.n_launch;
-    scatter_rows<<<T.n_sleaf, 128, 0, s>>>(uc, T.sleaf.get<int>(), T.n_sleaf, dim, ue);
+    // equivalent densities (uc UC2UE0) UC2UE1 straight into the leaves' rows of UE
+    ctx.n_launch += 2;
+    translate_gemm(s, T.n_sleaf, dim, dim, uc, dim, nullptr, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, nullptr,
+                   nullptr, false);
+    translate_gemm(s, T.n_sleaf, dim, dim, t1, dim, nullptr, ctx.dops.uc2ue1.get<double>(), dim, ue, dim,
+                   T.sleaf.get<int>(), nullptr, false);
   }
   ev(2);
   // ---- U2U, bottom-up
@@ -1532,11 +1510,11 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     for (int d = T.depth - 1; d >= 0; --d) {
       const long ni = T.n_internal[d];
       if (ni == 0) continue;
-      double* c = ctx.tmp_c.as<double>((size_t)ni * dim);
-      dgemm(ctx.cublas, (int)ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim,
-            ctx.dops.u2u.get<double>(), dim, c, dim, 0);
+      // the 8 children of the level's k-th internal node are the k-th block
+      // of 8 rows of the next level: one row of 8*dim values per parent
       ++ctx.n_launch;
-      scatter_rows<<<ni, 128, 0, s>>>(c, T.int_idx.get<int>() + T.int_off[d], ni, dim, ue);
+      translate_gemm(s, ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim, nullptr,
+                     ctx.dops.u2u.get<double>(), dim, ue, dim, T.int_idx.get<int>() + T.int_off[d], nullptr, false);
     }
   }
   // mixed form, Stokes kernel: the FP32 stages (V-list input, W list) read
@@ -1546,7 +1524,9 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   const double* ue32 = ue;
   if (sizeof(Real) == 4 && ke == 3 && T.src_counted && N > 0) {
     double* uc_ = ctx.ue_c.as<double>((size_t)N * dim);
-    dgemm(ctx.cublas, (int)N, dim, dim, ue, dim, ctx.dops.ue_proj.get<double>(), dim, uc_, dim, 0);
+    ++ctx.n_launch;
+    translate_gemm(s, N, dim, dim, ue, dim, nullptr, ctx.dops.ue_proj.get<double>(), dim, uc_, dim, nullptr, nullptr,
+                   false);
     ue32 = uc_;
   }
   ev(3);
@@ -1570,23 +1550,23 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   for (int d = 0; d < T.depth; ++d) {
     const long ni = T.n_internal[d];
     if (ni == 0) continue;
-    double* g = ctx.tmp_c.as<double>((size_t)ni * dim);
     ++ctx.n_launch;
-    gather_rows<<<ni, 128, 0, s>>>(dc, T.int_idx.get<int>() + T.int_off[d], ni, dim, keys, 0, g);
-    dgemm(ctx.cublas, (int)ni, 8 * dim, dim, g, dim, ctx.dops.d2d.get<double>(), 8 * dim,
-          dc + (size_t)T.level_off[d + 1] * dim, 8 * dim, 1);
+    translate_gemm(s, ni, 8 * dim, dim, dc, dim, T.int_idx.get<int>() + T.int_off[d], ctx.dops.d2d.get<double>(),
+                   8 * dim, dc + (size_t)T.level_off[d + 1] * dim, 8 * dim, nullptr, nullptr, true);
   }
   ev(8);
   // ---- D2T equivalent densities, then the fused near field
   double* pot = ctx.pot.as<double>(std::max(T.n_trg, 1L) * k1);
   if (T.n_tleaf > 0) {
-    double* g = ctx.tmp_c.as<double>((size_t)T.n_tleaf * dim);
     double* de = ctx.de_c.as<double>((size_t)T.n_tleaf * dim);
     double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * dim);
-    ++ctx.n_launch;
-    gather_rows<<<T.n_tleaf, 128, 0, s>>>(dc, T.tleaf.get<int>(), T.n_tleaf, dim, keys, 1, g);
-    dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, g, dim, ctx.dops.dc2de0.get<double>(), dim, t1, dim, 0);
-    dgemm(ctx.cublas, (int)T.n_tleaf, dim, dim, t1, dim, ctx.dops.dc2de1.get<double>(), dim, de, dim, 0);
+    // (2^-depth DC[leaf] DC2DE0) DC2DE1, the check potentials gathered from
+    // the leaves' rows of DC
+    ctx.n_launch += 2;
+    translate_gemm(s, T.n_tleaf, dim, dim, dc, dim, T.tleaf.get<int>(), ctx.dops.dc2de0.get<double>(), dim, t1, dim,
+                   nullptr, keys, false);
+    translate_gemm(s, T.n_tleaf, dim, dim, t1, dim, nullptr, ctx.dops.dc2de1.get<double>(), dim, de, dim, nullptr,
+                   nullptr, false);
     ev(12);
     ++ctx.n_launch;
     near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNF, 0, s>>>(

@@ -2,8 +2,6 @@
 // the last setup, interaction lists and evaluation buffers.
 #pragma once
 
-#include <cublas_v2.h>
-
 #include <array>
 #include <vector>
 
@@ -70,7 +68,6 @@ struct Context {
   DevOps dops;
   DevTree tree;
   cudaStream_t stream = nullptr;
-  cublasHandle_t cublas = nullptr;
   int device = 0;
   // evaluation buffers
   DevBuf den;             // sorted densities (Real, n_src x k0)
@@ -106,5 +103,10 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
 // eval.cu
 void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
 void upload_operators(Context& ctx);
+// translate.cu: C[crow(i)] (+)= 2^-depth(key[arow(i)]) A[arow(i)] B on the FP64
+// tensor cores (rows gathered / scattered through the index lists when given)
+void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long lda, const int* arows,
+                    const double* B, long ldb, double* C, long ldc, const int* crows, const MKey* scale_keys,
+                    bool accumulate);
 
 }  // namespace pvfmm_b200

@@ -7,9 +7,19 @@ mortonid_ref.npz   outputs of the reference's own Morton-id code
                    and NbrList().  Needs the reference tree (this container).
 oracle_*.npz       small FMM cases of the oracle (inputs, leaf ids, outputs),
                    regression pins of the oracle itself.
+reference_*.npz    the reference's own particle FMM (src/pvfmm-wrapper.cpp and
+                   the templates it instantiates, built from the reference
+                   sources by oracle/ref_fmm/build.sh) through its C interface
+                   PVFMMCreateContextDWorld / PVFMMEvalD, free space: inputs,
+                   outputs, and the octree (Morton ids, leaf flags, points per
+                   leaf) and interaction lists (U0, U1, U2, W, X, V1) it built.
+reference_config1.npz   the reference's output on the 100,000-point uniform
+                   Laplace case (m=6, 300 points per leaf); the inputs are
+                   regenerated from their seeds (checksums kept).
 
-Run:  python tests/golden/make_golden.py [--force]   (existing oracle_*.npz are
-kept unless --force)
+Run:  python tests/golden/make_golden.py [--force]   (existing oracle_*.npz and
+reference_*.npz are kept unless --force).  The reference tree is read from
+$PVFMM_REFERENCE (its build scripts' default otherwise).
 """
 import ctypes
 import os
@@ -80,8 +90,85 @@ def oracle_golden(force=False):
                             trg=trg, out=out, leaf_keys=np.array(fmm.tree.leaf_keys()))
 
 
+def points(dist, n, seed):
+    """Seeded point sets of the reference-pinned cases (also used by tests)."""
+    rng = np.random.default_rng(seed)
+    if dist == "unif":
+        return rng.random((n, 3))
+    if dist == "gauss":        # 8 isotropic Gaussians, sigma 0.02, clipped to the unit cube
+        c = rng.uniform(0.1, 0.9, (8, 3))
+        return np.clip(c[rng.integers(0, 8, n)] + 0.02 * rng.standard_normal((n, 3)), 0, 1)
+    if dist == "sphere":       # ellipsoid surface, semi-axes (0.45, 0.3, 0.15)
+        u = rng.standard_normal((n, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        return 0.5 + np.array([0.45, 0.3, 0.15]) * u
+    if dist == "coincident":   # half the points on one spot: a tree to the maximum depth
+        x = rng.random((n, 3))
+        x[: n // 2] = x[0]
+        x[n // 2: n // 2 + 20] = x[n - 1]
+        return x
+    raise ValueError(dist)
+
+
+# name: (kernel id of the C interface, m, max points per leaf, distribution,
+# n, separate targets, input seed)
+REFERENCE_CASES = {
+    "laplace_unif_m6": (0, 6, 50, "unif", 3000, False, 1),
+    "laplace_grad_unif_m6": (1, 6, 50, "unif", 3000, False, 1),   # same inputs: pot + grad
+    "laplace_gauss_m6": (0, 6, 50, "gauss", 5000, False, 2),
+    "laplace_gauss_m8": (0, 8, 120, "gauss", 8000, False, 3),
+    "laplace_sphere_m4": (0, 4, 40, "sphere", 4000, False, 4),
+    "laplace_coincident_m4": (0, 4, 60, "coincident", 3000, False, 5),
+    "laplace_sep_m6": (0, 6, 50, "unif", 3000, True, 6),
+    "stokes_vel_m4": (3, 4, 60, "unif", 3000, False, 7),
+    "stokes_vel_gauss_m6": (3, 6, 80, "gauss", 3000, False, 8),
+    "stokes_press_m4": (2, 4, 60, "unif", 2000, False, 9),
+    "stokes_grad_m4": (4, 4, 60, "unif", 2000, False, 10),
+    "biot_savart_m4": (5, 4, 60, "unif", 2000, False, 11),
+}
+KDIM = {0: (1, 1), 1: (1, 3), 2: (3, 1), 3: (3, 3), 4: (3, 9), 5: (3, 3)}
+
+
+def reference_case_inputs(name):
+    kid, m, mp, dist, n, sep, seed = REFERENCE_CASES[name]
+    src = points(dist, n, seed)
+    trg = points("unif", n // 2, seed + 100) * 0.8 + 0.1 if sep else None
+    den = np.random.default_rng(seed + 200).uniform(-1, 1, (n, KDIM[kid][0]))
+    return src, den, trg
+
+
+def config1_inputs():
+    """Laplace potential, 100,000 points i.i.d. uniform in [0,1)^3 (PCG64
+    seed 1), densities uniform [-1,1] (seed 2)."""
+    x = np.random.default_rng(1).random((100000, 3))
+    q = np.random.default_rng(2).uniform(-1, 1, 100000)
+    return x, q
+
+
+def reference_golden(force=False):
+    from oracle.ref_fmm import refpvfmm as R
+    if not R.available():
+        subprocess.run(["bash", os.path.join(ROOT, "oracle", "ref_fmm", "build.sh")], check=True)
+    for name, (kid, m, mp, dist, n, sep, seed) in REFERENCE_CASES.items():
+        path = os.path.join(HERE, f"reference_{name}.npz")
+        if not force and os.path.exists(path):
+            continue
+        src, den, trg = reference_case_inputs(name)
+        out, tree, lists = R.ref_eval(kid, m, mp, src, den, trg)
+        np.savez_compressed(path, kernel=kid, m=m, max_pts=mp, src=src, den=den,
+                            trg=np.zeros((0, 3)) if trg is None else trg, out=out,
+                            nodes=tree[:, :7].astype(np.int32), lists=lists[:, :4].astype(np.int32))
+    path = os.path.join(HERE, "reference_config1.npz")
+    if force or not os.path.exists(path):
+        x, q = config1_inputs()
+        out, tree, _ = R.ref_eval(0, 6, 300, x, q)
+        np.savez_compressed(path, out=out.reshape(-1), x_sum=x.sum(), q_sum=q.sum(), x_first=x[:4], q_first=q[:4],
+                            n_nodes=len(tree), n_leaves=int(tree[:, 4].sum()))
+
+
 if __name__ == "__main__":
-    if os.path.isdir("/root/reference"):
+    if os.path.isdir(os.environ.get("PVFMM_REFERENCE", "/root/reference")):
         morton_golden()
+        reference_golden(force="--force" in sys.argv)
     oracle_golden(force="--force" in sys.argv)
     print("golden fixtures written to", HERE)

@@ -1,0 +1,153 @@
+"""GPU parity against the reference's own particle FMM (fixtures
+tests/golden/reference_*.npz, written by the reference compiled from its
+sources; see tests/test_reference_pins.py for how they were made and why two
+cases carry wider bars).
+
+The plain FP64 CUDA path must build the reference's octree (the same Morton
+ids, leaf flags and points per leaf) and reproduce its outputs to 1e-12
+relative L2; the mixed form must stay within its accuracy bar (1e-6) of the
+reference.  The FP64 translation products (translate.cu) are checked against
+an FP64 product on the host.
+"""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import pvfmm_b200 as P
+from oracle import pvfmm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+GPU_KERNELS = {0, 1, 3}
+FIXTURES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "reference_*.npz"))
+                  if "config1" not in f and int(np.load(f)["kernel"]) in GPU_KERNELS)
+TOL = {"reference_laplace_coincident_m4.npz": 1e-7, "reference_stokes_vel_gauss_m6.npz": 1e-11}
+
+
+def gpu_eval(kid, m, mp, src, den, trg, prec=P.PRECISION_PLAIN):
+    ctx = P.FMMParticleContext(-1, mp, m, P.FMMKernel(kid), precision=prec)
+    s = np.ascontiguousarray(src).reshape(-1)
+    t = s if trg is None else np.ascontiguousarray(trg).reshape(-1)
+    out = ctx.evaluate(s, np.ascontiguousarray(den).reshape(-1), None, t, True)
+    return out, ctx
+
+
+def check_tree(ctx, nodes):
+    keys = ctx.tree_data(2).reshape(-1, 4)
+    leaf = ctx.tree_data(3)
+    src = ctx.tree_data(4).reshape(-1, 2)
+    trg = ctx.tree_data(5).reshape(-1, 2)
+    ours = {tuple(int(v) for v in k): i for i, k in enumerate(keys)}
+    ref = {tuple(int(v) for v in r[:4]): r for r in nodes}
+    assert set(ours) == set(ref), (len(ours), len(ref))
+    for k, i in ours.items():
+        r = ref[k]
+        assert bool(leaf[i]) == bool(r[4]), k
+        if leaf[i]:
+            assert int(trg[i][1] - trg[i][0]) == int(r[6]), k
+            assert int(src[i][1] - src[i][0]) == int(r[5]), k
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(f)[10:-4] for f in FIXTURES])
+def test_plain_matches_reference(path):
+    z = np.load(path)
+    kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
+    trg = z["trg"] if len(z["trg"]) else None
+    out, ctx = gpu_eval(kid, m, mp, z["src"], z["den"], trg)
+    check_tree(ctx, z["nodes"])
+    err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
+    assert err < TOL.get(os.path.basename(path), 1e-12), err
+    assert ctx.launch_count() > 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["laplace_unif_m6", "laplace_gauss_m8", "laplace_sep_m6", "laplace_grad_unif_m6"])
+def test_mixed_within_bar_of_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"reference_{name}.npz"))
+    kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
+    trg = z["trg"] if len(z["trg"]) else None
+    out, ctx = gpu_eval(kid, m, mp, z["src"], z["den"], trg, prec=P.PRECISION_MIXED)
+    ref = z["out"].reshape(len(out.reshape(-1)) // z["out"].shape[-1], -1)
+    o = out.reshape(ref.shape)
+    for k in range(ref.shape[1]):
+        assert O.rel_l2(o[:, k], ref[:, k]) < 1e-6, k
+    ctx.close()
+
+
+def test_potgrad_matches_reference_potential_and_gradient():
+    zp = np.load(os.path.join(GOLDEN, "reference_laplace_unif_m6.npz"))
+    zg = np.load(os.path.join(GOLDEN, "reference_laplace_grad_unif_m6.npz"))
+    out, ctx = gpu_eval(6, 6, 50, zp["src"], zp["den"], None)
+    out = out.reshape(-1, 4)
+    ref = np.concatenate([zp["out"].reshape(-1, 1), zg["out"].reshape(-1, 3)], axis=1)
+    for k in range(4):
+        assert O.rel_l2(out[:, k], ref[:, k]) < 1e-12, k
+    ctx.close()
+
+
+def test_config1_matches_reference_on_every_target():
+    """100,000 uniform points, Laplace potential, m=6, 300 points per leaf:
+    the plain form against the reference's output on all targets."""
+    z = np.load(os.path.join(GOLDEN, "reference_config1.npz"))
+    x = np.random.default_rng(1).random((100000, 3))
+    q = np.random.default_rng(2).uniform(-1, 1, 100000)
+    assert np.array_equal(x[:4], z["x_first"]) and np.array_equal(q[:4], z["q_first"])
+    assert x.sum() == z["x_sum"] and q.sum() == z["q_sum"]
+    out, ctx = gpu_eval(0, 6, 300, x, q, None)
+    assert ctx.tree_stats()["n_nodes"] == int(z["n_nodes"])
+    assert O.rel_l2(out.reshape(-1), z["out"]) < 1e-12
+    ctx.close()
+
+
+def _translate_check():
+    lib = P.load_library()
+    f = lib.PVFMMB200TranslateGemmCheck
+    f.restype = ctypes.c_int
+    vp = ctypes.c_void_p
+    f.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_int, vp, ctypes.c_long, vp, vp, vp, ctypes.c_long, vp, vp,
+                  ctypes.c_int]
+    return f
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@pytest.mark.parametrize("M,N,K,gather,scatter,scale,acc", [
+    (1000, 296, 296, False, False, False, False),     # S2U / D2T pseudo-inverse products
+    (777, 296, 2368, False, True, False, False),      # U2U: 8 children per row, rows scattered to parents
+    (333, 2368, 296, True, False, False, True),       # D2D: parents gathered, children accumulated
+    (1500, 296, 296, True, False, True, False),       # D2T first product: gathered, scaled by 2^-depth
+    (65, 152, 10, False, False, False, False),        # ragged tiles in every direction
+    (64 * 65536 + 70, 8, 4, False, False, False, False),   # more than one launch of row tiles
+])
+def test_translate_products_match_fp64_host_products(M, N, K, gather, scatter, scale, acc):
+    f = _translate_check()
+    rng = np.random.default_rng(M + N + K)
+    a_rows = M + 50 if gather else M
+    c_rows = M + 40 if scatter else M
+    A = rng.standard_normal((a_rows, K))
+    B = rng.standard_normal((K, N))
+    C = rng.standard_normal((c_rows, N)) if acc else np.zeros((c_rows, N))
+    arows = rng.permutation(a_rows)[:M].astype(np.int32) if gather else None
+    crows = rng.permutation(c_rows)[:M].astype(np.int32) if scatter else None
+    depth = rng.integers(0, 20, a_rows).astype(np.int32) if scale else None
+    want = C.copy()
+    Ag = A[arows] if gather else A
+    prod = Ag @ B
+    if scale:
+        prod *= np.ldexp(1.0, -depth[arows] if gather else -depth)[:, None]
+    if scatter:
+        want[crows] = prod + (C[crows] if acc else 0)
+    else:
+        want = prod + (C if acc else 0)
+    got = C.copy()
+    rc = f(M, N, K, _p(A), a_rows, _p(arows), _p(B), _p(got), c_rows, _p(crows), _p(depth), 1 if acc else 0)
+    assert rc == 0, P.last_error()
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err < 1e-14 * max(1, K / 64), err
