@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--extended-lambda", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-fopenmp,-O3", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
-SOURCES = ["precomp.cpp", "tree.cu", "eval.cu", "translate.cu", "capi.cu", "direct.cu"]
+SOURCES = ["precomp.cpp", "tree.cu", "eval.cu", "hadamard_tc.cu", "translate.cu", "capi.cu", "direct.cu"]
 
 
 def _newer(src: Path, obj: Path, deps) -> bool:

@@ -34,11 +34,23 @@ Handle* as_handle(const void* p) {
   return h;
 }
 
+// A bounded wait of the tensor-core V-list Hadamard that ran out (its error
+// word, copied to pinned memory at the end of the evaluation) fails the call
+// that observes it once the context's stream is synchronised.
+void check_tc5_error(Context& c) {
+  if (c.tc5_err_host && *(volatile int*)c.tc5_err_host != 0) {
+    const int e = *c.tc5_err_host;
+    *c.tc5_err_host = 0;
+    throw std::runtime_error("V-list tensor-core Hadamard: a bounded wait ran out (error word " + std::to_string(e) +
+                             "); the results of that evaluation are invalid");
+  }
+}
+
 void destroy_context(Context& c) {
   cudaSetDevice(c.device);
   if (c.stream) cudaStreamSynchronize(c.stream);
   DevBuf* bufs[] = {&c.dops.uc2ue0, &c.dops.uc2ue1, &c.dops.dc2de0, &c.dops.dc2de1, &c.dops.u2u, &c.dops.d2d,
-                    &c.dops.vop, &c.dops.vop_frag, &c.dops.ue_proj, &c.ue_c, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den, &c.pot, &c.ue, &c.dc,
+                    &c.dops.vop, &c.dops.vop_frag, &c.dops.vop_tc5, &c.tc5_err_buf, &c.dops.ue_proj, &c.ue_c, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den, &c.pot, &c.ue, &c.dc,
                     &c.uc_c, &c.tmp_c, &c.de_c, &c.spec_in, &c.spec_out, &c.scratch, &c.scratch2, &c.io_src,
                     &c.io_trg, &c.io_den, &c.io_val, &c.stat};
   for (DevBuf* b : bufs) b->release();
@@ -56,6 +68,7 @@ void destroy_context(Context& c) {
   if (c.stream) cudaStreamDestroy(c.stream);
   if (c.pinned) cudaFreeHost(c.pinned);
   if (c.chk) cudaFreeHost(c.chk);
+  if (c.tc5_err_host) cudaFreeHost(c.tc5_err_host);
   if (c.side) cudaStreamSynchronize(c.side);
   if (c.den_ev) cudaEventDestroy(c.den_ev);
   if (c.side) cudaStreamDestroy(c.side);
@@ -114,6 +127,7 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], user));
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(c.stream, c.ev[11], 0));
     }
+    check_tc5_error(c);  // a wait of the previous (asynchronous) evaluation that ran out
     if (n_trg <= 0) return 0;
     if (n_src <= 0) {
       PVFMM_CUDA_CHECK(cudaMemsetAsync(val, 0, (size_t)n_trg * c.ki.k1 * sizeof(T), c.stream));
@@ -135,6 +149,7 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(user, c.ev[10], 0));
     } else {
       PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+      check_tc5_error(c);
     }
     set_last_error("");
     return 0;
@@ -177,6 +192,7 @@ void eval_host(const T* src_pos, const T* sl_den, const T* dl_den, long n_src, c
       throw std::runtime_error(get_last_error());
     PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_trg * c.ki.k1 * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
     PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    check_tc5_error(c);
     set_last_error("");
   } catch (const std::exception& e) {
     const std::string msg = e.what();

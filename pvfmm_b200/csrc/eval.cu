@@ -1394,7 +1394,8 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
     const long np = std::min(chunk, T.n_vtrg - p0);
     if (ke == 1) {
       if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout, p0, np);
-      else launch_hadamard_tc(ctx, n3h, sin_, sout, p0, np);
+      else if (std::getenv("PVFMM_B200_HADAMARD_MMA_SYNC")) launch_hadamard_tc(ctx, n3h, sin_, sout, p0, np);
+      else launch_hadamard_tc5(ctx, n3h, sin_, sout, p0, np);
     } else {
       launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout, p0, np);
     }
@@ -1511,10 +1512,14 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
       const long ni = T.n_internal[d];
       if (ni == 0) continue;
       // the 8 children of the level's k-th internal node are the k-th block
-      // of 8 rows of the next level: one row of 8*dim values per parent
-      ++ctx.n_launch;
+      // of 8 rows of the next level: one row of 8*dim values per parent.  The
+      // long K (8 children) is split per child, so that the coarse levels
+      // with few parents still fill the GPU; the 8 pieces are added in order.
+      ctx.n_launch += 2;
+      double* part = ctx.tmp_c.as<double>((size_t)8 * ni * dim);
       translate_gemm(s, ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim, nullptr,
-                     ctx.dops.u2u.get<double>(), dim, ue, dim, T.int_idx.get<int>() + T.int_off[d], nullptr, false);
+                     ctx.dops.u2u.get<double>(), dim, ue, dim, T.int_idx.get<int>() + T.int_off[d], nullptr, false, 8,
+                     part);
     }
   }
   // mixed form, Stokes kernel: the FP32 stages (V-list input, W list) read
@@ -1536,6 +1541,10 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   } else {
     ev(4);
     ev(5);
+  }
+  if (ctx.tc5_err) {  // the tensor-core Hadamard's error word, checked by the caller after synchronising
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(ctx.tc5_err_host, ctx.tc5_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ctx.tc5_err = nullptr;
   }
   ev(6);
   // ---- X-list
@@ -1651,7 +1660,16 @@ void upload_operators(Context& ctx) {
   upload_vec<double>(ctx.dops.usurf, h.usurf, s);
   if (ctx.precision == 0) upload_vec<double>(ctx.dops.vop, h.vop, s);
   else upload_vec<float>(ctx.dops.vop, h.vop, s);
-  if (ctx.precision == 1 && ctx.ki.ke == 1) upload_vop_fragments(ctx);
+  if (ctx.precision == 1 && ctx.ki.ke == 1) {
+    upload_vop_fragments(ctx);
+    std::vector<float> lay;
+    hadamard_tc5_operator_layout(h.vop, 4 * ctx.m * ctx.m * (ctx.m + 1), lay);
+    float* dev = ctx.dops.vop_tc5.as<float>(lay.size());
+    PVFMM_CUDA_CHECK(cudaMemcpyAsync(dev, lay.data(), lay.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (!ctx.tc5_err_host) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.tc5_err_host, sizeof(int)));
+    *ctx.tc5_err_host = 0;
+  }
   if (ctx.precision == 1 && ctx.ki.ke == 3) upload_vec<double>(ctx.dops.ue_proj, h.ue_proj, s);
   int* fm = ctx.dops.fft_map.as<int>(h.fft_map.size());
   int* im = ctx.dops.ifft_map.as<int>(h.ifft_map.size());

@@ -52,6 +52,7 @@ struct DevTree {
 struct DevOps {
   DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
   DevBuf vop_frag;  // mixed form, ke = 1: Hadamard operators as TF32 hi/lo MMA fragments
+  DevBuf vop_tc5;   // mixed form, ke = 1: Hadamard operators in the tcgen05 shared-memory layout
   DevBuf ue_proj;   // mixed form: projector applied to the upward equivalent densities
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
@@ -90,6 +91,9 @@ struct Context {
   void* pinned = nullptr;
   size_t pinned_cap = 0;
   int* chk = nullptr;  // pinned slots for counts read back at the end of a tree build
+  int* tc5_err = nullptr;  // device error word of the running evaluation's tcgen05 Hadamard (nullptr: none)
+  DevBuf tc5_err_buf;
+  int* tc5_err_host = nullptr;  // pinned copy of it, read after the evaluation synchronises
   // host-pointer evaluations upload the densities on a side stream while the
   // tree is built; the evaluation waits for den_ev when den_pending
   cudaStream_t side = nullptr;
@@ -103,10 +107,16 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
 // eval.cu
 void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
 void upload_operators(Context& ctx);
+// hadamard_tc.cu: mixed-form V-list Hadamard of target parents [p0, p0+np)
+// on tcgen05 (rows of sout relative to p0), and its operator layout
+void launch_hadamard_tc5(Context& ctx, int n3h, const void* sin_, void* sout, long p0, long np);
+void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::vector<float>& out);
 // translate.cu: C[crow(i)] (+)= 2^-depth(key[arow(i)]) A[arow(i)] B on the FP64
-// tensor cores (rows gathered / scattered through the index lists when given)
+// tensor cores (rows gathered / scattered through the index lists when given);
+// with ksplit > 1 the K range is cut into ksplit equal pieces summed in
+// `partial` (ksplit * M * N doubles) and added in a fixed order
 void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long lda, const int* arows,
                     const double* B, long ldb, double* C, long ldc, const int* crows, const MKey* scale_keys,
-                    bool accumulate);
+                    bool accumulate, int ksplit = 1, double* partial = nullptr);
 
 }  // namespace pvfmm_b200

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     translate_gemm_kernel(int M, int N, int K, const double* __restrict__ A, long lda, const int* __restrict__ arows,
                           const double* __restrict__ B, long ldb, double* __restrict__ C, long ldc,
                           const int* __restrict__ crows, const MKey* __restrict__ keys, int accumulate,
-                          long m_base) {
+                          long m_base, int kchunk, double* __restrict__ partial) {
   __shared__ __align__(16) double As[2][kBM * kAStride];
   __shared__ __align__(16) double Bs[2][kBK * kBStride];
   __shared__ long arow_s[kBM];
@@ -70,6 +70,8 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   const long m0 = m_base + (long)blockIdx.y * kBM;
   const int n0 = blockIdx.x * kBN;
   const RowMap amap{arows};
+  // split K: this block sums k in [kbeg, kend) (the whole of K without a split)
+  const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
   if (tid < kBM) arow_s[tid] = m0 + tid < M ? amap(m0 + tid) : -1;
   __syncthreads();
   // copy plan: A tile 64 rows x 16 doubles = 512 chunks of 16 B, 2 per thread;
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
       const int c = tid + u * kThreadsG;
       const int r = c >> 3, kc = (c & 7) * 2;  // row, first double of the chunk
       const long ar = arow_s[r];
-      const bool v = ar >= 0 && k0 + kc < K;
+      const bool v = ar >= 0 && k0 + kc < kend;
       const double* src = v ? A + ar * lda + k0 + kc : A;
       cp16(&As[buf][r * kAStride + kc], src, v);
     }
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     for (int u = 0; u < 2; ++u) {
       const int c = tid + u * kThreadsG;
       const int r = c >> 5, nc = (c & 31) * 2;
-      const bool v = k0 + r < K && n0 + nc < N;
+      const bool v = k0 + r < kend && n0 + nc < N;
       const double* src = v ? B + (long)(k0 + r) * ldb + n0 + nc : B;
       cp16(&Bs[buf][r * kBStride + nc], src, v);
     }
@@ -99,12 +101,12 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  const int nk = (K + kBK - 1) / kBK;
-  issue(0, 0);
+  const int nk = (kend - kbeg + kBK - 1) / kBK;
+  issue(kbeg, 0);
   for (int ks = 0; ks < nk; ++ks) {
     const int buf = ks & 1;
     if (ks + 1 < nk) {
-      issue((ks + 1) * kBK, buf ^ 1);
+      issue(kbeg + (ks + 1) * kBK, buf ^ 1);
       cp_wait<1>();
     } else {
       cp_wait<0>();
@@ -131,6 +133,15 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   for (int i = 0; i < 4; ++i) {
     const long mi = m0 + wm * 32 + i * 8 + g;
     if (mi >= M) continue;
+    if (partial) {  // split K: plain partial sums, reduced by translate_reduce
+      double* prow = partial + ((long)blockIdx.z * M + mi) * N;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int n = n0 + wn * 16 + j * 8 + 2 * t;
+        if (n < N) *reinterpret_cast<double2*>(prow + n) = make_double2(acc[i][j][0], acc[i][j][1]);
+      }
+      continue;
+    }
     double s = 1.0;
     if (keys) s = ldexp(1.0, -(int)(keys[arow_s[mi - m0]].lo & 31u));
     const long cr = crows ? (long)crows[mi] : mi;
@@ -151,12 +162,29 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   }
 }
 
+// C[crow(i)][n] (+)= s(i) * sum_z partial[z][i][n], the K pieces added in order.
+__global__ void translate_reduce(long M, int N, int ksplit, const double* __restrict__ partial,
+                                 const int* __restrict__ arows, const int* __restrict__ crows,
+                                 const MKey* __restrict__ keys, int accumulate, double* __restrict__ C, long ldc) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= M * N) return;
+  const long i = e / N;
+  const int n = (int)(e % N);
+  double v = 0;
+  for (int z = 0; z < ksplit; ++z) v += partial[((long)z * M + i) * N + n];
+  if (keys) v *= ldexp(1.0, -(int)(keys[arows ? arows[i] : i].lo & 31u));
+  double* c = C + (crows ? (long)crows[i] : i) * ldc + n;
+  *c = accumulate ? *c + v : v;
+}
+
 }  // namespace
 
 void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long lda, const int* arows,
                     const double* B, long ldb, double* C, long ldc, const int* crows, const MKey* scale_keys,
-                    bool accumulate) {
+                    bool accumulate, int ksplit, double* partial) {
   if (M <= 0 || N <= 0) return;
+  if (ksplit < 1 || (ksplit > 1 && (!partial || K % ksplit != 0 || (K / ksplit) % 2 != 0)))
+    throw std::runtime_error("translate_gemm: bad K split");
   if ((N & 1) || (K & 1) || (lda & 1) || (ldb & 1) || (ldc & 1))
     throw std::runtime_error("translate_gemm: row lengths must be even (16-byte rows)");
   if (M >= (1L << 31)) throw std::runtime_error("translate_gemm: too many rows");
@@ -164,9 +192,15 @@ void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long 
   // A rows in L2); row tiles in launches of at most 65535
   const long tiles = (M + kBM - 1) / kBM;
   for (long t0 = 0; t0 < tiles; t0 += 65535) {
-    dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)std::min(65535L, tiles - t0));
+    dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)std::min(65535L, tiles - t0), (unsigned)ksplit);
     translate_gemm_kernel<<<grid, kThreadsG, 0, s>>>((int)M, N, K, A, lda, arows, B, ldb, C, ldc, crows, scale_keys,
-                                                      accumulate ? 1 : 0, t0 * kBM);
+                                                      accumulate ? 1 : 0, t0 * kBM, K / ksplit,
+                                                      ksplit > 1 ? partial : nullptr);
+    PVFMM_CUDA_CHECK(cudaGetLastError());
+  }
+  if (ksplit > 1) {
+    translate_reduce<<<(unsigned)((M * N + 255) / 256), 256, 0, s>>>(M, N, ksplit, partial, arows, crows, scale_keys,
+                                                                     accumulate ? 1 : 0, C, ldc);
     PVFMM_CUDA_CHECK(cudaGetLastError());
   }
 }
@@ -175,21 +209,24 @@ void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long 
 
 // Self-check of the FP64 translation product on random data (internal entry
 // point used by the GPU tests; no counterpart in the reference): computes
-// C[crow(i)] (+)= s(i) A[arow(i)] B on device copies of the host arrays and
-// copies C back.  arows / crows / depth may be NULL.  Returns 0 on success.
+// C[crow(i)] (+)= s(i) A[arow(i)] B on device copies of the host arrays (K
+// split into `ksplit` pieces when > 1) and copies C back.  arows / crows /
+// depth may be NULL.  Returns 0 on success.
 extern "C" int PVFMMB200TranslateGemmCheck(long M, int N, int K, const double* A, long a_rows, const int* arows,
                                            const double* B, double* C, long c_rows, const int* crows,
-                                           const int* depth_of_arow_target, int accumulate) {
+                                           const int* depth_of_arow_target, int accumulate, int ksplit) {
   using namespace pvfmm_b200;
   void* buf = nullptr;
   try {
     const size_t nA = (size_t)a_rows * K, nB = (size_t)K * N, nC = (size_t)c_rows * N;
-    const size_t bytes = (nA + nB + nC) * 8 + (size_t)M * 4 * 2 + (size_t)a_rows * sizeof(MKey) + 256;
+    const size_t nP = ksplit > 1 ? (size_t)ksplit * M * N : 0;
+    const size_t bytes = (nA + nB + nC + nP) * 8 + (size_t)M * 4 * 2 + (size_t)a_rows * sizeof(MKey) + 256;
     PVFMM_CUDA_CHECK(cudaMalloc(&buf, bytes));
     double* dA = (double*)buf;
     double* dB = dA + nA;
     double* dC = dB + nB;
-    int* dar = (int*)(dC + nC);
+    double* dP = dC + nC;
+    int* dar = (int*)(dP + nP);
     int* dcr = dar + M;
     MKey* dk = (MKey*)(((uintptr_t)(dcr + M) + 15) & ~(uintptr_t)15);
     PVFMM_CUDA_CHECK(cudaMemcpy(dA, A, nA * 8, cudaMemcpyHostToDevice));
@@ -203,7 +240,7 @@ extern "C" int PVFMMB200TranslateGemmCheck(long M, int N, int K, const double* A
       PVFMM_CUDA_CHECK(cudaMemcpy(dk, k.data(), a_rows * sizeof(MKey), cudaMemcpyHostToDevice));
     }
     translate_gemm(nullptr, M, N, K, dA, K, arows ? dar : nullptr, dB, N, dC, N, crows ? dcr : nullptr,
-                   depth_of_arow_target ? dk : nullptr, accumulate != 0);
+                   depth_of_arow_target ? dk : nullptr, accumulate != 0, ksplit, dP);
     PVFMM_CUDA_CHECK(cudaMemcpy(C, dC, nC * 8, cudaMemcpyDeviceToHost));
     cudaFree(buf);
     set_last_error("");

@@ -338,3 +338,21 @@ def test_tree_build_writes_stay_in_bounds_on_a_count_mismatch():
     f.argtypes = [ctypes.c_long, ctypes.c_long]
     for n, cap in [(1000, 600), (4096, 0), (300, 300)]:
         assert f(n, cap) == 0, P.last_error()
+
+
+def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
+    """The mixed form's V-list products on the 5th-generation tensor cores
+    (tcgen05, TMEM accumulators) and on the warp-level MMA path give the same
+    FMM result to well within the mixed form's accuracy (both carry each
+    product to ~2^-22 with a 3-term TF32 split; only the accumulation order
+    inside the tensor cores differs)."""
+    src = points("gauss", 40000, 41)
+    den = np.random.default_rng(42).uniform(-1, 1, 40000)
+    a, ctx = gpu_eval(6, 8, 128, src, den, src, prec=P.PRECISION_MIXED)
+    assert ctx.tree_stats()["n_vtrg"] > 200
+    ctx.close()
+    monkeypatch.setenv("PVFMM_B200_HADAMARD_MMA_SYNC", "1")
+    b, ctx = gpu_eval(6, 8, 128, src, den, src, prec=P.PRECISION_MIXED)
+    ctx.close()
+    for k in range(4):
+        assert O.rel_l2(a[:, k], b[:, k]) < 1e-7, k

@@ -110,7 +110,7 @@ def _translate_check():
     f.restype = ctypes.c_int
     vp = ctypes.c_void_p
     f.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_int, vp, ctypes.c_long, vp, vp, vp, ctypes.c_long, vp, vp,
-                  ctypes.c_int]
+                  ctypes.c_int, ctypes.c_int]
     return f
 
 
@@ -118,15 +118,17 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
-@pytest.mark.parametrize("M,N,K,gather,scatter,scale,acc", [
-    (1000, 296, 296, False, False, False, False),     # S2U / D2T pseudo-inverse products
-    (777, 296, 2368, False, True, False, False),      # U2U: 8 children per row, rows scattered to parents
-    (333, 2368, 296, True, False, False, True),       # D2D: parents gathered, children accumulated
-    (1500, 296, 296, True, False, True, False),       # D2T first product: gathered, scaled by 2^-depth
-    (65, 152, 10, False, False, False, False),        # ragged tiles in every direction
-    (64 * 65536 + 70, 8, 4, False, False, False, False),   # more than one launch of row tiles
+@pytest.mark.parametrize("M,N,K,gather,scatter,scale,acc,ksplit", [
+    (1000, 296, 296, False, False, False, False, 1),     # S2U / D2T pseudo-inverse products
+    (777, 296, 2368, False, True, False, False, 1),      # U2U: 8 children per row, rows scattered to parents
+    (777, 296, 2368, False, True, False, False, 8),      # U2U with K split per child
+    (3, 296, 2368, False, True, True, True, 8),          # split K with scaling and accumulation, few rows
+    (333, 2368, 296, True, False, False, True, 1),       # D2D: parents gathered, children accumulated
+    (1500, 296, 296, True, False, True, False, 1),       # D2T first product: gathered, scaled by 2^-depth
+    (65, 152, 10, False, False, False, False, 1),        # ragged tiles in every direction
+    (64 * 65536 + 70, 8, 4, False, False, False, False, 1),   # more than one launch of row tiles
 ])
-def test_translate_products_match_fp64_host_products(M, N, K, gather, scatter, scale, acc):
+def test_translate_products_match_fp64_host_products(M, N, K, gather, scatter, scale, acc, ksplit):
     f = _translate_check()
     rng = np.random.default_rng(M + N + K)
     a_rows = M + 50 if gather else M
@@ -147,7 +149,7 @@ def test_translate_products_match_fp64_host_products(M, N, K, gather, scatter, s
     else:
         want = prod + (C if acc else 0)
     got = C.copy()
-    rc = f(M, N, K, _p(A), a_rows, _p(arows), _p(B), _p(got), c_rows, _p(crows), _p(depth), 1 if acc else 0)
+    rc = f(M, N, K, _p(A), a_rows, _p(arows), _p(B), _p(got), c_rows, _p(crows), _p(depth), 1 if acc else 0, ksplit)
     assert rc == 0, P.last_error()
     err = np.abs(got - want).max() / np.abs(want).max()
     assert err < 1e-14 * max(1, K / 64), err
