@@ -46,8 +46,7 @@ KERNEL_DIMS = {
     FMMKernel.BiotSavartPotential: (3, 3),
     FMMKernel.LaplacePotGrad: (1, 4),
 }
-SUPPORTED = {FMMKernel.LaplacePotential, FMMKernel.LaplaceGradient, FMMKernel.StokesVelocity,
-             FMMKernel.LaplacePotGrad}
+SUPPORTED = set(FMMKernel)  # every PVFMMKernel value plus the pot+grad extension
 
 PRECISION_PLAIN = 0
 PRECISION_MIXED = 1

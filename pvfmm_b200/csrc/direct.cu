@@ -85,6 +85,9 @@ int ker_type(int kernel) {
     case kLaplaceGrad: return kKerLaplaceGrad;
     case kStokesVel: return kKerStokes;
     case kLaplacePotGrad: return kKerLaplacePG;
+    case kStokesPress: return kKerStokesPress;
+    case kStokesVelGrad: return kKerStokesGrad;
+    case kBiotSavart: return kKerBiotSavart;
     default: throw std::runtime_error("unsupported PVFMMKernel value " + std::to_string(kernel));
   }
 }
@@ -108,30 +111,27 @@ int choose_chunks(long n_src, long n_trg, long cap_chunks) {
 
 }  // namespace
 
+template <int Ker>
+void direct_eval_t(const double* src, const double* den, long n_src, const double* trg, double* out, long n_trg,
+                   int n_chunks, double* partial, cudaStream_t s) {
+  constexpr int KT = KerDims<Ker>::KT;
+  dim3 grid((unsigned)((n_trg + kDT - 1) / kDT), (unsigned)n_chunks);
+  const unsigned rb = (unsigned)((n_trg * KT + 255) / 256);
+  direct_partial_kernel<Ker><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
+  direct_reduce_kernel<KT><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(Ker), out);
+}
+
 // Launches the two kernels with `partial` holding n_chunks * n_trg * KT doubles.
 void direct_eval(int kernel, const double* src, const double* den, long n_src, const double* trg, double* out, long n_trg,
                  int n_chunks, double* partial, cudaStream_t s) {
-  const int kt = ker_type(kernel);
-  dim3 grid((unsigned)((n_trg + kDT - 1) / kDT), (unsigned)n_chunks);
-  const long nout = n_trg * (kernel == kLaplacePot ? 1 : kernel == kLaplacePotGrad ? 4 : 3);
-  const unsigned rb = (unsigned)((nout + 255) / 256);
-  switch (kt) {
-    case kKerLaplace:
-      direct_partial_kernel<kKerLaplace><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
-      direct_reduce_kernel<1><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplace), out);
-      break;
-    case kKerLaplaceGrad:
-      direct_partial_kernel<kKerLaplaceGrad><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
-      direct_reduce_kernel<3><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplaceGrad), out);
-      break;
-    case kKerStokes:
-      direct_partial_kernel<kKerStokes><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
-      direct_reduce_kernel<3><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerStokes), out);
-      break;
-    default:
-      direct_partial_kernel<kKerLaplacePG><<<grid, kDT, 0, s>>>(src, den, n_src, trg, n_trg, n_chunks, partial);
-      direct_reduce_kernel<4><<<rb, 256, 0, s>>>(partial, n_trg, n_chunks, ker_scale(kKerLaplacePG), out);
-      break;
+  switch (ker_type(kernel)) {
+    case kKerLaplace: direct_eval_t<kKerLaplace>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    case kKerLaplaceGrad: direct_eval_t<kKerLaplaceGrad>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    case kKerStokes: direct_eval_t<kKerStokes>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    case kKerStokesPress: direct_eval_t<kKerStokesPress>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    case kKerStokesGrad: direct_eval_t<kKerStokesGrad>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    case kKerBiotSavart: direct_eval_t<kKerBiotSavart>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
+    default: direct_eval_t<kKerLaplacePG>(src, den, n_src, trg, out, n_trg, n_chunks, partial, s); break;
   }
   PVFMM_CUDA_CHECK(cudaGetLastError());
 }

@@ -372,7 +372,9 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
   using V = typename Vec16<Real>::type;
   __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
   __shared__ double2 tile64[kF32 ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
-  __shared__ double red[kNF][2][KT];
+  // the partial sums of the final fixed-order reduction reuse the tiles
+  static_assert(sizeof(tiles) >= sizeof(double) * kNF * 2 * KT, "reduction buffer larger than the tiles");
+  double(*red)[2][KT] = reinterpret_cast<double(*)[2][KT]>(&tiles[0][0]);
   __shared__ NearSeg seg[kSegCap];
   __shared__ int start[kSegCap + 1];
   const int b = blockIdx.x;
@@ -537,7 +539,9 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
         buf ^= 1;
       }
     }
-    // fixed-order sum of the G partial sums of each target
+    // fixed-order sum of the G partial sums of each target (in the tiles'
+    // memory: every thread is done reading them past this barrier)
+    __syncthreads();
     if (active)
 #pragma unroll
       for (int k = 0; k < KT; ++k) {
@@ -577,7 +581,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
     int mode, const int* __restrict__ nodes, const MKey* __restrict__ keys, const int* __restrict__ slo,
     const int* __restrict__ shi, const int* __restrict__ x_off, const int* __restrict__ x_list,
     const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz,
-    const double* __restrict__ den, const double* __restrict__ usurf, int ns, double rad, double scale,
+    const double* __restrict__ den, const double* __restrict__ usurf, int ns, double rad, double scale, int deg,
     double* __restrict__ out) {
   constexpr int KT = KerDims<Ker>::KT;
   __shared__ Tile<double, KerDims<Ker>::KS> tl;
@@ -590,7 +594,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
   const double hr = half * rad;
   const int dim = ns * KT;
   double* o = mode == 0 ? out + (long)b * dim : out + (long)T * dim;
-  const double oscale = mode == 0 ? scale * ldexp(1.0, -dT) : scale;
+  const double oscale = mode == 0 ? scale * ldexp(1.0, -deg * dT) : scale;
   for (int c0 = 0; c0 < ns; c0 += kNT) {
     const Split sp(ns - c0);
     const int k = c0 + sp.ti;
@@ -756,7 +760,7 @@ template <class Real, int M>
 __global__ void __launch_bounds__(288) ifft_dn_kernel(int ke, int G, int ngroups, const int* __restrict__ vtrg,
                                                        const int* __restrict__ child0, const MKey* __restrict__ keys,
                                                        const Cplx<Real>* __restrict__ spec,
-                                                       const int* __restrict__ ifft_map, int ns,
+                                                       const int* __restrict__ ifft_map, int ns, int deg,
                                                        double* __restrict__ dc) {
   using F = FftSizes<Real, M>;
   constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
@@ -775,7 +779,7 @@ __global__ void __launch_bounds__(288) ifft_dn_kernel(int ke, int G, int ngroups
   const int c0 = child0[P];
   unsigned int X, Y, Z, dP;
   decode_key(keys[P], X, Y, Z, dP);
-  const double lscale = ldexp(1.0, (int)dP + 1);  // 2^(trg_scal * level of the children)
+  const double lscale = ldexp(1.0, deg * ((int)dP + 1));  // 2^(trg_scal * level of the children)
   const int dim = ns * ke;
   for (int j = threadIdx.x; j < N1; j += blockDim.x) {
     double sn, cs;
@@ -865,52 +869,48 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Hadamard products (VListHadamard, fmm_pts.txx:3249-3344), organised as a
-// register-tiled SIMT product per frequency f:
-//   OUT[P][j1] += sum_{offset o, source child j2} M[f][o][j1][j2] * IN[Q_o(P)][f][j2].
-// A block owns 128*PB target parents at one frequency; a thread owns PB of
-// them and all their 8 x ke outputs.  The offset blocks of frequency f sit in
-// shared memory (chunks of OC offsets), read by every thread at the same
-// address (broadcast).  The neighbour spectra of offset o+1 are copied
-// asynchronously into a second shared buffer while offset o is computed;
-// a thread only reads the rows it copied itself, so waiting on its own copy
-// group is enough.  Missing neighbours are zero-filled and skipped.
-template <class Real, int KE, int PB, int OC>
+// Hadamard products (VListHadamard, fmm_pts.txx:3249-3344) for vector
+// expansions, organised as a register-tiled SIMT product per frequency f:
+//   OUT[P][j1][c] += sum_{offset o, source child j2, i} M[f][o][j1][j2][i][c] * IN[Q_o(P)][f][j2][i]
+// (KI equivalent-density components i, KO check-potential components c).  A
+// block owns 128 target parents at one frequency and KOC output components
+// (blockIdx.z picks the group); a thread owns one parent.  The offset blocks
+// of frequency f sit in shared memory (chunks of OC offsets), read by every
+// thread at the same address (broadcast).  The neighbour spectra of offset
+// o+1 are copied asynchronously into a second shared buffer while offset o is
+// computed; a thread only reads the rows it copied itself, so waiting on its
+// own copy group is enough.  Missing neighbours are zero-filled and skipped.
+template <class Real, int KI, int KO, int KOC, int OC>
 __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, long vt_stride, const int* __restrict__ vtab,
                                                        const Cplx<Real>* __restrict__ spec_in,
                                                        const Cplx<Real>* __restrict__ vop,
                                                        Cplx<Real>* __restrict__ spec_out) {
-  constexpr int NG = 8 * KE;
-  constexpr int BLK = 64 * KE * KE;                              // complex entries per offset
-  constexpr int ROW = NG * sizeof(Cplx<Real>) / 16;              // 16-byte chunks per spectrum row
-  constexpr int STRIDE = NG + 16 / (int)sizeof(Cplx<Real>) * 1;  // padded row (complex), breaks bank aliasing
+  constexpr int NGI = 8 * KI, NGO = 8 * KOC;
+  constexpr int BLK = 64 * KI * KO;                               // complex entries per offset
+  constexpr int ROW = NGI * sizeof(Cplx<Real>) / 16;              // 16-byte chunks per input row
+  constexpr int STRIDE = NGI + 16 / (int)sizeof(Cplx<Real>);      // padded row (complex), breaks bank aliasing
   constexpr int NT = 128;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cplx<Real>* Ms = reinterpret_cast<Cplx<Real>*>(smem_raw);      // OC * BLK
-  Cplx<Real>* xb = Ms + OC * BLK;                                // 2 * NT*PB * STRIDE
+  Cplx<Real>* Ms = reinterpret_cast<Cplx<Real>*>(smem_raw);       // OC * BLK
+  Cplx<Real>* xb = Ms + OC * BLK;                                 // 2 * NT * STRIDE
   const int f = blockIdx.y;
-  const long base = (long)blockIdx.x * NT * PB + threadIdx.x;
-  Real ar[PB][NG], ai[PB][NG];
+  const int c0 = blockIdx.z * KOC;
+  const long p = (long)blockIdx.x * NT + threadIdx.x;
+  Real ar[NGO], ai[NGO];
 #pragma unroll
-  for (int k = 0; k < PB; ++k)
+  for (int j = 0; j < NGO; ++j) ar[j] = ai[j] = 0;
+  auto issue = [&](int o, int buf) {
+    const int q = (o < 26 && p < n_vtrg) ? __ldg(vtab + (long)o * vt_stride + p) : -1;
+    const Cplx<Real>* src = spec_in + ((long)(q < 0 ? 0 : q) * n3h + f) * NGI;
+    Cplx<Real>* dst = xb + ((long)buf * NT + threadIdx.x) * STRIDE;
 #pragma unroll
-    for (int j = 0; j < NG; ++j) ar[k][j] = ai[k][j] = 0;
-  auto issue = [&](int o, int buf, int* q) {
-#pragma unroll
-    for (int k = 0; k < PB; ++k) {
-      const long p = base + (long)k * NT;
-      q[k] = (o < 26 && p < n_vtrg) ? __ldg(vtab + (long)o * vt_stride + p) : -1;
-      const Cplx<Real>* src = spec_in + ((long)(q[k] < 0 ? 0 : q[k]) * n3h + f) * NG;
-      Cplx<Real>* dst = xb + ((long)buf * NT * PB + threadIdx.x + k * NT) * STRIDE;
-#pragma unroll
-      for (int c = 0; c < ROW; ++c)
-        cp_async16(reinterpret_cast<unsigned char*>(dst) + 16 * c, reinterpret_cast<const unsigned char*>(src) + 16 * c,
-                   q[k] >= 0 ? 16 : 0);
-    }
+    for (int c = 0; c < ROW; ++c)
+      cp_async16(reinterpret_cast<unsigned char*>(dst) + 16 * c, reinterpret_cast<const unsigned char*>(src) + 16 * c,
+                 q >= 0 ? 16 : 0);
     cp_async_commit();
+    return q;
   };
-  int qc[PB], qn[PB];
-  issue(0, 0, qc);
+  int qc = issue(0, 0), qn = -1;
   for (int oc = 0; oc < 26; oc += OC) {
     const int no = min(OC, 26 - oc);
     __syncthreads();
@@ -919,42 +919,38 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, lon
     __syncthreads();
     for (int oo = 0; oo < no; ++oo) {
       const int o = oc + oo;
-      issue(o + 1, (o + 1) & 1, qn);   // empty group past the last offset
-      cp_async_wait<1>();              // this thread's rows of offset o have landed
+      qn = issue(o + 1, (o + 1) & 1);   // empty group past the last offset
+      cp_async_wait<1>();               // this thread's row of offset o has landed
       const Cplx<Real>* Mo = Ms + oo * BLK;
-#pragma unroll
-      for (int k = 0; k < PB; ++k) {
-        if (qc[k] < 0) continue;
-        const Cplx<Real>* xr = xb + ((long)(o & 1) * NT * PB + threadIdx.x + k * NT) * STRIDE;
+      if (qc >= 0) {
+        const Cplx<Real>* xr = xb + ((long)(o & 1) * NT + threadIdx.x) * STRIDE;
 #pragma unroll
         for (int j2 = 0; j2 < 8; ++j2) {
-          Cplx<Real> x[KE];
+          Cplx<Real> x[KI];
 #pragma unroll
-          for (int i = 0; i < KE; ++i) x[i] = xr[j2 * KE + i];
+          for (int i = 0; i < KI; ++i) x[i] = xr[j2 * KI + i];
 #pragma unroll
           for (int j1 = 0; j1 < 8; ++j1)
 #pragma unroll
-            for (int i = 0; i < KE; ++i)
+            for (int i = 0; i < KI; ++i)
 #pragma unroll
-              for (int c = 0; c < KE; ++c) {
-                const Cplx<Real> a = Mo[((j1 * 8 + j2) * KE + i) * KE + c];
-                ar[k][j1 * KE + c] += a.re * x[i].re - a.im * x[i].im;
-                ai[k][j1 * KE + c] += a.re * x[i].im + a.im * x[i].re;
+              for (int c = 0; c < KOC; ++c) {
+                const Cplx<Real> a = Mo[((j1 * 8 + j2) * KI + i) * KO + c0 + c];
+                ar[j1 * KOC + c] += a.re * x[i].re - a.im * x[i].im;
+                ai[j1 * KOC + c] += a.re * x[i].im + a.im * x[i].re;
               }
         }
       }
-#pragma unroll
-      for (int k = 0; k < PB; ++k) qc[k] = qn[k];
+      qc = qn;
     }
   }
   cp_async_wait<0>();
+  if (p < n_vtrg) {
+    Cplx<Real>* out = spec_out + (p * n3h + f) * (8 * KO);
 #pragma unroll
-  for (int k = 0; k < PB; ++k) {
-    const long p = base + (long)k * NT;
-    if (p >= n_vtrg) continue;
-    Cplx<Real>* out = spec_out + (p * n3h + f) * NG;
+    for (int j1 = 0; j1 < 8; ++j1)
 #pragma unroll
-    for (int j = 0; j < NG; ++j) out[j] = {ar[k][j], ai[k][j]};
+      for (int c = 0; c < KOC; ++c) out[j1 * KO + c0 + c] = {ar[j1 * KOC + c], ai[j1 * KOC + c]};
   }
 }
 
@@ -1304,23 +1300,23 @@ void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real
 #define PVFMM_HAD_PB_F64 1
 #endif
 
-template <class Real, int KE, int PB, int OC>
+template <class Real, int KI, int KO, int OC>
 size_t hadamard_smem() {
-  constexpr int NG = 8 * KE;
-  constexpr int STRIDE = NG + 16 / (int)sizeof(Cplx<Real>);
-  return sizeof(Cplx<Real>) * ((size_t)OC * 64 * KE * KE + 2 * 128 * PB * STRIDE);
+  constexpr int STRIDE = 8 * KI + 16 / (int)sizeof(Cplx<Real>);
+  return sizeof(Cplx<Real>) * ((size_t)OC * 64 * KI * KO + 2 * 128 * STRIDE);
 }
 
-template <class Real, int KE, int PB, int OC>
+template <class Real, int KI, int KO, int KOC, int OC>
 void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0, long np) {
+  static_assert(KO % KOC == 0, "output components in whole groups");
   DevTree& T = ctx.tree;
-  const size_t sm = hadamard_smem<Real, KE, PB, OC>();
-  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_kernel<Real, KE, PB, OC>,
+  const size_t sm = hadamard_smem<Real, KI, KO, OC>();
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_kernel<Real, KI, KO, KOC, OC>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dim3 grid(ceil_div(np, 128 * PB), n3h);
+  dim3 grid(ceil_div(np, 128), n3h, KO / KOC);
   ++ctx.n_launch;
-  hadamard_kernel<Real, KE, PB, OC><<<grid, 128, sm, ctx.stream>>>(n3h, np, T.n_vtrg, T.vtab.get<int>() + p0, sin_,
-                                                                   ctx.dops.vop.get<Cplx<Real>>(), sout);
+  hadamard_kernel<Real, KI, KO, KOC, OC><<<grid, 128, sm, ctx.stream>>>(n3h, np, T.n_vtrg, T.vtab.get<int>() + p0,
+                                                                         sin_, ctx.dops.vop.get<Cplx<Real>>(), sout);
 }
 
 // ---------------------------------------------------------------------------
@@ -1336,14 +1332,19 @@ __global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict
   for (int j = 0; j < k0; ++j) out[i * k0 + j] = (double)((Tin)in[p * k0 + j] * (Tin)sc[j]);
 }
 
+// Output scales scale_x^trg_scal[k] of the C interface's rescale, per output
+// component (at most 9).
+struct OutScales {
+  double v[9];
+};
+
 template <class Tout>
-__global__ void unsort_values(const double* __restrict__ pot, const int* __restrict__ perm, long n, int k1, double s0,
-                              double s1, double s2, double s3, Tout* __restrict__ out) {
+__global__ void unsort_values(const double* __restrict__ pot, const int* __restrict__ perm, long n, int k1,
+                              OutScales sc, Tout* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const long p = perm[i];
-  const double sc[4] = {s0, s1, s2, s3};
-  for (int k = 0; k < k1; ++k) out[p * k1 + k] = (Tout)((Tout)pot[i * k1 + k] * (Tout)sc[k]);
+  for (int k = 0; k < k1; ++k) out[p * k1 + k] = (Tout)((Tout)pot[i * k1 + k] * (Tout)sc.v[k]);
 }
 
 template <class Real>
@@ -1370,52 +1371,57 @@ int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
 // allows).  With several chunks, stage 4 ends after the first chunk's
 // products and stage 5 covers the rest.
 template <class Real, int M>
-void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int ke, long chunk,
-                 const std::function<void(int)>& ev) {
+void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
+                 long chunk, const std::function<void(int)>& ev) {
   DevTree& T = ctx.tree;
   auto s = ctx.stream;
   using F = FftSizes<Real, M>;
-  const int ngrid = 8 * ke;
-  const int Gu = grids_per_block<F>(F::up_grid_bytes, F::tw_bytes, ngrid, 64 * 1024);
+  const int ngrid_up = 8 * kin, ngrid_dn = 8 * kout;
+  const int Gu = grids_per_block<F>(F::up_grid_bytes, F::tw_bytes, ngrid_up, 64 * 1024);
   const size_t sm_up = F::tw_bytes + Gu * F::up_grid_bytes;
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(fft_up_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_up));
   ++ctx.n_launch;
-  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid / Gu), F::threads(Gu), sm_up, s>>>(ke, Gu, ngrid / Gu, T.vsrc.get<int>(),
-                                                                     T.child0.get<int>(), ue,
-                                                                     ctx.dops.fft_map.get<int>(), ctx.ns, T.n_vsrc,
-                                                                     sin_);
+  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid_up / Gu), F::threads(Gu), sm_up, s>>>(
+      kin, Gu, ngrid_up / Gu, T.vsrc.get<int>(), T.child0.get<int>(), ue, ctx.dops.fft_map.get<int>(), ctx.ns,
+      T.n_vsrc, sin_);
   ev(4);
   const int n3h = F::N3H;
-  const int Gd = grids_per_block<F>(F::dn_grid_bytes, F::tw_bytes, ngrid, 80 * 1024);
+  const int Gd = grids_per_block<F>(F::dn_grid_bytes, F::tw_bytes, ngrid_dn, 80 * 1024);
   const size_t sm_dn = F::tw_bytes + Gd * F::dn_grid_bytes;
   PVFMM_CUDA_CHECK(
       cudaFuncSetAttribute(ifft_dn_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
   for (long p0 = 0; p0 < T.n_vtrg; p0 += chunk) {
     const long np = std::min(chunk, T.n_vtrg - p0);
-    if (ke == 1) {
+    if (kin == 1 && kout == 1) {
       if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout, p0, np);
       else if (std::getenv("PVFMM_B200_HADAMARD_MMA_SYNC")) launch_hadamard_tc(ctx, n3h, sin_, sout, p0, np);
       else launch_hadamard_tc5(ctx, n3h, sin_, sout, p0, np);
-    } else {
-      launch_hadamard<Real, 3, 1, 4>(ctx, n3h, sin_, sout, p0, np);
+    } else if (kout == 3) {  // Stokes velocity, Biot-Savart
+      launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, sin_, sout, p0, np);
+    } else if (kout == 1) {  // Stokes pressure
+      launch_hadamard<Real, 3, 1, 1, 4>(ctx, n3h, sin_, sout, p0, np);
+    } else {  // Stokes velocity gradient: 9 outputs in 3 groups of 3
+      launch_hadamard<Real, 3, 9, 3, 2>(ctx, n3h, sin_, sout, p0, np);
     }
     if (p0 == 0) ev(5);
     ++ctx.n_launch;
-    ifft_dn_kernel<Real, M><<<np * (ngrid / Gd), F::threads(Gd), sm_dn, s>>>(
-        ke, Gd, ngrid / Gd, T.vtrg.get<int>() + p0, T.child0.get<int>(), T.key.get<MKey>(), sout,
-        ctx.dops.ifft_map.get<int>(), ctx.ns, dc);
+    ifft_dn_kernel<Real, M><<<np * (ngrid_dn / Gd), F::threads(Gd), sm_dn, s>>>(
+        kout, Gd, ngrid_dn / Gd, T.vtrg.get<int>() + p0, T.child0.get<int>(), T.key.get<MKey>(), sout,
+        ctx.dops.ifft_map.get<int>(), ctx.ns, ctx.ki.deg, dc);
   }
 }
 
+// V-list of equivalent densities with kin components onto check potentials
+// with kout components.
 template <class Real>
-void vlist(Context& ctx, const double* ue, double* dc, int ke, const std::function<void(int)>& ev) {
+void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const std::function<void(int)>& ev) {
   DevTree& T = ctx.tree;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);
-  Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * 8 * ke);
+  Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * 8 * kin);
   // output spectra: all target parents at once when they fit in 90% of the
   // free device memory (counting this buffer's current allocation), else
   // chunks of that size
-  const size_t row = (size_t)n3h * 8 * ke * sizeof(Cplx<Real>);
+  const size_t row = (size_t)n3h * 8 * kout * sizeof(Cplx<Real>);
   long chunk = T.n_vtrg;
   if ((size_t)T.n_vtrg * row > ctx.spec_out.cap) {  // query the device only when the buffer must grow
     size_t free_b = 0, total_b = 0;
@@ -1428,16 +1434,16 @@ void vlist(Context& ctx, const double* ue, double* dc, int ke, const std::functi
     const long c = std::atol(e);
     if (c > 0) chunk = std::min(chunk, c);
   }
-  Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * ke);
+  Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * kout);
   switch (m) {
-    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
-    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, ke, chunk, ev); break;
+    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
     default: throw std::runtime_error("unsupported multipole order");
   }
 }
@@ -1446,7 +1452,11 @@ template <class Real, int KerS2T, int KerExp>
 void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float) {
   DevTree& T = ctx.tree;
   auto s = ctx.stream;
-  const int ns = ctx.ns, ke = ctx.ki.ke, dim = ns * ke;
+  // expansion dims: equivalent densities din = ns*kin, check potentials
+  // dout = ns*kout (kin = kout for Laplace and Stokes velocity); the
+  // pseudo-inverse factors pass through r = min(din, dout) values
+  const int ns = ctx.ns, kin = KerDims<KerExp>::KS, kout = KerDims<KerExp>::KT;
+  const int din = ns * kin, dout = ns * kout, rk = std::min(din, dout), deg = ctx.ki.deg;
   const int k0 = ctx.ki.k0, k1 = ctx.ki.k1;
   const long N = T.n_nodes;
   const MKey* keys = T.key.get<MKey>();
@@ -1460,11 +1470,12 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   }
   // densities (sorted, scaled by scale_x^src_scal: pvfmm-wrapper.cpp:522-541, 591-595)
   double* den = ctx.den.as<double>(std::max(T.n_src, 1L) * k0);
-  double ss[3], ts[4];
+  double ss[3];
+  OutScales ts;
   for (int j = 0; j < 3; ++j) ss[j] = den_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.src_scal[j])
                                                 : std::pow(T.scale_x, ctx.ki.src_scal[j]);
-  for (int j = 0; j < 4; ++j) ts[j] = out_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.trg_scal[j])
-                                                : std::pow(T.scale_x, ctx.ki.trg_scal[j]);
+  for (int j = 0; j < 9; ++j) ts.v[j] = out_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.trg_scal[j])
+                                                  : std::pow(T.scale_x, ctx.ki.trg_scal[j]);
   if (T.src_counted) {
     ++ctx.n_launch;
     if (den_float)
@@ -1474,10 +1485,10 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
       sort_densities<double><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const double*)den_in, T.src_perm.get<int>(),
                                                                     T.n_src, k0, ss[0], ss[1], ss[2], den);
   }
-  double* ue = ctx.ue.as<double>((size_t)N * dim);
-  double* dc = ctx.dc.as<double>((size_t)N * dim);
-  PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * dim * sizeof(double), s));
-  PVFMM_CUDA_CHECK(cudaMemsetAsync(dc, 0, (size_t)N * dim * sizeof(double), s));
+  double* ue = ctx.ue.as<double>((size_t)N * din);
+  double* dc = ctx.dc.as<double>((size_t)N * dout);
+  PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * din * sizeof(double), s));
+  PVFMM_CUDA_CHECK(cudaMemsetAsync(dc, 0, (size_t)N * dout * sizeof(double), s));
   const double* usurf = ctx.dops.usurf.get<double>();
   const double* sx = T.sx.get<double>();
   const double* sy = T.sy.get<double>();
@@ -1488,8 +1499,8 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   ev(1);
   // ---- S2U
   if (T.src_counted && T.n_sleaf > 0) {
-    double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dim);
-    double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * dim);
+    double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dout);
+    double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * rk);
     ++ctx.n_launch;
     // full FP64 rsqrt here in both forms: the check potentials feed the
     // FP64-cutoff pseudo-inverse, which amplifies their rounding into
@@ -1497,12 +1508,13 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     // V-list does not cancel those (one Newton step here raised the 4M-point
     // potential error from 3e-7 to 2.5e-6)
     surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
-        0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, uc);
+        0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, deg,
+        uc);
     // equivalent densities (uc UC2UE0) UC2UE1 straight into the leaves' rows of UE
     ctx.n_launch += 2;
-    translate_gemm(s, T.n_sleaf, dim, dim, uc, dim, nullptr, ctx.dops.uc2ue0.get<double>(), dim, t1, dim, nullptr,
+    translate_gemm(s, T.n_sleaf, rk, dout, uc, dout, nullptr, ctx.dops.uc2ue0.get<double>(), rk, t1, rk, nullptr,
                    nullptr, false);
-    translate_gemm(s, T.n_sleaf, dim, dim, t1, dim, nullptr, ctx.dops.uc2ue1.get<double>(), dim, ue, dim,
+    translate_gemm(s, T.n_sleaf, din, rk, t1, rk, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue, din,
                    T.sleaf.get<int>(), nullptr, false);
   }
   ev(2);
@@ -1512,13 +1524,13 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
       const long ni = T.n_internal[d];
       if (ni == 0) continue;
       // the 8 children of the level's k-th internal node are the k-th block
-      // of 8 rows of the next level: one row of 8*dim values per parent.  The
+      // of 8 rows of the next level: one row of 8*din values per parent.  The
       // long K (8 children) is split per child, so that the coarse levels
       // with few parents still fill the GPU; the 8 pieces are added in order.
       ctx.n_launch += 2;
-      double* part = ctx.tmp_c.as<double>((size_t)8 * ni * dim);
-      translate_gemm(s, ni, dim, 8 * dim, ue + (size_t)T.level_off[d + 1] * dim, 8 * dim, nullptr,
-                     ctx.dops.u2u.get<double>(), dim, ue, dim, T.int_idx.get<int>() + T.int_off[d], nullptr, false, 8,
+      double* part = ctx.tmp_c.as<double>((size_t)8 * ni * din);
+      translate_gemm(s, ni, din, 8 * din, ue + (size_t)T.level_off[d + 1] * din, 8 * din, nullptr,
+                     ctx.dops.u2u.get<double>(), din, ue, din, T.int_idx.get<int>() + T.int_off[d], nullptr, false, 8,
                      part);
     }
   }
@@ -1527,17 +1539,17 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   // FP32 cutoff (ue_c = ue P); the FP64 stages keep ue.  (2M-point m=10
   // Stokes error 3.3e-4 without, 2.8e-5 with; no change for Laplace.)
   const double* ue32 = ue;
-  if (sizeof(Real) == 4 && ke == 3 && T.src_counted && N > 0) {
-    double* uc_ = ctx.ue_c.as<double>((size_t)N * dim);
+  if (sizeof(Real) == 4 && kin == 3 && T.src_counted && N > 0) {
+    double* uc_ = ctx.ue_c.as<double>((size_t)N * din);
     ++ctx.n_launch;
-    translate_gemm(s, N, dim, dim, ue, dim, nullptr, ctx.dops.ue_proj.get<double>(), dim, uc_, dim, nullptr, nullptr,
+    translate_gemm(s, N, din, din, ue, din, nullptr, ctx.dops.ue_proj.get<double>(), din, uc_, din, nullptr, nullptr,
                    false);
     ue32 = uc_;
   }
   ev(3);
   // ---- V-list
   if (T.src_counted && T.n_vtrg > 0 && T.n_vsrc > 0) {
-    vlist<Real>(ctx, ue32, dc, ke, ev);
+    vlist<Real>(ctx, ue32, dc, kin, kout, ev);
   } else {
     ev(4);
     ev(5);
@@ -1552,7 +1564,7 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     ++ctx.n_launch;
     surface_check_kernel<KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
                                                            T.x_list.get<int>(), sx, sy, sz, den, usurf, ns, kRad0,
-                                                           kscale_exp, dc);
+                                                           kscale_exp, deg, dc);
   }
   ev(7);
   // ---- D2D, top-down
@@ -1560,21 +1572,21 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     const long ni = T.n_internal[d];
     if (ni == 0) continue;
     ++ctx.n_launch;
-    translate_gemm(s, ni, 8 * dim, dim, dc, dim, T.int_idx.get<int>() + T.int_off[d], ctx.dops.d2d.get<double>(),
-                   8 * dim, dc + (size_t)T.level_off[d + 1] * dim, 8 * dim, nullptr, nullptr, true);
+    translate_gemm(s, ni, 8 * dout, dout, dc, dout, T.int_idx.get<int>() + T.int_off[d], ctx.dops.d2d.get<double>(),
+                   8 * dout, dc + (size_t)T.level_off[d + 1] * dout, 8 * dout, nullptr, nullptr, true);
   }
   ev(8);
   // ---- D2T equivalent densities, then the fused near field
   double* pot = ctx.pot.as<double>(std::max(T.n_trg, 1L) * k1);
   if (T.n_tleaf > 0) {
-    double* de = ctx.de_c.as<double>((size_t)T.n_tleaf * dim);
-    double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * dim);
-    // (2^-depth DC[leaf] DC2DE0) DC2DE1, the check potentials gathered from
-    // the leaves' rows of DC
+    double* de = ctx.de_c.as<double>((size_t)T.n_tleaf * din);
+    double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * rk);
+    // (2^(-deg depth) DC[leaf] DC2DE0) DC2DE1, the check potentials gathered
+    // from the leaves' rows of DC
     ctx.n_launch += 2;
-    translate_gemm(s, T.n_tleaf, dim, dim, dc, dim, T.tleaf.get<int>(), ctx.dops.dc2de0.get<double>(), dim, t1, dim,
-                   nullptr, keys, false);
-    translate_gemm(s, T.n_tleaf, dim, dim, t1, dim, nullptr, ctx.dops.dc2de1.get<double>(), dim, de, dim, nullptr,
+    translate_gemm(s, T.n_tleaf, rk, dout, dc, dout, T.tleaf.get<int>(), ctx.dops.dc2de0.get<double>(), rk, t1, rk,
+                   nullptr, keys, false, 1, nullptr, deg);
+    translate_gemm(s, T.n_tleaf, din, rk, t1, rk, nullptr, ctx.dops.dc2de1.get<double>(), din, de, din, nullptr,
                    nullptr, false);
     ev(12);
     ++ctx.n_launch;
@@ -1589,11 +1601,11 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   // ---- output in input order, scaled by scale_x^trg_scal
   ++ctx.n_launch;
   if (out_float)
-    unsort_values<float><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts[0], ts[1],
-                                                                ts[2], ts[3], (float*)out);
+    unsort_values<float><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts,
+                                                                (float*)out);
   else
-    unsort_values<double><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts[0], ts[1],
-                                                                 ts[2], ts[3], (double*)out);
+    unsort_values<double><<<ceil_div(T.n_trg, 256), 256, 0, s>>>(pot, T.trg_perm.get<int>(), T.n_trg, k1, ts,
+                                                                 (double*)out);
   ev(10);
   PVFMM_CUDA_CHECK(cudaGetLastError());
 }
@@ -1670,7 +1682,7 @@ void upload_operators(Context& ctx) {
     if (!ctx.tc5_err_host) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.tc5_err_host, sizeof(int)));
     *ctx.tc5_err_host = 0;
   }
-  if (ctx.precision == 1 && ctx.ki.ke == 3) upload_vec<double>(ctx.dops.ue_proj, h.ue_proj, s);
+  if (ctx.precision == 1 && ctx.ki.ke == 3 && !h.ue_proj.empty()) upload_vec<double>(ctx.dops.ue_proj, h.ue_proj, s);
   int* fm = ctx.dops.fft_map.as<int>(h.fft_map.size());
   int* im = ctx.dops.ifft_map.as<int>(h.ifft_map.size());
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(fm, h.fft_map.data(), h.fft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -1696,6 +1708,19 @@ void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool 
     case kStokesVel:
       if (f32) evaluate_impl<float, kKerStokes, kKerStokes>(ctx, den_in, den_float, out, out_float);
       else evaluate_impl<double, kKerStokes, kKerStokes>(ctx, den_in, den_float, out, out_float);
+      break;
+    // the kernels that expand themselves (kernel.txx:894-901)
+    case kStokesPress:
+      if (f32) evaluate_impl<float, kKerStokesPress, kKerStokesPress>(ctx, den_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerStokesPress, kKerStokesPress>(ctx, den_in, den_float, out, out_float);
+      break;
+    case kStokesVelGrad:
+      if (f32) evaluate_impl<float, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, den_float, out, out_float);
+      break;
+    case kBiotSavart:
+      if (f32) evaluate_impl<float, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, den_float, out, out_float);
       break;
     default:
       throw std::runtime_error("unsupported kernel");

@@ -111,12 +111,12 @@ void upload_operators(Context& ctx);
 // on tcgen05 (rows of sout relative to p0), and its operator layout
 void launch_hadamard_tc5(Context& ctx, int n3h, const void* sin_, void* sout, long p0, long np);
 void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::vector<float>& out);
-// translate.cu: C[crow(i)] (+)= 2^-depth(key[arow(i)]) A[arow(i)] B on the FP64
+// translate.cu: C[crow(i)] (+)= 2^(-deg depth(key[arow(i)])) A[arow(i)] B on the FP64
 // tensor cores (rows gathered / scattered through the index lists when given);
 // with ksplit > 1 the K range is cut into ksplit equal pieces summed in
 // `partial` (ksplit * M * N doubles) and added in a fixed order
 void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long lda, const int* arows,
                     const double* B, long ldb, double* C, long ldc, const int* crows, const MKey* scale_keys,
-                    bool accumulate, int ksplit = 1, double* partial = nullptr);
+                    bool accumulate, int ksplit = 1, double* partial = nullptr, int deg = 1);
 
 }  // namespace pvfmm_b200

@@ -141,7 +141,15 @@ __device__ __forceinline__ double rsqrt_nr1(double r2) {
 // GenericKernel::Eval does after each source block (kernel.txx:1243-1246).
 // KS: number of source components, KT: number of target components.
 // ---------------------------------------------------------------------------
-enum KerType { kKerLaplace = 0, kKerLaplaceGrad = 1, kKerStokes = 2, kKerLaplacePG = 3 };
+enum KerType {
+  kKerLaplace = 0,
+  kKerLaplaceGrad = 1,
+  kKerStokes = 2,
+  kKerLaplacePG = 3,
+  kKerStokesPress = 4,  // stokes_press_, kernel.txx:1366-1378
+  kKerStokesGrad = 5,   // stokes_grad_, kernel.txx:1404-1432
+  kKerBiotSavart = 6    // biot_savart_, kernel.txx:1492-1506
+};
 
 template <int Ker>
 struct KerDims;
@@ -153,6 +161,12 @@ template <>
 struct KerDims<kKerStokes> { static constexpr int KS = 3, KT = 3; };
 template <>
 struct KerDims<kKerLaplacePG> { static constexpr int KS = 1, KT = 4; };
+template <>
+struct KerDims<kKerStokesPress> { static constexpr int KS = 3, KT = 1; };
+template <>
+struct KerDims<kKerStokesGrad> { static constexpr int KS = 3, KT = 9; };
+template <>
+struct KerDims<kKerBiotSavart> { static constexpr int KS = 3, KT = 3; };
 
 // Adds K(r) f to u (r = target - source).
 // Surface1 = true: the source is an equivalent-surface point at a distance
@@ -177,6 +191,28 @@ __device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* 
     u[1] += rx * fr3;
     u[2] += ry * fr3;
     u[3] += rz * fr3;
+  } else if constexpr (Ker == kKerStokesPress) {  // (r . f) / r^3
+    const Real rinv3 = rinv * rinv * rinv;
+    u[0] += (rx * f[0] + ry * f[1] + rz * f[2]) * rinv3;
+  } else if constexpr (Ker == kKerStokesGrad) {
+    // u[3i+j] += (delta_ij (r.f) + r_j f_i - f_j r_i - 3 (r.f) r_i r_j / r^2) / r^3
+    const Real rinv2 = rinv * rinv, rinv3 = rinv2 * rinv;
+    const Real ip = f[0] * rx + f[1] * ry + f[2] * rz;
+    const Real r[3] = {rx, ry, rz};
+    const Real c3 = (Real)3 * ip * rinv2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        Real v = r[j] * f[i] - f[j] * r[i] - c3 * r[i] * r[j];
+        if (i == j) v += ip;
+        u[3 * i + j] += v * rinv3;
+      }
+  } else if constexpr (Ker == kKerBiotSavart) {  // (f x r) / r^3
+    const Real rinv3 = rinv * rinv * rinv;
+    u[0] += rinv3 * (f[1] * rz - f[2] * ry);
+    u[1] += rinv3 * (f[2] * rx - f[0] * rz);
+    u[2] += rinv3 * (f[0] * ry - f[1] * rx);
   } else {  // Stokes velocity
     const Real rinv2 = rinv * rinv;
     const Real ip = (f[0] * rx + f[1] * ry + f[2] * rz) * rinv2;
@@ -186,8 +222,11 @@ __device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* 
   }
 }
 
+// 1/(8 pi) for Stokes velocity and velocity gradient, 1/(4 pi) otherwise
+// (the kernels' ScaleFactor, kernel.txx:1279, 1352, 1368, 1406, 1494).
 __host__ __device__ constexpr double ker_scale(int ker) {
-  return ker == kKerStokes ? 1.0 / (8 * 3.14159265358979323846) : 1.0 / (4 * 3.14159265358979323846);
+  return (ker == kKerStokes || ker == kKerStokesGrad) ? 1.0 / (8 * 3.14159265358979323846)
+                                                      : 1.0 / (4 * 3.14159265358979323846);
 }
 
 // ---------------------------------------------------------------------------

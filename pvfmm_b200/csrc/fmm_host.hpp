@@ -37,15 +37,16 @@ struct KernelInfo {
   int exp_kernel;          // ExpKernel of the expansions
   int ke;                  // dims of the expansion kernel (ke x ke)
   double src_scal[3];      // scale exponents of the s2t kernel (kernel.txx:64-196)
-  double trg_scal[4];
+  double trg_scal[9];
   int flops;               // per-pair flop count convention (kernel.txx:1277,1317,1352)
+  int deg;                 // degree of the expansion kernel, K(x/2) = 2^deg K(x): check -> equivalent
+                           // operators of level l are 2^(-deg l) times the level-0 ones
 };
 
-// Kernels the CUDA evaluation implements.
+// Kernels the CUDA evaluation implements (every PVFMMKernel value, plus the
+// Laplace potential+gradient).
 bool kernel_info(int id, KernelInfo* out);
-// kernel_info plus the kernels whose operators the host precompute builds
-// but whose evaluation the CUDA path does not implement yet (Stokes pressure,
-// Stokes velocity gradient, Biot-Savart; their scale exponents are not set).
+// Same as kernel_info (kept for the host precompute's callers).
 bool kernel_info_host(int id, KernelInfo* out);
 
 // Level-0 operators of one kernel and multipole order.  All FP64, row-major,

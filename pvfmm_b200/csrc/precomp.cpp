@@ -237,19 +237,34 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* get_last_error() { return g_last_error.c_str(); }
 
 bool kernel_info(int id, KernelInfo* out) {
+  // scale exponents of the C interface's rescale (src_scal / trg_scal, found by
+  // Kernel::Initialize, kernel.txx:64-196): a kernel of degree d, K(x/2) =
+  // 2^d K(x), has src_scal 0 and trg_scal d per component
   KernelInfo k{};
   switch (id) {
     case kLaplacePot:
-      k = {id, "laplace", 1, 1, kExpLaplace, 1, {0, 0, 0}, {1, 0, 0, 0}, 9};
+      k = {id, "laplace", 1, 1, kExpLaplace, 1, {0, 0, 0}, {1, 0, 0, 0}, 9, 1};
       break;
     case kLaplaceGrad:
-      k = {id, "laplace_grad", 1, 3, kExpLaplace, 1, {0, 0, 0}, {2, 2, 2, 0}, 16};
+      k = {id, "laplace_grad", 1, 3, kExpLaplace, 1, {0, 0, 0}, {2, 2, 2, 0}, 16, 1};
       break;
     case kStokesVel:
-      k = {id, "stokes_vel", 3, 3, kExpStokes, 3, {0, 0, 0}, {1, 1, 1, 0}, 29};
+      k = {id, "stokes_vel", 3, 3, kExpStokes, 3, {0, 0, 0}, {1, 1, 1, 0}, 29, 1};
       break;
     case kLaplacePotGrad:
-      k = {id, "laplace_potgrad", 1, 4, kExpLaplace, 1, {0, 0, 0}, {1, 2, 2, 2}, 18};
+      k = {id, "laplace_potgrad", 1, 4, kExpLaplace, 1, {0, 0, 0}, {1, 2, 2, 2}, 18, 1};
+      break;
+    // Stokes pressure, Stokes velocity gradient and Biot-Savart expand
+    // themselves (no separate expansion kernels, kernel.txx:894-901), with
+    // kin = 3 equivalent-density and kout = k1 check-potential components
+    case kStokesPress:  // StokesKernel<T>::pressure(), kernel.txx:1480-1483
+      k = {id, "stokes_press", 3, 1, kExpStokesPress, 3, {0, 0, 0}, {2, 0, 0, 0}, 16, 2};
+      break;
+    case kStokesVelGrad:  // StokesKernel<T>::vel_grad(), kernel.txx:1488-1491
+      k = {id, "stokes_grad", 3, 9, kExpStokesGrad, 3, {0, 0, 0}, {2, 2, 2, 2, 2, 2, 2, 2, 2}, 94, 2};
+      break;
+    case kBiotSavart:  // BiotSavartKernel<T>::potential(), kernel.txx:1508-1511
+      k = {id, "biot_savart", 3, 3, kExpBiotSavart, 3, {0, 0, 0}, {2, 2, 2, 0}, 24, 2};
       break;
     default:
       return false;
@@ -258,25 +273,7 @@ bool kernel_info(int id, KernelInfo* out) {
   return true;
 }
 
-bool kernel_info_host(int id, KernelInfo* out) {
-  if (kernel_info(id, out)) return true;
-  KernelInfo k{};
-  switch (id) {
-    case kStokesPress:  // StokesKernel<T>::pressure(), kernel.txx:1480-1483
-      k = {id, "stokes_press", 3, 1, kExpStokesPress, 3, {0, 0, 0}, {0, 0, 0, 0}, 16};
-      break;
-    case kStokesVelGrad:  // StokesKernel<T>::vel_grad(), kernel.txx:1488-1491
-      k = {id, "stokes_grad", 3, 9, kExpStokesGrad, 3, {0, 0, 0}, {0, 0, 0, 0}, 94};
-      break;
-    case kBiotSavart:  // BiotSavartKernel<T>::potential(), kernel.txx:1508-1511
-      k = {id, "biot_savart", 3, 3, kExpBiotSavart, 3, {0, 0, 0}, {0, 0, 0, 0}, 24};
-      break;
-    default:
-      return false;
-  }
-  *out = k;
-  return true;
-}
+bool kernel_info_host(int id, KernelInfo* out) { return kernel_info(id, out); }
 
 void exp_kernel_dims(int exp_kernel, int* kin, int* kout) {
   switch (exp_kernel) {

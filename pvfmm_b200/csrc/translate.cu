@@ -59,7 +59,7 @@ struct RowMap {
 __global__ void __launch_bounds__(kThreadsG, 2)
     translate_gemm_kernel(int M, int N, int K, const double* __restrict__ A, long lda, const int* __restrict__ arows,
                           const double* __restrict__ B, long ldb, double* __restrict__ C, long ldc,
-                          const int* __restrict__ crows, const MKey* __restrict__ keys, int accumulate,
+                          const int* __restrict__ crows, const MKey* __restrict__ keys, int deg, int accumulate,
                           long m_base, int kchunk, double* __restrict__ partial) {
   __shared__ __align__(16) double As[2][kBM * kAStride];
   __shared__ __align__(16) double Bs[2][kBK * kBStride];
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
       continue;
     }
     double s = 1.0;
-    if (keys) s = ldexp(1.0, -(int)(keys[arow_s[mi - m0]].lo & 31u));
+    if (keys) s = ldexp(1.0, -deg * (int)(keys[arow_s[mi - m0]].lo & 31u));
     const long cr = crows ? (long)crows[mi] : mi;
     double* crow = C + cr * ldc;
 #pragma unroll
@@ -165,14 +165,15 @@ __global__ void __launch_bounds__(kThreadsG, 2)
 // C[crow(i)][n] (+)= s(i) * sum_z partial[z][i][n], the K pieces added in order.
 __global__ void translate_reduce(long M, int N, int ksplit, const double* __restrict__ partial,
                                  const int* __restrict__ arows, const int* __restrict__ crows,
-                                 const MKey* __restrict__ keys, int accumulate, double* __restrict__ C, long ldc) {
+                                 const MKey* __restrict__ keys, int deg, int accumulate, double* __restrict__ C,
+                                 long ldc) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (e >= M * N) return;
   const long i = e / N;
   const int n = (int)(e % N);
   double v = 0;
   for (int z = 0; z < ksplit; ++z) v += partial[((long)z * M + i) * N + n];
-  if (keys) v *= ldexp(1.0, -(int)(keys[arows ? arows[i] : i].lo & 31u));
+  if (keys) v *= ldexp(1.0, -deg * (int)(keys[arows ? arows[i] : i].lo & 31u));
   double* c = C + (crows ? (long)crows[i] : i) * ldc + n;
   *c = accumulate ? *c + v : v;
 }
@@ -181,7 +182,7 @@ __global__ void translate_reduce(long M, int N, int ksplit, const double* __rest
 
 void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long lda, const int* arows,
                     const double* B, long ldb, double* C, long ldc, const int* crows, const MKey* scale_keys,
-                    bool accumulate, int ksplit, double* partial) {
+                    bool accumulate, int ksplit, double* partial, int deg) {
   if (M <= 0 || N <= 0) return;
   if (ksplit < 1 || (ksplit > 1 && (!partial || K % ksplit != 0 || (K / ksplit) % 2 != 0)))
     throw std::runtime_error("translate_gemm: bad K split");
@@ -194,13 +195,13 @@ void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long 
   for (long t0 = 0; t0 < tiles; t0 += 65535) {
     dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)std::min(65535L, tiles - t0), (unsigned)ksplit);
     translate_gemm_kernel<<<grid, kThreadsG, 0, s>>>((int)M, N, K, A, lda, arows, B, ldb, C, ldc, crows, scale_keys,
-                                                      accumulate ? 1 : 0, t0 * kBM, K / ksplit,
+                                                      deg, accumulate ? 1 : 0, t0 * kBM, K / ksplit,
                                                       ksplit > 1 ? partial : nullptr);
     PVFMM_CUDA_CHECK(cudaGetLastError());
   }
   if (ksplit > 1) {
     translate_reduce<<<(unsigned)((M * N + 255) / 256), 256, 0, s>>>(M, N, ksplit, partial, arows, crows, scale_keys,
-                                                                     accumulate ? 1 : 0, C, ldc);
+                                                                     deg, accumulate ? 1 : 0, C, ldc);
     PVFMM_CUDA_CHECK(cudaGetLastError());
   }
 }

@@ -62,8 +62,7 @@ def test_self_expanded_kernel_operators_reproduce_oracle_fmm(kid):
     """Stokes pressure (3->1), Stokes velocity gradient (3->9) and Biot-Savart
     (3->3) expand themselves, with rectangular check->equivalent factors: the
     library's host precompute drives the oracle FMM to the same result as the
-    oracle's own operators.  The CUDA evaluation does not take these kernels
-    yet: creating a context for one is an error."""
+    oracle's own operators."""
     K = O.KERNELS[kid]
     ops_lib = O.Operators.from_arrays(K, 4, P.precomp_operators(P.FMMKernel(kid), 4))
     rng = np.random.default_rng(50 + kid)
@@ -72,9 +71,6 @@ def test_self_expanded_kernel_operators_reproduce_oracle_fmm(kid):
     a = O.pvfmm_eval(kid, 4, 60, x, f, x, ops=ops_lib)
     b = O.pvfmm_eval(kid, 4, 60, x, f, x)
     assert O.rel_l2(a, b) < 1e-3 * O.rel_l2(b, O.direct_sum(kid, x, f, x))
-    lib = P.load_library()
-    assert not lib.PVFMMCreateContextExD(-1.0, 100, 4, kid, 0)
-    assert "unsupported" in P.last_error()
 
 
 def test_stokes_operators_reproduce_oracle_fmm():
@@ -119,14 +115,12 @@ def test_mixed_precompute_uses_fp32_cutoff():
 
 def test_invalid_arguments_fail_loudly():
     lib = P.load_library()
-    assert not lib.PVFMMCreateContextExD(-1.0, 100, 6, 5, 0)         # Biot-Savart: not implemented
+    assert not lib.PVFMMCreateContextExD(-1.0, 100, 6, 9, 0)         # not a PVFMMKernel value
     assert "unsupported" in P.last_error()
     assert not lib.PVFMMCreateContextExD(1.0, 100, 6, 0, 0)          # periodic box
     assert "periodic" in P.last_error()
     assert not lib.PVFMMCreateContextExD(-1.0, 100, 7, 0, 0)         # odd order
     assert P.last_error()
-    with pytest.raises(NotImplementedError):
-        P.FMMParticleContext(-1, 100, 6, P.FMMKernel.StokesPressure)
     assert P.precomp_operator.__doc__
 
 
