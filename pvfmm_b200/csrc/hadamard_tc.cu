@@ -217,25 +217,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int i = 0; i < 16; ++i) sum[i] = __fadd_rn(sum[i], d[i]);
     };
-    float4 xc[4], xn[4];
-    int oc = 0, on = 0;
-    if (nlive > 0) {
-      oc = __ffs(rem) - 1;
-      rem &= rem - 1;
-      gather(oc, xc);
-    }
-    for (int i = 0; i < nlive; ++i) {
+    // offset i of the tile's occupied list: TF32 split, A stage, MMAs,
+    // and the drain of offset i-1
+    auto step = [&](int i, int o, const float4 (&x)[4]) {
       const unsigned j = jglob + (unsigned)i;
-      if (i + 1 < nlive) {  // next offset's gathers in flight during this one
-        on = __ffs(rem) - 1;
-        rem &= rem - 1;
-        gather(on, xn);
-      }
       // TF32 hi / lo parts of the 16 values (K order = memory order)
       unsigned hi[16], lo[16];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        const float v[4] = {xc[c].x, xc[c].y, xc[c].z, xc[c].w};
+        const float v[4] = {x[c].x, x[c].y, x[c].z, x[c].w};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const unsigned h = tf32_rna(v[e]);
@@ -256,7 +246,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_after();
         const unsigned d_col = tmem + 64u + 16u * (j & 1u);
         const unsigned a_hi = tmem + a_col, a_lo = tmem + a_col + 16u;
-        const unsigned ob = b_base + (unsigned)oc * (4 * kOpBlockBytes);
+        const unsigned ob = b_base + (unsigned)o * (4 * kOpBlockBytes);
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           const unsigned long long bh = smem_desc(ob + (0 * 2 + ks) * kOpBlockBytes, 128, 256);
@@ -268,9 +258,41 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mma_commit(&bars[1 + (j & 1u)]);
       }
       if (i > 0) drain(j - 1);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) xc[c] = xn[c];
-      oc = on;
+    };
+    auto take = [&]() {
+      const int o = __ffs(rem) - 1;
+      rem &= rem - 1;
+      return o;
+    };
+    // three register sets in turn: the gathers of the next two offsets are
+    // in flight while one offset is processed
+    float4 xa[4], xb[4], xc[4];
+    int oa = 0, ob = 0, oc = 0;
+    if (nlive > 0) {
+      oa = take();
+      gather(oa, xa);
+    }
+    if (nlive > 1) {
+      ob = take();
+      gather(ob, xb);
+    }
+#pragma unroll 1
+    for (int i = 0; i < nlive; i += 3) {
+      if (i + 2 < nlive) {
+        oc = take();
+        gather(oc, xc);
+      }
+      step(i, oa, xa);
+      if (i + 3 < nlive) {
+        oa = take();
+        gather(oa, xa);
+      }
+      if (i + 1 < nlive) step(i + 1, ob, xb);
+      if (i + 4 < nlive) {
+        ob = take();
+        gather(ob, xb);
+      }
+      if (i + 2 < nlive) step(i + 2, oc, xc);
     }
     if (nlive > 0) drain(jglob + (unsigned)nlive - 1);
     jglob += (unsigned)nlive;
