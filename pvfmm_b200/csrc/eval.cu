@@ -345,6 +345,126 @@ __device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 pairs (add/sub/mul/fma .f32x2 of sm_100): the mixed form's near
+// field evaluates a source record against its thread's two targets in the two
+// halves of 64-bit registers, one instruction per operation for both targets
+// (the same round-to-nearest FP32 operations as two scalar evaluations).
+// ---------------------------------------------------------------------------
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+  f2_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
+  f2_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+  f2_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// Kernels with a packed form (the others evaluate the two targets in turn).
+template <int Ker>
+constexpr bool kHasPacked = Ker == kKerLaplace || Ker == kKerLaplaceGrad || Ker == kKerLaplacePG || Ker == kKerStokes;
+
+// ker_eval<Ker, float> for two targets at once: r = target - source per half,
+// f the source densities (the same in both halves).  1/r: one hardware
+// reciprocal square root per half (0 for r2 == 0) and one packed
+// Newton-Raphson step y <- y (3/2 - r2 y^2 / 2), as rsqrt_nr(float).
+template <int Ker>
+__device__ __forceinline__ void ker_eval_x2(f2_t rx, f2_t ry, f2_t rz, const f2_t* f, f2_t* u) {
+  const f2_t r2 = f2_fma(rz, rz, f2_fma(ry, ry, f2_mul(rx, rx)));
+  float a, b;
+  f2_unpack(r2, a, b);
+  float ya, yb;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ya) : "f"(a));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yb) : "f"(b));
+  ya = a > 0.f ? ya : 0.f;
+  yb = b > 0.f ? yb : 0.f;
+  f2_t y = f2_pack(ya, yb);
+  const f2_t half = f2_pack(0.5f, 0.5f), three_half = f2_pack(1.5f, 1.5f);
+  y = f2_mul(y, f2_sub(three_half, f2_mul(f2_mul(half, r2), f2_mul(y, y))));
+  if constexpr (Ker == kKerLaplace) {
+    u[0] = f2_fma(y, f[0], u[0]);
+  } else if constexpr (Ker == kKerLaplaceGrad) {
+    const f2_t fr3 = f2_mul(f2_mul(y, y), f2_mul(y, f[0]));
+    u[0] = f2_fma(rx, fr3, u[0]);
+    u[1] = f2_fma(ry, fr3, u[1]);
+    u[2] = f2_fma(rz, fr3, u[2]);
+  } else if constexpr (Ker == kKerLaplacePG) {
+    const f2_t fr = f2_mul(y, f[0]);
+    const f2_t fr3 = f2_mul(f2_mul(y, y), fr);
+    u[0] = f2_add(u[0], fr);
+    u[1] = f2_fma(rx, fr3, u[1]);
+    u[2] = f2_fma(ry, fr3, u[2]);
+    u[3] = f2_fma(rz, fr3, u[3]);
+  } else {  // Stokes velocity: u += (f + r (f.r) / r^2) / r
+    const f2_t ip = f2_mul(f2_fma(f[2], rz, f2_fma(f[1], ry, f2_mul(f[0], rx))), f2_mul(y, y));
+    u[0] = f2_fma(y, f2_fma(rx, ip, f[0]), u[0]);
+    u[1] = f2_fma(y, f2_fma(ry, ip, f[1]), u[1]);
+    u[2] = f2_fma(y, f2_fma(rz, ip, f[2]), u[2]);
+  }
+}
+
+// rec_sum2 for FP32 records with the packed pair evaluation.
+template <int Ker>
+__device__ __forceinline__ void rec_sum2_x2(const float4* tile, int n, int j0, int js, const Pt<float>& pa,
+                                            const Pt<float>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
+  constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
+  using R = Rec<float, KS>;
+  const f2_t px = f2_pack(pa.x, pb.x), py = f2_pack(pa.y, pb.y), pz = f2_pack(pa.z, pb.z);
+  const f2_t pxl = f2_pack(pa.xl, pb.xl), pyl = f2_pack(pa.yl, pb.yl), pzl = f2_pack(pa.zl, pb.zl);
+  // FP32 partial sums run over 16 records at most before going to FP64
+  const int step = 16 * js;
+  for (int jb = j0; jb < n; jb += step) {
+    const int jend = min(n, jb + step);
+    f2_t u[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) u[k] = 0ull;  // (0.f, 0.f)
+#pragma unroll kNearUnroll
+    for (int j = jb; j < jend; j += js) {
+      float v[R::NVP];
+#pragma unroll
+      for (int c = 0; c < R::NC; ++c) {
+        const float4 w = tile[c * kTile + j];
+        memcpy(&v[c * R::PER], &w, 16);
+      }
+      f2_t f[KS];
+#pragma unroll
+      for (int i = 0; i < KS; ++i) f[i] = f2_pack(v[R::F(i)], v[R::F(i)]);
+      const f2_t rx = f2_add(f2_sub(px, f2_pack(v[0], v[0])), f2_sub(pxl, f2_pack(v[4], v[4])));
+      const f2_t ry = f2_add(f2_sub(py, f2_pack(v[1], v[1])), f2_sub(pyl, f2_pack(v[5], v[5])));
+      const f2_t rz = f2_add(f2_sub(pz, f2_pack(v[2], v[2])), f2_sub(pzl, f2_pack(v[6], v[6])));
+      ker_eval_x2<Ker>(rx, ry, rz, f, u);
+    }
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+      float a, b;
+      f2_unpack(u[k], a, b);
+      acc[0][k] += (double)a;
+      acc[1][k] += (double)b;
+    }
+  }
+}
+
 // One list entry of a target leaf as a segment of the packed source stream:
 // the points of a leaf (kind 0, `node` = first point), the upward equivalent
 // surface of a node (kind 1, `node` = node index) or the leaf's own downward
@@ -535,7 +655,10 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
         }
         if (t + 1 < ntile) fetch(t + 1);
         __syncthreads();  // tiles[buf] complete; tiles[buf^1] no longer read (its readers passed this barrier)
-        if (active) rec_sum2<Real, Ker>(tiles[buf], n, g, G, pa, pb, acc);
+        if (active) {
+          if constexpr (kF32 && kHasPacked<Ker>) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pa, pb, acc);
+          else rec_sum2<Real, Ker>(tiles[buf], n, g, G, pa, pb, acc);
+        }
         buf ^= 1;
       }
     }

@@ -136,8 +136,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         const unsigned char* __restrict__ ops, float4* __restrict__ spec_out, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* Bs = smem;                                              // kOpBytes
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kOpBytes);  // [0] operators, [1..2] MMA done
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 4);
+  // mbarriers: [0] operators arrived, [1..2] MMAs of A stage 0/1 done,
+  // [3..4] A stage 0/1 written by all four warps
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kOpBytes);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 6);
   unsigned* live_s = tmem_slot + 1;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int f = blockIdx.y;
@@ -146,6 +148,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     mbar_init(&bars[2], 1);
+    mbar_init(&bars[3], kTcThreads / 32);
+    mbar_init(&bars[4], kTcThreads / 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -194,9 +198,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float sum[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) sum[i] = 0.f;
-    // neighbour row of offset o for this thread's parent (zeros when none)
-    auto gather = [&](int o, float4 (&x)[4]) {
-      const int q = in ? __ldg(vtab + (long)o * vt_stride + p) : -1;
+    // neighbour row q of this thread's parent for an offset (zeros when none);
+    // the index q is loaded one step before the row, so that the row loads
+    // never wait for it
+    auto qload = [&](int o) { return in ? __ldg(vtab + (long)o * vt_stride + p) : -1; };
+    auto gather = [&](int q, float4 (&x)[4]) {
       if (q >= 0) {
         const float4* r = spec_in + ((long)q * n3h + f) * 4;
 #pragma unroll
@@ -241,8 +247,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tmem_st16(tmem + lane_base + a_col + 16u, lo);
       tmem_wait_st();
       tc_fence_before();
-      __syncthreads();
+      __syncwarp();
+      // this warp's rows of A stage j&1 are written: one arrival per warp; the
+      // warps do not wait for each other, only the MMA-issuing thread waits
+      // for all four
+      if ((tid & 31) == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&bars[3 + (j & 1u)])) : "memory");
       if (tid == 0) {
+        mbar_wait(&bars[3 + (j & 1u)], (j >> 1) & 1u, err, kErrMma);
         tc_fence_after();
         const unsigned d_col = tmem + 64u + 16u * (j & 1u);
         const unsigned a_hi = tmem + a_col, a_lo = tmem + a_col + 16u;
@@ -264,35 +275,56 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       rem &= rem - 1;
       return o;
     };
-    // three register sets in turn: the gathers of the next two offsets are
-    // in flight while one offset is processed
+    // three register sets in turn: the rows of the next two offsets are in
+    // flight while one offset is processed, and the index of the one after
     float4 xa[4], xb[4], xc[4];
-    int oa = 0, ob = 0, oc = 0;
+    int oa = 0, ob = 0, oc = 0, qa = -1, qb = -1, qc = -1;
     if (nlive > 0) {
       oa = take();
-      gather(oa, xa);
+      qa = qload(oa);
     }
     if (nlive > 1) {
       ob = take();
-      gather(ob, xb);
+      qb = qload(ob);
     }
+    if (nlive > 2) {
+      oc = take();
+      qc = qload(oc);
+    }
+    if (nlive > 0) gather(qa, xa);
+    if (nlive > 1) gather(qb, xb);
 #pragma unroll 1
     for (int i = 0; i < nlive; i += 3) {
-      if (i + 2 < nlive) {
-        oc = take();
-        gather(oc, xc);
+      // invariant: rows of i (xa) and i+1 (xb) requested, index of i+2 (qc) loaded
+      int oa2 = 0, qa2 = -1;
+      if (i + 2 < nlive) gather(qc, xc);
+      if (i + 3 < nlive) {
+        oa2 = take();
+        qa2 = qload(oa2);
       }
       step(i, oa, xa);
       if (i + 3 < nlive) {
-        oa = take();
-        gather(oa, xa);
+        oa = oa2;
+        gather(qa2, xa);
+      }
+      int ob2 = 0, qb2 = -1;
+      if (i + 4 < nlive) {
+        ob2 = take();
+        qb2 = qload(ob2);
       }
       if (i + 1 < nlive) step(i + 1, ob, xb);
       if (i + 4 < nlive) {
-        ob = take();
-        gather(ob, xb);
+        ob = ob2;
+        gather(qb2, xb);
+      }
+      int oc2 = 0, qc2 = -1;
+      if (i + 5 < nlive) {
+        oc2 = take();
+        qc2 = qload(oc2);
       }
       if (i + 2 < nlive) step(i + 2, oc, xc);
+      oc = oc2;
+      qc = qc2;
     }
     if (nlive > 0) drain(jglob + (unsigned)nlive - 1);
     jglob += (unsigned)nlive;
@@ -352,7 +384,7 @@ void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::
 
 void launch_hadamard_tc5(Context& ctx, int n3h, const void* sin_, void* sout, long p0, long np) {
   DevTree& T = ctx.tree;
-  const size_t sm = (size_t)kOpBytes + 64;
+  const size_t sm = (size_t)kOpBytes + 64;  // operators, 5 mbarriers, TMEM address, live-offset word
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc5_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int tiles = 8;  // tiles of 128 target parents per CTA (operators staged once)
   dim3 grid((unsigned)((np + (long)kTcTile * tiles - 1) / ((long)kTcTile * tiles)), (unsigned)n3h);
