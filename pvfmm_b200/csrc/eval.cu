@@ -781,8 +781,8 @@ struct FftSizes {
 template <class Real, int M>
 __global__ void __launch_bounds__(288) fft_up_kernel(int ke, int G, int ngroups, const int* __restrict__ vsrc,
                                                       const int* __restrict__ child0, const double* __restrict__ ue,
-                                                      const int* __restrict__ fft_map, int ns, long n_q,
-                                                      Cplx<Real>* __restrict__ spec) {
+                                                      const int* __restrict__ fft_map, int ns, long n_q, int kz0,
+                                                      int nkz, Cplx<Real>* __restrict__ spec) {
   using F = FftSizes<Real, M>;
   constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H, A2S = F::A2S;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -855,8 +855,9 @@ __global__ void __launch_bounds__(288) fft_up_kernel(int ke, int G, int ngroups,
     }
   }
   __syncthreads();
-  // z -> kz: line = (gi, ky, kx), gi fastest; spectrum index f = kx + NH*(ky + N1*kz)
-  Cplx<Real>* out = spec + (long)q * N3H * ngrid;
+  // z -> kz: line = (gi, ky, kx), gi fastest; spectrum index f = kx + NH*(ky + N1*kz);
+  // only the slab kz in [kz0, kz0+nkz) is written, at f - N1*NH*kz0
+  Cplx<Real>* out = spec + (long)q * (N1 * NH * nkz) * ngrid;
   for (int i = threadIdx.x; i < gn * N1 * NH; i += blockDim.x) {
     const int gi = i % gn, l = i / gn;  // l = ky*NH + kx
     const Cplx<Real>* col = a2 + gi * A2S + l;
@@ -865,6 +866,7 @@ __global__ void __launch_bounds__(288) fft_up_kernel(int ke, int G, int ngroups,
     for (int z = 0; z < M; ++z) v[z] = col[z * N1 * NH];
 #pragma unroll
     for (int kz = 0; kz < N1; ++kz) {
+      if (kz < kz0 || kz >= kz0 + nkz) continue;
       Real re = 0, im = 0;
 #pragma unroll
       for (int z = 0; z < M; ++z) {
@@ -872,7 +874,7 @@ __global__ void __launch_bounds__(288) fft_up_kernel(int ke, int G, int ngroups,
         re += v[z].re * twr[w] - v[z].im * twi[w];
         im += v[z].re * twi[w] + v[z].im * twr[w];
       }
-      const int f = l + N1 * NH * kz;
+      const int f = l + N1 * NH * (kz - kz0);
       if (sizeof(Real) == 8 && ke == 1) spec[((long)f * 8 + gb + gi) * n_q + q] = {re, im};
       else out[(long)f * ngrid + gb + gi] = {re, im};
     }
@@ -883,8 +885,8 @@ template <class Real, int M>
 __global__ void __launch_bounds__(288) ifft_dn_kernel(int ke, int G, int ngroups, const int* __restrict__ vtrg,
                                                        const int* __restrict__ child0, const MKey* __restrict__ keys,
                                                        const Cplx<Real>* __restrict__ spec,
-                                                       const int* __restrict__ ifft_map, int ns, int deg,
-                                                       double* __restrict__ dc) {
+                                                       const int* __restrict__ ifft_map, int ns, int deg, int kz0,
+                                                       int nkz, double* __restrict__ dc) {
   using F = FftSizes<Real, M>;
   constexpr int N1 = F::N1, NH = F::NH, M3 = F::M3, N3H = F::N3H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -911,15 +913,17 @@ __global__ void __launch_bounds__(288) ifft_dn_kernel(int ke, int G, int ngroups
     twi[j] = (Real)sn;
   }
   __syncthreads();
-  const Cplx<Real>* in = spec + (long)vt * N3H * ngrid + gb;
+  const Cplx<Real>* in = spec + (long)vt * (N1 * NH * nkz) * ngrid + gb;
   // kz -> z in [M, 2M): line = (gi, ky, kx) read straight from the spectrum
   // row of the parent (gi fastest: neighbouring threads read neighbouring
-  // children of one frequency)
+  // children of one frequency).  With a slab of kz the transform of the
+  // slab's frequencies alone is added into dc (the transform is linear).
   for (int i = threadIdx.x; i < gn * N1 * NH; i += blockDim.x) {
     const int gi = i % gn, l = i / gn;  // l = ky*NH + kx
     Cplx<Real> v[N1];
 #pragma unroll
-    for (int kz = 0; kz < N1; ++kz) v[kz] = in[(long)(l + N1 * NH * kz) * ngrid + gi];
+    for (int kz = 0; kz < N1; ++kz)
+      v[kz] = (kz >= kz0 && kz < kz0 + nkz) ? in[(long)(l + N1 * NH * (kz - kz0)) * ngrid + gi] : Cplx<Real>{0, 0};
 #pragma unroll
     for (int zp = 0; zp < M; ++zp) {
       Real re = 0, im = 0;
@@ -1395,7 +1399,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 }
 
 // Target parents [p0, p0 + np) of the V-list; sout holds their rows.
-void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<float>* sout, long p0, long np) {
+void launch_hadamard_tc(Context& ctx, int n3h, long f_base, const Cplx<float>* sin_, Cplx<float>* sout, long p0,
+                        long np) {
   DevTree& T = ctx.tree;
   constexpr int MT = 2;
   const size_t sm = (size_t)26 * 4 * 32 * sizeof(float4) + (size_t)27 * kTcWarps * 16 * MT * sizeof(int);
@@ -1406,16 +1411,17 @@ void launch_hadamard_tc(Context& ctx, int n3h, const Cplx<float>* sin_, Cplx<flo
   hadamard_tc_kernel<MT><<<grid, 32 * kTcWarps, sm, ctx.stream>>>(
       n3h, np, T.n_vtrg, T.n_vsrc, chunks, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
       reinterpret_cast<const float4*>(sin_),
-      ctx.dops.vop_frag.get<float4>(), reinterpret_cast<float2*>(sout));
+      ctx.dops.vop_frag.get<float4>() + f_base * 26 * 4 * 32, reinterpret_cast<float2*>(sout));
 }
 
 template <class Real, int PB>
-void launch_hadamard_rd(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0, long np) {
+void launch_hadamard_rd(Context& ctx, int n3h, long f_base, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0,
+                        long np) {
   DevTree& T = ctx.tree;
   dim3 grid(ceil_div(np, 128 * PB), n3h);
   ++ctx.n_launch;
   hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0, sin_,
-                                                             ctx.dops.vop.get<Cplx<Real>>(), sout);
+                                                             ctx.dops.vop.get<Cplx<Real>>() + f_base * 26 * 64, sout);
 }
 
 // Target parents per thread (register tile) of the FP64 scalar Hadamard.
@@ -1430,7 +1436,8 @@ size_t hadamard_smem() {
 }
 
 template <class Real, int KI, int KO, int KOC, int OC>
-void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0, long np) {
+void launch_hadamard(Context& ctx, int n3h, long f_base, const Cplx<Real>* sin_, Cplx<Real>* sout, long p0,
+                     long np) {
   static_assert(KO % KOC == 0, "output components in whole groups");
   DevTree& T = ctx.tree;
   const size_t sm = hadamard_smem<Real, KI, KO, OC>();
@@ -1438,8 +1445,9 @@ void launch_hadamard(Context& ctx, int n3h, const Cplx<Real>* sin_, Cplx<Real>* 
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(ceil_div(np, 128), n3h, KO / KOC);
   ++ctx.n_launch;
-  hadamard_kernel<Real, KI, KO, KOC, OC><<<grid, 128, sm, ctx.stream>>>(n3h, np, T.n_vtrg, T.vtab.get<int>() + p0,
-                                                                         sin_, ctx.dops.vop.get<Cplx<Real>>(), sout);
+  hadamard_kernel<Real, KI, KO, KOC, OC><<<grid, 128, sm, ctx.stream>>>(
+      n3h, np, T.n_vtrg, T.vtab.get<int>() + p0, sin_, ctx.dops.vop.get<Cplx<Real>>() + f_base * 26 * 64 * KI * KO,
+      sout);
 }
 
 // ---------------------------------------------------------------------------
@@ -1495,7 +1503,7 @@ int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
 // products and stage 5 covers the rest.
 template <class Real, int M>
 void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
-                 long chunk, const std::function<void(int)>& ev) {
+                 long chunk, int nslab, const std::function<void(int)>& ev) {
   DevTree& T = ctx.tree;
   auto s = ctx.stream;
   using F = FftSizes<Real, M>;
@@ -1503,34 +1511,40 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
   const int Gu = grids_per_block<F>(F::up_grid_bytes, F::tw_bytes, ngrid_up, 64 * 1024);
   const size_t sm_up = F::tw_bytes + Gu * F::up_grid_bytes;
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(fft_up_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_up));
-  ++ctx.n_launch;
-  fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid_up / Gu), F::threads(Gu), sm_up, s>>>(
-      kin, Gu, ngrid_up / Gu, T.vsrc.get<int>(), T.child0.get<int>(), ue, ctx.dops.fft_map.get<int>(), ctx.ns,
-      T.n_vsrc, sin_);
-  ev(4);
-  const int n3h = F::N3H;
   const int Gd = grids_per_block<F>(F::dn_grid_bytes, F::tw_bytes, ngrid_dn, 80 * 1024);
   const size_t sm_dn = F::tw_bytes + Gd * F::dn_grid_bytes;
   PVFMM_CUDA_CHECK(
       cudaFuncSetAttribute(ifft_dn_kernel<Real, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dn));
-  for (long p0 = 0; p0 < T.n_vtrg; p0 += chunk) {
-    const long np = std::min(chunk, T.n_vtrg - p0);
-    if (kin == 1 && kout == 1) {
-      if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, sin_, sout, p0, np);
-      else if (std::getenv("PVFMM_B200_HADAMARD_MMA_SYNC")) launch_hadamard_tc(ctx, n3h, sin_, sout, p0, np);
-      else launch_hadamard_tc5(ctx, n3h, sin_, sout, p0, np);
-    } else if (kout == 3) {  // Stokes velocity, Biot-Savart
-      launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, sin_, sout, p0, np);
-    } else if (kout == 1) {  // Stokes pressure
-      launch_hadamard<Real, 3, 1, 1, 4>(ctx, n3h, sin_, sout, p0, np);
-    } else {  // Stokes velocity gradient: 9 outputs in 3 groups of 3
-      launch_hadamard<Real, 3, 9, 3, 2>(ctx, n3h, sin_, sout, p0, np);
-    }
-    if (p0 == 0) ev(5);
+  // slabs of kz (the slowest frequency index): each slab's forward DFT rows,
+  // products and inverse DFT contribution in turn (nslab = 1: all at once)
+  for (int sl = 0; sl < nslab; ++sl) {
+    const int kz0 = F::N1 * sl / nslab, nkz = F::N1 * (sl + 1) / nslab - kz0;
+    const int n3h = F::N1 * F::NH * nkz;           // the slab's frequencies
+    const long f_base = (long)F::N1 * F::NH * kz0;  // its first frequency
     ++ctx.n_launch;
-    ifft_dn_kernel<Real, M><<<np * (ngrid_dn / Gd), F::threads(Gd), sm_dn, s>>>(
-        kout, Gd, ngrid_dn / Gd, T.vtrg.get<int>() + p0, T.child0.get<int>(), T.key.get<MKey>(), sout,
-        ctx.dops.ifft_map.get<int>(), ctx.ns, ctx.ki.deg, dc);
+    fft_up_kernel<Real, M><<<T.n_vsrc * (ngrid_up / Gu), F::threads(Gu), sm_up, s>>>(
+        kin, Gu, ngrid_up / Gu, T.vsrc.get<int>(), T.child0.get<int>(), ue, ctx.dops.fft_map.get<int>(), ctx.ns,
+        T.n_vsrc, kz0, nkz, sin_);
+    if (sl == 0) ev(4);
+    for (long p0 = 0; p0 < T.n_vtrg; p0 += chunk) {
+      const long np = std::min(chunk, T.n_vtrg - p0);
+      if (kin == 1 && kout == 1) {
+        if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
+        else if (std::getenv("PVFMM_B200_HADAMARD_MMA_SYNC")) launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
+        else launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
+      } else if (kout == 3) {  // Stokes velocity, Biot-Savart
+        launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
+      } else if (kout == 1) {  // Stokes pressure
+        launch_hadamard<Real, 3, 1, 1, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
+      } else {  // Stokes velocity gradient: 9 outputs in 3 groups of 3
+        launch_hadamard<Real, 3, 9, 3, 2>(ctx, n3h, f_base, sin_, sout, p0, np);
+      }
+      if (p0 == 0 && sl == 0) ev(5);
+      ++ctx.n_launch;
+      ifft_dn_kernel<Real, M><<<np * (ngrid_dn / Gd), F::threads(Gd), sm_dn, s>>>(
+          kout, Gd, ngrid_dn / Gd, T.vtrg.get<int>() + p0, T.child0.get<int>(), T.key.get<MKey>(), sout,
+          ctx.dops.ifft_map.get<int>(), ctx.ns, ctx.ki.deg, kz0, nkz, dc);
+    }
   }
 }
 
@@ -1539,7 +1553,24 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
 template <class Real>
 void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const std::function<void(int)>& ev) {
   DevTree& T = ctx.tree;
-  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  const int m = ctx.m, n1 = 2 * m, n3h_all = 4 * m * m * (m + 1);
+  // input spectra of all source parents for a slab of kz: the whole spectrum
+  // (one slab) when it takes at most 45% of the free device memory (counting
+  // this buffer's current allocation), else the fewest slabs that do
+  const size_t in_all = (size_t)T.n_vsrc * n3h_all * 8 * kin * sizeof(Cplx<Real>);
+  int nslab = 1;
+  if (in_all > ctx.spec_in.cap) {
+    size_t free_b = 0, total_b = 0;
+    PVFMM_CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    const double avail = 0.45 * (double)(free_b + ctx.spec_in.cap + ctx.spec_out.cap);
+    while (nslab < n1 && (double)in_all / nslab > avail) ++nslab;
+  }
+  // PVFMM_B200_VLIST_SLABS sets the slab count (to exercise the slab path)
+  if (const char* e = std::getenv("PVFMM_B200_VLIST_SLABS")) {
+    const int v = std::atoi(e);
+    if (v > 0) nslab = std::min(v, n1);
+  }
+  const int n3h = n1 * (m + 1) * ((n1 + nslab - 1) / nslab);  // frequencies of the largest slab
   Cplx<Real>* sin_ = ctx.spec_in.as<Cplx<Real>>((size_t)T.n_vsrc * n3h * 8 * kin);
   // output spectra: all target parents at once when they fit in 90% of the
   // free device memory (counting this buffer's current allocation), else
@@ -1559,14 +1590,14 @@ void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const 
   }
   Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * kout);
   switch (m) {
-    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
-    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, kin, kout, chunk, ev); break;
+    case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 4: vlist_fft_t<Real, 4>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 6: vlist_fft_t<Real, 6>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 8: vlist_fft_t<Real, 8>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 10: vlist_fft_t<Real, 10>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 12: vlist_fft_t<Real, 12>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 14: vlist_fft_t<Real, 14>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
+    case 16: vlist_fft_t<Real, 16>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;
     default: throw std::runtime_error("unsupported multipole order");
   }
 }

@@ -108,8 +108,9 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
 void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
 void upload_operators(Context& ctx);
 // hadamard_tc.cu: mixed-form V-list Hadamard of target parents [p0, p0+np)
-// on tcgen05 (rows of sout relative to p0), and its operator layout
-void launch_hadamard_tc5(Context& ctx, int n3h, const void* sin_, void* sout, long p0, long np);
+// on tcgen05 (rows of sout relative to p0) over n3h frequencies starting at
+// frequency f_base of the operators, and its operator layout
+void launch_hadamard_tc5(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np);
 void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::vector<float>& out);
 // translate.cu: C[crow(i)] (+)= 2^(-deg depth(key[arow(i)])) A[arow(i)] B on the FP64
 // tensor cores (rows gathered / scattered through the index lists when given);

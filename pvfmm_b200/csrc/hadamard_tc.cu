@@ -6,24 +6,26 @@
 //   OUT[P][f] = sum over occupied offsets o of  IN[Q_o(P)][f] * B_o(f),
 // a 16-float spectrum row (8 children, re/im interleaved) times the 16 x 16
 // real form of the 8 x 8 complex operator block of offset o.  A CTA owns one
-// frequency and walks tiles of 128 target parents (M = 128 rows, one TMEM
-// lane per parent):
-//   - the 26 operator blocks of its frequency, each as TF32 hi and lo parts
+// frequency and runs four independent pipelines (warpgroups), each walking
+// tiles of 128 target parents (M = 128 rows, one TMEM lane per parent):
+//   - the 26 operator blocks of the frequency, each as TF32 hi and lo parts
 //     in the canonical K-major no-swizzle layout, arrive once by a bulk
-//     asynchronous copy (cp.async.bulk, 53 KB) and stay in shared memory;
+//     asynchronous copy (cp.async.bulk, 53 KB) and stay in shared memory for
+//     all four pipelines;
 //   - for each offset occupied by some parent of the tile, every thread
-//     gathers its parent's neighbour row (64 B, from L2), splits each value
-//     into TF32 hi + lo (both rounded to nearest) and stores them into an A
-//     stage in TMEM (tcgen05.st); one thread then issues 6 MMAs
-//     (2 K-steps x {lo*hi, hi*lo, hi*hi}) into a fresh 16-column TMEM
-//     accumulator and commits them to an mbarrier;
+//     stages its parent's neighbour row (64 B, from L2) with cp.async four
+//     offsets ahead, then splits each value into TF32 hi + lo (both rounded
+//     to nearest) and stores them into an A stage in TMEM (tcgen05.st); once
+//     the four warps of the pipeline have arrived on an mbarrier, one thread
+//     issues 6 MMAs (2 K-steps x {lo*hi, hi*lo, hi*hi}) into a fresh
+//     16-column TMEM accumulator and commits them to another mbarrier;
 //   - while the tensor cores work on offset j, the threads drain offset j-1's
 //     accumulator (tcgen05.ld) into their running FP32 sums with rounded FP32
 //     adds.  A fresh accumulator per offset keeps the tensor cores' own
 //     accumulation to 6 products (carried over all offsets, its rounding
 //     biased the far-field potential by ~2e-6).
-// TMEM: 2 A stages (hi 16 + lo 16 columns each) + 2 accumulators of 16
-// columns = 96 of 128 allocated columns per CTA.  Every wait is bounded: a
+// TMEM per pipeline: 2 A stages (hi 16 + lo 16 columns each) + 2 accumulators
+// of 16 columns (96 of 128 columns; 512 per CTA).  Every wait is bounded: a
 // wait that runs out sets the error word, and the host reports it.
 #include <cstring>
 
@@ -130,40 +132,66 @@ __device__ __forceinline__ unsigned tf32_rna(float x) {
 // Error word codes (bit set per failing wait kind).
 constexpr int kErrOperators = 1, kErrMma = 2;
 
-__global__ void __launch_bounds__(kTcThreads, 1)
+constexpr int kGroups = 4;                      // tile pipelines (warpgroups) per CTA
+constexpr int kStages = 5;                      // neighbour-row stages per pipeline
+constexpr int kAhead = kStages - 1;             // offsets whose rows are in flight
+constexpr int kRowBytes = 64;                   // one spectrum row: 8 children x complex FP32
+constexpr int kStageBytes = kTcTile * kRowBytes;
+constexpr size_t kSmemBytes = (size_t)kOpBytes + (size_t)kGroups * kStages * kStageBytes + 256;
+
+__device__ __forceinline__ void cp16(unsigned smem, const void* gmem, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem), "l"(gmem), "r"(valid ? 16 : 0)
+               : "memory");
+}
+
+// One CTA per SM: four independent tile pipelines (warpgroups of 128 threads,
+// one TMEM lane per parent) share the frequency's operator blocks.  In each
+// pipeline a thread stages its parent's neighbour rows with cp.async
+// kAhead offsets ahead of the one it multiplies (a thread only reads the rows
+// it copied itself, so its own copy groups order the stages); the 16-byte
+// chunks of row r sit at chunk slot c ^ ((r >> 1) & 3), so that the row reads
+// of a warp do not conflict on shared-memory banks.
+__global__ void __launch_bounds__(kGroups * kTcThreads, 1)
     hadamard_tc5_kernel(int n3h, long n_vtrg, long vt_stride, int tiles_per_cta, const int* __restrict__ vtab,
                         const unsigned* __restrict__ vmask, const float4* __restrict__ spec_in,
                         const unsigned char* __restrict__ ops, float4* __restrict__ spec_out, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* Bs = smem;                                              // kOpBytes
-  // mbarriers: [0] operators arrived, [1..2] MMAs of A stage 0/1 done,
-  // [3..4] A stage 0/1 written by all four warps
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kOpBytes);
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 6);
-  unsigned* live_s = tmem_slot + 1;
+  unsigned char* Bs = smem;                                          // kOpBytes
+  unsigned char* rows = smem + kOpBytes;                             // [group][stage][128 rows][64 B]
+  // mbarriers: [0] operators arrived; per group g at 1 + 4g: [+0, +1] MMAs of
+  // A stage 0/1 done, [+2, +3] A stage 0/1 written by the group's four warps
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(smem + kOpBytes + (size_t)kGroups * kStages * kStageBytes);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 1 + 4 * kGroups);
+  unsigned* live_s = tmem_slot + 1;                                  // [kGroups]
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int grp = tid / kTcThreads, gt = tid % kTcThreads, gwarp = gt >> 5;
   const int f = blockIdx.y;
+  unsigned long long* gbar = bars + 1 + 4 * grp;
 
   if (tid == 0) {
     mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_init(&bars[2], 1);
-    mbar_init(&bars[3], kTcThreads / 32);
-    mbar_init(&bars[4], kTcThreads / 32);
+    for (int g = 0; g < kGroups; ++g) {
+      mbar_init(&bars[1 + 4 * g + 0], 1);
+      mbar_init(&bars[1 + 4 * g + 1], 1);
+      mbar_init(&bars[1 + 4 * g + 2], kTcThreads / 32);
+      mbar_init(&bars[1 + 4 * g + 3], kTcThreads / 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kTmemCols)
+                 "r"(kTmemCols * kGroups)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   __syncthreads();
   tc_fence_after();
-  const unsigned tmem = *tmem_slot;
-  // TMEM map: columns [0,32) A stage 0 (hi 0-15, lo 16-31), [32,64) A stage 1,
-  // [64,80) accumulator 0, [80,96) accumulator 1; this warp's 32 lanes.
-  const unsigned lane_base = (unsigned)(warp * 32) << 16;
+  // this group's TMEM: columns [0,32) A stage 0 (hi 0-15, lo 16-31), [32,64)
+  // A stage 1, [64,80) accumulator 0, [80,96) accumulator 1; the group's four
+  // warps cover lanes 0-127
+  const unsigned tmem = *tmem_slot + kTmemCols * grp;
+  const unsigned lane_base = (unsigned)(gwarp * 32) << 16;
 
   // the frequency's operator blocks: one bulk copy, completion on bars[0]
   if (tid == 0) {
@@ -177,67 +205,98 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   mbar_wait(&bars[0], 0, err, kErrOperators);
   const unsigned b_base = smem_u32(Bs);
+  // this thread's row slot in each stage of its group
+  const unsigned row_base = smem_u32(rows) + (unsigned)(grp * kStages * kStageBytes + gt * kRowBytes);
+  const int swz = (gt >> 1) & 3;
 
-  unsigned jglob = 0;  // offsets processed by this CTA (mbarrier phase bookkeeping)
-  for (int tl = 0; tl < tiles_per_cta; ++tl) {
+  unsigned jglob = 0;  // offsets processed by this group (mbarrier phase bookkeeping)
+  for (int tl = grp; tl < tiles_per_cta; tl += kGroups) {
     const long p0 = ((long)blockIdx.x * tiles_per_cta + tl) * kTcTile;
-    if (p0 >= n_vtrg) break;
-    const long p = p0 + tid;
+    if (p0 >= n_vtrg) break;  // uniform across the group
+    const long p = p0 + gt;
     const bool in = p < n_vtrg;
-    // offsets occupied by some parent of the tile (CTA-uniform); the barrier
-    // keeps the reset after every thread's read of the previous tile's set
-    __syncthreads();
-    if (tid == 0) *live_s = 0;
-    __syncthreads();
+    // offsets occupied by some parent of the tile (uniform across the group);
+    // the named barrier keeps the reset after every read of the previous set
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
+    if (gt == 0) live_s[grp] = 0;
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
     const unsigned mine = in ? __ldg(vmask + p) : 0u;
     const unsigned wl = __reduce_or_sync(0xffffffffu, mine);
-    if ((tid & 31) == 0 && wl) atomicOr(live_s, wl);
-    __syncthreads();
-    unsigned rem = *live_s;
+    if ((gt & 31) == 0 && wl) atomicOr(&live_s[grp], wl);
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
+    unsigned rem = live_s[grp];
     const int nlive = __popc(rem);
     float sum[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) sum[i] = 0.f;
-    // neighbour row q of this thread's parent for an offset (zeros when none);
-    // the index q is loaded one step before the row, so that the row loads
-    // never wait for it
-    auto qload = [&](int o) { return in ? __ldg(vtab + (long)o * vt_stride + p) : -1; };
-    auto gather = [&](int q, float4 (&x)[4]) {
-      if (q >= 0) {
-        const float4* r = spec_in + ((long)q * n3h + f) * 4;
+    int olist[26];  // the tile's occupied offsets in increasing order
 #pragma unroll
-        for (int c = 0; c < 4; ++c) x[c] = __ldg(r + c);
-      } else {
+    for (int i = 0; i < 26; ++i) {
+      olist[i] = rem ? __ffs(rem) - 1 : 0;
+      rem &= rem ? rem - 1 : 0u;
+    }
+    // row of offset index i into stage i % kStages (zero-filled when the
+    // parent has no neighbour there); one copy group per offset index
+    auto stage_row = [&](int i, int q) {
+      const unsigned dst = row_base + (unsigned)((i % kStages) * kStageBytes);
+      const float4* src = spec_in + ((long)(q < 0 ? 0 : q) * n3h + f) * 4;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) x[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
+      for (int c = 0; c < 4; ++c) cp16(dst + 16u * (unsigned)(c ^ swz), src + c, q >= 0);
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
+    auto qload = [&](int i) { return (in && i < nlive) ? __ldg(vtab + (long)olist[i] * vt_stride + p) : -1; };
     auto drain = [&](unsigned j) {  // adds offset j's accumulator into sum
       const unsigned s = j & 1u;
-      mbar_wait(&bars[1 + s], (j >> 1) & 1u, err, kErrMma);
+      mbar_wait(&gbar[s], (j >> 1) & 1u, err, kErrMma);
       __syncwarp();
       tc_fence_after();
       float d[16];
       tmem_ld16(tmem + lane_base + 64u + 16u * s, d);
       tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) sum[i] = __fadd_rn(sum[i], d[i]);
+      for (int k = 0; k < 16; ++k) sum[k] = __fadd_rn(sum[k], d[k]);
     };
-    // offset i of the tile's occupied list: TF32 split, A stage, MMAs,
-    // and the drain of offset i-1
-    auto step = [&](int i, int o, const float4 (&x)[4]) {
+    // prologue: rows of offsets 0 .. kAhead-1 in flight, index of kAhead loaded
+    int qnext = qload(0);
+#pragma unroll
+    for (int i = 0; i < kAhead; ++i) {
+      const int q = qnext;
+      qnext = qload(i + 1);
+      stage_row(i, i < nlive ? q : -1);
+    }
+    for (int i = 0; i < nlive; ++i) {
       const unsigned j = jglob + (unsigned)i;
+      // rows of offset i + kAhead (an empty copy group past the end), index
+      // of the one after
+      {
+        const int q = qnext;
+        qnext = qload(i + kAhead + 1);
+        stage_row(i + kAhead, q);
+      }
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(kAhead) : "memory");  // offset i's row has landed
+      float v[16];
+      {
+        const unsigned src = row_base + (unsigned)((i % kStages) * kStageBytes);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          float4 w;
+          asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n"
+                       : "=f"(w.x), "=f"(w.y), "=f"(w.z), "=f"(w.w)
+                       : "r"(src + 16u * (unsigned)(c ^ swz))
+                       : "memory");
+          v[4 * c] = w.x;
+          v[4 * c + 1] = w.y;
+          v[4 * c + 2] = w.z;
+          v[4 * c + 3] = w.w;
+        }
+      }
       // TF32 hi / lo parts of the 16 values (K order = memory order)
       unsigned hi[16], lo[16];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const float v[4] = {x[c].x, x[c].y, x[c].z, x[c].w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const unsigned h = tf32_rna(v[e]);
-          hi[4 * c + e] = h;
-          lo[4 * c + e] = tf32_rna(v[e] - __uint_as_float(h));
-        }
+      for (int e = 0; e < 16; ++e) {
+        const unsigned h = tf32_rna(v[e]);
+        hi[e] = h;
+        lo[e] = tf32_rna(v[e] - __uint_as_float(h));
       }
       // A stage j&1 was last read by the MMAs of offset j-2, complete since
       // offset j-1 was drained (commits complete in order)
@@ -248,16 +307,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tmem_wait_st();
       tc_fence_before();
       __syncwarp();
-      // this warp's rows of A stage j&1 are written: one arrival per warp; the
-      // warps do not wait for each other, only the MMA-issuing thread waits
-      // for all four
-      if ((tid & 31) == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&bars[3 + (j & 1u)])) : "memory");
-      if (tid == 0) {
-        mbar_wait(&bars[3 + (j & 1u)], (j >> 1) & 1u, err, kErrMma);
+      // one arrival per warp; only the group's MMA-issuing thread waits for
+      // all four
+      if ((gt & 31) == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&gbar[2 + (j & 1u)])) : "memory");
+      if (gt == 0) {
+        mbar_wait(&gbar[2 + (j & 1u)], (j >> 1) & 1u, err, kErrMma);
         tc_fence_after();
         const unsigned d_col = tmem + 64u + 16u * (j & 1u);
         const unsigned a_hi = tmem + a_col, a_lo = tmem + a_col + 16u;
-        const unsigned ob = b_base + (unsigned)o * (4 * kOpBlockBytes);
+        const unsigned ob = b_base + (unsigned)olist[i] * (4 * kOpBlockBytes);
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           const unsigned long long bh = smem_desc(ob + (0 * 2 + ks) * kOpBlockBytes, 128, 256);
@@ -266,66 +325,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           mma_tf32(d_col, a_hi + 8u * ks, bl, kIdesc, true);
           mma_tf32(d_col, a_hi + 8u * ks, bh, kIdesc, true);
         }
-        mma_commit(&bars[1 + (j & 1u)]);
+        mma_commit(&gbar[j & 1u]);
       }
       if (i > 0) drain(j - 1);
-    };
-    auto take = [&]() {
-      const int o = __ffs(rem) - 1;
-      rem &= rem - 1;
-      return o;
-    };
-    // three register sets in turn: the rows of the next two offsets are in
-    // flight while one offset is processed, and the index of the one after
-    float4 xa[4], xb[4], xc[4];
-    int oa = 0, ob = 0, oc = 0, qa = -1, qb = -1, qc = -1;
-    if (nlive > 0) {
-      oa = take();
-      qa = qload(oa);
     }
-    if (nlive > 1) {
-      ob = take();
-      qb = qload(ob);
-    }
-    if (nlive > 2) {
-      oc = take();
-      qc = qload(oc);
-    }
-    if (nlive > 0) gather(qa, xa);
-    if (nlive > 1) gather(qb, xb);
-#pragma unroll 1
-    for (int i = 0; i < nlive; i += 3) {
-      // invariant: rows of i (xa) and i+1 (xb) requested, index of i+2 (qc) loaded
-      int oa2 = 0, qa2 = -1;
-      if (i + 2 < nlive) gather(qc, xc);
-      if (i + 3 < nlive) {
-        oa2 = take();
-        qa2 = qload(oa2);
-      }
-      step(i, oa, xa);
-      if (i + 3 < nlive) {
-        oa = oa2;
-        gather(qa2, xa);
-      }
-      int ob2 = 0, qb2 = -1;
-      if (i + 4 < nlive) {
-        ob2 = take();
-        qb2 = qload(ob2);
-      }
-      if (i + 1 < nlive) step(i + 1, ob, xb);
-      if (i + 4 < nlive) {
-        ob = ob2;
-        gather(qb2, xb);
-      }
-      int oc2 = 0, qc2 = -1;
-      if (i + 5 < nlive) {
-        oc2 = take();
-        qc2 = qload(oc2);
-      }
-      if (i + 2 < nlive) step(i + 2, oc, xc);
-      oc = oc2;
-      qc = qc2;
-    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // the empty trailing groups
     if (nlive > 0) drain(jglob + (unsigned)nlive - 1);
     jglob += (unsigned)nlive;
     if (in) {
@@ -338,7 +342,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tmem_slot),
+                 "r"(kTmemCols * kGroups)
+                 : "memory");
   }
 }
 
@@ -382,19 +388,19 @@ void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::
         }
 }
 
-void launch_hadamard_tc5(Context& ctx, int n3h, const void* sin_, void* sout, long p0, long np) {
+void launch_hadamard_tc5(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np) {
   DevTree& T = ctx.tree;
-  const size_t sm = (size_t)kOpBytes + 64;  // operators, 5 mbarriers, TMEM address, live-offset word
-  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc5_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const int tiles = 8;  // tiles of 128 target parents per CTA (operators staged once)
+  PVFMM_CUDA_CHECK(
+      cudaFuncSetAttribute(hadamard_tc5_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  const int tiles = 32;  // tiles of 128 target parents per CTA (operators staged once)
   dim3 grid((unsigned)((np + (long)kTcTile * tiles - 1) / ((long)kTcTile * tiles)), (unsigned)n3h);
   int* err = ctx.tc5_err_buf.as<int>(1);
   if (!ctx.tc5_err) PVFMM_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int), ctx.stream));  // once per evaluation
   ++ctx.n_launch;
-  hadamard_tc5_kernel<<<grid, kTcThreads, sm, ctx.stream>>>(
+  hadamard_tc5_kernel<<<grid, kGroups * kTcThreads, kSmemBytes, ctx.stream>>>(
       n3h, np, T.n_vtrg, tiles, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
-      reinterpret_cast<const float4*>(sin_), ctx.dops.vop_tc5.get<unsigned char>(), reinterpret_cast<float4*>(sout),
-      err);
+      reinterpret_cast<const float4*>(sin_), ctx.dops.vop_tc5.get<unsigned char>() + f_base * kOpBytes,
+      reinterpret_cast<float4*>(sout), err);
   PVFMM_CUDA_CHECK(cudaGetLastError());
   ctx.tc5_err = err;
 }

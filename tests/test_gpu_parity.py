@@ -356,3 +356,21 @@ def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
     ctx.close()
     for k in range(4):
         assert O.rel_l2(a[:, k], b[:, k]) < 1e-7, k
+
+
+@pytest.mark.parametrize("prec,kid", [(P.PRECISION_PLAIN, 6), (P.PRECISION_MIXED, 6), (P.PRECISION_PLAIN, 3)])
+def test_vlist_frequency_slabs_match_the_whole_spectrum(monkeypatch, prec, kid):
+    """When the source parents' spectra do not fit in device memory the V-list
+    runs in slabs of kz: each slab's forward DFT rows, products and inverse-DFT
+    contribution in turn (the transforms are linear).  The result equals the
+    one-slab evaluation to rounding."""
+    K = O.KERNELS[kid]
+    src = points("gauss", 20000, 51)
+    den = np.random.default_rng(52).uniform(-1, 1, (20000, K.k0))
+    whole, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=prec)
+    ctx.close()
+    monkeypatch.setenv("PVFMM_B200_VLIST_SLABS", "5")
+    sliced, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=prec)
+    ctx.close()
+    tol = 1e-13 if prec == P.PRECISION_PLAIN else 1e-7
+    assert O.rel_l2(sliced.reshape(-1), whole.reshape(-1)) < tol
