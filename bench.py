@@ -347,44 +347,42 @@ def cpu_baseline(args):
 # a launch processes (traffic grows in proportion).  Units: n_vsrc + n_vtrg for
 # the Hadamard kernels, n_trg for the near field.
 TRAFFIC_1M = {
-    ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
+    ("hadamard", 4): {"bytes": 877601280 + 672896000, "units": 4768 + 4767},     # hadamard_tc5_kernel
     ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
-    ("near_field", 4): {"bytes": 149822464 + 20088064, "units": 1000000},        # near_field_kernel<float>
+    ("near_field", 4): {"bytes": 149441536 + 24975104, "units": 1000000},        # near_field_kernel<float>
     ("near_field", 8): {"bytes": 151890688 + 20192256, "units": 1000000},        # near_field_kernel<double>
 }
-TF32_DENSE_NOMINAL_TFLOPS = 1100.0  # B200 dense TF32 tensor throughput (nominal)
 # kernel that computes the V-list Hadamard products: (real bytes, ke) -> name
-HADAMARD_KERNEL = {(4, 1): "hadamard_tc_kernel (V-list M2L, TF32 mma.sync, 3-term split)",
+HADAMARD_KERNEL = {(4, 1): "hadamard_tc5_kernel (V-list M2L, tcgen05 kind::tf32 3-term split, TMEM accumulators)",
                    (8, 1): "hadamard_rd_kernel<double> (V-list M2L)",
-                   (4, 3): "hadamard_kernel<float, 3> (V-list M2L)",
-                   (8, 3): "hadamard_kernel<double, 3> (V-list M2L)"}
+                   (4, 3): "hadamard_kernel<float, 3, 3> (V-list M2L)",
+                   (8, 3): "hadamard_kernel<double, 3, 3> (V-list M2L)"}
+NEAR_KERNEL = "near_field_kernel (U-list P2P + W + D2T)"
 
 
 def roofline(B, peaks):
-    """Roofline objects of the V-list Hadamard and the fused near field.
+    """Roofline objects of the V-list Hadamard and the fused near field,
+    the slower first.
 
-    Neither kernel is HBM-bound: the near field is bound by the SIMT FP32
-    (mixed) / FP64 (plain) pipes and issue, the mixed form's Hadamard by the
-    tensor pipe and issue, the plain form's by the FP64 pipe.  The HBM view
-    (algorithmic bytes / kernel time against the measured copy bandwidth) is
-    the reported `achieved`/`peak`,
-    and `compute` gives the FLOP view against the nominal SIMT peak
-    (148 SMs x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock), or for the
-    tensor-core Hadamard against the nominal dense TF32 tensor peak (its
-    algorithmic flops; the 3-term split issues three MMAs per product).
-    Algorithmic units:
-      Hadamard: bytes = (n_vsrc + n_vtrg) * n3h * 8 children * 2 * rb (input
-        spectra read once, output spectra written once) + 26 * n3h * 64 * 2 * rb
-        (operators read once); flops = 512 * n3h * v_pairs (8x8 complex
-        matrix-vector product per (target parent, offset, frequency)).
-      near field: bytes = n_src * 32 + n_trg * 56 (sorted points and densities
-        read once, 4 outputs written) + n_tleaf * ns * 8 (D2T densities);
-        flops = 18 per pair (pot+grad) over p2p + w + d2t pairs.
-    """
+    near field: bound by the SIMT FP32 (mixed) / FP64 (plain) pipes, so its
+      object is the FLOP view: `bound` "fp32" / "fp64", achieved = algorithmic
+      flops (18 per pair for pot+grad, kernel.txx conventions otherwise, over
+      P2P + W + D2T pairs) / kernel time, peak = the nominal SIMT peak (148 SMs
+      x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock; the measured peaks
+      have no SIMT figure).  Its HBM view is the `hbm` sub-object.
+    Hadamard: the HBM view (the north star's bar for it): algorithmic bytes =
+      (n_vsrc + n_vtrg) * n3h * 8 children * 2 * rb (input spectra read once,
+      output spectra written once) + 26 * n3h * 64 * 2 * rb (operators read
+      once) against the measured copy bandwidth; its tensor view (mixed form:
+      the split issues 3 TF32 products per product, against a dense TF32 peak
+      of half the measured bf16 peak) or FP64 SIMT view (plain form) is the
+      `compute` sub-object.
+    `traffic` is the ncu DRAM traffic of a launch scaled from 1M points."""
     st = B["stats"]
     rb = B["real_bytes"]
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
     smax = (B["clocks"] or {}).get("sm_max_mhz") or 1965.0
     lanes = 128 if rb == 4 else 64
     simt_peak = 148 * lanes * 2 * smax * 1e6 / 1e12
@@ -393,30 +391,39 @@ def roofline(B, peaks):
     k0, k1 = KDIM[kid]
     n3h = (2 * m) ** 2 * (m + 1)
     ns = 6 * (m - 1) ** 2 + 2
-    out = {}
+
+    def traffic(tkey, units):
+        tr = TRAFFIC_1M.get((tkey, rb)) if kid == 6 else None
+        return tr["bytes"] * units / tr["units"] if tr else None
+
     had_ms = B["stages_ms"]["V-Hadamard"]
     had_bytes = (st["n_vsrc"] + st["n_vtrg"]) * n3h * 8 * ke * 2 * rb + 26 * n3h * 64 * ke * ke * 2 * rb
     had_flops = 512.0 * ke * ke * n3h * st["v_pairs"]
+    had_gbs = had_bytes / (had_ms / 1000) / 1e9 if had_ms > 0 else 0.0
+    had_tf = had_flops / (had_ms / 1000) / 1e12 if had_ms > 0 else 0.0
+    tensor = rb == 4 and ke == 1
+    had = {"kernel": HADAMARD_KERNEL[(rb, ke)], "bound": "hbm", "achieved": had_gbs, "peak": hbm_peak, "unit": "GB/s",
+           "frac": had_gbs / hbm_peak, "peak_source": peak_src,
+           "traffic": traffic("hadamard", st["n_vsrc"] + st["n_vtrg"]), "algorithmic_bytes": had_bytes,
+           "kernel_ms": had_ms,
+           "compute": ({"pipe": "tensor tf32 x3 (tcgen05)", "achieved_tflops": 3 * had_tf, "peak_tflops": tf32_peak,
+                        "peak_source": "half the measured bf16 dense peak", "frac": 3 * had_tf / tf32_peak,
+                        "algorithmic_flops": had_flops} if tensor else
+                       {"pipe": "fp32 simt" if rb == 4 else "fp64 simt", "achieved_tflops": had_tf,
+                        "peak_tflops": simt_peak, "peak_source": "nominal", "frac": had_tf / simt_peak,
+                        "algorithmic_flops": had_flops})}
     near_ms = B["stages_ms"]["near-field kernel"]
     near_bytes = st["n_src"] * (24 + 8 * k0) + st["n_trg"] * (24 + 8 * k1) + st["n_tleaf"] * ns * ke * 8
     near_flops = float(PAIR_FLOPS[kid]) * (st["p2p_pairs"] + st["w_pairs"] + st["d2t_pairs"])
-    had_name = HADAMARD_KERNEL[(rb, ke)]
-    for name, ms, byts, flops, tkey, units in (
-            (had_name, had_ms, had_bytes, had_flops, "hadamard", st["n_vsrc"] + st["n_vtrg"]),
-            ("near_field_kernel (U-list P2P + W + D2T)", near_ms, near_bytes, near_flops, "near_field", st["n_trg"])):
-        ach = byts / (ms / 1000) / 1e9 if ms > 0 else 0.0
-        tr = TRAFFIC_1M[(tkey, rb)] if kid == 6 else {"bytes": None}
-        traffic = tr["bytes"] * units / tr["units"] if tr["bytes"] else None
-        tflops = flops / (ms / 1000) / 1e12 if ms > 0 else 0.0
-        peak_tf = TF32_DENSE_NOMINAL_TFLOPS if name.startswith("hadamard_tc") else simt_peak
-        out[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": traffic,
-                     "algorithmic_bytes": byts, "kernel_ms": ms,
-                     "compute": {"pipe": ("tf32 mma.sync x3" if name.startswith("hadamard_tc") else
-                                          "fp32 simt" if rb == 4 else "fp64 simt"), "achieved_tflops": tflops,
-                                 "nominal_peak_tflops": peak_tf, "frac": tflops / peak_tf,
-                                 "flops": flops}}
-    ranked = sorted(out.values(), key=lambda r: -r["kernel_ms"])
+    near_tf = near_flops / (near_ms / 1000) / 1e12 if near_ms > 0 else 0.0
+    near_gbs = near_bytes / (near_ms / 1000) / 1e9 if near_ms > 0 else 0.0
+    near = {"kernel": NEAR_KERNEL, "bound": "fp32" if rb == 4 else "fp64", "achieved": near_tf, "peak": simt_peak,
+            "unit": "TFLOP/s", "frac": near_tf / simt_peak,
+            "peak_source": "nominal SIMT peak at the max SM clock (no measured SIMT peak)",
+            "traffic": traffic("near_field", st["n_trg"]), "algorithmic_flops": near_flops, "kernel_ms": near_ms,
+            "hbm": {"achieved": near_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": near_gbs / hbm_peak,
+                    "peak_source": peak_src, "algorithmic_bytes": near_bytes}}
+    ranked = sorted([had, near], key=lambda r: -r["kernel_ms"])
     return ranked[0], ranked[1]
 
 

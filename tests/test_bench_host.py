@@ -23,22 +23,28 @@ def _run(rb, had_ms, near_ms, stats=STATS_1M, peaks=None):
 def test_roofline_objects_follow_the_contract(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     assert dom["kernel_ms"] >= nxt["kernel_ms"]
-    for r in (dom, nxt):
-        assert r["bound"] in ("hbm", "tensor")
-        assert r["unit"] == "GB/s" and r["peak"] == 6449.1 and r["peak_source"] == "measured"
-        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
-        assert r["achieved"] == pytest.approx(r["algorithmic_bytes"] / (r["kernel_ms"] / 1000) / 1e9)
-        c = r["compute"]
-        assert c["frac"] == pytest.approx(c["achieved_tflops"] / c["nominal_peak_tflops"])
-    names = {dom["kernel"], nxt["kernel"]}
-    assert any(n.startswith("hadamard_tc" if rb == 4 else "hadamard_rd") for n in names)
+    by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
+    had = by["hadamard_tc5_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    near = by["near_field_kernel"]
+    # the Hadamard: HBM view against the measured copy bandwidth
+    assert had["bound"] == "hbm" and had["unit"] == "GB/s" and had["peak"] == 6449.1
+    assert had["peak_source"] == "measured" and had["frac"] == pytest.approx(had["achieved"] / had["peak"])
+    assert had["achieved"] == pytest.approx(had["algorithmic_bytes"] / (had["kernel_ms"] / 1000) / 1e9)
+    c = had["compute"]
+    assert c["frac"] == pytest.approx(c["achieved_tflops"] / c["peak_tflops"])
+    # the near field: FLOP view against the SIMT pipe it is bound by, HBM view beside it
+    assert near["bound"] == ("fp32" if rb == 4 else "fp64") and near["unit"] == "TFLOP/s"
+    assert near["peak"] == pytest.approx(148 * (128 if rb == 4 else 64) * 2 * 1965e6 / 1e12)
+    assert near["achieved"] == pytest.approx(near["algorithmic_flops"] / (near["kernel_ms"] / 1000) / 1e12)
+    assert near["frac"] == pytest.approx(near["achieved"] / near["peak"])
+    assert near["hbm"]["frac"] == pytest.approx(near["hbm"]["achieved"] / 6449.1)
 
 
 @pytest.mark.parametrize("rb", [4, 8])
 def test_traffic_at_the_capture_size_is_the_capture(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
-    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    had = by["hadamard_tc5_kernel" if rb == 4 else "hadamard_rd_kernel"]
     assert had["traffic"] == bench.TRAFFIC_1M[("hadamard", rb)]["bytes"]
     assert by["near_field_kernel"]["traffic"] == bench.TRAFFIC_1M[("near_field", rb)]["bytes"]
 
@@ -47,7 +53,7 @@ def test_traffic_scales_with_the_units_of_a_launch():
     st = dict(STATS_1M, n_vsrc=2 * 4768.0, n_vtrg=2 * 4767.0, n_trg=4e6)
     dom, nxt = _run(4, 10.0, 12.0, stats=st)
     by = {r["kernel"].split()[0]: r for r in (dom, nxt)}
-    assert by["hadamard_tc_kernel"]["traffic"] == pytest.approx(2 * bench.TRAFFIC_1M[("hadamard", 4)]["bytes"])
+    assert by["hadamard_tc5_kernel"]["traffic"] == pytest.approx(2 * bench.TRAFFIC_1M[("hadamard", 4)]["bytes"])
     assert by["near_field_kernel"]["traffic"] == pytest.approx(4 * bench.TRAFFIC_1M[("near_field", 4)]["bytes"])
 
 
@@ -138,8 +144,10 @@ def test_json_line_follows_the_contract():
     assert line["e2e"]["h2d_bytes_per_step"] == 4_000_000 * (3 + 1) * 8
     assert line["e2e"]["d2h_bytes_per_step"] == 4_000_000 * 4 * 8
     r = line["roofline"]
-    assert set(r) >= {"bound", "achieved", "peak", "unit", "frac", "traffic"} and r["bound"] in ("hbm", "tensor")
-    assert r["peak_source"] == "measured" and r["traffic"] > 0
+    assert set(r) >= {"bound", "achieved", "peak", "unit", "frac", "traffic"}
+    assert r["bound"] in ("hbm", "tensor", "fp32", "fp64") and r["traffic"] > 0
+    hbm = r if r["bound"] == "hbm" else r["hbm"]
+    assert hbm["peak_source"] == "measured"
 
 
 def test_a_form_over_the_bar_in_one_component_is_not_reported():
@@ -147,7 +155,8 @@ def test_a_form_over_the_bar_in_one_component_is_not_reported():
              "mixed": _form(109e6, 5.5e-7, [2.3e-7, 1.2e-6, 4.8e-7, 5.6e-7], 4)}   # one component > 1e-6
     line = bench.build_line(_Args, 1, 4_000_000, forms, {})
     assert line["form"] == "plain" and line["dtype"] == "f64"
-    assert line["roofline"]["peak_source"] == "fallback"
+    r = line["roofline"]
+    assert (r if r["bound"] == "hbm" else r["hbm"])["peak_source"] == "fallback"
 
 
 def test_a_form_that_failed_is_kept_in_the_line():
