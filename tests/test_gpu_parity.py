@@ -372,7 +372,7 @@ def test_vlist_frequency_slabs_match_the_whole_spectrum(monkeypatch, prec, kid):
     monkeypatch.setenv("PVFMM_B200_VLIST_SLABS", "5")
     sliced, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=prec)
     ctx.close()
-    # plain: FP64 rounding only; mixed: the slabs' FP32 inverse DFTs round
+    # plain: FP64 rounding only (2e-13 for Stokes); mixed: the slabs' FP32 inverse DFTs round
     # differently from one whole transform (measured 2e-7), within its bar
-    tol = 1e-13 if prec == P.PRECISION_PLAIN else 1e-6
+    tol = 1e-12 if prec == P.PRECISION_PLAIN else 1e-6
     assert O.rel_l2(sliced.reshape(-1), whole.reshape(-1)) < tol
