@@ -1501,6 +1501,13 @@ int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
 // output spectra of one chunk at a time; one chunk when device memory
 // allows).  With several chunks, stage 4 ends after the first chunk's
 // products and stage 5 covers the rest.
+// The mixed form's scalar Hadamard runs on tcgen05 when PVFMM_B200_HADAMARD is
+// "tcgen05" (the warp-level MMA kernel otherwise, or with "mma").
+bool use_tc5(const Context& ctx) {
+  const char* e = std::getenv("PVFMM_B200_HADAMARD");
+  return e && std::strcmp(e, "tcgen05") == 0;
+}
+
 template <class Real, int M>
 void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
                  long chunk, int nslab, const std::function<void(int)>& ev) {
@@ -1530,8 +1537,8 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
       const long np = std::min(chunk, T.n_vtrg - p0);
       if (kin == 1 && kout == 1) {
         if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
-        else if (std::getenv("PVFMM_B200_HADAMARD_MMA_SYNC")) launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
-        else launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
+        else if (use_tc5(ctx)) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
+        else launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
       } else if (kout == 3) {  // Stokes velocity, Biot-Savart
         launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
       } else if (kout == 1) {  // Stokes pressure

@@ -348,10 +348,11 @@ def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
     inside the tensor cores differs)."""
     src = points("gauss", 40000, 41)
     den = np.random.default_rng(42).uniform(-1, 1, 40000)
+    monkeypatch.setenv("PVFMM_B200_HADAMARD", "tcgen05")
     a, ctx = gpu_eval(6, 8, 128, src, den, src, prec=P.PRECISION_MIXED)
     assert ctx.tree_stats()["n_vtrg"] > 200
     ctx.close()
-    monkeypatch.setenv("PVFMM_B200_HADAMARD_MMA_SYNC", "1")
+    monkeypatch.setenv("PVFMM_B200_HADAMARD", "mma")
     b, ctx = gpu_eval(6, 8, 128, src, den, src, prec=P.PRECISION_MIXED)
     ctx.close()
     for k in range(4):
