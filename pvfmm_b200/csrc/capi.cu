@@ -60,7 +60,7 @@ void destroy_context(Context& c) {
   DevTree& T = c.tree;
   DevBuf* tb[] = {&T.key, &T.leaf, &T.parent, &T.child0, &T.src_lo, &T.src_hi, &T.trg_lo, &T.trg_hi, &T.colleague,
                   &T.int_idx, &T.src_perm, &T.trg_perm, &T.src_key, &T.trg_key, &T.src_leaf, &T.trg_leaf, &T.sx,
-                  &T.sy, &T.sz, &T.tx, &T.ty, &T.tz, &T.sleaf, &T.tleaf, &T.vsrc, &T.vtrg, &T.node2vsrc, &T.vtab, &T.vmask,
+                  &T.sy, &T.sz, &T.tx, &T.ty, &T.tz, &T.sleaf, &T.tleaf, &T.vsrc, &T.vtrg, &T.node2vsrc, &T.vtab, &T.vmask, &T.vmorton, &T.vunion, &T.vucount, &T.vlocal,
                   &T.xtrg, &T.x_off, &T.x_list, &T.p_off, &T.p_list, &T.w_off, &T.w_list};
   for (DevBuf* b : tb) b->release();
   if (c.events_ready)

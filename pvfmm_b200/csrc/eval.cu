@@ -1595,6 +1595,10 @@ void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const 
     const long c = std::atol(e);
     if (c > 0) chunk = std::min(chunk, c);
   }
+  // the tcgen05 Hadamard walks tiles of Morton-consecutive targets, which stay
+  // inside windows of 2048 positions: its chunks are whole windows
+  if (sizeof(Real) == 4 && kin == 1 && kout == 1 && use_tc5(ctx) && chunk < T.n_vtrg)
+    chunk = std::max(2048L, chunk / 2048 * 2048);
   Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * kout);
   switch (m) {
     case 2: vlist_fft_t<Real, 2>(ctx, ue, dc, sin_, sout, kin, kout, chunk, nslab, ev); break;

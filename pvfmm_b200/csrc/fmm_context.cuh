@@ -39,6 +39,12 @@ struct DevTree {
   DevBuf node2vsrc;                   // int per node (-1)
   DevBuf vtab;                        // int[26] per vtrg: vsrc index per colleague offset (-1)
   DevBuf vmask;                       // unsigned per vtrg: bit o set when vtab[o] >= 0 (vtrg sorted by it)
+  DevBuf vmorton;                     // int per vtrg: position of the target of each Morton rank
+  // tiles of 128 Morton-consecutive V-list targets (tcgen05 Hadamard): the
+  // sorted union of their source parents and each (target, offset)'s index
+  // into it; built on first use after a tree build
+  DevBuf vunion, vucount, vlocal;
+  bool vtiles_valid = false;
   DevBuf xtrg;                        // target nodes with X-list entries
   DevBuf x_off, x_list;               // CSR over xtrg
   DevBuf p_off, p_list;               // CSR over tleaf: P2P source leaves

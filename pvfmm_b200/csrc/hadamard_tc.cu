@@ -133,35 +133,124 @@ __device__ __forceinline__ unsigned tf32_rna(float x) {
 constexpr int kErrOperators = 1, kErrMma = 2;
 
 constexpr int kGroups = 4;                      // tile pipelines (warpgroups) per CTA
-constexpr int kStages = 5;                      // neighbour-row stages per pipeline
-constexpr int kAhead = kStages - 1;             // offsets whose rows are in flight
 constexpr int kRowBytes = 64;                   // one spectrum row: 8 children x complex FP32
-constexpr int kStageBytes = kTcTile * kRowBytes;
-constexpr size_t kSmemBytes = (size_t)kOpBytes + (size_t)kGroups * kStages * kStageBytes + 256;
+constexpr int kUnionEntries = kTcTile * 26;     // (target, offset) pairs of a tile
+constexpr int kUnionCap = 512;                  // union rows a pipeline stages in shared memory
+constexpr int kLocalStride = 32;                // offsets per target in the local-index table (26 used)
+constexpr int kUnionBytes = kUnionCap * kRowBytes;
+constexpr int kLocalBytes = kTcTile * kLocalStride * 2;
+constexpr int kGroupBytes = kUnionBytes + kLocalBytes;
+constexpr size_t kSmemBytes = (size_t)kOpBytes + (size_t)kGroups * kGroupBytes + 256;
+constexpr unsigned short kNoSource = 0xffff;
 
 __device__ __forceinline__ void cp16(unsigned smem, const void* gmem, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem), "l"(gmem), "r"(valid ? 16 : 0)
                : "memory");
 }
 
+// Source unions of the tiles of 128 Morton-consecutive V-list targets (one
+// block per tile): the (target, offset) pairs of the tile are sorted by source
+// parent (bitonic sort of 4096 keys in shared memory), the distinct sources
+// form the tile's union (sorted), and each pair gets the index of its source
+// in the union (kNoSource where the target has no source at that offset).
+// The tiles of a Morton window share most of their neighbours: at 300k
+// Gaussian points a tile's 3,328 pairs reference ~270 distinct sources.
+__global__ void __launch_bounds__(512) vlist_tile_unions(long n_vtrg, long vt_stride, const int* __restrict__ vtab,
+                                                         const int* __restrict__ vmorton, int* __restrict__ vunion,
+                                                         int* __restrict__ vucount, unsigned short* __restrict__ vlocal) {
+  constexpr int NE = 4096, NT = 512;
+  __shared__ unsigned long long e[NE];  // source << 32 | pair index; ~0 = no source
+  __shared__ int wsum[NT / 32];
+  const int tid = threadIdx.x;
+  const long tile = blockIdx.x;
+  unsigned short* loc = vlocal + tile * kTcTile * kLocalStride;
+  for (int i = tid; i < kTcTile * kLocalStride; i += NT) loc[i] = kNoSource;
+  for (int i = tid; i < NE; i += NT) {
+    unsigned long long v = ~0ull;
+    if (i < kUnionEntries) {
+      const int r = i / 26, o = i % 26;
+      const long k = tile * kTcTile + r;
+      const int q = k < n_vtrg ? vtab[(long)o * vt_stride + vmorton[k]] : -1;
+      if (q >= 0) v = (unsigned long long)(unsigned)q << 32 | (unsigned)i;
+    }
+    e[i] = v;
+  }
+  __syncthreads();
+  for (int k = 2; k <= NE; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < NE; i += NT) {
+        const int l = i ^ j;
+        if (l > i) {
+          const unsigned long long a = e[i], b = e[l];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            e[i] = b;
+            e[l] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  // thread t owns entries [8t, 8t+8): distinct-source flags, then a block scan
+  constexpr int PER = NE / NT;
+  int cnt = 0;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = tid * PER + u;
+    const unsigned long long v = e[i];
+    if (v != ~0ull && (i == 0 || (e[i - 1] >> 32) != (v >> 32))) ++cnt;
+  }
+  const int lane = tid & 31, w = tid >> 5;
+  int inc = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += y;
+  }
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int x = 0; x < w; ++x) before += wsum[x];
+  int pos = before + inc - cnt - 1;  // index of the last distinct source before this thread's entries
+  int* un = vunion + tile * kUnionEntries;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = tid * PER + u;
+    const unsigned long long v = e[i];
+    if (v == ~0ull) continue;
+    if (i == 0 || (e[i - 1] >> 32) != (v >> 32)) {
+      ++pos;
+      un[pos] = (int)(v >> 32);
+    }
+    const int pair = (int)(v & 0xffffffffu), r = pair / 26, o = pair % 26;
+    loc[r * kLocalStride + o] = (unsigned short)pos;
+  }
+  if (tid == NT - 1) {
+    int total = 0;
+    for (int x = 0; x < NT / 32; ++x) total += wsum[x];
+    vucount[tile] = total;
+  }
+}
+
 // One CTA per SM: four independent tile pipelines (warpgroups of 128 threads,
-// one TMEM lane per parent) share the frequency's operator blocks.  In each
-// pipeline a thread stages its parent's neighbour rows with cp.async
-// kAhead offsets ahead of the one it multiplies (a thread only reads the rows
-// it copied itself, so its own copy groups order the stages); the 16-byte
-// chunks of row r sit at chunk slot c ^ ((r >> 1) & 3), so that the row reads
-// of a warp do not conflict on shared-memory banks.
+// one TMEM lane per target) share the frequency's operator blocks.  A tile is
+// 128 Morton-consecutive targets; at its start the pipeline stages the rows
+// of the tile's source union at this frequency (up to kUnionCap rows; the
+// chunks of row u at slot c ^ ((u >> 1) & 3), against bank conflicts) and the
+// tile's local-index table, so that each (target, offset) row is then read
+// from shared memory.
 __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
-    hadamard_tc5_kernel(int n3h, long n_vtrg, long vt_stride, int tiles_per_cta, const int* __restrict__ vtab,
-                        const unsigned* __restrict__ vmask, const float4* __restrict__ spec_in,
-                        const unsigned char* __restrict__ ops, float4* __restrict__ spec_out, int* __restrict__ err) {
+    hadamard_tc5_kernel(int n3h, long p0, long np, long vt_stride, int tiles_per_cta, const int* __restrict__ vmorton,
+                        const unsigned* __restrict__ vmask, const int* __restrict__ vunion,
+                        const int* __restrict__ vucount, const unsigned short* __restrict__ vlocal,
+                        const float4* __restrict__ spec_in, const unsigned char* __restrict__ ops,
+                        float4* __restrict__ spec_out, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* Bs = smem;                                          // kOpBytes
-  unsigned char* rows = smem + kOpBytes;                             // [group][stage][128 rows][64 B]
+  unsigned char* gsm = smem + kOpBytes;                              // [group]: union rows, local indices
   // mbarriers: [0] operators arrived; per group g at 1 + 4g: [+0, +1] MMAs of
   // A stage 0/1 done, [+2, +3] A stage 0/1 written by the group's four warps
-  unsigned long long* bars =
-      reinterpret_cast<unsigned long long*>(smem + kOpBytes + (size_t)kGroups * kStages * kStageBytes);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kOpBytes + (size_t)kGroups * kGroupBytes);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 1 + 4 * kGroups);
   unsigned* live_s = tmem_slot + 1;                                  // [kGroups]
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -205,46 +294,52 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
   }
   mbar_wait(&bars[0], 0, err, kErrOperators);
   const unsigned b_base = smem_u32(Bs);
-  // this thread's row slot in each stage of its group
-  const unsigned row_base = smem_u32(rows) + (unsigned)(grp * kStages * kStageBytes + gt * kRowBytes);
-  const int swz = (gt >> 1) & 3;
+  const unsigned union_base = smem_u32(gsm) + (unsigned)(grp * kGroupBytes);
+  const unsigned local_base = union_base + kUnionBytes;
+  const long n_tiles = (np + kTcTile - 1) / kTcTile;
 
   unsigned jglob = 0;  // offsets processed by this group (mbarrier phase bookkeeping)
   for (int tl = grp; tl < tiles_per_cta; tl += kGroups) {
-    const long p0 = ((long)blockIdx.x * tiles_per_cta + tl) * kTcTile;
-    if (p0 >= n_vtrg) break;  // uniform across the group
-    const long p = p0 + gt;
-    const bool in = p < n_vtrg;
-    // offsets occupied by some parent of the tile (uniform across the group);
-    // the named barrier keeps the reset after every read of the previous set
+    const long tile = (long)blockIdx.x * tiles_per_cta + tl;  // within the chunk
+    if (tile >= n_tiles) break;                                // uniform across the group
+    const long tg = p0 / kTcTile + tile;                       // tile of the whole V-list
+    const long k = p0 + tile * kTcTile + gt;                   // this thread's Morton rank
+    const bool in = k < p0 + np;
+    const long p = in ? (long)__ldg(vmorton + k) : 0;          // its position (output row p - p0)
+    // every thread of the group is done with the previous tile's shared rows
     asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
     if (gt == 0) live_s[grp] = 0;
+    // stage the tile's union rows (at this frequency) and local-index table
+    const int nu = __ldg(vucount + tg);
+    const int ns_ = min(nu, kUnionCap);
+    const int* un = vunion + tg * kUnionEntries;
+    for (int u = gt; u < ns_; u += kTcThreads) {
+      const float4* src = spec_in + ((long)__ldg(un + u) * n3h + f) * 4;
+      const unsigned dst = union_base + (unsigned)(u * kRowBytes);
+      const int sw = (u >> 1) & 3;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) cp16(dst + 16u * (unsigned)(c ^ sw), src + c, true);
+    }
+    {
+      const unsigned char* lsrc = reinterpret_cast<const unsigned char*>(vlocal + tg * kTcTile * kLocalStride);
+#pragma unroll
+      for (int c = 0; c < kLocalBytes / 16 / kTcThreads; ++c) {
+        const int chunk = gt + c * kTcThreads;
+        cp16(local_base + 16u * (unsigned)chunk, lsrc + 16 * chunk, true);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
     const unsigned mine = in ? __ldg(vmask + p) : 0u;
     const unsigned wl = __reduce_or_sync(0xffffffffu, mine);
     if ((gt & 31) == 0 && wl) atomicOr(&live_s[grp], wl);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(kTcThreads) : "memory");
     unsigned rem = live_s[grp];
     const int nlive = __popc(rem);
     float sum[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) sum[i] = 0.f;
-    int olist[26];  // the tile's occupied offsets in increasing order
-#pragma unroll
-    for (int i = 0; i < 26; ++i) {
-      olist[i] = rem ? __ffs(rem) - 1 : 0;
-      rem &= rem ? rem - 1 : 0u;
-    }
-    // row of offset index i into stage i % kStages (zero-filled when the
-    // parent has no neighbour there); one copy group per offset index
-    auto stage_row = [&](int i, int q) {
-      const unsigned dst = row_base + (unsigned)((i % kStages) * kStageBytes);
-      const float4* src = spec_in + ((long)(q < 0 ? 0 : q) * n3h + f) * 4;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) cp16(dst + 16u * (unsigned)(c ^ swz), src + c, q >= 0);
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
-    auto qload = [&](int i) { return (in && i < nlive) ? __ldg(vtab + (long)olist[i] * vt_stride + p) : -1; };
     auto drain = [&](unsigned j) {  // adds offset j's accumulator into sum
       const unsigned s = j & 1u;
       mbar_wait(&gbar[s], (j >> 1) & 1u, err, kErrMma);
@@ -254,36 +349,40 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
       tmem_ld16(tmem + lane_base + 64u + 16u * s, d);
       tmem_wait_ld();
 #pragma unroll
-      for (int k = 0; k < 16; ++k) sum[k] = __fadd_rn(sum[k], d[k]);
+      for (int k2 = 0; k2 < 16; ++k2) sum[k2] = __fadd_rn(sum[k2], d[k2]);
     };
-    // prologue: rows of offsets 0 .. kAhead-1 in flight, index of kAhead loaded
-    int qnext = qload(0);
-#pragma unroll
-    for (int i = 0; i < kAhead; ++i) {
-      const int q = qnext;
-      qnext = qload(i + 1);
-      stage_row(i, i < nlive ? q : -1);
-    }
     for (int i = 0; i < nlive; ++i) {
+      const int o = __ffs(rem) - 1;
+      rem &= rem - 1;
       const unsigned j = jglob + (unsigned)i;
-      // rows of offset i + kAhead (an empty copy group past the end), index
-      // of the one after
-      {
-        const int q = qnext;
-        qnext = qload(i + kAhead + 1);
-        stage_row(i + kAhead, q);
-      }
-      asm volatile("cp.async.wait_group %0;\n" ::"n"(kAhead) : "memory");  // offset i's row has landed
+      // this target's neighbour row at offset o: from the staged union, from
+      // L2 past the staged rows, zeros without a source
+      unsigned short u;
+      asm volatile("ld.shared.u16 %0, [%1];\n" : "=h"(u) : "r"(local_base + 2u * (unsigned)(gt * kLocalStride + o)));
       float v[16];
-      {
-        const unsigned src = row_base + (unsigned)((i % kStages) * kStageBytes);
+      if (u == kNoSource) {
+#pragma unroll
+        for (int e2 = 0; e2 < 16; ++e2) v[e2] = 0.f;
+      } else if (u < kUnionCap) {
+        const unsigned src = union_base + (unsigned)(u * kRowBytes);
+        const int sw = (u >> 1) & 3;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           float4 w;
           asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n"
                        : "=f"(w.x), "=f"(w.y), "=f"(w.z), "=f"(w.w)
-                       : "r"(src + 16u * (unsigned)(c ^ swz))
+                       : "r"(src + 16u * (unsigned)(c ^ sw))
                        : "memory");
+          v[4 * c] = w.x;
+          v[4 * c + 1] = w.y;
+          v[4 * c + 2] = w.z;
+          v[4 * c + 3] = w.w;
+        }
+      } else {
+        const float4* r = spec_in + ((long)__ldg(un + u) * n3h + f) * 4;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float4 w = __ldg(r + c);
           v[4 * c] = w.x;
           v[4 * c + 1] = w.y;
           v[4 * c + 2] = w.z;
@@ -293,10 +392,10 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
       // TF32 hi / lo parts of the 16 values (K order = memory order)
       unsigned hi[16], lo[16];
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        const unsigned h = tf32_rna(v[e]);
-        hi[e] = h;
-        lo[e] = tf32_rna(v[e] - __uint_as_float(h));
+      for (int e2 = 0; e2 < 16; ++e2) {
+        const unsigned h = tf32_rna(v[e2]);
+        hi[e2] = h;
+        lo[e2] = tf32_rna(v[e2] - __uint_as_float(h));
       }
       // A stage j&1 was last read by the MMAs of offset j-2, complete since
       // offset j-1 was drained (commits complete in order)
@@ -316,7 +415,7 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
         tc_fence_after();
         const unsigned d_col = tmem + 64u + 16u * (j & 1u);
         const unsigned a_hi = tmem + a_col, a_lo = tmem + a_col + 16u;
-        const unsigned ob = b_base + (unsigned)olist[i] * (4 * kOpBlockBytes);
+        const unsigned ob = b_base + (unsigned)o * (4 * kOpBlockBytes);
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           const unsigned long long bh = smem_desc(ob + (0 * 2 + ks) * kOpBlockBytes, 128, 256);
@@ -329,13 +428,12 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
       }
       if (i > 0) drain(j - 1);
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // the empty trailing groups
     if (nlive > 0) drain(jglob + (unsigned)nlive - 1);
     jglob += (unsigned)nlive;
     if (in) {
-      float4* o = spec_out + (p * n3h + f) * 4;
+      float4* out = spec_out + ((p - p0) * n3h + f) * 4;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) o[c] = make_float4(sum[4 * c], sum[4 * c + 1], sum[4 * c + 2], sum[4 * c + 3]);
+      for (int c = 0; c < 4; ++c) out[c] = make_float4(sum[4 * c], sum[4 * c + 1], sum[4 * c + 2], sum[4 * c + 3]);
     }
   }
   tc_fence_before();
@@ -390,17 +488,33 @@ void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::
 
 void launch_hadamard_tc5(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np) {
   DevTree& T = ctx.tree;
+  // Morton ranks and pattern positions agree on windows of 2048 targets, so a
+  // chunk must consist of whole windows (or run to the end)
+  if (p0 % 2048 != 0 || (p0 + np != T.n_vtrg && np % 2048 != 0))
+    throw std::runtime_error("tcgen05 Hadamard: chunk of target parents not made of whole Morton windows");
+  const long all_tiles = (T.n_vtrg + kTcTile - 1) / kTcTile;
+  if (!T.vtiles_valid) {  // the tiles' source unions, once per tree
+    int* un = T.vunion.as<int>((size_t)all_tiles * kUnionEntries);
+    int* uc = T.vucount.as<int>(all_tiles);
+    unsigned short* lc = T.vlocal.as<unsigned short>((size_t)all_tiles * kTcTile * kLocalStride);
+    ++ctx.n_launch;
+    vlist_tile_unions<<<(unsigned)all_tiles, 512, 0, ctx.stream>>>(T.n_vtrg, T.n_vtrg, T.vtab.get<int>(),
+                                                                   T.vmorton.get<int>(), un, uc, lc);
+    PVFMM_CUDA_CHECK(cudaGetLastError());
+    T.vtiles_valid = true;
+  }
   PVFMM_CUDA_CHECK(
       cudaFuncSetAttribute(hadamard_tc5_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-  const int tiles = 32;  // tiles of 128 target parents per CTA (operators staged once)
-  dim3 grid((unsigned)((np + (long)kTcTile * tiles - 1) / ((long)kTcTile * tiles)), (unsigned)n3h);
+  const int tiles = 32;  // tiles of 128 targets per CTA (operators staged once)
+  const long n_tiles = (np + kTcTile - 1) / kTcTile;
+  dim3 grid((unsigned)((n_tiles + tiles - 1) / tiles), (unsigned)n3h);
   int* err = ctx.tc5_err_buf.as<int>(1);
   if (!ctx.tc5_err) PVFMM_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int), ctx.stream));  // once per evaluation
   ++ctx.n_launch;
   hadamard_tc5_kernel<<<grid, kGroups * kTcThreads, kSmemBytes, ctx.stream>>>(
-      n3h, np, T.n_vtrg, tiles, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
-      reinterpret_cast<const float4*>(sin_), ctx.dops.vop_tc5.get<unsigned char>() + f_base * kOpBytes,
-      reinterpret_cast<float4*>(sout), err);
+      n3h, p0, np, T.n_vtrg, tiles, T.vmorton.get<int>(), T.vmask.get<unsigned>(), T.vunion.get<int>(),
+      T.vucount.get<int>(), T.vlocal.get<unsigned short>(), reinterpret_cast<const float4*>(sin_),
+      ctx.dops.vop_tc5.get<unsigned char>() + f_base * kOpBytes, reinterpret_cast<float4*>(sout), err);
   PVFMM_CUDA_CHECK(cudaGetLastError());
   ctx.tc5_err = err;
 }

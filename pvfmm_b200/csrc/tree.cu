@@ -469,6 +469,17 @@ __global__ void vlist_keys(const int* __restrict__ vtrg, long n_vtrg, const int*
   }
   key[i] = (unsigned long long)(i / kVsortWindow) << 26 | m;
 }
+// Pattern order from the sorted Morton ranks: position p takes the node of
+// rank rank_sorted[p]; vmorton[rank] = p.
+__global__ void vlist_reorder(const int* __restrict__ vtrg_morton, const int* __restrict__ rank_sorted, long n,
+                              int* __restrict__ vtrg_sorted, int* __restrict__ vmorton) {
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int r = rank_sorted[p];
+  vtrg_sorted[p] = vtrg_morton[r];
+  vmorton[r] = (int)p;
+}
+
 __global__ void vlist_patterns(const unsigned long long* __restrict__ key, long n, unsigned* __restrict__ mask) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i < n) mask[i] = (unsigned)(key[i] & ((1u << 26) - 1));
@@ -984,20 +995,33 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       // that the Hadamard kernels can skip the offsets that are empty for all
       // the parents of a tile while a block's parents stay close in space.
       // Every target is computed independently: the order changes no value.
+      // The sort carries each target's Morton rank: vmorton[rank] is the
+      // target's position in the pattern order (ranks and positions stay
+      // within the same window, so windows of Morton order are contiguous
+      // ranges of positions too).
       unsigned long long* key = ctx.t[10].as<unsigned long long>(T.n_vtrg);
       unsigned long long* keys_sorted = ctx.t[13].as<unsigned long long>(T.n_vtrg);
       int* vs = ctx.t[11].as<int>(T.n_vtrg);
+      int* rank_in = ctx.t[12].as<int>(T.n_vtrg);
+      int* rank_sorted = ctx.t[14].as<int>(T.n_vtrg);
       ++ctx.n_launch;
       vlist_keys<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), T.n_vtrg, coll, n2v, key);
+      ++ctx.n_launch;
+      iota_kernel<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(rank_in, T.n_vtrg);
       int end_bit = 27;
       while (end_bit < 64 && ((T.n_vtrg - 1) / kVsortWindow) >> (end_bit - 26)) ++end_bit;
       size_t bytes = 0;
-      cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, keys_sorted, T.vtrg.get<int>(), vs, (int)T.n_vtrg, 0,
+      cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, keys_sorted, rank_in, rank_sorted, (int)T.n_vtrg, 0,
                                       end_bit, s);
       void* tmp = ctx.scratch.ensure(bytes);
-      cub::DeviceRadixSort::SortPairs(tmp, bytes, key, keys_sorted, T.vtrg.get<int>(), vs, (int)T.n_vtrg, 0, end_bit,
+      cub::DeviceRadixSort::SortPairs(tmp, bytes, key, keys_sorted, rank_in, rank_sorted, (int)T.n_vtrg, 0, end_bit,
                                       s);
+      int* vmorton = T.vmorton.as<int>(T.n_vtrg);
+      ++ctx.n_launch;
+      vlist_reorder<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(T.vtrg.get<int>(), rank_sorted, T.n_vtrg, vs,
+                                                                      vmorton);
       PVFMM_CUDA_CHECK(cudaMemcpyAsync(T.vtrg.get<int>(), vs, T.n_vtrg * sizeof(int), cudaMemcpyDeviceToDevice, s));
+      T.vtiles_valid = false;
       ++ctx.n_launch;
       vlist_patterns<<<ceil_div(T.n_vtrg, kThreads), kThreads, 0, s>>>(keys_sorted, T.n_vtrg, vm);
       ++ctx.n_launch;
