@@ -15,8 +15,9 @@
 // 8*ns*ke x ns*ke) stays in L2 across the whole launch; the rows of A are
 // read once per column tile.
 //
-// Tiling: a block computes a 64 x 64 tile of C with 8 warps (2 x 4), each warp
-// a 32 x 16 tile = 4 x 2 MMA tiles of 8 x 8, FP64 accumulators in registers.
+// Tiling: a block computes a 128 x 64 tile of C with 8 warps (4 x 2), each
+// warp a 32 x 32 tile = 4 x 4 MMA tiles of 8 x 8, FP64 accumulators in
+// registers (each A and B fragment feeds four MMAs).
 // K advances in steps of 16; the A and B tiles of the next step are copied
 // into shared memory with 16-byte cp.async while the current step runs.
 // Row lengths are even (ns = 6(m-1)^2+2), so every row of A, B and C starts
@@ -28,10 +29,11 @@
 namespace pvfmm_b200 {
 namespace {
 
-constexpr int kBM = 64, kBN = 64, kBK = 16;
+constexpr int kBM = 128, kBN = 64, kBK = 16;
 constexpr int kAStride = kBK + 4;  // doubles per A row in shared memory
 constexpr int kBStride = kBN + 8;  // doubles per B row in shared memory
 constexpr int kThreadsG = 256;
+constexpr int kSmemG = (int)sizeof(double) * (2 * kBM * kAStride + 2 * kBK * kBStride) + (int)sizeof(long) * kBM;
 
 __device__ __forceinline__ void cp16(void* smem, const void* gmem, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -61,12 +63,13 @@ __global__ void __launch_bounds__(kThreadsG, 2)
                           const double* __restrict__ B, long ldb, double* __restrict__ C, long ldc,
                           const int* __restrict__ crows, const MKey* __restrict__ keys, int deg, int accumulate,
                           long m_base, int kchunk, double* __restrict__ partial) {
-  __shared__ __align__(16) double As[2][kBM * kAStride];
-  __shared__ __align__(16) double Bs[2][kBK * kBStride];
-  __shared__ long arow_s[kBM];
+  extern __shared__ __align__(16) double tsm[];
+  double(*As)[kBM * kAStride] = reinterpret_cast<double(*)[kBM * kAStride]>(tsm);
+  double(*Bs)[kBK * kBStride] = reinterpret_cast<double(*)[kBK * kBStride]>(tsm + 2 * kBM * kAStride);
+  long* arow_s = reinterpret_cast<long*>(tsm + 2 * kBM * kAStride + 2 * kBK * kBStride);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = warp >> 2, wn = warp & 3;  // warp tile (32 rows) x (16 cols)
+  const int wm = warp >> 1, wn = warp & 1;  // warp tile (32 rows) x (32 cols)
   const long m0 = m_base + (long)blockIdx.y * kBM;
   const int n0 = blockIdx.x * kBN;
   const RowMap amap{arows};
@@ -74,11 +77,11 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
   if (tid < kBM) arow_s[tid] = m0 + tid < M ? amap(m0 + tid) : -1;
   __syncthreads();
-  // copy plan: A tile 64 rows x 16 doubles = 512 chunks of 16 B, 2 per thread;
-  // B tile 16 rows x 64 doubles = 512 chunks, 2 per thread
+  // copy plan: A tile 128 rows x 16 doubles = 1024 chunks of 16 B, 4 per
+  // thread; B tile 16 rows x 64 doubles = 512 chunks, 2 per thread
   auto issue = [&](int k0, int buf) {
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < 4; ++u) {
       const int c = tid + u * kThreadsG;
       const int r = c >> 3, kc = (c & 7) * 2;  // row, first double of the chunk
       const long ar = arow_s[r];
@@ -96,11 +99,11 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     }
     cp_commit();
   };
-  double acc[4][2][2];
+  double acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nk = (kend - kbeg + kBK - 1) / kBK;
   issue(kbeg, 0);
   for (int ks = 0; ks < nk; ++ks) {
@@ -113,18 +116,18 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     }
     __syncthreads();
     const double* as = As[buf] + (wm * 32) * kAStride;
-    const double* bs = Bs[buf] + wn * 16;
+    const double* bs = Bs[buf] + wn * 32;
 #pragma unroll
     for (int kk = 0; kk < kBK; kk += 4) {
-      double a[4], b[2];
+      double a[4], b[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i] = as[(i * 8 + g) * kAStride + kk + t];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) b[j] = bs[(kk + t) * kBStride + j * 8 + g];
+      for (int j = 0; j < 4; ++j) b[j] = bs[(kk + t) * kBStride + j * 8 + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) dmma(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
     }
     __syncthreads();  // buffer buf is refilled by the next step's issue
   }
@@ -136,8 +139,8 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     if (partial) {  // split K: plain partial sums, reduced by translate_reduce
       double* prow = partial + ((long)blockIdx.z * M + mi) * N;
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int n = n0 + wn * 16 + j * 8 + 2 * t;
+      for (int j = 0; j < 4; ++j) {
+        const int n = n0 + wn * 32 + j * 8 + 2 * t;
         if (n < N) *reinterpret_cast<double2*>(prow + n) = make_double2(acc[i][j][0], acc[i][j][1]);
       }
       continue;
@@ -147,8 +150,8 @@ __global__ void __launch_bounds__(kThreadsG, 2)
     const long cr = crows ? (long)crows[mi] : mi;
     double* crow = C + cr * ldc;
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int n = n0 + wn * 16 + j * 8 + 2 * t;
+    for (int j = 0; j < 4; ++j) {
+      const int n = n0 + wn * 32 + j * 8 + 2 * t;
       if (n >= N) continue;  // N is even: n < N implies n + 1 < N
       double2 v = make_double2(acc[i][j][0] * s, acc[i][j][1] * s);
       double2* p = reinterpret_cast<double2*>(crow + n);
@@ -189,12 +192,13 @@ void translate_gemm(cudaStream_t s, long M, int N, int K, const double* A, long 
   if ((N & 1) || (K & 1) || (lda & 1) || (ldb & 1) || (ldc & 1))
     throw std::runtime_error("translate_gemm: row lengths must be even (16-byte rows)");
   if (M >= (1L << 31)) throw std::runtime_error("translate_gemm: too many rows");
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(translate_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemG));
   // the column tiles of one row tile are consecutive blocks (they share the
   // A rows in L2); row tiles in launches of at most 65535
   const long tiles = (M + kBM - 1) / kBM;
   for (long t0 = 0; t0 < tiles; t0 += 65535) {
     dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)std::min(65535L, tiles - t0), (unsigned)ksplit);
-    translate_gemm_kernel<<<grid, kThreadsG, 0, s>>>((int)M, N, K, A, lda, arows, B, ldb, C, ldc, crows, scale_keys,
+    translate_gemm_kernel<<<grid, kThreadsG, kSmemG, s>>>((int)M, N, K, A, lda, arows, B, ldb, C, ldc, crows, scale_keys,
                                                       deg, accumulate ? 1 : 0, t0 * kBM, K / ksplit,
                                                       ksplit > 1 ? partial : nullptr);
     PVFMM_CUDA_CHECK(cudaGetLastError());
