@@ -347,13 +347,13 @@ def cpu_baseline(args):
 # a launch processes (traffic grows in proportion).  Units: n_vsrc + n_vtrg for
 # the Hadamard kernels, n_trg for the near field.
 TRAFFIC_1M = {
-    ("hadamard", 4): {"bytes": 877601280 + 672896000, "units": 4768 + 4767},     # hadamard_tc5_kernel
+    ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
     ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
     ("near_field", 4): {"bytes": 149441536 + 24975104, "units": 1000000},        # near_field_kernel<float>
     ("near_field", 8): {"bytes": 151890688 + 20192256, "units": 1000000},        # near_field_kernel<double>
 }
 # kernel that computes the V-list Hadamard products: (real bytes, ke) -> name
-HADAMARD_KERNEL = {(4, 1): "hadamard_tc5_kernel (V-list M2L, tcgen05 kind::tf32 3-term split, TMEM accumulators)",
+HADAMARD_KERNEL = {(4, 1): "hadamard_tc_kernel (V-list M2L, TF32 mma.sync x3 split)",
                    (8, 1): "hadamard_rd_kernel<double> (V-list M2L)",
                    (4, 3): "hadamard_kernel<float, 3, 3> (V-list M2L)",
                    (8, 3): "hadamard_kernel<double, 3, 3> (V-list M2L)"}
@@ -406,7 +406,7 @@ def roofline(B, peaks):
            "frac": had_gbs / hbm_peak, "peak_source": peak_src,
            "traffic": traffic("hadamard", st["n_vsrc"] + st["n_vtrg"]), "algorithmic_bytes": had_bytes,
            "kernel_ms": had_ms,
-           "compute": ({"pipe": "tensor tf32 x3 (tcgen05)", "achieved_tflops": 3 * had_tf, "peak_tflops": tf32_peak,
+           "compute": ({"pipe": "tensor tf32 x3 (mma.sync)", "achieved_tflops": 3 * had_tf, "peak_tflops": tf32_peak,
                         "peak_source": "half the measured bf16 dense peak", "frac": 3 * had_tf / tf32_peak,
                         "algorithmic_flops": had_flops} if tensor else
                        {"pipe": "fp32 simt" if rb == 4 else "fp64 simt", "achieved_tflops": had_tf,

@@ -1501,17 +1501,14 @@ int grids_per_block(size_t per_grid, size_t fixed, int ngrid, size_t budget) {
 // output spectra of one chunk at a time; one chunk when device memory
 // allows).  With several chunks, stage 4 ends after the first chunk's
 // products and stage 5 covers the rest.
-// Kernel of the mixed form's scalar Hadamard: PVFMM_B200_HADAMARD = "mma"
-// (warp-level MMAs gathering from L2), "tcu" (warp-level MMAs fed from the
-// tiles' staged source unions) or "tcgen05" (tcgen05 with TMEM accumulators).
-enum HadamardKind { kHadMma = 0, kHadTcu = 1, kHadTc5 = 2 };
-HadamardKind hadamard_kind() {
+// Kernel of the mixed form's scalar Hadamard: the warp-level MMA kernel
+// gathering from L2 (hadamard_tc_kernel), or with PVFMM_B200_HADAMARD=tcgen05
+// the tcgen05 kernel with TMEM accumulators over tiles of Morton-consecutive
+// targets (hadamard_tc.cu).
+bool use_tc5(const Context&) {
   const char* e = std::getenv("PVFMM_B200_HADAMARD");
-  if (e && std::strcmp(e, "tcgen05") == 0) return kHadTc5;
-  if (e && std::strcmp(e, "tcu") == 0) return kHadTcu;
-  return kHadMma;
+  return e && std::strcmp(e, "tcgen05") == 0;
 }
-bool use_tc5(const Context&) { return hadamard_kind() != kHadMma; }  // tile-based kernels
 
 template <class Real, int M>
 void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
@@ -1542,8 +1539,7 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
       const long np = std::min(chunk, T.n_vtrg - p0);
       if (kin == 1 && kout == 1) {
         if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
-        else if (hadamard_kind() == kHadTc5) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
-        else if (hadamard_kind() == kHadTcu) launch_hadamard_tcu(ctx, n3h, f_base, sin_, sout, p0, np);
+        else if (use_tc5(ctx)) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
         else launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
       } else if (kout == 3) {  // Stokes velocity, Biot-Savart
         launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
@@ -1601,8 +1597,8 @@ void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const 
     const long c = std::atol(e);
     if (c > 0) chunk = std::min(chunk, c);
   }
-  // the tile-based Hadamard kernels walk tiles of Morton-consecutive targets,
-  // which stay inside windows of 2048 positions: their chunks are whole windows
+  // the tcgen05 Hadamard walks tiles of Morton-consecutive targets, which stay
+  // inside windows of 2048 positions: its chunks are whole windows
   if (sizeof(Real) == 4 && kin == 1 && kout == 1 && use_tc5(ctx) && chunk < T.n_vtrg)
     chunk = std::max(2048L, chunk / 2048 * 2048);
   Cplx<Real>* sout = ctx.spec_out.as<Cplx<Real>>((size_t)std::min(chunk, T.n_vtrg) * n3h * 8 * kout);

@@ -117,8 +117,6 @@ void upload_operators(Context& ctx);
 // on tcgen05 (rows of sout relative to p0) over n3h frequencies starting at
 // frequency f_base of the operators, and its operator layout
 void launch_hadamard_tc5(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np);
-// the same products with warp-level MMAs fed from the tiles' staged source unions
-void launch_hadamard_tcu(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np);
 void hadamard_tc5_operator_layout(const std::vector<double>& vop, int n3h, std::vector<float>& out);
 // translate.cu: C[crow(i)] (+)= 2^(-deg depth(key[arow(i)])) A[arow(i)] B on the FP64
 // tensor cores (rows gathered / scattered through the index lists when given);

@@ -446,160 +446,6 @@ __global__ void __launch_bounds__(kGroups * kTcThreads, 1)
   }
 }
 
-// ---------------------------------------------------------------------------
-// The same products with warp-level MMAs (mma.sync m16n8k8 TF32, 3-term
-// split) fed from the staged unions: a block (8 warps, 16 targets each) walks
-// tiles of 128 Morton-consecutive targets at one frequency; per tile it stages
-// the tile's source-union rows (at most kUnionCap, the rest read from L2) and
-// local-index table in shared memory, so that every A fragment comes from
-// shared memory instead of an L2 gather.  Lane (g, t) takes the 16-byte piece
-// t (children 2t and 2t+1, re and im) of rows g and g+8, the fragment order of
-// hadamard_tc_kernel; the B fragments of the frequency (the layout of
-// hadamard_tc_kernel's operator fragments) stay staged over the block's tiles.
-// Each offset's products go to a fresh fragment and join the running sum with
-// rounded FP32 adds (the tensor cores' own accumulation over all offsets
-// biased the far-field potential).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void mma16x8x8(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
-}
-
-constexpr int kTcuWarps = 8;
-constexpr int kTcuThreads = 32 * kTcuWarps;
-constexpr int kFragBytes = 26 * 4 * 32 * 16;  // a frequency's B fragments: [offset][block][lane] float4
-constexpr size_t kTcuSmem = (size_t)kFragBytes + kUnionBytes + kLocalBytes + 64;
-
-__global__ void __launch_bounds__(kTcuThreads, 2)
-    hadamard_tcu_kernel(int n3h, long p0, long np, int tiles_per_block, const int* __restrict__ vmorton,
-                        const unsigned* __restrict__ vmask, const int* __restrict__ vunion,
-                        const int* __restrict__ vucount, const unsigned short* __restrict__ vlocal,
-                        const float4* __restrict__ spec_in, const float4* __restrict__ bfrag,
-                        float2* __restrict__ spec_out) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const float4* Bs = reinterpret_cast<const float4*>(smem);  // [26][4][32]
-  const unsigned bs_base = smem_u32(smem);
-  const unsigned union_base = bs_base + kFragBytes;
-  const unsigned local_base = union_base + kUnionBytes;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int f = blockIdx.y;
-  // the frequency's operator fragments
-  for (int i = tid; i < kFragBytes / 16; i += kTcuThreads)
-    cp16(bs_base + 16u * (unsigned)i, bfrag + (long)f * (kFragBytes / 16) + i, true);
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  const long n_tiles = (np + kTcTile - 1) / kTcTile;
-  for (int tl = 0; tl < tiles_per_block; ++tl) {
-    const long tile = (long)blockIdx.x * tiles_per_block + tl;
-    if (tile >= n_tiles) break;  // uniform across the block
-    const long tg = p0 / kTcTile + tile;
-    __syncthreads();  // every warp is done with the previous tile's rows
-    const int nu = __ldg(vucount + tg);
-    const int nst = min(nu, kUnionCap);
-    const int* un = vunion + tg * kUnionEntries;
-    for (int u = tid; u < nst; u += kTcuThreads) {
-      const float4* src = spec_in + ((long)__ldg(un + u) * n3h + f) * 4;
-      const unsigned dst = union_base + (unsigned)(u * kRowBytes);
-      const int sw = (u >> 1) & 3;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) cp16(dst + 16u * (unsigned)(c ^ sw), src + c, true);
-    }
-    {
-      const unsigned char* lsrc = reinterpret_cast<const unsigned char*>(vlocal + tg * kTcTile * kLocalStride);
-#pragma unroll
-      for (int c = 0; c < kLocalBytes / 16 / kTcuThreads; ++c) {
-        const int chunk = tid + c * kTcuThreads;
-        cp16(local_base + 16u * (unsigned)chunk, lsrc + 16 * chunk, true);
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    // this warp's 16 targets: rows 16 warp + g (+ 8) of the tile
-    const long kbase = p0 + tile * kTcTile + 16 * warp;
-    unsigned mine = 0;
-    if (lane < 16 && kbase + lane < p0 + np) mine = __ldg(vmask + __ldg(vmorton + kbase + lane));
-    unsigned live = __reduce_or_sync(0xffffffffu, mine);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-    float acc[2][4];
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) acc[nt][i] = 0.f;
-    // piece t of row r (of the tile) for offset o: from the staged union, from
-    // L2 past the staged rows, zeros without a source
-    auto piece = [&](int r, int o) {
-      unsigned short u;
-      asm volatile("ld.shared.u16 %0, [%1];\n" : "=h"(u) : "r"(local_base + 2u * (unsigned)(r * kLocalStride + o)));
-      float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (u != kNoSource) {
-        if (u < kUnionCap) {
-          const unsigned a = union_base + (unsigned)(u * kRowBytes) + 16u * (unsigned)(t ^ ((u >> 1) & 3));
-          asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n" : "=f"(w.x), "=f"(w.y), "=f"(w.z), "=f"(w.w) : "r"(a));
-        } else {
-          w = __ldg(spec_in + ((long)__ldg(un + u) * n3h + f) * 4 + t);
-        }
-      }
-      return w;
-    };
-    const int r0 = 16 * warp + g, r1 = r0 + 8;
-    while (live) {
-      const int o = __ffs(live) - 1;
-      live &= live - 1;
-      const float4 x0 = piece(r0, o), x1 = piece(r1, o);
-      unsigned ah[2][4], al[2][4];
-      split_tf32(x0.x, ah[0][0], al[0][0]);
-      split_tf32(x1.x, ah[0][1], al[0][1]);
-      split_tf32(x0.y, ah[0][2], al[0][2]);
-      split_tf32(x1.y, ah[0][3], al[0][3]);
-      split_tf32(x0.z, ah[1][0], al[1][0]);
-      split_tf32(x1.z, ah[1][1], al[1][1]);
-      split_tf32(x0.w, ah[1][2], al[1][2]);
-      split_tf32(x1.w, ah[1][3], al[1][3]);
-      float4 bq[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) bq[i] = Bs[(o * 4 + i) * 32 + lane];
-      float d[2][4];
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) d[nt][i] = 0.f;
-#pragma unroll
-      for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-          const float4 b = bq[s * 2 + nt];
-          const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
-          const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
-          mma16x8x8(d[nt], al[s], bh0, bh1);
-          mma16x8x8(d[nt], ah[s], bl0, bl1);
-          mma16x8x8(d[nt], ah[s], bh0, bh1);
-        }
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) acc[nt][i] = __fadd_rn(acc[nt][i], d[nt][i]);
-    }
-    // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); column
-    // n = nt*8 + 2t (+1) is child j1 = 4nt + t, re (im)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long k = kbase + g + 8 * h;
-      if (k >= p0 + np) continue;
-      const long p = __ldg(vmorton + k);
-      float2* out = spec_out + ((p - p0) * n3h + f) * 8;
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) out[4 * nt + t] = make_float2(acc[nt][2 * h], acc[nt][2 * h + 1]);
-    }
-  }
-}
-
 }  // namespace
 
 // Operator blocks in the layout hadamard_tc5_kernel stages: per frequency f
@@ -660,23 +506,6 @@ void ensure_tile_unions(Context& ctx) {
 void check_window_chunk(const Context& ctx, long p0, long np) {
   if (p0 % 2048 != 0 || (p0 + np != ctx.tree.n_vtrg && np % 2048 != 0))
     throw std::runtime_error("V-list Hadamard: chunk of target parents not made of whole Morton windows");
-}
-
-void launch_hadamard_tcu(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np) {
-  DevTree& T = ctx.tree;
-  check_window_chunk(ctx, p0, np);
-  ensure_tile_unions(ctx);
-  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tcu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kTcuSmem));
-  const int tiles = 4;  // tiles of 128 targets per block (operator fragments staged once)
-  const long n_tiles = (np + kTcTile - 1) / kTcTile;
-  dim3 grid((unsigned)((n_tiles + tiles - 1) / tiles), (unsigned)n3h);
-  ++ctx.n_launch;
-  hadamard_tcu_kernel<<<grid, kTcuThreads, kTcuSmem, ctx.stream>>>(
-      n3h, p0, np, tiles, T.vmorton.get<int>(), T.vmask.get<unsigned>(), T.vunion.get<int>(), T.vucount.get<int>(),
-      T.vlocal.get<unsigned short>(), reinterpret_cast<const float4*>(sin_),
-      ctx.dops.vop_frag.get<float4>() + f_base * 26 * 4 * 32, reinterpret_cast<float2*>(sout));
-  PVFMM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_hadamard_tc5(Context& ctx, int n3h, long f_base, const void* sin_, void* sout, long p0, long np) {

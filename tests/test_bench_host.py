@@ -24,7 +24,7 @@ def test_roofline_objects_follow_the_contract(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     assert dom["kernel_ms"] >= nxt["kernel_ms"]
     by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
-    had = by["hadamard_tc5_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
     near = by["near_field_kernel"]
     # the Hadamard: HBM view against the measured copy bandwidth
     assert had["bound"] == "hbm" and had["unit"] == "GB/s" and had["peak"] == 6449.1
@@ -44,7 +44,7 @@ def test_roofline_objects_follow_the_contract(rb):
 def test_traffic_at_the_capture_size_is_the_capture(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
-    had = by["hadamard_tc5_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
     assert had["traffic"] == bench.TRAFFIC_1M[("hadamard", rb)]["bytes"]
     assert by["near_field_kernel"]["traffic"] == bench.TRAFFIC_1M[("near_field", rb)]["bytes"]
 
@@ -53,7 +53,7 @@ def test_traffic_scales_with_the_units_of_a_launch():
     st = dict(STATS_1M, n_vsrc=2 * 4768.0, n_vtrg=2 * 4767.0, n_trg=4e6)
     dom, nxt = _run(4, 10.0, 12.0, stats=st)
     by = {r["kernel"].split()[0]: r for r in (dom, nxt)}
-    assert by["hadamard_tc5_kernel"]["traffic"] == pytest.approx(2 * bench.TRAFFIC_1M[("hadamard", 4)]["bytes"])
+    assert by["hadamard_tc_kernel"]["traffic"] == pytest.approx(2 * bench.TRAFFIC_1M[("hadamard", 4)]["bytes"])
     assert by["near_field_kernel"]["traffic"] == pytest.approx(4 * bench.TRAFFIC_1M[("near_field", 4)]["bytes"])
 
 

@@ -340,17 +340,16 @@ def test_tree_build_writes_stay_in_bounds_on_a_count_mismatch():
         assert f(n, cap) == 0, P.last_error()
 
 
-@pytest.mark.parametrize("kind", ["tcgen05", "tcu"])
-def test_tile_hadamards_agree_with_mma_sync_hadamard(monkeypatch, kind):
-    """The mixed form's V-list products of the tile-based kernels (tcgen05 with
-    TMEM accumulators; warp-level MMAs fed from the tiles' staged source
-    unions) and of the warp-level MMA kernel gathering from L2 give the same
-    FMM result to well within the mixed form's accuracy (all carry each
-    product to ~2^-22 with a 3-term TF32 split; only the accumulation order
-    inside the tensor cores differs)."""
+def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
+    """The mixed form's V-list products on the 5th-generation tensor cores
+    (tcgen05, TMEM accumulators, tiles of Morton-consecutive targets with their
+    source unions staged in shared memory) and on the warp-level MMA path give
+    the same FMM result to well within the mixed form's accuracy (both carry
+    each product to ~2^-22 with a 3-term TF32 split; only the accumulation
+    order inside the tensor cores differs)."""
     src = points("gauss", 40000, 41)
     den = np.random.default_rng(42).uniform(-1, 1, 40000)
-    monkeypatch.setenv("PVFMM_B200_HADAMARD", kind)
+    monkeypatch.setenv("PVFMM_B200_HADAMARD", "tcgen05")
     a, ctx = gpu_eval(6, 8, 128, src, den, src, prec=P.PRECISION_MIXED)
     assert ctx.tree_stats()["n_vtrg"] > 200
     ctx.close()
