@@ -31,10 +31,9 @@
 extern "C" {
 #endif
 
-/* Kernel functions; values 0-5 as in the reference (include/pvfmm.h:21-28).
- * Implemented: LaplacePotential, LaplaceGradient, StokesVelocity, and the
- * extension LaplacePotGrad (potential and -grad in one pass, 4 outputs).
- * The other reference values are rejected with an error. */
+/* Kernel functions; values 0-5 as in the reference (include/pvfmm.h:21-28),
+ * all implemented, plus the extension LaplacePotGrad (potential and -grad in
+ * one pass, 4 outputs). */
 enum PVFMMKernel {
   PVFMMLaplacePotential    = 0,
   PVFMMLaplaceGradient     = 1,
@@ -64,8 +63,21 @@ void* PVFMMCreateContextFWorld(float box_size, int n, int m, enum PVFMMKernel ke
 
 /* Replaces PVFMMEvalD/F (reference include/pvfmm.h:290-291,
  * src/pvfmm-wrapper.cpp:445-811).  Host pointers.  setup=1 rebuilds the tree
- * for new positions; setup=0 reuses it (same positions, new densities).
- * dl_den must be NULL (double-layer sources are not implemented). */
+ * for new positions; setup=0 reuses it (same positions, new densities, the
+ * same of sl_den / dl_den passed as at setup).
+ *
+ * sl_den: single-layer densities (k0 per source) or NULL.
+ * dl_den: double-layer values (k0 + 3 per source) or NULL; only the
+ * LaplacePotential and StokesVelocity kernels have double-layer kernels (any
+ * other kernel with dl_den is an error).  The values are used as the
+ * reference uses them: the first k0 are scaled like densities (times scale_x
+ * of the bounding-box map), the last three are not, and the kernels read
+ * them in the reference's order -- Laplace (kernel.txx:1299-1311) takes
+ * values 0-2 as the normal and value 3 as the density; Stokes
+ * (kernel.txx:1437-1456) takes values 0-2 as the density f and 3-5 as the
+ * normal n, with n.f formed as v0 v3 + v1 v1 + v2 v2.  Passing both
+ * densities counts every source twice in the leaf-size rule, as the
+ * reference does (fmm_node.txx:81-92). */
 void PVFMMEvalD(const double* src_pos, const double* sl_den, const double* dl_den, long n_src,
                 const double* trg_pos, double* trg_val, long n_trg, const void* ctx, int setup);
 void PVFMMEvalF(const float* src_pos, const float* sl_den, const float* dl_den, long n_src,
@@ -119,6 +131,13 @@ int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_de
                      const double* trg_pos, double* trg_val, long n_trg, int setup, void* stream);
 int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den, long n_src,
                      const float* trg_pos, float* trg_val, long n_trg, int setup, void* stream);
+
+/* PVFMMEvalDeviceD/F with double-layer values as well (dl_den as in
+ * PVFMMEvalD; either density may be NULL). */
+int PVFMMEvalLayersDeviceD(const void* ctx, const double* src_pos, const double* sl_den, const double* dl_den,
+                           long n_src, const double* trg_pos, double* trg_val, long n_trg, int setup, void* stream);
+int PVFMMEvalLayersDeviceF(const void* ctx, const float* src_pos, const float* sl_den, const float* dl_den,
+                           long n_src, const float* trg_pos, float* trg_val, long n_trg, int setup, void* stream);
 
 /* Evaluation with the roles of sources and targets exchanged (for adjoints and
  * gradients; no counterpart in the reference):

@@ -137,6 +137,48 @@ class KernelFn:
         return (den @ self.matrix(src, trg)).reshape(-1, self.k1)
 
 
+@dataclass(frozen=True)
+class DblKernelFn:
+    """A double-layer kernel: each source carries k0 + 3 values (a density and
+    a normal), and the kernel is bilinear in them, so it has no matrix form.
+    ``eval`` follows the reference's uKerEval for the kernel literally,
+    including which source value it reads as which quantity."""
+    name: str
+    k0: int             # values per source point (k0 of the kernel + 3)
+    k1: int
+    flops: int
+
+    def eval(self, src: np.ndarray, val: np.ndarray, trg: np.ndarray, chunk: int = 256) -> np.ndarray:
+        src = np.asarray(src, dtype=np.float64).reshape(-1, 3)
+        trg = np.asarray(trg, dtype=np.float64).reshape(-1, 3)
+        val = np.asarray(val, dtype=np.float64).reshape(-1, self.k0)
+        out = np.zeros((trg.shape[0], self.k1))
+        if src.shape[0] == 0 or trg.shape[0] == 0:
+            return out
+        for a in range(0, trg.shape[0], chunk):
+            r = trg[a:a + chunk, None, :] - src[None, :, :]            # (nt, ns, 3)
+            r2 = np.einsum("ijk,ijk->ij", r, r)
+            with np.errstate(divide="ignore"):
+                rinv = np.where(r2 > 0, 1.0 / np.sqrt(np.where(r2 > 0, r2, 1.0)), 0.0)
+            rinv3 = rinv ** 3
+            if self.name == "laplace_dbl":
+                # kernel.txx:1299-1311: u += (r . f[0:3]) f[3] / r^3, scale 1/(4 pi)
+                rdn = np.einsum("ijk,jk->ij", r, val[:, 0:3])
+                out[a:a + chunk, 0] = (rdn * rinv3) @ val[:, 3] / (4 * math.pi)
+            elif self.name == "stokes_sym_dip":
+                # kernel.txx:1437-1456: f = v[0:3], n = v[3:6],
+                # n_dot_f = v0 v3 + v1 v1 + v2 v2 (as the reference computes it),
+                # u_k += r_k (n_dot_f - 3 (r.n)(r.f) / r^2) / r^3, scale -1/(8 pi)
+                rdf = np.einsum("ijk,jk->ij", r, val[:, 0:3])
+                rdn = np.einsum("ijk,jk->ij", r, val[:, 3:6])
+                ndf = val[:, 0] * val[:, 3] + val[:, 1] * val[:, 1] + val[:, 2] * val[:, 2]
+                common = (ndf[None, :] - 3.0 * rdn * rdf * rinv * rinv) * rinv3
+                out[a:a + chunk] = np.einsum("ijk,ij->ik", r, common) * (-1.0 / (8 * math.pi))
+            else:
+                raise ValueError(self.name)
+        return out
+
+
 LAPLACE = KernelFn("laplace", 1, 1, 9)
 LAPLACE_GRAD = KernelFn("laplace_grad", 1, 3, 16)
 LAPLACE_PG = KernelFn("laplace_potgrad", 1, 4, 18)
@@ -144,6 +186,8 @@ STOKES = KernelFn("stokes_vel", 3, 3, 29)
 STOKES_PRESS = KernelFn("stokes_press", 3, 1, 16, deg=2.0)
 STOKES_GRAD = KernelFn("stokes_grad", 3, 9, 94, deg=2.0)
 BIOT_SAVART = KernelFn("biot_savart", 3, 3, 24, deg=2.0)
+LAPLACE_DBL = DblKernelFn("laplace_dbl", 4, 1, 17)
+STOKES_DBL = DblKernelFn("stokes_sym_dip", 6, 3, 35)
 
 
 @dataclass(frozen=True)
@@ -152,6 +196,10 @@ class Kernel:
 
     ``src_scal``/``trg_scal`` are the scale exponents detected by
     Kernel::Initialize (include/kernel.txx:64-196): K(x/2) = 2^(s_i+t_j) K(x).
+    ``dbl`` holds the double-layer kernels of the source->check sub-kernels
+    (s2m, s2l) and of the source->target one (s2t); None where the reference's
+    sub-kernel has none (its EvalListPts asserts one is there,
+    fmm_pts.txx:4362).
     """
     name: str
     k0: int
@@ -160,15 +208,19 @@ class Kernel:
     exp: KernelFn          # s2m, s2l, m2m, m2l, l2l
     src_scal: tuple
     trg_scal: tuple
+    dbl: tuple = (None, None)
 
 
 KERNELS = {
     # LaplaceKernel<T>::potential(), include/kernel.txx:1333-1338
-    LAPLACE_POTENTIAL: Kernel("laplace", 1, 1, LAPLACE, LAPLACE, (0.0,), (1.0,)),
+    LAPLACE_POTENTIAL: Kernel("laplace", 1, 1, LAPLACE, LAPLACE, (0.0,), (1.0,), (LAPLACE_DBL, LAPLACE_DBL)),
     # LaplaceKernel<T>::gradient(), include/kernel.txx:1339-1344
-    LAPLACE_GRADIENT: Kernel("laplace_grad", 1, 3, LAPLACE_GRAD, LAPLACE, (0.0,), (2.0, 2.0, 2.0)),
+    # (its s2m/s2l sub-kernels are the potential kernel, with a double layer;
+    # its s2t kernel has none)
+    LAPLACE_GRADIENT: Kernel("laplace_grad", 1, 3, LAPLACE_GRAD, LAPLACE, (0.0,), (2.0, 2.0, 2.0), (LAPLACE_DBL, None)),
     # StokesKernel<T>::velocity(), include/kernel.txx:1475-1479
-    STOKES_VELOCITY: Kernel("stokes_vel", 3, 3, STOKES, STOKES, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0)),
+    STOKES_VELOCITY: Kernel("stokes_vel", 3, 3, STOKES, STOKES, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0),
+                            (STOKES_DBL, STOKES_DBL)),
     # extension: potential + gradient in one pass (expansions use the potential)
     LAPLACE_POTGRAD: Kernel("laplace_potgrad", 1, 4, LAPLACE_PG, LAPLACE, (0.0,), (1.0, 2.0, 2.0, 2.0)),
     # StokesKernel<T>::pressure() / vel_grad(), BiotSavartKernel<T>::potential()
@@ -337,13 +389,18 @@ class Tree:
     """Single-rank particle octree with PVFMM's refinement and balance."""
 
     def __init__(self, src_keys, trg_keys, grid_keys, max_pts, max_depth=MAX_DEPTH,
-                 src_counted=True):
+                 src_counted=True, src_weight=None):
+        """``src_weight``: how many point sets the source positions stand for
+        (the single-layer src_coord and the double-layer surf_coord each count
+        in SubdivCond and pt_cnt[0], fmm_node.txx:81-92, fmm_pts.txx:1332-1333);
+        0 when the call passes neither density."""
         self.max_pts = max_pts
         self.max_depth = max_depth
         self.src_keys = src_keys
         self.trg_keys = trg_keys
         self.grid_keys = grid_keys
-        self.src_counted = src_counted
+        self.src_weight = (1 if src_counted else 0) if src_weight is None else int(src_weight)
+        self.src_counted = self.src_weight > 0
         refined = self._refine()
         self.internal = self._balance(refined)
         self._build_nodes()
@@ -364,7 +421,7 @@ class Tree:
             return True
         s = self._range(self.src_keys, X, Y, Z, d) if self.src_counted else (0, 0)
         t = self._range(self.trg_keys, X, Y, Z, d)
-        return (s[1] - s[0]) + (t[1] - t[0]) > self.max_pts
+        return self.src_weight * (s[1] - s[0]) + (t[1] - t[0]) > self.max_pts
 
     def _refine(self):
         """RefineTree (mpi_tree.txx:403-492): the coarsest tree in which no
@@ -550,7 +607,7 @@ def build_lists(tree: Tree, nsrf: int):
             S = N[s]
             if S.n_src == 0:
                 continue
-            if S.leaf and S.n_src <= nsrf:
+            if S.leaf and S.n_src * tree.src_weight <= nsrf:     # pt_cnt[0] counts both layers
                 P.append(s)
             else:
                 Wk.append(s)
@@ -747,7 +804,7 @@ class FMM:
 
     # ------------------------------------------------------------------
     def setup(self, src_c: np.ndarray, trg_c: np.ndarray, real=np.float64, src_counted=True,
-              pt_coord="seed"):
+              pt_coord="seed", src_weight=None):
         """Tree for unit-box coordinates (pvfmm-wrapper.cpp:543-775).  The
         tree's point set is the context's seed grid (pt_coord="seed",
         pvfmm-wrapper.cpp:416-432) or the targets (pt_coord="trg", the C++
@@ -758,7 +815,8 @@ class FMM:
             _, grid_keys = sorted_keys(seed_grid_coords(self.max_pts, real))
         else:
             grid_keys = trg_keys
-        self.tree = Tree(src_keys, trg_keys, grid_keys, self.max_pts, src_counted=src_counted)
+        self.tree = Tree(src_keys, trg_keys, grid_keys, self.max_pts, src_counted=src_counted,
+                         src_weight=src_weight)
         self.src = np.asarray(src_c, dtype=np.float64)[self.src_perm]
         self.trg = np.asarray(trg_c, dtype=np.float64)[self.trg_perm]
         self.lists = build_lists(self.tree, self.ns)
@@ -766,11 +824,17 @@ class FMM:
     def _corner(self, n: Node):
         return np.array([n.X, n.Y, n.Z], dtype=np.float64) / TWO30
 
-    def evaluate(self, den_sorted: np.ndarray) -> np.ndarray:
-        """RunFMM (fmm_tree.txx:237-264) on sorted densities; returns the
-        sorted target values (n_trg, k1)."""
+    def evaluate(self, den_sorted: np.ndarray | None, surf_sorted: np.ndarray | None = None) -> np.ndarray:
+        """RunFMM (fmm_tree.txx:237-264) on sorted single-layer densities
+        and/or sorted double-layer values (k0 + 3 per point); returns the
+        sorted target values (n_trg, k1).  The double layer enters where the
+        sources' points do: S2U, X-list and U-list (EvalListPts calls the
+        sub-kernel's dbl_layer_poten on surf_value, fmm_pts.txx:4346-4366)."""
         K = self.kernel
         ke, kt = K.exp, K.s2t
+        kd_exp, kd_s2t = K.dbl
+        if surf_sorted is not None and (kd_exp is None or kd_s2t is None):
+            raise ValueError(f"kernel {K.name} has no double-layer kernel")
         ops, m, ns = self.ops, self.m, self.ns
         tree = self.tree
         N = tree.nodes
@@ -779,8 +843,20 @@ class FMM:
         # component, so a check->equivalent operator at level l is 2^(-deg l)
         # times the level-0 one (fmm_pts.txx:2447-2465).
         e_exp = ke.deg - EXP_SRC_SCAL
-        den = np.asarray(den_sorted, dtype=np.float64).reshape(-1, K.k0)
+        den = None if den_sorted is None else np.asarray(den_sorted, dtype=np.float64).reshape(-1, K.k0)
+        surf = None if surf_sorted is None else np.asarray(surf_sorted, dtype=np.float64).reshape(-1, K.k0 + 3)
         nn = len(N)
+
+        def from_points(kfn, kdbl, lo, hi, T, pts):
+            """Potentials at `pts` (relative to T's corner) of the source points
+            [lo, hi): single layer plus double layer."""
+            r = np.zeros((len(pts), kfn.k1))
+            if den is not None:
+                r += kfn.eval(self.src[lo:hi] - self._corner(T), den[lo:hi], pts)
+            if surf is not None:
+                r += kdbl.eval(self.src[lo:hi] - self._corner(T), surf[lo:hi], pts)
+            return r
+
         ue = np.zeros((nn, ns * k0))
         dc = np.zeros((nn, ns * k1e))
         out = np.zeros((len(self.trg), K.k1))
@@ -810,8 +886,7 @@ class FMM:
         z3 = np.zeros(3)
         for i, n in enumerate(N):
             if n.leaf and n.n_src > 0:
-                chk = ke.eval(pts_rel(self.src, n.src[0], n.src[1], n), den[n.src[0]:n.src[1]],
-                              u_check_surf(m, z3, n.depth))
+                chk = from_points(ke, kd_exp, n.src[0], n.src[1], n, u_check_surf(m, z3, n.depth))
                 ue[i] = ((chk.reshape(-1) * 2.0 ** (-e_exp * n.depth)) @ ops.uc2ue0) @ ops.uc2ue1
         tick("S2U")
         # --- U2U bottom-up (fmm_pts.txx:2602-2630, EvalList) ------------
@@ -832,7 +907,7 @@ class FMM:
             pts = d_check_surf(m, z3, T.depth)
             for s in srcs:
                 S = N[s]
-                dc[t] += ke.eval(pts_rel(self.src, S.src[0], S.src[1], T), den[S.src[0]:S.src[1]], pts).reshape(-1)
+                dc[t] += from_points(ke, kd_exp, S.src[0], S.src[1], T, pts).reshape(-1)
         tick("X-List")
         # --- W-list (fmm_pts.txx:4746-5022) ------------------------------
         for t, srcs in wl.items():
@@ -847,8 +922,11 @@ class FMM:
             if not srcs:
                 continue
             idx = np.concatenate([np.arange(N[s].src[0], N[s].src[1]) for s in srcs])
-            out[T.trg[0]:T.trg[1]] += kt.eval(self.src[idx] - self._corner(T), den[idx],
-                                              pts_rel(self.trg, T.trg[0], T.trg[1], T))
+            tp = pts_rel(self.trg, T.trg[0], T.trg[1], T)
+            if den is not None:
+                out[T.trg[0]:T.trg[1]] += kt.eval(self.src[idx] - self._corner(T), den[idx], tp)
+            if surf is not None:
+                out[T.trg[0]:T.trg[1]] += kd_s2t.eval(self.src[idx] - self._corner(T), surf[idx], tp)
         tick("D2T+W+U")
         # --- V-list via FFT (fmm_pts.txx:3597-3759, 2689-2858) ----------
         self._vlist(ue, dc, v1)
@@ -918,12 +996,24 @@ class FMM:
 # ----------------------------------------------------------------------------
 # C-ABI style entry (PVFMMEval, pvfmm-wrapper.cpp:445-811)
 # ----------------------------------------------------------------------------
-def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None, return_fmm=False):
-    """FP64 PVFMMEvalD(src, sl_den, NULL, n_src, trg, trg_val, n_trg, ctx, setup=1)."""
+def surf_scal(K: Kernel, scale: float) -> np.ndarray:
+    """Scaling of the double-layer values (pvfmm-wrapper.cpp:521-535): the
+    first k0 values by scale * scale^src_scal, the last three by 1."""
+    return np.array([scale * scale ** e for e in K.src_scal] + [1.0, 1.0, 1.0])
+
+
+def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None, return_fmm=False,
+               dl_den=None):
+    """FP64 PVFMMEvalD(src, sl_den, dl_den, n_src, trg, trg_val, n_trg, ctx,
+    setup=1).  Either density may be None (NULL); dl_den holds k0 + 3 values
+    per source (pvfmm.h:269-272)."""
     K = KERNELS[kernel_id]
     src_pos = np.asarray(src_pos, dtype=np.float64).reshape(-1, 3)
     trg_pos = np.asarray(trg_pos, dtype=np.float64).reshape(-1, 3)
-    sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
+    if sl_den is not None:
+        sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
+    if dl_den is not None:
+        dl_den = np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3)
     scale, shift = bounding_box_map(src_pos, trg_pos)
     src_c = map_points(src_pos, scale, shift)
     trg_c = map_points(trg_pos, scale, shift)
@@ -931,30 +1021,37 @@ def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, o
     trg_scal = np.array([scale ** e for e in K.trg_scal])
     fmm = FMM(kernel_id, m, max_pts, ops)
     t0 = time.perf_counter()
-    fmm.setup(src_c, trg_c)
+    fmm.setup(src_c, trg_c, src_weight=(sl_den is not None) + (dl_den is not None))
     setup_ms = 1000 * (time.perf_counter() - t0)
-    den = (sl_den * src_scal[None, :])[fmm.src_perm]
-    out_sorted = fmm.evaluate(den)
+    fmm.io_scal = (src_scal, trg_scal, surf_scal(K, scale))
+    out = _eval_scaled(fmm, sl_den, dl_den)
     fmm.stage_ms["setup"] = setup_ms
-    out = np.empty_like(out_sorted)
-    out[fmm.trg_perm] = out_sorted
-    out = out * trg_scal[None, :]
-    fmm.io_scal = (src_scal, trg_scal)
     if return_fmm:
         return out, fmm
     return out
 
 
-def pvfmm_eval_setup0(fmm: "FMM", sl_den) -> np.ndarray:
-    """PVFMMEvalD with setup=0 (src/pvfmm-wrapper.cpp:637-654): the tree of a
-    previous pvfmm_eval(..., return_fmm=True) on the same points, new
-    densities."""
-    src_scal, trg_scal = fmm.io_scal
-    den = (np.asarray(sl_den, dtype=np.float64).reshape(-1, fmm.kernel.k0) * src_scal[None, :])[fmm.src_perm]
-    out_sorted = fmm.evaluate(den)
+def _eval_scaled(fmm: "FMM", sl_den, dl_den) -> np.ndarray:
+    src_scal, trg_scal, sf_scal = fmm.io_scal
+    K = fmm.kernel
+    if sl_den is None and dl_den is None:           # no source points at all
+        fmm.stage_ms = {}
+        return np.zeros((len(fmm.trg), K.k1))
+    den = None if sl_den is None else \
+        (np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0) * src_scal[None, :])[fmm.src_perm]
+    surf = None if dl_den is None else \
+        (np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3) * sf_scal[None, :])[fmm.src_perm]
+    out_sorted = fmm.evaluate(den, surf)
     out = np.empty_like(out_sorted)
     out[fmm.trg_perm] = out_sorted
     return out * trg_scal[None, :]
+
+
+def pvfmm_eval_setup0(fmm: "FMM", sl_den, dl_den=None) -> np.ndarray:
+    """PVFMMEvalD with setup=0 (src/pvfmm-wrapper.cpp:637-654): the tree of a
+    previous pvfmm_eval(..., return_fmm=True) on the same points, new
+    densities (the same ones NULL as before)."""
+    return _eval_scaled(fmm, sl_den, dl_den)
 
 
 def ptfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None):
@@ -987,6 +1084,30 @@ def direct_sum(kernel_id: int, src_pos, sl_den, trg_pos, chunk=2048) -> np.ndarr
     for a in range(0, len(trg), chunk):
         out[a:a + chunk] = K.s2t.eval(src, den, trg[a:a + chunk])
     return out
+
+
+def direct_sum_mapped(kernel_id: int, src_pos, sl_den, trg_pos, dl_den=None, chunk=512) -> np.ndarray:
+    """FP64 direct sum of what PVFMMEvalD approximates: both layers evaluated
+    in the reference's unit-box frame, on the densities scaled as it scales
+    them, and the result scaled back (pvfmm-wrapper.cpp:458-541, 800-808).
+    For single-layer densities this equals direct_sum; for double-layer
+    values it is the quantity the reference's FMM converges to."""
+    K = KERNELS[kernel_id]
+    src = np.asarray(src_pos, dtype=np.float64).reshape(-1, 3)
+    trg = np.asarray(trg_pos, dtype=np.float64).reshape(-1, 3)
+    scale, shift = bounding_box_map(src, trg)
+    src_c, trg_c = map_points(src, scale, shift), map_points(trg, scale, shift)
+    src_scal = np.array([scale ** e for e in K.src_scal])
+    trg_scal = np.array([scale ** e for e in K.trg_scal])
+    out = np.zeros((len(trg), K.k1))
+    for a in range(0, len(trg), chunk):
+        if sl_den is not None:
+            den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0) * src_scal[None, :]
+            out[a:a + chunk] += K.s2t.eval(src_c, den, trg_c[a:a + chunk])
+        if dl_den is not None:
+            surf = np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3) * surf_scal(K, scale)[None, :]
+            out[a:a + chunk] += K.dbl[1].eval(src_c, surf, trg_c[a:a + chunk])
+    return out * trg_scal[None, :]
 
 
 def rel_l2(a, b) -> float:

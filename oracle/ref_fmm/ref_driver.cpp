@@ -44,8 +44,10 @@ std::vector<RefNode*> nodes_of(const void* ctx_) {
 extern "C" {
 
 // Nodes of the last tree, one record of 10 int64 per node in the tree's node
-// order: X, Y, Z, depth, leaf, #sources, #targets (points held by the leaf),
-// pt_cnt[0], pt_cnt[1], 0.  Returns the node count; writes at most cap records.
+// order: X, Y, Z, depth, leaf, #sources, #targets (points held by the leaf;
+// a source position counts once whether it carries single-layer values,
+// double-layer values or both), pt_cnt[0], pt_cnt[1], 0.  Returns the node
+// count; writes at most cap records.
 long ref_tree_nodes(const void* ctx, int64_t* out, long cap) {
   std::vector<RefNode*> nodes = nodes_of(ctx);
   for (long i = 0; i < (long)nodes.size() && i < cap; ++i) {
@@ -53,7 +55,7 @@ long ref_tree_nodes(const void* ctx, int64_t* out, long cap) {
     int64_t* r = out + 10 * i;
     node_key(n, r);
     r[4] = n->IsLeaf() ? 1 : 0;
-    r[5] = (int64_t)(n->src_coord.Dim() / 3);
+    r[5] = (int64_t)(std::max(n->src_coord.Dim(), n->surf_coord.Dim()) / 3);
     r[6] = (int64_t)(n->trg_coord.Dim() / 3);
     r[7] = (int64_t)n->pt_cnt[0];
     r[8] = (int64_t)n->pt_cnt[1];

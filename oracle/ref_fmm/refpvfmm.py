@@ -97,15 +97,18 @@ class RefContext:
         if not self.ctx:
             raise RuntimeError("reference context creation failed")
 
-    def evaluate(self, src, den, trg, setup=True) -> np.ndarray:
+    def evaluate(self, src, den, trg, setup=True, dl=None) -> np.ndarray:
+        """PVFMMEvalD(src, den, dl, ...): `den` (n, k0) single-layer
+        densities or None, `dl` (n, k0+3) double-layer values or None."""
         src = np.ascontiguousarray(src, dtype=np.float64).reshape(-1)
-        den = np.ascontiguousarray(den, dtype=np.float64).reshape(-1)
+        den = None if den is None else np.ascontiguousarray(den, dtype=np.float64).reshape(-1)
+        dl = None if dl is None else np.ascontiguousarray(dl, dtype=np.float64).reshape(-1)
         same = trg is None
         trg = src if same else np.ascontiguousarray(trg, dtype=np.float64).reshape(-1)
         n_src, n_trg = len(src) // 3, len(trg) // 3
         out = np.zeros(n_trg * self.k1)
-        self.lib.PVFMMEvalD(_p(src), _p(den), None, n_src, _p(trg), _p(out), n_trg, ctypes.c_void_p(self.ctx),
-                            1 if setup else 0)
+        self.lib.PVFMMEvalD(_p(src), None if den is None else _p(den), None if dl is None else _p(dl), n_src,
+                            _p(trg), _p(out), n_trg, ctypes.c_void_p(self.ctx), 1 if setup else 0)
         return out.reshape(n_trg, self.k1)
 
     def tree(self):
@@ -168,10 +171,10 @@ def profile_report() -> list:
     return rows
 
 
-def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0):
+def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None):
     ctx = RefContext(kernel, m, max_pts, threads)
     try:
-        out = ctx.evaluate(src, den, trg)
+        out = ctx.evaluate(src, den, trg, dl=dl)
         return out, ctx.tree(), ctx.lists()
     finally:
         ctx.close()

@@ -74,6 +74,8 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMEvalF": (None, [vp, vp, vp, cl, vp, vp, cl, vp, ci]),
         "PVFMMEvalDeviceD": (ci, [vp, vp, vp, cl, vp, vp, cl, ci, vp]),
         "PVFMMEvalDeviceF": (ci, [vp, vp, vp, cl, vp, vp, cl, ci, vp]),
+        "PVFMMEvalLayersDeviceD": (ci, [vp, vp, vp, vp, cl, vp, vp, cl, ci, vp]),
+        "PVFMMEvalLayersDeviceF": (ci, [vp, vp, vp, vp, cl, vp, vp, cl, ci, vp]),
         "PVFMMEvalAdjointDeviceD": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
         "PVFMMEvalAdjointDeviceF": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
         "PVFMMSetUnitBox": (ci, [vp, ci]),
@@ -221,26 +223,34 @@ class FMMParticleContext:
         if sl_den is not None:
             self._check("sl_den", sl_den, self.k0, n_src)
         if dl_den is not None:
-            raise NotImplementedError("double-layer densities are not implemented")
+            # k0 + 3 values per source (the reference's wrapper.py:155 checks
+            # for 6, which fits StokesVelocity only)
+            self._check("dl_den", dl_den, self.k0 + 3, n_src)
         self._check("trg_pos", trg_pos, 3)
         n_trg = trg_pos.size // 3
         trg_val = np.empty(n_trg * self.k1, dtype=self.dtype)
         f = self._lib.PVFMMEvalD if self.dtype == np.float64 else self._lib.PVFMMEvalF
         same = trg_pos is src_pos
-        f(_ptr(src_pos), _ptr(sl_den), None, n_src, _ptr(src_pos) if same else _ptr(trg_pos), _ptr(trg_val),
-          n_trg, self._ptr, int(setup))
+        f(_ptr(src_pos), _ptr(sl_den), _ptr(dl_den), n_src, _ptr(src_pos) if same else _ptr(trg_pos),
+          _ptr(trg_val), n_trg, self._ptr, int(setup))
         err = last_error()
         if err:
             raise RuntimeError(f"PVFMMEval failed: {err}")
         return trg_val
 
     def evaluate_device(self, src_ptr: int, den_ptr: Optional[int], n_src: int, trg_ptr: int, out_ptr: int,
-                        n_trg: int, setup: bool = True, stream: int = 0) -> None:
-        """PVFMMEvalDevice* on raw CUDA pointers (e.g. torch ``tensor.data_ptr()``)."""
-        f = self._lib.PVFMMEvalDeviceD if self.dtype == np.float64 else self._lib.PVFMMEvalDeviceF
-        rc = f(self._ptr, ctypes.c_void_p(src_ptr), ctypes.c_void_p(den_ptr) if den_ptr else None, n_src,
-               ctypes.c_void_p(trg_ptr), ctypes.c_void_p(out_ptr), n_trg, int(setup),
-               ctypes.c_void_p(stream) if stream else None)
+                        n_trg: int, setup: bool = True, stream: int = 0, dl_ptr: Optional[int] = None) -> None:
+        """PVFMMEvalDevice* on raw CUDA pointers (e.g. torch ``tensor.data_ptr()``);
+        with ``dl_ptr`` (double-layer values) PVFMMEvalLayersDevice*."""
+        vp = ctypes.c_void_p
+        common = (n_src, vp(trg_ptr), vp(out_ptr), n_trg, int(setup), vp(stream) if stream else None)
+        den = vp(den_ptr) if den_ptr else None
+        if dl_ptr:
+            f = self._lib.PVFMMEvalLayersDeviceD if self.dtype == np.float64 else self._lib.PVFMMEvalLayersDeviceF
+            rc = f(self._ptr, vp(src_ptr), den, vp(dl_ptr), *common)
+        else:
+            f = self._lib.PVFMMEvalDeviceD if self.dtype == np.float64 else self._lib.PVFMMEvalDeviceF
+            rc = f(self._ptr, vp(src_ptr), den, *common)
         if rc != 0:
             raise RuntimeError(f"PVFMMEvalDevice failed: {last_error()}")
 

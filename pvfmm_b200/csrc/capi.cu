@@ -113,8 +113,8 @@ void* create_context(double box_size, int n, int m, int kernel, int precision, b
 }
 
 template <class T>
-int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const T* trg, T* val, long n_trg, int setup,
-                void* stream) {
+int eval_device(const void* ctx_, const T* src, const T* den, const T* dl, long n_src, const T* trg, T* val,
+                long n_trg, int setup, void* stream) {
   try {
     Handle* h = as_handle(ctx_);
     Context& c = h->ctx;
@@ -128,6 +128,8 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(c.stream, c.ev[11], 0));
     }
     check_tc5_error(c);  // a wait of the previous (asynchronous) evaluation that ran out
+    if (dl && c.kernel != PVFMMLaplacePotential && c.kernel != PVFMMStokesVelocity)
+      throw std::runtime_error("double-layer densities (dl_den) need the LaplacePotential or StokesVelocity kernel");
     if (n_trg <= 0) return 0;
     if (n_src <= 0) {
       PVFMM_CUDA_CHECK(cudaMemsetAsync(val, 0, (size_t)n_trg * c.ki.k1 * sizeof(T), c.stream));
@@ -137,13 +139,13 @@ int eval_device(const void* ctx_, const T* src, const T* den, long n_src, const 
     const bool alias = (src == trg) && (n_src == n_trg);
     if (setup || !c.tree.valid) {
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
-      build_tree(c, src, n_src, trg, n_trg, is_f, den != nullptr, alias);
+      build_tree(c, src, n_src, trg, n_trg, is_f, (den != nullptr) + (dl != nullptr), alias);
     } else if (c.tree.n_src != n_src || c.tree.n_trg != n_trg) {
       throw std::runtime_error("setup=0 requires the point counts of the last setup");
     } else {
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
     }
-    evaluate(c, den, is_f, val, is_f);
+    evaluate(c, den, dl, is_f, val, is_f);
     if (stream && user != c.stream) {
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[10], c.stream));
       PVFMM_CUDA_CHECK(cudaStreamWaitEvent(user, c.ev[10], 0));
@@ -167,28 +169,32 @@ void eval_host(const T* src_pos, const T* sl_den, const T* dl_den, long n_src, c
     Handle* h = as_handle(ctx_);
     Context& c = h->ctx;
     k1 = c.ki.k1;
-    if (dl_den) throw std::runtime_error("double-layer densities (dl_den) are not supported");
     PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
     if (n_trg <= 0) return;
     const bool alias = (src_pos == trg_pos) && (n_src == n_trg);
     T* d_src = c.io_src.as<T>(std::max(n_src, 1L) * 3);
     T* d_den = sl_den ? c.io_den.as<T>(std::max(n_src, 1L) * c.ki.k0) : nullptr;
+    T* d_dl = dl_den ? c.io_dl.as<T>(std::max(n_src, 1L) * (c.ki.k0 + 3)) : nullptr;
     T* d_trg = alias ? d_src : c.io_trg.as<T>(n_trg * 3);
     T* d_val = c.io_val.as<T>(n_trg * c.ki.k1);
     if (n_src > 0) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_src, src_pos, n_src * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
     if (!alias) PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_trg, trg_pos, n_trg * 3 * sizeof(T), cudaMemcpyHostToDevice, c.stream));
-    if (n_src > 0 && sl_den) {
+    if (n_src > 0 && (sl_den || dl_den)) {
       // the densities are first read after the tree build: upload them on a
-      // side stream meanwhile (overlaps when sl_den is pinned host memory)
+      // side stream meanwhile (overlaps when they are pinned host memory)
       if (!c.side) {
         PVFMM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
         PVFMM_CUDA_CHECK(cudaEventCreateWithFlags(&c.den_ev, cudaEventDisableTiming));
       }
-      PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.side));
+      if (sl_den)
+        PVFMM_CUDA_CHECK(cudaMemcpyAsync(d_den, sl_den, n_src * c.ki.k0 * sizeof(T), cudaMemcpyHostToDevice, c.side));
+      if (dl_den)
+        PVFMM_CUDA_CHECK(
+            cudaMemcpyAsync(d_dl, dl_den, n_src * (c.ki.k0 + 3) * sizeof(T), cudaMemcpyHostToDevice, c.side));
       PVFMM_CUDA_CHECK(cudaEventRecord(c.den_ev, c.side));
       c.den_pending = true;
     }
-    if (eval_device<T>(ctx_, d_src, d_den, n_src, d_trg, d_val, n_trg, setup, c.stream) != 0)
+    if (eval_device<T>(ctx_, d_src, d_den, d_dl, n_src, d_trg, d_val, n_trg, setup, c.stream) != 0)
       throw std::runtime_error(get_last_error());
     PVFMM_CUDA_CHECK(cudaMemcpyAsync(trg_val, d_val, n_trg * c.ki.k1 * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
     PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
@@ -227,14 +233,15 @@ int eval_adjoint(const void* ctx, const T* src, long n_src, const T* trg, const 
   try {
     Handle* h = as_handle(ctx);
     Context& c = h->ctx;
-    if (src == trg && n_src == n_trg) return eval_device<T>(ctx, trg, trg_den, n_trg, src, src_val, n_src, setup, stream);
+    if (src == trg && n_src == n_trg)
+      return eval_device<T>(ctx, trg, trg_den, nullptr, n_trg, src, src_val, n_src, setup, stream);
     if (!h->adjoint) {
       h->adjoint = create_context(-1.0, c.max_pts, c.m, c.kernel, c.precision, c.float_api);
       if (!h->adjoint) throw std::runtime_error(std::string("companion context: ") + get_last_error());
       as_handle(h->adjoint)->ctx.unit_box = c.unit_box;
       setup = 1;
     }
-    return eval_device<T>(h->adjoint, trg, trg_den, n_trg, src, src_val, n_src, setup, stream);
+    return eval_device<T>(h->adjoint, trg, trg_den, nullptr, n_trg, src, src_val, n_src, setup, stream);
   } catch (const std::exception& e) {
     set_last_error(e.what());
     return 1;
@@ -281,13 +288,21 @@ void PVFMMEvalF(const float* src_pos, const float* sl_den, const float* dl_den, 
   eval_host<float>(src_pos, sl_den, dl_den, n_src, trg_pos, trg_val, n_trg, ctx, setup);
 }
 
+int PVFMMEvalLayersDeviceD(const void* ctx, const double* src_pos, const double* sl_den, const double* dl_den,
+                           long n_src, const double* trg_pos, double* trg_val, long n_trg, int setup, void* stream) {
+  return eval_device<double>(ctx, src_pos, sl_den, dl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+}
+int PVFMMEvalLayersDeviceF(const void* ctx, const float* src_pos, const float* sl_den, const float* dl_den,
+                           long n_src, const float* trg_pos, float* trg_val, long n_trg, int setup, void* stream) {
+  return eval_device<float>(ctx, src_pos, sl_den, dl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+}
 int PVFMMEvalDeviceD(const void* ctx, const double* src_pos, const double* sl_den, long n_src, const double* trg_pos,
                      double* trg_val, long n_trg, int setup, void* stream) {
-  return eval_device<double>(ctx, src_pos, sl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+  return eval_device<double>(ctx, src_pos, sl_den, nullptr, n_src, trg_pos, trg_val, n_trg, setup, stream);
 }
 int PVFMMEvalDeviceF(const void* ctx, const float* src_pos, const float* sl_den, long n_src, const float* trg_pos,
                      float* trg_val, long n_trg, int setup, void* stream) {
-  return eval_device<float>(ctx, src_pos, sl_den, n_src, trg_pos, trg_val, n_trg, setup, stream);
+  return eval_device<float>(ctx, src_pos, sl_den, nullptr, n_src, trg_pos, trg_val, n_trg, setup, stream);
 }
 
 int PVFMMEvalAdjointDeviceD(const void* ctx, const double* src_pos, long n_src, const double* trg_pos,

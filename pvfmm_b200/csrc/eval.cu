@@ -477,7 +477,10 @@ struct NearSeg {
 };
 constexpr int kSegCap = 128;  // list entries per batch
 
-template <class Real, int Ker>
+// kDbl: the double-layer pass, P2P sources only (surface values in `den`),
+// added to pot.  with_p2p = 0: no P2P sources (no single-layer densities;
+// the W and D2T entries still come from the expansions).
+template <class Real, int Ker, bool kDbl = false>
 __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS_F32 : PVFMM_NEAR_MIN_BLOCKS_F64)
     near_field_kernel(const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo,
                       const int* __restrict__ thi, const int* __restrict__ slo, const int* __restrict__ shi,
@@ -486,12 +489,12 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
                       const double* __restrict__ tz, const double* __restrict__ sx, const double* __restrict__ sy,
                       const double* __restrict__ sz, const double* __restrict__ den, const double* __restrict__ ue,
                       const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
-                      double* __restrict__ pot) {
+                      int with_p2p, double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   constexpr bool kF32 = sizeof(Real) == 4;
   using V = typename Vec16<Real>::type;
   __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
-  __shared__ double2 tile64[kF32 ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
+  __shared__ double2 tile64[kF32 && !kDbl ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
   // the partial sums of the final fixed-order reduction reuse the tiles
   static_assert(sizeof(tiles) >= sizeof(double) * kNF * 2 * KT, "reduction buffer larger than the tiles");
   double(*red)[2][KT] = reinterpret_cast<double(*)[2][KT]>(&tiles[0][0]);
@@ -504,9 +507,9 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
   node_geom(keys[T], cx, cy, cz, half, dT);
   const int t0 = tlo[T], nt = thi[T] - t0;
   const int dim = ns * KS;
-  const int wb = w_off[T], nW = w_off[T + 1] - wb;
-  const int pbeg = p_off[T], nP = p_off[T + 1] - pbeg;
-  const int nD = (de && !kF32) ? 1 : 0;  // plain form: D2T is a segment of the stream
+  const int wb = kDbl ? 0 : w_off[T], nW = kDbl ? 0 : w_off[T + 1] - wb;
+  const int pbeg = p_off[T], nP = with_p2p ? p_off[T + 1] - pbeg : 0;
+  const int nD = (!kDbl && de && !kF32) ? 1 : 0;  // plain form: D2T is a segment of the stream
   const int n_ent = nD + nW + nP;
   int buf = 0;
   for (int c0 = 0; c0 < nt; c0 += 2 * kNF) {
@@ -525,7 +528,7 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
     // D2T of the mixed form: the downward equivalent densities come from the
     // FP64-cutoff pseudo-inverse, whose large cancelling components only FP64
     // sums resolve, so they are evaluated from FP64 records.
-    if constexpr (kF32) {
+    if constexpr (kF32 && !kDbl) {
       if (de) {
         const double hr = half * kRad1;
         const double* dens = de + (long)b * dim;
@@ -684,7 +687,7 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
           for (int k = 0; k < KT; ++k) sum[k] += red[gg * nc + ti][t][k];
         const long o = (long)(t0 + c0 + ti + (t ? nc : 0)) * KT;
 #pragma unroll
-        for (int k = 0; k < KT; ++k) pot[o + k] = sum[k] * scale;
+        for (int k = 0; k < KT; ++k) pot[o + k] = kDbl ? pot[o + k] + sum[k] * scale : sum[k] * scale;
       }
     }
   }
@@ -697,6 +700,8 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
 // operator).  mode 1 (X, fmm_pts.txx:4444-4736): node = xtrg[b], sources =
 // the X list, added to DC[node].
 // ---------------------------------------------------------------------------
+// mode 2: as mode 0, added to the row (the double-layer pass after the single
+// layer's).
 // Surface1 (mode 0 only): the check surface lies at least 1.2 half-widths
 // from every point of the leaf, so FP64 needs one Newton step (mixed form).
 template <int Ker, bool Surface1 = false>
@@ -716,8 +721,8 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
   node_geom(keys[T], cx, cy, cz, half, dT);
   const double hr = half * rad;
   const int dim = ns * KT;
-  double* o = mode == 0 ? out + (long)b * dim : out + (long)T * dim;
-  const double oscale = mode == 0 ? scale * ldexp(1.0, -deg * dT) : scale;
+  double* o = mode != 1 ? out + (long)b * dim : out + (long)T * dim;
+  const double oscale = mode != 1 ? scale * ldexp(1.0, -deg * dT) : scale;
   for (int c0 = 0; c0 < ns; c0 += kNT) {
     const Split sp(ns - c0);
     const int k = c0 + sp.ti;
@@ -731,7 +736,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
     double acc[KT];
 #pragma unroll
     for (int c = 0; c < KT; ++c) acc[c] = 0;
-    if (mode == 0) {
+    if (mode != 1) {
       point_sources<double, Ker, Surface1>(tl, sx, sy, sz, den, slo[T], shi[T], 0, 0, 0, sp, pt, acc);
     } else {
       for (int q = x_off[T]; q < x_off[T + 1]; ++q) {
@@ -742,7 +747,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
         point_sources<double, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], sxc - cx, syc - cy, szc - cz, sp, pt, acc);
       }
     }
-    reduce_store<KT>(red, sp, acc, oscale, o + c0 * KT, mode == 1);
+    reduce_store<KT>(red, sp, acc, oscale, o + c0 * KT, mode != 0);
   }
 }
 
@@ -1453,21 +1458,23 @@ void launch_hadamard(Context& ctx, int n3h, long f_base, const Cplx<Real>* sin_,
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------
-template <class Tin>
-__global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict__ perm, long n, int k0, double s0,
-                               double s1, double s2, double* __restrict__ out) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const long p = perm[i];
-  const double sc[3] = {s0, s1, s2};
-  for (int j = 0; j < k0; ++j) out[i * k0 + j] = (double)((Tin)in[p * k0 + j] * (Tin)sc[j]);
-}
-
-// Output scales scale_x^trg_scal[k] of the C interface's rescale, per output
-// component (at most 9).
+// Per-component scales of the C interface's rescale (at most 9 components):
+// scale_x^src_scal of the densities, scale_x * scale_x^src_scal and 1 of the
+// double-layer values, scale_x^trg_scal of the outputs.
 struct OutScales {
   double v[9];
 };
+
+// Densities (k values per point) in sorted order, each scaled in the input
+// precision as the reference scales them (pvfmm-wrapper.cpp:591-599).
+template <class Tin>
+__global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict__ perm, long n, int k,
+                               OutScales sc, double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long p = perm[i];
+  for (int j = 0; j < k; ++j) out[i * k + j] = (double)((Tin)in[p * k + j] * (Tin)sc.v[j]);
+}
 
 template <class Tout>
 __global__ void unsort_values(const double* __restrict__ pot, const int* __restrict__ perm, long n, int k1,
@@ -1616,8 +1623,18 @@ void vlist(Context& ctx, const double* ue, double* dc, int kin, int kout, const 
 }
 
 template <class Real, int KerS2T, int KerExp>
-void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float) {
+void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float) {
   DevTree& T = ctx.tree;
+  // double-layer kernels of the source -> check and source -> target
+  // sub-kernels (Laplace potential: laplace_dbl_poten; Stokes velocity:
+  // stokes_sym_dip; kernel.txx:1334-1340, 1470-1473)
+  constexpr int KerDblExp = KerExp == kKerLaplace ? kKerLaplaceDbl : KerExp == kKerStokes ? kKerStokesDbl : -1;
+  constexpr int KerDblS2T = KerS2T == kKerLaplace ? kKerLaplaceDbl : KerS2T == kKerStokes ? kKerStokesDbl : -1;
+  const bool has_sl = den_in != nullptr, has_dl = dl_in != nullptr;
+  if (has_dl && (KerDblExp < 0 || KerDblS2T < 0))
+    throw std::runtime_error("this kernel has no double-layer kernel (dl_den must be NULL)");
+  if (T.src_counted && (int)has_sl + (int)has_dl != T.src_weight)
+    throw std::runtime_error("setup=0 requires the same densities (sl_den, dl_den) passed or NULL as at setup");
   auto s = ctx.stream;
   // expansion dims: equivalent densities din = ns*kin, check potentials
   // dout = ns*kout (kin = kout for Laplace and Stokes velocity); the
@@ -1637,21 +1654,29 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   }
   // densities (sorted, scaled by scale_x^src_scal: pvfmm-wrapper.cpp:522-541, 591-595)
   double* den = ctx.den.as<double>(std::max(T.n_src, 1L) * k0);
-  double ss[3];
-  OutScales ts;
-  for (int j = 0; j < 3; ++j) ss[j] = den_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.src_scal[j])
-                                                : std::pow(T.scale_x, ctx.ki.src_scal[j]);
-  for (int j = 0; j < 9; ++j) ts.v[j] = out_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.trg_scal[j])
-                                                  : std::pow(T.scale_x, ctx.ki.trg_scal[j]);
-  if (T.src_counted) {
+  // double-layer values (sorted, scaled by surf_scal: scale_x * scale_x^src_scal
+  // for the k0 densities, 1 for the normal; pvfmm-wrapper.cpp:528-535, 596-599)
+  double* surf = has_dl ? ctx.surf.as<double>(std::max(T.n_src, 1L) * (k0 + 3)) : nullptr;
+  OutScales ss, sf, ts;
+  for (int j = 0; j < 9; ++j) {
+    ss.v[j] = den_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.src_scal[j % 3])
+                        : std::pow(T.scale_x, ctx.ki.src_scal[j % 3]);
+    ts.v[j] = out_float ? (double)std::pow((float)T.scale_x, (float)ctx.ki.trg_scal[j])
+                        : std::pow(T.scale_x, ctx.ki.trg_scal[j]);
+  }
+  for (int j = 0; j < 9; ++j)
+    sf.v[j] = j >= k0 ? 1.0 : den_float ? (double)((float)T.scale_x * (float)ss.v[j]) : T.scale_x * ss.v[j];
+  auto sort_vals = [&](const void* in, int k, const OutScales& sc, double* o) {
     ++ctx.n_launch;
     if (den_float)
-      sort_densities<float><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const float*)den_in, T.src_perm.get<int>(), T.n_src,
-                                                                   k0, ss[0], ss[1], ss[2], den);
+      sort_densities<float><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const float*)in, T.src_perm.get<int>(), T.n_src,
+                                                                   k, sc, o);
     else
-      sort_densities<double><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const double*)den_in, T.src_perm.get<int>(),
-                                                                    T.n_src, k0, ss[0], ss[1], ss[2], den);
-  }
+      sort_densities<double><<<ceil_div(T.n_src, 256), 256, 0, s>>>((const double*)in, T.src_perm.get<int>(),
+                                                                    T.n_src, k, sc, o);
+  };
+  if (T.src_counted && has_sl) sort_vals(den_in, k0, ss, den);
+  if (T.src_counted && has_dl) sort_vals(dl_in, k0 + 3, sf, surf);
   double* ue = ctx.ue.as<double>((size_t)N * din);
   double* dc = ctx.dc.as<double>((size_t)N * dout);
   PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * din * sizeof(double), s));
@@ -1674,9 +1699,18 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     // near-null components of the equivalent densities; the mixed form's FP32
     // V-list does not cancel those (one Newton step here raised the 4M-point
     // potential error from 3e-7 to 2.5e-6)
-    surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
-        0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, deg,
-        uc);
+    if (has_sl)
+      surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
+          0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, deg,
+          uc);
+    if constexpr (KerDblExp >= 0) {
+      if (has_dl) {
+        ++ctx.n_launch;
+        surface_check_kernel<KerDblExp, false><<<T.n_sleaf, kNT, 0, s>>>(
+            has_sl ? 2 : 0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, surf, usurf, ns, kRad1,
+            ker_scale(KerDblExp), deg, uc);
+      }
+    }
     // equivalent densities (uc UC2UE0) UC2UE1 straight into the leaves' rows of UE
     ctx.n_launch += 2;
     translate_gemm(s, T.n_sleaf, rk, dout, uc, dout, nullptr, ctx.dops.uc2ue0.get<double>(), rk, t1, rk, nullptr,
@@ -1729,9 +1763,18 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
   // ---- X-list
   if (T.src_counted && T.n_xtrg > 0) {
     ++ctx.n_launch;
-    surface_check_kernel<KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
-                                                           T.x_list.get<int>(), sx, sy, sz, den, usurf, ns, kRad0,
-                                                           kscale_exp, deg, dc);
+    if (has_sl)
+      surface_check_kernel<KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
+                                                             T.x_list.get<int>(), sx, sy, sz, den, usurf, ns, kRad0,
+                                                             kscale_exp, deg, dc);
+    if constexpr (KerDblExp >= 0) {
+      if (has_dl) {
+        ++ctx.n_launch;
+        surface_check_kernel<KerDblExp><<<T.n_xtrg, kNT, 0, s>>>(
+            1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(), T.x_list.get<int>(), sx, sy, sz, surf, usurf,
+            ns, kRad0, ker_scale(KerDblExp), deg, dc);
+      }
+    }
   }
   ev(7);
   // ---- D2D, top-down
@@ -1760,7 +1803,17 @@ void evaluate_impl(Context& ctx, const void* den_in, bool den_float, void* out, 
     near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNF, 0, s>>>(
         T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
         T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
-        T.tz.get<double>(), sx, sy, sz, den, ue32, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T), pot);
+        T.tz.get<double>(), sx, sy, sz, den, ue32, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T),
+        has_sl ? 1 : 0, pot);
+    if constexpr (KerDblS2T >= 0) {
+      if (has_dl) {  // the double layer's P2P sources, added
+        ++ctx.n_launch;
+        near_field_kernel<Real, KerDblS2T, true><<<T.n_tleaf, kNF, 0, s>>>(
+            T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
+            T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
+            T.tz.get<double>(), sx, sy, sz, surf, nullptr, nullptr, usurf, ns, ker_scale(KerDblS2T), 1, pot);
+      }
+    }
   } else {
     ev(12);
   }
@@ -1857,37 +1910,37 @@ void upload_operators(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
-void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float) {
+void evaluate(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float) {
   const bool f32 = ctx.precision == 1;
   switch (ctx.kernel) {
     case kLaplacePot:
-      if (f32) evaluate_impl<float, kKerLaplace, kKerLaplace>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerLaplace, kKerLaplace>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerLaplace, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerLaplace, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     case kLaplaceGrad:
-      if (f32) evaluate_impl<float, kKerLaplaceGrad, kKerLaplace>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerLaplaceGrad, kKerLaplace>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerLaplaceGrad, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerLaplaceGrad, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     case kLaplacePotGrad:
-      if (f32) evaluate_impl<float, kKerLaplacePG, kKerLaplace>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerLaplacePG, kKerLaplace>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerLaplacePG, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerLaplacePG, kKerLaplace>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     case kStokesVel:
-      if (f32) evaluate_impl<float, kKerStokes, kKerStokes>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerStokes, kKerStokes>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerStokes, kKerStokes>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerStokes, kKerStokes>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     // the kernels that expand themselves (kernel.txx:894-901)
     case kStokesPress:
-      if (f32) evaluate_impl<float, kKerStokesPress, kKerStokesPress>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerStokesPress, kKerStokesPress>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerStokesPress, kKerStokesPress>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerStokesPress, kKerStokesPress>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     case kStokesVelGrad:
-      if (f32) evaluate_impl<float, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerStokesGrad, kKerStokesGrad>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     case kBiotSavart:
-      if (f32) evaluate_impl<float, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, den_float, out, out_float);
-      else evaluate_impl<double, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, den_float, out, out_float);
+      if (f32) evaluate_impl<float, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, dl_in, den_float, out, out_float);
+      else evaluate_impl<double, kKerBiotSavart, kKerBiotSavart>(ctx, den_in, dl_in, den_float, out, out_float);
       break;
     default:
       throw std::runtime_error("unsupported kernel");

@@ -27,7 +27,12 @@ struct DevTree {
   std::vector<long> int_off;
   // point data (sorted)
   long n_src = 0, n_trg = 0;
-  bool src_counted = true;            // false when sl_den == NULL
+  // point sets the source positions stand for: 1 per density passed
+  // (sl_den single layer, dl_den double layer), 0 when neither is; each
+  // counts in the refinement and in pt_cnt[0] (fmm_node.txx:81-92,
+  // fmm_pts.txx:1332-1333)
+  int src_weight = 1;
+  bool src_counted = true;            // src_weight > 0
   DevBuf src_perm, trg_perm;          // int: sorted index -> input index
   DevBuf src_key, trg_key;            // MKey (sorted)
   DevBuf src_leaf, trg_leaf;          // int: leaf node id of each sorted point
@@ -78,6 +83,7 @@ struct Context {
   int device = 0;
   // evaluation buffers
   DevBuf den;             // sorted densities (Real, n_src x k0)
+  DevBuf surf;            // sorted double-layer values (FP64, n_src x (k0 + 3))
   DevBuf ue_c;            // mixed form: projected upward equivalent densities
   DevBuf pot;             // sorted target values (Real, n_trg x k1)
   DevBuf ue, dc;          // per node (Real)
@@ -86,6 +92,7 @@ struct Context {
   DevBuf scratch;         // sort / scan temporaries
   DevBuf scratch2;
   DevBuf io_src, io_trg, io_den, io_val;  // staging for host-pointer calls
+  DevBuf io_dl;
   DevBuf stat;            // small status / reduction buffer
   DevBuf t[24];           // temporaries of the tree build, reused across calls
   std::vector<DevBuf> lvlR, lvlS;  // per-level internal-node keys (refined / balanced)
@@ -109,9 +116,11 @@ struct Context {
 
 // tree.cu
 void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
-                bool src_counted, bool trg_alias);
+                int src_weight, bool trg_alias);
 // eval.cu
-void evaluate(Context& ctx, const void* den_in, bool den_float, void* out, bool out_float);
+// den_in: single-layer densities (n_src x k0) or NULL; dl_in: double-layer
+// values (n_src x (k0 + 3)) or NULL; both in the input order and precision
+void evaluate(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float);
 void upload_operators(Context& ctx);
 // hadamard_tc.cu: mixed-form V-list Hadamard of target parents [p0, p0+np)
 // on tcgen05 (rows of sout relative to p0) over n3h frequencies starting at

@@ -148,7 +148,11 @@ enum KerType {
   kKerLaplacePG = 3,
   kKerStokesPress = 4,  // stokes_press_, kernel.txx:1366-1378
   kKerStokesGrad = 5,   // stokes_grad_, kernel.txx:1404-1432
-  kKerBiotSavart = 6    // biot_savart_, kernel.txx:1492-1506
+  kKerBiotSavart = 6,   // biot_savart_, kernel.txx:1492-1506
+  // double-layer kernels: KS = k0 + 3 source values per point (density and
+  // normal, read in the order the reference's uKerEval reads them)
+  kKerLaplaceDbl = 7,   // laplace_dbl_poten_, kernel.txx:1299-1311
+  kKerStokesDbl = 8     // stokes_sym_dip_, kernel.txx:1437-1456
 };
 
 template <int Ker>
@@ -167,6 +171,10 @@ template <>
 struct KerDims<kKerStokesGrad> { static constexpr int KS = 3, KT = 9; };
 template <>
 struct KerDims<kKerBiotSavart> { static constexpr int KS = 3, KT = 3; };
+template <>
+struct KerDims<kKerLaplaceDbl> { static constexpr int KS = 4, KT = 1; };
+template <>
+struct KerDims<kKerStokesDbl> { static constexpr int KS = 6, KT = 3; };
 
 // Adds K(r) f to u (r = target - source).
 // Surface1 = true: the source is an equivalent-surface point at a distance
@@ -213,6 +221,20 @@ __device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* 
     u[0] += rinv3 * (f[1] * rz - f[2] * ry);
     u[1] += rinv3 * (f[2] * rx - f[0] * rz);
     u[2] += rinv3 * (f[0] * ry - f[1] * rx);
+  } else if constexpr (Ker == kKerLaplaceDbl) {  // (r . f[0:3]) f[3] / r^3
+    const Real rinv3 = rinv * rinv * rinv;
+    u[0] += (rx * f[0] + ry * f[1] + rz * f[2]) * rinv3 * f[3];
+  } else if constexpr (Ker == kKerStokesDbl) {
+    // f = v[0:3], n = v[3:6]; n.f is formed as v0 v3 + v1 v1 + v2 v2, as the
+    // reference forms it; u += r (n.f - 3 (r.n)(r.f) / r^2) / r^3
+    const Real rinv2 = rinv * rinv, rinv3 = rinv2 * rinv;
+    const Real rdf = f[0] * rx + f[1] * ry + f[2] * rz;
+    const Real rdn = f[3] * rx + f[4] * ry + f[5] * rz;
+    const Real ndf = f[0] * f[3] + f[1] * f[1] + f[2] * f[2];
+    const Real common = (ndf - (Real)3 * rdn * rdf * rinv2) * rinv3;
+    u[0] += rx * common;
+    u[1] += ry * common;
+    u[2] += rz * common;
   } else {  // Stokes velocity
     const Real rinv2 = rinv * rinv;
     const Real ip = (f[0] * rx + f[1] * ry + f[2] * rz) * rinv2;
@@ -222,10 +244,12 @@ __device__ __forceinline__ void ker_eval(Real rx, Real ry, Real rz, const Real* 
   }
 }
 
-// 1/(8 pi) for Stokes velocity and velocity gradient, 1/(4 pi) otherwise
-// (the kernels' ScaleFactor, kernel.txx:1279, 1352, 1368, 1406, 1494).
+// 1/(8 pi) for Stokes velocity and velocity gradient, -1/(8 pi) for the
+// Stokes double layer, 1/(4 pi) otherwise (the kernels' ScaleFactor,
+// kernel.txx:1278, 1301, 1353, 1368, 1407, 1436, 1494).
 __host__ __device__ constexpr double ker_scale(int ker) {
   return (ker == kKerStokes || ker == kKerStokesGrad) ? 1.0 / (8 * 3.14159265358979323846)
+         : ker == kKerStokesDbl                       ? -1.0 / (8 * 3.14159265358979323846)
                                                       : 1.0 / (4 * 3.14159265358979323846);
 }
 

@@ -143,9 +143,10 @@ __global__ void assemble_keys(const unsigned long long* __restrict__ hi, const u
 }
 
 // ------------------------------------------------------------------ refine
+// sw: point sets the source positions stand for (1 per density passed)
 __global__ void refine_level(const MKey* __restrict__ cur, long n_cur, int d, const MKey* __restrict__ sk, long n_s,
-                             const MKey* __restrict__ tk, long n_t, const MKey* __restrict__ gk, long n_g, long max_pts,
-                             int max_depth, int* __restrict__ split) {
+                             int sw, const MKey* __restrict__ tk, long n_t, const MKey* __restrict__ gk, long n_g,
+                             long max_pts, int max_depth, int* __restrict__ split) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n_cur) return;
   unsigned int X, Y, Z, dd;
@@ -155,7 +156,7 @@ __global__ void refine_level(const MKey* __restrict__ cur, long n_cur, int d, co
     const MKey b = cur[i], e = node_end_key(X, Y, Z, d);
     const long g = lower_bound_key(gk, n_g, e) - lower_bound_key(gk, n_g, b);
     long c = 0;
-    if (sk) c += lower_bound_key(sk, n_s, e) - lower_bound_key(sk, n_s, b);
+    if (sk) c += sw * (lower_bound_key(sk, n_s, e) - lower_bound_key(sk, n_s, b));
     c += lower_bound_key(tk, n_t, e) - lower_bound_key(tk, n_t, b);
     s = (g > max_pts || c > max_pts) ? 1 : 0;
   }
@@ -364,7 +365,8 @@ __global__ void gather_coords(const double* __restrict__ in, const int* __restri
 __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf, const int* __restrict__ parent,
                             const int* __restrict__ child0, const int* __restrict__ coll, const int* __restrict__ slo,
                             const int* __restrict__ shi, const int* __restrict__ tlo, const int* __restrict__ thi,
-                            long nsrf, int mode, int* __restrict__ p_cnt, int* __restrict__ x_cnt, int* __restrict__ w_cnt,
+                            long nsrf, int sw, int mode, int* __restrict__ p_cnt, int* __restrict__ x_cnt,
+                            int* __restrict__ w_cnt,
                             int* __restrict__ v_cnt, const int* __restrict__ p_off, const int* __restrict__ x_off,
                             const int* __restrict__ w_off, int* __restrict__ p_list, int* __restrict__ x_list,
                             int* __restrict__ w_list) {
@@ -398,7 +400,7 @@ __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf
             if (ns_ch <= 0) continue;
             if (max(abs(rx), max(abs(ry), abs(rz))) <= 3) {
               ADD(pl, np, ch);  // U2
-            } else if (leaf[ch] && ns_ch <= nsrf) {
+            } else if (leaf[ch] && (long)ns_ch * sw <= nsrf) {  // pt_cnt[0] counts each layer
               ADD(pl, np, ch);  // W handled as P2P (fmm_pts.txx:5325)
             } else {
               ADD(wl, nw, ch);  // W (fmm_pts.txx:4929)
@@ -758,7 +760,7 @@ static std::vector<MKey> seed_grid_keys(int max_pts, bool real_float) {
 }
 
 void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
-                bool src_counted, bool trg_alias) {
+                int src_weight, bool trg_alias) {
   if (n_src < 1 || n_trg < 1) throw std::runtime_error("build_tree needs at least one source and one target");
   if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, kChkSlots * sizeof(int)));
   DevTree& T = ctx.tree;
@@ -766,7 +768,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   T.valid = false;
   T.n_src = n_src;
   T.n_trg = n_trg;
-  T.src_counted = src_counted && n_src > 0;
+  T.src_weight = n_src > 0 ? src_weight : 0;
+  T.src_counted = T.src_weight > 0;
   // 1. bounding box and map
   double bs[6], bt[6];
   if (pos_float) {
@@ -843,9 +846,9 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       int* split = ctx.t[3].as<int>(n_cur);
       int* offs = ctx.t[23].as<int>(n_cur);
       ++ctx.n_launch;
-      refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b->get<MKey>(), n_cur, d, sk, T.n_src, tk,
-                                                                   T.n_trg, d_gk, n_gk, ctx.max_pts,
-                                                                   kMaxDepth, split);
+      refine_level<<<ceil_div(n_cur, kThreads), kThreads, 0, s>>>(cur_b->get<MKey>(), n_cur, d, sk, T.n_src,
+                                                                   T.src_weight, tk, T.n_trg, d_gk, n_gk,
+                                                                   ctx.max_pts, kMaxDepth, split);
       const long n_split = exclusive_scan(ctx, split, offs, n_cur);
       if (n_split == 0) break;
       if ((long)ctx.lvlR.size() <= d) ctx.lvlR.resize(d + 1);
@@ -962,8 +965,9 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* vc = ctx.t[0].as<int>(N);
     const long nsrf = ctx.ns;
     ++ctx.n_launch;
-    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 0, pc, xc,
-                                                 wc, vc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf,
+                                                 T.src_weight, 0, pc, xc, wc, vc, nullptr, nullptr, nullptr, nullptr,
+                                                 nullptr, nullptr);
     int* po = T.p_off.as<int>(N + 1);
     int* xo = T.x_off.as<int>(N + 1);
     int* wo = T.w_off.as<int>(N + 1);
@@ -985,8 +989,9 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* xl = T.x_list.as<int>(std::max(T.n_x, 1L));
     int* wl = T.w_list.as<int>(std::max(T.n_w, 1L));
     ++ctx.n_launch;
-    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf, 1, nullptr,
-                                                 nullptr, nullptr, nullptr, po, xo, wo, pl, xl, wl);
+    build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf,
+                                                 T.src_weight, 1, nullptr, nullptr, nullptr, nullptr, po, xo, wo, pl,
+                                                 xl, wl);
     int* vt = T.vtab.as<int>(std::max(T.n_vtrg, 1L) * 26);
     unsigned* vm = T.vmask.as<unsigned>(std::max(T.n_vtrg, 1L));
     if (T.n_vtrg > 0) {

@@ -125,16 +125,34 @@ REFERENCE_CASES = {
     "stokes_press_m4": (2, 4, 60, "unif", 2000, False, 9),
     "stokes_grad_m4": (4, 4, 60, "unif", 2000, False, 10),
     "biot_savart_m4": (5, 4, 60, "unif", 2000, False, 11),
+    # double-layer sources (dl_den: k0 + 3 values per point), alone or with
+    # single-layer densities on the same points
+    "laplace_dl_unif_m6": (0, 6, 50, "unif", 3000, False, 12, "dl"),
+    "laplace_sldl_gauss_m6": (0, 6, 50, "gauss", 4000, True, 13, "sldl"),
+    "stokes_dl_m4": (3, 4, 60, "unif", 2000, False, 14, "dl"),
+    "stokes_sldl_gauss_m4": (3, 4, 60, "gauss", 2000, True, 15, "sldl"),
 }
 KDIM = {0: (1, 1), 1: (1, 3), 2: (3, 1), 3: (3, 3), 4: (3, 9), 5: (3, 3)}
 
 
+def case_spec(name):
+    """(kernel, m, max_pts, distribution, n, separate targets, seed, layers),
+    layers "sl" (single layer), "dl" (double layer) or "sldl" (both)."""
+    spec = REFERENCE_CASES[name]
+    return spec if len(spec) == 8 else spec + ("sl",)
+
+
 def reference_case_inputs(name):
-    kid, m, mp, dist, n, sep, seed = REFERENCE_CASES[name]
+    """src, sl_den (None when not passed), trg (None: the sources), dl_den
+    (None when not passed)."""
+    kid, m, mp, dist, n, sep, seed, layers = case_spec(name)
     src = points(dist, n, seed)
     trg = points("unif", n // 2, seed + 100) * 0.8 + 0.1 if sep else None
-    den = np.random.default_rng(seed + 200).uniform(-1, 1, (n, KDIM[kid][0]))
-    return src, den, trg
+    den = np.random.default_rng(seed + 200).uniform(-1, 1, (n, KDIM[kid][0])) if "sl" in layers else None
+    dl = None
+    if "dl" in layers:
+        dl = np.random.default_rng(seed + 300).uniform(-1, 1, (n, KDIM[kid][0] + 3))
+    return src, den, trg, dl
 
 
 def config1_inputs():
@@ -149,15 +167,18 @@ def reference_golden(force=False):
     from oracle.ref_fmm import refpvfmm as R
     if not R.available():
         subprocess.run(["bash", os.path.join(ROOT, "oracle", "ref_fmm", "build.sh")], check=True)
-    for name, (kid, m, mp, dist, n, sep, seed) in REFERENCE_CASES.items():
+    for name in REFERENCE_CASES:
+        kid, m, mp = case_spec(name)[:3]
         path = os.path.join(HERE, f"reference_{name}.npz")
         if not force and os.path.exists(path):
             continue
-        src, den, trg = reference_case_inputs(name)
-        out, tree, lists = R.ref_eval(kid, m, mp, src, den, trg)
-        np.savez_compressed(path, kernel=kid, m=m, max_pts=mp, src=src, den=den,
+        src, den, trg, dl = reference_case_inputs(name)
+        out, tree, lists = R.ref_eval(kid, m, mp, src, den, trg, dl=dl)
+        extra = {} if dl is None else {"dl": dl}     # an empty den means sl_den = NULL
+        np.savez_compressed(path, kernel=kid, m=m, max_pts=mp, src=src,
+                            den=np.zeros((0, KDIM[kid][0])) if den is None else den,
                             trg=np.zeros((0, 3)) if trg is None else trg, out=out,
-                            nodes=tree[:, :7].astype(np.int32), lists=lists[:, :4].astype(np.int32))
+                            nodes=tree[:, :7].astype(np.int32), lists=lists[:, :4].astype(np.int32), **extra)
     path = os.path.join(HERE, "reference_config1.npz")
     if force or not os.path.exists(path):
         x, q = config1_inputs()

@@ -378,3 +378,30 @@ def test_vlist_frequency_slabs_match_the_whole_spectrum(monkeypatch, prec, kid):
     # differently from one whole transform (measured 2e-7), within its bar
     tol = 1e-12 if prec == P.PRECISION_PLAIN else 1e-6
     assert O.rel_l2(sliced.reshape(-1), whole.reshape(-1)) < tol
+
+
+def test_double_layer_setup0_and_rejections():
+    """setup=0 with new double-layer values equals a fresh setup=1; a setup=0
+    call must pass the same densities as its setup; kernels without a
+    double-layer kernel reject dl_den with a message and NaN outputs."""
+    rng = np.random.default_rng(77)
+    src = points("gauss", 3000, 78)
+    trg = points("unif", 1000, 79)
+    sl = rng.uniform(-1, 1, 3000)
+    dl1 = rng.uniform(-1, 1, 3000 * 4)
+    dl2 = rng.uniform(-1, 1, 3000 * 4)
+    s, t = src.reshape(-1), trg.reshape(-1)
+    ctx = P.FMMParticleContext(-1, 40, 6, P.FMMKernel.LaplacePotential)
+    ctx.evaluate(s, sl, dl1, t, True)
+    again = ctx.evaluate(s, sl, dl2, t, False)
+    fresh = P.FMMParticleContext(-1, 40, 6, P.FMMKernel.LaplacePotential)
+    want = fresh.evaluate(s, sl, dl2, t, True)
+    assert O.rel_l2(again, want) < 1e-14
+    with pytest.raises(RuntimeError, match="same densities"):
+        ctx.evaluate(s, None, dl2, t, False)
+    ctx.close()
+    fresh.close()
+    g = P.FMMParticleContext(-1, 40, 6, P.FMMKernel.LaplaceGradient)
+    with pytest.raises(RuntimeError, match="double-layer"):
+        g.evaluate(s, sl, dl1, t, True)
+    g.close()

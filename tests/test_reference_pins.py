@@ -25,6 +25,18 @@ Two cases have wider bars, for reasons outside the algorithm:
   sum).  With the reference's own factors, read by the library from the
   precompute file the reference writes, the match is 6e-13; the live test
   below checks that whenever the reference library is built here.
+* Stokes with double-layer sources (1e-11, 1e-10): the same pseudo-inverse
+  spread, larger here because the double layer's check potentials (a 1/r^2
+  kernel) are larger (2.4e-12 and 2.5e-11 on the library's factors; 6.5e-13
+  and 1.1e-12 on the reference's own, checked live below).
+
+Four fixtures carry double-layer sources (dl_den, k0 + 3 values per point),
+alone or next to single-layer densities on the same points: they pin the
+double-layer kernels as the reference evaluates them (laplace_dbl_poten reads
+the first three values as the normal and the fourth as the density;
+stokes_sym_dip forms n.f as v0 v3 + v1 v1 + v2 v2), the scaling the reference
+gives them (pvfmm-wrapper.cpp:521-535) and the tree and lists that result when
+both point sets count (fmm_node.txx:81-92).
 
 When the reference library is built here (oracle/_ref), live cases on fresh
 points are compared the same way.
@@ -42,7 +54,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 FIXTURES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "reference_*.npz")) if "config1" not in f)
 LIST_NAMES = {8: "U0", 9: "U1", 10: "U2", 12: "W", 13: "X", 14: "V1"}
-TOL = {"reference_laplace_coincident_m4.npz": 1e-7, "reference_stokes_vel_gauss_m6.npz": 1e-11}
+TOL = {"reference_laplace_coincident_m4.npz": 1e-7, "reference_stokes_vel_gauss_m6.npz": 1e-11,
+       "reference_stokes_dl_m4.npz": 1e-11, "reference_stokes_sldl_gauss_m4.npz": 1e-10}
 
 _OPS = {}
 
@@ -80,13 +93,21 @@ def check_tree_and_lists(fmm, nodes, lists):
     assert ol == rl
 
 
+def fixture_densities(z):
+    """(sl_den, dl_den) of a fixture; an empty array or a missing one is NULL."""
+    den = z["den"] if len(z["den"]) else None
+    dl = z["dl"] if "dl" in z.files and len(z["dl"]) else None
+    return den, dl
+
+
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(f)[10:-4] for f in FIXTURES])
 def test_oracle_matches_reference(path):
     z = np.load(path)
     kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
-    src, den = z["src"], z["den"]
+    src = z["src"]
+    den, dl = fixture_densities(z)
     trg = z["trg"] if len(z["trg"]) else src
-    out, fmm = O.pvfmm_eval(kid, m, mp, src, den, trg, ops=library_ops(kid, m), return_fmm=True)
+    out, fmm = O.pvfmm_eval(kid, m, mp, src, den, trg, ops=library_ops(kid, m), return_fmm=True, dl_den=dl)
     check_tree_and_lists(fmm, z["nodes"], z["lists"])
     err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
     assert err < TOL.get(os.path.basename(path), 1e-12), err
@@ -119,23 +140,36 @@ def test_live_reference_matches_oracle():
     assert O.rel_l2(ours.reshape(-1), out.reshape(-1)) < 1e-12
 
 
-def test_library_reads_the_reference_precompute_file(tmp_path, monkeypatch):
+@pytest.mark.parametrize("name,tol", [("stokes_vel_gauss_m6", 1e-12), ("stokes_sldl_gauss_m4", 2e-12)])
+def test_library_reads_the_reference_precompute_file(tmp_path, monkeypatch, name, tol):
     """The library's operator cache reads the pseudo-inverse factors from the
     precompute file the reference itself writes (Precomp_<kernel>_m<m>.data in
     $PVFMM_DIR, include/precomp_mat.txx:213-300); with those factors the
-    oracle on the library's operators matches the reference to 1e-12 on the
-    Stokes m=6 case."""
+    oracle on the library's operators matches the reference to ~1e-12 on the
+    Stokes cases whose fixtures carry wider bars."""
     from oracle.ref_fmm import refpvfmm as R
     if not R.available():
         pytest.skip("reference library not built here (oracle/ref_fmm/build.sh)")
     monkeypatch.setenv("PVFMM_DIR", str(tmp_path))
-    z = np.load(os.path.join(GOLDEN, "reference_stokes_vel_gauss_m6.npz"))
-    src, den = z["src"], z["den"]
-    ctx = R.RefContext(3, 6, 80)            # writes $PVFMM_DIR/Precomp_stokes_vel_m6.data
-    out = ctx.evaluate(src, den, None)
+    z = np.load(os.path.join(GOLDEN, f"reference_{name}.npz"))
+    kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
+    src = z["src"]
+    den, dl = fixture_densities(z)
+    trg = z["trg"] if len(z["trg"]) else None
+    ctx = R.RefContext(kid, m, mp)          # writes $PVFMM_DIR/Precomp_stokes_vel_m<m>.data
+    out = ctx.evaluate(src, den, trg, dl=dl)
     ctx.close()
-    assert (tmp_path / "Precomp_stokes_vel_m6.data").exists()
+    assert (tmp_path / f"Precomp_stokes_vel_m{m}.data").exists()
     assert np.array_equal(out.reshape(-1), z["out"].reshape(-1))      # the reference is deterministic
-    ops = O.Operators.from_arrays(O.KERNELS[3], 6, P.precomp_operators(P.FMMKernel(3), 6, 0))
-    ours = O.pvfmm_eval(3, 6, 80, src, den, src, ops=ops)
-    assert O.rel_l2(ours.reshape(-1), out.reshape(-1)) < 1e-12
+    ops = O.Operators.from_arrays(O.KERNELS[kid], m, P.precomp_operators(P.FMMKernel(kid), m, 0))
+    ours = O.pvfmm_eval(kid, m, mp, src, den, src if trg is None else trg, ops=ops, dl_den=dl)
+    assert O.rel_l2(ours.reshape(-1), out.reshape(-1)) < tol
+
+
+def test_double_layer_needs_a_double_layer_kernel():
+    """The reference's LaplaceGradient has no double-layer source->target
+    kernel (its EvalListPts would call a null function); the oracle refuses."""
+    rng = np.random.default_rng(9)
+    x = rng.random((300, 3))
+    with pytest.raises(ValueError):
+        O.pvfmm_eval(1, 4, 40, x, None, x, dl_den=rng.uniform(-1, 1, (300, 4)))
