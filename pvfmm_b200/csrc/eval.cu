@@ -1403,6 +1403,167 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
   }
 }
 
+// ---------------------------------------------------------------------------
+// Hadamard products of the mixed form for 3-component expansions (Stokes
+// velocity, pressure and velocity gradient, Biot-Savart) on the tensor cores,
+// with the same TF32 3-term split as hadamard_tc_kernel.  Per frequency f and
+// group z of KOC output components:
+//   OUT[P][(j1, c, re|im)] += sum_o sum_(j2, i, re|im) IN[Q_o(P)][(j2, i, re|im)] B_o[..][(j1, c, re|im)]
+// a real GEMM with K = 48 (8 children x 3 components x re|im, 6 k-steps) and
+// N = 16 KOC (2 KOC n-tiles), B_o the real form of the complex block
+// M[f][o][(j1, c)][(j2, i)].  A warp owns 16 target parents (rows); lane
+// (g, t) loads the 16-byte pieces u = 0..2 at float 16u + 4t of the 48-float
+// input rows g and g+8, which are its A fragments for k-steps 2u and 2u+1
+// when the K order is chosen as k-step 2u+v, column c -> float
+// 16u + 4(c % 4) + 2v + c / 4.  The B fragments of an offset (18 KB for
+// KOC = 3) are too many to stage for all 26 offsets, so the block streams
+// them offset by offset into a double buffer in shared memory (cp.async,
+// one barrier per offset), shared by its 8 warps; offsets that no parent of
+// the block has are skipped, those that no parent of a warp has are skipped
+// by that warp.  Each pair of k-steps accumulates in a fresh fragment that
+// joins the running sum with a rounded FP32 add (see hadamard_tc_kernel).
+// ---------------------------------------------------------------------------
+constexpr int kTc3Warps = 8;
+
+template <int KOC>
+__global__ void __launch_bounds__(32 * kTc3Warps, 2)
+    hadamard_tc3_kernel(int n3h, long n_vtrg, long vt_stride, int ko, const int* __restrict__ vtab,
+                        const unsigned* __restrict__ vmask, const float4* __restrict__ spec_in,
+                        const float4* __restrict__ bfrag, float2* __restrict__ spec_out) {
+  constexpr int NNT = 2 * KOC;        // n-tiles of the group
+  constexpr int NB = 6 * NNT;         // (k-step, n-tile) fragment blocks per offset
+  constexpr int NP = kTc3Warps * 16;  // target parents of the block
+  extern __shared__ float4 Bs[];      // [2][NB][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
+  int* qs = reinterpret_cast<int*>(Bs + 2 * NB * 32);  // [26][NP] source parent of each (offset, parent)
+  unsigned* wl = reinterpret_cast<unsigned*>(qs + 26 * NP);  // [kTc3Warps] occupied offsets of each warp
+  const int f = blockIdx.y, z = blockIdx.z, ngroups = gridDim.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long pb = (long)blockIdx.x * NP;
+  for (int i = threadIdx.x; i < 26 * NP; i += 32 * kTc3Warps) {
+    const int o = i / NP;
+    const long p = pb + i % NP;
+    qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
+  }
+  {
+    const long p = pb + warp * 16 + (lane & 15);
+    unsigned m = (lane < 16 && p < n_vtrg) ? __ldg(vmask + p) : 0u;
+    m = __reduce_or_sync(0xffffffffu, m);
+    if (lane == 0) wl[warp] = m;
+  }
+  __syncthreads();
+  unsigned blive = 0;
+#pragma unroll
+  for (int w = 0; w < kTc3Warps; ++w) blive |= wl[w];
+  const unsigned wlive = wl[warp];
+  const float4* bsrc = bfrag + ((long)f * 26 * ngroups + z) * NB * 32;  // + o * ngroups * NB * 32
+  auto stage = [&](int o, int buf) {
+    const float4* src = bsrc + (long)o * ngroups * NB * 32;
+    float4* dst = Bs + buf * NB * 32;
+    for (int i = threadIdx.x; i < NB * 32; i += 32 * kTc3Warps) cp_async16(dst + i, src + i, 16);
+  };
+  const int w0 = warp * 16;
+  auto load = [&](int o, float4 (&x)[3][2]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = qs[o * NP + w0 + g + 8 * h];
+      const float4* row = spec_in + ((long)(q < 0 ? 0 : q) * n3h + f) * 12 + t;
+#pragma unroll
+      for (int u = 0; u < 3; ++u) x[u][h] = q >= 0 ? __ldg(row + 4 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  float acc[NNT][4];
+#pragma unroll
+  for (int nt = 0; nt < NNT; ++nt)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[nt][i] = 0.f;
+  float4 xn[3][2];
+  unsigned rem = blive;
+  int oc = rem ? __ffs(rem) - 1 : 0;
+  if (rem) {
+    stage(oc, 0);
+    if (wlive >> oc & 1u) load(oc, xn);
+  }
+  cp_async_commit();
+#pragma unroll 1
+  for (int k = 0; rem; ++k) {
+    rem &= rem - 1;
+    const int on = rem ? __ffs(rem) - 1 : -1;
+    cp_async_wait<0>();  // this thread's copies of offset oc have landed
+    __syncthreads();     // everyone's have; every warp is done with the other buffer
+    if (on >= 0) stage(on, (k + 1) & 1);
+    cp_async_commit();
+    if (wlive >> oc & 1u) {
+      unsigned ah[6][4], al[6][4];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        tf32_split(xn[u][0].x, ah[2 * u][0], al[2 * u][0]);
+        tf32_split(xn[u][1].x, ah[2 * u][1], al[2 * u][1]);
+        tf32_split(xn[u][0].y, ah[2 * u][2], al[2 * u][2]);
+        tf32_split(xn[u][1].y, ah[2 * u][3], al[2 * u][3]);
+        tf32_split(xn[u][0].z, ah[2 * u + 1][0], al[2 * u + 1][0]);
+        tf32_split(xn[u][1].z, ah[2 * u + 1][1], al[2 * u + 1][1]);
+        tf32_split(xn[u][0].w, ah[2 * u + 1][2], al[2 * u + 1][2]);
+        tf32_split(xn[u][1].w, ah[2 * u + 1][3], al[2 * u + 1][3]);
+      }
+      if (on >= 0 && (wlive >> on & 1u)) load(on, xn);  // the next offset's rows, in flight meanwhile
+      const float4* bq = Bs + (k & 1) * NB * 32 + lane;
+#pragma unroll
+      for (int nt = 0; nt < NNT; ++nt)
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+            const int sk = 2 * u + v;
+            const float4 b = bq[(sk * NNT + nt) * 32];
+            const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
+            const unsigned bl0 = __float_as_uint(b.z), bl1 = __float_as_uint(b.w);
+            mma_tf32_16x8x8(d, al[sk], bh0, bh1);
+            mma_tf32_16x8x8(d, ah[sk], bl0, bl1);
+            mma_tf32_16x8x8(d, ah[sk], bh0, bh1);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[nt][i] += d[i];
+        }
+    } else if (on >= 0 && (wlive >> on & 1u)) {
+      load(on, xn);
+    }
+    oc = on;
+  }
+  cp_async_wait<0>();
+  // C fragment: (row g, cols 2t, 2t+1) and (row g+8, same cols); columns
+  // nt*8 + 2t (+1) are the re (im) part of output element e = 4nt + t =
+  // j1 * KOC + c of the group.
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const long p = pb + w0 + g + 8 * h;
+    if (p >= n_vtrg) continue;
+    float2* out = spec_out + (p * n3h + f) * (8 * ko) + z * KOC;
+#pragma unroll
+    for (int nt = 0; nt < NNT; ++nt) {
+      const int e = 4 * nt + t;
+      out[(e / KOC) * ko + e % KOC] = make_float2(acc[nt][2 * h], acc[nt][2 * h + 1]);
+    }
+  }
+}
+
+template <int KOC>
+void launch_hadamard_tc3(Context& ctx, int n3h, long f_base, int ko, const Cplx<float>* sin_, Cplx<float>* sout,
+                         long p0, long np) {
+  DevTree& T = ctx.tree;
+  constexpr int NB = 12 * KOC, NP = kTc3Warps * 16;
+  const int ngroups = ko / KOC;
+  const size_t sm = (size_t)2 * NB * 32 * sizeof(float4) + (size_t)26 * NP * sizeof(int) + kTc3Warps * sizeof(int);
+  PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc3_kernel<KOC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(ceil_div(np, (long)NP), n3h, ngroups);
+  ++ctx.n_launch;
+  hadamard_tc3_kernel<KOC><<<grid, 32 * kTc3Warps, sm, ctx.stream>>>(
+      n3h, np, T.n_vtrg, ko, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
+      reinterpret_cast<const float4*>(sin_), ctx.dops.vop_frag.get<float4>() + f_base * 26 * ngroups * NB * 32,
+      reinterpret_cast<float2*>(sout));
+}
+
 // Target parents [p0, p0 + np) of the V-list; sout holds their rows.
 void launch_hadamard_tc(Context& ctx, int n3h, long f_base, const Cplx<float>* sin_, Cplx<float>* sout, long p0,
                         long np) {
@@ -1516,6 +1677,13 @@ bool use_tc5(const Context&) {
   const char* e = std::getenv("PVFMM_B200_HADAMARD");
   return e && std::strcmp(e, "tcgen05") == 0;
 }
+// Mixed-form Hadamard of 3-component expansions: tensor cores
+// (hadamard_tc3_kernel), or with PVFMM_B200_HADAMARD3=simt the FP32 SIMT
+// kernel (hadamard_kernel).
+bool use_simt3() {
+  const char* e = std::getenv("PVFMM_B200_HADAMARD3");
+  return e && std::strcmp(e, "simt") == 0;
+}
 
 template <class Real, int M>
 void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
@@ -1548,6 +1716,11 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
         if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
         else if (use_tc5(ctx)) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
         else launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
+      } else if (sizeof(Real) == 4 && !use_simt3()) {  // mixed form, 3-component expansions: tensor cores
+        if constexpr (sizeof(Real) == 4) {
+          if (kout == 1) launch_hadamard_tc3<1>(ctx, n3h, f_base, 1, sin_, sout, p0, np);
+          else launch_hadamard_tc3<3>(ctx, n3h, f_base, kout, sin_, sout, p0, np);
+        }
       } else if (kout == 3) {  // Stokes velocity, Biot-Savart
         launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
       } else if (kout == 1) {  // Stokes pressure
@@ -1880,6 +2053,47 @@ static void upload_vop_fragments(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
 }
 
+// B fragments of hadamard_tc3_kernel: for frequency f, offset o, output group
+// z (KOC components), block (k-step s = 2u + v, n-tile nt) and lane (g, t):
+// b0 = B[(e_in, re)][(e_out, re|im)], b1 = B[(e_in, im)][(e_out, re|im)] with
+// input element e_in = 8u + 2t + v = j2 * 3 + i, output element
+// e_out = 4 nt + g / 2 = j1 * KOC + c (component z KOC + c), re|im = g % 2;
+// stored as [f][o][z][block][lane] float4 = (b0 hi, b1 hi, b0 lo, b1 lo).
+// Built on the device from the FP32 operator blocks vop[f][o][j1][j2][i][c].
+__global__ void vop3_fragments_kernel(long n, int ko, int koc, const float2* __restrict__ vop,
+                                      float4* __restrict__ frag) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int nnt = 2 * koc, nb = 6 * nnt, ngroups = ko / koc;
+  const int lane = (int)(idx % 32);
+  const int blk = (int)(idx / 32 % nb);
+  const long fo = idx / 32 / nb / ngroups;  // f * 26 + o
+  const int z = (int)(idx / 32 / nb % ngroups);
+  const int sk = blk / nnt, nt = blk % nnt;
+  const int g = lane >> 2, t = lane & 3, u = sk >> 1, v = sk & 1;
+  const int e_in = 8 * u + 2 * t + v, e_out = 4 * nt + g / 2, pout = g & 1;
+  const int j2 = e_in / 3, i = e_in % 3, j1 = e_out / koc, c = z * koc + e_out % koc;
+  const float2 mv = vop[((fo * 8 + j1) * 8 + j2) * 3 * ko + i * ko + c];
+  const float b0 = pout == 0 ? mv.x : mv.y;   // from (e_in, re)
+  const float b1 = pout == 0 ? -mv.y : mv.x;  // from (e_in, im)
+  unsigned h0, l0, h1, l1;
+  tf32_split(b0, h0, l0);
+  tf32_split(b1, h1, l1);
+  frag[idx] = make_float4(__uint_as_float(h0), __uint_as_float(h1), __uint_as_float(l0), __uint_as_float(l1));
+}
+
+static void upload_vop3_fragments(Context& ctx) {
+  const HostOperators& h = ctx.hops;
+  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  const int ko = h.kout, koc = ko == 1 ? 1 : 3;
+  const long n = (long)n3h * 26 * (ko / koc) * (12 * koc) * 32;
+  float4* dev = ctx.dops.vop_frag.as<float4>(n);
+  ++ctx.n_launch;
+  vop3_fragments_kernel<<<ceil_div(n, 256L), 256, 0, ctx.stream>>>(n, ko, koc, ctx.dops.vop.get<float2>(), dev);
+  PVFMM_CUDA_CHECK(cudaGetLastError());
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+}
+
 void upload_operators(Context& ctx) {
   const HostOperators& h = ctx.hops;
   auto s = ctx.stream;
@@ -1908,6 +2122,7 @@ void upload_operators(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(fm, h.fft_map.data(), h.fft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(im, h.ifft_map.data(), h.ifft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (ctx.precision == 1 && ctx.ki.ke == 3) upload_vop3_fragments(ctx);  // from the uploaded FP32 vop
 }
 
 void evaluate(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float) {

@@ -62,7 +62,7 @@ struct DevTree {
 // Device copies of the operators in the working precision.
 struct DevOps {
   DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
-  DevBuf vop_frag;  // mixed form, ke = 1: Hadamard operators as TF32 hi/lo MMA fragments
+  DevBuf vop_frag;  // mixed form: Hadamard operators as TF32 hi/lo MMA fragments
   DevBuf vop_tc5;   // mixed form, ke = 1: Hadamard operators in the tcgen05 shared-memory layout
   DevBuf ue_proj;   // mixed form: projector applied to the upward equivalent densities
   DevBuf usurf;     // ns x 3 (Real)

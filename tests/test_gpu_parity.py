@@ -360,7 +360,28 @@ def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
         assert O.rel_l2(a[:, k], b[:, k]) < 1e-7, k
 
 
-@pytest.mark.parametrize("prec,kid", [(P.PRECISION_PLAIN, 6), (P.PRECISION_MIXED, 6), (P.PRECISION_PLAIN, 3)])
+@pytest.mark.parametrize("kid", [3, 2, 4, 5])
+def test_tensor_core_hadamard_of_vector_expansions_agrees_with_simt(monkeypatch, kid):
+    """The mixed form's V-list products of the 3-component expansions (Stokes
+    velocity, pressure, velocity gradient; Biot-Savart) on the tensor cores
+    (TF32 3-term split, K = 48, streamed operator fragments) and in FP32 SIMT
+    give the same FMM result to well within the mixed form's accuracy."""
+    K = O.KERNELS[kid]
+    src = points("gauss", 20000, 43)
+    den = np.random.default_rng(44).uniform(-1, 1, (20000, K.k0))
+    monkeypatch.setenv("PVFMM_B200_HADAMARD3", "simt")
+    a, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=P.PRECISION_MIXED)
+    assert ctx.tree_stats()["n_vtrg"] > 100
+    ctx.close()
+    monkeypatch.delenv("PVFMM_B200_HADAMARD3")
+    b, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=P.PRECISION_MIXED)
+    ctx.close()
+    for k in range(K.k1):
+        assert O.rel_l2(b[:, k], a[:, k]) < 2e-7, k
+
+
+@pytest.mark.parametrize("prec,kid", [(P.PRECISION_PLAIN, 6), (P.PRECISION_MIXED, 6), (P.PRECISION_PLAIN, 3),
+                                      (P.PRECISION_MIXED, 3)])
 def test_vlist_frequency_slabs_match_the_whole_spectrum(monkeypatch, prec, kid):
     """When the source parents' spectra do not fit in device memory the V-list
     runs in slabs of kz: each slab's forward DFT rows, products and inverse-DFT
