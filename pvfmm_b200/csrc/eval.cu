@@ -385,6 +385,26 @@ __device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
 template <int Ker>
 constexpr bool kHasPacked = Ker == kKerLaplace || Ker == kKerLaplaceGrad || Ker == kKerLaplacePG || Ker == kKerStokes;
 
+// Packed records (one source density): every value stored twice, (v, v), so
+// that a 16-byte shared-memory load yields two f32x2 operands with no register
+// moves to duplicate them: chunks (x, x, y, y) (z, z, f, f) (xl, xl, yl, yl)
+// (zl, zl, 0, 0).
+#ifndef PVFMM_NEAR_DUP
+#define PVFMM_NEAR_DUP 1
+#endif
+template <class Real, int Ker>
+constexpr bool kDupRec = PVFMM_NEAR_DUP && sizeof(Real) == 4 && kHasPacked<Ker> && KerDims<Ker>::KS == 1;
+constexpr int kDupNC = 4;  // 16-byte chunks of a packed record
+
+__device__ __forceinline__ void rec_store_dup(float4* tile, int j, double x, double y, double z, float f) {
+  const float xh = (float)x, yh = (float)y, zh = (float)z;
+  const float xl = (float)(x - (double)xh), yl = (float)(y - (double)yh), zl = (float)(z - (double)zh);
+  tile[0 * kTile + j] = make_float4(xh, xh, yh, yh);
+  tile[1 * kTile + j] = make_float4(zh, zh, f, f);
+  tile[2 * kTile + j] = make_float4(xl, xl, yl, yl);
+  tile[3 * kTile + j] = make_float4(zl, zl, 0.f, 0.f);
+}
+
 // ker_eval<Ker, float> for two targets at once: r = target - source per half,
 // f the source densities (the same in both halves).  1/r: one hardware
 // reciprocal square root per half (0 for r2 == 0) and one packed
@@ -421,6 +441,40 @@ __device__ __forceinline__ void ker_eval_x2(f2_t rx, f2_t ry, f2_t rz, const f2_
     u[0] = f2_fma(y, f2_fma(rx, ip, f[0]), u[0]);
     u[1] = f2_fma(y, f2_fma(ry, ip, f[1]), u[1]);
     u[2] = f2_fma(y, f2_fma(rz, ip, f[2]), u[2]);
+  }
+}
+
+// rec_sum2_x2 on packed records (kDupRec).
+template <int Ker>
+__device__ __forceinline__ void rec_sum2_dup(const float4* tile, int n, int j0, int js, const Pt<float>& pa,
+                                             const Pt<float>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
+  constexpr int KT = KerDims<Ker>::KT;
+  const f2_t px = f2_pack(pa.x, pb.x), py = f2_pack(pa.y, pb.y), pz = f2_pack(pa.z, pb.z);
+  const f2_t pxl = f2_pack(pa.xl, pb.xl), pyl = f2_pack(pa.yl, pb.yl), pzl = f2_pack(pa.zl, pb.zl);
+  const ulonglong2* t2 = reinterpret_cast<const ulonglong2*>(tile);
+  const int step = 16 * js;
+  for (int jb = j0; jb < n; jb += step) {
+    const int jend = min(n, jb + step);
+    f2_t u[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) u[k] = 0ull;
+#pragma unroll kNearUnroll
+    for (int j = jb; j < jend; j += js) {
+      const ulonglong2 c0 = t2[0 * kTile + j], c1 = t2[1 * kTile + j];
+      const ulonglong2 c2 = t2[2 * kTile + j], c3 = t2[3 * kTile + j];
+      const f2_t rx = f2_add(f2_sub(px, c0.x), f2_sub(pxl, c2.x));
+      const f2_t ry = f2_add(f2_sub(py, c0.y), f2_sub(pyl, c2.y));
+      const f2_t rz = f2_add(f2_sub(pz, c1.x), f2_sub(pzl, c3.x));
+      const f2_t f[1] = {c1.y};
+      ker_eval_x2<Ker>(rx, ry, rz, f, u);
+    }
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+      float a, b;
+      f2_unpack(u[k], a, b);
+      acc[0][k] += (double)a;
+      acc[1][k] += (double)b;
+    }
   }
 }
 
@@ -492,8 +546,9 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
                       int with_p2p, double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   constexpr bool kF32 = sizeof(Real) == 4;
+  constexpr bool kDup = kDupRec<Real, Ker>;
   using V = typename Vec16<Real>::type;
-  __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
+  __shared__ V tiles[2][(kDup ? kDupNC : Rec<Real, KS>::NC) * kTile];
   __shared__ double2 tile64[kF32 && !kDbl ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
   // the partial sums of the final fixed-order reduction reuse the tiles
   static_assert(sizeof(tiles) >= sizeof(double) * kNF * 2 * KT, "reduction buffer larger than the tiles");
@@ -653,13 +708,15 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
             Real f[KS];
 #pragma unroll
             for (int c = 0; c < KS; ++c) f[c] = (Real)rf_[u][c];
-            rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
+            if constexpr (kDup) rec_store_dup(tiles[buf], j, rx_[u], ry_[u], rz_[u], (float)f[0]);
+            else rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
           }
         }
         if (t + 1 < ntile) fetch(t + 1);
         __syncthreads();  // tiles[buf] complete; tiles[buf^1] no longer read (its readers passed this barrier)
         if (active) {
-          if constexpr (kF32 && kHasPacked<Ker>) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pa, pb, acc);
+          if constexpr (kDup) rec_sum2_dup<Ker>(tiles[buf], n, g, G, pa, pb, acc);
+          else if constexpr (kF32 && kHasPacked<Ker>) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pa, pb, acc);
           else rec_sum2<Real, Ker>(tiles[buf], n, g, G, pa, pb, acc);
         }
         buf ^= 1;
