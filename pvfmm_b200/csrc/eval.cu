@@ -232,6 +232,9 @@ constexpr int kNF = 128;        // threads per near-field block
 #ifndef PVFMM_NEAR_MIN_BLOCKS_F32
 #define PVFMM_NEAR_MIN_BLOCKS_F32 5  // resident blocks per SM the register budget is sized for
 #endif
+#ifndef PVFMM_NEAR_MIN_BLOCKS_F32_K1
+#define PVFMM_NEAR_MIN_BLOCKS_F32_K1 6  // the same for one source density (Laplace kernels)
+#endif
 #ifndef PVFMM_NEAR_MIN_BLOCKS_F64
 #define PVFMM_NEAR_MIN_BLOCKS_F64 5
 #endif
@@ -241,6 +244,10 @@ constexpr int kNF = 128;        // threads per near-field block
 #ifndef PVFMM_NEAR_UNROLL
 #define PVFMM_NEAR_UNROLL 1
 #endif
+#ifndef PVFMM_NEAR_GMAX
+#define PVFMM_NEAR_GMAX 16  // most thread groups splitting the source records of a small leaf
+#endif
+
 constexpr int kNearUnroll = PVFMM_NEAR_UNROLL;      // unroll of the record loop
 constexpr int kTile = PVFMM_NEAR_TILE_MULT * kNF;  // source records per tile
 constexpr int kRPT = kTile / kNF;                   // records each thread fetches per tile
@@ -385,26 +392,6 @@ __device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
 template <int Ker>
 constexpr bool kHasPacked = Ker == kKerLaplace || Ker == kKerLaplaceGrad || Ker == kKerLaplacePG || Ker == kKerStokes;
 
-// Packed records (one source density): every value stored twice, (v, v), so
-// that a 16-byte shared-memory load yields two f32x2 operands with no register
-// moves to duplicate them: chunks (x, x, y, y) (z, z, f, f) (xl, xl, yl, yl)
-// (zl, zl, 0, 0).
-#ifndef PVFMM_NEAR_DUP
-#define PVFMM_NEAR_DUP 1
-#endif
-template <class Real, int Ker>
-constexpr bool kDupRec = PVFMM_NEAR_DUP && sizeof(Real) == 4 && kHasPacked<Ker> && KerDims<Ker>::KS == 1;
-constexpr int kDupNC = 4;  // 16-byte chunks of a packed record
-
-__device__ __forceinline__ void rec_store_dup(float4* tile, int j, double x, double y, double z, float f) {
-  const float xh = (float)x, yh = (float)y, zh = (float)z;
-  const float xl = (float)(x - (double)xh), yl = (float)(y - (double)yh), zl = (float)(z - (double)zh);
-  tile[0 * kTile + j] = make_float4(xh, xh, yh, yh);
-  tile[1 * kTile + j] = make_float4(zh, zh, f, f);
-  tile[2 * kTile + j] = make_float4(xl, xl, yl, yl);
-  tile[3 * kTile + j] = make_float4(zl, zl, 0.f, 0.f);
-}
-
 // ker_eval<Ker, float> for two targets at once: r = target - source per half,
 // f the source densities (the same in both halves).  1/r: one hardware
 // reciprocal square root per half (0 for r2 == 0) and one packed
@@ -441,40 +428,6 @@ __device__ __forceinline__ void ker_eval_x2(f2_t rx, f2_t ry, f2_t rz, const f2_
     u[0] = f2_fma(y, f2_fma(rx, ip, f[0]), u[0]);
     u[1] = f2_fma(y, f2_fma(ry, ip, f[1]), u[1]);
     u[2] = f2_fma(y, f2_fma(rz, ip, f[2]), u[2]);
-  }
-}
-
-// rec_sum2_x2 on packed records (kDupRec).
-template <int Ker>
-__device__ __forceinline__ void rec_sum2_dup(const float4* tile, int n, int j0, int js, const Pt<float>& pa,
-                                             const Pt<float>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
-  constexpr int KT = KerDims<Ker>::KT;
-  const f2_t px = f2_pack(pa.x, pb.x), py = f2_pack(pa.y, pb.y), pz = f2_pack(pa.z, pb.z);
-  const f2_t pxl = f2_pack(pa.xl, pb.xl), pyl = f2_pack(pa.yl, pb.yl), pzl = f2_pack(pa.zl, pb.zl);
-  const ulonglong2* t2 = reinterpret_cast<const ulonglong2*>(tile);
-  const int step = 16 * js;
-  for (int jb = j0; jb < n; jb += step) {
-    const int jend = min(n, jb + step);
-    f2_t u[KT];
-#pragma unroll
-    for (int k = 0; k < KT; ++k) u[k] = 0ull;
-#pragma unroll kNearUnroll
-    for (int j = jb; j < jend; j += js) {
-      const ulonglong2 c0 = t2[0 * kTile + j], c1 = t2[1 * kTile + j];
-      const ulonglong2 c2 = t2[2 * kTile + j], c3 = t2[3 * kTile + j];
-      const f2_t rx = f2_add(f2_sub(px, c0.x), f2_sub(pxl, c2.x));
-      const f2_t ry = f2_add(f2_sub(py, c0.y), f2_sub(pyl, c2.y));
-      const f2_t rz = f2_add(f2_sub(pz, c1.x), f2_sub(pzl, c3.x));
-      const f2_t f[1] = {c1.y};
-      ker_eval_x2<Ker>(rx, ry, rz, f, u);
-    }
-#pragma unroll
-    for (int k = 0; k < KT; ++k) {
-      float a, b;
-      f2_unpack(u[k], a, b);
-      acc[0][k] += (double)a;
-      acc[1][k] += (double)b;
-    }
   }
 }
 
@@ -535,7 +488,9 @@ constexpr int kSegCap = 128;  // list entries per batch
 // added to pot.  with_p2p = 0: no P2P sources (no single-layer densities;
 // the W and D2T entries still come from the expansions).
 template <class Real, int Ker, bool kDbl = false>
-__global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS_F32 : PVFMM_NEAR_MIN_BLOCKS_F64)
+__global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_BLOCKS_F64
+                                       : KerDims<Ker>::KS == 1 ? PVFMM_NEAR_MIN_BLOCKS_F32_K1
+                                                               : PVFMM_NEAR_MIN_BLOCKS_F32)
     near_field_kernel(const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo,
                       const int* __restrict__ thi, const int* __restrict__ slo, const int* __restrict__ shi,
                       const int* __restrict__ p_off, const int* __restrict__ p_list, const int* __restrict__ w_off,
@@ -546,13 +501,14 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
                       int with_p2p, double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   constexpr bool kF32 = sizeof(Real) == 4;
-  constexpr bool kDup = kDupRec<Real, Ker>;
+  constexpr bool kPacked = kF32 && kHasPacked<Ker>;
+  constexpr int TPT = 2;  // targets per thread
   using V = typename Vec16<Real>::type;
-  __shared__ V tiles[2][(kDup ? kDupNC : Rec<Real, KS>::NC) * kTile];
+  __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
   __shared__ double2 tile64[kF32 && !kDbl ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
   // the partial sums of the final fixed-order reduction reuse the tiles
-  static_assert(sizeof(tiles) >= sizeof(double) * kNF * 2 * KT, "reduction buffer larger than the tiles");
-  double(*red)[2][KT] = reinterpret_cast<double(*)[2][KT]>(&tiles[0][0]);
+  static_assert(sizeof(tiles) >= sizeof(double) * kNF * TPT * KT, "reduction buffer larger than the tiles");
+  double(*red)[TPT][KT] = reinterpret_cast<double(*)[TPT][KT]>(&tiles[0][0]);
   __shared__ NearSeg seg[kSegCap];
   __shared__ int start[kSegCap + 1];
   const int b = blockIdx.x;
@@ -567,19 +523,26 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
   const int nD = (!kDbl && de && !kF32) ? 1 : 0;  // plain form: D2T is a segment of the stream
   const int n_ent = nD + nW + nP;
   int buf = 0;
-  for (int c0 = 0; c0 < nt; c0 += 2 * kNF) {
-    const int m = min(2 * kNF, nt - c0);
-    const int nc = (m + 1) >> 1;
-    const int G = min(8, kNF / nc);
+  for (int c0 = 0; c0 < nt; c0 += TPT * kNF) {
+    // thread (ti, g): targets ti + q nc (q < TPT) of the chunk, source records
+    // g, g + G, ... of every tile
+    const int m = min(TPT * kNF, nt - c0);
+    const int nc = (m + TPT - 1) / TPT;
+    const int G = min(PVFMM_NEAR_GMAX, kNF / nc);
     const int ti = threadIdx.x % nc, g = threadIdx.x / nc;
     const bool active = g < G;
-    const bool vb = ti + nc < m;
-    const int ta = t0 + c0 + ti, tb = vb ? ta + nc : ta;
-    const Pt<Real> pa = make_pt<Real>(tx[ta], ty[ta], tz[ta]);
-    const Pt<Real> pb = make_pt<Real>(tx[tb], ty[tb], tz[tb]);
-    double acc[2][KT];
+    int tq[TPT];
+    Pt<Real> pt[TPT];
 #pragma unroll
-    for (int k = 0; k < KT; ++k) acc[0][k] = acc[1][k] = 0;
+    for (int q = 0; q < TPT; ++q) {
+      tq[q] = t0 + c0 + (ti + q * nc < m ? ti + q * nc : ti);  // a missing target repeats the first
+      pt[q] = make_pt<Real>(tx[tq[q]], ty[tq[q]], tz[tq[q]]);
+    }
+    double acc[TPT][KT];
+#pragma unroll
+    for (int q = 0; q < TPT; ++q)
+#pragma unroll
+      for (int k = 0; k < KT; ++k) acc[q][k] = 0;
     // D2T of the mixed form: the downward equivalent densities come from the
     // FP64-cutoff pseudo-inverse, whose large cancelling components only FP64
     // sums resolve, so they are evaluated from FP64 records.
@@ -587,8 +550,6 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
       if (de) {
         const double hr = half * kRad1;
         const double* dens = de + (long)b * dim;
-        const Pt<double> pa64 = make_pt<double>(tx[ta], ty[ta], tz[ta]);
-        const Pt<double> pb64 = make_pt<double>(tx[tb], ty[tb], tz[tb]);
         for (int k0 = 0; k0 < ns; k0 += kTile) {
           const int n = min(kTile, ns - k0);
           __syncthreads();
@@ -600,7 +561,14 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
             rec_store<double, KS>(tile64, i, hr * usurf[k * 3 + 0], hr * usurf[k * 3 + 1], hr * usurf[k * 3 + 2], f);
           }
           __syncthreads();
-          if (active) rec_sum2<double, Ker, true>(tile64, n, g, G, pa64, pb64, acc);
+          if (active)
+#pragma unroll
+            for (int h = 0; h < TPT / 2; ++h) {
+              const Pt<double> pa64 = make_pt<double>(tx[tq[2 * h]], ty[tq[2 * h]], tz[tq[2 * h]]);
+              const Pt<double> pb64 = make_pt<double>(tx[tq[2 * h + 1]], ty[tq[2 * h + 1]], tz[tq[2 * h + 1]]);
+              rec_sum2<double, Ker, true>(tile64, n, g, G, pa64, pb64,
+                                          *reinterpret_cast<double(*)[2][KT]>(&acc[2 * h][0]));
+            }
         }
       }
     }
@@ -708,16 +676,14 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
             Real f[KS];
 #pragma unroll
             for (int c = 0; c < KS; ++c) f[c] = (Real)rf_[u][c];
-            if constexpr (kDup) rec_store_dup(tiles[buf], j, rx_[u], ry_[u], rz_[u], (float)f[0]);
-            else rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
+            rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
           }
         }
         if (t + 1 < ntile) fetch(t + 1);
         __syncthreads();  // tiles[buf] complete; tiles[buf^1] no longer read (its readers passed this barrier)
         if (active) {
-          if constexpr (kDup) rec_sum2_dup<Ker>(tiles[buf], n, g, G, pa, pb, acc);
-          else if constexpr (kF32 && kHasPacked<Ker>) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pa, pb, acc);
-          else rec_sum2<Real, Ker>(tiles[buf], n, g, G, pa, pb, acc);
+          if constexpr (kPacked) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pt[0], pt[1], acc);
+          else rec_sum2<Real, Ker>(tiles[buf], n, g, G, pt[0], pt[1], acc);
         }
         buf ^= 1;
       }
@@ -727,22 +693,21 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 4 ? PVFMM_NEAR_MIN_BLOCKS
     __syncthreads();
     if (active)
 #pragma unroll
-      for (int k = 0; k < KT; ++k) {
-        red[threadIdx.x][0][k] = acc[0][k];
-        red[threadIdx.x][1][k] = acc[1][k];
-      }
+      for (int q = 0; q < TPT; ++q)
+#pragma unroll
+        for (int k = 0; k < KT; ++k) red[threadIdx.x][q][k] = acc[q][k];
     __syncthreads();
     if (active && g == 0) {
 #pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        if (t == 1 && !vb) break;
+      for (int q = 0; q < TPT; ++q) {
+        if (ti + q * nc >= m) break;
         double sum[KT];
 #pragma unroll
-        for (int k = 0; k < KT; ++k) sum[k] = red[ti][t][k];
+        for (int k = 0; k < KT; ++k) sum[k] = red[ti][q][k];
         for (int gg = 1; gg < G; ++gg)
 #pragma unroll
-          for (int k = 0; k < KT; ++k) sum[k] += red[gg * nc + ti][t][k];
-        const long o = (long)(t0 + c0 + ti + (t ? nc : 0)) * KT;
+          for (int k = 0; k < KT; ++k) sum[k] += red[gg * nc + ti][q][k];
+        const long o = (long)(t0 + c0 + ti + q * nc) * KT;
 #pragma unroll
         for (int k = 0; k < KT; ++k) pot[o + k] = kDbl ? pot[o + k] + sum[k] * scale : sum[k] * scale;
       }
