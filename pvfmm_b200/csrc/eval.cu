@@ -1121,6 +1121,7 @@ __global__ void __launch_bounds__(128) hadamard_kernel(int n3h, long n_vtrg, lon
 template <class Real, int PB>
 __global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc,
                                                              const int* __restrict__ vtab,
+                                                             const unsigned* __restrict__ vmask,
                                                           const Cplx<Real>* __restrict__ spec_in,
                                                           const Cplx<Real>* __restrict__ vop,
                                                           Cplx<Real>* __restrict__ spec_out) {
@@ -1197,16 +1198,32 @@ __global__ void __launch_bounds__(128, 4) hadamard_rd_kernel(int n3h, long n_vtr
       }
     }
   };
-  // two register sets in turn: the gathers of offset o+1 are in flight while
-  // offset o is multiplied (26 offsets, an even count)
-  load(0, xc, mc);
-  __syncthreads();
+  __syncthreads();  // Ms staged
+  // the offsets occupied for any parent of the warp, in increasing order (the
+  // targets are ordered by occupied-offset pattern, so the others are
+  // common); two register sets in turn: the gathers of the next offset are in
+  // flight while one is multiplied
+  unsigned pm = 0;
+#pragma unroll
+  for (int k = 0; k < PB; ++k) pm |= pin[k] ? __ldg(vmask + prow[k]) : 0u;
+  unsigned rem = __reduce_or_sync(0xffffffffu, pm);
+  const int nlive = __popc(rem);
+  auto take = [&]() {
+    const int o = __ffs(rem) - 1;
+    rem &= rem - 1;
+    return o;
+  };
+  int oc = nlive > 0 ? take() : 0;
+  if (nlive > 0) load(oc, xc, mc);
 #pragma unroll 1
-  for (int o = 0; o < 26; o += 2) {
-    load(o + 1, xn, mn);
-    compute(o, xc, mc);
-    if (o + 2 < 26) load(o + 2, xc, mc);
-    compute(o + 1, xn, mn);
+  for (int i = 0; i < nlive; i += 2) {
+    const int on = i + 1 < nlive ? take() : -1;
+    if (on >= 0) load(on, xn, mn);
+    compute(oc, xc, mc);
+    const int onn = i + 2 < nlive ? take() : -1;
+    if (onn >= 0) load(onn, xc, mc);
+    if (on >= 0) compute(on, xn, mn);
+    oc = onn;
   }
 #pragma unroll
   for (int k = 0; k < PB; ++k) {
@@ -1586,6 +1603,131 @@ void launch_hadamard_tc3(Context& ctx, int n3h, long f_base, int ko, const Cplx<
       reinterpret_cast<float2*>(sout));
 }
 
+// ---------------------------------------------------------------------------
+// Hadamard products of the plain form for 3-component expansions on the FP64
+// tensor cores (mma.sync m8n8k4 .f64).  The same real GEMM per frequency f and
+// output group z as hadamard_tc3_kernel, K = 48 in 12 k-steps of 4, N = 16 KOC
+// in 2 KOC n-tiles of 8, in FP64 with no split.  A warp owns 8 target parents
+// (rows); lane (g, t) holds row g, and with the K order k-step s, column
+// c -> double 12c + s its A values for all 12 k-steps are the contiguous
+// doubles 12t .. 12t+11 of the row (6 16-byte loads).  The B fragments of an
+// offset (18 KB for KOC = 3) are streamed offset by offset into a double
+// buffer in shared memory (cp.async, one barrier per offset) shared by the
+// block's 8 warps; offsets no parent of the block has are skipped, those no
+// parent of a warp has are skipped by that warp.
+// ---------------------------------------------------------------------------
+constexpr int kDmWarps = 8;
+
+template <int KOC>
+__global__ void __launch_bounds__(32 * kDmWarps, 2)
+    hadamard_dmma3_kernel(int n3h, long n_vtrg, long vt_stride, int ko, const int* __restrict__ vtab,
+                          const unsigned* __restrict__ vmask, const double2* __restrict__ spec_in,
+                          const double* __restrict__ bfrag, double2* __restrict__ spec_out) {
+  constexpr int NNT = 2 * KOC;       // n-tiles of the group
+  constexpr int NB = 12 * NNT;       // (k-step, n-tile) fragment blocks per offset
+  constexpr int NP = kDmWarps * 8;   // target parents of the block
+  extern __shared__ double Bd[];     // [2][NB][32 lanes]
+  int* qs = reinterpret_cast<int*>(Bd + 2 * NB * 32);  // [26][NP]
+  unsigned* wl = reinterpret_cast<unsigned*>(qs + 26 * NP);  // [kDmWarps]
+  const int f = blockIdx.y, z = blockIdx.z, ngroups = gridDim.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long pb = (long)blockIdx.x * NP;
+  for (int i = threadIdx.x; i < 26 * NP; i += 32 * kDmWarps) {
+    const int o = i / NP;
+    const long p = pb + i % NP;
+    qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
+  }
+  {
+    const long p = pb + warp * 8 + (lane & 7);
+    unsigned m = (lane < 8 && p < n_vtrg) ? __ldg(vmask + p) : 0u;
+    m = __reduce_or_sync(0xffffffffu, m);
+    if (lane == 0) wl[warp] = m;
+  }
+  __syncthreads();
+  unsigned blive = 0;
+#pragma unroll
+  for (int w = 0; w < kDmWarps; ++w) blive |= wl[w];
+  const unsigned wlive = wl[warp];
+  const double* bsrc = bfrag + ((long)f * 26 * ngroups + z) * NB * 32;
+  auto stage = [&](int o, int buf) {
+    const double2* src = reinterpret_cast<const double2*>(bsrc + (long)o * ngroups * NB * 32);
+    double2* dst = reinterpret_cast<double2*>(Bd + buf * NB * 32);
+    for (int i = threadIdx.x; i < NB * 16; i += 32 * kDmWarps) cp_async16(dst + i, src + i, 16);
+  };
+  const int w0 = warp * 8;
+  auto load = [&](int o, double2 (&x)[6]) {
+    const int q = qs[o * NP + w0 + g];
+    const double2* row = spec_in + ((long)(q < 0 ? 0 : q) * n3h + f) * 24 + 6 * t;
+#pragma unroll
+    for (int u = 0; u < 6; ++u) x[u] = q >= 0 ? __ldg(row + u) : make_double2(0.0, 0.0);
+  };
+  double acc[NNT][2];
+#pragma unroll
+  for (int nt = 0; nt < NNT; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
+  double2 xc[6], xn[6];
+  unsigned rem = blive;
+  int oc = rem ? __ffs(rem) - 1 : 0;
+  if (rem) {
+    stage(oc, 0);
+    if (wlive >> oc & 1u) load(oc, xn);
+  }
+  cp_async_commit();
+#pragma unroll 1
+  for (int k = 0; rem; ++k) {
+    rem &= rem - 1;
+    const int on = rem ? __ffs(rem) - 1 : -1;
+    cp_async_wait<0>();  // this thread's copies of offset oc have landed
+    __syncthreads();     // everyone's have; every warp is done with the other buffer
+    if (on >= 0) stage(on, (k + 1) & 1);
+    cp_async_commit();
+    if (wlive >> oc & 1u) {
+#pragma unroll
+      for (int u = 0; u < 6; ++u) xc[u] = xn[u];
+      if (on >= 0 && (wlive >> on & 1u)) load(on, xn);  // the next offset's row, in flight meanwhile
+      const double* bq = Bd + (k & 1) * NB * 32 + lane;
+#pragma unroll
+      for (int sk = 0; sk < 12; ++sk) {
+        const double a = sk & 1 ? xc[sk >> 1].y : xc[sk >> 1].x;
+#pragma unroll
+        for (int nt = 0; nt < NNT; ++nt) dmma(acc[nt], a, bq[(sk * NNT + nt) * 32]);
+      }
+    } else if (on >= 0 && (wlive >> on & 1u)) {
+      load(on, xn);
+    }
+    oc = on;
+  }
+  cp_async_wait<0>();
+  // C fragment: (row g, cols 2t, 2t+1): the re and im part of output element
+  // e = 4 nt + t = j1 * KOC + c of the group
+  const long p = pb + w0 + g;
+  if (p < n_vtrg) {
+    double2* out = spec_out + (p * n3h + f) * (8 * ko) + z * KOC;
+#pragma unroll
+    for (int nt = 0; nt < NNT; ++nt) {
+      const int e = 4 * nt + t;
+      out[(e / KOC) * ko + e % KOC] = make_double2(acc[nt][0], acc[nt][1]);
+    }
+  }
+}
+
+template <int KOC>
+void launch_hadamard_dmma3(Context& ctx, int n3h, long f_base, int ko, const Cplx<double>* sin_, Cplx<double>* sout,
+                           long p0, long np) {
+  DevTree& T = ctx.tree;
+  constexpr int NB = 24 * KOC, NP = kDmWarps * 8;
+  const int ngroups = ko / KOC;
+  const size_t sm = (size_t)2 * NB * 32 * sizeof(double) + (size_t)26 * NP * sizeof(int) + kDmWarps * sizeof(int);
+  PVFMM_CUDA_CHECK(
+      cudaFuncSetAttribute(hadamard_dmma3_kernel<KOC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(ceil_div(np, (long)NP), n3h, ngroups);
+  ++ctx.n_launch;
+  hadamard_dmma3_kernel<KOC><<<grid, 32 * kDmWarps, sm, ctx.stream>>>(
+      n3h, np, T.n_vtrg, ko, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
+      reinterpret_cast<const double2*>(sin_), ctx.dops.vop_frag.get<double>() + f_base * 26 * ngroups * NB * 32,
+      reinterpret_cast<double2*>(sout));
+}
+
 // Target parents [p0, p0 + np) of the V-list; sout holds their rows.
 void launch_hadamard_tc(Context& ctx, int n3h, long f_base, const Cplx<float>* sin_, Cplx<float>* sout, long p0,
                         long np) {
@@ -1608,7 +1750,8 @@ void launch_hadamard_rd(Context& ctx, int n3h, long f_base, const Cplx<Real>* si
   DevTree& T = ctx.tree;
   dim3 grid(ceil_div(np, 128 * PB), n3h);
   ++ctx.n_launch;
-  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0, sin_,
+  hadamard_rd_kernel<Real, PB><<<grid, 128, 0, ctx.stream>>>(n3h, np, T.n_vtrg, T.n_vsrc, T.vtab.get<int>() + p0,
+                                                             T.vmask.get<unsigned>() + p0, sin_,
                                                              ctx.dops.vop.get<Cplx<Real>>() + f_base * 26 * 64, sout);
 }
 
@@ -1699,9 +1842,9 @@ bool use_tc5(const Context&) {
   const char* e = std::getenv("PVFMM_B200_HADAMARD");
   return e && std::strcmp(e, "tcgen05") == 0;
 }
-// Mixed-form Hadamard of 3-component expansions: tensor cores
-// (hadamard_tc3_kernel), or with PVFMM_B200_HADAMARD3=simt the FP32 SIMT
-// kernel (hadamard_kernel).
+// Hadamard of 3-component expansions: tensor cores (hadamard_tc3_kernel in
+// the mixed form, hadamard_dmma3_kernel in the plain form), or with
+// PVFMM_B200_HADAMARD3=simt the SIMT kernel (hadamard_kernel).
 bool use_simt3() {
   const char* e = std::getenv("PVFMM_B200_HADAMARD3");
   return e && std::strcmp(e, "simt") == 0;
@@ -1738,10 +1881,13 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
         if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
         else if (use_tc5(ctx)) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
         else launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
-      } else if (sizeof(Real) == 4 && !use_simt3()) {  // mixed form, 3-component expansions: tensor cores
+      } else if (!use_simt3()) {  // 3-component expansions: tensor cores (TF32 x3 or FP64)
         if constexpr (sizeof(Real) == 4) {
           if (kout == 1) launch_hadamard_tc3<1>(ctx, n3h, f_base, 1, sin_, sout, p0, np);
           else launch_hadamard_tc3<3>(ctx, n3h, f_base, kout, sin_, sout, p0, np);
+        } else {
+          if (kout == 1) launch_hadamard_dmma3<1>(ctx, n3h, f_base, 1, sin_, sout, p0, np);
+          else launch_hadamard_dmma3<3>(ctx, n3h, f_base, kout, sin_, sout, p0, np);
         }
       } else if (kout == 3) {  // Stokes velocity, Biot-Savart
         launch_hadamard<Real, 3, 3, 3, 4>(ctx, n3h, f_base, sin_, sout, p0, np);
@@ -2104,6 +2250,45 @@ __global__ void vop3_fragments_kernel(long n, int ko, int koc, const float2* __r
   frag[idx] = make_float4(__uint_as_float(h0), __uint_as_float(h1), __uint_as_float(l0), __uint_as_float(l1));
 }
 
+// B fragments of hadamard_dmma3_kernel: for frequency f, offset o, output
+// group z, block (k-step s, n-tile nt) and lane (g, t): b = B[k][n] with
+// k = double 12t + s of the input row (element e_in = k / 2 = j2 * 3 + i,
+// re|im = k % 2) and n = 8 nt + g (element e_out = n / 2 = j1 * KOC + c,
+// re|im = g % 2); stored as [f][o][z][block][lane] doubles.  Built on the
+// device from the FP64 operator blocks.
+__global__ void vop_dmma3_fragments_kernel(long n, int ko, int koc, const double2* __restrict__ vop,
+                                           double* __restrict__ frag) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int nnt = 2 * koc, nb = 12 * nnt, ngroups = ko / koc;
+  const int lane = (int)(idx % 32);
+  const int blk = (int)(idx / 32 % nb);
+  const int z = (int)(idx / 32 / nb % ngroups);
+  const long fo = idx / 32 / nb / ngroups;  // f * 26 + o
+  const int sk = blk / nnt, nt = blk % nnt;
+  const int g = lane >> 2, t = lane & 3;
+  const int k = 12 * t + sk, e_in = k / 2, pin = k % 2;
+  const int e_out = 4 * nt + g / 2, pout = g & 1;
+  const int j2 = e_in / 3, i = e_in % 3, j1 = e_out / koc, c = z * koc + e_out % koc;
+  const double2 mv = vop[((fo * 8 + j1) * 8 + j2) * 3 * ko + i * ko + c];
+  // real form of the complex product: [re; im] of the input times
+  // [[Re, Im], [-Im, Re]] gives [re; im] of the output
+  frag[idx] = pin == 0 ? (pout == 0 ? mv.x : mv.y) : (pout == 0 ? -mv.y : mv.x);
+}
+
+static void upload_vop_dmma3_fragments(Context& ctx) {
+  const HostOperators& h = ctx.hops;
+  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  const int ko = h.kout, koc = ko == 1 ? 1 : 3;
+  const long n = (long)n3h * 26 * (ko / koc) * (24 * koc) * 32;
+  double* dev = ctx.dops.vop_frag.as<double>(n);
+  ++ctx.n_launch;
+  vop_dmma3_fragments_kernel<<<ceil_div(n, 256L), 256, 0, ctx.stream>>>(n, ko, koc, ctx.dops.vop.get<double2>(),
+                                                                         dev);
+  PVFMM_CUDA_CHECK(cudaGetLastError());
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+}
+
 static void upload_vop3_fragments(Context& ctx) {
   const HostOperators& h = ctx.hops;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);
@@ -2145,6 +2330,7 @@ void upload_operators(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(im, h.ifft_map.data(), h.ifft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
   if (ctx.precision == 1 && ctx.ki.ke == 3) upload_vop3_fragments(ctx);  // from the uploaded FP32 vop
+  if (ctx.precision == 0 && ctx.ki.ke == 3) upload_vop_dmma3_fragments(ctx);  // from the uploaded FP64 vop
 }
 
 void evaluate(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float) {

@@ -45,13 +45,6 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// D (8x8) += A (8x4, row) * B (4x8, col).  Lane l = 4g + t holds
-// a = A[g][t], b = B[t][g], d = (D[g][2t], D[g][2t+1]).
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
-}
 
 struct RowMap {
   const int* rows;  // nullptr: identity

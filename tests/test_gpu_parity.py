@@ -360,27 +360,30 @@ def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
         assert O.rel_l2(a[:, k], b[:, k]) < 1e-7, k
 
 
+@pytest.mark.parametrize("prec", [P.PRECISION_MIXED, P.PRECISION_PLAIN])
 @pytest.mark.parametrize("kid", [3, 2, 4, 5])
-def test_tensor_core_hadamard_of_vector_expansions_agrees_with_simt(monkeypatch, kid):
-    """The mixed form's V-list products of the 3-component expansions (Stokes
-    velocity, pressure, velocity gradient; Biot-Savart) on the tensor cores
-    (TF32 3-term split, K = 48, streamed operator fragments) and in FP32 SIMT
-    give the same FMM result within the mixed form's accuracy (3e-7 apart on
-    this case: both round each product to FP32 accuracy, the SIMT kernel in
-    FP32 FMA chains over 624 terms, the tensor cores through the split
-    products and fresh accumulators)."""
+def test_tensor_core_hadamard_of_vector_expansions_agrees_with_simt(monkeypatch, kid, prec):
+    """The V-list products of the 3-component expansions (Stokes velocity,
+    pressure, velocity gradient; Biot-Savart) on the tensor cores (mixed: TF32
+    3-term split, plain: FP64; K = 48, streamed operator fragments) and in SIMT
+    give the same FMM result: to rounding in the plain form, within the mixed
+    form's accuracy in the mixed one (3e-7 apart on this case: both round each
+    product to FP32 accuracy, the SIMT kernel in FP32 FMA chains over 624
+    terms, the tensor cores through the split products and fresh
+    accumulators)."""
     K = O.KERNELS[kid]
     src = points("gauss", 20000, 43)
     den = np.random.default_rng(44).uniform(-1, 1, (20000, K.k0))
     monkeypatch.setenv("PVFMM_B200_HADAMARD3", "simt")
-    a, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=P.PRECISION_MIXED)
+    a, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=prec)
     assert ctx.tree_stats()["n_vtrg"] > 100
     ctx.close()
     monkeypatch.delenv("PVFMM_B200_HADAMARD3")
-    b, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=P.PRECISION_MIXED)
+    b, ctx = gpu_eval(kid, 6, 40, src, den, src, prec=prec)
     ctx.close()
+    tol = 1e-6 if prec == P.PRECISION_MIXED else 1e-13
     for k in range(K.k1):
-        assert O.rel_l2(b[:, k], a[:, k]) < 1e-6, k
+        assert O.rel_l2(b[:, k], a[:, k]) < tol, k
 
 
 @pytest.mark.parametrize("prec,kid", [(P.PRECISION_PLAIN, 6), (P.PRECISION_MIXED, 6), (P.PRECISION_PLAIN, 3),
