@@ -62,6 +62,12 @@ WORKLOADS = {
     "ellipsoid30m": dict(kernel=0, m=8, max_pts=128, n=30_000_000, gen="ellipsoid", seeds=(41, 42), check_seed=44,
                          n_check=1000, desc="laplace potential FMM (setup=1 per step), {n} points uniform by area on "
                                             "the (0.45, 0.3, 0.15) ellipsoid, m=8, 128/leaf"),
+    # the differentiable Laplace potential: one step = forward (pot+grad FMM)
+    # + backward (swapped-role FMM on the forward's tree) through
+    # pvfmm_b200.autograd.LaplaceFMM, sources = targets
+    "autograd1m": dict(kernel=6, m=8, max_pts=256, n=1_000_000, gen="uniform", seeds=(31, 32), check_seed=33,
+                       n_check=500, desc="differentiable laplace potential (forward + backward, autograd), {n} "
+                                         "uniform points, m=8, 256/leaf"),
 }
 W = WORKLOADS["gaussian4m"]
 KDIM = {0: (1, 1), 3: (3, 3), 6: (1, 4)}          # kernel id -> (k0, k1)
@@ -472,6 +478,68 @@ def build_line(args, world, N, forms, peaks):
     }
 
 
+def run_autograd(args, world, torch, barrier, max_over_ranks):
+    """Forward + backward of the differentiable Laplace potential
+    (pvfmm_b200.autograd.LaplaceFMM, mixed form) on one set of points: per
+    step phi = FMM(y, q), L = <g, phi>, L.backward() (a swapped-role FMM on the
+    forward's octree).  The gradients are checked against an FP64 direct sum
+    on a sample of points before the timed steps."""
+    from pvfmm_b200.autograd import LaplaceFMM
+    N = args.n
+    x, q = make_points(W, N)
+    y = torch.tensor(x, device="cuda", requires_grad=True)
+    d = torch.tensor(np.ascontiguousarray(q.reshape(-1)), device="cuda", requires_grad=True)
+    g = torch.tensor(np.random.default_rng(W["check_seed"]).uniform(-1, 1, N), device="cuda")
+    fmm = LaplaceFMM(max_points=W["max_pts"], multipole_order=W["m"], precision="mixed")
+
+    def step():
+        y.grad = None
+        d.grad = None
+        phi = fmm(y, d)
+        (phi * g).sum().backward()
+
+    try:
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        # dL/dq_j = sum_i G(y_j - y_i) g_i; dL/dy_j adds the source role,
+        # q_j sum_i g_i (y_i - y_j) / (4 pi r^3), and the target role,
+        # g_j grad phi(y_j) = -g_j sum_i q_i (y_j - y_i) / (4 pi r^3): direct
+        # sums with densities g and q, evaluated at a sample of the points
+        idx = np.random.default_rng(W["check_seed"] + 1).choice(N, W["n_check"], replace=False)
+        ref = direct_gpu(torch, 6, x, g.cpu().numpy(), idx)   # [G g, sum g r / r^3] at the sample
+        ref_q = direct_gpu(torch, 6, x, q, idx)                 # [G q, sum q r / r^3]
+        got_q = d.grad.cpu().numpy()[idx]
+        got_y = y.grad.cpu().numpy()[idx]
+        want_y = -q.reshape(-1)[idx, None] * ref[:, 1:] - g.cpu().numpy()[idx, None] * ref_q[:, 1:]
+        err_q = float(np.linalg.norm(got_q - ref[:, 0]) / np.linalg.norm(ref[:, 0]))
+        err_y = float(np.linalg.norm(got_y - want_y) / np.linalg.norm(want_y))
+        clocks = ClockSampler(torch.cuda.current_device())
+        barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        cl = clocks.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    finally:
+        fmm.close()
+    value = job_throughput(world, N, ms)
+    return {"metric": "targets/s differentiable Laplace FMM (forward + backward), rel-L2 of the gradients vs FP64 "
+                      "direct", "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": W["desc"].format(n=N) + ", form=mixed",
+                       "l2": "no flush: per-step working set exceeds the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "rel_l2_grad_den": err_q, "rel_l2_grad_pos": err_y, "clocks": cl,
+            "e2e": None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -502,6 +570,13 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
     barrier, max_over_ranks = rank_tools(world, "cuda")
+    if args.workload == "autograd1m":
+        line = run_autograd(args, world, torch, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     N = args.n
     kid = W["kernel"]
