@@ -355,7 +355,7 @@ def cpu_baseline(args):
 TRAFFIC_1M = {
     ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
     ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
-    ("near_field", 4): {"bytes": 149441536 + 24975104, "units": 1000000},        # near_field_kernel<float>
+    ("near_field", 4): {"bytes": 149489664 + 25314816, "units": 1000000},        # near_field_kernel<float>
     ("near_field", 8): {"bytes": 151890688 + 20192256, "units": 1000000},        # near_field_kernel<double>
 }
 # kernel that computes the V-list Hadamard products: (real bytes, ke) -> name
