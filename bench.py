@@ -354,15 +354,16 @@ def cpu_baseline(args):
 # the Hadamard kernels, n_trg for the near field.
 TRAFFIC_1M = {
     ("hadamard", 4): {"bytes": 844786176 + 671260416, "units": 4768 + 4767},     # hadamard_tc_kernel
-    ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},   # hadamard_rd_kernel<double>
+    # hadamard_rd_kernel<double> capture; hadamard_dmma1_kernel reads and writes the same spectra
+    ("hadamard", 8): {"bytes": 1470638080 + 1367394304, "units": 4768 + 4767},
     ("near_field", 4): {"bytes": 149489664 + 25314816, "units": 1000000},        # near_field_kernel<float>
     ("near_field", 8): {"bytes": 151890688 + 20192256, "units": 1000000},        # near_field_kernel<double>
 }
 # kernel that computes the V-list Hadamard products: (real bytes, ke) -> name
 HADAMARD_KERNEL = {(4, 1): "hadamard_tc_kernel (V-list M2L, TF32 mma.sync x3 split)",
-                   (8, 1): "hadamard_rd_kernel<double> (V-list M2L)",
-                   (4, 3): "hadamard_kernel<float, 3, 3> (V-list M2L)",
-                   (8, 3): "hadamard_kernel<double, 3, 3> (V-list M2L)"}
+                   (8, 1): "hadamard_dmma1_kernel (V-list M2L, FP64 mma.sync m8n8k4)",
+                   (4, 3): "hadamard_tc3_kernel<3> (V-list M2L, TF32 mma.sync x3 split)",
+                   (8, 3): "hadamard_dmma3_kernel<3> (V-list M2L, FP64 mma.sync m8n8k4)"}
 NEAR_KERNEL = "near_field_kernel (U-list P2P + W + D2T)"
 
 
@@ -381,8 +382,9 @@ def roofline(B, peaks):
       output spectra written once) + 26 * n3h * 64 * 2 * rb (operators read
       once) against the measured copy bandwidth; its tensor view (mixed form:
       the split issues 3 TF32 products per product, against a dense TF32 peak
-      of half the measured bf16 peak) or FP64 SIMT view (plain form) is the
-      `compute` sub-object.
+      of half the measured bf16 peak) or FP64 tensor view (plain form, against
+      the nominal FP64 peak, the same for the FP64 tensor cores and the FP64
+      pipe) is the `compute` sub-object.
     `traffic` is the ncu DRAM traffic of a launch scaled from 1M points."""
     st = B["stats"]
     rb = B["real_bytes"]
@@ -407,7 +409,7 @@ def roofline(B, peaks):
     had_flops = 512.0 * ke * ke * n3h * st["v_pairs"]
     had_gbs = had_bytes / (had_ms / 1000) / 1e9 if had_ms > 0 else 0.0
     had_tf = had_flops / (had_ms / 1000) / 1e12 if had_ms > 0 else 0.0
-    tensor = rb == 4 and ke == 1
+    tensor = rb == 4
     had = {"kernel": HADAMARD_KERNEL[(rb, ke)], "bound": "hbm", "achieved": had_gbs, "peak": hbm_peak, "unit": "GB/s",
            "frac": had_gbs / hbm_peak, "peak_source": peak_src,
            "traffic": traffic("hadamard", st["n_vsrc"] + st["n_vtrg"]), "algorithmic_bytes": had_bytes,
@@ -415,7 +417,7 @@ def roofline(B, peaks):
            "compute": ({"pipe": "tensor tf32 x3 (mma.sync)", "achieved_tflops": 3 * had_tf, "peak_tflops": tf32_peak,
                         "peak_source": "half the measured bf16 dense peak", "frac": 3 * had_tf / tf32_peak,
                         "algorithmic_flops": had_flops} if tensor else
-                       {"pipe": "fp32 simt" if rb == 4 else "fp64 simt", "achieved_tflops": had_tf,
+                       {"pipe": "fp64 tensor (mma.sync m8n8k4)", "achieved_tflops": had_tf,
                         "peak_tflops": simt_peak, "peak_source": "nominal", "frac": had_tf / simt_peak,
                         "algorithmic_flops": had_flops})}
     near_ms = B["stages_ms"]["near-field kernel"]

@@ -1711,6 +1711,146 @@ __global__ void __launch_bounds__(32 * kDmWarps, 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Hadamard products of the plain form for scalar expansions (ke = 1) on the
+// FP64 tensor cores: per frequency the real GEMM OUT[P][(j1, re|im)] +=
+// sum_o IN[Q_o(P)][(j2, re|im)] B_o[..][..] with K = N = 16 (4 k-steps, 2
+// n-tiles of mma.sync m8n8k4 .f64).  A warp owns MT tiles of 8 target parents;
+// with the K order k-step s, column t -> child 2t + s/2, re|im = s % 2, lane
+// (g, t) needs children 2t and 2t+1 of row g: two 16-byte pieces of the
+// piece-major input spectra (IN[f][child][Q], so the gathers of Morton-close
+// parents coalesce), gathered from L2 two offsets ahead.  A block stages its
+// frequency's B fragments (26 offsets, 53 KB) once and walks `chunks` chunks
+// of target parents; each warp walks only the offsets occupied for one of its
+// parents.
+// ---------------------------------------------------------------------------
+constexpr int kDm1Warps = 8;
+
+template <int MT>
+__global__ void __launch_bounds__(32 * kDm1Warps, 2)
+    hadamard_dmma1_kernel(int n3h, long n_vtrg, long vt_stride, long n_vsrc, int chunks, const int* __restrict__ vtab,
+                          const unsigned* __restrict__ vmask, const double2* __restrict__ spec_in,
+                          const double* __restrict__ bfrag, double2* __restrict__ spec_out) {
+  extern __shared__ double Bs1[];  // [26 offsets][8 blocks (s, nt)][32 lanes]
+  constexpr int NP = kDm1Warps * 8 * MT;  // target parents of a chunk
+  int* qs = reinterpret_cast<int*>(Bs1 + 26 * 8 * 32);  // [26][NP]
+  unsigned* ms = reinterpret_cast<unsigned*>(qs + 26 * NP);  // [NP]
+  const int f = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  {
+    const double2* src = reinterpret_cast<const double2*>(bfrag + (long)f * 26 * 8 * 32);
+    double2* dst = reinterpret_cast<double2*>(Bs1);
+    for (int i = threadIdx.x; i < 26 * 8 * 16; i += 32 * kDm1Warps) dst[i] = __ldg(src + i);
+  }
+  const double2* in0 = spec_in + ((long)f * 8 + 2 * t) * n_vsrc;  // child 2t; child 2t+1 at + n_vsrc
+  for (int c = 0; c < chunks; ++c) {
+    const long pb = ((long)blockIdx.x * chunks + c) * NP;
+    if (pb >= n_vtrg) break;
+    if (c > 0) __syncthreads();  // every warp is done with the previous chunk's qs
+    for (int i = threadIdx.x; i < 26 * NP; i += 32 * kDm1Warps) {
+      const int o = i / NP;
+      const long p = pb + i % NP;
+      qs[i] = p < n_vtrg ? __ldg(vtab + (long)o * vt_stride + p) : -1;
+    }
+    for (int i = threadIdx.x; i < NP; i += 32 * kDm1Warps) ms[i] = pb + i < n_vtrg ? __ldg(vmask + pb + i) : 0u;
+    __syncthreads();
+    const int w0 = warp * 8 * MT;
+    double acc[MT][2][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+    unsigned live = 0;
+    for (int k = lane; k < 8 * MT; k += 32) live |= ms[w0 + k];
+    live = __reduce_or_sync(0xffffffffu, live);
+    double2 xa[MT][2], xb[MT][2], xc[MT][2];
+    auto load = [&](int o, double2 (&x)[MT][2]) {
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const int q = qs[o * NP + w0 + mt * 8 + g];
+        x[mt][0] = q >= 0 ? __ldg(in0 + q) : make_double2(0.0, 0.0);
+        x[mt][1] = q >= 0 ? __ldg(in0 + n_vsrc + q) : make_double2(0.0, 0.0);
+      }
+    };
+    auto compute = [&](int o, const double2 (&x)[MT][2]) {
+      double b[4][2];
+#pragma unroll
+      for (int sk = 0; sk < 4; ++sk)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) b[sk][nt] = Bs1[((o * 4 + sk) * 2 + nt) * 32 + lane];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const double a[4] = {x[mt][0].x, x[mt][0].y, x[mt][1].x, x[mt][1].y};
+#pragma unroll
+        for (int sk = 0; sk < 4; ++sk)
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt) dmma(acc[mt][nt], a[sk], b[sk][nt]);
+      }
+    };
+    unsigned rem = live;
+    const int nlive = __popc(live);
+    auto take = [&]() {
+      const int o = __ffs(rem) - 1;
+      rem &= rem - 1;
+      return o;
+    };
+    int oa = 0, ob = 0, oc = 0;
+    if (nlive > 0) {
+      oa = take();
+      load(oa, xa);
+    }
+    if (nlive > 1) {
+      ob = take();
+      load(ob, xb);
+    }
+#pragma unroll 1
+    for (int i = 0; i < nlive; i += 3) {
+      if (i + 2 < nlive) {
+        oc = take();
+        load(oc, xc);
+      }
+      compute(oa, xa);
+      if (i + 3 < nlive) {
+        oa = take();
+        load(oa, xa);
+      }
+      if (i + 1 < nlive) compute(ob, xb);
+      if (i + 4 < nlive) {
+        ob = take();
+        load(ob, xb);
+      }
+      if (i + 2 < nlive) compute(oc, xc);
+    }
+    // C fragment: (row g, cols 2t, 2t+1) of n-tile nt = the re and im part of
+    // child j1 = 4 nt + t
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const long p = pb + w0 + mt * 8 + g;
+      if (p >= n_vtrg) continue;
+      double2* out = spec_out + (p * n3h + f) * 8;
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) out[4 * nt + t] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+    }
+  }
+}
+
+void launch_hadamard_dmma1(Context& ctx, int n3h, long f_base, const Cplx<double>* sin_, Cplx<double>* sout, long p0,
+                           long np) {
+  DevTree& T = ctx.tree;
+  constexpr int MT = 2;
+  const size_t sm = (size_t)26 * 8 * 32 * sizeof(double) + (size_t)27 * kDm1Warps * 8 * MT * sizeof(int);
+  PVFMM_CUDA_CHECK(
+      cudaFuncSetAttribute(hadamard_dmma1_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int chunks = 8;
+  dim3 grid(ceil_div(np, (long)8 * MT * kDm1Warps * chunks), n3h);
+  ++ctx.n_launch;
+  hadamard_dmma1_kernel<MT><<<grid, 32 * kDm1Warps, sm, ctx.stream>>>(
+      n3h, np, T.n_vtrg, T.n_vsrc, chunks, T.vtab.get<int>() + p0, T.vmask.get<unsigned>() + p0,
+      reinterpret_cast<const double2*>(sin_), ctx.dops.vop_frag.get<double>() + f_base * 26 * 8 * 32,
+      reinterpret_cast<double2*>(sout));
+}
+
 template <int KOC>
 void launch_hadamard_dmma3(Context& ctx, int n3h, long f_base, int ko, const Cplx<double>* sin_, Cplx<double>* sout,
                            long p0, long np) {
@@ -1849,6 +1989,13 @@ bool use_simt3() {
   const char* e = std::getenv("PVFMM_B200_HADAMARD3");
   return e && std::strcmp(e, "simt") == 0;
 }
+// Plain-form Hadamard of scalar expansions: FP64 tensor cores
+// (hadamard_dmma1_kernel), or with PVFMM_B200_HADAMARD=simt the FP64 SIMT
+// kernel (hadamard_rd_kernel).
+bool use_simt1() {
+  const char* e = std::getenv("PVFMM_B200_HADAMARD");
+  return e && std::strcmp(e, "simt") == 0;
+}
 
 template <class Real, int M>
 void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, Cplx<Real>* sout, int kin, int kout,
@@ -1878,7 +2025,10 @@ void vlist_fft_t(Context& ctx, const double* ue, double* dc, Cplx<Real>* sin_, C
     for (long p0 = 0; p0 < T.n_vtrg; p0 += chunk) {
       const long np = std::min(chunk, T.n_vtrg - p0);
       if (kin == 1 && kout == 1) {
-        if constexpr (sizeof(Real) == 8) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
+        if constexpr (sizeof(Real) == 8) {
+          if (use_simt1()) launch_hadamard_rd<Real, PVFMM_HAD_PB_F64>(ctx, n3h, f_base, sin_, sout, p0, np);
+          else launch_hadamard_dmma1(ctx, n3h, f_base, sin_, sout, p0, np);
+        }
         else if (use_tc5(ctx)) launch_hadamard_tc5(ctx, n3h, f_base, sin_, sout, p0, np);
         else launch_hadamard_tc(ctx, n3h, f_base, sin_, sout, p0, np);
       } else if (!use_simt3()) {  // 3-component expansions: tensor cores (TF32 x3 or FP64)
@@ -2276,6 +2426,31 @@ __global__ void vop_dmma3_fragments_kernel(long n, int ko, int koc, const double
   frag[idx] = pin == 0 ? (pout == 0 ? mv.x : mv.y) : (pout == 0 ? -mv.y : mv.x);
 }
 
+// B fragments of hadamard_dmma1_kernel: for frequency f, offset o, block
+// (k-step s, n-tile nt) and lane (g, t): b = B[k][n] with k = (child
+// 2t + s/2, re|im s % 2) and n = 8 nt + g (child 4 nt + g/2, re|im g % 2);
+// stored as [f][o][s][nt][lane] doubles.
+__global__ void vop_dmma1_fragments_kernel(long n, const double2* __restrict__ vop, double* __restrict__ frag) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int lane = (int)(idx % 32), nt = (int)(idx / 32 % 2), sk = (int)(idx / 64 % 4);
+  const long fo = idx / 256;  // f * 26 + o
+  const int g = lane >> 2, t = lane & 3;
+  const int j2 = 2 * t + (sk >> 1), pin = sk & 1, j1 = 4 * nt + g / 2, pout = g & 1;
+  const double2 mv = vop[(fo * 8 + j1) * 8 + j2];
+  frag[idx] = pin == 0 ? (pout == 0 ? mv.x : mv.y) : (pout == 0 ? -mv.y : mv.x);
+}
+
+static void upload_vop_dmma1_fragments(Context& ctx) {
+  const int m = ctx.m, n3h = 4 * m * m * (m + 1);
+  const long n = (long)n3h * 26 * 8 * 32;
+  double* dev = ctx.dops.vop_frag.as<double>(n);
+  ++ctx.n_launch;
+  vop_dmma1_fragments_kernel<<<ceil_div(n, 256L), 256, 0, ctx.stream>>>(n, ctx.dops.vop.get<double2>(), dev);
+  PVFMM_CUDA_CHECK(cudaGetLastError());
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+}
+
 static void upload_vop_dmma3_fragments(Context& ctx) {
   const HostOperators& h = ctx.hops;
   const int m = ctx.m, n3h = 4 * m * m * (m + 1);
@@ -2331,6 +2506,7 @@ void upload_operators(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));
   if (ctx.precision == 1 && ctx.ki.ke == 3) upload_vop3_fragments(ctx);  // from the uploaded FP32 vop
   if (ctx.precision == 0 && ctx.ki.ke == 3) upload_vop_dmma3_fragments(ctx);  // from the uploaded FP64 vop
+  if (ctx.precision == 0 && ctx.ki.ke == 1) upload_vop_dmma1_fragments(ctx);
 }
 
 void evaluate(Context& ctx, const void* den_in, const void* dl_in, bool den_float, void* out, bool out_float) {

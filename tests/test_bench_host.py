@@ -24,7 +24,7 @@ def test_roofline_objects_follow_the_contract(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     assert dom["kernel_ms"] >= nxt["kernel_ms"]
     by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
-    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_dmma1_kernel"]
     near = by["near_field_kernel"]
     # the Hadamard: HBM view against the measured copy bandwidth
     assert had["bound"] == "hbm" and had["unit"] == "GB/s" and had["peak"] == 6449.1
@@ -44,7 +44,7 @@ def test_roofline_objects_follow_the_contract(rb):
 def test_traffic_at_the_capture_size_is_the_capture(rb):
     dom, nxt = _run(rb, 3.26, 3.18)
     by = {r["kernel"].split()[0].split("<")[0]: r for r in (dom, nxt)}
-    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_rd_kernel"]
+    had = by["hadamard_tc_kernel" if rb == 4 else "hadamard_dmma1_kernel"]
     assert had["traffic"] == bench.TRAFFIC_1M[("hadamard", rb)]["bytes"]
     assert by["near_field_kernel"]["traffic"] == bench.TRAFFIC_1M[("near_field", rb)]["bytes"]
 

@@ -360,6 +360,25 @@ def test_tcgen05_hadamard_agrees_with_mma_sync_hadamard(monkeypatch):
         assert O.rel_l2(a[:, k], b[:, k]) < 1e-7, k
 
 
+@pytest.mark.parametrize("kid", [0, 6])
+def test_fp64_tensor_core_hadamard_agrees_with_simt(monkeypatch, kid):
+    """The plain form's scalar V-list products on the FP64 tensor cores
+    (mma.sync m8n8k4 .f64) and in FP64 SIMT give the same FMM result to FP64
+    rounding."""
+    K = O.KERNELS[kid]
+    src = points("gauss", 30000, 45)
+    den = np.random.default_rng(46).uniform(-1, 1, (30000, K.k0))
+    monkeypatch.setenv("PVFMM_B200_HADAMARD", "simt")
+    a, ctx = gpu_eval(kid, 8, 60, src, den, src, prec=P.PRECISION_PLAIN)
+    assert ctx.tree_stats()["n_vtrg"] > 100
+    ctx.close()
+    monkeypatch.delenv("PVFMM_B200_HADAMARD")
+    b, ctx = gpu_eval(kid, 8, 60, src, den, src, prec=P.PRECISION_PLAIN)
+    ctx.close()
+    for k in range(K.k1):
+        assert O.rel_l2(b[:, k], a[:, k]) < 1e-12, k
+
+
 @pytest.mark.parametrize("prec", [P.PRECISION_MIXED, P.PRECISION_PLAIN])
 @pytest.mark.parametrize("kid", [3, 2, 4, 5])
 def test_tensor_core_hadamard_of_vector_expansions_agrees_with_simt(monkeypatch, kid, prec):
