@@ -193,6 +193,14 @@ int PVFMMKernelEvalDeviceNoAllocD(enum PVFMMKernel kernel, const double* src_pos
  * Returns 0 on success. */
 int PVFMMSetUnitBox(void* ctx, int on);
 
+/* Layer-points mode (on != 0), for the reference C++ interface's separate
+ * single- and double-layer point sets (include/pvfmm.txx:216-244: src_coord
+ * and surf_coord both count in the leaf-size rule): the source points passed
+ * are the two sets concatenated, each carrying its own layer's values and
+ * zeros for the other, and every source point counts once in the tree.  The
+ * next evaluation rebuilds the tree.  Returns 0 on success. */
+int PVFMMSetLayerPoints(void* ctx, int on);
+
 /* Last error message of the calling thread ("" if none). */
 const char* PVFMMGetLastError(void);
 

@@ -19,7 +19,10 @@
 // As in the reference C++ interface (unlike PVFMMEval), coordinates must lie
 // in [0,1)^3 and are used as given: no bounding-box rescale and no seed grid
 // (the tree's point set is the targets, include/pvfmm.txx:229-240).
-// Differences: single rank; free space only; double-layer data must be empty.
+// Double-layer sources have their own point set (surf_coord, k0 + 3 values
+// per point) for the kernels with a double-layer kernel (LaplaceKernel<T>::
+// potential(), StokesKernel<T>::velocity()).
+// Differences: single rank; free space only.
 // Real = float runs the mixed-precision form.
 #ifndef PVFMM_B200_PVFMM_HPP_
 #define PVFMM_B200_PVFMM_HPP_
@@ -132,6 +135,11 @@ class PtFMM_Tree {
   PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
              const std::vector<Real>& trg_coord, int max_pts)
       : src_(src_coord), den_(src_value), trg_(trg_coord), max_pts_(max_pts) {}
+  // with a separate double-layer point set (surf_coord, k0 + 3 values per point)
+  PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
+             const std::vector<Real>& surf_coord, const std::vector<Real>& surf_value,
+             const std::vector<Real>& trg_coord, int max_pts)
+      : src_(src_coord), den_(src_value), surf_(surf_coord), dl_(surf_value), trg_(trg_coord), max_pts_(max_pts) {}
   ~PtFMM_Tree() { release(); }
   PtFMM_Tree(const PtFMM_Tree&) = delete;
   PtFMM_Tree& operator=(const PtFMM_Tree&) = delete;
@@ -143,25 +151,44 @@ class PtFMM_Tree {
     release();
     const Kernel<Real>* k = mat->kernel();
     if (!k) throw std::runtime_error("SetupFMM: PtFMM not initialized");
+    k0_ = k->ker_dim[0];
     k1_ = k->ker_dim[1];
     const int precision = std::is_same<Real, float>::value ? PVFMMPrecisionMixed : PVFMMPrecisionPlain;
     ctx_ = PVFMMCreateContextExD(-1.0, max_pts_, mat->MultipoleOrder(), k->id, precision);
     if (!ctx_) throw std::runtime_error(PVFMMGetLastError());
     if (PVFMMSetUnitBox(ctx_, 1) != 0) throw std::runtime_error(PVFMMGetLastError());
+    // both point sets count in the tree (include/fmm_node.txx:81-92): they are
+    // passed concatenated, each point with its own layer's values
+    if (!surf_.empty() && PVFMMSetLayerPoints(ctx_, 1) != 0) throw std::runtime_error(PVFMMGetLastError());
     needs_setup_ = true;
   }
   // Clears expansions between evaluations (reference FMM_Tree::ClearFMMData);
   // every evaluation here starts from cleared expansions.
   void ClearFMMData() {}
 
-  void evaluate(std::vector<Real>& trg_val, const std::vector<Real>* sl_density) {
+  void evaluate(std::vector<Real>& trg_val, const std::vector<Real>* sl_density,
+                const std::vector<Real>* dl_density = nullptr) {
     if (!ctx_) throw std::runtime_error("PtFMM_Evaluate: call SetupFMM first");
     if (sl_density) den_ = *sl_density;
-    const long ns = (long)src_.size() / 3, nt = (long)trg_.size() / 3;
-    std::vector<double> s(src_.begin(), src_.end()), d(den_.begin(), den_.end()), t(trg_.begin(), trg_.end());
+    if (dl_density) dl_ = *dl_density;
+    const long n_sl = (long)src_.size() / 3, n_dl = (long)surf_.size() / 3, nt = (long)trg_.size() / 3;
+    const long ns = n_sl + n_dl;
+    std::vector<double> s(src_.begin(), src_.end()), t(trg_.begin(), trg_.end());
+    s.insert(s.end(), surf_.begin(), surf_.end());
+    std::vector<double> d, dl;
+    if (n_dl == 0) {
+      d.assign(den_.begin(), den_.end());
+    } else {  // single-layer points then double-layer points, zeros for the other layer
+      if (den_.size() != (size_t)(n_sl * k0_) || dl_.size() != (size_t)(n_dl * (k0_ + 3)))
+        throw std::runtime_error("PtFMM_Evaluate: density sizes do not match the point sets");
+      d.assign((size_t)ns * k0_, 0.0);
+      std::copy(den_.begin(), den_.end(), d.begin());
+      dl.assign((size_t)ns * (k0_ + 3), 0.0);
+      std::copy(dl_.begin(), dl_.end(), dl.begin() + (size_t)n_sl * (k0_ + 3));
+    }
     std::vector<double> out((size_t)nt * k1_);
-    PVFMMEvalD(s.data(), d.empty() ? nullptr : d.data(), nullptr, ns, t.data(), out.data(), nt, ctx_,
-               needs_setup_ ? 1 : 0);
+    PVFMMEvalD(s.data(), d.empty() ? nullptr : d.data(), dl.empty() ? nullptr : dl.data(), ns, t.data(),
+               out.data(), nt, ctx_, needs_setup_ ? 1 : 0);
     const std::string err = PVFMMGetLastError();
     if (!err.empty()) throw std::runtime_error(err);
     needs_setup_ = false;
@@ -172,9 +199,9 @@ class PtFMM_Tree {
   void release() {
     if (ctx_) PVFMMDestroyContextD(&ctx_);
   }
-  std::vector<Real> src_, den_, trg_;
+  std::vector<Real> src_, den_, surf_, dl_, trg_;
   int max_pts_;
-  int k1_ = 1;
+  int k0_ = 1, k1_ = 1;
   void* ctx_ = nullptr;
   bool needs_setup_ = true;
 };
@@ -187,9 +214,7 @@ PtFMM_Tree<Real>* PtFMM_CreateTree(const std::vector<Real>& sl_coord, const std:
   (void)comm;
   (void)init_depth;
   if (bndry != FreeSpace) throw std::runtime_error("PtFMM_CreateTree: only FreeSpace is supported");
-  if (!dl_coord.empty() || !dl_density.empty())
-    throw std::runtime_error("PtFMM_CreateTree: double-layer sources are not supported");
-  return new PtFMM_Tree<Real>(sl_coord, sl_density, trg_coord, max_pts);
+  return new PtFMM_Tree<Real>(sl_coord, sl_density, dl_coord, dl_density, trg_coord, max_pts);
 }
 
 template <class Real>
@@ -206,8 +231,7 @@ template <class Real>
 void PtFMM_Evaluate(const PtFMM_Tree<Real>* tree, std::vector<Real>& trg_val, size_t loc_size = 0,
                     const std::vector<Real>* sl_density = nullptr, const std::vector<Real>* dl_density = nullptr) {
   (void)loc_size;
-  if (dl_density) throw std::runtime_error("PtFMM_Evaluate: double-layer densities are not supported");
-  const_cast<PtFMM_Tree<Real>*>(tree)->evaluate(trg_val, sl_density);
+  const_cast<PtFMM_Tree<Real>*>(tree)->evaluate(trg_val, sl_density, dl_density);
 }
 
 }  // namespace pvfmm

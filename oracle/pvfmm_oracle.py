@@ -1054,20 +1054,31 @@ def pvfmm_eval_setup0(fmm: "FMM", sl_den, dl_den=None) -> np.ndarray:
     return _eval_scaled(fmm, sl_den, dl_den)
 
 
-def ptfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None):
+def ptfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None, dl_pos=None, dl_den=None):
     """C++ interface: PtFMM_CreateTree + SetupFMM + PtFMM_Evaluate
     (pvfmm.txx:216-328).  Coordinates in [0,1)^3 are used as given (no
     bounding-box map, so no kernel-exponent scaling) and the tree's point set
-    is the targets."""
+    is the targets.  The double layer has its own point set (surf_coord,
+    dl_pos with k0 + 3 values per point, unscaled); both sets count in the
+    leaf-size rule and pt_cnt[0] (fmm_node.txx:81-92, fmm_pts.txx:1332-1333),
+    so they are evaluated as one source set, each point carrying its own
+    layer's values and zeros for the other (zero values add exact zeros)."""
     K = KERNELS[kernel_id]
     src_c = np.asarray(src_pos, dtype=np.float64).reshape(-1, 3)
     trg_c = np.asarray(trg_pos, dtype=np.float64).reshape(-1, 3)
+    sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
+    surf = None
+    if dl_pos is not None:
+        dl_c = np.asarray(dl_pos, dtype=np.float64).reshape(-1, 3)
+        dl_v = np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3)
+        surf = np.concatenate([np.zeros((len(src_c), K.k0 + 3)), dl_v])
+        sl_den = np.concatenate([sl_den, np.zeros((len(dl_c), K.k0))])
+        src_c = np.concatenate([src_c, dl_c])
     if src_c.min() < 0 or trg_c.min() < 0 or src_c.max() >= 1 or trg_c.max() >= 1:
         raise ValueError("coordinates must lie in [0,1)^3")
-    sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
     fmm = FMM(kernel_id, m, max_pts, ops)
     fmm.setup(src_c, trg_c, pt_coord="trg")
-    out_sorted = fmm.evaluate(sl_den[fmm.src_perm])
+    out_sorted = fmm.evaluate(sl_den[fmm.src_perm], None if surf is None else surf[fmm.src_perm])
     out = np.empty_like(out_sorted)
     out[fmm.trg_perm] = out_sorted
     return out

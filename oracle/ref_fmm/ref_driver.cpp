@@ -132,4 +132,33 @@ long ref_profile_report(char* buf, long cap) {
   return (long)table.size();
 }
 
+// The reference's C++ particle interface (include/pvfmm.txx:216-328): a tree
+// over single-layer points (n_sl, may be 0) and a separate double-layer point
+// set (n_dl, may be 0; k0 + 3 values per point) with the targets as the
+// tree's point set, coordinates in [0,1)^3 used as given, FreeSpace;
+// PtFMM_Evaluate writes n_trg * k1 values to out.  Returns 0, or 1 for an
+// unknown kernel.
+int ref_ptfmm_eval(int kernel, int m, int max_pts, long n_sl, const double* sl_coord, const double* sl_den,
+                   long n_dl, const double* dl_coord, const double* dl_den, long n_trg, const double* trg_coord,
+                   double* out) {
+  const pvfmm::Kernel<double>* ker = nullptr;
+  if (kernel == PVFMMLaplacePotential) ker = &pvfmm::LaplaceKernel<double>::potential();
+  if (kernel == PVFMMLaplaceGradient) ker = &pvfmm::LaplaceKernel<double>::gradient();
+  if (kernel == PVFMMStokesVelocity) ker = &pvfmm::StokesKernel<double>::velocity();
+  if (!ker) return 1;
+  const int k0 = ker->ker_dim[0], k1 = ker->ker_dim[1];
+  std::vector<double> sc(sl_coord, sl_coord + 3 * n_sl), sv(sl_den, sl_den + k0 * n_sl);
+  std::vector<double> dc(dl_coord, dl_coord + 3 * n_dl), dv(dl_den, dl_den + (k0 + 3) * n_dl);
+  std::vector<double> tc(trg_coord, trg_coord + 3 * n_trg);
+  pvfmm::PtFMM<double> matrices;
+  matrices.Initialize(m, MPI_COMM_WORLD, ker);
+  auto* tree = pvfmm::PtFMM_CreateTree(sc, sv, dc, dv, tc, MPI_COMM_WORLD, max_pts, pvfmm::FreeSpace);
+  tree->SetupFMM(&matrices);
+  std::vector<double> val;
+  pvfmm::PtFMM_Evaluate(tree, val, n_trg);
+  std::memcpy(out, val.data(), sizeof(double) * std::min<size_t>(val.size(), (size_t)n_trg * k1));
+  delete tree;
+  return 0;
+}
+
 }  // extern "C"

@@ -71,6 +71,8 @@ def load():
     lib.ref_profile_enable.argtypes = [ctypes.c_int]
     lib.ref_profile_report.restype = lg
     lib.ref_profile_report.argtypes = [vp, lg]
+    lib.ref_ptfmm_eval.restype = ctypes.c_int
+    lib.ref_ptfmm_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, lg, vp, vp, lg, vp, vp, lg, vp, vp]
     _lib = lib
     return lib
 
@@ -178,3 +180,24 @@ def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None):
         return out, ctx.tree(), ctx.lists()
     finally:
         ctx.close()
+
+
+def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, threads=0):
+    """The reference's C++ interface (PtFMM_CreateTree with separate single-
+    and double-layer point sets, SetupFMM, PtFMM_Evaluate; coordinates in
+    [0,1)^3 as given).  Either point set may be empty (shape (0, 3))."""
+    lib = load()
+    if threads:
+        lib.ref_set_threads(threads)
+    k0, k1 = KDIM[kernel]
+    sc = np.ascontiguousarray(sl_coord, dtype=np.float64).reshape(-1)
+    sv = np.ascontiguousarray(sl_den, dtype=np.float64).reshape(-1)
+    dc = np.ascontiguousarray(dl_coord, dtype=np.float64).reshape(-1)
+    dv = np.ascontiguousarray(dl_den, dtype=np.float64).reshape(-1)
+    tc = np.ascontiguousarray(trg, dtype=np.float64).reshape(-1)
+    n_trg = len(tc) // 3
+    out = np.zeros(n_trg * k1)
+    if lib.ref_ptfmm_eval(kernel, m, max_pts, len(sc) // 3, _p(sc), _p(sv), len(dc) // 3, _p(dc), _p(dv), n_trg,
+                          _p(tc), _p(out)) != 0:
+        raise ValueError(f"kernel {kernel} is not driven through the C++ interface here")
+    return out.reshape(n_trg, k1)

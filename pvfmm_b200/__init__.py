@@ -79,6 +79,7 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMEvalAdjointDeviceD": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
         "PVFMMEvalAdjointDeviceF": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
         "PVFMMSetUnitBox": (ci, [vp, ci]),
+        "PVFMMSetLayerPoints": (ci, [vp, ci]),
         "PVFMMKernelEvalD": (ci, [ci, vp, vp, cl, vp, vp, cl]),
         "PVFMMKernelEvalDeviceNoAllocD": (ci, [ci, vp, vp, cl, vp, vp, cl, vp]),
         "PVFMMDestroyContextD": (None, [ctypes.POINTER(vp)]),
@@ -269,6 +270,12 @@ class FMMParticleContext:
         """Tree rule of the reference C++ interface: coordinates used as given
         in [0,1)^3, tree points = targets (PVFMMSetUnitBox)."""
         if self._lib.PVFMMSetUnitBox(self._ptr, int(on)) != 0:
+            raise RuntimeError(last_error())
+
+    def set_layer_points(self, on: bool = True) -> None:
+        """Separate single- and double-layer point sets, passed concatenated
+        (each point counts once in the tree; PVFMMSetLayerPoints)."""
+        if self._lib.PVFMMSetLayerPoints(self._ptr, int(on)) != 0:
             raise RuntimeError(last_error())
 
     def stage_times(self) -> dict:

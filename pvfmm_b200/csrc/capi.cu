@@ -140,7 +140,9 @@ int eval_device(const void* ctx_, const T* src, const T* den, const T* dl, long 
     const bool alias = (src == trg) && (n_src == n_trg);
     if (setup || !c.tree.valid) {
       PVFMM_CUDA_CHECK(cudaEventRecord(c.ev[11], c.stream));
-      build_tree(c, src, n_src, trg, n_trg, is_f, (den != nullptr) + (dl != nullptr), alias);
+      const int w = c.layer_points ? ((den || dl) ? 1 : 0) : (den != nullptr) + (dl != nullptr);
+      build_tree(c, src, n_src, trg, n_trg, is_f, w, alias);
+      c.tree.layers = (den ? 1 : 0) | (dl ? 2 : 0);
     } else if (c.tree.n_src != n_src || c.tree.n_trg != n_trg) {
       throw std::runtime_error("setup=0 requires the point counts of the last setup");
     } else {
@@ -313,6 +315,19 @@ int PVFMMEvalAdjointDeviceD(const void* ctx, const double* src_pos, long n_src, 
 int PVFMMEvalAdjointDeviceF(const void* ctx, const float* src_pos, long n_src, const float* trg_pos,
                             const float* trg_den, long n_trg, float* src_val, int setup, void* stream) {
   return eval_adjoint<float>(ctx, src_pos, n_src, trg_pos, trg_den, n_trg, src_val, setup, stream);
+}
+
+int PVFMMSetLayerPoints(void* ctx, int on) {
+  try {
+    Handle* h = as_handle(ctx);
+    h->ctx.layer_points = on != 0;
+    h->ctx.tree.valid = false;
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
 }
 
 int PVFMMSetUnitBox(void* ctx, int on) {

@@ -2124,7 +2124,7 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   const bool has_sl = den_in != nullptr, has_dl = dl_in != nullptr;
   if (has_dl && (KerDblExp < 0 || KerDblS2T < 0))
     throw std::runtime_error("this kernel has no double-layer kernel (dl_den must be NULL)");
-  if (T.src_counted && (int)has_sl + (int)has_dl != T.src_weight)
+  if (T.src_counted && T.layers != ((int)has_sl | (int)has_dl << 1))
     throw std::runtime_error("setup=0 requires the same densities (sl_den, dl_den) passed or NULL as at setup");
   auto s = ctx.stream;
   // expansion dims: equivalent densities din = ns*kin, check potentials

@@ -33,6 +33,7 @@ struct DevTree {
   // fmm_pts.txx:1332-1333)
   int src_weight = 1;
   bool src_counted = true;            // src_weight > 0
+  int layers = 1;                     // densities passed at setup: 1 single layer, 2 double layer, 3 both
   DevBuf src_perm, trg_perm;          // int: sorted index -> input index
   DevBuf src_key, trg_key;            // MKey (sorted)
   DevBuf src_leaf, trg_leaf;          // int: leaf node id of each sorted point
@@ -76,6 +77,10 @@ struct Context {
   int precision = 0;      // 0 plain FP64, 1 mixed FP32
   bool float_api = false; // created by the F entry points
   bool unit_box = false;  // coordinates used as given in [0,1)^3, tree points = targets
+  // source points carry one layer each (the C++ interface's separate single-
+  // and double-layer point sets, passed concatenated with zero values for the
+  // other layer): a source counts once in the tree whatever densities are passed
+  bool layer_points = false;
   HostOperators hops;
   DevOps dops;
   DevTree tree;

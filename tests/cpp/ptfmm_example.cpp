@@ -2,10 +2,13 @@
 // include/pvfmm.hpp (examples/src/example1.cpp:59-112): kernel object,
 // PtFMM::Initialize, PtFMM_CreateTree, SetupFMM, PtFMM_Evaluate, a second
 // evaluation with new densities after ClearFMMData, ker_poten and BuildMatrix.
-// Writes inputs and outputs as raw doubles for the Python test to compare
-// against the oracle.
+// With n_dl > 0 the tree also holds a separate double-layer point set
+// (PtFMM_CreateTree with surf_coord / surf_value, k0 + 3 values per point),
+// and the second evaluation passes new values for both layers.  Writes inputs
+// and outputs as raw doubles for the Python test to compare against the
+// oracle.
 //
-// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f>
+// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f> [n_dl]
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -45,7 +48,7 @@ void put(std::vector<double>& out, const std::vector<Real>& v) {
 }
 
 template <class Real>
-int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_t seed) {
+int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_t seed, long n_dl) {
   Rng rng{seed};
   const pvfmm::Kernel<Real>& ker = kernel_of<Real>(kid);
   const int k0 = ker.ker_dim[0], k1 = ker.ker_dim[1];
@@ -54,16 +57,22 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
   for (auto& x : trg) x = (Real)rng.uniform();
   for (auto& x : den) x = (Real)(2 * rng.uniform() - 1);
   for (auto& x : den2) x = (Real)(2 * rng.uniform() - 1);
+  std::vector<Real> dl(3 * n_dl), dd((k0 + 3) * n_dl), dd2((k0 + 3) * n_dl);
+  for (auto& x : dl) x = (Real)rng.uniform();
+  for (auto& x : dd) x = (Real)(2 * rng.uniform() - 1);
+  for (auto& x : dd2) x = (Real)(2 * rng.uniform() - 1);
 
   MPI_Comm comm = MPI_COMM_WORLD;
   pvfmm::PtFMM<Real> matrices;
   matrices.Initialize(m, comm, &ker);
-  pvfmm::PtFMM_Tree<Real>* tree = pvfmm::PtFMM_CreateTree(src, den, trg, comm, max_pts, pvfmm::FreeSpace);
+  pvfmm::PtFMM_Tree<Real>* tree =
+      n_dl > 0 ? pvfmm::PtFMM_CreateTree(src, den, dl, dd, trg, comm, max_pts, pvfmm::FreeSpace)
+               : pvfmm::PtFMM_CreateTree(src, den, trg, comm, max_pts, pvfmm::FreeSpace);
   tree->SetupFMM(&matrices);
   std::vector<Real> val1, val2;
   pvfmm::PtFMM_Evaluate(tree, val1, nt);
   tree->ClearFMMData();
-  pvfmm::PtFMM_Evaluate(tree, val2, nt, &den2);
+  pvfmm::PtFMM_Evaluate(tree, val2, nt, &den2, n_dl > 0 ? &dd2 : nullptr);
   delete tree;
 
   // ker_poten accumulates: evaluate the first 64 targets twice over 200 sources
@@ -85,6 +94,9 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
   put(out, val2);
   put(out, kp);
   put(out, mat);
+  put(out, dl);
+  put(out, dd);
+  put(out, dd2);
   FILE* f = std::fopen(path, "wb");
   if (!f) return 2;
   std::fwrite(out.data(), sizeof(double), out.size(), f);
@@ -95,16 +107,17 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 9) {
-    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f\n", argv[0]);
+  if (argc != 9 && argc != 10) {
+    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f [n_dl]\n", argv[0]);
     return 1;
   }
   try {
     const int kid = std::atoi(argv[2]), m = std::atoi(argv[3]), mp = std::atoi(argv[4]);
     const long ns = std::atol(argv[5]), nt = std::atol(argv[6]);
     const uint64_t seed = std::strtoull(argv[7], nullptr, 10);
-    if (std::string(argv[8]) == "f") return run<float>(argv[1], kid, m, mp, ns, nt, seed);
-    return run<double>(argv[1], kid, m, mp, ns, nt, seed);
+    const long n_dl = argc == 10 ? std::atol(argv[9]) : 0;
+    if (std::string(argv[8]) == "f") return run<float>(argv[1], kid, m, mp, ns, nt, seed, n_dl);
+    return run<double>(argv[1], kid, m, mp, ns, nt, seed, n_dl);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 3;

@@ -155,6 +155,23 @@ def reference_case_inputs(name):
     return src, den, trg, dl
 
 
+# The reference's C++ interface (PtFMM_CreateTree with a separate
+# double-layer point set): kernel, m, max_pts, seed
+CPP_DL_CASES = {"laplace_dl_m6": (0, 6, 50, 21), "stokes_dl_m4": (3, 4, 60, 22)}
+
+
+def cpp_dl_inputs(name):
+    """Single-layer points (uniform), double-layer points (denser towards a
+    corner), targets (uniform), all in [0,1)^3, and their values."""
+    kid, _, _, seed = CPP_DL_CASES[name]
+    rng = np.random.default_rng(seed)
+    k0 = KDIM[kid][0]
+    sl = rng.random((2000, 3))
+    dl = rng.random((1500, 3)) ** 2
+    trg = rng.random((1000, 3))
+    return sl, rng.uniform(-1, 1, (2000, k0)), dl, rng.uniform(-1, 1, (1500, k0 + 3)), trg
+
+
 def config1_inputs():
     """Laplace potential, 100,000 points i.i.d. uniform in [0,1)^3 (PCG64
     seed 1), densities uniform [-1,1] (seed 2)."""
@@ -179,6 +196,13 @@ def reference_golden(force=False):
                             den=np.zeros((0, KDIM[kid][0])) if den is None else den,
                             trg=np.zeros((0, 3)) if trg is None else trg, out=out,
                             nodes=tree[:, :7].astype(np.int32), lists=lists[:, :4].astype(np.int32), **extra)
+    for name, (kid, m, mp, seed) in CPP_DL_CASES.items():
+        path = os.path.join(HERE, f"refcpp_{name}.npz")
+        if not force and os.path.exists(path):
+            continue
+        sl, sd, dl, dd, trg = cpp_dl_inputs(name)
+        out = R.ref_ptfmm_eval(kid, m, mp, sl, sd, dl, dd, trg)
+        np.savez_compressed(path, kernel=kid, m=m, max_pts=mp, sl=sl, sd=sd, dl=dl, dd=dd, trg=trg, out=out)
     path = os.path.join(HERE, "reference_config1.npz")
     if force or not os.path.exists(path):
         x, q = config1_inputs()

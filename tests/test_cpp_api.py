@@ -45,7 +45,7 @@ def _read(path):
     k0, k1 = int(a[0]), int(a[1])
     pos = 2
     parts = []
-    for _ in range(8):
+    for _ in range(11):
         n = int(a[pos])
         parts.append(a[pos + 1: pos + 1 + n])
         pos += 1 + n
@@ -76,7 +76,7 @@ def test_cpp_interface_matches_oracle(tmp_path, kid, m, mp, ns, nt, real, tol):
     r = subprocess.run([exe, out, str(kid), str(m), str(mp), str(ns), str(nt), "7", real],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
-    k0, k1, (src, den, den2, trg, val1, val2, kp, mat) = _read(out)
+    k0, k1, (src, den, den2, trg, val1, val2, kp, mat, _, _, _) = _read(out)
     K = O.KERNELS[kid]
     assert (k0, k1) == (K.k0, K.k1)
     src = src.reshape(-1, 3)
@@ -121,3 +121,25 @@ def test_host_kernel_eval_matches_direct_sum():
         out = np.full(300 * K.k1, 0.5)
         P.kernel_eval(P.FMMKernel(kid), s, q, t, out)
         assert O.rel_l2(out - 0.5, O.direct_sum(kid, s, q, t)) < 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kid,m,tol", [(0, 6, 1e-12), (3, 4, 1e-11)])
+def test_cpp_interface_double_layer_points_match_oracle(tmp_path, kid, m, tol):
+    """PtFMM_CreateTree with a separate double-layer point set (surf_coord,
+    surf_value) and PtFMM_Evaluate with new values for both layers, against the
+    oracle's C++-interface path (both point sets count in the tree; the
+    oracle is pinned to the reference's own C++ interface in
+    tests/test_reference_pins.py)."""
+    exe = _compile(tmp_path)
+    out = str(tmp_path / "out.bin")
+    r = subprocess.run([exe, out, str(kid), str(m), "60", "1500", "1200", "11", "d", "900"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    k0, k1, (src, den, den2, trg, val1, val2, _, _, dl, dd, dd2) = _read(out)
+    src, trg, dl = src.reshape(-1, 3), trg.reshape(-1, 3), dl.reshape(-1, 3)
+    ops = _ops(kid, m)
+    ref1 = O.ptfmm_eval(kid, m, 60, src, den, trg, ops=ops, dl_pos=dl, dl_den=dd)
+    ref2 = O.ptfmm_eval(kid, m, 60, src, den2, trg, ops=ops, dl_pos=dl, dl_den=dd2)
+    assert O.rel_l2(val1, ref1) < tol
+    assert O.rel_l2(val2, ref2) < tol
