@@ -996,17 +996,22 @@ class FMM:
 # ----------------------------------------------------------------------------
 # C-ABI style entry (PVFMMEval, pvfmm-wrapper.cpp:445-811)
 # ----------------------------------------------------------------------------
-def surf_scal(K: Kernel, scale: float) -> np.ndarray:
+def surf_scal(K: Kernel, scale: float, real=np.float64) -> np.ndarray:
     """Scaling of the double-layer values (pvfmm-wrapper.cpp:521-535): the
-    first k0 values by scale * scale^src_scal, the last three by 1."""
-    return np.array([scale * scale ** e for e in K.src_scal] + [1.0, 1.0, 1.0])
+    first k0 values by scale * scale^src_scal, the last three by 1 (in the
+    interface's precision `real`)."""
+    real = np.dtype(real).type
+    return np.array([real(scale) * real(scale) ** real(e) for e in K.src_scal] + [1.0, 1.0, 1.0], dtype=real)
 
 
 def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, ops=None, return_fmm=False,
-               dl_den=None):
-    """FP64 PVFMMEvalD(src, sl_den, dl_den, n_src, trg, trg_val, n_trg, ctx,
+               dl_den=None, real=np.float64):
+    """PVFMMEvalD(src, sl_den, dl_den, n_src, trg, trg_val, n_trg, ctx,
     setup=1).  Either density may be None (NULL); dl_den holds k0 + 3 values
-    per source (pvfmm.h:269-272)."""
+    per source (pvfmm.h:269-272).  real=np.float32 follows PVFMMEvalF up to
+    the FMM itself: the bounding box, the mapped coordinates, the seed grid
+    and the density and output scales in FP32 (pvfmm-wrapper.cpp:458-599);
+    the FMM runs in FP64 on those values."""
     K = KERNELS[kernel_id]
     src_pos = np.asarray(src_pos, dtype=np.float64).reshape(-1, 3)
     trg_pos = np.asarray(trg_pos, dtype=np.float64).reshape(-1, 3)
@@ -1014,16 +1019,18 @@ def pvfmm_eval(kernel_id: int, m: int, max_pts: int, src_pos, sl_den, trg_pos, o
         sl_den = np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0)
     if dl_den is not None:
         dl_den = np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3)
-    scale, shift = bounding_box_map(src_pos, trg_pos)
-    src_c = map_points(src_pos, scale, shift)
-    trg_c = map_points(trg_pos, scale, shift)
-    src_scal = np.array([scale ** e for e in K.src_scal])
-    trg_scal = np.array([scale ** e for e in K.trg_scal])
+    rt = np.dtype(real).type
+    scale, shift = bounding_box_map(src_pos, trg_pos, real)
+    src_c = map_points(src_pos, scale, shift, real).astype(np.float64)
+    trg_c = map_points(trg_pos, scale, shift, real).astype(np.float64)
+    src_scal = np.array([rt(scale) ** rt(e) for e in K.src_scal], dtype=rt).astype(np.float64)
+    trg_scal = np.array([rt(scale) ** rt(e) for e in K.trg_scal], dtype=rt).astype(np.float64)
     fmm = FMM(kernel_id, m, max_pts, ops)
     t0 = time.perf_counter()
-    fmm.setup(src_c, trg_c, src_weight=(sl_den is not None) + (dl_den is not None))
+    fmm.setup(src_c, trg_c, real=real, src_weight=(sl_den is not None) + (dl_den is not None))
     setup_ms = 1000 * (time.perf_counter() - t0)
-    fmm.io_scal = (src_scal, trg_scal, surf_scal(K, scale))
+    fmm.io_scal = (src_scal, trg_scal, surf_scal(K, scale, real).astype(np.float64))
+    fmm.io_real = rt
     out = _eval_scaled(fmm, sl_den, dl_den)
     fmm.stage_ms["setup"] = setup_ms
     if return_fmm:
@@ -1037,10 +1044,11 @@ def _eval_scaled(fmm: "FMM", sl_den, dl_den) -> np.ndarray:
     if sl_den is None and dl_den is None:           # no source points at all
         fmm.stage_ms = {}
         return np.zeros((len(fmm.trg), K.k1))
+    rt = getattr(fmm, "io_real", np.float64)   # densities scaled in the interface's precision
     den = None if sl_den is None else \
-        (np.asarray(sl_den, dtype=np.float64).reshape(-1, K.k0) * src_scal[None, :])[fmm.src_perm]
+        (np.asarray(sl_den, dtype=rt).reshape(-1, K.k0) * src_scal.astype(rt)[None, :]).astype(np.float64)[fmm.src_perm]
     surf = None if dl_den is None else \
-        (np.asarray(dl_den, dtype=np.float64).reshape(-1, K.k0 + 3) * sf_scal[None, :])[fmm.src_perm]
+        (np.asarray(dl_den, dtype=rt).reshape(-1, K.k0 + 3) * sf_scal.astype(rt)[None, :]).astype(np.float64)[fmm.src_perm]
     out_sorted = fmm.evaluate(den, surf)
     out = np.empty_like(out_sorted)
     out[fmm.trg_perm] = out_sorted

@@ -1463,6 +1463,10 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 // joins the running sum with a rounded FP32 add (see hadamard_tc_kernel).
 // ---------------------------------------------------------------------------
 constexpr int kTc3Warps = 8;
+#ifndef PVFMM_TC3_OPB
+#define PVFMM_TC3_OPB 1  // offsets whose B fragments are staged per barrier
+#endif
+constexpr int kTc3Opb = PVFMM_TC3_OPB;
 
 template <int KOC>
 __global__ void __launch_bounds__(32 * kTc3Warps, 2)
@@ -1472,8 +1476,9 @@ __global__ void __launch_bounds__(32 * kTc3Warps, 2)
   constexpr int NNT = 2 * KOC;        // n-tiles of the group
   constexpr int NB = 6 * NNT;         // (k-step, n-tile) fragment blocks per offset
   constexpr int NP = kTc3Warps * 16;  // target parents of the block
-  extern __shared__ float4 Bs[];      // [2][NB][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
-  int* qs = reinterpret_cast<int*>(Bs + 2 * NB * 32);  // [26][NP] source parent of each (offset, parent)
+  constexpr int OPB = kTc3Opb;
+  extern __shared__ float4 Bs[];      // [2][OPB][NB][32 lanes]: (b0 hi, b1 hi, b0 lo, b1 lo)
+  int* qs = reinterpret_cast<int*>(Bs + 2 * OPB * NB * 32);  // [26][NP] source parent of each (offset, parent)
   unsigned* wl = reinterpret_cast<unsigned*>(qs + 26 * NP);  // [kTc3Warps] occupied offsets of each warp
   const int f = blockIdx.y, z = blockIdx.z, ngroups = gridDim.z;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1496,10 +1501,18 @@ __global__ void __launch_bounds__(32 * kTc3Warps, 2)
   for (int w = 0; w < kTc3Warps; ++w) blive |= wl[w];
   const unsigned wlive = wl[warp];
   const float4* bsrc = bfrag + ((long)f * 26 * ngroups + z) * NB * 32;  // + o * ngroups * NB * 32
-  auto stage = [&](int o, int buf) {
-    const float4* src = bsrc + (long)o * ngroups * NB * 32;
-    float4* dst = Bs + buf * NB * 32;
-    for (int i = threadIdx.x; i < NB * 32; i += 32 * kTc3Warps) cp_async16(dst + i, src + i, 16);
+  // the next (up to) OPB block-live offsets of srem into buffer buf
+  unsigned srem = blive;
+  auto stage_group = [&](int buf) {
+#pragma unroll
+    for (int j = 0; j < OPB; ++j) {
+      if (!srem) break;
+      const int o = __ffs(srem) - 1;
+      srem &= srem - 1;
+      const float4* src = bsrc + (long)o * ngroups * NB * 32;
+      float4* dst = Bs + (buf * OPB + j) * NB * 32;
+      for (int i = threadIdx.x; i < NB * 32; i += 32 * kTc3Warps) cp_async16(dst + i, src + i, 16);
+    }
   };
   const int w0 = warp * 16;
   auto load = [&](int o, float4 (&x)[3][2]) {
@@ -1520,7 +1533,7 @@ __global__ void __launch_bounds__(32 * kTc3Warps, 2)
   unsigned rem = blive;
   int oc = rem ? __ffs(rem) - 1 : 0;
   if (rem) {
-    stage(oc, 0);
+    stage_group(0);
     if (wlive >> oc & 1u) load(oc, xn);
   }
   cp_async_commit();
@@ -1528,10 +1541,13 @@ __global__ void __launch_bounds__(32 * kTc3Warps, 2)
   for (int k = 0; rem; ++k) {
     rem &= rem - 1;
     const int on = rem ? __ffs(rem) - 1 : -1;
-    cp_async_wait<0>();  // this thread's copies of offset oc have landed
-    __syncthreads();     // everyone's have; every warp is done with the other buffer
-    if (on >= 0) stage(on, (k + 1) & 1);
-    cp_async_commit();
+    const int grp = k / OPB, slot = k % OPB;
+    if (slot == 0) {
+      cp_async_wait<0>();  // this thread's copies of the group's offsets have landed
+      __syncthreads();     // everyone's have; every warp is done with the other buffer
+      stage_group((grp + 1) & 1);
+      cp_async_commit();
+    }
     if (wlive >> oc & 1u) {
       unsigned ah[6][4], al[6][4];
 #pragma unroll
@@ -1546,7 +1562,7 @@ __global__ void __launch_bounds__(32 * kTc3Warps, 2)
         tf32_split(xn[u][1].w, ah[2 * u + 1][3], al[2 * u + 1][3]);
       }
       if (on >= 0 && (wlive >> on & 1u)) load(on, xn);  // the next offset's rows, in flight meanwhile
-      const float4* bq = Bs + (k & 1) * NB * 32 + lane;
+      const float4* bq = Bs + ((grp & 1) * OPB + slot) * NB * 32 + lane;
 #pragma unroll
       for (int nt = 0; nt < NNT; ++nt)
 #pragma unroll
@@ -1593,7 +1609,8 @@ void launch_hadamard_tc3(Context& ctx, int n3h, long f_base, int ko, const Cplx<
   DevTree& T = ctx.tree;
   constexpr int NB = 12 * KOC, NP = kTc3Warps * 16;
   const int ngroups = ko / KOC;
-  const size_t sm = (size_t)2 * NB * 32 * sizeof(float4) + (size_t)26 * NP * sizeof(int) + kTc3Warps * sizeof(int);
+  const size_t sm = (size_t)2 * kTc3Opb * NB * 32 * sizeof(float4) + (size_t)26 * NP * sizeof(int) +
+                    kTc3Warps * sizeof(int);
   PVFMM_CUDA_CHECK(cudaFuncSetAttribute(hadamard_tc3_kernel<KOC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(ceil_div(np, (long)NP), n3h, ngroups);
   ++ctx.n_launch;
