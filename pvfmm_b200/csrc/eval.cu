@@ -1464,7 +1464,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 // ---------------------------------------------------------------------------
 constexpr int kTc3Warps = 8;
 #ifndef PVFMM_TC3_OPB
-#define PVFMM_TC3_OPB 1  // offsets whose B fragments are staged per barrier
+#define PVFMM_TC3_OPB 2  // offsets whose B fragments are staged per barrier
 #endif
 constexpr int kTc3Opb = PVFMM_TC3_OPB;
 
