@@ -1456,8 +1456,9 @@ __global__ void __launch_bounds__(32 * kTcWarps, PVFMM_TC_MIN_BLOCKS) hadamard_t
 // when the K order is chosen as k-step 2u+v, column c -> float
 // 16u + 4(c % 4) + 2v + c / 4.  The B fragments of an offset (18 KB for
 // KOC = 3) are too many to stage for all 26 offsets, so the block streams
-// them offset by offset into a double buffer in shared memory (cp.async,
-// one barrier per offset), shared by its 8 warps; offsets that no parent of
+// them, PVFMM_TC3_OPB offsets at a time, into a double buffer in shared
+// memory (cp.async, one barrier per group; two offsets per group measured
+// 3% faster than one at 2M Stokes points), shared by its 8 warps; offsets that no parent of
 // the block has are skipped, those that no parent of a warp has are skipped
 // by that warp.  Each pair of k-steps accumulates in a fresh fragment that
 // joins the running sum with a rounded FP32 add (see hadamard_tc_kernel).
