@@ -250,7 +250,15 @@ constexpr int kNF = 128;        // threads per near-field block
 
 constexpr int kNearUnroll = PVFMM_NEAR_UNROLL;      // unroll of the record loop
 constexpr int kTile = PVFMM_NEAR_TILE_MULT * kNF;  // source records per tile
-constexpr int kRPT = kTile / kNF;                   // records each thread fetches per tile
+#ifndef PVFMM_NEAR_TILE_MULT_K1
+#define PVFMM_NEAR_TILE_MULT_K1 2
+#endif
+// records per tile of the near-field kernel for Real, Ker (the FP32 kernels
+// with one source density have the smallest records)
+template <class Real, int Ker>
+constexpr int near_tile() {
+  return sizeof(Real) == 4 && KerDims<Ker>::KS == 1 ? PVFMM_NEAR_TILE_MULT_K1 * kNF : kTile;
+}
 
 template <class Real>
 struct Vec16 {
@@ -272,7 +280,7 @@ struct Rec {
   __host__ __device__ static constexpr int F(int i) { return kLo ? (i == 0 ? 3 : 6 + i) : 3 + i; }
 };
 
-template <class Real, int KS>
+template <class Real, int KS, int TS = kTile>
 __device__ __forceinline__ void rec_store(typename Vec16<Real>::type* tile, int j, double x, double y, double z,
                                           const Real* f) {
   using R = Rec<Real, KS>;
@@ -293,13 +301,13 @@ __device__ __forceinline__ void rec_store(typename Vec16<Real>::type* tile, int 
   for (int c = 0; c < R::NC; ++c) {
     typename Vec16<Real>::type w;
     memcpy(&w, &v[c * R::PER], 16);
-    tile[c * kTile + j] = w;
+    tile[c * TS + j] = w;
   }
 }
 
 // Adds the records j = j0, j0+js, ... < n to two targets (FP64 accumulators;
 // FP32 sums never run over more than one tile).
-template <class Real, int Ker, bool Surface1 = false>
+template <class Real, int Ker, bool Surface1 = false, int TS = kTile>
 __device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile, int n, int j0, int js,
                                          const Pt<Real>& pa, const Pt<Real>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
@@ -316,7 +324,7 @@ __device__ __forceinline__ void rec_sum2(const typename Vec16<Real>::type* tile,
     Real v[R::NVP];
 #pragma unroll
     for (int c = 0; c < R::NC; ++c) {
-      const typename Vec16<Real>::type w = tile[c * kTile + j];
+      const typename Vec16<Real>::type w = tile[c * TS + j];
       memcpy(&v[c * R::PER], &w, 16);
     }
     Real f[KS];
@@ -432,7 +440,7 @@ __device__ __forceinline__ void ker_eval_x2(f2_t rx, f2_t ry, f2_t rz, const f2_
 }
 
 // rec_sum2 for FP32 records with the packed pair evaluation.
-template <int Ker>
+template <int Ker, int TS = kTile>
 __device__ __forceinline__ void rec_sum2_x2(const float4* tile, int n, int j0, int js, const Pt<float>& pa,
                                             const Pt<float>& pb, double (&acc)[2][KerDims<Ker>::KT]) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
@@ -451,7 +459,7 @@ __device__ __forceinline__ void rec_sum2_x2(const float4* tile, int n, int j0, i
       float v[R::NVP];
 #pragma unroll
       for (int c = 0; c < R::NC; ++c) {
-        const float4 w = tile[c * kTile + j];
+        const float4 w = tile[c * TS + j];
         memcpy(&v[c * R::PER], &w, 16);
       }
       f2_t f[KS];
@@ -503,10 +511,15 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
   constexpr bool kF32 = sizeof(Real) == 4;
   constexpr bool kPacked = kF32 && kHasPacked<Ker>;
   constexpr int TPT = 2;  // targets per thread
+  constexpr int TILE = near_tile<Real, Ker>();  // source records per tile
+  constexpr int RPT = TILE / kNF;                 // records each thread fetches per tile
   using V = typename Vec16<Real>::type;
-  __shared__ V tiles[2][Rec<Real, KS>::NC * kTile];
-  __shared__ double2 tile64[kF32 && !kDbl ? Rec<double, KS>::NC * kTile : 1];  // FP64 D2T records of the mixed form
-  // the partial sums of the final fixed-order reduction reuse the tiles
+  __shared__ V tiles[2][Rec<Real, KS>::NC * TILE];
+  // the FP64 D2T records of the mixed form come first and reuse the tiles
+  // (a barrier separates their last read from the first tile store), and so
+  // do the partial sums of the final fixed-order reduction
+  static_assert(Rec<double, KS>::NC * 16 <= 2 * Rec<Real, KS>::NC * (int)sizeof(V), "D2T records fit the tiles");
+  double2* tile64 = reinterpret_cast<double2*>(&tiles[0][0]);
   static_assert(sizeof(tiles) >= sizeof(double) * kNF * TPT * KT, "reduction buffer larger than the tiles");
   double(*red)[TPT][KT] = reinterpret_cast<double(*)[TPT][KT]>(&tiles[0][0]);
   __shared__ NearSeg seg[kSegCap];
@@ -550,15 +563,16 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
       if (de) {
         const double hr = half * kRad1;
         const double* dens = de + (long)b * dim;
-        for (int k0 = 0; k0 < ns; k0 += kTile) {
-          const int n = min(kTile, ns - k0);
+        for (int k0 = 0; k0 < ns; k0 += TILE) {
+          const int n = min(TILE, ns - k0);
           __syncthreads();
           for (int i = threadIdx.x; i < n; i += kNF) {
             const int k = k0 + i;
             double f[KS];
 #pragma unroll
             for (int c = 0; c < KS; ++c) f[c] = dens[k * KS + c];
-            rec_store<double, KS>(tile64, i, hr * usurf[k * 3 + 0], hr * usurf[k * 3 + 1], hr * usurf[k * 3 + 2], f);
+            rec_store<double, KS, TILE>(tile64, i, hr * usurf[k * 3 + 0], hr * usurf[k * 3 + 1],
+                                        hr * usurf[k * 3 + 2], f);
           }
           __syncthreads();
           if (active)
@@ -566,7 +580,7 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
             for (int h = 0; h < TPT / 2; ++h) {
               const Pt<double> pa64 = make_pt<double>(tx[tq[2 * h]], ty[tq[2 * h]], tz[tq[2 * h]]);
               const Pt<double> pb64 = make_pt<double>(tx[tq[2 * h + 1]], ty[tq[2 * h + 1]], tz[tq[2 * h + 1]]);
-              rec_sum2<double, Ker, true>(tile64, n, g, G, pa64, pb64,
+              rec_sum2<double, Ker, true, TILE>(tile64, n, g, G, pa64, pb64,
                                           *reinterpret_cast<double(*)[2][KT]>(&acc[2 * h][0]));
             }
         }
@@ -631,13 +645,13 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
       }
       __syncthreads();
       const int total = start[ne];
-      const int ntile = (total + kTile - 1) / kTile;
+      const int ntile = (total + TILE - 1) / TILE;
       // records j = threadIdx.x + u * kNF of a tile, fetched one tile ahead
-      double rx_[kRPT], ry_[kRPT], rz_[kRPT], rf_[kRPT][KS];
+      double rx_[RPT], ry_[RPT], rz_[RPT], rf_[RPT][KS];
       auto fetch = [&](int t) {
 #pragma unroll
-        for (int u = 0; u < kRPT; ++u) {
-          const int r = t * kTile + threadIdx.x + u * kNF;
+        for (int u = 0; u < RPT; ++u) {
+          const int r = t * TILE + threadIdx.x + u * kNF;
           if (r >= total) continue;
           int lo = 0, hi = ne;  // largest s with start[s] <= r
           while (hi - lo > 1) {
@@ -668,22 +682,22 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
       };
       if (ntile > 0) fetch(0);
       for (int t = 0; t < ntile; ++t) {
-        const int n = min(kTile, total - t * kTile);
+        const int n = min(TILE, total - t * TILE);
 #pragma unroll
-        for (int u = 0; u < kRPT; ++u) {
+        for (int u = 0; u < RPT; ++u) {
           const int j = threadIdx.x + u * kNF;
           if (j < n) {
             Real f[KS];
 #pragma unroll
             for (int c = 0; c < KS; ++c) f[c] = (Real)rf_[u][c];
-            rec_store<Real, KS>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
+            rec_store<Real, KS, TILE>(tiles[buf], j, rx_[u], ry_[u], rz_[u], f);
           }
         }
         if (t + 1 < ntile) fetch(t + 1);
         __syncthreads();  // tiles[buf] complete; tiles[buf^1] no longer read (its readers passed this barrier)
         if (active) {
-          if constexpr (kPacked) rec_sum2_x2<Ker>(tiles[buf], n, g, G, pt[0], pt[1], acc);
-          else rec_sum2<Real, Ker>(tiles[buf], n, g, G, pt[0], pt[1], acc);
+          if constexpr (kPacked) rec_sum2_x2<Ker, TILE>(tiles[buf], n, g, G, pt[0], pt[1], acc);
+          else rec_sum2<Real, Ker, false, TILE>(tiles[buf], n, g, G, pt[0], pt[1], acc);
         }
         buf ^= 1;
       }
