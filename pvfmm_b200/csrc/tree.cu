@@ -529,14 +529,21 @@ __global__ void iota_kernel(int* __restrict__ a, long n) {
   if (i < n) a[i] = (int)i;
 }
 
-// Exclusive prefix sum of n ints; returns the total (synchronous read).
+// Pinned host slots of a tree build (ctx.chk): the deferred counts, two
+// slots for the totals read back at once, and 12 doubles of bounding boxes.
+constexpr int kChkLists = 40, kChkLeaves = 48, kChkScan = 60, kChkSlots = 64;
+constexpr size_t kChkBytes = kChkSlots * sizeof(int) + 12 * sizeof(double);
+inline double* chk_bbox(Context& ctx) { return reinterpret_cast<double*>(ctx.chk + kChkSlots); }
+
+// Exclusive prefix sum of n ints; returns the total (synchronous read through
+// pinned slots).
 long exclusive_scan(Context& ctx, const int* in, int* out, long n) {
   if (n <= 0) return 0;
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx.stream);
   void* tmp = ctx.scratch2.ensure(bytes);
   cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx.stream);
-  int h[2];
+  int* h = ctx.chk + kChkScan;
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(&h[0], out + n - 1, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(&h[1], in + n - 1, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
@@ -545,7 +552,6 @@ long exclusive_scan(Context& ctx, const int* in, int* out, long n) {
 
 // Pinned count slots of a tree build: [0, kMaxDepth] internal nodes per level,
 // then the compacted list sizes and the leaf count.
-constexpr int kChkLists = 40, kChkLeaves = 48, kChkSlots = 64;
 static_assert(kMaxDepth < kChkLists, "per-level slots overlap the list slots");
 
 // Exclusive prefix sum of n ints without reading the total back; the total
@@ -715,8 +721,8 @@ void point_bbox(Context& ctx, const T* pos, long n, double* host6) {
   bbox_partial<T><<<nb, kThreads, 0, ctx.stream>>>(pos, n, part);
   ++ctx.n_launch;
   bbox_final<<<1, kThreads, 0, ctx.stream>>>(part, nb, part + (size_t)nb * 6);
+  // host6: pinned; the caller synchronises
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(host6, part + (size_t)nb * 6, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
-  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
 }
 
 template <class T>
@@ -762,7 +768,7 @@ static std::vector<MKey> seed_grid_keys(int max_pts, bool real_float) {
 void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_pos, long n_trg, bool pos_float,
                 int src_weight, bool trg_alias) {
   if (n_src < 1 || n_trg < 1) throw std::runtime_error("build_tree needs at least one source and one target");
-  if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, kChkSlots * sizeof(int)));
+  if (!ctx.chk) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.chk, kChkBytes));
   DevTree& T = ctx.tree;
   auto& s = ctx.stream;
   T.valid = false;
@@ -770,18 +776,21 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   T.n_trg = n_trg;
   T.src_weight = n_src > 0 ? src_weight : 0;
   T.src_counted = T.src_weight > 0;
-  // 1. bounding box and map
-  double bs[6], bt[6];
+  // 1. bounding box and map (both boxes read back with one synchronisation)
+  double* bs = chk_bbox(ctx);
+  double* bt = bs + 6;
   if (pos_float) {
     point_bbox<float>(ctx, (const float*)src_pos, n_src, bs);
-    if (trg_alias) std::copy(bs, bs + 6, bt);
-    else point_bbox<float>(ctx, (const float*)trg_pos, n_trg, bt);
-    if (!ctx.unit_box) bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
+    if (!trg_alias) point_bbox<float>(ctx, (const float*)trg_pos, n_trg, bt);
   } else {
     point_bbox<double>(ctx, (const double*)src_pos, n_src, bs);
-    if (trg_alias) std::copy(bs, bs + 6, bt);
-    else point_bbox<double>(ctx, (const double*)trg_pos, n_trg, bt);
-    if (!ctx.unit_box) bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
+    if (!trg_alias) point_bbox<double>(ctx, (const double*)trg_pos, n_trg, bt);
+  }
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+  if (trg_alias) std::copy(bs, bs + 6, bt);
+  if (!ctx.unit_box) {
+    if (pos_float) bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
+    else bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
   }
   if (ctx.unit_box) {
     // C++ interface (include/pvfmm.txx:216-244): coordinates are used as
