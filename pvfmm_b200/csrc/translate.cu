@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kBM = 128, kBN = 64, kBK = 16;
 constexpr int kAStride = kBK + 4;  // doubles per A row in shared memory
-constexpr int kBStride = kBN + 8;  // doubles per B row in shared memory
+constexpr int kBStride = kBN + 4;  // doubles per B row in shared memory (B fragment loads conflict-free)
 constexpr int kThreadsG = 256;
 constexpr int kSmemG = (int)sizeof(double) * (2 * kBM * kAStride + 2 * kBK * kBStride) + (int)sizeof(long) * kBM;
 
