@@ -759,6 +759,45 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
   const int dim = ns * KT;
   double* o = mode != 1 ? out + (long)b * dim : out + (long)T * dim;
   const double oscale = mode != 1 ? scale * ldexp(1.0, -deg * dT) : scale;
+  // a leaf's own sources (mode 0, 2) that fit one tile are staged once for
+  // every chunk of check points; a chunk of kNT points (one group) then writes
+  // its sums directly, with no block barrier
+  const int lo0 = slo[T], n0 = shi[T] - lo0;
+  if (mode != 1 && n0 <= kNT) {
+    if (threadIdx.x < n0) {
+      const int p = lo0 + threadIdx.x;
+      tile_store(tl, threadIdx.x, sx[p], sy[p], sz[p]);
+#pragma unroll
+      for (int i = 0; i < KerDims<Ker>::KS; ++i) tl.f[i][threadIdx.x] = den[(long)p * KerDims<Ker>::KS + i];
+    }
+    __syncthreads();
+    for (int c0 = 0; c0 < ns; c0 += kNT) {
+      const Split sp(ns - c0);
+      const int k = c0 + sp.ti;
+      double px = 0, py = 0, pz = 0;
+      if (sp.active) {
+        px = hr * usurf[k * 3 + 0];
+        py = hr * usurf[k * 3 + 1];
+        pz = hr * usurf[k * 3 + 2];
+      }
+      const Pt<double> pt = make_pt<double>(px, py, pz);
+      double acc[KT];
+#pragma unroll
+      for (int c = 0; c < KT; ++c) acc[c] = 0;
+      if (sp.active) tile_sum<double, Ker, Surface1>(tl, n0, sp.g, sp.G, pt, acc);
+      if (sp.G == 1) {
+        if (sp.active)
+#pragma unroll
+          for (int c = 0; c < KT; ++c) {
+            double* dst = o + (c0 + sp.ti) * KT + c;
+            *dst = mode == 2 ? *dst + acc[c] * oscale : acc[c] * oscale;
+          }
+      } else {
+        reduce_store<KT>(red, sp, acc, oscale, o + c0 * KT, mode != 0);
+      }
+    }
+    return;
+  }
   for (int c0 = 0; c0 < ns; c0 += kNT) {
     const Split sp(ns - c0);
     const int k = c0 + sp.ti;
