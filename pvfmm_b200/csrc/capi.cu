@@ -51,7 +51,7 @@ void destroy_context(Context& c) {
   if (c.stream) cudaStreamSynchronize(c.stream);
   DevBuf* bufs[] = {&c.dops.uc2ue0, &c.dops.uc2ue1, &c.dops.dc2de0, &c.dops.dc2de1, &c.dops.u2u,
                     &c.dops.d2d, &c.dops.vop, &c.dops.vop_frag, &c.dops.vop_tc5, &c.tc5_err_buf,
-                    &c.dops.ue_proj, &c.ue_c, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den,
+                    &c.dops.ue_basis, &c.ue_c, &c.dops.usurf, &c.dops.fft_map, &c.dops.ifft_map, &c.den,
                     &c.surf, &c.pot, &c.ue, &c.dc, &c.uc_c, &c.tmp_c, &c.de_c, &c.spec_in, &c.spec_out,
                     &c.scratch, &c.scratch2, &c.io_src, &c.io_trg, &c.io_den, &c.io_dl, &c.io_val, &c.stat};
   for (DevBuf* b : bufs) b->release();

@@ -2202,7 +2202,10 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   // dout = ns*kout (kin = kout for Laplace and Stokes velocity); the
   // pseudo-inverse factors pass through r = min(din, dout) values
   const int ns = ctx.ns, kin = KerDims<KerExp>::KS, kout = KerDims<KerExp>::KT;
-  const int din = ns * kin, dout = ns * kout, rk = std::min(din, dout), deg = ctx.ki.deg;
+  const int din = ns * kin, dout = ns * kout, deg = ctx.ki.deg;
+  // inner widths of the upward and downward check -> equivalent products
+  // (the kept singular directions, padded to even)
+  const int ru = ctx.ru, rd = ctx.rd;
   const int k0 = ctx.ki.k0, k1 = ctx.ki.k1;
   const long N = T.n_nodes;
   const MKey* keys = T.key.get<MKey>();
@@ -2243,6 +2246,19 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   double* dc = ctx.dc.as<double>((size_t)N * dout);
   PVFMM_CUDA_CHECK(cudaMemsetAsync(ue, 0, (size_t)N * din * sizeof(double), s));
   PVFMM_CUDA_CHECK(cudaMemsetAsync(dc, 0, (size_t)N * dout * sizeof(double), s));
+  // mixed form, Stokes kernel: the FP32 stages (V-list input, W list) read
+  // the upward equivalent densities projected onto the directions above the
+  // FP32 cutoff (ue32 = ue U_k U_k^T); the FP64 stages keep ue.  (2M-point
+  // m=10 Stokes error 3.3e-4 without, 2.8e-5 with; no change for Laplace.)
+  // The leaves' rows come from the first r32 columns of the S2U
+  // intermediate, the internal nodes' from ue after U2U; leaves without
+  // sources keep zero rows.
+  const bool proj32 = sizeof(Real) == 4 && kin == 3 && T.src_counted && N > 0 && ctx.r32 > 0;
+  double* ue32 = nullptr;
+  if (proj32) {
+    ue32 = ctx.ue_c.as<double>((size_t)N * din);
+    PVFMM_CUDA_CHECK(cudaMemsetAsync(ue32, 0, (size_t)N * din * sizeof(double), s));
+  }
   const double* usurf = ctx.dops.usurf.get<double>();
   const double* sx = T.sx.get<double>();
   const double* sy = T.sy.get<double>();
@@ -2254,7 +2270,7 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   // ---- S2U
   if (T.src_counted && T.n_sleaf > 0) {
     double* uc = ctx.uc_c.as<double>((size_t)T.n_sleaf * dout);
-    double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * rk);
+    double* t1 = ctx.tmp_c.as<double>((size_t)T.n_sleaf * ru);
     ++ctx.n_launch;
     // full FP64 rsqrt here in both forms: the check potentials feed the
     // FP64-cutoff pseudo-inverse, which amplifies their rounding into
@@ -2275,10 +2291,15 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
     }
     // equivalent densities (uc UC2UE0) UC2UE1 straight into the leaves' rows of UE
     ctx.n_launch += 2;
-    translate_gemm(s, T.n_sleaf, rk, dout, uc, dout, nullptr, ctx.dops.uc2ue0.get<double>(), rk, t1, rk, nullptr,
+    translate_gemm(s, T.n_sleaf, ru, dout, uc, dout, nullptr, ctx.dops.uc2ue0.get<double>(), ru, t1, ru, nullptr,
                    nullptr, false);
-    translate_gemm(s, T.n_sleaf, din, rk, t1, rk, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue, din,
+    translate_gemm(s, T.n_sleaf, din, ru, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue, din,
                    T.sleaf.get<int>(), nullptr, false);
+    if (proj32) {  // (t1 columns 0..r32) (UC2UE1 rows 0..r32) = ue U_k U_k^T of the leaves
+      ++ctx.n_launch;
+      translate_gemm(s, T.n_sleaf, din, ctx.r32, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue32, din,
+                     T.sleaf.get<int>(), nullptr, false);
+    }
   }
   ev(2);
   // ---- U2U, bottom-up
@@ -2297,18 +2318,22 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
                      part);
     }
   }
-  // mixed form, Stokes kernel: the FP32 stages (V-list input, W list) read
-  // the upward equivalent densities projected onto the directions above the
-  // FP32 cutoff (ue_c = ue P); the FP64 stages keep ue.  (2M-point m=10
-  // Stokes error 3.3e-4 without, 2.8e-5 with; no change for Laplace.)
-  const double* ue32 = ue;
-  if (sizeof(Real) == 4 && kin == 3 && T.src_counted && N > 0) {
-    double* uc_ = ctx.ue_c.as<double>((size_t)N * din);
-    ++ctx.n_launch;
-    translate_gemm(s, N, din, din, ue, din, nullptr, ctx.dops.ue_proj.get<double>(), din, uc_, din, nullptr, nullptr,
-                   false);
-    ue32 = uc_;
+  // the internal nodes' projected rows: (ue U_k) U_k^T through a compact
+  // n_internal x r32 intermediate
+  if (proj32) {
+    long nint = 0;
+    for (int d = 0; d < T.depth; ++d) nint += T.n_internal[d];
+    if (nint > 0) {
+      const int r32 = ctx.r32;
+      double* tp = ctx.tmp_c.as<double>((size_t)nint * r32);
+      ctx.n_launch += 2;
+      translate_gemm(s, nint, r32, din, ue, din, T.int_idx.get<int>(), ctx.dops.ue_basis.get<double>(), r32, tp, r32,
+                     nullptr, nullptr, false);
+      translate_gemm(s, nint, din, r32, tp, r32, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue32, din,
+                     T.int_idx.get<int>(), nullptr, false);
+    }
   }
+  if (!proj32) ue32 = ue;
   ev(3);
   // ---- V-list
   if (T.src_counted && T.n_vtrg > 0 && T.n_vsrc > 0) {
@@ -2352,13 +2377,13 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   double* pot = ctx.pot.as<double>(std::max(T.n_trg, 1L) * k1);
   if (T.n_tleaf > 0) {
     double* de = ctx.de_c.as<double>((size_t)T.n_tleaf * din);
-    double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * rk);
+    double* t1 = ctx.uc_c.as<double>((size_t)T.n_tleaf * rd);
     // (2^(-deg depth) DC[leaf] DC2DE0) DC2DE1, the check potentials gathered
     // from the leaves' rows of DC
     ctx.n_launch += 2;
-    translate_gemm(s, T.n_tleaf, rk, dout, dc, dout, T.tleaf.get<int>(), ctx.dops.dc2de0.get<double>(), rk, t1, rk,
+    translate_gemm(s, T.n_tleaf, rd, dout, dc, dout, T.tleaf.get<int>(), ctx.dops.dc2de0.get<double>(), rd, t1, rd,
                    nullptr, keys, false, 1, nullptr, deg);
-    translate_gemm(s, T.n_tleaf, din, rk, t1, rk, nullptr, ctx.dops.dc2de1.get<double>(), din, de, din, nullptr,
+    translate_gemm(s, T.n_tleaf, din, rd, t1, rd, nullptr, ctx.dops.dc2de1.get<double>(), din, de, din, nullptr,
                    nullptr, false);
     ev(12);
     ++ctx.n_launch;
@@ -2547,13 +2572,65 @@ static void upload_vop3_fragments(Context& ctx) {
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
 }
 
+// Check -> equivalent factors C2E0 (rows x r) and C2E1 (r x cols) without the
+// directions the cutoff dropped: a zero column of C2E0 multiplies its row of
+// C2E1 by zero, so the product is unchanged when both are left out.  The
+// directions listed in `first` come first (padded to an even count with a
+// zero direction, *n_first), then the other kept ones; the inner width *rc is
+// padded to even as well (the translation products take 16-byte rows).
+void compact_factors(const std::vector<double>& c0, const std::vector<double>& c1, int rows, int r, int cols,
+                     const std::vector<int>& first, std::vector<double>& o0, std::vector<double>& o1, int* rc,
+                     int* n_first) {
+  std::vector<int> order(first);
+  if (order.size() & 1) order.push_back(-1);
+  *n_first = (int)order.size();
+  std::vector<char> taken(r, 0);
+  for (int j : first) taken[j] = 1;
+  for (int j = 0; j < r; ++j) {
+    if (taken[j]) continue;
+    bool kept = false;
+    for (int i = 0; i < rows && !kept; ++i) kept = c0[(size_t)i * r + j] != 0.0;
+    if (kept) order.push_back(j);
+  }
+  if (order.size() & 1) order.push_back(-1);
+  if (order.empty()) order.assign(2, -1);
+  const int n = (int)order.size();
+  *rc = n;
+  o0.assign((size_t)rows * n, 0.0);
+  o1.assign((size_t)n * cols, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const int j = order[k];
+    if (j < 0) continue;
+    for (int i = 0; i < rows; ++i) o0[(size_t)i * n + k] = c0[(size_t)i * r + j];
+    std::copy(c1.begin() + (size_t)j * cols, c1.begin() + (size_t)(j + 1) * cols, o1.begin() + (size_t)k * cols);
+  }
+}
+
 void upload_operators(Context& ctx) {
   const HostOperators& h = ctx.hops;
   auto s = ctx.stream;
-  upload_vec<double>(ctx.dops.uc2ue0, h.uc2ue0, s);
-  upload_vec<double>(ctx.dops.uc2ue1, h.uc2ue1, s);
-  upload_vec<double>(ctx.dops.dc2de0, h.dc2de0, s);
-  upload_vec<double>(ctx.dops.dc2de1, h.dc2de1, s);
+  {
+    const int din = h.ns * h.kin, dout = h.ns * h.kout, rk = std::min(din, dout);
+    const bool proj32 = ctx.precision == 1 && ctx.ki.ke == 3;
+    std::vector<double> a0, a1, b0, b1;
+    int nf = 0;
+    compact_factors(h.uc2ue0, h.uc2ue1, dout, rk, din, proj32 ? h.ue32_dirs : std::vector<int>(), a0, a1, &ctx.ru,
+                    &ctx.r32);
+    compact_factors(h.dc2de0, h.dc2de1, dout, rk, din, std::vector<int>(), b0, b1, &ctx.rd, &nf);
+    upload_vec<double>(ctx.dops.uc2ue0, a0, s);
+    upload_vec<double>(ctx.dops.uc2ue1, a1, s);
+    upload_vec<double>(ctx.dops.dc2de0, b0, s);
+    upload_vec<double>(ctx.dops.dc2de1, b1, s);
+    if (proj32) {
+      // U_k (din x r32): the transpose of the first r32 rows of the compacted
+      // UC2UE1, so that ue U_k U_k^T is the projection onto those directions
+      std::vector<double> ub((size_t)din * std::max(ctx.r32, 1), 0.0);
+      for (int k = 0; k < ctx.r32; ++k)
+        for (int a = 0; a < din; ++a) ub[(size_t)a * ctx.r32 + k] = a1[(size_t)k * din + a];
+      upload_vec<double>(ctx.dops.ue_basis, ub, s);
+    }
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  }
   upload_vec<double>(ctx.dops.u2u, h.u2u, s);
   upload_vec<double>(ctx.dops.d2d, h.d2d, s);
   upload_vec<double>(ctx.dops.usurf, h.usurf, s);
@@ -2569,7 +2646,6 @@ void upload_operators(Context& ctx) {
     if (!ctx.tc5_err_host) PVFMM_CUDA_CHECK(cudaMallocHost((void**)&ctx.tc5_err_host, sizeof(int)));
     *ctx.tc5_err_host = 0;
   }
-  if (ctx.precision == 1 && ctx.ki.ke == 3 && !h.ue_proj.empty()) upload_vec<double>(ctx.dops.ue_proj, h.ue_proj, s);
   int* fm = ctx.dops.fft_map.as<int>(h.fft_map.size());
   int* im = ctx.dops.ifft_map.as<int>(h.ifft_map.size());
   PVFMM_CUDA_CHECK(cudaMemcpyAsync(fm, h.fft_map.data(), h.fft_map.size() * sizeof(int), cudaMemcpyHostToDevice, s));

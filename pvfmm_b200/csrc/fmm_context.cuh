@@ -65,7 +65,7 @@ struct DevOps {
   DevBuf uc2ue0, uc2ue1, dc2de0, dc2de1, u2u, d2d, vop;
   DevBuf vop_frag;  // mixed form: Hadamard operators as TF32 hi/lo MMA fragments
   DevBuf vop_tc5;   // mixed form, ke = 1: Hadamard operators in the tcgen05 shared-memory layout
-  DevBuf ue_proj;   // mixed form: projector applied to the upward equivalent densities
+  DevBuf ue_basis;  // mixed Stokes form: din x r32, the upward directions above the FP32 cutoff
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
 };
@@ -83,6 +83,10 @@ struct Context {
   bool layer_points = false;
   HostOperators hops;
   DevOps dops;
+  // inner widths of the uploaded check -> equivalent factors: the directions
+  // the cutoff kept, padded to even (upward ru, downward rd); the first r32
+  // upward ones span the mixed Stokes form's projection (0 otherwise)
+  int ru = 0, rd = 0, r32 = 0;
   DevTree tree;
   cudaStream_t stream = nullptr;
   int device = 0;

@@ -66,6 +66,7 @@ struct HostOperators {
   // cutoff 4*eps32*max; the mixed form applies it to the upward equivalent
   // densities before its FP32 stages
   std::vector<double> ue_proj;
+  std::vector<int> ue32_dirs;           // the singular directions j (rows of UC2UE1) spanning ue_proj
   std::vector<double> dc2de0, dc2de1;
   std::vector<double> u2u;              // (8*ns*kin) x (ns*kin), row block c = child octant c
   std::vector<double> d2d;              // (ns*kout) x (8*ns*kout), column block c = child octant c

@@ -497,8 +497,10 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
     for (double v : f[0].S) smax = std::max(smax, std::fabs(v));
     const double cut32 = 4.0 * eps32 * smax;
     ops.ue_proj.assign((size_t)din * din, 0.0);
+    ops.ue32_dirs.clear();
     for (int j = 0; j < rk; ++j) {
       if (!(f[0].S[j] > cut32)) continue;
+      ops.ue32_dirs.push_back(j);
       for (int a = 0; a < din; ++a) {
         const double ua = Ut[(size_t)j * din + a];
         double* row = &ops.ue_proj[(size_t)a * din];
