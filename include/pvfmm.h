@@ -9,10 +9,16 @@
  *   densities  [q1 ... qn] (k0 values per point: 1 for Laplace, 3 for Stokes)
  *   outputs    n_trg x k1 values, overwritten (not accumulated)
  *
- * Free space only: box_size <= 0 maps the points into the unit box with the
- * reference's bounding-box rule and rescales densities and outputs by the
- * kernel's scale exponents (src/pvfmm-wrapper.cpp:458-541, 800-808).
- * box_size > 0 (periodic) is rejected with an error.
+ * Boundaries: box_size <= 0 is free space: the points are mapped into the
+ * unit box with the reference's bounding-box rule and densities and outputs
+ * are rescaled by the kernel's scale exponents (src/pvfmm-wrapper.cpp:458-541,
+ * 800-808).  box_size > 0 is periodic with period box_size in x, y and z
+ * (src/pvfmm-wrapper.cpp:397-404, 512-517): the points are scaled by
+ * 1/box_size and wrapped into the unit cube, the interaction lists wrap
+ * around it, and the images beyond the root's 3x3x3 block enter through the
+ * boundary operator of the reference's default build (PVFMM_EXTENDED_BC: the
+ * images of the 5x5x5 block; PVFMMSetPeriodicBC selects the lattice sum over
+ * all images or adds a user operator).
  *
  * Errors: the reference signatures return void.  On failure an evaluation
  * fills trg_val with NaN and records a message for PVFMMGetLastError().
@@ -121,6 +127,24 @@ enum PVFMMPrecision {
 /* Context on double-precision inputs with an explicit precision form, so the
  * plain and the mixed form can run on the same FP64 inputs. */
 void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision);
+
+/* Boundary operator of a periodic context (box_size > 0), replacing
+ * FMM_Pts::SetM2C and the reference's build option PVFMM_EXTENDED_BC
+ * (include/fmm_pts.txx:790-1232, 2642-2686):
+ *   lattice 0 (the default): the images in the 5x5x5 block around the root
+ *     outside its 3x3x3 block (the reference built with PVFMM_EXTENDED_BC, its
+ *     CMake default), plus m2c when not NULL: an (ns*k0) x (ns*k1) row-major
+ *     operator from the root's upward equivalent density to its downward
+ *     check potential, ns = 6(m-1)^2+2, added as SetM2C's operator is;
+ *   lattice 1: the lattice sum over all images (the reference built without
+ *     that option: zero-average projections, the unit volume potential's far
+ *     field and the corner correction; for LaplacePotential and
+ *     StokesVelocity the potential of the mean density is taken out of the
+ *     outputs); LaplacePotential, LaplaceGradient and StokesVelocity only,
+ *     m2c must be NULL.
+ * Returns 0, or -1 (message in PVFMMGetLastError()) for a free-space context,
+ * an unsupported kernel or bad arguments. */
+int PVFMMSetPeriodicBC(void* ctx, int lattice, const double* m2c);
 
 /* Evaluation on device pointers (CUDA global memory).  The work is ordered
  * after the work already queued on `stream` (a cudaStream_t) and `stream`
@@ -241,7 +265,15 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n);
  * 0 UC2UE0, 1 UC2UE1, 2 DC2DE0, 3 DC2DE1, 4 U2U (8 stacked, child-major rows),
  * 5 D2D (8 stacked, child-major columns), 6 unit surface (ns x 3),
  * 7 V-list Hadamard operators (complex, [f][offset 26][j1 8][j2 8][k0][k1]),
- * 8 projector onto the upward equivalent directions above the FP32 cutoff.
+ * 8 projector onto the upward equivalent directions above the FP32 cutoff,
+ * 9 periodic boundary operator ((ns*kin) x (ns*kout): root upward
+ * equivalent density -> root downward check potential of the periodic images
+ * outside the root's 3x3x3 block; BC_Type of BoundaryType Periodic,
+ * include/fmm_pts.txx:790-1232) as the reference's default build forms it
+ * (PVFMM_EXTENDED_BC: the images of the 5x5x5 block), 10 the same operator
+ * as the lattice sum over all images (the reference built without that
+ * option; Laplace potential / gradient and Stokes velocity only).  Precision
+ * is ignored for both.
  * Returns the element count needed (copies at most n).
  *
  * Operator cache (contexts and this function alike): when the environment

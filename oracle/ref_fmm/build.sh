@@ -35,4 +35,6 @@ build() {  # isa flags, library suffix
 }
 build "-march=x86-64-v3" avx2 &
 build "-march=x86-64-v4" avx512 &
-wait %1 && wait %2
+# periodic boundaries without PVFMM_EXTENDED_BC (the lattice sum of all images)
+build "-march=x86-64-v3 -DPVFMM_REF_LATTICE_BC" avx2_lattice &
+wait %1 && wait %2 && wait %3

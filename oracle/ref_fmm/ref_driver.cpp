@@ -94,6 +94,24 @@ long ref_tree_lists(const void* ctx, int64_t* out, long cap) {
   return cnt;
 }
 
+// The reference's integral of a kernel's expansion (m2l) kernel over the
+// box [0, r]^3 at target s with a constant unit density (cheb_integ of degree
+// 0, include/cheb_utils.txx:1037), the input of its periodic-boundary
+// precompute: out[j + k*k0] as cheb_integ returns it.  Returns the number of
+// values, or -1 for an unknown kernel.
+int ref_cheb_integ0(int kernel, const double* s, double r, double* out) {
+  const pvfmm::Kernel<double>* ker = nullptr;
+  if (kernel == PVFMMLaplacePotential) ker = &pvfmm::LaplaceKernel<double>::potential();
+  if (kernel == PVFMMLaplaceGradient) ker = &pvfmm::LaplaceKernel<double>::gradient();
+  if (kernel == PVFMMStokesVelocity) ker = &pvfmm::StokesKernel<double>::velocity();
+  if (!ker) return -1;
+  ker->Initialize(false);
+  double sc[3] = {s[0], s[1], s[2]};
+  std::vector<double> v = pvfmm::cheb_integ<double>(0, sc, r, *ker->k_m2l);
+  std::memcpy(out, v.data(), sizeof(double) * v.size());
+  return (int)v.size();
+}
+
 // Sets the number of OpenMP threads the reference uses (0 leaves the
 // current setting) and returns the count in effect.
 int ref_set_threads(int n) {

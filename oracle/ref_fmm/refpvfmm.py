@@ -33,26 +33,40 @@ def _isa() -> str:
     return "avx512" if " avx512f" in flags and " avx512dq" in flags and " avx512vl" in flags else "avx2"
 
 
-def library_path(isa: str | None = None) -> str:
+def library_path(isa: str | None = None, lattice: bool = False) -> str:
+    """The reference library for an instruction set; lattice=True: the build
+    without PVFMM_EXTENDED_BC (periodic lattice sum; AVX2 code only)."""
+    if lattice:
+        return os.path.join(REF_DIR, "libpvfmm_ref_avx2_lattice.so")
     return os.path.join(REF_DIR, f"libpvfmm_ref_{isa or _isa()}.so")
 
 
-def available() -> bool:
-    return os.path.exists(library_path())
+def available(lattice: bool = False) -> bool:
+    return os.path.exists(library_path(lattice=lattice))
 
 
-def load():
-    """Loads the reference library for this host's instruction set.  The
-    reference reads and writes its precompute files in $PVFMM_DIR (or the
-    working directory); a private temporary directory is used when unset."""
+_libs = {}
+
+
+def load(lattice: bool = False):
+    """Loads the reference library for this host's instruction set (or the
+    lattice-sum build).  The reference reads and writes its precompute files
+    in $PVFMM_DIR (or the working directory); a private temporary directory is
+    used when unset.  The two builds write precompute files of the same name
+    with different periodic operators, so the lattice build gets a directory
+    of its own."""
     global _lib
-    if _lib is not None:
-        return _lib
-    path = library_path()
+    if lattice in _libs:
+        return _libs[lattice]
+    path = library_path(lattice=lattice)
     if not os.path.exists(path):
         raise RuntimeError(f"reference library not built: {path} (run oracle/ref_fmm/build.sh)")
     if not os.environ.get("PVFMM_DIR"):
         os.environ["PVFMM_DIR"] = tempfile.mkdtemp(prefix="pvfmm_ref_precomp_")
+    if lattice:
+        # the library reads PVFMM_DIR when a context is created; contexts of
+        # the lattice build are created under a directory of their own
+        _lattice_dir[0] = tempfile.mkdtemp(prefix="pvfmm_ref_precomp_lattice_")
     lib = ctypes.CDLL(path)
     vp, lg = ctypes.c_void_p, ctypes.c_long
     lib.PVFMMCreateContextDWorld.restype = vp
@@ -73,8 +87,15 @@ def load():
     lib.ref_profile_report.argtypes = [vp, lg]
     lib.ref_ptfmm_eval.restype = ctypes.c_int
     lib.ref_ptfmm_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, lg, vp, vp, lg, vp, vp, lg, vp, vp]
-    _lib = lib
+    lib.ref_cheb_integ0.restype = ctypes.c_int
+    lib.ref_cheb_integ0.argtypes = [ctypes.c_int, vp, ctypes.c_double, vp]
+    _libs[lattice] = lib
+    if not lattice:
+        _lib = lib
     return lib
+
+
+_lattice_dir = [None]
 
 
 def _p(a):
@@ -86,16 +107,26 @@ KDIM = {0: (1, 1), 1: (1, 3), 2: (3, 1), 3: (3, 3), 4: (3, 9), 5: (3, 3)}
 
 
 class RefContext:
-    """A reference PVFMM context: free space (box_size = -1), `max_pts`
-    points per leaf, multipole order m, kernel id of the C interface."""
+    """A reference PVFMM context: free space (box_size <= 0) or periodic with
+    period box_size (the 5x5x5-image boundary operator of the default build,
+    or with lattice=True the lattice-sum build), `max_pts` points per leaf,
+    multipole order m, kernel id of the C interface."""
 
-    def __init__(self, kernel: int, m: int, max_pts: int, threads: int = 0):
-        self.lib = load()
+    def __init__(self, kernel: int, m: int, max_pts: int, threads: int = 0, box_size: float = -1.0,
+                 lattice: bool = False):
+        self.lib = load(lattice)
         if threads:
             self.lib.ref_set_threads(threads)
         self.kernel = kernel
         self.k0, self.k1 = KDIM[kernel]
-        self.ctx = self.lib.PVFMMCreateContextDWorld(-1.0, max_pts, m, kernel)
+        saved = os.environ.get("PVFMM_DIR")
+        if lattice:
+            os.environ["PVFMM_DIR"] = _lattice_dir[0]
+        try:
+            self.ctx = self.lib.PVFMMCreateContextDWorld(box_size, max_pts, m, kernel)
+        finally:
+            if lattice and saved is not None:
+                os.environ["PVFMM_DIR"] = saved
         if not self.ctx:
             raise RuntimeError("reference context creation failed")
 
@@ -173,8 +204,8 @@ def profile_report() -> list:
     return rows
 
 
-def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None):
-    ctx = RefContext(kernel, m, max_pts, threads)
+def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None, box_size=-1.0, lattice=False):
+    ctx = RefContext(kernel, m, max_pts, threads, box_size=box_size, lattice=lattice)
     try:
         out = ctx.evaluate(src, den, trg, dl=dl)
         return out, ctx.tree(), ctx.lists()

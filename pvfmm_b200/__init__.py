@@ -80,6 +80,7 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMEvalAdjointDeviceF": (ci, [vp, vp, cl, vp, vp, cl, vp, ci, vp]),
         "PVFMMSetUnitBox": (ci, [vp, ci]),
         "PVFMMSetLayerPoints": (ci, [vp, ci]),
+        "PVFMMSetPeriodicBC": (ci, [vp, ci, vp]),
         "PVFMMKernelEvalD": (ci, [ci, vp, vp, cl, vp, vp, cl]),
         "PVFMMKernelEvalDeviceNoAllocD": (ci, [ci, vp, vp, cl, vp, vp, cl, vp]),
         "PVFMMDestroyContextD": (None, [ctypes.POINTER(vp)]),
@@ -270,6 +271,15 @@ class FMMParticleContext:
         """Tree rule of the reference C++ interface: coordinates used as given
         in [0,1)^3, tree points = targets (PVFMMSetUnitBox)."""
         if self._lib.PVFMMSetUnitBox(self._ptr, int(on)) != 0:
+            raise RuntimeError(last_error())
+
+    def set_periodic_bc(self, lattice: bool = False, m2c: Optional[np.ndarray] = None) -> None:
+        """Boundary operator of a periodic context (box_size > 0; see
+        PVFMMSetPeriodicBC): the 5x5x5-image form of the reference's default
+        build plus an optional (ns*k0) x (ns*k1) operator ``m2c`` (FMM_Pts::
+        SetM2C), or with ``lattice`` the lattice sum over all images."""
+        a = None if m2c is None else np.ascontiguousarray(m2c, dtype=np.float64).reshape(-1)
+        if self._lib.PVFMMSetPeriodicBC(self._ptr, int(bool(lattice)), None if a is None else _ptr(a)) != 0:
             raise RuntimeError(last_error())
 
     def set_layer_points(self, on: bool = True) -> None:

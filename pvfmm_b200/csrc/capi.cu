@@ -62,7 +62,8 @@ void destroy_context(Context& c) {
   DevBuf* tb[] = {&T.key, &T.leaf, &T.parent, &T.child0, &T.src_lo, &T.src_hi, &T.trg_lo, &T.trg_hi, &T.colleague,
                   &T.int_idx, &T.src_perm, &T.trg_perm, &T.src_key, &T.trg_key, &T.src_leaf, &T.trg_leaf, &T.sx,
                   &T.sy, &T.sz, &T.tx, &T.ty, &T.tz, &T.sleaf, &T.tleaf, &T.vsrc, &T.vtrg, &T.node2vsrc, &T.vtab, &T.vmask, &T.vmorton, &T.vunion, &T.vucount, &T.vlocal,
-                  &T.xtrg, &T.x_off, &T.x_list, &T.p_off, &T.p_list, &T.w_off, &T.w_list};
+                  &T.xtrg, &T.x_off, &T.x_list, &T.p_off, &T.p_list, &T.w_off, &T.w_list, &T.p_img, &T.x_img,
+                  &T.w_img, &c.dops.bc};
   for (DevBuf* b : tb) b->release();
   if (c.events_ready)
     for (auto& e : c.ev) cudaEventDestroy(e);
@@ -75,9 +76,20 @@ void destroy_context(Context& c) {
   if (c.side) cudaStreamDestroy(c.side);
 }
 
+// Periodic boundary operator of the context (BC_Type, fmm_pts.txx:790-1232)
+// in device memory: the 5x5x5-image form plus the user's operator, or the
+// lattice sum.
+void upload_bc(Context& c) {
+  std::vector<double> M = build_bc_operator(c.kernel, c.m, c.bc_lattice != 0);
+  if (!c.bc_user.empty())
+    for (size_t i = 0; i < M.size(); ++i) M[i] += c.bc_user[i];
+  double* d = c.dops.bc.as<double>(M.size());
+  PVFMM_CUDA_CHECK(cudaMemcpyAsync(d, M.data(), M.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+}
+
 void* create_context(double box_size, int n, int m, int kernel, int precision, bool float_api) {
   try {
-    if (box_size > 0) throw std::runtime_error("periodic boundary conditions (box_size > 0) are not supported");
     if (n < 1) throw std::runtime_error("max points per leaf must be positive");
     KernelInfo ki;
     if (!kernel_info(kernel, &ki)) throw std::runtime_error("unsupported PVFMMKernel value " + std::to_string(kernel));
@@ -105,6 +117,13 @@ void* create_context(double box_size, int n, int m, int kernel, int precision, b
     for (auto& e : c.ev) PVFMM_CUDA_CHECK(cudaEventCreate(&e));
     c.events_ready = true;
     upload_operators(c);
+    // box_size > 0: periodic boundaries (pvfmm-wrapper.cpp:397-404), with the
+    // boundary operator of the reference's default build
+    if (box_size > 0) {
+      c.periodic = true;
+      c.box_size = box_size;
+      upload_bc(c);
+    }
     set_last_error("");
     return h.release();
   } catch (const std::exception& e) {
@@ -236,12 +255,22 @@ int eval_adjoint(const void* ctx, const T* src, long n_src, const T* trg, const 
   try {
     Handle* h = as_handle(ctx);
     Context& c = h->ctx;
+    // the lattice form takes the mean density's potential out at the targets,
+    // which the role exchange does not transpose
+    if (c.periodic && c.bc_lattice)
+      throw std::runtime_error("the adjoint evaluation needs free space or the 5x5x5-image periodic form");
     if (src == trg && n_src == n_trg)
       return eval_device<T>(ctx, trg, trg_den, nullptr, n_trg, src, src_val, n_src, setup, stream);
     if (!h->adjoint) {
-      h->adjoint = create_context(-1.0, c.max_pts, c.m, c.kernel, c.precision, c.float_api);
+      h->adjoint = create_context(c.periodic ? c.box_size : -1.0, c.max_pts, c.m, c.kernel, c.precision,
+                                  c.float_api);
       if (!h->adjoint) throw std::runtime_error(std::string("companion context: ") + get_last_error());
-      as_handle(h->adjoint)->ctx.unit_box = c.unit_box;
+      Context& a = as_handle(h->adjoint)->ctx;
+      a.unit_box = c.unit_box;
+      if (c.periodic && !c.bc_user.empty()) {  // the periodic images' operator is symmetric in the roles
+        a.bc_user = c.bc_user;
+        upload_bc(a);
+      }
       setup = 1;
     }
     return eval_device<T>(h->adjoint, trg, trg_den, nullptr, n_trg, src, src_val, n_src, setup, stream);
@@ -280,6 +309,41 @@ void* PVFMMCreateContextFWorld(float box_size, int n, int m, enum PVFMMKernel ke
 }
 void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision) {
   return create_context(box_size, n, m, (int)kernel, precision, false);
+}
+
+int PVFMMSetPeriodicBC(void* ctx, int lattice, const double* m2c) {
+  try {
+    Context& c = as_handle(ctx)->ctx;
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    if (!c.periodic) throw std::runtime_error("the context has free-space boundaries (box_size <= 0)");
+    if (lattice != 0 && lattice != 1) throw std::runtime_error("lattice must be 0 or 1");
+    if (lattice && m2c) throw std::runtime_error("a user operator adds to the 5x5x5-image form only (lattice 0)");
+    if (lattice && !lattice_bc_supported(c.kernel))
+      throw std::runtime_error("the periodic lattice sum needs the LaplacePotential, LaplaceGradient or "
+                               "StokesVelocity kernel");
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // no evaluation reads the operator while it changes
+    const int kin = c.hops.kin, kout = c.hops.kout;
+    std::vector<double> user;
+    if (m2c) user.assign(m2c, m2c + (size_t)c.ns * kin * c.ns * kout);
+    const int old_lattice = c.bc_lattice;
+    std::vector<double> old_user = c.bc_user;
+    c.bc_lattice = lattice;
+    c.bc_user = std::move(user);
+    try {
+      upload_bc(c);
+    } catch (...) {
+      c.bc_lattice = old_lattice;
+      c.bc_user = std::move(old_user);
+      throw;
+    }
+    Handle* h = as_handle(ctx);
+    if (h->adjoint) destroy(&h->adjoint);  // rebuilt with the new operator on its next use
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return -1;
+  }
 }
 
 void PVFMMEvalD(const double* src_pos, const double* sl_den, const double* dl_den, long n_src, const double* trg_pos,
@@ -548,8 +612,21 @@ long PVFMMGetTreeData(const void* ctx, int what, void* out, long n) {
 long PVFMMPrecompOperator(enum PVFMMKernel kernel, int m, int precision, int which, double* out, long n) {
   static std::mutex mu;
   static HostOperators ops;
+  static std::vector<double> bc;
+  static int bc_kernel = -1, bc_m = 0, bc_which = 0;
   std::lock_guard<std::mutex> lock(mu);
   try {
+    if (which == 9 || which == 10) {  // periodic boundary operator: 5x5x5 images / lattice sum
+      if (bc_kernel != (int)kernel || bc_m != m || bc_which != which) {
+        bc_kernel = -1;
+        bc = build_bc_operator((int)kernel, m, which == 10);
+        bc_kernel = (int)kernel;
+        bc_m = m;
+        bc_which = which;
+      }
+      if (out && n > 0) std::memcpy(out, bc.data(), sizeof(double) * std::min<long>(n, (long)bc.size()));
+      return (long)bc.size();
+    }
     if (ops.kernel != (int)kernel || ops.m != m || ops.mixed != (precision == 1))
       build_operators((int)kernel, m, precision == 1, ops);
     const std::vector<double>* v = nullptr;

@@ -62,6 +62,14 @@ __device__ __forceinline__ void node_geom(const MKey& k, double& cx, double& cy,
   depth = (int)d;
 }
 
+// Periodic boundaries: moves a source node's centre by the unit-cube image
+// shift of its list entry (code (sx+1) + 3(sy+1) + 9(sz+1)).
+__device__ __forceinline__ void image_shift(unsigned char code, double& cx, double& cy, double& cz) {
+  cx += (double)(code % 3) - 1.0;
+  cy += (double)((code / 3) % 3) - 1.0;
+  cz += (double)(code / 9) - 1.0;
+}
+
 // ---------------------------------------------------------------------------
 // Source tiles in shared memory and the per-thread evaluation loop.
 // ---------------------------------------------------------------------------
@@ -502,11 +510,12 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
     near_field_kernel(const int* __restrict__ tleaf, const MKey* __restrict__ keys, const int* __restrict__ tlo,
                       const int* __restrict__ thi, const int* __restrict__ slo, const int* __restrict__ shi,
                       const int* __restrict__ p_off, const int* __restrict__ p_list, const int* __restrict__ w_off,
-                      const int* __restrict__ w_list, const double* __restrict__ tx, const double* __restrict__ ty,
-                      const double* __restrict__ tz, const double* __restrict__ sx, const double* __restrict__ sy,
-                      const double* __restrict__ sz, const double* __restrict__ den, const double* __restrict__ ue,
-                      const double* __restrict__ de, const double* __restrict__ usurf, int ns, double scale,
-                      int with_p2p, double* __restrict__ pot) {
+                      const int* __restrict__ w_list, const unsigned char* __restrict__ p_img,
+                      const unsigned char* __restrict__ w_img, const double* __restrict__ tx,
+                      const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ sx,
+                      const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ den,
+                      const double* __restrict__ ue, const double* __restrict__ de, const double* __restrict__ usurf,
+                      int ns, double scale, int with_p2p, double* __restrict__ pot) {
   constexpr int KS = KerDims<Ker>::KS, KT = KerDims<Ker>::KT;
   constexpr bool kF32 = sizeof(Real) == 4;
   constexpr bool kPacked = kF32 && kHasPacked<Ker>;
@@ -598,10 +607,12 @@ __global__ void __launch_bounds__(kNF, sizeof(Real) == 8       ? PVFMM_NEAR_MIN_
           cnt = ns;
         } else {
           const bool is_w = e < nD + nW;
-          const int S = is_w ? w_list[wb + e - nD] : p_list[pbeg + e - nD - nW];
+          const int q = is_w ? wb + e - nD : pbeg + e - nD - nW;
+          const int S = is_w ? w_list[q] : p_list[q];
           double sxc, syc, szc, sh;
           int dS;
           node_geom(keys[S], sxc, syc, szc, sh, dS);
+          if (p_img) image_shift(is_w ? w_img[q] : p_img[q], sxc, syc, szc);
           sg.ox = (float)(sxc - cx);
           sg.oy = (float)(syc - cy);
           sg.oz = (float)(szc - cz);
@@ -744,7 +755,8 @@ template <int Ker, bool Surface1 = false>
 __global__ void __launch_bounds__(kNT) surface_check_kernel(
     int mode, const int* __restrict__ nodes, const MKey* __restrict__ keys, const int* __restrict__ slo,
     const int* __restrict__ shi, const int* __restrict__ x_off, const int* __restrict__ x_list,
-    const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz,
+    const unsigned char* __restrict__ x_img, const double* __restrict__ sx, const double* __restrict__ sy,
+    const double* __restrict__ sz,
     const double* __restrict__ den, const double* __restrict__ usurf, int ns, double rad, double scale, int deg,
     double* __restrict__ out) {
   constexpr int KT = KerDims<Ker>::KT;
@@ -819,6 +831,7 @@ __global__ void __launch_bounds__(kNT) surface_check_kernel(
         double sxc, syc, szc, sh;
         int dS;
         node_geom(keys[S], sxc, syc, szc, sh, dS);
+        if (x_img) image_shift(x_img[q], sxc, syc, szc);
         point_sources<double, Ker>(tl, sx, sy, sz, den, slo[S], shi[S], sxc - cx, syc - cy, szc - cz, sp, pt, acc);
       }
     }
@@ -2013,6 +2026,45 @@ __global__ void sort_densities(const Tin* __restrict__ in, const int* __restrict
   for (int j = 0; j < k; ++j) out[i * k + j] = (double)((Tin)in[p * k + j] * (Tin)sc.v[j]);
 }
 
+// Periodic lattice sum: subtracts from every target value the volume
+// potential of the mean source density, taken as the sum of the root's
+// upward equivalent density per component (the reference's PostProcessing,
+// fmm_pts.txx:5741-5771, with laplace_vol_poten -|x|^2/6 and
+// stokes_vol_poten -(|x|^2 - x_l^2)/4 of kernel.txx:1289-1295, 1456-1467) at
+// the target's unit-cube position x.  kin = k1 = 1 (Laplace potential) or 3
+// (Stokes velocity).  Every block forms the sums itself (ns*kin values).
+__global__ void __launch_bounds__(256) periodic_mean_correction(
+    long n_trg, const int* __restrict__ trg_leaf, const MKey* __restrict__ keys, const double* __restrict__ tx,
+    const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ ue_root, int ns, int kin,
+    int k1, double* __restrict__ pot) {
+  __shared__ double part[256][3];
+  __shared__ double avg[3];
+  double a[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < ns; i += blockDim.x)
+    for (int k = 0; k < kin && k < 3; ++k) a[k] += ue_root[(long)i * kin + k];
+  for (int k = 0; k < 3; ++k) part[threadIdx.x][k] = a[k];
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0;
+    for (int j = 0; j < (int)blockDim.x; ++j) v += part[j][threadIdx.x];
+    avg[threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n_trg; t += (long)gridDim.x * blockDim.x) {
+    double cx, cy, cz, half;
+    int d;
+    node_geom(keys[trg_leaf[t]], cx, cy, cz, half, d);
+    const double x = tx[t] + cx, y = ty[t] + cy, z = tz[t] + cz;
+    if (k1 == 1) {
+      pot[t] += avg[0] * (x * x + y * y + z * z) / 6;
+    } else {
+      pot[t * 3 + 0] += avg[0] * (y * y + z * z) / 4;
+      pot[t * 3 + 1] += avg[1] * (x * x + z * z) / 4;
+      pot[t * 3 + 2] += avg[2] * (x * x + y * y) / 4;
+    }
+  }
+}
+
 template <class Tout>
 __global__ void unsort_values(const double* __restrict__ pot, const int* __restrict__ perm, long n, int k1,
                               OutScales sc, Tout* __restrict__ out) {
@@ -2209,6 +2261,10 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   const int k0 = ctx.ki.k0, k1 = ctx.ki.k1;
   const long N = T.n_nodes;
   const MKey* keys = T.key.get<MKey>();
+  // periodic boundaries: image codes of the list entries (null: free space)
+  const unsigned char* pimg = ctx.periodic ? T.p_img.get<unsigned char>() : nullptr;
+  const unsigned char* wimg = ctx.periodic ? T.w_img.get<unsigned char>() : nullptr;
+  const unsigned char* ximg = ctx.periodic ? T.x_img.get<unsigned char>() : nullptr;
   const std::function<void(int)> ev = [&](int i) {
     if (ctx.events_ready) PVFMM_CUDA_CHECK(cudaEventRecord(ctx.ev[i], s));
   };
@@ -2279,13 +2335,13 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
     // potential error from 3e-7 to 2.5e-6)
     if (has_sl)
       surface_check_kernel<KerExp, false><<<T.n_sleaf, kNT, 0, s>>>(
-          0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, deg,
+          0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, nullptr, sx, sy, sz, den, usurf, ns, kRad1, kscale_exp, deg,
           uc);
     if constexpr (KerDblExp >= 0) {
       if (has_dl) {
         ++ctx.n_launch;
         surface_check_kernel<KerDblExp, false><<<T.n_sleaf, kNT, 0, s>>>(
-            has_sl ? 2 : 0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, sx, sy, sz, surf, usurf, ns, kRad1,
+            has_sl ? 2 : 0, T.sleaf.get<int>(), keys, slo, shi, nullptr, nullptr, nullptr, sx, sy, sz, surf, usurf, ns, kRad1,
             ker_scale(KerDblExp), deg, uc);
       }
     }
@@ -2334,6 +2390,13 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
     }
   }
   if (!proj32) ue32 = ue;
+  // periodic boundaries (PeriodicBC, fmm_pts.txx:2642-2676): the root's
+  // downward check potential of the images beyond its 3x3x3 block
+  if (ctx.periodic && T.src_counted && N > 0) {
+    ++ctx.n_launch;
+    translate_gemm(s, 1, dout, din, ue, din, nullptr, ctx.dops.bc.get<double>(), dout, dc, dout, nullptr, nullptr,
+                   true);
+  }
   ev(3);
   // ---- V-list
   if (T.src_counted && T.n_vtrg > 0 && T.n_vsrc > 0) {
@@ -2352,13 +2415,13 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
     ++ctx.n_launch;
     if (has_sl)
       surface_check_kernel<KerExp><<<T.n_xtrg, kNT, 0, s>>>(1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(),
-                                                             T.x_list.get<int>(), sx, sy, sz, den, usurf, ns, kRad0,
+                                                             T.x_list.get<int>(), ximg, sx, sy, sz, den, usurf, ns, kRad0,
                                                              kscale_exp, deg, dc);
     if constexpr (KerDblExp >= 0) {
       if (has_dl) {
         ++ctx.n_launch;
         surface_check_kernel<KerDblExp><<<T.n_xtrg, kNT, 0, s>>>(
-            1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(), T.x_list.get<int>(), sx, sy, sz, surf, usurf,
+            1, T.xtrg.get<int>(), keys, slo, shi, T.x_off.get<int>(), T.x_list.get<int>(), ximg, sx, sy, sz, surf, usurf,
             ns, kRad0, ker_scale(KerDblExp), deg, dc);
       }
     }
@@ -2389,20 +2452,29 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
     ++ctx.n_launch;
     near_field_kernel<Real, KerS2T><<<T.n_tleaf, kNF, 0, s>>>(
         T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
-        T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
-        T.tz.get<double>(), sx, sy, sz, den, ue32, T.src_counted ? de : nullptr, usurf, ns, ker_scale(KerS2T),
-        has_sl ? 1 : 0, pot);
+        T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), pimg, wimg, T.tx.get<double>(),
+        T.ty.get<double>(), T.tz.get<double>(), sx, sy, sz, den, ue32, T.src_counted ? de : nullptr, usurf, ns,
+        ker_scale(KerS2T), has_sl ? 1 : 0, pot);
     if constexpr (KerDblS2T >= 0) {
       if (has_dl) {  // the double layer's P2P sources, added
         ++ctx.n_launch;
         near_field_kernel<Real, KerDblS2T, true><<<T.n_tleaf, kNF, 0, s>>>(
             T.tleaf.get<int>(), keys, T.trg_lo.get<int>(), T.trg_hi.get<int>(), slo, shi, T.p_off.get<int>(),
-            T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), T.tx.get<double>(), T.ty.get<double>(),
-            T.tz.get<double>(), sx, sy, sz, surf, nullptr, nullptr, usurf, ns, ker_scale(KerDblS2T), 1, pot);
+            T.p_list.get<int>(), T.w_off.get<int>(), T.w_list.get<int>(), pimg, wimg, T.tx.get<double>(),
+            T.ty.get<double>(), T.tz.get<double>(), sx, sy, sz, surf, nullptr, nullptr, usurf, ns,
+            ker_scale(KerDblS2T), 1, pot);
       }
     }
   } else {
     ev(12);
+  }
+  // periodic lattice sum of a kernel with a volume potential: the potential
+  // of the mean density is taken out (PostProcessing, fmm_pts.txx:5741-5771)
+  if (ctx.periodic && ctx.bc_lattice && T.src_counted && T.n_trg > 0 &&
+      (ctx.kernel == kLaplacePot || ctx.kernel == kStokesVel)) {
+    ++ctx.n_launch;
+    periodic_mean_correction<<<592, 256, 0, s>>>(T.n_trg, T.trg_leaf.get<int>(), keys, T.tx.get<double>(),
+                                                 T.ty.get<double>(), T.tz.get<double>(), ue, ns, kin, k1, pot);
   }
   ev(9);
   // ---- output in input order, scaled by scale_x^trg_scal

@@ -55,6 +55,9 @@ struct DevTree {
   DevBuf x_off, x_list;               // CSR over xtrg
   DevBuf p_off, p_list;               // CSR over tleaf: P2P source leaves
   DevBuf w_off, w_list;               // CSR over tleaf: W source nodes
+  // periodic boundaries: the image code of each p / x / w list entry
+  // ((sx+1) + 3(sy+1) + 9(sz+1), the unit-cube shift that places the source)
+  DevBuf p_img, x_img, w_img;
   long n_p2p = 0, n_x = 0, n_w = 0;   // list sizes
   double scale_x = 1, shift_x[3] = {0, 0, 0};
   bool valid = false;
@@ -66,6 +69,7 @@ struct DevOps {
   DevBuf vop_frag;  // mixed form: Hadamard operators as TF32 hi/lo MMA fragments
   DevBuf vop_tc5;   // mixed form, ke = 1: Hadamard operators in the tcgen05 shared-memory layout
   DevBuf ue_basis;  // mixed Stokes form: din x r32, the upward directions above the FP32 cutoff
+  DevBuf bc;        // periodic boundaries: din x dout, root upward equivalent -> root downward check
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
 };
@@ -87,6 +91,13 @@ struct Context {
   // the cutoff kept, padded to even (upward ru, downward rd); the first r32
   // upward ones span the mixed Stokes form's projection (0 otherwise)
   int ru = 0, rd = 0, r32 = 0;
+  // periodic boundaries (box_size > 0): points scaled by 1 / box_size and
+  // wrapped into the unit cube; bc_lattice selects the lattice-sum operator,
+  // bc_user an operator added to the 5x5x5-image one (empty: none)
+  bool periodic = false;
+  double box_size = 0;
+  int bc_lattice = 0;
+  std::vector<double> bc_user;
   DevTree tree;
   cudaStream_t stream = nullptr;
   int device = 0;

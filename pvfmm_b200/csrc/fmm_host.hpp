@@ -81,6 +81,16 @@ struct HostOperators {
 // (and so for D2D), the mixed form's downward chain.
 void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool down_eps32 = false);
 
+// Periodic boundary operator (BoundaryType Periodic, fmm_pts.txx:790-1232):
+// (ns*kin) x (ns*kout), root upward equivalent density -> root downward check
+// potential of the periodic images outside the root's 3x3x3 block.  lattice
+// false: the images of the 5x5x5 block (the reference built with
+// PVFMM_EXTENDED_BC, its CMake default), any kernel; lattice true: the full
+// lattice sum (the option off), for the kernels lattice_bc_supported()
+// accepts (Laplace potential and gradient, Stokes velocity); throws otherwise.
+bool lattice_bc_supported(int kernel);
+std::vector<double> build_bc_operator(int kernel, int m, bool lattice);
+
 // One-sided Jacobi SVD of a rows x cols row-major matrix (rows >= cols):
 // A = U diag(S) V^T with U rows x cols (column j scaled to unit length, or
 // zero when S_j == 0), V cols x cols.  Public for the CPU tests.

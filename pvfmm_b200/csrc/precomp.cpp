@@ -605,4 +605,329 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
   }
 }
 
+// ---------------------------------------------------------------------------
+// Periodic boundary operator (the reference's BC_Type precompute for
+// BoundaryType Periodic == PXYZ, include/fmm_pts.txx:790-1232): the linear
+// map from the root's upward equivalent density to the downward check
+// potential of the periodic images outside the root's 3x3x3 block.  Two
+// forms, as the reference's build option PVFMM_EXTENDED_BC selects: the
+// images of the 5x5x5 block only (option on, the reference's CMake default;
+// a user operator may be added to it), or the lattice sum over all images
+// (option off: 45 levels of coarsened images, zero-average projections, the
+// far field of the unit volume potential and the corner correction; all
+// products at order m+2 and brought back to order m at the end).
+// ---------------------------------------------------------------------------
+namespace {
+
+// Gauss-Legendre nodes and weights on [0, 1] (Newton iteration on P_n from
+// the Chebyshev-like initial guesses cos(pi (i + 3/4) / (n + 1/2))).
+void gauss_legendre01(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double z = std::cos(kPi * (i + 0.75) / (n + 0.5)), dp = 1;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = 0.5 * (1 - z);
+    w[i] = 1.0 / ((1 - z * z) * dp * dp);  // 2 / ((1 - z^2) P_n'^2) on [-1, 1], halved
+  }
+}
+
+// Integral of the expansion kernel (homogeneous of degree -1) over the box
+// [lo, lo + side]^3 at target x, out[k*ke + l] for source component k and
+// target component l: the box is the signed union of the six pyramids with
+// apex x over its faces, and along each pyramid's rays the degree -1 kernel
+// integrates in closed form, leaving (h_F / 2) int_F K(x - z) dA_z with h_F
+// the signed distance from x to face F (outward normal).  The faces are
+// smooth integrands for targets off their planes: composite Gauss-Legendre,
+// panels of side <= 1/2 with 16 x 16 nodes.  (The reference evaluates these
+// integrals with its Chebyshev quadrature, cheb_integ, include/cheb_utils.txx:1037.)
+void box_integral(int exp_kernel, int ke, const double* x, double lo, double side, double* out) {
+  static thread_local std::vector<double> gx, gw;
+  if (gx.empty()) gauss_legendre01(16, gx, gw);
+  const int G = (int)gx.size();
+  const int P = std::max(1, (int)std::ceil(side / 0.5 - 1e-12));
+  const double ps = side / P;
+  std::vector<double> nodes, wts, K;
+  for (int i = 0; i < ke * ke; ++i) out[i] = 0;
+  for (int f = 0; f < 6; ++f) {
+    const int a = f >> 1;               // normal axis
+    const double plane = lo + ((f & 1) ? side : 0.0);
+    const double h = (f & 1) ? plane - x[a] : x[a] - plane;  // outward normal distance from x
+    if (h == 0.0) continue;
+    const int b = (a + 1) % 3, c = (a + 2) % 3;
+    nodes.clear();
+    wts.clear();
+    for (int pb = 0; pb < P; ++pb)
+      for (int pc = 0; pc < P; ++pc)
+        for (int ib = 0; ib < G; ++ib)
+          for (int ic = 0; ic < G; ++ic) {
+            double z[3];
+            z[a] = plane;
+            z[b] = lo + (pb + gx[ib]) * ps;
+            z[c] = lo + (pc + gx[ic]) * ps;
+            nodes.insert(nodes.end(), z, z + 3);
+            wts.push_back(gw[ib] * gw[ic] * ps * ps);
+          }
+    const int n = (int)wts.size();
+    K.resize((size_t)n * ke * ke);
+    exp_kernel_matrix(exp_kernel, nodes.data(), n, x, 1, K.data());  // [i*ke + k][l]
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < ke; ++k)
+        for (int l = 0; l < ke; ++l) out[k * ke + l] += 0.5 * h * wts[i] * K[((size_t)i * ke + k) * ke + l];
+  }
+}
+
+// Surface of order p around the box with lower corner c at depth `depth`
+// (side 2^-depth) scaled by rad about its centre (u_equiv_surf and its
+// siblings, include/fmm_pts.txx:54-160).
+std::vector<double> box_surface(const std::vector<double>& u, const double* c, int depth, double rad) {
+  const double r = 0.5 * std::ldexp(1.0, -depth);
+  const double ctr[3] = {c[0] + r, c[1] + r, c[2] + r};
+  return place_surface(u, ctr, r, rad);
+}
+
+std::vector<double> kmat(int exp_kernel, int ke, const std::vector<double>& src, const std::vector<double>& trg) {
+  const int ns = (int)src.size() / 3, nt = (int)trg.size() / 3;
+  std::vector<double> M((size_t)ns * ke * nt * ke);
+  exp_kernel_matrix(exp_kernel, src.data(), ns, trg.data(), nt, M.data());
+  return M;
+}
+
+// The reference's volume potential of a unit density (vol_poten, kernel.txx:
+// 1289-1295 Laplace, :1456-1467 Stokes) at n points: out[k][i*ke + l].
+void vol_poten(int exp_kernel, const double* p, int n, double* out) {
+  const int ke = exp_kernel == kExpStokes ? 3 : 1;
+  for (int i = 0; i < n * ke * ke; ++i) out[i] = 0;
+  for (int i = 0; i < n; ++i) {
+    const double x = p[3 * i], y = p[3 * i + 1], z = p[3 * i + 2];
+    if (ke == 1) {
+      out[i] = -(x * x + y * y + z * z) / 6;
+    } else {
+      const double r2[3] = {y * y + z * z, x * x + z * z, x * x + y * y};
+      for (int k = 0; k < 3; ++k) out[(size_t)k * n * 3 + i * 3 + k] = -r2[k] / 4;
+    }
+  }
+}
+
+}  // namespace
+
+bool lattice_bc_supported(int kernel) { return kernel == kLaplacePot || kernel == kLaplaceGrad || kernel == kStokesVel; }
+
+std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
+  KernelInfo ki;
+  if (!kernel_info_host(kernel, &ki)) throw std::runtime_error("periodic boundaries: unknown kernel");
+  if (!lattice) {
+    // the reference's default build (PVFMM_EXTENDED_BC, :1189-1232): the
+    // images in [-2, 2]^3 outside [-1, 1]^3 at order m, nothing beyond them
+    int kin, kout;
+    exp_kernel_dims(ki.exp_kernel, &kin, &kout);
+    const std::vector<double> u = unit_surface(m);
+    const int ns = (int)u.size() / 3;
+    const double zero[3] = {0, 0, 0};
+    const std::vector<double> dk = box_surface(u, zero, 0, kRad0);
+    std::vector<double> M((size_t)ns * kin * ns * kout, 0.0), T(M.size());
+    for (int x0 = -2; x0 <= 2; ++x0)
+      for (int x1 = -2; x1 <= 2; ++x1)
+        for (int x2 = -2; x2 <= 2; ++x2) {
+          if (std::abs(x0) <= 1 && std::abs(x1) <= 1 && std::abs(x2) <= 1) continue;
+          const double c[3] = {(double)x0, (double)x1, (double)x2};
+          const std::vector<double> src = box_surface(u, c, 0, kRad0);
+          exp_kernel_matrix(ki.exp_kernel, src.data(), ns, dk.data(), ns, T.data());
+          for (size_t i = 0; i < M.size(); ++i) M[i] += T[i];
+        }
+    return M;
+  }
+  if (!lattice_bc_supported(kernel)) throw std::runtime_error("periodic lattice sum: kernel not supported");
+  const int ex = ki.exp_kernel, ke = ki.ke;
+  // the reference attaches the volume potential to the Laplace potential and
+  // Stokes velocity kernels only (the gradient kernel's expansion kernel has none)
+  const bool has_vol = kernel == kLaplacePot || kernel == kStokesVel;
+  const int m1 = m + 2;  // mult_upsample = 2
+  const std::vector<double> u1 = unit_surface(m1), u0 = unit_surface(m);
+  const int ns1 = (int)u1.size() / 3, ns0 = (int)u0.size() / 3;
+  const int n1 = ns1 * ke, n0 = ns0 * ke;
+  const double eps = std::ldexp(1.0, -52);
+  const double zero[3] = {0, 0, 0}, mone[3] = {-1, -1, -1}, mhalf[3] = {-0.5, -0.5, -0.5};
+  // pseudo-inverse factors at order m1, depth 0 (side 1); depth -1 (side 2)
+  // follows from homogeneity: the kernel matrices scale by 2^-deg, their
+  // pseudo-inverses by 2^deg
+  std::vector<double> uc0, uc1, dc0, dc1;
+  pinv_factors(kmat(ex, ke, box_surface(u1, zero, 0, kRad0), box_surface(u1, zero, 0, kRad1)), n1, n1, eps, uc0, uc1);
+  pinv_factors(kmat(ex, ke, box_surface(u1, zero, 0, kRad1), box_surface(u1, zero, 0, kRad0)), n1, n1, eps, dc0, dc1);
+  const double up = std::ldexp(1.0, ki.deg);
+  std::vector<double> uc0m(uc0), dc0m(dc0);
+  for (double& v : uc0m) v *= up;
+  for (double& v : dc0m) v *= up;
+  auto add = [](std::vector<double>& a, const std::vector<double>& b) {
+    for (size_t i = 0; i < a.size(); ++i) a[i] += b[i];
+  };
+  // zero-average projections (:859-911): Pe removes from an equivalent
+  // density the multiple of a unit volume source (row-normalised), Pc the
+  // mean of each check-potential component
+  std::vector<double> Pe((size_t)n1 * n1, 0.0), Pc((size_t)n1 * n1, 0.0);
+  {
+    const std::vector<double> uc = box_surface(u1, zero, 0, kRad1);
+    std::vector<double> s2c((size_t)ke * n1);
+    std::vector<double> I(ke * ke);
+    for (int i = 0; i < ns1; ++i) {
+      box_integral(ex, ke, &uc[3 * i], 0.0, 1.0, I.data());
+      for (int j = 0; j < ke; ++j)
+        for (int k = 0; k < ke; ++k) s2c[(size_t)j * n1 + i * ke + k] = I[k * ke + j];
+    }
+    std::vector<double> s2e = matmul(matmul(s2c, uc0, ke, n1, n1), uc1, ke, n1, n1);
+    for (int j = 0; j < ke; ++j) {
+      double s = 0;
+      for (int c = 0; c < n1; ++c) s += s2e[(size_t)j * n1 + c];
+      for (int c = 0; c < n1; ++c) s2e[(size_t)j * n1 + c] /= s;
+    }
+    for (int r = 0; r < n1; ++r) {
+      Pe[(size_t)r * n1 + r] += 1;
+      Pc[(size_t)r * n1 + r] += 1;
+      for (int c = 0; c < n1; ++c) Pe[(size_t)r * n1 + c] -= s2e[(size_t)(r % ke) * n1 + c];
+    }
+    for (int i = 0; i < ns1; ++i)
+      for (int j = 0; j < ns1; ++j)
+        for (int k = 0; k < ke; ++k) Pc[((size_t)i * ke + k) * n1 + j * ke + k] -= 1.0 / ns1;
+  }
+  // M2M: the 8 children (side 1) of a side-2 parent, each with the same
+  // equivalent density, to the parent's equivalent density
+  std::vector<double> M2M((size_t)n1 * n1, 0.0);
+  {
+    const std::vector<double> ck = box_surface(u1, mone, -1, kRad1);
+    for (int c = 0; c < 8; ++c) {
+      const double sb[3] = {-1.0 + (c & 1), -1.0 + ((c >> 1) & 1), -1.0 + ((c >> 2) & 1)};
+      add(M2M, kmat(ex, ke, box_surface(u1, sb, 0, kRad0), ck));
+    }
+    M2M = matmul(matmul(M2M, uc0m, n1, n1, n1), uc1, n1, n1, n1);
+  }
+  // L2L: parent (side 2) downward check -> child (side 1) downward check
+  std::vector<double> L2L =
+      matmul(dc0m, matmul(dc1, kmat(ex, ke, box_surface(u1, mone, -1, kRad1), box_surface(u1, mone, 0, kRad0)), n1,
+                          n1, n1),
+             n1, n1, n1);
+  // M2L: the images at offsets in [-2, 3]^3 outside [-1, 1]^3 to the root's
+  // downward check surface
+  std::vector<double> M2L((size_t)n1 * n1, 0.0);
+  {
+    const std::vector<double> dk = box_surface(u1, zero, 0, kRad0);
+    for (int k0 = -2; k0 < 4; ++k0)
+      for (int k1 = -2; k1 < 4; ++k1)
+        for (int k2 = -2; k2 < 4; ++k2) {
+          if (std::abs(k0) <= 1 && std::abs(k1) <= 1 && std::abs(k2) <= 1) continue;
+          const double sb[3] = {(double)k0, (double)k1, (double)k2};
+          add(M2L, kmat(ex, ke, box_surface(u1, sb, 0, kRad0), dk));
+        }
+  }
+  M2M = matmul(matmul(Pe, M2M, n1, n1, n1), Pe, n1, n1, n1);
+  L2L = matmul(matmul(Pc, L2L, n1, n1, n1), Pc, n1, n1, n1);
+  M2L = matmul(matmul(Pe, M2L, n1, n1, n1), Pc, n1, n1, n1);
+  // lattice levels (PVFMM_BC_LEVELS = 45): M = M2L + M2M (Pr M Pc) L2L, the
+  // level scalings Pr = 2^-src_scal = 1 and Pc = 2^-trg_scal = 2^-deg of the
+  // degree -deg expansion kernel
+  std::vector<double> M = M2L;
+  const double pc = std::ldexp(1.0, -ki.deg);
+  for (int level = 1; level < 45; ++level) {
+    std::vector<double> T = matmul(matmul(M2M, M, n1, n1, n1), L2L, n1, n1, n1);
+    for (size_t i = 0; i < M.size(); ++i) M[i] = M2L[i] + pc * T[i];
+  }
+  // far field of the unit volume potential (:1001-1034): the analytic
+  // potential minus the 3x3x3 block's integral, on the check surface of the
+  // block's centre box
+  if (has_vol) {
+    const double c1[3] = {1, 1, 1};
+    const std::vector<double> dc = box_surface(u1, c1, 0, kRad0);
+    std::vector<double> far((size_t)ke * n1);
+    vol_poten(ex, dc.data(), ns1, far.data());
+    std::vector<double> I(ke * ke);
+    for (int i = 0; i < ns1; ++i) {
+      box_integral(ex, ke, &dc[3 * i], 0.0, 3.0, I.data());
+      for (int j = 0; j < ke; ++j)
+        for (int k = 0; k < ke; ++k) far[(size_t)j * n1 + i * ke + k] -= I[k * ke + j];
+    }
+    for (int i = 0; i < ns1; ++i)
+      for (int k = 0; k < ke; ++k)
+        for (int j = 0; j < n1; ++j) M[((size_t)i * ke + k) * n1 + j] += far[(size_t)k * n1 + j];
+  }
+  // corner correction (:1036-1161): the constant and linear parts of the
+  // potential, fitted to its values at the root's 8 corners (the far images
+  // through M, the 3x3x3 block's images through the upward equivalent
+  // surface), are removed on the check surface
+  {
+    double corner[24];
+    for (int i = 0; i < 8; ++i) {
+      corner[3 * i] = i & 1;
+      corner[3 * i + 1] = (i >> 1) & 1;
+      corner[3 * i + 2] = (i >> 2) & 1;
+    }
+    const std::vector<double> ue = box_surface(u1, zero, 0, kRad0), de = box_surface(u1, zero, 0, kRad1),
+                              dk = box_surface(u1, zero, 0, kRad0);
+    const std::vector<double> cp(corner, corner + 24);
+    std::vector<double> cv =
+        matmul(matmul(M, dc0, n1, n1, n1), matmul(dc1, kmat(ex, ke, de, cp), n1, n1, 8 * ke), n1, n1, 8 * ke);
+    for (int k = 0; k < 8; ++k)
+      for (int j0 = -1; j0 <= 1; ++j0)
+        for (int j1 = -1; j1 <= 1; ++j1)
+          for (int j2 = -1; j2 <= 1; ++j2) {
+            const std::vector<double> pt = {corner[3 * k] - j0, corner[3 * k + 1] - j1, corner[3 * k + 2] - j2};
+            if (std::fabs(pt[0] - 0.5) < 1 && std::fabs(pt[1] - 0.5) < 1 && std::fabs(pt[2] - 0.5) < 1) continue;
+            const std::vector<double> E = kmat(ex, ke, ue, pt);  // n1 x ke
+            for (int i = 0; i < n1; ++i)
+              for (int l = 0; l < ke; ++l) cv[(size_t)i * 8 * ke + k * ke + l] += E[(size_t)i * ke + l];
+          }
+    if (has_vol) {
+      std::vector<double> va((size_t)ke * 8 * ke);
+      vol_poten(ex, corner, 8, va.data());
+      for (int j = 0; j < ns1; ++j)
+        for (int k = 0; k < ke; ++k)
+          for (int i = 0; i < 8 * ke; ++i) cv[((size_t)j * ke + k) * 8 * ke + i] -= va[(size_t)k * 8 * ke + i];
+    }
+    // coefficients of a + bx + cy + dz + exy + fxz + gyz + hxyz through the
+    // inverse of the corners' Vandermonde matrix (nonsingular); the constant
+    // and linear terms are enabled for PXYZ
+    std::vector<double> V(64), Vi;
+    for (int i = 0; i < 8; ++i) {
+      const double x = corner[3 * i], y = corner[3 * i + 1], z = corner[3 * i + 2];
+      const double row[8] = {1, x, y, z, x * y, x * z, y * z, x * y * z};
+      for (int r = 0; r < 8; ++r) V[r * 8 + i] = row[r];
+    }
+    {
+      std::vector<double> c0, c1;
+      pinv_factors(V, 8, 8, eps, c0, c1);
+      Vi = matmul(c0, c1, 8, 8, 8);  // V^+ (8 x 8)
+    }
+    for (int i = 0; i < n1; ++i)
+      for (int l = 0; l < ke; ++l) {
+        // values of equivalent entry i, check component l at the 8 corners
+        double coef[4] = {0, 0, 0, 0};
+        for (int q = 0; q < 4; ++q)
+          for (int k = 0; k < 8; ++k) coef[q] += cv[(size_t)i * 8 * ke + k * ke + l] * Vi[k * 8 + q];
+        for (int p = 0; p < ns1; ++p)
+          M[(size_t)i * n1 + p * ke + l] -=
+              coef[0] + coef[1] * dk[3 * p] + coef[2] * dk[3 * p + 1] + coef[3] * dk[3 * p + 2];
+      }
+  }
+  // back to order m (:1164-1188): order-m equivalent -> order-m1 equivalent,
+  // order-m1 downward equivalent -> order-m check
+  std::vector<double> up_m =
+      matmul(matmul(kmat(ex, ke, box_surface(u0, mhalf, 0, kRad0), box_surface(u1, mhalf, 0, kRad1)), uc0, n0, n1,
+                    n1),
+             uc1, n0, n1, n1);
+  std::vector<double> dn_m =
+      matmul(dc0, matmul(dc1, kmat(ex, ke, box_surface(u1, mhalf, 0, kRad1), box_surface(u0, mhalf, 0, kRad0)), n1,
+                         n1, n0),
+             n1, n1, n0);
+  return matmul(matmul(up_m, M, n0, n1, n1), dn_m, n0, n1, n0);
+}
+
 }  // namespace pvfmm_b200

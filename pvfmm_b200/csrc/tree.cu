@@ -88,21 +88,28 @@ __global__ void bbox_final(const double* __restrict__ part, int nb, double* __re
 // ------------------------------------------------------------------ keys
 // c = pos*scale + shift in the input precision, without fused multiply-add
 // (pvfmm-wrapper.cpp:582-586), wrapped into [0,1); Morton coordinate
-// floor(c*2^30) (mortonid.txx:39-53).
+// floor(c*2^30) (mortonid.txx:39-53).  The reference wraps by adding or
+// subtracting 1 until c lies in [0,1); every step but the last is exact, so
+// c - floor(c) (one rounding, then 1 -> 0) is the same value and takes no
+// loop for coordinates far outside a periodic box.
 template <class T>
 __device__ __forceinline__ T map_coord(T x, T s, T sh);
 template <>
 __device__ __forceinline__ double map_coord<double>(double x, double s, double sh) {
   double c = __dadd_rn(__dmul_rn(x, s), sh);
-  while (c < 0.0) c = __dadd_rn(c, 1.0);
-  while (c >= 1.0) c = __dadd_rn(c, -1.0);
+  if (!(c >= 0.0 && c < 1.0) && c == c) {
+    c = __dadd_rn(c, -floor(c));
+    if (c >= 1.0) c = __dadd_rn(c, -1.0);
+  }
   return c;
 }
 template <>
 __device__ __forceinline__ float map_coord<float>(float x, float s, float sh) {
   float c = __fadd_rn(__fmul_rn(x, s), sh);
-  while (c < 0.f) c = __fadd_rn(c, 1.f);
-  while (c >= 1.f) c = __fadd_rn(c, -1.f);
+  if (!(c >= 0.f && c < 1.f) && c == c) {
+    c = __fadd_rn(c, -floorf(c));
+    if (c >= 1.f) c = __fadd_rn(c, -1.f);
+  }
   return c;
 }
 
@@ -182,7 +189,7 @@ __global__ void make_children(const MKey* __restrict__ cur, const int* __restric
 // For internal node X at level d: parents (level d-1) of its 3^3 neighbours
 // clipped to the unit box; per axis these are parent(x) and the parent on the
 // side of x within its parent.  Invalid candidates get the sentinel key.
-__global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, MKey* __restrict__ out) {
+__global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, int periodic, MKey* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   unsigned int q[3], dd;
@@ -193,8 +200,11 @@ __global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, MKey* __r
   for (int a = 0; a < 3; ++a) {
     const long p0 = (long)(q[a] & pmask);
     cand[a][0] = p0;
-    if (q[a] & w) cand[a][1] = (q[a] + (long)w < (long)kTwo30) ? p0 + 2L * w : -1;
-    else cand[a][1] = ((long)q[a] - (long)w >= 0) ? p0 - 2L * w : -1;
+    // the neighbour parent across the near face; outside the unit cube it
+    // wraps around for periodic boundaries (NbrList, mortonid.cpp:15-55)
+    long c = (q[a] & w) ? p0 + 2L * w : p0 - 2L * w;
+    if (c < 0 || c >= (long)kTwo30) c = periodic ? (c + (long)kTwo30) % (long)kTwo30 : -1;
+    cand[a][1] = c;
   }
   for (int c = 0; c < 8; ++c) {
     const long x = cand[0][c & 1], y = cand[1][(c >> 1) & 1], z = cand[2][(c >> 2) & 1];
@@ -303,13 +313,16 @@ __global__ void node_ranges(const MKey* __restrict__ keys, long n, const MKey* _
 // at offset floor((c + d) / 2), which exists at this level iff that colleague
 // is internal (every internal node has all 8 children in the level arrays).
 // Same result as searching the level's sorted keys (interac_list.txx:98-130).
+// Periodic boundaries: every colleague of the root is the root itself (one
+// image per slot, mpi_tree.txx:1142-1168), and the rule above then wraps the
+// colleagues of every level around the unit cube.
 __global__ void colleagues_kernel(long base, long n_level, const int* __restrict__ parent,
-                                  const int* __restrict__ child0, int* __restrict__ coll) {
+                                  const int* __restrict__ child0, int periodic, int* __restrict__ coll) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n_level) return;
   const long v = base + i;
   if (v == 0) {
-    for (int ci = 0; ci < 27; ++ci) coll[ci] = ci == 13 ? 0 : -1;
+    for (int ci = 0; ci < 27; ++ci) coll[ci] = (ci == 13 || periodic) ? 0 : -1;
     return;
   }
   const int P = parent[v];
@@ -360,8 +373,32 @@ __global__ void gather_coords(const double* __restrict__ in, const int* __restri
 }
 
 // ------------------------------------------------------------------ lists
+// Image of colleague c at slot ci of node v (periodic boundaries): the
+// shift, in units of the unit cube, that moves c to the slot's position next
+// to v, coded (sx+1) + 3(sy+1) + 9(sz+1) with s in {-1, 0, 1}; 13 = none.
+// The reference stores the same shifts as coord_shift per interaction
+// (fmm_pts.txx:2490-2500, 4646-4656, 4932-4942).
+__device__ __forceinline__ unsigned char image_code(const MKey* keys, long v, int ci, long c) {
+  unsigned int X[3], Y[3], dv, dc;
+  decode_key(keys[v], X[0], X[1], X[2], dv);
+  decode_key(keys[c], Y[0], Y[1], Y[2], dc);
+  const long w = (long)(kTwo30 >> dv);
+  const int off[3] = {ci % 3 - 1, (ci / 3) % 3 - 1, ci / 9 - 1};
+  int code = 0, mul = 1;
+  for (int a = 0; a < 3; ++a) {
+    const long e = (long)X[a] + off[a] * w - (long)Y[a];  // a multiple of 2^30
+    const int sh = e < 0 ? -1 : (e > 0 ? 1 : 0);
+    code += (sh + 1) * mul;
+    mul *= 3;
+  }
+  return (unsigned char)code;
+}
+
 // One pass per target node (n_trg > 0); `mode` 0 counts, 1 fills.
 // Relative coordinates follow InteracList::BuildList (interac_list.txx:98-279).
+// With image arrays (periodic boundaries) every entry also gets the image
+// code of its source (U1 / U2 / W: of the node's colleague; U0 / X: of the
+// parent's colleague).
 __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf, const int* __restrict__ parent,
                             const int* __restrict__ child0, const int* __restrict__ coll, const int* __restrict__ slo,
                             const int* __restrict__ shi, const int* __restrict__ tlo, const int* __restrict__ thi,
@@ -369,25 +406,38 @@ __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf
                             int* __restrict__ w_cnt,
                             int* __restrict__ v_cnt, const int* __restrict__ p_off, const int* __restrict__ x_off,
                             const int* __restrict__ w_off, int* __restrict__ p_list, int* __restrict__ x_list,
-                            int* __restrict__ w_list) {
+                            int* __restrict__ w_list, const MKey* __restrict__ keys, unsigned char* __restrict__ p_img,
+                            unsigned char* __restrict__ x_img, unsigned char* __restrict__ w_img) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= n_nodes) return;
   const int nt = thi[t] - tlo[t];
   int np = 0, nx = 0, nw = 0, nv = 0;
   if (nt > 0) {
     const bool tleaf = leaf[t];
+    const bool img = mode && p_img;
     int* pl = mode ? p_list + p_off[t] : nullptr;
     int* xl = mode ? x_list + x_off[t] : nullptr;
     int* wl = mode ? w_list + w_off[t] : nullptr;
-#define ADD(list, cnt, v) \
-  do {                    \
-    if (mode) list[cnt] = (v); \
-    ++cnt;                \
+    unsigned char* pi = img ? p_img + p_off[t] : nullptr;
+    unsigned char* xi = img ? x_img + x_off[t] : nullptr;
+    unsigned char* wi = img ? w_img + w_off[t] : nullptr;
+    unsigned char code = 13;
+#define ADD(list, cnt, v)      \
+  do {                         \
+    if (mode) {                \
+      list[cnt] = (v);         \
+      if (img) list##_img_[cnt] = code; \
+    }                          \
+    ++cnt;                     \
   } while (0)
+    unsigned char* pl_img_ = pi;
+    unsigned char* xl_img_ = xi;
+    unsigned char* wl_img_ = wi;
     if (tleaf) {
       for (int ci = 0; ci < 27; ++ci) {
         const int c = coll[t * 27 + ci];
         if (c < 0) continue;
+        if (img) code = image_code(keys, t, ci, c);
         if (leaf[c]) {
           if (shi[c] > slo[c]) ADD(pl, np, c);  // U1
         } else {
@@ -420,6 +470,7 @@ __global__ void build_lists(long n_nodes, const unsigned char* __restrict__ leaf
         const int c = coll[(long)p * 27 + ci];
         if (c < 0 || !leaf[c]) continue;
         if (shi[c] <= slo[c]) continue;
+        if (img) code = image_code(keys, p, ci, c);
         const int rx = (ci % 3) * 4 - 4 - ((p2n & 1) ? 2 : 0) + 1;
         const int ry = ((ci / 3) % 3) * 4 - 4 - ((p2n & 2) ? 2 : 0) + 1;
         const int rz = (ci / 9) * 4 - 4 - ((p2n & 4) ? 2 : 0) + 1;
@@ -788,11 +839,16 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   }
   PVFMM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
   if (trg_alias) std::copy(bs, bs + 6, bt);
-  if (!ctx.unit_box) {
+  if (!ctx.unit_box && !ctx.periodic) {
     if (pos_float) bbox_scale_shift<float>(bs, bt, T.scale_x, T.shift_x);
     else bbox_scale_shift<double>(bs, bt, T.scale_x, T.shift_x);
   }
-  if (ctx.unit_box) {
+  if (ctx.periodic) {
+    // periodic boundaries (pvfmm-wrapper.cpp:512-517): scale 1 / box_size in
+    // the interface precision, no shift; the mapping wraps into [0,1)
+    T.scale_x = pos_float ? (double)(1.0f / (float)ctx.box_size) : 1.0 / ctx.box_size;
+    T.shift_x[0] = T.shift_x[1] = T.shift_x[2] = 0.0;
+  } else if (ctx.unit_box) {
     // C++ interface (include/pvfmm.txx:216-244): coordinates are used as
     // given, so they must lie in the unit cube.
     for (const double* b : {bs, bt})
@@ -885,7 +941,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
       PVFMM_CUDA_CHECK(cudaMemcpyAsync(cand, ctx.lvlR[d - 1].get<MKey>(), nR[d - 1] * sizeof(MKey),
                                        cudaMemcpyDeviceToDevice, s));
       ++ctx.n_launch;
-      nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d, cand + nR[d - 1]);
+      nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d,
+                                                                 ctx.periodic ? 1 : 0, cand + nR[d - 1]);
       nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1], d - 1);
     }
   }
@@ -947,7 +1004,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   for (int d = 0; d <= D; ++d) {
     const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
     ++ctx.n_launch;
-    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0, coll);
+    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0, ctx.periodic ? 1 : 0,
+                                                                   coll);
   }
   // 9. compact node lists.  The compacted lists are sized for all N nodes so
   //    that the eight counts are read back together at one synchronisation.
@@ -976,7 +1034,7 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     ++ctx.n_launch;
     build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf,
                                                  T.src_weight, 0, pc, xc, wc, vc, nullptr, nullptr, nullptr, nullptr,
-                                                 nullptr, nullptr);
+                                                 nullptr, nullptr, keys, nullptr, nullptr, nullptr);
     int* po = T.p_off.as<int>(N + 1);
     int* xo = T.x_off.as<int>(N + 1);
     int* wo = T.w_off.as<int>(N + 1);
@@ -997,10 +1055,13 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
     int* pl = T.p_list.as<int>(std::max(T.n_p2p, 1L));
     int* xl = T.x_list.as<int>(std::max(T.n_x, 1L));
     int* wl = T.w_list.as<int>(std::max(T.n_w, 1L));
+    unsigned char* pim = ctx.periodic ? T.p_img.as<unsigned char>(std::max(T.n_p2p, 1L)) : nullptr;
+    unsigned char* xim = ctx.periodic ? T.x_img.as<unsigned char>(std::max(T.n_x, 1L)) : nullptr;
+    unsigned char* wim = ctx.periodic ? T.w_img.as<unsigned char>(std::max(T.n_w, 1L)) : nullptr;
     ++ctx.n_launch;
     build_lists<<<ceil_div(N, 128), 128, 0, s>>>(N, leaf, parent, child0, coll, slo, shi, tlo, thi, nsrf,
                                                  T.src_weight, 1, nullptr, nullptr, nullptr, nullptr, po, xo, wo, pl,
-                                                 xl, wl);
+                                                 xl, wl, keys, pim, xim, wim);
     int* vt = T.vtab.as<int>(std::max(T.n_vtrg, 1L) * 26);
     unsigned* vm = T.vmask.as<unsigned>(std::max(T.n_vtrg, 1L));
     if (T.n_vtrg > 0) {

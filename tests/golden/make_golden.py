@@ -16,6 +16,13 @@ reference_*.npz    the reference's own particle FMM (src/pvfmm-wrapper.cpp and
 reference_config1.npz   the reference's output on the 100,000-point uniform
                    Laplace case (m=6, 300 points per leaf); the inputs are
                    regenerated from their seeds (checksums kept).
+reference_periodic_*.npz   the same, periodic (box_size > 0), from the
+                   reference's default build (PVFMM_EXTENDED_BC) and, for the
+                   lattice_* cases, from its build without that option
+                   (oracle/_ref/libpvfmm_ref_avx2_lattice.so).
+reference_bc_*.npz the periodic boundary operator (BC_Type entry 3 of the
+                   reference's precompute file) through M V and M^T V for
+                   seeded V.
 
 Run:  python tests/golden/make_golden.py [--force]   (existing oracle_*.npz and
 reference_*.npz are kept unless --force).  The reference tree is read from
@@ -180,6 +187,93 @@ def config1_inputs():
     return x, q
 
 
+# Periodic boundaries (box_size > 0): kernel, m, max_pts, distribution, n
+# sources, separate targets, seed, box size, lattice (False: the reference's
+# default build, the 5x5x5-image boundary operator; True: the build without
+# PVFMM_EXTENDED_BC, the lattice sum).  The points are scaled to the box and
+# a tenth of them moved by whole periods, so that the wrap is exercised.
+PERIODIC_CASES = {
+    "laplace_unif_m6": (0, 6, 50, "unif", 3000, False, 31, 2.0, False),
+    "laplace_grad_unif_m6": (1, 6, 50, "unif", 3000, False, 31, 2.0, False),
+    "laplace_gauss_m6": (0, 6, 50, "gauss", 4000, False, 32, 1.0, False),
+    "laplace_sep_m6": (0, 6, 50, "unif", 3000, True, 33, 1.0, False),
+    "laplace_small_m6": (0, 6, 50, "unif", 300, False, 34, 1.0, False),
+    "stokes_vel_m4": (3, 4, 60, "unif", 2000, False, 35, 1.0, False),
+    "lattice_laplace_unif_m6": (0, 6, 50, "unif", 3000, False, 36, 1.0, True),
+    "lattice_laplace_grad_gauss_m6": (1, 6, 50, "gauss", 3000, False, 37, 1.0, True),
+    "lattice_stokes_vel_m4": (3, 4, 60, "unif", 2000, False, 38, 1.5, True),
+}
+# periodic boundary operators pinned through their action on seeded vectors:
+# kernel, m, lattice
+PERIODIC_OPERATORS = {"laplace_m6": (0, 6, False), "stokes_vel_m4": (3, 4, False),
+                      "lattice_laplace_m6": (0, 6, True), "lattice_laplace_grad_m6": (1, 6, True),
+                      "lattice_stokes_vel_m4": (3, 4, True)}
+
+
+def periodic_case_inputs(name):
+    """src, sl_den, trg (None: the sources) of a periodic case, in box units."""
+    kid, m, mp, dist, n, sep, seed, box, lattice = PERIODIC_CASES[name]
+    rng = np.random.default_rng(seed + 500)
+    src = points(dist, n, seed) * box
+    shift = rng.integers(-2, 3, (n, 3)) * box
+    src = src + np.where(rng.random((n, 1)) < 0.1, shift, 0.0)
+    trg = points("unif", n // 2, seed + 100) * box if sep else None
+    den = np.random.default_rng(seed + 200).uniform(-1, 1, (n, KDIM[kid][0]))
+    return src, den, trg
+
+
+def periodic_operator_probe(kid, m):
+    """The seeded vectors (n x 4) the operator fixtures multiply."""
+    n = (6 * (m - 1) ** 2 + 2) * KDIM[kid][0]
+    return np.random.default_rng(1000 + kid * 16 + m).standard_normal((n, 4))
+
+
+def _periodic_case(name):
+    from oracle.ref_fmm import refpvfmm as R
+    kid, m, mp, dist, n, sep, seed, box, lattice = PERIODIC_CASES[name]
+    src, den, trg = periodic_case_inputs(name)
+    out, tree, lists = R.ref_eval(kid, m, mp, src, den, trg, box_size=box, lattice=lattice)
+    np.savez_compressed(os.path.join(HERE, f"reference_periodic_{name}.npz"), kernel=kid, m=m, max_pts=mp, src=src,
+                        den=den, trg=np.zeros((0, 3)) if trg is None else trg, out=out, box=box, lattice=lattice,
+                        nodes=tree[:, :7].astype(np.int32))
+
+
+def _periodic_operator(name):
+    import struct
+    from oracle.ref_fmm import refpvfmm as R
+    kid, m, lattice = PERIODIC_OPERATORS[name]
+    ctx = R.RefContext(kid, m, 50, box_size=1.0, lattice=lattice)
+    ctx.close()
+    # the reference's precompute file holds BC_Type entry 3 (BoundaryType PXYZ == Periodic)
+    d = R._lattice_dir[0] if lattice else os.environ["PVFMM_DIR"]
+    kname = {0: "laplace", 1: "laplace_grad", 3: "stokes_vel"}[kid]
+    b = open(os.path.join(d, f"Precomp_{kname}_m{m}.data"), "rb").read()
+    pos, M = 8, None
+    for t in range(16):
+        cnt = struct.unpack_from("i", b, pos)[0]
+        pos += 4
+        for j in range(cnt):
+            n1, n2 = struct.unpack_from("ii", b, pos)
+            pos += 8
+            if t == 15 and j == 3:
+                M = np.frombuffer(b, dtype=np.float64, count=n1 * n2, offset=pos).reshape(n1, n2)
+            pos += 8 * n1 * n2
+    V = periodic_operator_probe(kid, m)
+    np.savez_compressed(os.path.join(HERE, f"reference_bc_{name}.npz"), kernel=kid, m=m, lattice=lattice,
+                        MtV=M.T @ V, MV=M @ V, norm=np.linalg.norm(M))
+
+
+def periodic_golden(force=False):
+    """One process per fixture: the two reference builds are not loaded into
+    one process."""
+    for name in PERIODIC_CASES:
+        if force or not os.path.exists(os.path.join(HERE, f"reference_periodic_{name}.npz")):
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--periodic-case", name], check=True)
+    for name in PERIODIC_OPERATORS:
+        if force or not os.path.exists(os.path.join(HERE, f"reference_bc_{name}.npz")):
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--periodic-operator", name], check=True)
+
+
 def reference_golden(force=False):
     from oracle.ref_fmm import refpvfmm as R
     if not R.available():
@@ -212,8 +306,15 @@ def reference_golden(force=False):
 
 
 if __name__ == "__main__":
+    if "--periodic-case" in sys.argv:
+        _periodic_case(sys.argv[sys.argv.index("--periodic-case") + 1])
+        sys.exit(0)
+    if "--periodic-operator" in sys.argv:
+        _periodic_operator(sys.argv[sys.argv.index("--periodic-operator") + 1])
+        sys.exit(0)
     if os.path.isdir(os.environ.get("PVFMM_REFERENCE", "/root/reference")):
         morton_golden()
         reference_golden(force="--force" in sys.argv)
+        periodic_golden(force="--force" in sys.argv)
     oracle_golden(force="--force" in sys.argv)
     print("golden fixtures written to", HERE)

@@ -117,8 +117,6 @@ def test_invalid_arguments_fail_loudly():
     lib = P.load_library()
     assert not lib.PVFMMCreateContextExD(-1.0, 100, 6, 9, 0)         # not a PVFMMKernel value
     assert "unsupported" in P.last_error()
-    assert not lib.PVFMMCreateContextExD(1.0, 100, 6, 0, 0)          # periodic box
-    assert "periodic" in P.last_error()
     assert not lib.PVFMMCreateContextExD(-1.0, 100, 7, 0, 0)         # odd order
     assert P.last_error()
     assert P.precomp_operator.__doc__

@@ -1,0 +1,141 @@
+"""Periodic boundaries (box_size > 0) on the GPU against the reference's own
+particle FMM (tests/golden/reference_periodic_*.npz, written by the reference
+built from its sources: the default build with PVFMM_EXTENDED_BC and, for the
+lattice_* cases, the build without it; tests/golden/make_golden.py).
+
+The plain FP64 path must build the reference's periodic octree (2:1 balance
+across the periodic faces) and reproduce its outputs; the mixed form must
+stay within its accuracy bar.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import pvfmm_b200 as P
+from oracle import pvfmm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+from make_golden import PERIODIC_CASES  # noqa: E402
+
+CASES = sorted(PERIODIC_CASES)
+# the lattice operator carries the ~1e-11 SVD differences of its order m+2
+# pseudo-inverses (tests/test_periodic_operator.py) into the outputs
+TOL = {False: 1e-12, True: 1e-10}
+
+
+def load(name):
+    z = np.load(os.path.join(HERE, "golden", f"reference_periodic_{name}.npz"))
+    trg = z["trg"] if len(z["trg"]) else None
+    return z, trg
+
+
+def run(z, trg, prec=P.PRECISION_PLAIN, lattice=None, m2c=None, dtype=np.float64):
+    kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
+    ctx = P.FMMParticleContext(float(z["box"]), mp, m, P.FMMKernel(kid), dtype=dtype,
+                               precision=None if dtype == np.float32 else prec)
+    if lattice is None:
+        lattice = bool(z["lattice"])
+    if lattice or m2c is not None:
+        ctx.set_periodic_bc(lattice, m2c)
+    s = np.ascontiguousarray(z["src"], dtype=dtype).reshape(-1)
+    t = s if trg is None else np.ascontiguousarray(trg, dtype=dtype).reshape(-1)
+    out = ctx.evaluate(s, np.ascontiguousarray(z["den"], dtype=dtype).reshape(-1), None, t, True)
+    return out, ctx
+
+
+def check_tree(ctx, nodes):
+    keys = ctx.tree_data(2).reshape(-1, 4)
+    leaf = ctx.tree_data(3)
+    src = ctx.tree_data(4).reshape(-1, 2)
+    trg = ctx.tree_data(5).reshape(-1, 2)
+    ours = {tuple(int(v) for v in k): i for i, k in enumerate(keys)}
+    ref = {tuple(int(v) for v in r[:4]): r for r in nodes}
+    assert set(ours) == set(ref), (len(ours), len(ref))
+    for k, i in ours.items():
+        r = ref[k]
+        assert bool(leaf[i]) == bool(r[4]), k
+        if leaf[i]:
+            assert int(trg[i][1] - trg[i][0]) == int(r[6]), k
+            assert int(src[i][1] - src[i][0]) == int(r[5]), k
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_periodic_plain_matches_reference(name):
+    z, trg = load(name)
+    out, ctx = run(z, trg)
+    check_tree(ctx, z["nodes"])
+    err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
+    assert err < TOL[bool(z["lattice"])], err
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["laplace_unif_m6", "laplace_gauss_m6", "lattice_laplace_unif_m6",
+                                  "lattice_stokes_vel_m4", "stokes_vel_m4"])
+def test_periodic_mixed_within_bar(name):
+    z, trg = load(name)
+    plain, c0 = run(z, trg)
+    mixed, c1 = run(z, trg, prec=P.PRECISION_MIXED)
+    ref = z["out"].reshape(-1)
+    # the mixed form against the reference: its own bar over the plain form's
+    # truncation error at these orders
+    e_plain = O.rel_l2(plain.reshape(-1), ref)
+    e_mixed = O.rel_l2(mixed.reshape(-1), ref)
+    assert e_mixed < max(1e-6, 1.5 * e_plain), (e_mixed, e_plain)
+    c0.close()
+    c1.close()
+
+
+def test_periodic_float_interface():
+    z, trg = load("laplace_unif_m6")
+    out, ctx = run(z, trg, dtype=np.float32)
+    assert O.rel_l2(out.reshape(-1).astype(np.float64), z["out"].reshape(-1)) < 1e-5
+    ctx.close()
+
+
+def test_periodic_setup0_reuses_the_tree():
+    z, trg = load("laplace_gauss_m6")
+    kid, m, mp = int(z["kernel"]), int(z["m"]), int(z["max_pts"])
+    ctx = P.FMMParticleContext(float(z["box"]), mp, m, P.FMMKernel(kid))
+    s = np.ascontiguousarray(z["src"]).reshape(-1)
+    d0 = np.ascontiguousarray(z["den"]).reshape(-1)
+    d1 = np.random.default_rng(5).uniform(-1, 1, d0.size)
+    ctx.evaluate(s, d0, None, s, True)
+    a = ctx.evaluate(s, d1, None, s, False)
+    b = ctx.evaluate(s, d1, None, s, True)
+    assert O.rel_l2(a, b) < 1e-14
+    ctx.close()
+
+
+def test_periodic_user_operator_enters_linearly():
+    """The user operator of the 5x5x5-image form adds to the boundary
+    operator (FMM_Pts::SetM2C): outputs are affine in it."""
+    z, trg = load("laplace_small_m6")
+    m = int(z["m"])
+    M = P.precomp_operator(P.FMMKernel.LaplacePotential, m, 0, 9)
+    base, c0 = run(z, trg)
+    plus, c1 = run(z, trg, m2c=M)
+    minus, c2 = run(z, trg, m2c=-M)
+    assert O.rel_l2(plus - base, base - minus) < 1e-12
+    assert O.rel_l2(plus, base) > 1e-6   # the operator matters
+    for c in (c0, c1, c2):
+        c.close()
+
+
+def test_periodic_bc_option_rejections():
+    free = P.FMMParticleContext(-1.0, 50, 6, P.FMMKernel.LaplacePotential)
+    with pytest.raises(RuntimeError, match="free-space"):
+        free.set_periodic_bc(True)
+    free.close()
+    per = P.FMMParticleContext(1.0, 50, 4, P.FMMKernel.StokesPressure)
+    with pytest.raises(RuntimeError, match="lattice"):
+        per.set_periodic_bc(True)
+    per.close()
+    per = P.FMMParticleContext(1.0, 50, 6, P.FMMKernel.LaplacePotential)
+    with pytest.raises(RuntimeError):
+        per.set_periodic_bc(True, np.zeros((152, 152)))
+    per.close()
