@@ -62,6 +62,13 @@ WORKLOADS = {
     "ellipsoid30m": dict(kernel=0, m=8, max_pts=128, n=30_000_000, gen="ellipsoid", seeds=(41, 42), check_seed=44,
                          n_check=1000, desc="laplace potential FMM (setup=1 per step), {n} points uniform by area on "
                                             "the (0.45, 0.3, 0.15) ellipsoid, m=8, 128/leaf"),
+    # periodic boundaries (box_size 1, the lattice sum over all images),
+    # checked against an Ewald sum up to the additive constant of a periodic
+    # potential
+    "periodic4m": dict(kernel=0, m=8, max_pts=256, n=4_000_000, gen="neutral", seeds=(51, 52), check_seed=53,
+                       n_check=200, box=1.0, lattice=True,
+                       desc="periodic laplace potential FMM (period 1, lattice sum over all images, setup=1 per "
+                            "step), {n} uniform points, charge-neutral densities, m=8, 256/leaf"),
     # the differentiable Laplace potential: one step = forward (pot+grad FMM)
     # + backward (swapped-role FMM on the forward's tree) through
     # pvfmm_b200.autograd.LaplaceFMM, sources = targets
@@ -81,6 +88,9 @@ def make_points(w, n):
     s0, s1 = w["seeds"]
     if w["gen"] == "uniform":
         return np.random.default_rng(s0).random((n, 3)), np.random.default_rng(s1).uniform(-1, 1, n)
+    if w["gen"] == "neutral":  # uniform densities with their mean taken out (a periodic cell without net charge)
+        q = np.random.default_rng(s1).uniform(-1, 1, n)
+        return np.random.default_rng(s0).random((n, 3)), q - q.mean()
     if w["gen"] == "stokes":
         return np.random.default_rng(s0).random((n, 3)), np.random.default_rng(s1).standard_normal((n, 3))
     if w["gen"] == "ellipsoid":
@@ -131,6 +141,58 @@ def direct_gpu(torch, kid, x, q, idx):
             if kid == 6:
                 out[:, 1:] += (d * (qr * rinv * rinv)[:, :, None]).sum(1)
     return (out / (8 * math.pi if kid == 3 else 4 * math.pi)).cpu().numpy()
+
+
+def ewald_gpu(torch, x, q, idx, alpha=5.5, kmax=10):
+    """Periodic potential of the 1/(4 pi r) kernel in the unit cell (Ewald
+    sum with a neutralising background) at targets x[idx], which are sources
+    (their self term removed); FP64 on the GPU.  alpha = 5.5: the real-space
+    sum over the 27 nearest images is complete to erfc(5.5) ~ 7e-15; kmax =
+    10: the reciprocal sum to exp(-(2 pi 10)^2 / (4 alpha^2)) ~ 1e-14.  The
+    structure factor is separable, S(k) = sum_j q_j ex_j(kx) ey_j(ky) ez_j(kz),
+    so it is formed as small matrix products."""
+    dev, f64, c128 = "cuda", torch.float64, torch.complex128
+    X = torch.as_tensor(x, device=dev, dtype=f64)
+    Q = torch.as_tensor(q, device=dev, dtype=f64).reshape(-1)
+    T = X[torch.as_tensor(idx, device=dev)]
+    phi = torch.zeros(T.shape[0], device=dev, dtype=f64)
+    chunk = 1 << 16
+    shifts = torch.tensor([[a, b, c] for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)], device=dev,
+                          dtype=f64)
+    for a in range(0, X.shape[0], chunk):
+        d0 = T[:, None, :] - X[None, a:a + chunk, :]
+        qa = Q[a:a + chunk]
+        for sh in shifts:
+            d = d0 + sh
+            r = torch.sqrt((d * d).sum(-1))
+            v = torch.where(r > 0, torch.special.erfc(alpha * r) / r.clamp_min(1e-300), torch.zeros_like(r))
+            phi += (v * qa[None, :]).sum(1) / (4 * math.pi)
+    ks = torch.arange(-kmax, kmax + 1, device=dev, dtype=f64) * (2 * math.pi)
+    nk = ks.numel()
+    S = torch.zeros((nk, nk, nk), device=dev, dtype=c128)
+    for a in range(0, X.shape[0], chunk):
+        xa = X[a:a + chunk]
+        e = [torch.exp(-1j * xa[:, i:i + 1].to(c128) * ks[None, :].to(c128)) for i in range(3)]  # (n, nk)
+        w = Q[a:a + chunk].to(c128)[:, None] * e[0]                                                   # (n, kx)
+        # S[kx, ky, kz] += sum_j w[j, kx] ey[j, ky] ez[j, kz]
+        S += torch.einsum("jx,jy,jz->xyz", w, e[1], e[2])
+    kx, ky, kz = torch.meshgrid(ks, ks, ks, indexing="ij")
+    k2 = kx * kx + ky * ky + kz * kz
+    wk = torch.where(k2 > 0, torch.exp(-k2 / (4 * alpha * alpha)) / k2.clamp_min(1e-300), torch.zeros_like(k2))
+    et = [torch.exp(1j * T[:, i:i + 1].to(c128) * ks[None, :].to(c128)) for i in range(3)]        # (t, nk)
+    phi += torch.einsum("xyz,tx,ty,tz->t", (wk.to(c128) * S), et[0], et[1], et[2]).real
+    phi -= Q[torch.as_tensor(idx, device=dev)] * alpha / (2 * math.pi ** 1.5)
+    return phi.cpu().numpy()[:, None]
+
+
+def rel_err(out, ref, periodic):
+    """Relative L2 error; for a periodic potential, defined up to an additive
+    constant, after the mean difference is removed."""
+    d = out - ref
+    if periodic:
+        d = d - d.mean(axis=0)
+        ref = ref - ref.mean(axis=0)
+    return float(np.linalg.norm(d) / np.linalg.norm(ref))
 
 
 class ClockSampler:
@@ -258,7 +320,8 @@ def reference_contexts(threads):
     its C interface, one context per C-interface kernel of the workload."""
     from oracle.ref_fmm import refpvfmm as R
     t0 = time.perf_counter()
-    ctxs = [R.RefContext(k, W["m"], W["max_pts"], threads=threads) for k in REFERENCE_KERNELS[W["kernel"]]]
+    ctxs = [R.RefContext(k, W["m"], W["max_pts"], threads=threads, box_size=W.get("box", -1.0),
+                         lattice=W.get("lattice", False)) for k in REFERENCE_KERNELS[W["kernel"]]]
     return R, ctxs, 1000 * (time.perf_counter() - t0)
 
 
@@ -586,7 +649,8 @@ def main():
     x, q = make_points(W, N)
     q = np.ascontiguousarray(q.reshape(-1))
     idx = np.random.default_rng(W["check_seed"]).choice(N, W["n_check"], replace=False)
-    ref = direct_gpu(torch, kid, x, q, idx)
+    periodic = W.get("box", -1.0) > 0
+    ref = ewald_gpu(torch, x, q, idx) if periodic else direct_gpu(torch, kid, x, q, idx)
     torch.cuda.empty_cache()  # the direct sum's temporaries go back to the device
     d_x = torch.as_tensor(x, device="cuda")
     d_q = torch.as_tensor(q, device="cuda")
@@ -596,7 +660,9 @@ def main():
     def run_form(form):
         prec = P.PRECISION_PLAIN if form == "plain" else P.PRECISION_MIXED
         t_ctx = time.perf_counter()
-        ctx = P.FMMParticleContext(-1, W["max_pts"], W["m"], P.FMMKernel(kid), precision=prec)
+        ctx = P.FMMParticleContext(W.get("box", -1.0), W["max_pts"], W["m"], P.FMMKernel(kid), precision=prec)
+        if W.get("lattice"):
+            ctx.set_periodic_bc(True)
         context_ms = 1000 * (time.perf_counter() - t_ctx)  # operator precompute + upload, outside the timed steps
         try:
             def step():
@@ -607,8 +673,8 @@ def main():
                 step()
             torch.cuda.synchronize()
             out = d_out.cpu().numpy()[idx]
-            err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
-            err_comp = [float(np.linalg.norm(out[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])) for k in range(k1)]
+            err = rel_err(out, ref, periodic)
+            err_comp = [rel_err(out[:, k], ref[:, k], periodic) for k in range(k1)]
             stats = ctx.tree_stats()
             l0 = ctx.launch_count()
             clocks = ClockSampler(local)

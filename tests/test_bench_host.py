@@ -178,3 +178,12 @@ def test_a_line_where_no_form_meets_the_bar_says_so():
     forms["plain"] = _form(58e6, 2.1e-7, [6e-8, 2.5e-7, 1.8e-7, 2.0e-7], 8)
     line = bench.build_line(_Args, 1, 4_000_000, forms, {})
     assert line["meets_bar"] is True and line["form"] == "plain"
+
+
+def test_periodic_error_ignores_the_additive_constant():
+    """A periodic potential is defined up to a constant: the periodic
+    workload's error against its Ewald sum removes the mean difference."""
+    ref = np.random.default_rng(0).standard_normal((50, 1))
+    assert bench.rel_err(ref + 3.0, ref, True) < 1e-15
+    assert bench.rel_err(ref + 3.0, ref, False) > 1.0
+    assert bench.WORKLOADS["periodic4m"]["box"] > 0
