@@ -109,6 +109,12 @@ def points(dist, n, seed):
         u = rng.standard_normal((n, 3))
         u /= np.linalg.norm(u, axis=1, keepdims=True)
         return 0.5 + np.array([0.45, 0.3, 0.15]) * u
+    if dist == "corner":       # two clusters across the periodic faces (corner and an edge), the rest uniform
+        x = rng.random((n, 3))
+        k = n // 3
+        x[:k] = 0.03 * rng.standard_normal((k, 3))                      # around (0, 0, 0)
+        x[k:2 * k] = np.array([0.5, 1.0, 0.0]) + 0.03 * rng.standard_normal((k, 3))
+        return x                                                          # wrapped by the periodic map
     if dist == "coincident":   # half the points on one spot: a tree to the maximum depth
         x = rng.random((n, 3))
         x[: n // 2] = x[0]
@@ -199,6 +205,10 @@ PERIODIC_CASES = {
     "laplace_sep_m6": (0, 6, 50, "unif", 3000, True, 33, 1.0, False),
     "laplace_small_m6": (0, 6, 50, "unif", 300, False, 34, 1.0, False),
     "stokes_vel_m4": (3, 4, 60, "unif", 2000, False, 35, 1.0, False),
+    # clusters across the faces: adaptive leaves whose U, W and X lists wrap
+    "laplace_corner_m6": (0, 6, 40, "corner", 4000, False, 39, 1.0, False),
+    "stokes_vel_corner_m4": (3, 4, 40, "corner", 3000, True, 40, 1.0, False),
+    "lattice_laplace_corner_m6": (0, 6, 40, "corner", 4000, False, 41, 1.0, True),
     "lattice_laplace_unif_m6": (0, 6, 50, "unif", 3000, False, 36, 1.0, True),
     "lattice_laplace_grad_gauss_m6": (1, 6, 50, "gauss", 3000, False, 37, 1.0, True),
     "lattice_stokes_vel_m4": (3, 4, 60, "unif", 2000, False, 38, 1.5, True),
