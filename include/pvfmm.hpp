@@ -37,7 +37,9 @@
 
 namespace pvfmm {
 
-enum BoundaryType { FreeSpace = 0, Periodic = 1 };
+// Boundary types with the reference's values (include/mpi_tree.hpp:23-30);
+// the C interface builds FreeSpace and Periodic (== PXYZ).
+enum BoundaryType { FreeSpace = 0, PX, PXY, PXYZ, Periodic = PXYZ };
 
 // Kernel object (reference include/kernel.hpp:27-106).  ker_poten is the
 // direct evaluation k_out += sum_s K(trg - src) v_src (include/kernel.hpp:40-41),
@@ -133,13 +135,14 @@ template <class Real>
 class PtFMM_Tree {
  public:
   PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
-             const std::vector<Real>& trg_coord, int max_pts)
-      : src_(src_coord), den_(src_value), trg_(trg_coord), max_pts_(max_pts) {}
+             const std::vector<Real>& trg_coord, int max_pts, BoundaryType bndry = FreeSpace)
+      : src_(src_coord), den_(src_value), trg_(trg_coord), max_pts_(max_pts), periodic_(bndry == Periodic) {}
   // with a separate double-layer point set (surf_coord, k0 + 3 values per point)
   PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
              const std::vector<Real>& surf_coord, const std::vector<Real>& surf_value,
-             const std::vector<Real>& trg_coord, int max_pts)
-      : src_(src_coord), den_(src_value), surf_(surf_coord), dl_(surf_value), trg_(trg_coord), max_pts_(max_pts) {}
+             const std::vector<Real>& trg_coord, int max_pts, BoundaryType bndry = FreeSpace)
+      : src_(src_coord), den_(src_value), surf_(surf_coord), dl_(surf_value), trg_(trg_coord), max_pts_(max_pts),
+        periodic_(bndry == Periodic) {}
   ~PtFMM_Tree() { release(); }
   PtFMM_Tree(const PtFMM_Tree&) = delete;
   PtFMM_Tree& operator=(const PtFMM_Tree&) = delete;
@@ -154,7 +157,8 @@ class PtFMM_Tree {
     k0_ = k->ker_dim[0];
     k1_ = k->ker_dim[1];
     const int precision = std::is_same<Real, float>::value ? PVFMMPrecisionMixed : PVFMMPrecisionPlain;
-    ctx_ = PVFMMCreateContextExD(-1.0, max_pts_, mat->MultipoleOrder(), k->id, precision);
+    // periodic: period 1, the unit cube itself (the coordinates are used as given)
+    ctx_ = PVFMMCreateContextExD(periodic_ ? 1.0 : -1.0, max_pts_, mat->MultipoleOrder(), k->id, precision);
     if (!ctx_) throw std::runtime_error(PVFMMGetLastError());
     if (PVFMMSetUnitBox(ctx_, 1) != 0) throw std::runtime_error(PVFMMGetLastError());
     // both point sets count in the tree (include/fmm_node.txx:81-92): they are
@@ -201,6 +205,7 @@ class PtFMM_Tree {
   }
   std::vector<Real> src_, den_, surf_, dl_, trg_;
   int max_pts_;
+  bool periodic_ = false;
   int k0_ = 1, k1_ = 1;
   void* ctx_ = nullptr;
   bool needs_setup_ = true;
@@ -213,8 +218,9 @@ PtFMM_Tree<Real>* PtFMM_CreateTree(const std::vector<Real>& sl_coord, const std:
                                    BoundaryType bndry = FreeSpace, int init_depth = 0) {
   (void)comm;
   (void)init_depth;
-  if (bndry != FreeSpace) throw std::runtime_error("PtFMM_CreateTree: only FreeSpace is supported");
-  return new PtFMM_Tree<Real>(sl_coord, sl_density, dl_coord, dl_density, trg_coord, max_pts);
+  if (bndry != FreeSpace && bndry != Periodic)
+    throw std::runtime_error("PtFMM_CreateTree: FreeSpace or Periodic boundaries only");
+  return new PtFMM_Tree<Real>(sl_coord, sl_density, dl_coord, dl_density, trg_coord, max_pts, bndry);
 }
 
 template <class Real>

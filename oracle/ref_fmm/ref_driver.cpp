@@ -156,9 +156,20 @@ long ref_profile_report(char* buf, long cap) {
 // tree's point set, coordinates in [0,1)^3 used as given, FreeSpace;
 // PtFMM_Evaluate writes n_trg * k1 values to out.  Returns 0, or 1 for an
 // unknown kernel.
+int ref_ptfmm_eval_bc(int kernel, int m, int max_pts, int periodic, long n_sl, const double* sl_coord,
+                      const double* sl_den, long n_dl, const double* dl_coord, const double* dl_den, long n_trg,
+                      const double* trg_coord, double* out);
 int ref_ptfmm_eval(int kernel, int m, int max_pts, long n_sl, const double* sl_coord, const double* sl_den,
                    long n_dl, const double* dl_coord, const double* dl_den, long n_trg, const double* trg_coord,
                    double* out) {
+  return ref_ptfmm_eval_bc(kernel, m, max_pts, 0, n_sl, sl_coord, sl_den, n_dl, dl_coord, dl_den, n_trg, trg_coord,
+                           out);
+}
+
+// The same with the boundary type: periodic != 0 gives BoundaryType Periodic.
+int ref_ptfmm_eval_bc(int kernel, int m, int max_pts, int periodic, long n_sl, const double* sl_coord,
+                      const double* sl_den, long n_dl, const double* dl_coord, const double* dl_den, long n_trg,
+                      const double* trg_coord, double* out) {
   const pvfmm::Kernel<double>* ker = nullptr;
   if (kernel == PVFMMLaplacePotential) ker = &pvfmm::LaplaceKernel<double>::potential();
   if (kernel == PVFMMLaplaceGradient) ker = &pvfmm::LaplaceKernel<double>::gradient();
@@ -170,7 +181,8 @@ int ref_ptfmm_eval(int kernel, int m, int max_pts, long n_sl, const double* sl_c
   std::vector<double> tc(trg_coord, trg_coord + 3 * n_trg);
   pvfmm::PtFMM<double> matrices;
   matrices.Initialize(m, MPI_COMM_WORLD, ker);
-  auto* tree = pvfmm::PtFMM_CreateTree(sc, sv, dc, dv, tc, MPI_COMM_WORLD, max_pts, pvfmm::FreeSpace);
+  auto* tree = pvfmm::PtFMM_CreateTree(sc, sv, dc, dv, tc, MPI_COMM_WORLD, max_pts,
+                                       periodic ? pvfmm::Periodic : pvfmm::FreeSpace);
   tree->SetupFMM(&matrices);
   std::vector<double> val;
   pvfmm::PtFMM_Evaluate(tree, val, n_trg);

@@ -87,6 +87,9 @@ def load(lattice: bool = False):
     lib.ref_profile_report.argtypes = [vp, lg]
     lib.ref_ptfmm_eval.restype = ctypes.c_int
     lib.ref_ptfmm_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, lg, vp, vp, lg, vp, vp, lg, vp, vp]
+    lib.ref_ptfmm_eval_bc.restype = ctypes.c_int
+    lib.ref_ptfmm_eval_bc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, lg, vp, vp, lg, vp,
+                                      vp, lg, vp, vp]
     lib.ref_cheb_integ0.restype = ctypes.c_int
     lib.ref_cheb_integ0.argtypes = [ctypes.c_int, vp, ctypes.c_double, vp]
     _libs[lattice] = lib
@@ -213,11 +216,13 @@ def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None, box_siz
         ctx.close()
 
 
-def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, threads=0):
+def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, threads=0, periodic=False,
+                   lattice=False):
     """The reference's C++ interface (PtFMM_CreateTree with separate single-
     and double-layer point sets, SetupFMM, PtFMM_Evaluate; coordinates in
-    [0,1)^3 as given).  Either point set may be empty (shape (0, 3))."""
-    lib = load()
+    [0,1)^3 as given; BoundaryType Periodic when periodic, from the lattice
+    build when lattice).  Either point set may be empty (shape (0, 3))."""
+    lib = load(lattice)
     if threads:
         lib.ref_set_threads(threads)
     k0, k1 = KDIM[kernel]
@@ -228,7 +233,15 @@ def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, 
     tc = np.ascontiguousarray(trg, dtype=np.float64).reshape(-1)
     n_trg = len(tc) // 3
     out = np.zeros(n_trg * k1)
-    if lib.ref_ptfmm_eval(kernel, m, max_pts, len(sc) // 3, _p(sc), _p(sv), len(dc) // 3, _p(dc), _p(dv), n_trg,
-                          _p(tc), _p(out)) != 0:
+    saved = os.environ.get("PVFMM_DIR")
+    if lattice:
+        os.environ["PVFMM_DIR"] = _lattice_dir[0]
+    try:
+        rc = lib.ref_ptfmm_eval_bc(kernel, m, max_pts, 1 if periodic else 0, len(sc) // 3, _p(sc), _p(sv),
+                                   len(dc) // 3, _p(dc), _p(dv), n_trg, _p(tc), _p(out))
+    finally:
+        if lattice and saved is not None:
+            os.environ["PVFMM_DIR"] = saved
+    if rc != 0:
         raise ValueError(f"kernel {kernel} is not driven through the C++ interface here")
     return out.reshape(n_trg, k1)

@@ -4,11 +4,11 @@
 // evaluation with new densities after ClearFMMData, ker_poten and BuildMatrix.
 // With n_dl > 0 the tree also holds a separate double-layer point set
 // (PtFMM_CreateTree with surf_coord / surf_value, k0 + 3 values per point),
-// and the second evaluation passes new values for both layers.  Writes inputs
-// and outputs as raw doubles for the Python test to compare against the
-// oracle.
+// and the second evaluation passes new values for both layers.  With a
+// trailing "periodic" the tree has BoundaryType Periodic.  Writes inputs and
+// outputs as raw doubles for the Python test to compare against the oracle.
 //
-// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f> [n_dl]
+// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f> [n_dl [periodic]]
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -48,7 +48,8 @@ void put(std::vector<double>& out, const std::vector<Real>& v) {
 }
 
 template <class Real>
-int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_t seed, long n_dl) {
+int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_t seed, long n_dl,
+        pvfmm::BoundaryType bndry) {
   Rng rng{seed};
   const pvfmm::Kernel<Real>& ker = kernel_of<Real>(kid);
   const int k0 = ker.ker_dim[0], k1 = ker.ker_dim[1];
@@ -66,8 +67,8 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
   pvfmm::PtFMM<Real> matrices;
   matrices.Initialize(m, comm, &ker);
   pvfmm::PtFMM_Tree<Real>* tree =
-      n_dl > 0 ? pvfmm::PtFMM_CreateTree(src, den, dl, dd, trg, comm, max_pts, pvfmm::FreeSpace)
-               : pvfmm::PtFMM_CreateTree(src, den, trg, comm, max_pts, pvfmm::FreeSpace);
+      n_dl > 0 ? pvfmm::PtFMM_CreateTree(src, den, dl, dd, trg, comm, max_pts, bndry)
+               : pvfmm::PtFMM_CreateTree(src, den, trg, comm, max_pts, bndry);
   tree->SetupFMM(&matrices);
   std::vector<Real> val1, val2;
   pvfmm::PtFMM_Evaluate(tree, val1, nt);
@@ -107,17 +108,19 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 9 && argc != 10) {
-    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f [n_dl]\n", argv[0]);
+  if (argc < 9 || argc > 11) {
+    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f [n_dl [periodic]]\n", argv[0]);
     return 1;
   }
   try {
     const int kid = std::atoi(argv[2]), m = std::atoi(argv[3]), mp = std::atoi(argv[4]);
     const long ns = std::atol(argv[5]), nt = std::atol(argv[6]);
     const uint64_t seed = std::strtoull(argv[7], nullptr, 10);
-    const long n_dl = argc == 10 ? std::atol(argv[9]) : 0;
-    if (std::string(argv[8]) == "f") return run<float>(argv[1], kid, m, mp, ns, nt, seed, n_dl);
-    return run<double>(argv[1], kid, m, mp, ns, nt, seed, n_dl);
+    const long n_dl = argc >= 10 ? std::atol(argv[9]) : 0;
+    const pvfmm::BoundaryType bndry =
+        argc == 11 && std::string(argv[10]) == "periodic" ? pvfmm::Periodic : pvfmm::FreeSpace;
+    if (std::string(argv[8]) == "f") return run<float>(argv[1], kid, m, mp, ns, nt, seed, n_dl, bndry);
+    return run<double>(argv[1], kid, m, mp, ns, nt, seed, n_dl, bndry);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 3;

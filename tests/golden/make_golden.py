@@ -23,6 +23,8 @@ reference_periodic_*.npz   the same, periodic (box_size > 0), from the
 reference_bc_*.npz the periodic boundary operator (BC_Type entry 3 of the
                    reference's precompute file) through M V and M^T V for
                    seeded V.
+refcppbc_*.npz     the reference's C++ interface (PtFMM_CreateTree,
+                   PtFMM_Evaluate) with BoundaryType Periodic.
 
 Run:  python tests/golden/make_golden.py [--force]   (existing oracle_*.npz and
 reference_*.npz are kept unless --force).  The reference tree is read from
@@ -273,6 +275,34 @@ def _periodic_operator(name):
                         MtV=M.T @ V, MV=M @ V, norm=np.linalg.norm(M))
 
 
+# The reference's C++ interface with BoundaryType Periodic (coordinates in
+# [0,1)^3 as given): kernel, m, max_pts, seed, double-layer points, lattice
+CPP_PERIODIC_CASES = {"laplace_m6": (0, 6, 50, 51, False, False), "stokes_vel_m4": (3, 4, 60, 52, False, False),
+                      "laplace_dl_m6": (0, 6, 50, 53, True, False), "lattice_laplace_m6": (0, 6, 50, 54, False, True)}
+
+
+def cpp_periodic_inputs(name):
+    """Single-layer points (clustered across the periodic faces), their
+    values, double-layer points and values (empty unless the case has them),
+    targets (uniform); all in [0,1)^3."""
+    kid, _, _, seed, with_dl, _ = CPP_PERIODIC_CASES[name]
+    rng = np.random.default_rng(seed)
+    k0 = KDIM[kid][0]
+    sl = points("corner", 2000, seed) % 1.0
+    dl = rng.random((1200 if with_dl else 0, 3))
+    trg = rng.random((1000, 3))
+    return sl, rng.uniform(-1, 1, (2000, k0)), dl, rng.uniform(-1, 1, (len(dl), k0 + 3)), trg
+
+
+def _cpp_periodic_case(name):
+    from oracle.ref_fmm import refpvfmm as R
+    kid, m, mp, _, _, lattice = CPP_PERIODIC_CASES[name]
+    sl, sd, dl, dd, trg = cpp_periodic_inputs(name)
+    out = R.ref_ptfmm_eval(kid, m, mp, sl, sd, dl, dd, trg, periodic=True, lattice=lattice)
+    np.savez_compressed(os.path.join(HERE, f"refcppbc_{name}.npz"), kernel=kid, m=m, max_pts=mp, lattice=lattice,
+                        sl=sl, sd=sd, dl=dl, dd=dd, trg=trg, out=out)
+
+
 def periodic_golden(force=False):
     """One process per fixture: the two reference builds are not loaded into
     one process."""
@@ -282,6 +312,9 @@ def periodic_golden(force=False):
     for name in PERIODIC_OPERATORS:
         if force or not os.path.exists(os.path.join(HERE, f"reference_bc_{name}.npz")):
             subprocess.run([sys.executable, os.path.abspath(__file__), "--periodic-operator", name], check=True)
+    for name in CPP_PERIODIC_CASES:
+        if force or not os.path.exists(os.path.join(HERE, f"refcppbc_{name}.npz")):
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--cpp-periodic-case", name], check=True)
 
 
 def reference_golden(force=False):
@@ -321,6 +354,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--periodic-operator" in sys.argv:
         _periodic_operator(sys.argv[sys.argv.index("--periodic-operator") + 1])
+        sys.exit(0)
+    if "--cpp-periodic-case" in sys.argv:
+        _cpp_periodic_case(sys.argv[sys.argv.index("--cpp-periodic-case") + 1])
         sys.exit(0)
     if os.path.isdir(os.environ.get("PVFMM_REFERENCE", "/root/reference")):
         morton_golden()

@@ -143,3 +143,27 @@ def test_cpp_interface_double_layer_points_match_oracle(tmp_path, kid, m, tol):
     ref2 = O.ptfmm_eval(kid, m, 60, src, den2, trg, ops=ops, dl_pos=dl, dl_den=dd2)
     assert O.rel_l2(val1, ref1) < tol
     assert O.rel_l2(val2, ref2) < tol
+
+
+@pytest.mark.gpu
+def test_cpp_interface_periodic_tree(tmp_path):
+    """PtFMM_CreateTree(..., pvfmm::Periodic) in the header: a periodic
+    context of period 1 in unit-box mode (pinned to the reference's C++
+    interface in tests/test_gpu_periodic.py)."""
+    exe = _compile(tmp_path)
+    out = str(tmp_path / "out.bin")
+    r = subprocess.run([exe, out, "0", "6", "60", "2500", "1500", "13", "d", "0", "periodic"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    _, _, (src, den, den2, trg, val1, val2, _, _, _, _, _) = _read(out)
+    ctx = P.FMMParticleContext(1.0, 60, 6, P.FMMKernel.LaplacePotential)
+    ctx.set_unit_box(True)
+    ref1 = ctx.evaluate(src, den, None, trg, True)
+    ref2 = ctx.evaluate(src, den2, None, trg, False)
+    assert O.rel_l2(val1, ref1) < 1e-14
+    assert O.rel_l2(val2, ref2) < 1e-14
+    free = P.FMMParticleContext(-1.0, 60, 6, P.FMMKernel.LaplacePotential)
+    free.set_unit_box(True)
+    assert O.rel_l2(val1, free.evaluate(src, den, None, trg, True)) > 1e-3   # the images matter
+    ctx.close()
+    free.close()

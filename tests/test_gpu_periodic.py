@@ -139,3 +139,33 @@ def test_periodic_bc_option_rejections():
     with pytest.raises(RuntimeError):
         per.set_periodic_bc(True, np.zeros((152, 152)))
     per.close()
+
+
+from make_golden import CPP_PERIODIC_CASES  # noqa: E402
+
+
+@pytest.mark.parametrize("name", sorted(CPP_PERIODIC_CASES))
+def test_cpp_interface_periodic_matches_reference(name):
+    """The C++ interface's periodic tree (PtFMM_CreateTree(..., Periodic):
+    coordinates in the unit cube as given, the targets as the tree's points;
+    include/pvfmm.hpp does what this test does through the C interface)
+    against the reference's own C++ interface (tests/golden/refcppbc_*.npz)."""
+    z = np.load(os.path.join(HERE, "golden", f"refcppbc_{name}.npz"))
+    kid, m, mp, lattice = int(z["kernel"]), int(z["m"]), int(z["max_pts"]), bool(z["lattice"])
+    ctx = P.FMMParticleContext(1.0, mp, m, P.FMMKernel(kid))
+    ctx.set_unit_box(True)
+    if lattice:
+        ctx.set_periodic_bc(True)
+    sl, sd, dl, dd, trg = z["sl"], z["sd"], z["dl"], z["dd"], z["trg"]
+    k0 = sd.shape[1]
+    if len(dl):
+        ctx.set_layer_points(True)
+        s = np.concatenate([sl, dl])
+        d = np.concatenate([sd, np.zeros((len(dl), k0))])
+        v = np.concatenate([np.zeros((len(sl), k0 + 3)), dd])
+        out = ctx.evaluate(s.reshape(-1), d.reshape(-1), v.reshape(-1), trg.reshape(-1), True)
+    else:
+        out = ctx.evaluate(sl.reshape(-1), sd.reshape(-1), None, trg.reshape(-1), True)
+    err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
+    assert err < (1e-10 if lattice or kid == 3 else 1e-12), err
+    ctx.close()

@@ -178,7 +178,7 @@ def test_double_layer_needs_a_double_layer_kernel():
         O.pvfmm_eval(1, 4, 40, x, None, x, dl_den=rng.uniform(-1, 1, (300, 4)))
 
 
-CPP_FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "refcpp_*.npz")))
+CPP_FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "refcpp_*.npz")))  # free space (refcppbc_*: periodic)
 
 
 @pytest.mark.parametrize("path", CPP_FIXTURES, ids=[os.path.basename(f)[7:-4] for f in CPP_FIXTURES])
