@@ -141,7 +141,9 @@ void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kern
  *     field and the corner correction; for LaplacePotential and
  *     StokesVelocity the potential of the mean density is taken out of the
  *     outputs); LaplacePotential, LaplaceGradient and StokesVelocity only,
- *     m2c must be NULL.
+ *     m2c must be NULL.  With PVFMM_DIR set, the lattice operator is kept in
+ *     PVFMM_DIR/Precomp_<kernel name>_m<m>_lattice_bc.data (int rows, int
+ *     cols, FP64 values) and read back by later contexts.
  * Returns 0, or -1 (message in PVFMMGetLastError()) for a free-space context,
  * an unsupported kernel or bad arguments. */
 int PVFMMSetPeriodicBC(void* ctx, int lattice, const double* m2c);

@@ -722,6 +722,8 @@ void vol_poten(int exp_kernel, const double* p, int n, double* out) {
 
 }  // namespace
 
+std::vector<double> lattice_bc(const KernelInfo& ki, int m);
+
 bool lattice_bc_supported(int kernel) { return kernel == kLaplacePot || kernel == kLaplaceGrad || kernel == kStokesVel; }
 
 std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
@@ -749,7 +751,43 @@ std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
     return M;
   }
   if (!lattice_bc_supported(kernel)) throw std::runtime_error("periodic lattice sum: kernel not supported");
+  // operator file (with PVFMM_DIR, beside the pseudo-inverse factors): int
+  // rows, int cols, rows*cols FP64 values; the order m+2 SVDs of the lattice
+  // sum take minutes for Stokes at m >= 10
+  const std::string base = cache_path(ki, m);
+  const std::string path = base.empty() ? "" : base.substr(0, base.size() - 5) + "_lattice_bc.data";
+  {
+    const int n = 6 * (m - 1) * (m - 1) + 2, dim = n * ki.ke;
+    std::ifstream in(path, std::ios::binary);
+    if (!path.empty() && in) {
+      int rc[2] = {0, 0};
+      std::vector<double> M((size_t)dim * dim);
+      in.read(reinterpret_cast<char*>(rc), sizeof(rc));
+      if (!in || rc[0] != dim || rc[1] != dim) throw std::runtime_error("operator file " + path + ": wrong sizes");
+      in.read(reinterpret_cast<char*>(M.data()), (std::streamsize)(M.size() * sizeof(double)));
+      if (!in) throw std::runtime_error("operator file " + path + ": truncated");
+      return M;
+    }
+  }
+  std::vector<double> M = lattice_bc(ki, m);
+  if (!path.empty()) {  // written through a temporary file renamed into place; an unwritable directory is skipped
+    const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+    if (FILE* fp = std::fopen(tmp.c_str(), "wb")) {
+      const int dim = (int)std::lround(std::sqrt((double)M.size()));
+      const int rc[2] = {dim, dim};
+      bool ok = std::fwrite(rc, sizeof(int), 2, fp) == 2 &&
+                std::fwrite(M.data(), sizeof(double), M.size(), fp) == M.size();
+      ok = (std::fclose(fp) == 0) && ok;
+      if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+    }
+  }
+  return M;
+}
+
+// The lattice sum itself (the reference built without PVFMM_EXTENDED_BC).
+std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
   const int ex = ki.exp_kernel, ke = ki.ke;
+  const int kernel = ki.id;
   // the reference attaches the volume potential to the Laplace potential and
   // Stokes velocity kernels only (the gradient kernel's expansion kernel has none)
   const bool has_vol = kernel == kLaplacePot || kernel == kStokesVel;

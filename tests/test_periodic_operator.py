@@ -43,3 +43,24 @@ def test_lattice_form_rejects_kernels_without_it():
     M = P.precomp_operator(P.FMMKernel.StokesPressure, 4, 0, 9)
     ns = 6 * 3 * 3 + 2
     assert M.size == ns * 3 * ns
+
+
+def test_lattice_operator_file(tmp_path):
+    """With PVFMM_DIR the lattice operator is written once and read back
+    (the same values); a file of the wrong size is an error."""
+    import subprocess
+    code = ("import numpy as np, pvfmm_b200 as P, time; "
+            "t=time.time(); a=P.precomp_operator(P.FMMKernel.LaplacePotential, 4, 0, 10); "
+            "print(len(a), a[:3].tolist())")
+    env = dict(os.environ, PVFMM_DIR=str(tmp_path))
+    root = os.path.dirname(HERE)
+    r1 = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=600)
+    assert r1.returncode == 0, r1.stderr
+    files = [f for f in os.listdir(tmp_path) if f.endswith("_lattice_bc.data")]
+    assert files == ["Precomp_laplace_m4_lattice_bc.data"]
+    r2 = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=600)
+    assert r2.returncode == 0 and r2.stdout == r1.stdout
+    with open(tmp_path / files[0], "r+b") as f:
+        f.truncate(100)
+    r3 = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=600)
+    assert r3.returncode != 0 and "operator file" in r3.stderr
