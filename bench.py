@@ -69,6 +69,17 @@ WORKLOADS = {
                        n_check=200, box=1.0, lattice=True,
                        desc="periodic laplace potential FMM (period 1, lattice sum over all images, setup=1 per "
                             "step), {n} uniform points, charge-neutral densities, m=8, 256/leaf"),
+    # the remaining kernels of the C interface (Stokes pressure, velocity
+    # gradient, Biot-Savart): 1M uniform points, N(0,1) source vectors, m=6
+    "stokespress1m": dict(kernel=2, m=6, max_pts=200, n=1_000_000, gen="stokes", seeds=(61, 62), check_seed=63,
+                          n_check=500, desc="stokes pressure FMM (setup=1 per step), {n} uniform points, N(0,1) "
+                                            "forces, m=6, 200/leaf"),
+    "stokesgrad1m": dict(kernel=4, m=6, max_pts=200, n=1_000_000, gen="stokes", seeds=(64, 65), check_seed=66,
+                         n_check=500, desc="stokes velocity gradient FMM (setup=1 per step), {n} uniform points, "
+                                           "N(0,1) forces, m=6, 200/leaf"),
+    "biotsavart1m": dict(kernel=5, m=6, max_pts=200, n=1_000_000, gen="stokes", seeds=(67, 68), check_seed=69,
+                         n_check=500, desc="biot-savart FMM (setup=1 per step), {n} uniform points, N(0,1) "
+                                           "currents, m=6, 200/leaf"),
     # the differentiable Laplace potential: one step = forward (pot+grad FMM)
     # + backward (swapped-role FMM on the forward's tree) through
     # pvfmm_b200.autograd.LaplaceFMM, sources = targets
@@ -77,8 +88,9 @@ WORKLOADS = {
                                          "uniform points, m=8, 256/leaf"),
 }
 W = WORKLOADS["gaussian4m"]
-KDIM = {0: (1, 1), 3: (3, 3), 6: (1, 4)}          # kernel id -> (k0, k1)
-PAIR_FLOPS = {0: 9, 3: 29, 6: 18}                 # flops per pair (kernel.txx:1277,1317,1352; pot+grad 18)
+KDIM = {0: (1, 1), 2: (3, 1), 3: (3, 3), 4: (3, 9), 5: (3, 3), 6: (1, 4)}   # kernel id -> (k0, k1)
+# flops per pair (kernel.txx:1277, 1352, 1367, 1406, 1493; pot+grad 18)
+PAIR_FLOPS = {0: 9, 2: 16, 3: 29, 4: 94, 5: 24, 6: 18}
 
 
 def make_points(w, n):
@@ -120,8 +132,11 @@ def gaussian_mixture(n, seed_c=11, seed_p=12, seed_q=13):
 
 def direct_gpu(torch, kid, x, q, idx):
     """FP64 direct sum at targets x[idx] over all points (GPU, torch), r == 0
-    excluded: Laplace potential (0), Stokes velocity (3) or Laplace potential
-    and r q / r^3 (6), with the kernels' 1/(4 pi) or 1/(8 pi)."""
+    excluded, r = target - source: Laplace potential (0), Stokes pressure
+    (r.f / r^3, 2), Stokes velocity (3), Stokes velocity gradient ((delta_ij
+    r.f + r_j f_i - f_j r_i - 3 r.f r_i r_j / r^2) / r^3, 4), Biot-Savart
+    (f x r / r^3, 5) or Laplace potential and r q / r^3 (6), with the
+    kernels' 1/(8 pi) (3, 4) or 1/(4 pi)."""
     X = torch.as_tensor(x, device="cuda", dtype=torch.float64)
     Q = torch.as_tensor(q, device="cuda", dtype=torch.float64).reshape(X.shape[0], -1)
     T = X[torch.as_tensor(idx, device="cuda")]
@@ -135,12 +150,27 @@ def direct_gpu(torch, kid, x, q, idx):
         if kid == 3:
             ip = torch.einsum("tsk,sk->ts", d, qa) * rinv * rinv
             out += torch.einsum("ts,sk->tk", rinv, qa) + torch.einsum("ts,tsk->tk", rinv * ip, d)
+        elif kid in (2, 4, 5):
+            r3 = rinv * rinv * rinv
+            rf = torch.einsum("tsk,sk->ts", d, qa)
+            if kid == 2:
+                out[:, 0] += (rf * r3).sum(1)
+            elif kid == 5:
+                out += torch.einsum("ts,tsk->tk", r3, torch.cross(qa[None, :, :].expand_as(d), d, dim=-1))
+            else:
+                c3 = 3 * rf * rinv * rinv
+                for i in range(3):
+                    for j in range(3):
+                        v = d[:, :, j] * qa[None, :, i] - qa[None, :, j] * d[:, :, i] - c3 * d[:, :, i] * d[:, :, j]
+                        if i == j:
+                            v = v + rf
+                        out[:, 3 * i + j] += (v * r3).sum(1)
         else:
             qr = rinv * qa[None, :, 0]
             out[:, 0] += qr.sum(1)
             if kid == 6:
                 out[:, 1:] += (d * (qr * rinv * rinv)[:, :, None]).sum(1)
-    return (out / (8 * math.pi if kid == 3 else 4 * math.pi)).cpu().numpy()
+    return (out / (8 * math.pi if kid in (3, 4) else 4 * math.pi)).cpu().numpy()
 
 
 def ewald_gpu(torch, x, q, idx, alpha=5.5, kmax=10):
@@ -289,7 +319,7 @@ def job_throughput(world, n, ms):
 # as these C-interface kernels in turn, on the same points (one step = all of
 # them).  PVFMMKernel ids: 0 Laplace potential, 1 Laplace gradient, 3 Stokes
 # velocity.
-REFERENCE_KERNELS = {0: (0,), 3: (3,), 6: (0, 1)}
+REFERENCE_KERNELS = {0: (0,), 2: (2,), 3: (3,), 4: (4,), 5: (5,), 6: (0, 1)}
 REF_STAGES = ("InitFMM_Tree", "SetupFMM", "S2U", "U2U", "U-List", "V-List", "W-List", "X-List", "D2D", "D2T")
 
 
@@ -367,7 +397,8 @@ def run_reference(args, world, rank):
         c.close()
     ms = 1000 * float(np.mean(times))
     value = n / (ms / 1000)
-    kernels = "+".join({0: "LaplacePotential", 1: "LaplaceGradient", 3: "StokesVelocity"}[k]
+    kernels = "+".join({0: "LaplacePotential", 1: "LaplaceGradient", 2: "StokesPressure", 3: "StokesVelocity",
+                        4: "StokesVelocityGrad", 5: "BiotSavartPotential"}[k]
                        for k in REFERENCE_KERNELS[W["kernel"]])
     sample = (f"{n} of the workload's {args.n} points (seed 15), the reference's PVFMMEvalD ({kernels}), FP64, "
               f"setup=1 per step, {cores} threads on {cpu_model()}")
