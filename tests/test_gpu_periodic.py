@@ -169,3 +169,28 @@ def test_cpp_interface_periodic_matches_reference(name):
     err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
     assert err < (1e-10 if lattice or kid == 3 else 1e-12), err
     ctx.close()
+
+
+def test_periodic_adjoint_is_the_transposed_image_sum():
+    """The adjoint evaluation of a periodic context (5x5x5 images, whose sum
+    is symmetric in the roles): <g, A q> = <A^T g, q> to FMM accuracy with
+    separate sources and targets; the lattice form is rejected."""
+    import torch
+    rng = np.random.default_rng(9)
+    ns, nt = 3000, 2000
+    s = torch.as_tensor(rng.random((ns, 3)), device="cuda")
+    t = torch.as_tensor(rng.random((nt, 3)), device="cuda")
+    q = torch.as_tensor(rng.uniform(-1, 1, ns), device="cuda")
+    g = torch.as_tensor(rng.uniform(-1, 1, nt), device="cuda")
+    ctx = P.FMMParticleContext(1.0, 50, 8, P.FMMKernel.LaplacePotential)
+    aq = torch.empty(nt, device="cuda", dtype=torch.float64)
+    atg = torch.empty(ns, device="cuda", dtype=torch.float64)
+    ctx.evaluate_device(s.data_ptr(), q.data_ptr(), ns, t.data_ptr(), aq.data_ptr(), nt, True, 0)
+    ctx.evaluate_adjoint_device(s.data_ptr(), ns, t.data_ptr(), g.data_ptr(), nt, atg.data_ptr(), True, 0)
+    torch.cuda.synchronize()
+    lhs, rhs = float((g * aq).sum()), float((atg * q).sum())
+    assert abs(lhs - rhs) < 1e-6 * float(g.norm() * aq.norm())
+    ctx.set_periodic_bc(True)
+    with pytest.raises(RuntimeError, match="adjoint"):
+        ctx.evaluate_adjoint_device(s.data_ptr(), ns, t.data_ptr(), g.data_ptr(), nt, atg.data_ptr(), True, 0)
+    ctx.close()
