@@ -148,6 +148,15 @@ void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kern
  * an unsupported kernel or bad arguments. */
 int PVFMMSetPeriodicBC(void* ctx, int lattice, const double* m2c);
 
+/* Periodic axes of a periodic context (the reference's BoundaryType PX, PXY
+ * and PXYZ == Periodic, include/mpi_tree.hpp:23-30, which its C++ interface
+ * selects in PtFMM_CreateTree): 1 = x, 3 = x and y, 7 = x, y and z (the
+ * default, the only one the C interface's box_size gives).  Along the other
+ * axes the unit cube is free space.  The next evaluation rebuilds the tree.
+ * Returns 0, or -1 (message in PVFMMGetLastError()) for a free-space context
+ * or another mask. */
+int PVFMMSetPeriodicAxes(void* ctx, int axes);
+
 /* Evaluation on device pointers (CUDA global memory).  The work is ordered
  * after the work already queued on `stream` (a cudaStream_t) and `stream`
  * waits for its completion; with NULL it is ordered after the legacy default

@@ -37,8 +37,9 @@
 
 namespace pvfmm {
 
-// Boundary types with the reference's values (include/mpi_tree.hpp:23-30);
-// the C interface builds FreeSpace and Periodic (== PXYZ).
+// Boundary types with the reference's values (include/mpi_tree.hpp:23-30):
+// free space, or periodic along x (PX), x and y (PXY) or all axes (PXYZ ==
+// Periodic).
 enum BoundaryType { FreeSpace = 0, PX, PXY, PXYZ, Periodic = PXYZ };
 
 // Kernel object (reference include/kernel.hpp:27-106).  ker_poten is the
@@ -136,13 +137,13 @@ class PtFMM_Tree {
  public:
   PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
              const std::vector<Real>& trg_coord, int max_pts, BoundaryType bndry = FreeSpace)
-      : src_(src_coord), den_(src_value), trg_(trg_coord), max_pts_(max_pts), periodic_(bndry == Periodic) {}
+      : src_(src_coord), den_(src_value), trg_(trg_coord), max_pts_(max_pts), bndry_(bndry) {}
   // with a separate double-layer point set (surf_coord, k0 + 3 values per point)
   PtFMM_Tree(const std::vector<Real>& src_coord, const std::vector<Real>& src_value,
              const std::vector<Real>& surf_coord, const std::vector<Real>& surf_value,
              const std::vector<Real>& trg_coord, int max_pts, BoundaryType bndry = FreeSpace)
       : src_(src_coord), den_(src_value), surf_(surf_coord), dl_(surf_value), trg_(trg_coord), max_pts_(max_pts),
-        periodic_(bndry == Periodic) {}
+        bndry_(bndry) {}
   ~PtFMM_Tree() { release(); }
   PtFMM_Tree(const PtFMM_Tree&) = delete;
   PtFMM_Tree& operator=(const PtFMM_Tree&) = delete;
@@ -157,9 +158,13 @@ class PtFMM_Tree {
     k0_ = k->ker_dim[0];
     k1_ = k->ker_dim[1];
     const int precision = std::is_same<Real, float>::value ? PVFMMPrecisionMixed : PVFMMPrecisionPlain;
-    // periodic: period 1, the unit cube itself (the coordinates are used as given)
-    ctx_ = PVFMMCreateContextExD(periodic_ ? 1.0 : -1.0, max_pts_, mat->MultipoleOrder(), k->id, precision);
+    // periodic: period 1, the unit cube itself (the coordinates are used as
+    // given), along x (PX), x and y (PXY) or all axes (PXYZ == Periodic)
+    ctx_ = PVFMMCreateContextExD(bndry_ != FreeSpace ? 1.0 : -1.0, max_pts_, mat->MultipoleOrder(), k->id, precision);
     if (!ctx_) throw std::runtime_error(PVFMMGetLastError());
+    if (bndry_ == PX || bndry_ == PXY) {
+      if (PVFMMSetPeriodicAxes(ctx_, bndry_ == PX ? 1 : 3) != 0) throw std::runtime_error(PVFMMGetLastError());
+    }
     if (PVFMMSetUnitBox(ctx_, 1) != 0) throw std::runtime_error(PVFMMGetLastError());
     // both point sets count in the tree (include/fmm_node.txx:81-92): they are
     // passed concatenated, each point with its own layer's values
@@ -205,7 +210,7 @@ class PtFMM_Tree {
   }
   std::vector<Real> src_, den_, surf_, dl_, trg_;
   int max_pts_;
-  bool periodic_ = false;
+  BoundaryType bndry_ = FreeSpace;
   int k0_ = 1, k1_ = 1;
   void* ctx_ = nullptr;
   bool needs_setup_ = true;
@@ -218,8 +223,8 @@ PtFMM_Tree<Real>* PtFMM_CreateTree(const std::vector<Real>& sl_coord, const std:
                                    BoundaryType bndry = FreeSpace, int init_depth = 0) {
   (void)comm;
   (void)init_depth;
-  if (bndry != FreeSpace && bndry != Periodic)
-    throw std::runtime_error("PtFMM_CreateTree: FreeSpace or Periodic boundaries only");
+  if (bndry != FreeSpace && bndry != PX && bndry != PXY && bndry != PXYZ)
+    throw std::runtime_error("PtFMM_CreateTree: unknown boundary type");
   return new PtFMM_Tree<Real>(sl_coord, sl_density, dl_coord, dl_density, trg_coord, max_pts, bndry);
 }
 

@@ -166,7 +166,8 @@ int ref_ptfmm_eval(int kernel, int m, int max_pts, long n_sl, const double* sl_c
                            out);
 }
 
-// The same with the boundary type: periodic != 0 gives BoundaryType Periodic.
+// The same with the boundary type: `periodic` is the BoundaryType value
+// (0 FreeSpace, 1 PX, 2 PXY, 3 PXYZ == Periodic).
 int ref_ptfmm_eval_bc(int kernel, int m, int max_pts, int periodic, long n_sl, const double* sl_coord,
                       const double* sl_den, long n_dl, const double* dl_coord, const double* dl_den, long n_trg,
                       const double* trg_coord, double* out) {
@@ -181,8 +182,8 @@ int ref_ptfmm_eval_bc(int kernel, int m, int max_pts, int periodic, long n_sl, c
   std::vector<double> tc(trg_coord, trg_coord + 3 * n_trg);
   pvfmm::PtFMM<double> matrices;
   matrices.Initialize(m, MPI_COMM_WORLD, ker);
-  auto* tree = pvfmm::PtFMM_CreateTree(sc, sv, dc, dv, tc, MPI_COMM_WORLD, max_pts,
-                                       periodic ? pvfmm::Periodic : pvfmm::FreeSpace);
+  if (periodic < 0 || periodic > 3) return 1;
+  auto* tree = pvfmm::PtFMM_CreateTree(sc, sv, dc, dv, tc, MPI_COMM_WORLD, max_pts, (pvfmm::BoundaryType)periodic);
   tree->SetupFMM(&matrices);
   std::vector<double> val;
   pvfmm::PtFMM_Evaluate(tree, val, n_trg);

@@ -217,11 +217,12 @@ def ref_eval(kernel, m, max_pts, src, den, trg=None, threads=0, dl=None, box_siz
 
 
 def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, threads=0, periodic=False,
-                   lattice=False):
+                   lattice=False, bndry=None):
     """The reference's C++ interface (PtFMM_CreateTree with separate single-
     and double-layer point sets, SetupFMM, PtFMM_Evaluate; coordinates in
-    [0,1)^3 as given; BoundaryType Periodic when periodic, from the lattice
-    build when lattice).  Either point set may be empty (shape (0, 3))."""
+    [0,1)^3 as given; BoundaryType Periodic when periodic, or the BoundaryType
+    value bndry (0 FreeSpace, 1 PX, 2 PXY, 3 PXYZ); from the lattice build
+    when lattice).  Either point set may be empty (shape (0, 3))."""
     lib = load(lattice)
     if threads:
         lib.ref_set_threads(threads)
@@ -237,7 +238,8 @@ def ref_ptfmm_eval(kernel, m, max_pts, sl_coord, sl_den, dl_coord, dl_den, trg, 
     if lattice:
         os.environ["PVFMM_DIR"] = _lattice_dir[0]
     try:
-        rc = lib.ref_ptfmm_eval_bc(kernel, m, max_pts, 1 if periodic else 0, len(sc) // 3, _p(sc), _p(sv),
+        bt = bndry if bndry is not None else (3 if periodic else 0)
+        rc = lib.ref_ptfmm_eval_bc(kernel, m, max_pts, bt, len(sc) // 3, _p(sc), _p(sv),
                                    len(dc) // 3, _p(dc), _p(dv), n_trg, _p(tc), _p(out))
     finally:
         if lattice and saved is not None:

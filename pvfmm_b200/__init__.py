@@ -81,6 +81,7 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         "PVFMMSetUnitBox": (ci, [vp, ci]),
         "PVFMMSetLayerPoints": (ci, [vp, ci]),
         "PVFMMSetPeriodicBC": (ci, [vp, ci, vp]),
+        "PVFMMSetPeriodicAxes": (ci, [vp, ci]),
         "PVFMMKernelEvalD": (ci, [ci, vp, vp, cl, vp, vp, cl]),
         "PVFMMKernelEvalDeviceNoAllocD": (ci, [ci, vp, vp, cl, vp, vp, cl, vp]),
         "PVFMMDestroyContextD": (None, [ctypes.POINTER(vp)]),
@@ -280,6 +281,12 @@ class FMMParticleContext:
         SetM2C), or with ``lattice`` the lattice sum over all images."""
         a = None if m2c is None else np.ascontiguousarray(m2c, dtype=np.float64).reshape(-1)
         if self._lib.PVFMMSetPeriodicBC(self._ptr, int(bool(lattice)), None if a is None else _ptr(a)) != 0:
+            raise RuntimeError(last_error())
+
+    def set_periodic_axes(self, axes: int) -> None:
+        """Periodic axes of a periodic context (PVFMMSetPeriodicAxes): 1 = x
+        (BoundaryType PX), 3 = x and y (PXY), 7 = all (PXYZ, the default)."""
+        if self._lib.PVFMMSetPeriodicAxes(self._ptr, int(axes)) != 0:
             raise RuntimeError(last_error())
 
     def set_layer_points(self, on: bool = True) -> None:

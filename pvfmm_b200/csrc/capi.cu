@@ -80,7 +80,7 @@ void destroy_context(Context& c) {
 // in device memory: the 5x5x5-image form plus the user's operator, or the
 // lattice sum.
 void upload_bc(Context& c) {
-  std::vector<double> M = build_bc_operator(c.kernel, c.m, c.bc_lattice != 0);
+  std::vector<double> M = build_bc_operator(c.kernel, c.m, c.bc_lattice != 0, c.periodic_axes);
   if (!c.bc_user.empty())
     for (size_t i = 0; i < M.size(); ++i) M[i] += c.bc_user[i];
   double* d = c.dops.bc.as<double>(M.size());
@@ -267,8 +267,9 @@ int eval_adjoint(const void* ctx, const T* src, long n_src, const T* trg, const 
       if (!h->adjoint) throw std::runtime_error(std::string("companion context: ") + get_last_error());
       Context& a = as_handle(h->adjoint)->ctx;
       a.unit_box = c.unit_box;
-      if (c.periodic && !c.bc_user.empty()) {  // the periodic images' operator is symmetric in the roles
+      if (c.periodic && (!c.bc_user.empty() || c.periodic_axes != 7)) {  // symmetric in the roles
         a.bc_user = c.bc_user;
+        a.periodic_axes = c.periodic_axes;
         upload_bc(a);
       }
       setup = 1;
@@ -309,6 +310,32 @@ void* PVFMMCreateContextFWorld(float box_size, int n, int m, enum PVFMMKernel ke
 }
 void* PVFMMCreateContextExD(double box_size, int n, int m, enum PVFMMKernel kernel, int precision) {
   return create_context(box_size, n, m, (int)kernel, precision, false);
+}
+
+int PVFMMSetPeriodicAxes(void* ctx, int axes) {
+  try {
+    Context& c = as_handle(ctx)->ctx;
+    PVFMM_CUDA_CHECK(cudaSetDevice(c.device));
+    if (!c.periodic) throw std::runtime_error("the context has free-space boundaries (box_size <= 0)");
+    if (axes != 1 && axes != 3 && axes != 7) throw std::runtime_error("periodic axes must be 1 (x), 3 (xy) or 7 (xyz)");
+    PVFMM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    const int old = c.periodic_axes;
+    c.periodic_axes = axes;
+    try {
+      upload_bc(c);
+    } catch (...) {
+      c.periodic_axes = old;
+      throw;
+    }
+    if (axes != old) c.tree.valid = false;  // the tree's balance and lists depend on the axes
+    Handle* h = as_handle(ctx);
+    if (h->adjoint) destroy(&h->adjoint);
+    set_last_error("");
+    return 0;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return -1;
+  }
 }
 
 int PVFMMSetPeriodicBC(void* ctx, int lattice, const double* m2c) {

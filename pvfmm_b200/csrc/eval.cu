@@ -2470,7 +2470,7 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   }
   // periodic lattice sum of a kernel with a volume potential: the potential
   // of the mean density is taken out (PostProcessing, fmm_pts.txx:5741-5771)
-  if (ctx.periodic && ctx.bc_lattice && T.src_counted && T.n_trg > 0 &&
+  if (ctx.periodic && ctx.periodic_axes == 7 && ctx.bc_lattice && T.src_counted && T.n_trg > 0 &&
       (ctx.kernel == kLaplacePot || ctx.kernel == kStokesVel)) {
     ++ctx.n_launch;
     periodic_mean_correction<<<592, 256, 0, s>>>(T.n_trg, T.trg_leaf.get<int>(), keys, T.tx.get<double>(),

@@ -95,6 +95,7 @@ struct Context {
   // wrapped into the unit cube; bc_lattice selects the lattice-sum operator,
   // bc_user an operator added to the 5x5x5-image one (empty: none)
   bool periodic = false;
+  int periodic_axes = 7;  // bit 0 x, bit 1 y, bit 2 z: 7 = PXYZ (the C interface), 1 = PX, 3 = PXY
   double box_size = 0;
   int bc_lattice = 0;
   std::vector<double> bc_user;

@@ -89,7 +89,9 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
 // lattice sum (the option off), for the kernels lattice_bc_supported()
 // accepts (Laplace potential and gradient, Stokes velocity); throws otherwise.
 bool lattice_bc_supported(int kernel);
-std::vector<double> build_bc_operator(int kernel, int m, bool lattice);
+// axes: the periodic axes (bit 0 x, bit 1 y, bit 2 z; 1 = PX, 3 = PXY,
+// 7 = PXYZ == Periodic).
+std::vector<double> build_bc_operator(int kernel, int m, bool lattice, int axes = 7);
 
 // One-sided Jacobi SVD of a rows x cols row-major matrix (rows >= cols):
 // A = U diag(S) V^T with U rows x cols (column j scaled to unit length, or

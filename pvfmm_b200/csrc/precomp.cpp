@@ -722,16 +722,24 @@ void vol_poten(int exp_kernel, const double* p, int n, double* out) {
 
 }  // namespace
 
-std::vector<double> lattice_bc(const KernelInfo& ki, int m);
+std::vector<double> lattice_bc(const KernelInfo& ki, int m, int axes);
+
+// An image offset is taken when every axis it moves along is periodic
+// (axes: bit 0 x, bit 1 y, bit 2 z; BoundaryType PX 1, PXY 3, PXYZ 7).
+bool image_axes_ok(int axes, int x0, int x1, int x2) {
+  return (x0 == 0 || (axes & 1)) && (x1 == 0 || (axes & 2)) && (x2 == 0 || (axes & 4));
+}
 
 bool lattice_bc_supported(int kernel) { return kernel == kLaplacePot || kernel == kLaplaceGrad || kernel == kStokesVel; }
 
-std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
+std::vector<double> build_bc_operator(int kernel, int m, bool lattice, int axes) {
   KernelInfo ki;
   if (!kernel_info_host(kernel, &ki)) throw std::runtime_error("periodic boundaries: unknown kernel");
+  if (axes != 1 && axes != 3 && axes != 7) throw std::runtime_error("periodic axes must be x, xy or xyz");
   if (!lattice) {
     // the reference's default build (PVFMM_EXTENDED_BC, :1189-1232): the
-    // images in [-2, 2]^3 outside [-1, 1]^3 at order m, nothing beyond them
+    // images in [-2, 2]^3 outside [-1, 1]^3 (along the periodic axes) at
+    // order m, nothing beyond them
     int kin, kout;
     exp_kernel_dims(ki.exp_kernel, &kin, &kout);
     const std::vector<double> u = unit_surface(m);
@@ -743,6 +751,7 @@ std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
       for (int x1 = -2; x1 <= 2; ++x1)
         for (int x2 = -2; x2 <= 2; ++x2) {
           if (std::abs(x0) <= 1 && std::abs(x1) <= 1 && std::abs(x2) <= 1) continue;
+          if (!image_axes_ok(axes, x0, x1, x2)) continue;
           const double c[3] = {(double)x0, (double)x1, (double)x2};
           const std::vector<double> src = box_surface(u, c, 0, kRad0);
           exp_kernel_matrix(ki.exp_kernel, src.data(), ns, dk.data(), ns, T.data());
@@ -755,7 +764,9 @@ std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
   // rows, int cols, rows*cols FP64 values; the order m+2 SVDs of the lattice
   // sum take minutes for Stokes at m >= 10
   const std::string base = cache_path(ki, m);
-  const std::string path = base.empty() ? "" : base.substr(0, base.size() - 5) + "_lattice_bc.data";
+  const std::string path = base.empty() ? ""
+                                         : base.substr(0, base.size() - 5) + "_lattice_bc" +
+                                               (axes == 1 ? "_px" : axes == 3 ? "_pxy" : "") + ".data";
   {
     const int n = 6 * (m - 1) * (m - 1) + 2, dim = n * ki.ke;
     std::ifstream in(path, std::ios::binary);
@@ -769,7 +780,7 @@ std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
       return M;
     }
   }
-  std::vector<double> M = lattice_bc(ki, m);
+  std::vector<double> M = lattice_bc(ki, m, axes);
   if (!path.empty()) {  // written through a temporary file renamed into place; an unwritable directory is skipped
     const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
     if (FILE* fp = std::fopen(tmp.c_str(), "wb")) {
@@ -785,12 +796,13 @@ std::vector<double> build_bc_operator(int kernel, int m, bool lattice) {
 }
 
 // The lattice sum itself (the reference built without PVFMM_EXTENDED_BC).
-std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
+std::vector<double> lattice_bc(const KernelInfo& ki, int m, int axes) {
   const int ex = ki.exp_kernel, ke = ki.ke;
   const int kernel = ki.id;
   // the reference attaches the volume potential to the Laplace potential and
-  // Stokes velocity kernels only (the gradient kernel's expansion kernel has none)
-  const bool has_vol = kernel == kLaplacePot || kernel == kStokesVel;
+  // Stokes velocity kernels only (the gradient kernel's expansion kernel has
+  // none), and uses it for PXYZ only
+  const bool has_vol = (kernel == kLaplacePot || kernel == kStokesVel) && axes == 7;
   const int m1 = m + 2;  // mult_upsample = 2
   const std::vector<double> u1 = unit_surface(m1), u0 = unit_surface(m);
   const int ns1 = (int)u1.size() / 3, ns0 = (int)u0.size() / 3;
@@ -844,6 +856,7 @@ std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
   {
     const std::vector<double> ck = box_surface(u1, mone, -1, kRad1);
     for (int c = 0; c < 8; ++c) {
+      if (!image_axes_ok(axes, c & 1, (c >> 1) & 1, (c >> 2) & 1)) continue;
       const double sb[3] = {-1.0 + (c & 1), -1.0 + ((c >> 1) & 1), -1.0 + ((c >> 2) & 1)};
       add(M2M, kmat(ex, ke, box_surface(u1, sb, 0, kRad0), ck));
     }
@@ -863,6 +876,7 @@ std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
       for (int k1 = -2; k1 < 4; ++k1)
         for (int k2 = -2; k2 < 4; ++k2) {
           if (std::abs(k0) <= 1 && std::abs(k1) <= 1 && std::abs(k2) <= 1) continue;
+          if (!image_axes_ok(axes, k0, k1, k2)) continue;
           const double sb[3] = {(double)k0, (double)k1, (double)k2};
           add(M2L, kmat(ex, ke, box_surface(u1, sb, 0, kRad0), dk));
         }
@@ -917,6 +931,7 @@ std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
       for (int j0 = -1; j0 <= 1; ++j0)
         for (int j1 = -1; j1 <= 1; ++j1)
           for (int j2 = -1; j2 <= 1; ++j2) {
+            if (!image_axes_ok(axes, j0, j1, j2)) continue;
             const std::vector<double> pt = {corner[3 * k] - j0, corner[3 * k + 1] - j1, corner[3 * k + 2] - j2};
             if (std::fabs(pt[0] - 0.5) < 1 && std::fabs(pt[1] - 0.5) < 1 && std::fabs(pt[2] - 0.5) < 1) continue;
             const std::vector<double> E = kmat(ex, ke, ue, pt);  // n1 x ke
@@ -932,7 +947,9 @@ std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
     }
     // coefficients of a + bx + cy + dz + exy + fxz + gyz + hxyz through the
     // inverse of the corners' Vandermonde matrix (nonsingular); the constant
-    // and linear terms are enabled for PXYZ
+    // term and the linear terms of the periodic axes are enabled (PXYZ: a,
+    // b, c, d; PXY: a, b, c; PX: a, b)
+    const double en[4] = {1.0, 1.0, (axes & 2) ? 1.0 : 0.0, (axes & 4) ? 1.0 : 0.0};
     std::vector<double> V(64), Vi;
     for (int i = 0; i < 8; ++i) {
       const double x = corner[3 * i], y = corner[3 * i + 1], z = corner[3 * i + 2];
@@ -951,8 +968,8 @@ std::vector<double> lattice_bc(const KernelInfo& ki, int m) {
         for (int q = 0; q < 4; ++q)
           for (int k = 0; k < 8; ++k) coef[q] += cv[(size_t)i * 8 * ke + k * ke + l] * Vi[k * 8 + q];
         for (int p = 0; p < ns1; ++p)
-          M[(size_t)i * n1 + p * ke + l] -=
-              coef[0] + coef[1] * dk[3 * p] + coef[2] * dk[3 * p + 1] + coef[3] * dk[3 * p + 2];
+          M[(size_t)i * n1 + p * ke + l] -= en[0] * coef[0] + en[1] * coef[1] * dk[3 * p] +
+                                            en[2] * coef[2] * dk[3 * p + 1] + en[3] * coef[3] * dk[3 * p + 2];
       }
   }
   // back to order m (:1164-1188): order-m equivalent -> order-m1 equivalent,

@@ -189,6 +189,7 @@ __global__ void make_children(const MKey* __restrict__ cur, const int* __restric
 // For internal node X at level d: parents (level d-1) of its 3^3 neighbours
 // clipped to the unit box; per axis these are parent(x) and the parent on the
 // side of x within its parent.  Invalid candidates get the sentinel key.
+// periodic: the mask of periodic axes (bit 0 x, bit 1 y, bit 2 z; 0 = free space)
 __global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, int periodic, MKey* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -203,7 +204,7 @@ __global__ void nbr_parents(const MKey* __restrict__ S, long n, int d, int perio
     // the neighbour parent across the near face; outside the unit cube it
     // wraps around for periodic boundaries (NbrList, mortonid.cpp:15-55)
     long c = (q[a] & w) ? p0 + 2L * w : p0 - 2L * w;
-    if (c < 0 || c >= (long)kTwo30) c = periodic ? (c + (long)kTwo30) % (long)kTwo30 : -1;
+    if (c < 0 || c >= (long)kTwo30) c = ((periodic >> a) & 1) ? (c + (long)kTwo30) % (long)kTwo30 : -1;
     cand[a][1] = c;
   }
   for (int c = 0; c < 8; ++c) {
@@ -313,16 +314,22 @@ __global__ void node_ranges(const MKey* __restrict__ keys, long n, const MKey* _
 // at offset floor((c + d) / 2), which exists at this level iff that colleague
 // is internal (every internal node has all 8 children in the level arrays).
 // Same result as searching the level's sorted keys (interac_list.txx:98-130).
-// Periodic boundaries: every colleague of the root is the root itself (one
-// image per slot, mpi_tree.txx:1142-1168), and the rule above then wraps the
-// colleagues of every level around the unit cube.
+// Periodic boundaries: every colleague of the root along the periodic axes
+// (mask `periodic`: bit 0 x, bit 1 y, bit 2 z) is the root itself (one image
+// per slot, mpi_tree.txx:1142-1168), and the rule above then wraps the
+// colleagues of every level around the unit cube along those axes.
 __global__ void colleagues_kernel(long base, long n_level, const int* __restrict__ parent,
                                   const int* __restrict__ child0, int periodic, int* __restrict__ coll) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n_level) return;
   const long v = base + i;
   if (v == 0) {
-    for (int ci = 0; ci < 27; ++ci) coll[ci] = (ci == 13 || periodic) ? 0 : -1;
+    for (int ci = 0; ci < 27; ++ci) {
+      const int dx = ci % 3 - 1, dy = (ci / 3) % 3 - 1, dz = ci / 9 - 1;
+      const bool img = periodic && (dx == 0 || (periodic & 1)) && (dy == 0 || (periodic & 2)) &&
+                       (dz == 0 || (periodic & 4));
+      coll[ci] = (ci == 13 || img) ? 0 : -1;
+    }
     return;
   }
   const int P = parent[v];
@@ -942,7 +949,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
                                        cudaMemcpyDeviceToDevice, s));
       ++ctx.n_launch;
       nbr_parents<<<ceil_div(nS[d], kThreads), kThreads, 0, s>>>(ctx.lvlS[d].get<MKey>(), nS[d], d,
-                                                                 ctx.periodic ? 1 : 0, cand + nR[d - 1]);
+                                                                 ctx.periodic ? ctx.periodic_axes : 0,
+                                                                 cand + nR[d - 1]);
       nS[d - 1] = sort_unique(ctx, cand, nc, ctx.lvlS[d - 1], d - 1);
     }
   }
@@ -1004,8 +1012,8 @@ void build_tree(Context& ctx, const void* src_pos, long n_src, const void* trg_p
   for (int d = 0; d <= D; ++d) {
     const long base = T.level_off[d], nl = T.level_off[d + 1] - base;
     ++ctx.n_launch;
-    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0, ctx.periodic ? 1 : 0,
-                                                                   coll);
+    colleagues_kernel<<<ceil_div(nl, kThreads), kThreads, 0, s>>>(base, nl, parent, child0,
+                                                                   ctx.periodic ? ctx.periodic_axes : 0, coll);
   }
   // 9. compact node lists.  The compacted lists are sized for all N nodes so
   //    that the eight counts are read back together at one synchronisation.

@@ -5,10 +5,10 @@
 // With n_dl > 0 the tree also holds a separate double-layer point set
 // (PtFMM_CreateTree with surf_coord / surf_value, k0 + 3 values per point),
 // and the second evaluation passes new values for both layers.  With a
-// trailing "periodic" the tree has BoundaryType Periodic.  Writes inputs and
+// trailing "periodic", "px" or "pxy" the tree has that BoundaryType.  Writes inputs and
 // outputs as raw doubles for the Python test to compare against the oracle.
 //
-// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f> [n_dl [periodic]]
+// usage: ptfmm_example <out.bin> <kernel id> <m> <max_pts> <n_src> <n_trg> <seed> <real: d|f> [n_dl [periodic|px|pxy]]
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -109,7 +109,7 @@ int run(const char* path, int kid, int m, int max_pts, long ns, long nt, uint64_
 
 int main(int argc, char** argv) {
   if (argc < 9 || argc > 11) {
-    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f [n_dl [periodic]]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s out kernel m max_pts n_src n_trg seed d|f [n_dl [periodic|px|pxy]]\n", argv[0]);
     return 1;
   }
   try {
@@ -117,8 +117,11 @@ int main(int argc, char** argv) {
     const long ns = std::atol(argv[5]), nt = std::atol(argv[6]);
     const uint64_t seed = std::strtoull(argv[7], nullptr, 10);
     const long n_dl = argc >= 10 ? std::atol(argv[9]) : 0;
-    const pvfmm::BoundaryType bndry =
-        argc == 11 && std::string(argv[10]) == "periodic" ? pvfmm::Periodic : pvfmm::FreeSpace;
+    const std::string bc = argc == 11 ? argv[10] : "";
+    const pvfmm::BoundaryType bndry = bc == "periodic" ? pvfmm::Periodic
+                                      : bc == "px"     ? pvfmm::PX
+                                      : bc == "pxy"    ? pvfmm::PXY
+                                                       : pvfmm::FreeSpace;
     if (std::string(argv[8]) == "f") return run<float>(argv[1], kid, m, mp, ns, nt, seed, n_dl, bndry);
     return run<double>(argv[1], kid, m, mp, ns, nt, seed, n_dl, bndry);
   } catch (const std::exception& e) {

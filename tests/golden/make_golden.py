@@ -275,17 +275,24 @@ def _periodic_operator(name):
                         MtV=M.T @ V, MV=M @ V, norm=np.linalg.norm(M))
 
 
-# The reference's C++ interface with BoundaryType Periodic (coordinates in
-# [0,1)^3 as given): kernel, m, max_pts, seed, double-layer points, lattice
-CPP_PERIODIC_CASES = {"laplace_m6": (0, 6, 50, 51, False, False), "stokes_vel_m4": (3, 4, 60, 52, False, False),
-                      "laplace_dl_m6": (0, 6, 50, 53, True, False), "lattice_laplace_m6": (0, 6, 50, 54, False, True)}
+# The reference's C++ interface with periodic boundaries (coordinates in
+# [0,1)^3 as given): kernel, m, max_pts, seed, double-layer points, lattice,
+# BoundaryType (3 PXYZ == Periodic, 2 PXY, 1 PX)
+CPP_PERIODIC_CASES = {"laplace_m6": (0, 6, 50, 51, False, False, 3), "stokes_vel_m4": (3, 4, 60, 52, False, False, 3),
+                      "laplace_dl_m6": (0, 6, 50, 53, True, False, 3),
+                      "lattice_laplace_m6": (0, 6, 50, 54, False, True, 3),
+                      "px_laplace_m6": (0, 6, 50, 55, False, False, 1),
+                      "pxy_laplace_m6": (0, 6, 50, 56, False, False, 2),
+                      "pxy_stokes_vel_m4": (3, 4, 60, 57, False, False, 2),
+                      "lattice_px_laplace_m6": (0, 6, 50, 58, False, True, 1),
+                      "lattice_pxy_stokes_vel_m4": (3, 4, 60, 59, False, True, 2)}
 
 
 def cpp_periodic_inputs(name):
     """Single-layer points (clustered across the periodic faces), their
     values, double-layer points and values (empty unless the case has them),
     targets (uniform); all in [0,1)^3."""
-    kid, _, _, seed, with_dl, _ = CPP_PERIODIC_CASES[name]
+    kid, _, _, seed, with_dl, _, _ = CPP_PERIODIC_CASES[name]
     rng = np.random.default_rng(seed)
     k0 = KDIM[kid][0]
     sl = points("corner", 2000, seed) % 1.0
@@ -296,11 +303,11 @@ def cpp_periodic_inputs(name):
 
 def _cpp_periodic_case(name):
     from oracle.ref_fmm import refpvfmm as R
-    kid, m, mp, _, _, lattice = CPP_PERIODIC_CASES[name]
+    kid, m, mp, _, _, lattice, bndry = CPP_PERIODIC_CASES[name]
     sl, sd, dl, dd, trg = cpp_periodic_inputs(name)
-    out = R.ref_ptfmm_eval(kid, m, mp, sl, sd, dl, dd, trg, periodic=True, lattice=lattice)
+    out = R.ref_ptfmm_eval(kid, m, mp, sl, sd, dl, dd, trg, lattice=lattice, bndry=bndry)
     np.savez_compressed(os.path.join(HERE, f"refcppbc_{name}.npz"), kernel=kid, m=m, max_pts=mp, lattice=lattice,
-                        sl=sl, sd=sd, dl=dl, dd=dd, trg=trg, out=out)
+                        bndry=bndry, sl=sl, sd=sd, dl=dl, dd=dd, trg=trg, out=out)
 
 
 def periodic_golden(force=False):

@@ -146,18 +146,21 @@ def test_cpp_interface_double_layer_points_match_oracle(tmp_path, kid, m, tol):
 
 
 @pytest.mark.gpu
-def test_cpp_interface_periodic_tree(tmp_path):
-    """PtFMM_CreateTree(..., pvfmm::Periodic) in the header: a periodic
-    context of period 1 in unit-box mode (pinned to the reference's C++
-    interface in tests/test_gpu_periodic.py)."""
+@pytest.mark.parametrize("bc,axes", [("periodic", 7), ("px", 1), ("pxy", 3)])
+def test_cpp_interface_periodic_tree(tmp_path, bc, axes):
+    """PtFMM_CreateTree(..., pvfmm::Periodic / PX / PXY) in the header: a
+    periodic context of period 1 in unit-box mode with those periodic axes
+    (pinned to the reference's C++ interface in tests/test_gpu_periodic.py)."""
     exe = _compile(tmp_path)
     out = str(tmp_path / "out.bin")
-    r = subprocess.run([exe, out, "0", "6", "60", "2500", "1500", "13", "d", "0", "periodic"],
+    r = subprocess.run([exe, out, "0", "6", "60", "2500", "1500", "13", "d", "0", bc],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     _, _, (src, den, den2, trg, val1, val2, _, _, _, _, _) = _read(out)
     ctx = P.FMMParticleContext(1.0, 60, 6, P.FMMKernel.LaplacePotential)
     ctx.set_unit_box(True)
+    if axes != 7:
+        ctx.set_periodic_axes(axes)
     ref1 = ctx.evaluate(src, den, None, trg, True)
     ref2 = ctx.evaluate(src, den2, None, trg, False)
     assert O.rel_l2(val1, ref1) < 1e-14

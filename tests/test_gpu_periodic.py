@@ -146,14 +146,18 @@ from make_golden import CPP_PERIODIC_CASES  # noqa: E402
 
 @pytest.mark.parametrize("name", sorted(CPP_PERIODIC_CASES))
 def test_cpp_interface_periodic_matches_reference(name):
-    """The C++ interface's periodic tree (PtFMM_CreateTree(..., Periodic):
-    coordinates in the unit cube as given, the targets as the tree's points;
-    include/pvfmm.hpp does what this test does through the C interface)
-    against the reference's own C++ interface (tests/golden/refcppbc_*.npz)."""
+    """The C++ interface's periodic trees (PtFMM_CreateTree(..., PX / PXY /
+    Periodic): coordinates in the unit cube as given, the targets as the
+    tree's points; include/pvfmm.hpp does what this test does through the C
+    interface) against the reference's own C++ interface
+    (tests/golden/refcppbc_*.npz)."""
     z = np.load(os.path.join(HERE, "golden", f"refcppbc_{name}.npz"))
     kid, m, mp, lattice = int(z["kernel"]), int(z["m"]), int(z["max_pts"]), bool(z["lattice"])
+    axes = {1: 1, 2: 3, 3: 7}[int(z["bndry"])]          # BoundaryType PX, PXY, PXYZ -> periodic axes
     ctx = P.FMMParticleContext(1.0, mp, m, P.FMMKernel(kid))
     ctx.set_unit_box(True)
+    if axes != 7:
+        ctx.set_periodic_axes(axes)
     if lattice:
         ctx.set_periodic_bc(True)
     sl, sd, dl, dd, trg = z["sl"], z["sd"], z["dl"], z["dd"], z["trg"]
@@ -167,7 +171,11 @@ def test_cpp_interface_periodic_matches_reference(name):
     else:
         out = ctx.evaluate(sl.reshape(-1), sd.reshape(-1), None, trg.reshape(-1), True)
     err = O.rel_l2(out.reshape(-1), z["out"].reshape(-1))
-    assert err < (1e-10 if lattice or kid == 3 else 1e-12), err
+    # the lattice sums carry the two builds' SVD differences: the operators
+    # differ by ~1e-11, and by 3.6e-9 for the doubly periodic Stokes lattice
+    # (its level sums grow logarithmically and cancel)
+    tol = (1e-8 if kid == 3 and axes == 3 else 1e-10) if lattice else (1e-10 if kid == 3 else 1e-12)
+    assert err < tol, err
     ctx.close()
 
 
