@@ -471,7 +471,7 @@ def roofline(B, peaks):
       P2P + W + D2T pairs) / kernel time, peak = the nominal SIMT peak (148 SMs
       x 128 FP32 or 64 FP64 lanes x 2 flops x max SM clock; the measured peaks
       have no SIMT figure).  Its HBM view is the `hbm` sub-object.
-    Hadamard: the HBM view (the north star's bar for it): algorithmic bytes =
+    Hadamard: the HBM view (the streaming bound it is held to): algorithmic bytes =
       (n_vsrc + n_vtrg) * n3h * 8 children * 2 * rb (input spectra read once,
       output spectra written once) + 26 * n3h * 64 * 2 * rb (operators read
       once) against the measured copy bandwidth; its tensor view (mixed form:
