@@ -2346,15 +2346,29 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
       }
     }
     // equivalent densities (uc UC2UE0) UC2UE1 straight into the leaves' rows of UE
-    ctx.n_launch += 2;
+    ++ctx.n_launch;
     translate_gemm(s, T.n_sleaf, ru, dout, uc, dout, nullptr, ctx.dops.uc2ue0.get<double>(), ru, t1, ru, nullptr,
                    nullptr, false);
-    translate_gemm(s, T.n_sleaf, din, ru, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue, din,
-                   T.sleaf.get<int>(), nullptr, false);
-    if (proj32) {  // (t1 columns 0..r32) (UC2UE1 rows 0..r32) = ue U_k U_k^T of the leaves
+    if (!proj32) {
       ++ctx.n_launch;
-      translate_gemm(s, T.n_sleaf, din, ctx.r32, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue32, din,
+      translate_gemm(s, T.n_sleaf, din, ru, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue, din,
                      T.sleaf.get<int>(), nullptr, false);
+    } else {
+      // the first r32 directions give the leaves' projected rows, ue U_k U_k^T
+      // = (t1 columns 0..r32) (UC2UE1 rows 0..r32); ue adds the other
+      // directions to a copy of them (both arrays are zero outside the
+      // leaves' rows here)
+      const int r32 = ctx.r32;
+      ++ctx.n_launch;
+      translate_gemm(s, T.n_sleaf, din, r32, t1, ru, nullptr, ctx.dops.uc2ue1.get<double>(), din, ue32, din,
+                     T.sleaf.get<int>(), nullptr, false);
+      PVFMM_CUDA_CHECK(cudaMemcpyAsync(ue, ue32, (size_t)N * din * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      if (ru > r32) {
+        ++ctx.n_launch;
+        translate_gemm(s, T.n_sleaf, din, ru - r32, t1 + r32, ru, nullptr,
+                       ctx.dops.uc2ue1.get<double>() + (size_t)r32 * din, din, ue, din, T.sleaf.get<int>(), nullptr,
+                       true);
+      }
     }
   }
   ev(2);
