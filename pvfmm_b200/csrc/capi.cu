@@ -63,7 +63,7 @@ void destroy_context(Context& c) {
                   &T.int_idx, &T.src_perm, &T.trg_perm, &T.src_key, &T.trg_key, &T.src_leaf, &T.trg_leaf, &T.sx,
                   &T.sy, &T.sz, &T.tx, &T.ty, &T.tz, &T.sleaf, &T.tleaf, &T.vsrc, &T.vtrg, &T.node2vsrc, &T.vtab, &T.vmask, &T.vmorton, &T.vunion, &T.vucount, &T.vlocal,
                   &T.xtrg, &T.x_off, &T.x_list, &T.p_off, &T.p_list, &T.w_off, &T.w_list, &T.p_img, &T.x_img,
-                  &T.w_img, &c.dops.bc};
+                  &T.w_img, &c.dops.bc, &c.dops.d2d_f2};
   for (DevBuf* b : tb) b->release();
   if (c.events_ready)
     for (auto& e : c.ev) cudaEventDestroy(e);

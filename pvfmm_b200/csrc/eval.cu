@@ -2445,9 +2445,19 @@ void evaluate_impl(Context& ctx, const void* den_in, const void* dl_in, bool den
   for (int d = 0; d < T.depth; ++d) {
     const long ni = T.n_internal[d];
     if (ni == 0) continue;
-    ++ctx.n_launch;
-    translate_gemm(s, ni, 8 * dout, dout, dc, dout, T.int_idx.get<int>() + T.int_off[d], ctx.dops.d2d.get<double>(),
-                   8 * dout, dc + (size_t)T.level_off[d + 1] * dout, 8 * dout, nullptr, nullptr, true);
+    if (ctx.d2d_factored) {  // (parents' dc DC2DE0) over the kept directions, then DC2DE1 M_pe2c
+      double* tp = ctx.tmp_c.as<double>((size_t)ni * rd);
+      ctx.n_launch += 2;
+      translate_gemm(s, ni, rd, dout, dc, dout, T.int_idx.get<int>() + T.int_off[d], ctx.dops.dc2de0.get<double>(),
+                     rd, tp, rd, nullptr, nullptr, false);
+      translate_gemm(s, ni, 8 * dout, rd, tp, rd, nullptr, ctx.dops.d2d_f2.get<double>(), 8 * dout,
+                     dc + (size_t)T.level_off[d + 1] * dout, 8 * dout, nullptr, nullptr, true);
+    } else {
+      ++ctx.n_launch;
+      translate_gemm(s, ni, 8 * dout, dout, dc, dout, T.int_idx.get<int>() + T.int_off[d],
+                     ctx.dops.d2d.get<double>(), 8 * dout, dc + (size_t)T.level_off[d + 1] * dout, 8 * dout, nullptr,
+                     nullptr, true);
+    }
   }
   ev(8);
   // ---- D2T equivalent densities, then the fused near field
@@ -2666,7 +2676,7 @@ static void upload_vop3_fragments(Context& ctx) {
 // padded to even as well (the translation products take 16-byte rows).
 void compact_factors(const std::vector<double>& c0, const std::vector<double>& c1, int rows, int r, int cols,
                      const std::vector<int>& first, std::vector<double>& o0, std::vector<double>& o1, int* rc,
-                     int* n_first) {
+                     int* n_first, std::vector<int>* order_out = nullptr) {
   std::vector<int> order(first);
   if (order.size() & 1) order.push_back(-1);
   *n_first = (int)order.size();
@@ -2690,6 +2700,7 @@ void compact_factors(const std::vector<double>& c0, const std::vector<double>& c
     for (int i = 0; i < rows; ++i) o0[(size_t)i * n + k] = c0[(size_t)i * r + j];
     std::copy(c1.begin() + (size_t)j * cols, c1.begin() + (size_t)(j + 1) * cols, o1.begin() + (size_t)k * cols);
   }
+  if (order_out) *order_out = std::move(order);
 }
 
 void upload_operators(Context& ctx) {
@@ -2702,11 +2713,24 @@ void upload_operators(Context& ctx) {
     int nf = 0;
     compact_factors(h.uc2ue0, h.uc2ue1, dout, rk, din, proj32 ? h.ue32_dirs : std::vector<int>(), a0, a1, &ctx.ru,
                     &ctx.r32);
-    compact_factors(h.dc2de0, h.dc2de1, dout, rk, din, std::vector<int>(), b0, b1, &ctx.rd, &nf);
+    std::vector<int> dorder;
+    compact_factors(h.dc2de0, h.dc2de1, dout, rk, din, std::vector<int>(), b0, b1, &ctx.rd, &nf, &dorder);
     upload_vec<double>(ctx.dops.uc2ue0, a0, s);
     upload_vec<double>(ctx.dops.uc2ue1, a1, s);
     upload_vec<double>(ctx.dops.dc2de0, b0, s);
     upload_vec<double>(ctx.dops.dc2de1, b1, s);
+    // D2D = DC2DE0 (DC2DE1 M_pe2c): through the rd kept downward directions
+    // the two products take 2 rd dout (1 + 8) flops per parent against
+    // 16 dout^2 for the formed operator (mixed Stokes form: rd = 520 of 1464)
+    ctx.d2d_factored = !h.d2d_f2.empty() && 9L * ctx.rd < 8L * dout;
+    if (ctx.d2d_factored) {
+      std::vector<double> f2((size_t)ctx.rd * 8 * dout, 0.0);
+      for (int k = 0; k < ctx.rd; ++k)
+        if (dorder[k] >= 0)
+          std::copy(h.d2d_f2.begin() + (size_t)dorder[k] * 8 * dout,
+                    h.d2d_f2.begin() + (size_t)(dorder[k] + 1) * 8 * dout, f2.begin() + (size_t)k * 8 * dout);
+      upload_vec<double>(ctx.dops.d2d_f2, f2, s);
+    }
     if (proj32) {
       // U_k (din x r32): the transpose of the first r32 rows of the compacted
       // UC2UE1, so that ue U_k U_k^T is the projection onto those directions

@@ -70,6 +70,7 @@ struct DevOps {
   DevBuf vop_tc5;   // mixed form, ke = 1: Hadamard operators in the tcgen05 shared-memory layout
   DevBuf ue_basis;  // mixed Stokes form: din x r32, the upward directions above the FP32 cutoff
   DevBuf bc;        // periodic boundaries: din x dout, root upward equivalent -> root downward check
+  DevBuf d2d_f2;    // rd x (8 dout): D2D through the kept downward directions (when rd is small)
   DevBuf usurf;     // ns x 3 (Real)
   DevBuf fft_map, ifft_map;
 };
@@ -91,6 +92,7 @@ struct Context {
   // the cutoff kept, padded to even (upward ru, downward rd); the first r32
   // upward ones span the mixed Stokes form's projection (0 otherwise)
   int ru = 0, rd = 0, r32 = 0;
+  bool d2d_factored = false;  // D2D as (dc DC2DE0) d2d_f2 over rd directions
   // periodic boundaries (box_size > 0): points scaled by 1 / box_size and
   // wrapped into the unit cube; bc_lattice selects the lattice-sum operator,
   // bc_user an operator added to the 5x5x5-image one (empty: none)

@@ -70,6 +70,7 @@ struct HostOperators {
   std::vector<double> dc2de0, dc2de1;
   std::vector<double> u2u;              // (8*ns*kin) x (ns*kin), row block c = child octant c
   std::vector<double> d2d;              // (ns*kout) x (8*ns*kout), column block c = child octant c
+  std::vector<double> d2d_f2;           // r x (8*ns*kout): D2D = DC2DE0 * d2d_f2 (DC2DE1 * M_pe2c per block)
   std::vector<double> vop;              // complex (re,im): [n3h][26][8][8][kin][kout]
   std::vector<int> fft_map, ifft_map;   // ns grid indices (x + n1*y + n1*n1*z)
 };

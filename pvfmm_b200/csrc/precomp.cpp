@@ -511,6 +511,7 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
   // U2U (:582-606): (M_ce2c * UC2UE0) * UC2UE1, child c of a level-0 parent.
   ops.u2u.assign((size_t)8 * din * din, 0.0);
   ops.d2d.assign((size_t)dout * 8 * dout, 0.0);
+  ops.d2d_f2.assign((size_t)rk * 8 * dout, 0.0);
   for (int c = 0; c < 8; ++c) {
     const double cc[3] = {((c & 1) ? 0.25 : -0.25), ((c & 2) ? 0.25 : -0.25), ((c & 4) ? 0.25 : -0.25)};
     {
@@ -527,9 +528,13 @@ void build_operators(int kernel, int m, bool mixed, HostOperators& ops, bool dow
       auto cc2 = place_surface(ops.usurf, cc, 0.25, kRad0);
       std::vector<double> M((size_t)din * dout);
       exp_kernel_matrix(ki.exp_kernel, pe.data(), ns, cc2.data(), ns, M.data());
-      auto T = matmul(ops.dc2de0, matmul(ops.dc2de1, M, rk, din, dout), dout, rk, dout);
+      auto F = matmul(ops.dc2de1, M, rk, din, dout);
+      auto T = matmul(ops.dc2de0, F, dout, rk, dout);
       for (int r = 0; r < dout; ++r)
         std::memcpy(&ops.d2d[(size_t)r * 8 * dout + (size_t)c * dout], &T[(size_t)r * dout], sizeof(double) * dout);
+      for (int r = 0; r < rk; ++r)
+        std::memcpy(&ops.d2d_f2[(size_t)r * 8 * dout + (size_t)c * dout], &F[(size_t)r * dout],
+                    sizeof(double) * dout);
     }
   }
   // FFT maps (:2703-2712, :2790-2797): lattice index s = (u+1)(m-1)/2.
