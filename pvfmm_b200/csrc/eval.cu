@@ -2721,8 +2721,10 @@ void upload_operators(Context& ctx) {
     upload_vec<double>(ctx.dops.dc2de1, b1, s);
     // D2D = DC2DE0 (DC2DE1 M_pe2c): through the rd kept downward directions
     // the two products take 2 rd dout (1 + 8) flops per parent against
-    // 16 dout^2 for the formed operator (mixed Stokes form: rd = 520 of 1464)
-    ctx.d2d_factored = !h.d2d_f2.empty() && 9L * ctx.rd < 8L * dout;
+    // 16 dout^2 for the formed operator (mixed Stokes form: rd = 520 of
+    // 1464); taken when that saves a quarter of the flops, since the split
+    // adds a launch and an intermediate per level
+    ctx.d2d_factored = !h.d2d_f2.empty() && 3L * ctx.rd < 2L * dout;
     if (ctx.d2d_factored) {
       std::vector<double> f2((size_t)ctx.rd * 8 * dout, 0.0);
       for (int k = 0; k < ctx.rd; ++k)
